@@ -1,0 +1,215 @@
+/*
+ * relearn_b200 — C ABI of the B200 structural-plasticity hot path.
+ *
+ * One context holds one network on one GPU: neuron positions and signal
+ * types, the linear octree over them, the Izhikevich / calcium / synaptic
+ * element state, the synapse list and the scratch the kernels need.  All
+ * arrays crossing this boundary are caller-owned HOST buffers with plain
+ * pointers and sizes; the context owns all device memory.  No C++ types and
+ * no exceptions cross the boundary: every entry point returns an rl_status,
+ * and rl_last_error() gives a message for the last failing call.
+ *
+ * Threading: a context is used by one host thread at a time (not
+ * re-entrant); several contexts may share a device.
+ *
+ * The entry points replace the following reference interfaces (paths relative
+ * to relearn/source in tuda-hpclab/relearn):
+ *   Algorithm (algorithm/Algorithm.h:48-197) selected by --algorithm barnes-hut
+ *     init(n)                        -> rl_set_positions
+ *     prepare_update_connectivity    -> rl_prepare_update_connectivity
+ *     update_connectivity(n)         -> rl_update_connectivity
+ *   NeuronModel (neurons/models/NeuronModelBase.h) selected by
+ *   --neuron-model izhikevich, with CalciumCalculator and SynapticElements
+ *   as driven by Neurons (neurons/Neurons.cpp:351-384)
+ *     update_electrical_activity + update_calcium + update_number_elements
+ *                                    -> rl_activity_block
+ *   Neurons::update_connectivity (neurons/Neurons.cpp:588-608)
+ *                                    -> rl_plasticity_update
+ *   Simulation::simulate (sim/Simulation.cpp:388-480) -> rl_simulate
+ */
+#ifndef RELEARN_B200_H
+#define RELEARN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RL_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RL_API __attribute__((visibility("default")))
+#else
+#define RL_API
+#endif
+
+typedef enum rl_status {
+    RL_OK = 0,
+    RL_ERR_INVALID = 1,   /* bad argument, size or state (RelearnException::check) */
+    RL_ERR_OOM = 2,       /* device allocation failed */
+    RL_ERR_DEVICE = 3,    /* CUDA runtime error, or no usable device */
+    RL_ERR_TIMEOUT = 4,   /* a bounded device wait ran out */
+    RL_ERR_OVERFLOW = 5,  /* a fixed-capacity device structure overflowed */
+    RL_ERR_UNSUPPORTED = 6 /* configuration outside what this build implements */
+} rl_status;
+
+/* Element types, in the reference's order (SynapticElementType). */
+enum { RL_AXON = 0, RL_DENDRITE_EXC = 1, RL_DENDRITE_INH = 2 };
+
+/* Signal types (SignalType): 0 excitatory, 1 inhibitory. */
+enum { RL_EXCITATORY = 0, RL_INHIBITORY = 1 };
+
+/* Parameters of one network.  Defaults of the reference are given in
+ * brackets; rl_config_default() fills them. */
+typedef struct rl_config {
+    uint32_t num_neurons;
+    uint32_t plasticity_interval; /* [100] Config::plasticity_update_step */
+    uint32_t h_model;             /* [10] Euler substeps of the neuron model */
+    uint32_t h_calcium;           /* [10] Euler substeps of the calcium */
+    uint64_t seed;                /* key of the Philox stream */
+    double box_min[3];            /* simulation box (root cell) */
+    double box_max[3];
+    double theta;                 /* [0.3] Barnes-Hut acceptance criterion, (0, 0.5] */
+    double sigma;                 /* [750] Gaussian kernel sigma (um) */
+    double mu;                    /* [0] Gaussian kernel offset */
+    double iz_a, iz_b, iz_c, iz_d, iz_v_spike, iz_k1, iz_k2, iz_k3;
+    double beta;                  /* [0.001] calcium increase per spike */
+    double tau_c;                 /* [10000] calcium decay time */
+    double target_calcium;        /* [0.7] */
+    double initial_calcium;       /* [0] */
+    double growth_rate[3];        /* [1e-4] nu per element type */
+    double min_calcium[3];        /* eta per element type [0.4, 0.1, 0.0] */
+    double retract_ratio[3];      /* [0] vacant retract ratio per element type */
+    double conductance;           /* synaptic_equally_weighted conductance */
+    double noise_mean;            /* normal background input mean */
+    double noise_stddev;          /* normal background input stddev */
+    int32_t device;               /* CUDA device ordinal */
+    int32_t reserved;
+} rl_config;
+
+/* One synapse creation request (SynapseCreationRequest,
+ * neurons/helper/SynapseCreationRequests.h) plus the vacant-axon index j. */
+typedef struct rl_request {
+    uint32_t target;
+    uint32_t source;
+    uint32_t j;
+    uint32_t signal;
+} rl_request;
+
+/* One synapse: target (dendrite side), source (axon side), weight +1/-1. */
+typedef struct rl_synapse {
+    uint32_t target;
+    uint32_t source;
+    int32_t weight;
+    uint32_t reserved;
+} rl_synapse;
+
+/* Counters accumulated by a context. */
+typedef struct rl_stats {
+    uint64_t searches;           /* single-element Barnes-Hut searches run */
+    uint64_t requests;           /* requests emitted by the searches */
+    uint64_t synapses_created;   /* requests accepted by the connector */
+    uint64_t bound_to_delete;    /* bound elements the commits asked to delete */
+    uint64_t activity_steps;     /* activity steps run */
+    uint64_t plasticity_updates; /* plasticity updates run */
+    uint64_t gpu_launches;       /* kernels this library launched */
+    uint64_t num_nodes;          /* octree nodes */
+    uint32_t max_level;          /* deepest octree level */
+    uint32_t reserved;
+} rl_stats;
+
+/* Fill *cfg with the reference defaults for n neurons in the given cube. */
+RL_API void rl_config_default(rl_config* cfg, uint32_t num_neurons, double side);
+
+/* Create a context for cfg->num_neurons neurons on cfg->device. */
+RL_API rl_status rl_ctx_create(const rl_config* cfg, void** ctx);
+RL_API rl_status rl_ctx_destroy(void* ctx);
+RL_API const char* rl_last_error(void* ctx);
+RL_API const char* rl_status_string(rl_status s);
+RL_API int32_t rl_abi_version(void);
+
+/* Algorithm::init / OctreeAlgorithm::init (algorithm/Internal/OctreeAlgorithm.h:58-67):
+ * positions (N x 3 doubles, row-major) and signal types (N bytes); builds the
+ * octree on the device (Morton keys, radix sort, PR-octree).  Positions must
+ * lie in the configured box and be pairwise distinct. */
+RL_API rl_status rl_set_positions(void* ctx, const double* xyz, const uint8_t* signal);
+
+/* Octree size after rl_set_positions. */
+RL_API rl_status rl_tree_info(void* ctx, uint64_t* num_nodes, uint32_t* max_level);
+
+/* Canonical dump of the octree in breadth-first order (root, then level by
+ * level, children in octant order): level, neuron id (-1 for inner nodes),
+ * child mask, index of the first child (-1 for leaves), cell box (x3),
+ * vacant dendrite counts and their positions (x3, NaN when absent).
+ * Every pointer may be NULL to skip that field. */
+RL_API rl_status rl_dump_tree(void* ctx, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax,
+                       uint32_t* cnt_exc, uint32_t* cnt_inh, double* pos_exc, double* pos_inh);
+
+/* Algorithm::prepare_update_connectivity (algorithm/Algorithm.h) ->
+ * OctreeAlgorithm::update_tree (algorithm/Internal/OctreeAlgorithm.h:100-238):
+ * stores the vacant axon counts for the next search, writes the vacant
+ * dendrite counts into the leaves and reduces counts and centroids bottom-up.
+ * `update` (nullable) marks neurons that take part in plasticity. */
+RL_API rl_status rl_prepare_update_connectivity(void* ctx, const uint8_t* signal, const uint32_t* vacant_axons, const uint32_t* vacant_exc,
+                                         const uint32_t* vacant_inh, const uint8_t* update);
+
+/* The search half of Algorithm::update_connectivity
+ * (BarnesHut::find_target_neurons, algorithm/BarnesHutInternal/BarnesHut.cpp:36-94):
+ * one Barnes-Hut search per vacant axon element; returns the requests in
+ * (source, j) order.  *count receives the number of requests; at most
+ * `capacity` are copied to out (out may be NULL). */
+RL_API rl_status rl_find_targets(void* ctx, uint32_t step, rl_request* out, uint64_t capacity, uint64_t* count);
+
+/* Algorithm::update_connectivity (algorithm/Internal/ExchangingAlgorithm.h:58-87):
+ * search, then the connector (algorithm/Connector.cpp:33-197).  Connects
+ * elements in the context's own element state, appends the synapses to the
+ * context's synapse list and returns them (accepted requests, in connector
+ * order).  *created receives their number. */
+RL_API rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* out, uint64_t capacity, uint64_t* created);
+
+/* Synaptic-element state per type (RL_AXON, RL_DENDRITE_EXC, RL_DENDRITE_INH):
+ * grown (double), delta since the last commit (double), connected and vacant
+ * counts (uint32).  NULL pointers are skipped. */
+RL_API rl_status rl_set_elements(void* ctx, int type, const double* grown, const double* delta, const uint32_t* connected, const uint32_t* vacant);
+RL_API rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uint32_t* connected, uint32_t* vacant);
+
+/* Neuron state: membrane potential x, recovery u, calcium, fired flag of the
+ * last step, and the input of the last step.  NULL pointers are skipped. */
+RL_API rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const double* calcium, const uint8_t* fired);
+RL_API rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input);
+
+/* Enable flags (NeuronsExtraInfo disable flags): 1 enabled, 0 disabled. */
+RL_API rl_status rl_set_enabled(void* ctx, const uint8_t* enabled);
+
+/* Synapse list (NetworkGraph plastic edges).  rl_get_edges aggregates equal
+ * (target, source) pairs, drops zero weights and sorts by (target, source);
+ * *count receives the number of aggregated edges. */
+RL_API rl_status rl_add_edges(void* ctx, uint64_t m, const uint32_t* target, const uint32_t* source, const int32_t* weight);
+RL_API rl_status rl_get_edges(void* ctx, uint32_t* target, uint32_t* source, int32_t* weight, uint64_t capacity, uint64_t* count);
+
+/* Activity steps first_step .. first_step+nsteps-1 without plasticity:
+ * input (synaptic_equally_weighted + normal), Izhikevich, calcium, growth
+ * deltas — one fused kernel per step (NeuronModelCPU::update_electrical_activity,
+ * CalciumCalculatorCPU::update_calcium, SynapticElementsCPU::update_number_elements). */
+RL_API rl_status rl_activity_block(void* ctx, uint32_t first_step, uint32_t nsteps);
+
+/* One plasticity update at `step` (Neurons::update_connectivity): commit of
+ * the three element types, tree update, search, connector, graph rebuild. */
+RL_API rl_status rl_plasticity_update(void* ctx, uint32_t step);
+
+/* Simulation::simulate over steps first_step .. first_step+nsteps-1: one
+ * activity step each, a plasticity update when step % interval == 0. */
+RL_API rl_status rl_simulate(void* ctx, uint32_t first_step, uint32_t nsteps);
+
+/* Block until all work of the context has finished. */
+RL_API rl_status rl_synchronize(void* ctx);
+
+RL_API rl_status rl_get_stats(void* ctx, rl_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RELEARN_B200_H */

@@ -1,0 +1,214 @@
+// ORACLE — test infrastructure only.  Not part of the product; only tests/,
+// __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
+//
+// Oracle-side statement of the injected random stream and of the arithmetic
+// that both sides must evaluate identically:
+//   * Philox4x32-10 (Salmon et al., SC'11) keyed on
+//     (seed, step, neuron, sub-index, stream, depth); replaces RandomHolder
+//     (relearn/source/util/Random.h:70-284) at ProbabilityPicker.h:108-109,
+//     Connector.cpp:71 and NormalActivityInputCPU.cpp:35.
+//   * exp / log written from the mathematics (Cody-Waite reduction, Taylor and
+//     atanh series) standing in for glibc's std::exp (Gaussian.h:66,
+//     GrowthCurves.h:51); set use_libm to evaluate std::exp / std::log instead.
+//   * hypot of three arguments as libstdc++ evaluates it
+//     (Vec3.hpp:549-551 -> std::hypot(x, y, z)).
+//   * Wichura AS241 normal quantile for the background input.
+// Build with -ffp-contract=off: no multiply-add contraction.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+namespace oracle {
+
+inline uint64_t bits_of(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return u;
+}
+inline double from_bits(uint64_t u) {
+    double x;
+    std::memcpy(&x, &u, 8);
+    return x;
+}
+
+struct Words {
+    uint32_t w[4];
+};
+
+inline Words philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+    uint32_t c[4] = { c0, c1, c2, c3 };
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c[0] = n0;
+        c[1] = n1;
+        c[2] = n2;
+        c[3] = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return Words{ { c[0], c[1], c[2], c[3] } };
+}
+
+enum : uint32_t { S_BH = 1, S_CONNECT = 2, S_NOISE = 3, S_DELETE = 4 };
+
+inline Words stream_draw(uint64_t seed, uint32_t step, uint32_t neuron, uint32_t sub, uint32_t stream, uint32_t depth) {
+    return philox(step, neuron, sub, (stream << 24) | (depth & 0xFFFFFFu), (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+inline uint64_t take53(const Words& r) {
+    return ((uint64_t)r.w[0] << 21) | (uint64_t)(r.w[1] >> 11);
+}
+inline double unit_closed_open(const Words& r) {
+    return (double)take53(r) * 0x1.0p-53;
+}
+inline double unit_open(const Words& r) {
+    return ((double)take53(r) + 0.5) * 0x1.0p-53;
+}
+inline uint64_t take64(const Words& r) {
+    return ((uint64_t)r.w[0] << 32) | (uint64_t)r.w[1];
+}
+
+// ---- exp: exp(x) = 2^k exp(r), |r| <= ln2/2
+inline double times_pow2(double y, int k) {
+    if (k > 1023) {
+        y *= from_bits((uint64_t)(2046) << 52);
+        k -= 1023;
+        if (k > 1023) {
+            k = 1023;
+        }
+        return y * from_bits((uint64_t)(k + 1023) << 52);
+    }
+    if (k < -1021) {
+        const double t = y * from_bits((uint64_t)(k + 54 + 1023) << 52);
+        return t * from_bits((uint64_t)(1023 - 54) << 52);
+    }
+    return y * from_bits((uint64_t)(k + 1023) << 52);
+}
+
+inline double own_exp(double x) {
+    if (std::isnan(x)) {
+        return x;
+    }
+    if (x > 709.782712893384) {
+        return HUGE_VAL;
+    }
+    if (x < -745.1332191019412) {
+        return 0.0;
+    }
+    const double ln2_hi = 0.6931467056274414;      // ln 2, low 32 mantissa bits cleared
+    const double ln2_lo = 4.7493250390316726e-07;  // ln 2 - ln2_hi
+    const double k = std::floor(x * 1.4426950408889634 + 0.5);
+    const double r = (x - k * ln2_hi) - k * ln2_lo;
+    // 1/n! for n = 13 .. 2
+    static const double inv_fact[12] = { 1.6059043836821614599e-10, 2.0876756987868098979e-09, 2.5052108385441718775e-08,
+                                         2.7557319223985890653e-07, 2.7557319223985890653e-06, 2.4801587301587301587e-05,
+                                         1.9841269841269841270e-04, 1.3888888888888888889e-03, 8.3333333333333333333e-03,
+                                         4.1666666666666666667e-02, 1.6666666666666666667e-01, 0.5 };
+    double p = inv_fact[0];
+    for (int i = 1; i < 12; ++i) {
+        p = p * r + inv_fact[i];
+    }
+    const double y = 1.0 + (r + (r * r) * p);
+    return times_pow2(y, (int)k);
+}
+
+inline double own_log(double x) {
+    const uint64_t b = bits_of(x);
+    int e = (int)((b >> 52) & 0x7FF) - 1023;
+    double m = from_bits((b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull);
+    if (m > 1.4142135623730951) {
+        m *= 0.5;
+        e += 1;
+    }
+    const double f = m - 1.0;
+    const double s = f / (2.0 + f);
+    const double z = s * s;
+    double R = 1.0 / 23.0;
+    for (int d = 21; d >= 3; d -= 2) {
+        R = R * z + 1.0 / (double)d;
+    }
+    R = R * z;
+    const double two_s = 2.0 * s;
+    const double logm = two_s + two_s * R;
+    const double ed = (double)e;
+    return ed * 0.6931467056274414 + (logm + ed * 4.7493250390316726e-07);
+}
+
+// libstdc++ <cmath> three-argument hypot: a = max(|x|,|y|,|z|),
+// a * sqrt((x/a)^2 + (y/a)^2 + (z/a)^2).
+inline double hypot3(double x, double y, double z) {
+    x = std::fabs(x);
+    y = std::fabs(y);
+    z = std::fabs(z);
+    const double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+    if (a == 0.0) {
+        return 0.0;
+    }
+    return a * std::sqrt((x / a) * (x / a) + (y / a) * (y / a) + (z / a) * (z / a));
+}
+
+// AS241 (Wichura 1988) normal quantile; `lg` is the log to use.
+template <typename Log>
+inline double as241(double p, Log lg) {
+    const double q = p - 0.5;
+    if (std::fabs(q) <= 0.425) {
+        const double r = 0.180625 - q * q;
+        static const double A[8] = { 2.5090809287301226727e+3, 3.3430575583588128105e+4, 6.7265770927008700853e+4, 4.5921953931549871457e+4,
+                                     1.3731693765509461125e+4, 1.9715909503065514427e+3, 1.3314166789178437745e+2, 3.3871328727963666080e+0 };
+        static const double B[8] = { 5.2264952788528545610e+3, 2.8729085735721942674e+4, 3.9307895800092710610e+4, 2.1213794301586595867e+4,
+                                     5.3941960214247511077e+3, 6.8718700749205790830e+2, 4.2313330701600911252e+1, 1.0 };
+        double num = A[0];
+        double den = B[0];
+        for (int i = 1; i < 8; ++i) {
+            num = num * r + A[i];
+        }
+        for (int i = 1; i < 8; ++i) {
+            den = den * r + B[i];
+        }
+        return (num * q) / den;
+    }
+    double r = q < 0.0 ? p : 1.0 - p;
+    r = std::sqrt(-lg(r));
+    double num;
+    double den;
+    if (r <= 5.0) {
+        r = r - 1.6;
+        static const double C[8] = { 7.7454501427834140764e-4, 2.2723844989269184583e-2, 2.4178072517745061177e-1, 1.2704582524523683826e+0,
+                                     3.6478483247632046050e+0, 5.7694972214606914055e+0, 4.6303378461565452959e+0, 1.4234371107496835773e+0 };
+        static const double D[8] = { 1.0507500716444168432e-9, 5.4759380849953449460e-4, 1.5198666563616457197e-2, 1.4810397642748007459e-1,
+                                     6.8976733498510000455e-1, 1.6763848301838038494e+0, 2.0531916266377588219e+0, 1.0 };
+        num = C[0];
+        den = D[0];
+        for (int i = 1; i < 8; ++i) {
+            num = num * r + C[i];
+        }
+        for (int i = 1; i < 8; ++i) {
+            den = den * r + D[i];
+        }
+    } else {
+        r = r - 5.0;
+        static const double E[8] = { 2.0103343992922881327e-7, 2.7115555687434875782e-5, 1.2426609473880784386e-3, 2.6532189526576123093e-2,
+                                     2.9656057182850489123e-1, 1.7848265399172913358e+0, 5.4637849111641143699e+0, 6.6579046435011037772e+0 };
+        static const double F[8] = { 2.0442631033899397856e-15, 1.4215117583164458887e-7, 1.8463183175100546818e-5, 7.8686913114561325910e-4,
+                                     1.4875361290850614853e-2, 1.3692988092273580531e-1, 5.9983220655588793769e-1, 1.0 };
+        num = E[0];
+        den = F[0];
+        for (int i = 1; i < 8; ++i) {
+            num = num * r + E[i];
+        }
+        for (int i = 1; i < 8; ++i) {
+            den = den * r + F[i];
+        }
+    }
+    const double x = num / den;
+    return q < 0.0 ? -x : x;
+}
+
+}  // namespace oracle

@@ -1,0 +1,255 @@
+// Fused activity step (input + Izhikevich + calcium + growth) and the commit
+// of the synaptic elements at a plasticity update.
+//
+// Reference semantics (relearn/source/neurons), one rank, in the order of
+// Simulation::simulate (sim/Simulation.cpp:443-453):
+//   * CombinedActivityInputCPU::update_input_range: input = 0; += synaptic; += normal
+//     - SynapticEquallyWeightedActivityInputCPU::update_local_input
+//       (input/SynapticEquallyWeightedActivityInputCPU.cpp:21-48):
+//       conductance * sum of the weights of in-edges whose source fired in the
+//       previous step (an integer sum, exact in any order)
+//     - NormalActivityInputCPU::update_input_range (input/NormalActivityInputCPU.cpp:21-39)
+//   * IzhikevichModelCPU::update_activity (models/izhikevich/IzhikevichModelCPU.cpp:75-125)
+//   * CalciumCalculatorCPU::update_current_calcium (calcium/CalciumCalculatorCPU.cpp:40-103)
+//   * update_number_elements_openmp + gaussian_growth_curve
+//     (synaptic_elements/SynapticElementsCPU.cpp:25-49, GrowthCurves.h:30-53)
+//   * ElementBaseBase::update (synaptic_elements/ElementBaseBase.h:420-481) at a
+//     plasticity update.
+// All state is structure-of-arrays in HBM; one thread per neuron reads and
+// writes each of its words once per step.
+#include "rl_context.cuh"
+#include "rl_math.cuh"
+
+namespace rl {
+namespace {
+
+struct ActArgs {
+    uint32_t n;
+    uint32_t step;
+    uint64_t seed;
+    const uint8_t* enabled;
+    const uint32_t* csr_off;
+    const uint32_t* csr_src;
+    const int32_t* csr_w;
+    const uint8_t* fired_prev;
+    uint8_t* fired_cur;
+    double* x;
+    double* u;
+    double* calcium;
+    const double* target;
+    double* input;
+    double* delta0;
+    double* delta1;
+    double* delta2;
+    double conductance, noise_mean, noise_stddev;
+    uint32_t h_model, h_calcium;
+    double a, ab, c, d, v_spike, k1, k2, k3, scale_m;
+    double beta, tau_inv, scale_c;
+    double eta[3], nu[3];
+    int has_edges;
+};
+
+__device__ __forceinline__ double growth_curve(double current, double eta, double eps) {
+    if (eta == eps) {
+        return current == eta ? 0.0 : -1.0;
+    }
+    const double factor_inv = 1.0 / 1.6651092223153955127063292897904020952611777045288814583336582344;
+    const double xi = (eta + eps) * 0.5;
+    const double zeta = (eta - eps) * factor_inv;
+    const double diff = current - xi;
+    const double quot = diff / zeta;
+    const double prod = quot * quot;
+    return (2.0 * rl_exp(-prod)) - 1.0;
+}
+
+__global__ void __launch_bounds__(256) k_activity(ActArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    if (!A.enabled[i]) {
+        A.input[i] = 0.0;
+        A.fired_cur[i] = A.fired_prev[i];
+        A.delta0[i] = A.delta0[i] + 0.0;
+        A.delta1[i] = A.delta1[i] + 0.0;
+        A.delta2[i] = A.delta2[i] + 0.0;
+        return;
+    }
+    long long isum = 0;
+    if (A.has_edges) {
+        const uint32_t e0 = A.csr_off[i], e1 = A.csr_off[i + 1];
+        for (uint32_t e = e0; e < e1; ++e) {
+            if (A.fired_prev[A.csr_src[e]]) {
+                isum += A.csr_w[e];
+            }
+        }
+    }
+    double input = 0.0;
+    input += (double)isum * A.conductance;
+    input += background_normal(A.seed, A.step, i, A.noise_mean, A.noise_stddev);
+    A.input[i] = input;
+
+    double xv = A.x[i];
+    double uv = A.u[i];
+    uint8_t spiked = 0;
+    for (uint32_t it = 0; it < A.h_model; ++it) {
+        const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
+        const double u_inc = (A.ab * xv) - (A.a * uv);
+        xv += x_inc * A.scale_m;
+        uv += u_inc * A.scale_m;
+        if (xv >= A.v_spike) {
+            xv = A.c;
+            uv += A.d;
+            spiked = 1;
+            break;
+        }
+    }
+    A.x[i] = xv;
+    A.u[i] = uv;
+    A.fired_cur[i] = spiked;
+
+    double ca = A.calcium[i];
+    const double local_beta = A.beta * (double)(spiked ? 1 : 0);
+    for (uint32_t it = 0; it < A.h_calcium; ++it) {
+        ca += A.scale_c * (ca * A.tau_inv + local_beta);
+    }
+    A.calcium[i] = ca;
+
+    const double tgt = A.target[i];
+    double* deltas[3] = { A.delta0, A.delta1, A.delta2 };
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const double eta = A.eta[t];
+        const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
+        const double inc = growth_curve(ca, eta, eps) * A.nu[t];
+        deltas[t][i] = deltas[t][i] + inc;
+    }
+}
+
+struct CommitArgs {
+    uint32_t n;
+    const uint8_t* enabled;
+    double* grown[3];
+    double* delta[3];
+    uint32_t* connected[3];
+    uint32_t* vacant[3];
+    double retract[3];
+    unsigned long long* to_delete;
+};
+
+__global__ void k_commit(CommitArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n || !A.enabled[i]) {
+        return;
+    }
+    uint32_t del_total = 0;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const double current_count = A.grown[t][i];
+        const double current_delta = A.delta[t][i];
+        const uint32_t conn_int = A.connected[t][i];
+        const double conn = (double)conn_int;
+        const double current_vacant = current_count - conn;
+        const double new_vacant = current_vacant + current_delta;
+        const double keep = 1.0 - A.retract[t];
+        if (new_vacant >= 0.0) {
+            const double after = keep * new_vacant;
+            A.grown[t][i] = after + conn;
+            A.delta[t][i] = 0.0;
+            A.vacant[t][i] = (uint32_t)after;
+        } else if (current_count + current_delta <= 0.0) {
+            A.grown[t][i] = 0.0;
+            A.delta[t][i] = 0.0;
+            A.vacant[t][i] = 0u;
+            A.connected[t][i] = 0u;
+            del_total += conn_int;
+        } else {
+            const double new_count = current_count + current_delta;
+            const double new_conn = floor(new_count);
+            const double num_vacant = new_count - new_conn;
+            A.grown[t][i] = (keep * num_vacant) + new_conn;
+            A.delta[t][i] = 0.0;
+            A.vacant[t][i] = 0u;
+            A.connected[t][i] = (uint32_t)new_conn;
+            del_total += (uint32_t)(conn - new_conn);
+        }
+    }
+    if (del_total) {
+        atomicAdd(A.to_delete, (unsigned long long)del_total);
+    }
+}
+
+}  // namespace
+
+void run_activity_step(Ctx& c, uint32_t step) {
+    const rl_config& k = c.cfg;
+    ActArgs A;
+    A.n = c.n;
+    A.step = step;
+    A.seed = k.seed;
+    A.enabled = c.nr.enabled.p;
+    A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
+    A.csr_off = c.graph.offsets.p;
+    A.csr_src = c.graph.src.p;
+    A.csr_w = c.graph.weight.p;
+    A.fired_prev = c.nr.fired[c.nr.cur].p;
+    A.fired_cur = c.nr.fired[c.nr.cur ^ 1].p;
+    A.x = c.nr.x.p;
+    A.u = c.nr.u.p;
+    A.calcium = c.nr.calcium.p;
+    A.target = c.nr.target.p;
+    A.input = c.nr.input.p;
+    A.delta0 = c.nr.delta[0].p;
+    A.delta1 = c.nr.delta[1].p;
+    A.delta2 = c.nr.delta[2].p;
+    A.conductance = k.conductance;
+    A.noise_mean = k.noise_mean;
+    A.noise_stddev = k.noise_stddev;
+    A.h_model = k.h_model;
+    A.h_calcium = k.h_calcium;
+    A.a = k.iz_a;
+    A.ab = k.iz_a * k.iz_b;
+    A.c = k.iz_c;
+    A.d = k.iz_d;
+    A.v_spike = k.iz_v_spike;
+    A.k1 = k.iz_k1;
+    A.k2 = k.iz_k2;
+    A.k3 = k.iz_k3;
+    A.scale_m = 1.0 / (double)k.h_model;
+    A.beta = k.beta;
+    A.tau_inv = -1.0 / k.tau_c;
+    A.scale_c = 1.0 / (double)k.h_calcium;
+    for (int t = 0; t < 3; ++t) {
+        A.eta[t] = k.min_calcium[t];
+        A.nu[t] = k.growth_rate[t];
+    }
+    k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
+    RL_LAUNCH_CHECK();
+    c.nr.cur ^= 1;
+    c.stats.activity_steps += 1;
+}
+
+uint64_t run_commit(Ctx& c) {
+    CommitArgs A;
+    A.n = c.n;
+    A.enabled = c.nr.enabled.p;
+    for (int t = 0; t < 3; ++t) {
+        A.grown[t] = c.nr.grown[t].p;
+        A.delta[t] = c.nr.delta[t].p;
+        A.connected[t] = c.nr.connected[t].p;
+        A.vacant[t] = c.nr.vacant[t].p;
+        A.retract[t] = c.cfg.retract_ratio[t];
+    }
+    unsigned long long* d_del = reinterpret_cast<unsigned long long*>(c.counters.p) + 1;
+    RL_CUDA_TRY(cudaMemsetAsync(d_del, 0, sizeof(unsigned long long), c.stream));
+    A.to_delete = d_del;
+    k_commit<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
+    RL_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&h, d_del, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    c.stats.bound_to_delete += h;
+    return h;
+}
+
+}  // namespace rl

@@ -1,0 +1,534 @@
+// Barnes-Hut target search: one search per vacant axon element.
+//
+// Reference semantics (relearn/source/algorithm):
+//   BarnesHut::find_target_neurons (BarnesHutInternal/BarnesHut.cpp:36-94),
+//   BarnesHutBase::find_target_neurons / find_target_neuron /
+//   get_nodes_to_consider / test_acceptance_criterion (BarnesHutBase.h:72-298),
+//   Kernel::pick_target / create_probability_interval (Kernel/Kernel.h:61-173),
+//   GaussianDistributionKernel::get_probability (Kernel/Gaussian.h:62-68),
+//   ProbabilityPicker::pick_target (util/ProbabilityPicker.h:46-112).
+//
+// A descent collects candidates by a depth-first walk that visits the
+// children of every expanded node in descending octant order (the
+// reference's LIFO stack), sums their weights in that order, draws
+// r in [0, nextafter(total)) and picks the first candidate whose running sum
+// reaches r.  Bit-exactness needs the same candidate order and the same
+// sequential FP64 additions, so every sum here is a per-lane sequential sum in
+// that order.
+//
+// Work split on the GPU:
+//   * The descent from the root (about 3,000 candidates per search at 1M
+//     neurons) runs as a warp packet: the 32 lanes are 32 searches whose
+//     sources are adjacent in Morton order; the warp walks one shared
+//     depth-first stack, a node is expanded when any lane expands it, and each
+//     lane evaluates and sums only the nodes it would visit itself.  Node
+//     records are loaded once per warp (broadcast).  The running sum at the
+//     start of every child subtree of the root is kept as a checkpoint, so the
+//     pick re-walks a single root-child subtree per lane instead of the whole
+//     candidate list.
+//   * Deeper descents (a handful of candidates) run per lane: a sum pass and a
+//     pick pass over the chosen node's subtree.
+#include "rl_context.cuh"
+#include "rl_math.cuh"
+
+namespace rl {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kStackDepth = kMaxLevels + 4;
+
+enum : int { ST_DISCARD = 0, ST_EXPAND = 1, ST_ACCEPT = 2 };
+
+struct SearchArgs {
+    const double4* rec;  // records of the searched dendrite type
+    const uint2* topo;
+    const double* maxdim;
+    const double *px, *py, *pz;
+    const uint32_t* list_src;
+    const uint32_t* list_j;
+    uint64_t begin, end;  // segment of the search list
+    int32_t* target;
+    double theta, mu, scale;
+    uint64_t seed;
+    uint32_t step;
+    uint32_t* err;
+    unsigned long long* touched;
+};
+
+__device__ __forceinline__ uint32_t rcount(const double4& r) {
+    return (uint32_t)__double_as_longlong(r.w);
+}
+
+struct Eval {
+    int status;
+    double w;
+};
+
+// test_acceptance_criterion + calculate_attractiveness_to_connect for one node.
+__device__ __forceinline__ Eval evaluate(const double4& r, uint2 t, double md, double sx, double sy, double sz, uint32_t source, double theta, double mu,
+                                         double scale, bool fallback) {
+    Eval e{ ST_DISCARD, 0.0 };
+    const uint32_t cnt = rcount(r);
+    if (cnt == 0) {
+        return e;
+    }
+    const double d = rl_hypot3(r.x - sx, r.y - sy, r.z - sz);
+    if (d == 0.0) {
+        return e;
+    }
+    const bool leaf = topo_leaf(t.y);
+    if (!leaf && !(md < theta * d)) {
+        e.status = ST_EXPAND;
+        return e;
+    }
+    e.status = ST_ACCEPT;
+    if (leaf && t.x == source) {
+        e.w = 0.0;  // a neuron never connects to itself
+    } else if (!fallback) {
+        const double num = (d - mu) * (d - mu);
+        e.w = (rl_exp(num * scale) * 1.0) * (double)cnt;
+    } else {
+        e.w = (double)cnt / d;
+    }
+    return e;
+}
+
+__device__ __forceinline__ uint32_t child_index(uint2 t, int octant) {
+    return t.x + (uint32_t)__popc(topo_mask(t.y) & ((1u << octant) - 1u));
+}
+
+// Random number of ProbabilityPicker::pick_target(values, key) for a total.
+__device__ __forceinline__ double pick_threshold(double total, uint64_t seed, uint32_t step, uint32_t source, uint32_t j, uint32_t depth) {
+    const double next = next_up_eps(total);
+    const u32x4 w = draw(seed, step, source, j, STREAM_BH_PICK, depth);
+    double r = uniform01(w) * next;
+    if (r >= next) {
+        r = total;
+    }
+    if (!(r > 0.0)) {
+        r = 4.9406564584124654e-324;  // r == 0 picks the first positive weight
+    }
+    return r;
+}
+
+// Per-lane depth-first walk below `sub` (not evaluating `sub` itself when
+// `include_root` is false).  Mode 0 sums all weights; mode 1 stops at the first
+// candidate whose running sum reaches r and returns it.
+struct WalkResult {
+    double sum;
+    int32_t picked;  // node index in pick mode, -1 otherwise
+    uint32_t touched;
+    bool overflow;
+};
+
+__device__ WalkResult lane_walk(const SearchArgs& A, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r, double sx, double sy,
+                                double sz, uint32_t source, bool fallback) {
+    WalkResult res{ start_sum, -1, 0, false };
+    uint32_t fnode[kStackDepth];
+    uint32_t frem[kStackDepth];
+    int depth = 0;
+    if (include_root) {
+        const double4 rr = ldg4(&A.rec[sub]);
+        const uint2 tt = __ldg(&A.topo[sub]);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+        ++res.touched;
+        if (e.status == ST_ACCEPT) {
+            res.sum += e.w;
+            if (pick_mode && res.sum >= r) {
+                res.picked = (int32_t)sub;
+            }
+            return res;
+        }
+        if (e.status == ST_DISCARD) {
+            return res;
+        }
+    }
+    {
+        const uint2 tt = __ldg(&A.topo[sub]);
+        fnode[0] = sub;
+        frem[0] = topo_mask(tt.y);
+        depth = 1;
+    }
+    while (depth > 0) {
+        const int top = depth - 1;
+        const uint32_t rem = frem[top];
+        if (rem == 0) {
+            --depth;
+            continue;
+        }
+        const int oct = 31 - __clz(rem);
+        frem[top] = rem & ~(1u << oct);
+        const uint2 pt = __ldg(&A.topo[fnode[top]]);
+        const uint32_t child = child_index(pt, oct);
+        const double4 rr = ldg4(&A.rec[child]);
+        const uint2 tt = __ldg(&A.topo[child]);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+        ++res.touched;
+        if (e.status == ST_ACCEPT) {
+            res.sum += e.w;
+            if (pick_mode && res.sum >= r) {
+                res.picked = (int32_t)child;
+                return res;
+            }
+        } else if (e.status == ST_EXPAND) {
+            if (depth >= kStackDepth) {
+                res.overflow = true;
+                return res;
+            }
+            fnode[depth] = child;
+            frem[depth] = topo_mask(tt.y);
+            ++depth;
+        }
+    }
+    return res;
+}
+
+// Warp-packet walk over the whole tree for the lanes in `lanes`; each lane
+// returns its sequential sum and the running sum before every root child.
+__device__ double packet_walk(const SearchArgs& A, uint32_t lanes, double sx, double sy, double sz, uint32_t source, bool fallback, double* cp_lane,
+                              uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
+    const int lane = threadIdx.x & 31;
+    const bool me = (lanes >> lane) & 1u;
+    double sum = 0.0;
+    const uint2 root = __ldg(&A.topo[0]);
+    if (lane == 0) {
+        s_node[0] = 0;
+        s_rem[0] = topo_mask(root.y);
+        s_act[0] = lanes;
+    }
+    __syncwarp();
+    int depth = 1;
+    while (depth > 0) {
+        const int top = depth - 1;
+        const uint32_t rem = s_rem[top];
+        if (rem == 0) {
+            --depth;
+            continue;
+        }
+        const uint32_t node = s_node[top];
+        const uint32_t act = s_act[top];
+        const int oct = 31 - __clz(rem);
+        __syncwarp();
+        if (lane == 0) {
+            s_rem[top] = rem & ~(1u << oct);
+        }
+        if (depth == 1 && me) {
+            cp_lane[oct * 32] = sum;  // running sum before the subtree of root child `oct`
+        }
+        const uint2 pt = __ldg(&A.topo[node]);
+        const uint32_t child = child_index(pt, oct);
+        const double4 rr = ldg4(&A.rec[child]);
+        const uint2 tt = __ldg(&A.topo[child]);
+        const double md = __ldg(&A.maxdim[child]);
+        int status = ST_DISCARD;
+        if ((act >> lane) & 1u) {
+            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+            status = e.status;
+            ++touched;
+            if (e.status == ST_ACCEPT) {
+                sum += e.w;
+            }
+        }
+        const uint32_t expand = __ballot_sync(0xFFFFFFFFu, status == ST_EXPAND);
+        __syncwarp();
+        if (expand) {
+            if (depth >= kStackDepth) {
+                overflow = true;
+                break;
+            }
+            if (lane == 0) {
+                s_node[depth] = child;
+                s_rem[depth] = topo_mask(tt.y);
+                s_act[depth] = expand;
+            }
+            ++depth;
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    return sum;
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
+    __shared__ uint32_t s_node[kWarpsPerBlock][kStackDepth];
+    __shared__ uint32_t s_rem[kWarpsPerBlock][kStackDepth];
+    __shared__ uint32_t s_act[kWarpsPerBlock][kStackDepth];
+    __shared__ double s_cp[kWarpsPerBlock][8 * 32];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint64_t warp_global = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
+    const uint64_t idx = A.begin + warp_global * 32 + lane;
+    if (A.begin + warp_global * 32 >= A.end) {
+        return;  // whole warp idle
+    }
+    const bool active = idx < A.end;
+    const uint32_t source = active ? A.list_src[idx] : 0u;
+    const uint32_t j = active ? A.list_j[idx] : 0u;
+    const double sx = active ? A.px[source] : 0.0;
+    const double sy = active ? A.py[source] : 0.0;
+    const double sz = active ? A.pz[source] : 0.0;
+    double* cp = &s_cp[wib][lane];
+    uint32_t touched = 0;
+    bool overflow = false;
+    uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
+
+    // ---- descent 0: warp packet over the whole tree
+    double total = packet_walk(A, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], touched, overflow);
+    bool fallback = false;
+    const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total == 0.0);
+    if (need_fb) {
+        uint32_t t2 = 0;
+        const double fb = packet_walk(A, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], t2, overflow);
+        if ((need_fb >> lane) & 1u) {
+            total = fb;
+            fallback = true;
+        }
+    }
+    int32_t result = -1;
+    bool done = !active;
+    if (active && total == 0.0) {
+        done = true;  // no candidate: the search fails
+    }
+    uint32_t sub = 0;
+    if (!done) {
+        const double r = pick_threshold(total, A.seed, A.step, source, j, 0);
+        // the crossing lies in the last root-child subtree (DFS order) whose
+        // checkpoint is below r
+        const uint2 root = __ldg(&A.topo[0]);
+        const uint32_t mask = topo_mask(root.y);
+        int cstar = -1;
+        for (int oct = 7; oct >= 0; --oct) {
+            if ((mask >> oct) & 1u) {
+                if (cp[oct * 32] < r) {
+                    cstar = oct;
+                } else {
+                    break;
+                }
+            }
+        }
+        if (cstar < 0) {
+            atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
+            done = true;
+        } else {
+            const uint32_t c0 = child_index(root, cstar);
+            const WalkResult wr = lane_walk(A, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
+            overflow |= wr.overflow;
+            if (wr.picked < 0) {
+                atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
+                done = true;
+            } else {
+                sub = (uint32_t)wr.picked;
+            }
+        }
+    }
+    // ---- deeper descents, per lane
+    for (uint32_t depth = 1; !done; ++depth) {
+        if (depth > (uint32_t)kStackDepth) {
+            overflow = true;  // a descent always moves one level down; cannot recur this often
+            break;
+        }
+        const uint2 st = __ldg(&A.topo[sub]);
+        if (topo_leaf(st.y)) {
+            result = (int32_t)st.x;
+            done = true;
+            break;
+        }
+        WalkResult s1 = lane_walk(A, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
+        touched += s1.touched;
+        bool fb = false;
+        if (s1.sum == 0.0) {
+            s1 = lane_walk(A, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
+            fb = true;
+        }
+        overflow |= s1.overflow;
+        if (s1.sum == 0.0) {
+            done = true;
+            break;
+        }
+        const double r = pick_threshold(s1.sum, A.seed, A.step, source, j, depth);
+        const WalkResult s2 = lane_walk(A, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
+        if (s2.picked < 0) {
+            atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
+            done = true;
+            break;
+        }
+        sub = (uint32_t)s2.picked;
+    }
+    if (overflow) {
+        atomicOr(A.err, (uint32_t)DERR_STACK);
+        result = -1;
+    }
+    if (active) {
+        A.target[idx] = result;
+    }
+    // touched-node counter (reference-equivalent acceptance tests)
+    unsigned long long t = touched;
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+    }
+    if (lane == 0) {
+        atomicAdd(A.touched, t);
+    }
+}
+
+// ---------------------------------------------------------- search list
+__global__ void k_search_counts(uint32_t n, const uint32_t* __restrict__ morton, const uint8_t* __restrict__ enabled, const uint8_t* __restrict__ signal,
+                                const uint32_t* __restrict__ vacant, uint32_t* __restrict__ cnt_exc, uint32_t* __restrict__ cnt_inh) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) {
+        return;
+    }
+    const uint32_t nid = morton[r];
+    const uint32_t v = enabled[nid] ? vacant[nid] : 0u;
+    const bool inh = signal[nid] != 0;
+    cnt_exc[r] = inh ? 0u : v;
+    cnt_inh[r] = inh ? v : 0u;
+}
+
+__global__ void k_search_fill(uint32_t n, const uint32_t* __restrict__ morton, const uint8_t* __restrict__ enabled, const uint8_t* __restrict__ signal,
+                              const uint32_t* __restrict__ vacant, const uint32_t* __restrict__ off_exc, const uint32_t* __restrict__ off_inh,
+                              uint64_t num_exc, uint32_t* __restrict__ list_src, uint32_t* __restrict__ list_j) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) {
+        return;
+    }
+    const uint32_t nid = morton[r];
+    const uint32_t v = enabled[nid] ? vacant[nid] : 0u;
+    const bool inh = signal[nid] != 0;
+    const uint64_t base = inh ? num_exc + off_inh[r] : off_exc[r];
+    for (uint32_t j = 0; j < v; ++j) {
+        list_src[base + j] = nid;
+        list_j[base + j] = j;
+    }
+}
+
+__global__ void k_fill_u32(uint32_t* p, uint64_t n, uint32_t v) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        p[i] = v;
+    }
+}
+
+// BarnesHutBase::find_target_neurons stops a neuron's loop at its first
+// failed search: record the smallest failing j per source.
+__global__ void k_first_fail(uint64_t m, const uint32_t* __restrict__ list_src, const uint32_t* __restrict__ list_j, const int32_t* __restrict__ target,
+                             uint32_t* __restrict__ first_fail) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m && target[i] < 0) {
+        atomicMin(&first_fail[list_src[i]], list_j[i]);
+    }
+}
+
+__global__ void k_req_count(uint32_t n, const uint32_t* __restrict__ first_fail, const uint32_t* __restrict__ vacant, const uint8_t* __restrict__ enabled,
+                            uint32_t* __restrict__ cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const uint32_t v = enabled[i] ? vacant[i] : 0u;
+    const uint32_t f = first_fail[i];
+    cnt[i] = f < v ? f : v;
+}
+
+__global__ void k_req_scatter(uint64_t m, const uint32_t* __restrict__ list_src, const uint32_t* __restrict__ list_j, const int32_t* __restrict__ target,
+                              const uint32_t* __restrict__ first_fail, const uint32_t* __restrict__ off, const uint8_t* __restrict__ signal,
+                              uint32_t* __restrict__ rt, uint32_t* __restrict__ rs, uint32_t* __restrict__ rj, uint32_t* __restrict__ rg) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) {
+        return;
+    }
+    const uint32_t s = list_src[i];
+    const uint32_t j = list_j[i];
+    if (j >= first_fail[s] || target[i] < 0) {
+        return;
+    }
+    const uint32_t o = off[s] + j;
+    rt[o] = (uint32_t)target[i];
+    rs[o] = s;
+    rj[o] = j;
+    rg[o] = signal[s];
+}
+
+}  // namespace
+
+void run_search(Ctx& c, uint32_t step) {
+    const uint32_t n = c.n;
+    cudaStream_t st = c.stream;
+    Search& S = c.search;
+    S.counts.ensure(2 * (size_t)n + 2);
+    uint32_t* cnt_exc = S.counts.p;
+    uint32_t* cnt_inh = S.counts.p + n;
+    k_search_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, c.tree.morton.p, c.nr.enabled.p, c.nr.signal.p, c.nr.search_vacant.p, cnt_exc, cnt_inh);
+    RL_LAUNCH_CHECK();
+    const uint64_t num_exc = exclusive_scan_u32(cnt_exc, cnt_exc, n, c.prim, st);
+    const uint64_t num_inh = exclusive_scan_u32(cnt_inh, cnt_inh, n, c.prim, st);
+    const uint64_t m = num_exc + num_inh;
+    S.num_searches = m;
+    S.num_exc = num_exc;
+    S.first_fail.ensure(n);
+    S.req_count.ensure(n);
+    S.req_off.ensure(n);
+    k_fill_u32<<<blocks_for(n, 256), 256, 0, st>>>(S.first_fail.p, n, 0xFFFFFFFFu);
+    RL_LAUNCH_CHECK();
+    if (m > 0) {
+        S.src.ensure(m);
+        S.jj.ensure(m);
+        S.target.ensure(m);
+        k_search_fill<<<blocks_for(n, 256), 256, 0, st>>>(n, c.tree.morton.p, c.nr.enabled.p, c.nr.signal.p, c.nr.search_vacant.p, cnt_exc, cnt_inh,
+                                                          num_exc, S.src.p, S.jj.p);
+        RL_LAUNCH_CHECK();
+        if (c.tree.root_is_leaf) {
+            // one neuron: its only candidate is itself (find_target_neuron returns nothing)
+            RL_CUDA_TRY(cudaMemsetAsync(S.target.p, 0xFF, m * sizeof(int32_t), st));
+        } else {
+            SearchArgs A;
+            A.topo = c.tree.topo.p;
+            A.maxdim = c.tree.maxdim.p;
+            A.px = c.nr.px.p;
+            A.py = c.nr.py.p;
+            A.pz = c.nr.pz.p;
+            A.list_src = S.src.p;
+            A.list_j = S.jj.p;
+            A.target = S.target.p;
+            A.theta = c.cfg.theta;
+            A.mu = c.cfg.mu;
+            A.scale = -1.0 / (c.cfg.sigma * c.cfg.sigma);
+            A.seed = c.cfg.seed;
+            A.step = step;
+            A.err = c.err.p;
+            A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
+            for (int t = 0; t < 2; ++t) {
+                A.rec = c.tree.rec[t].p;
+                A.begin = t == 0 ? 0 : num_exc;
+                A.end = t == 0 ? num_exc : m;
+                if (A.end <= A.begin) {
+                    continue;
+                }
+                const uint64_t warps = (A.end - A.begin + 31) / 32;
+                const unsigned blocks = (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+                k_search<<<blocks, kWarpsPerBlock * 32, 0, st>>>(A);
+                RL_LAUNCH_CHECK();
+            }
+        }
+        k_first_fail<<<blocks_for(m, 256), 256, 0, st>>>(m, S.src.p, S.jj.p, S.target.p, S.first_fail.p);
+        RL_LAUNCH_CHECK();
+    }
+    k_req_count<<<blocks_for(n, 256), 256, 0, st>>>(n, S.first_fail.p, c.nr.search_vacant.p, c.nr.enabled.p, S.req_count.p);
+    RL_LAUNCH_CHECK();
+    const uint64_t nreq = exclusive_scan_u32(S.req_count.p, S.req_off.p, n, c.prim, st);
+    S.num_requests = nreq;
+    S.req_tgt.ensure(nreq);
+    S.req_src.ensure(nreq);
+    S.req_j.ensure(nreq);
+    S.req_sig.ensure(nreq);
+    if (m > 0) {
+        k_req_scatter<<<blocks_for(m, 256), 256, 0, st>>>(m, S.src.p, S.jj.p, S.target.p, S.first_fail.p, S.req_off.p, c.nr.signal.p, S.req_tgt.p,
+                                                          S.req_src.p, S.req_j.p, S.req_sig.p);
+        RL_LAUNCH_CHECK();
+    }
+    check_device_error(c, "barnes-hut search");
+    c.stats.searches += m;
+    c.stats.requests += nreq;
+}
+
+}  // namespace rl

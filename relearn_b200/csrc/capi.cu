@@ -1,0 +1,530 @@
+// C ABI of librelearn_b200 (declared in include/relearn_b200.h).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "rl_context.cuh"
+
+namespace rl {
+
+void check_device_error(Ctx& c, const char* phase) {
+    uint32_t h = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&h, c.err.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    if (h == 0) {
+        return;
+    }
+    RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
+    std::string msg = std::string(phase) + ": device error";
+    rl_status st = RL_ERR_DEVICE;
+    if (h & DERR_OUT_OF_BOX) {
+        msg += " [position outside the simulation box]";
+        st = RL_ERR_INVALID;
+    }
+    if (h & DERR_DUPLICATE) {
+        msg += " [two positions coincide within 42 octree levels]";
+        st = RL_ERR_INVALID;
+    }
+    if (h & DERR_STACK) {
+        msg += " [traversal stack overflow]";
+        st = RL_ERR_OVERFLOW;
+    }
+    if (h & DERR_NO_CROSSING) {
+        msg += " [pick found no crossing]";
+    }
+    if (h & DERR_CAPACITY) {
+        msg += " [buffer capacity]";
+        st = RL_ERR_OVERFLOW;
+    }
+    if (h & DERR_CONNECT) {
+        msg += " [connector element underflow]";
+    }
+    if (h & DERR_TIMEOUT) {
+        msg += " [bounded wait ran out]";
+        st = RL_ERR_TIMEOUT;
+    }
+    throw Error{ st, msg };
+}
+
+namespace {
+
+template <typename T>
+void upload(DBuf<T>& d, const T* h, size_t n, cudaStream_t st) {
+    RL_CUDA_TRY(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+template <typename T>
+void download(T* h, const DBuf<T>& d, size_t n, cudaStream_t st) {
+    RL_CUDA_TRY(cudaMemcpyAsync(h, d.p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+}
+
+__global__ void k_fill_f64(double* p, uint64_t n, double v) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        p[i] = v;
+    }
+}
+
+void fill(DBuf<double>& d, size_t n, double v, cudaStream_t st) {
+    k_fill_f64<<<blocks_for(n, 256), 256, 0, st>>>(d.p, n, v);
+    RL_LAUNCH_CHECK();
+}
+
+void validate(const rl_config& k) {
+    RL_CHECK(k.num_neurons > 0, RL_ERR_INVALID, "num_neurons must be positive");
+    RL_CHECK(k.num_neurons < (1u << 30), RL_ERR_UNSUPPORTED, "num_neurons must be below 2^30");
+    RL_CHECK(k.theta > 0.0 && k.theta <= 0.5, RL_ERR_INVALID, "theta must lie in (0, 0.5] (Constants::bh_max_theta)");
+    RL_CHECK(k.sigma > 0.0, RL_ERR_INVALID, "sigma must be positive");
+    RL_CHECK(k.h_model >= 1 && k.h_model <= 1000, RL_ERR_INVALID, "h_model must lie in [1, 1000]");
+    RL_CHECK(k.h_calcium >= 1 && k.h_calcium <= 1000, RL_ERR_INVALID, "h_calcium must lie in [1, 1000]");
+    RL_CHECK(k.noise_stddev > 0.0, RL_ERR_INVALID, "noise_stddev must be positive");
+    for (int a = 0; a < 3; ++a) {
+        RL_CHECK(k.box_min[a] <= k.box_max[a], RL_ERR_INVALID, "box_min must not exceed box_max");
+        RL_CHECK(k.retract_ratio[a] >= 0.0 && k.retract_ratio[a] <= 1.0, RL_ERR_INVALID, "retract ratio must lie in [0, 1]");
+    }
+}
+
+void create(Ctx& c, const rl_config& k) {
+    validate(k);
+    c.cfg = k;
+    c.n = k.num_neurons;
+    c.device = k.device;
+    int count = 0;
+    RL_CUDA_TRY(cudaGetDeviceCount(&count));
+    RL_CHECK(k.device >= 0 && k.device < count, RL_ERR_DEVICE, "no such CUDA device");
+    RL_CUDA_TRY(cudaSetDevice(k.device));
+    RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    const size_t n = c.n;
+    Neurons& N = c.nr;
+    N.px.alloc(n);
+    N.py.alloc(n);
+    N.pz.alloc(n);
+    N.signal.alloc(n);
+    N.enabled.alloc(n);
+    N.update.alloc(n);
+    N.x.alloc(n);
+    N.u.alloc(n);
+    N.calcium.alloc(n);
+    N.target.alloc(n);
+    N.input.alloc(n);
+    N.fired[0].alloc(n);
+    N.fired[1].alloc(n);
+    for (int t = 0; t < 3; ++t) {
+        N.grown[t].alloc(n);
+        N.delta[t].alloc(n);
+        N.connected[t].alloc(n);
+        N.vacant[t].alloc(n);
+        RL_CUDA_TRY(cudaMemsetAsync(N.grown[t].p, 0, n * sizeof(double), c.stream));
+        RL_CUDA_TRY(cudaMemsetAsync(N.delta[t].p, 0, n * sizeof(double), c.stream));
+        RL_CUDA_TRY(cudaMemsetAsync(N.connected[t].p, 0, n * sizeof(uint32_t), c.stream));
+        RL_CUDA_TRY(cudaMemsetAsync(N.vacant[t].p, 0, n * sizeof(uint32_t), c.stream));
+    }
+    N.search_vacant.alloc(n);
+    RL_CUDA_TRY(cudaMemsetAsync(N.search_vacant.p, 0, n * sizeof(uint32_t), c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(N.signal.p, 0, n, c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(N.enabled.p, 1, n, c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(N.update.p, 1, n, c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(N.fired[0].p, 0, n, c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(N.fired[1].p, 0, n, c.stream));
+    // IzhikevichModelBase::init_neurons (models/izhikevich/IzhikevichModelBase.cpp:59-66)
+    fill(N.x, n, k.iz_c, c.stream);
+    fill(N.u, n, 0.0, c.stream);
+    fill(N.calcium, n, k.initial_calcium, c.stream);
+    fill(N.target, n, k.target_calcium, c.stream);
+    fill(N.input, n, 0.0, c.stream);
+    c.graph.offsets.alloc(n + 1);
+    RL_CUDA_TRY(cudaMemsetAsync(c.graph.offsets.p, 0, (n + 1) * sizeof(uint32_t), c.stream));
+    c.err.alloc(1);
+    RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
+    c.counters.alloc(4);
+    RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+}
+
+void require_tree(Ctx& c) {
+    RL_CHECK(c.positions_set, RL_ERR_INVALID, "rl_set_positions has not been called");
+}
+
+void plasticity_update(Ctx& c, uint32_t step) {
+    require_tree(c);
+    // SynapseDeletionFinderCPU::delete_synapses: commit the three element types
+    run_commit(c);
+    // Neurons::create_synapses: search from the committed vacant axons
+    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));
+    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
+    update_tree(c);
+    run_search(c, step);
+    run_connector(c, step);
+    rebuild_graph(c);
+    c.stats.plasticity_updates += 1;
+}
+
+Ctx* as_ctx(void* p) {
+    return static_cast<Ctx*>(p);
+}
+
+template <typename F>
+rl_status guarded(void* ctx, F&& f) {
+    if (!ctx) {
+        return RL_ERR_INVALID;
+    }
+    Ctx& c = *as_ctx(ctx);
+    try {
+        RL_CUDA_TRY(cudaSetDevice(c.device));
+        f(c);
+        return RL_OK;
+    } catch (const Error& e) {
+        c.last_error = e.message;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        c.last_error = "host allocation failed";
+        return RL_ERR_OOM;
+    } catch (...) {
+        c.last_error = "unexpected host exception";
+        return RL_ERR_INVALID;
+    }
+}
+
+}  // namespace
+}  // namespace rl
+
+using rl::Ctx;
+
+extern "C" {
+
+int32_t rl_abi_version(void) {
+    return RL_ABI_VERSION;
+}
+
+const char* rl_status_string(rl_status s) {
+    switch (s) {
+        case RL_OK: return "ok";
+        case RL_ERR_INVALID: return "invalid argument or state";
+        case RL_ERR_OOM: return "device allocation failed";
+        case RL_ERR_DEVICE: return "CUDA device error";
+        case RL_ERR_TIMEOUT: return "bounded device wait ran out";
+        case RL_ERR_OVERFLOW: return "device buffer overflow";
+        case RL_ERR_UNSUPPORTED: return "unsupported configuration";
+    }
+    return "unknown status";
+}
+
+void rl_config_default(rl_config* k, uint32_t num_neurons, double side) {
+    std::memset(k, 0, sizeof(*k));
+    k->num_neurons = num_neurons;
+    k->plasticity_interval = 100;
+    k->h_model = 10;
+    k->h_calcium = 10;
+    k->seed = 1;
+    for (int a = 0; a < 3; ++a) {
+        k->box_min[a] = 0.0;
+        k->box_max[a] = side;
+        k->growth_rate[a] = 1e-4;
+        k->retract_ratio[a] = 0.0;
+    }
+    k->theta = 0.3;
+    k->sigma = 750.0;
+    k->mu = 0.0;
+    k->iz_a = 0.1;
+    k->iz_b = 0.2;
+    k->iz_c = -65.0;
+    k->iz_d = 2.0;
+    k->iz_v_spike = 30.0;
+    k->iz_k1 = 0.04;
+    k->iz_k2 = 5.0;
+    k->iz_k3 = 140.0;
+    k->beta = 0.001;
+    k->tau_c = 10000.0;
+    k->target_calcium = 0.7;
+    k->initial_calcium = 0.0;
+    k->min_calcium[0] = 0.4;
+    k->min_calcium[1] = 0.1;
+    k->min_calcium[2] = 0.0;
+    k->conductance = 1.0;
+    k->noise_mean = 5.0;
+    k->noise_stddev = 2.0;
+    k->device = 0;
+}
+
+rl_status rl_ctx_create(const rl_config* cfg, void** out) {
+    if (!cfg || !out) {
+        return RL_ERR_INVALID;
+    }
+    *out = nullptr;
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) {
+        return RL_ERR_OOM;
+    }
+    try {
+        rl::create(*c, *cfg);
+    } catch (const rl::Error& e) {
+        std::fprintf(stderr, "rl_ctx_create: %s\n", e.message.c_str());
+        delete c;
+        return e.status;
+    }
+    *out = c;
+    return RL_OK;
+}
+
+rl_status rl_ctx_destroy(void* ctx) {
+    if (!ctx) {
+        return RL_ERR_INVALID;
+    }
+    Ctx* c = static_cast<Ctx*>(ctx);
+    cudaSetDevice(c->device);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    delete c;
+    return RL_OK;
+}
+
+const char* rl_last_error(void* ctx) {
+    return ctx ? static_cast<Ctx*>(ctx)->last_error.c_str() : "null context";
+}
+
+rl_status rl_set_positions(void* ctx, const double* xyz, const uint8_t* signal) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(xyz != nullptr && signal != nullptr, RL_ERR_INVALID, "positions and signal types are required");
+        for (uint32_t i = 0; i < c.n; ++i) {
+            RL_CHECK(signal[i] <= 1, RL_ERR_INVALID, "signal type must be 0 or 1");
+        }
+        rl::upload(c.nr.signal, signal, c.n, c.stream);
+        rl::build_octree(c, xyz);
+        c.positions_set = true;
+        c.stats.num_nodes = c.tree.num_nodes;
+        c.stats.max_level = c.tree.max_level;
+    });
+}
+
+rl_status rl_tree_info(void* ctx, uint64_t* num_nodes, uint32_t* max_level) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        if (num_nodes) *num_nodes = c.tree.num_nodes;
+        if (max_level) *max_level = c.tree.max_level;
+    });
+}
+
+rl_status rl_dump_tree(void* ctx, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax,
+                       uint32_t* cnt_exc, uint32_t* cnt_inh, double* pos_exc, double* pos_inh) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        rl::dump_tree(c, level, neuron, child_mask, first_child, bmin, bmax, cnt_exc, cnt_inh, pos_exc, pos_inh);
+    });
+}
+
+rl_status rl_prepare_update_connectivity(void* ctx, const uint8_t* signal, const uint32_t* vacant_axons, const uint32_t* vacant_exc,
+                                         const uint32_t* vacant_inh, const uint8_t* update) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        RL_CHECK(vacant_axons && vacant_exc && vacant_inh, RL_ERR_INVALID, "vacant element arrays are required");
+        if (signal) {
+            rl::upload(c.nr.signal, signal, c.n, c.stream);
+        }
+        rl::upload(c.nr.search_vacant, vacant_axons, c.n, c.stream);
+        rl::upload(c.nr.vacant[0], vacant_axons, c.n, c.stream);
+        rl::upload(c.nr.vacant[1], vacant_exc, c.n, c.stream);
+        rl::upload(c.nr.vacant[2], vacant_inh, c.n, c.stream);
+        if (update) {
+            rl::upload(c.nr.update, update, c.n, c.stream);
+        } else {
+            RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
+        }
+        rl::update_tree(c);
+        rl::check_device_error(c, "prepare_update_connectivity");
+    });
+}
+
+rl_status rl_find_targets(void* ctx, uint32_t step, rl_request* out, uint64_t capacity, uint64_t* count) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        rl::run_search(c, step);
+        const uint64_t m = c.search.num_requests;
+        if (count) *count = m;
+        const uint64_t k = m < capacity ? m : capacity;
+        if (out && k) {
+            std::vector<uint32_t> t(k), s(k), j(k), g(k);
+            RL_CUDA_TRY(cudaMemcpyAsync(t.data(), c.search.req_tgt.p, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(s.data(), c.search.req_src.p, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(j.data(), c.search.req_j.p, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(g.data(), c.search.req_sig.p, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            for (uint64_t i = 0; i < k; ++i) {
+                out[i] = rl_request{ t[i], s[i], j[i], g[i] };
+            }
+        }
+    });
+}
+
+rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* out, uint64_t capacity, uint64_t* created) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        rl::run_search(c, step);
+        const uint64_t before = c.graph.num_new;
+        const uint64_t m = rl::run_connector(c, step);
+        if (created) *created = m;
+        const uint64_t k = m < capacity ? m : capacity;
+        if (out && k) {
+            std::vector<uint32_t> t(k), s(k);
+            std::vector<int32_t> w(k);
+            RL_CUDA_TRY(cudaMemcpyAsync(t.data(), c.graph.new_tgt.p + before, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(s.data(), c.graph.new_src.p + before, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(w.data(), c.graph.new_w.p + before, k * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            for (uint64_t i = 0; i < k; ++i) {
+                out[i] = rl_synapse{ t[i], s[i], w[i], 0u };
+            }
+        }
+        rl::rebuild_graph(c);
+    });
+}
+
+rl_status rl_set_elements(void* ctx, int type, const double* grown, const double* delta, const uint32_t* connected, const uint32_t* vacant) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(type >= 0 && type < 3, RL_ERR_INVALID, "element type must be 0, 1 or 2");
+        if (grown) rl::upload(c.nr.grown[type], grown, c.n, c.stream);
+        if (delta) rl::upload(c.nr.delta[type], delta, c.n, c.stream);
+        if (connected) rl::upload(c.nr.connected[type], connected, c.n, c.stream);
+        if (vacant) rl::upload(c.nr.vacant[type], vacant, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uint32_t* connected, uint32_t* vacant) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(type >= 0 && type < 3, RL_ERR_INVALID, "element type must be 0, 1 or 2");
+        if (grown) rl::download(grown, c.nr.grown[type], c.n, c.stream);
+        if (delta) rl::download(delta, c.nr.delta[type], c.n, c.stream);
+        if (connected) rl::download(connected, c.nr.connected[type], c.n, c.stream);
+        if (vacant) rl::download(vacant, c.nr.vacant[type], c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const double* calcium, const uint8_t* fired) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        if (x) rl::upload(c.nr.x, x, c.n, c.stream);
+        if (u) rl::upload(c.nr.u, u, c.n, c.stream);
+        if (calcium) rl::upload(c.nr.calcium, calcium, c.n, c.stream);
+        if (fired) rl::upload(c.nr.fired[c.nr.cur], fired, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        if (x) rl::download(x, c.nr.x, c.n, c.stream);
+        if (u) rl::download(u, c.nr.u, c.n, c.stream);
+        if (calcium) rl::download(calcium, c.nr.calcium, c.n, c.stream);
+        if (fired) rl::download(fired, c.nr.fired[c.nr.cur], c.n, c.stream);
+        if (input) rl::download(input, c.nr.input, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_set_enabled(void* ctx, const uint8_t* enabled) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(enabled != nullptr, RL_ERR_INVALID, "enabled flags are required");
+        rl::upload(c.nr.enabled, enabled, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_add_edges(void* ctx, uint64_t m, const uint32_t* target, const uint32_t* source, const int32_t* weight) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(m == 0 || (target && source && weight), RL_ERR_INVALID, "edge arrays are required");
+        rl::add_edges_host(c, m, target, source, weight);
+    });
+}
+
+rl_status rl_get_edges(void* ctx, uint32_t* target, uint32_t* source, int32_t* weight, uint64_t capacity, uint64_t* count) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::rebuild_graph(c);
+        const uint64_t m = c.graph.num_edges;
+        std::vector<uint32_t> off(c.n + 1), s(m);
+        std::vector<int32_t> w(m);
+        RL_CUDA_TRY(cudaMemcpyAsync(off.data(), c.graph.offsets.p, (c.n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+        if (m) {
+            RL_CUDA_TRY(cudaMemcpyAsync(s.data(), c.graph.src.p, m * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(w.data(), c.graph.weight.p, m * 4, cudaMemcpyDeviceToHost, c.stream));
+        }
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        // aggregate (target, source) pairs, drop zero weights (NetworkGraph::add_edge)
+        uint64_t k = 0;
+        std::vector<std::pair<uint32_t, int32_t>> row;
+        for (uint32_t t = 0; t < c.n; ++t) {
+            row.clear();
+            for (uint32_t e = off[t]; e < off[t + 1]; ++e) {
+                row.emplace_back(s[e], w[e]);
+            }
+            std::sort(row.begin(), row.end());
+            for (size_t a = 0; a < row.size();) {
+                size_t b = a;
+                int64_t sum = 0;
+                while (b < row.size() && row[b].first == row[a].first) {
+                    sum += row[b].second;
+                    ++b;
+                }
+                if (sum != 0) {
+                    if (k < capacity) {
+                        if (target) target[k] = t;
+                        if (source) source[k] = row[a].first;
+                        if (weight) weight[k] = (int32_t)sum;
+                    }
+                    ++k;
+                }
+                a = b;
+            }
+        }
+        if (count) *count = k;
+    });
+}
+
+rl_status rl_activity_block(void* ctx, uint32_t first_step, uint32_t nsteps) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::rebuild_graph(c);
+        for (uint32_t s = 0; s < nsteps; ++s) {
+            rl::run_activity_step(c, first_step + s);
+        }
+    });
+}
+
+rl_status rl_plasticity_update(void* ctx, uint32_t step) {
+    return rl::guarded(ctx, [&](Ctx& c) { rl::plasticity_update(c, step); });
+}
+
+rl_status rl_simulate(void* ctx, uint32_t first_step, uint32_t nsteps) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        rl::rebuild_graph(c);
+        const uint32_t interval = c.cfg.plasticity_interval;
+        for (uint32_t s = 0; s < nsteps; ++s) {
+            const uint32_t step = first_step + s;
+            rl::run_activity_step(c, step);
+            if (interval > 0 && step % interval == 0) {
+                rl::plasticity_update(c, step);
+            }
+        }
+    });
+}
+
+rl_status rl_synchronize(void* ctx) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        rl::check_device_error(c, "synchronize");
+    });
+}
+
+rl_status rl_get_stats(void* ctx, rl_stats* out) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(out != nullptr, RL_ERR_INVALID, "null output");
+        *out = c.stats;
+        out->gpu_launches = rl::g_launches;
+        out->num_nodes = c.tree.num_nodes;
+        out->max_level = c.tree.max_level;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,623 @@
+// Linear octree over the neuron positions, built on the device, and the
+// bottom-up aggregation of vacant dendrites.
+//
+// Reference semantics (relearn/source):
+//   * Octree::insert / OctreeNode::insert (algorithm/Internal/octree/Octree.h:201-209,
+//     OctreeNode.h:153-250) build the point-region octree: one neuron per leaf,
+//     a cell splits until its two neurons fall into different octants.  The
+//     result does not depend on insertion order.
+//   * Cell::get_octant_for_position (Cell.h:104-137): bit = !(x < (min+max)/2);
+//     Cell::get_size_for_octant (Cell.h:145-178): child box via the midpoint.
+//   * OctreeNodeUpdater::update_node (OctreeNodeHelper.h:43-152): per dendrite
+//     type, count = sum of child counts; position = (sum over children in
+//     octant order of child_position * count) / count, clipped to the cell.
+//
+// Construction here: each neuron computes its octant digits level by level
+// with exactly the reference's midpoint comparisons (two 63-bit words, 42
+// levels), the keys are radix sorted, and the octree nodes are the distinct
+// digit prefixes shared by at least two neurons (inner nodes) plus one leaf per
+// neuron at the first level where its prefix is unique.  Nodes are laid out
+// breadth-first (level, then Morton order), so the children of a node are
+// contiguous and in octant order.
+#include "rl_context.cuh"
+#include "rl_math.cuh"
+
+#include <algorithm>
+
+namespace rl {
+namespace {
+
+__device__ __forceinline__ int octant_step(double p, double& lo, double& hi) {
+    const double mid = (lo + hi) / 2.0;
+    if (p < mid) {
+        hi = mid;
+        return 0;
+    }
+    lo = mid;
+    return 1;
+}
+
+__global__ void k_keys(uint32_t n, const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz, double3 bmin,
+                       double3 bmax, uint64_t* __restrict__ key0, uint64_t* __restrict__ key1, uint32_t* __restrict__ idx, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const double x = px[i], y = py[i], z = pz[i];
+    idx[i] = i;
+    if (!(bmin.x <= x && x <= bmax.x && bmin.y <= y && y <= bmax.y && bmin.z <= z && z <= bmax.z)) {
+        atomicOr(err, (uint32_t)DERR_OUT_OF_BOX);
+        key0[i] = 0;
+        key1[i] = 0;
+        return;
+    }
+    double lx = bmin.x, hx = bmax.x, ly = bmin.y, hy = bmax.y, lz = bmin.z, hz = bmax.z;
+    uint64_t k0 = 0, k1 = 0;
+    for (int l = 0; l < kLevelsPerWord; ++l) {
+        const int bx = octant_step(x, lx, hx);
+        const int by = octant_step(y, ly, hy);
+        const int bz = octant_step(z, lz, hz);
+        k0 = (k0 << 3) | (uint64_t)(bx | (by << 1) | (bz << 2));
+    }
+    for (int l = 0; l < kLevelsPerWord; ++l) {
+        const int bx = octant_step(x, lx, hx);
+        const int by = octant_step(y, ly, hy);
+        const int bz = octant_step(z, lz, hz);
+        k1 = (k1 << 3) | (uint64_t)(bx | (by << 1) | (bz << 2));
+    }
+    key0[i] = k0;
+    key1[i] = k1;
+}
+
+// Neurons whose first words agree are ordered by the second word (runs are
+// tiny: the cell of a 21-level prefix is 2^-21 of the box).
+__global__ void k_fix_runs(uint32_t n, uint64_t* __restrict__ k0s, uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= n) {
+        return;
+    }
+    if (k0s[i] != k0s[i + 1] || (i > 0 && k0s[i - 1] == k0s[i])) {
+        return;
+    }
+    uint32_t end = i + 1;
+    while (end + 1 < n && k0s[end + 1] == k0s[i]) {
+        ++end;
+    }
+    for (uint32_t a = i + 1; a <= end; ++a) {
+        const uint32_t v = idx[a];
+        const uint64_t kv = key1[v];
+        uint32_t b = a;
+        while (b > i && key1[idx[b - 1]] > kv) {
+            idx[b] = idx[b - 1];
+            --b;
+        }
+        idx[b] = v;
+    }
+    for (uint32_t a = i; a < end; ++a) {
+        if (key1[idx[a]] == key1[idx[a + 1]]) {
+            atomicOr(err, (uint32_t)DERR_DUPLICATE);
+        }
+    }
+}
+
+__device__ __forceinline__ int common_levels(uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1) {
+    const uint64_t x = a0 ^ b0;
+    if (x) {
+        return (__clzll((long long)x) - 1) / 3;
+    }
+    const uint64_t y = a1 ^ b1;
+    if (y) {
+        return kLevelsPerWord + (__clzll((long long)y) - 1) / 3;
+    }
+    return kMaxLevels;  // identical keys (flagged as duplicate elsewhere)
+}
+
+// lcp[i] = common levels of sorted neighbours i and i+1, for i < n-1.
+__global__ void k_lcp(uint32_t n, const uint64_t* __restrict__ k0s, const uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1,
+                      int32_t* __restrict__ lcp, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= n) {
+        return;
+    }
+    const int c = common_levels(k0s[i], key1[idx[i]], k0s[i + 1], key1[idx[i + 1]]);
+    if (c >= kMaxLevels) {
+        atomicOr(err, (uint32_t)DERR_DUPLICATE);
+    }
+    lcp[i] = c;
+}
+
+__device__ __forceinline__ int lcp_at(const int32_t* lcp, int64_t i, uint32_t n) {
+    return (i < 0 || i >= (int64_t)n - 1) ? -1 : lcp[i];
+}
+
+// Nodes starting at sorted position i occupy levels [s_i, e_i]:
+// s_i = lcp(i-1) + 1, e_i = max(lcp(i-1), lcp(i)) + 1; the last is the leaf.
+__global__ void k_node_counts(uint32_t n, const int32_t* __restrict__ lcp, uint32_t* __restrict__ cnt, uint32_t* __restrict__ maxlev) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const int a = lcp_at(lcp, (int64_t)i - 1, n);
+    const int b = lcp_at(lcp, i, n);
+    const int s = a + 1;
+    const int e = (a > b ? a : b) + 1;
+    cnt[i] = (uint32_t)(e - s + 1);
+    atomicMax(maxlev, (uint32_t)e);
+}
+
+__global__ void k_node_keys(uint32_t n, const int32_t* __restrict__ lcp, const uint32_t* __restrict__ base, uint32_t* __restrict__ skey,
+                            uint32_t* __restrict__ sval) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const int a = lcp_at(lcp, (int64_t)i - 1, n);
+    const int b = lcp_at(lcp, i, n);
+    const int s = a + 1;
+    const int e = (a > b ? a : b) + 1;
+    uint32_t m = base[i];
+    for (int l = s; l <= e; ++l, ++m) {
+        skey[m] = (uint32_t)l * n + i;
+        sval[m] = m;
+    }
+}
+
+__global__ void k_invert(uint32_t m, const uint32_t* __restrict__ sval, uint32_t* __restrict__ bfs_of) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < m) {
+        bfs_of[sval[b]] = b;
+    }
+}
+
+__device__ __forceinline__ int digit_at(uint64_t k0, uint64_t k1, int level) {
+    // level 1..42
+    if (level <= kLevelsPerWord) {
+        return (int)((k0 >> (3 * (kLevelsPerWord - level))) & 7u);
+    }
+    return (int)((k1 >> (3 * (2 * kLevelsPerWord - level))) & 7u);
+}
+
+struct FillArgs {
+    uint32_t n, m;
+    const uint32_t* skey;
+    const uint32_t* sval;
+    const uint32_t* bfs_of;
+    const int32_t* lcp;
+    const uint64_t* k0s;
+    const uint64_t* key1;
+    const uint32_t* idx;
+    const double *px, *py, *pz;
+    double3 bmin, bmax;
+    double4* rec0;
+    double4* rec1;
+    uint2* topo;
+    double* maxdim;
+    double *bx0, *by0, *bz0, *bx1, *by1, *bz1;
+    uint32_t* first_key;
+    uint32_t* leaf_of;
+    int32_t* parent;
+    uint32_t* level_count;
+};
+
+__global__ void k_fill(FillArgs A) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= A.m) {
+        return;
+    }
+    const uint32_t key = A.skey[b];
+    const uint32_t l = key / A.n;
+    const uint32_t i = key - l * A.n;
+    const uint32_t mi = A.sval[b];
+    const int a = lcp_at(A.lcp, (int64_t)i - 1, A.n);
+    const int bb = lcp_at(A.lcp, i, A.n);
+    const int s = a + 1;
+    const int e = (a > bb ? a : bb) + 1;
+    const bool leaf = (int)l == e;
+    const uint32_t neuron = A.idx[i];
+    const uint64_t k0 = A.k0s[i];
+    const uint64_t k1 = A.key1[neuron];
+    // cell box: descend l levels along the digits of the first neuron
+    double lx = A.bmin.x, hx = A.bmax.x, ly = A.bmin.y, hy = A.bmax.y, lz = A.bmin.z, hz = A.bmax.z;
+    for (int lev = 1; lev <= (int)l; ++lev) {
+        const int d = digit_at(k0, k1, lev);
+        const double mx = (lx + hx) / 2.0, my = (ly + hy) / 2.0, mz = (lz + hz) / 2.0;
+        if (d & 1) lx = mx; else hx = mx;
+        if (d & 2) ly = my; else hy = my;
+        if (d & 4) lz = mz; else hz = mz;
+    }
+    A.bx0[b] = lx;
+    A.by0[b] = ly;
+    A.bz0[b] = lz;
+    A.bx1[b] = hx;
+    A.by1[b] = hy;
+    A.bz1[b] = hz;
+    const double dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    // std::max({x, y, z}) of Vec3::get_maximum
+    double md = dx;
+    if (md < dy) md = dy;
+    if (md < dz) md = dz;
+    A.maxdim[b] = md;
+    A.first_key[b] = i;
+    const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (leaf) {
+        const double4 p = make_double4(A.px[neuron], A.py[neuron], A.pz[neuron], 0.0);
+        A.rec0[b] = p;
+        A.rec1[b] = p;
+        A.topo[b] = make_uint2(neuron, (1u << 8) | (l << 16));
+        A.leaf_of[neuron] = b;
+    } else {
+        A.rec0[b] = zero;
+        A.rec1[b] = zero;
+        A.topo[b] = make_uint2(A.bfs_of[mi + 1], (l << 16));
+    }
+    if (l == 0) {
+        A.parent[b] = -1;
+    } else if ((int)l > s) {
+        A.parent[b] = (int32_t)A.bfs_of[mi - 1];
+    } else {
+        A.parent[b] = -2;  // resolved by k_parent_search
+    }
+    atomicAdd(&A.level_count[l], 1u);
+}
+
+// For a node that is the first node of its start position, the parent is the
+// last node of the previous level that starts at or before it.
+__global__ void k_parent_search(uint32_t m, const uint32_t* __restrict__ level_off, const uint32_t* __restrict__ first_key, const uint2* topo_in,
+                                int32_t* __restrict__ parent) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m || parent[b] != -2) {
+        return;
+    }
+    const uint32_t l = topo_level(topo_in[b].y);
+    const uint32_t i = first_key[b];
+    uint32_t lo = level_off[l - 1], hi = level_off[l];  // search [lo, hi)
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (first_key[mid] <= i) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    parent[b] = (int32_t)lo;
+}
+
+__global__ void k_child_mask(uint32_t m, const int32_t* __restrict__ parent, const uint32_t* __restrict__ first_key, const uint64_t* __restrict__ k0s,
+                             const uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1, uint2* topo) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m) {
+        return;
+    }
+    const int32_t p = parent[b];
+    if (p < 0) {
+        return;
+    }
+    const uint32_t i = first_key[b];
+    const uint32_t l = topo_level(topo[b].y);
+    const int d = digit_at(k0s[i], key1[idx[i]], (int)l);
+    atomicOr(&topo[p].y, 1u << d);
+}
+
+// ------------------------------------------------------------ aggregation
+__global__ void k_leaf_counts(uint32_t n, const uint32_t* __restrict__ leaf_of, const uint8_t* __restrict__ enabled, const uint8_t* __restrict__ update,
+                              const uint32_t* __restrict__ vac_exc, const uint32_t* __restrict__ vac_inh, double4* rec0, double4* rec1) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const uint32_t leaf = leaf_of[i];
+    const bool on = enabled[i] && update[i];
+    const uint32_t ce = on ? vac_exc[i] : 0u;
+    const uint32_t ci = on ? vac_inh[i] : 0u;
+    reinterpret_cast<long long*>(&rec0[leaf])[3] = (long long)ce;
+    reinterpret_cast<long long*>(&rec1[leaf])[3] = (long long)ci;
+}
+
+__device__ __forceinline__ uint32_t rec_count(const double4& r) {
+    return (uint32_t)__double_as_longlong(r.w);
+}
+
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ void stcg4(double4* p, const double4& v) {
+    __stcg(reinterpret_cast<double2*>(p), make_double2(v.x, v.y));
+    __stcg(reinterpret_cast<double2*>(p) + 1, make_double2(v.z, v.w));
+}
+
+// OctreeNodeUpdater::update_node for one dendrite type.
+__device__ __forceinline__ double4 update_type(const double4* rec, const uint2* topo, uint32_t base, uint32_t mask, double lx, double ly, double lz,
+                                               double hx, double hy, double hz) {
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    uint32_t total = 0;
+    uint32_t k = 0;
+    for (int c = 0; c < 8; ++c) {
+        if (!((mask >> c) & 1u)) {
+            continue;
+        }
+        const uint32_t child = base + k++;
+        const double4 r = ldcg4(&rec[child]);
+        const uint32_t cnt = rec_count(r);
+        total += cnt;
+        const bool has = topo_leaf(__ldg(&topo[child].y)) || cnt > 0;
+        if (has) {
+            const double kd = (double)cnt;
+            ax = ax + r.x * kd;
+            ay = ay + r.y * kd;
+            az = az + r.z * kd;
+        }
+    }
+    if (total == 0) {
+        const double nan = __longlong_as_double(0x7FF8000000000000ll);
+        return make_double4(nan, nan, nan, 0.0);
+    }
+    const double td = (double)total;
+    double x = ax / td, y = ay / td, z = az / td;
+    x = x < lx ? lx : (hx < x ? hx : x);
+    y = y < ly ? ly : (hy < y ? hy : y);
+    z = z < lz ? lz : (hz < z ? hz : z);
+    return make_double4(x, y, z, __longlong_as_double((long long)total));
+}
+
+struct ReduceArgs {
+    uint32_t n;
+    const uint32_t* leaf_of;
+    const int32_t* parent;
+    const uint2* topo;
+    const double *bx0, *by0, *bz0, *bx1, *by1, *bz1;
+    double4* rec0;
+    double4* rec1;
+    uint32_t* arrive;
+};
+
+// One thread per leaf walks up; the last child to arrive at a node computes
+// it (reading all children in octant order), so every node is computed once
+// and in the reference's summation order.
+__global__ void k_reduce(ReduceArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    int32_t node = A.parent[A.leaf_of[i]];
+    while (node >= 0) {
+        __threadfence();
+        const uint2 t = A.topo[node];
+        const uint32_t mask = topo_mask(t.y);
+        const uint32_t old = atomicAdd(&A.arrive[node], 1u);
+        if (old + 1 != (uint32_t)__popc(mask)) {
+            return;
+        }
+        __threadfence();
+        const double lx = A.bx0[node], ly = A.by0[node], lz = A.bz0[node];
+        const double hx = A.bx1[node], hy = A.by1[node], hz = A.bz1[node];
+        const double4 r0 = update_type(A.rec0, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
+        const double4 r1 = update_type(A.rec1, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
+        stcg4(&A.rec0[node], r0);
+        stcg4(&A.rec1[node], r1);
+        node = A.parent[node];
+    }
+}
+
+}  // namespace
+
+void build_octree(Ctx& c, const double* h_xyz) {
+    const uint32_t n = c.n;
+    cudaStream_t st = c.stream;
+    Tree& T = c.tree;
+    // positions to SoA on the host side of the copy
+    std::vector<double> hx(n), hy(n), hz(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        hx[i] = h_xyz[3 * (size_t)i];
+        hy[i] = h_xyz[3 * (size_t)i + 1];
+        hz[i] = h_xyz[3 * (size_t)i + 2];
+    }
+    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.px.p, hx.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.py.p, hy.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.pz.p, hz.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), st));
+
+    DBuf<uint64_t> key0, key1;
+    DBuf<uint32_t> idx;
+    key0.alloc(n);
+    key1.alloc(n);
+    idx.alloc(n);
+    const double3 bmin = make_double3(c.cfg.box_min[0], c.cfg.box_min[1], c.cfg.box_min[2]);
+    const double3 bmax = make_double3(c.cfg.box_max[0], c.cfg.box_max[1], c.cfg.box_max[2]);
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, c.nr.px.p, c.nr.py.p, c.nr.pz.p, bmin, bmax, key0.p, key1.p, idx.p, c.err.p);
+    RL_LAUNCH_CHECK();
+    check_device_error(c, "octree keys");
+    // sort on the first word (63 bits), then order ties by the second word
+    DBuf<uint64_t> k0s;
+    k0s.alloc(n);
+    RL_CUDA_TRY(cudaMemcpyAsync(k0s.p, key0.p, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    radix_sort_u64(k0s.p, idx.p, n, 63, c.prim, st);
+    k_fix_runs<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, c.err.p);
+    RL_LAUNCH_CHECK();
+    DBuf<int32_t> lcp;
+    lcp.alloc(n);
+    k_lcp<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, lcp.p, c.err.p);
+    RL_LAUNCH_CHECK();
+    check_device_error(c, "octree keys");
+
+    DBuf<uint32_t> cnt, base, maxlev;
+    cnt.alloc(n);
+    base.alloc(n);
+    maxlev.alloc(1);
+    RL_CUDA_TRY(cudaMemsetAsync(maxlev.p, 0, sizeof(uint32_t), st));
+    k_node_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, lcp.p, cnt.p, maxlev.p);
+    RL_LAUNCH_CHECK();
+    const uint32_t m = exclusive_scan_u32(cnt.p, base.p, n, c.prim, st);
+    uint32_t max_level = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&max_level, maxlev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    RL_CHECK((uint64_t)(max_level + 1) * n < 0xFFFFFFFFull, RL_ERR_UNSUPPORTED, "octree too deep for the node key");
+
+    DBuf<uint32_t> skey, sval, bfs_of;
+    skey.alloc(m);
+    sval.alloc(m);
+    bfs_of.alloc(m);
+    k_node_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, lcp.p, base.p, skey.p, sval.p);
+    RL_LAUNCH_CHECK();
+    int bits = 1;
+    while (bits < 32 && ((uint64_t)1 << bits) <= (uint64_t)(max_level + 1) * n) {
+        ++bits;
+    }
+    radix_sort_u32(skey.p, sval.p, m, bits, c.prim, st);
+    k_invert<<<blocks_for(m, 256), 256, 0, st>>>(m, sval.p, bfs_of.p);
+    RL_LAUNCH_CHECK();
+
+    T.num_nodes = m;
+    T.max_level = max_level;
+    for (int t = 0; t < 2; ++t) {
+        T.rec[t].alloc(m);
+    }
+    T.topo.alloc(m);
+    T.maxdim.alloc(m);
+    for (int a = 0; a < 3; ++a) {
+        T.bmin[a].alloc(m);
+        T.bmax[a].alloc(m);
+    }
+    T.parent.alloc(m);
+    T.first_key.alloc(m);
+    T.leaf_of.alloc(n);
+    T.morton.alloc(n);
+    T.arrive.alloc(m);
+    RL_CUDA_TRY(cudaMemcpyAsync(T.morton.p, idx.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+
+    DBuf<uint32_t> level_count;
+    level_count.alloc(kMaxLevels + 2);
+    RL_CUDA_TRY(cudaMemsetAsync(level_count.p, 0, (kMaxLevels + 2) * sizeof(uint32_t), st));
+    FillArgs A;
+    A.n = n;
+    A.m = m;
+    A.skey = skey.p;
+    A.sval = sval.p;
+    A.bfs_of = bfs_of.p;
+    A.lcp = lcp.p;
+    A.k0s = k0s.p;
+    A.key1 = key1.p;
+    A.idx = idx.p;
+    A.px = c.nr.px.p;
+    A.py = c.nr.py.p;
+    A.pz = c.nr.pz.p;
+    A.bmin = bmin;
+    A.bmax = bmax;
+    A.rec0 = T.rec[0].p;
+    A.rec1 = T.rec[1].p;
+    A.topo = T.topo.p;
+    A.maxdim = T.maxdim.p;
+    A.bx0 = T.bmin[0].p;
+    A.by0 = T.bmin[1].p;
+    A.bz0 = T.bmin[2].p;
+    A.bx1 = T.bmax[0].p;
+    A.by1 = T.bmax[1].p;
+    A.bz1 = T.bmax[2].p;
+    A.first_key = T.first_key.p;
+    A.leaf_of = T.leaf_of.p;
+    A.parent = T.parent.p;
+    A.level_count = level_count.p;
+    k_fill<<<blocks_for(m, 256), 256, 0, st>>>(A);
+    RL_LAUNCH_CHECK();
+    std::vector<uint32_t> hcount(kMaxLevels + 2, 0);
+    RL_CUDA_TRY(cudaMemcpyAsync(hcount.data(), level_count.p, hcount.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<uint32_t> hoff(kMaxLevels + 3, 0);
+    for (int l = 0; l < kMaxLevels + 2; ++l) {
+        hoff[l + 1] = hoff[l] + hcount[l];
+    }
+    DBuf<uint32_t> level_off;
+    level_off.alloc(hoff.size());
+    RL_CUDA_TRY(cudaMemcpyAsync(level_off.p, hoff.data(), hoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    k_parent_search<<<blocks_for(m, 256), 256, 0, st>>>(m, level_off.p, T.first_key.p, T.topo.p, T.parent.p);
+    RL_LAUNCH_CHECK();
+    k_child_mask<<<blocks_for(m, 256), 256, 0, st>>>(m, T.parent.p, T.first_key.p, k0s.p, idx.p, key1.p, T.topo.p);
+    RL_LAUNCH_CHECK();
+    uint2 root;
+    RL_CUDA_TRY(cudaMemcpyAsync(&root, T.topo.p, sizeof(uint2), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    T.root_is_leaf = topo_leaf(root.y);
+    T.root_neuron = root.x;
+    check_device_error(c, "octree build");
+}
+
+void update_tree(Ctx& c) {
+    const uint32_t n = c.n;
+    cudaStream_t st = c.stream;
+    Tree& T = c.tree;
+    k_leaf_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, T.leaf_of.p, c.nr.enabled.p, c.nr.update.p, c.nr.vacant[1].p, c.nr.vacant[2].p, T.rec[0].p,
+                                                      T.rec[1].p);
+    RL_LAUNCH_CHECK();
+    if (T.root_is_leaf) {
+        return;
+    }
+    RL_CUDA_TRY(cudaMemsetAsync(T.arrive.p, 0, T.num_nodes * sizeof(uint32_t), st));
+    ReduceArgs A;
+    A.n = n;
+    A.leaf_of = T.leaf_of.p;
+    A.parent = T.parent.p;
+    A.topo = T.topo.p;
+    A.bx0 = T.bmin[0].p;
+    A.by0 = T.bmin[1].p;
+    A.bz0 = T.bmin[2].p;
+    A.bx1 = T.bmax[0].p;
+    A.by1 = T.bmax[1].p;
+    A.bz1 = T.bmax[2].p;
+    A.rec0 = T.rec[0].p;
+    A.rec1 = T.rec[1].p;
+    A.arrive = T.arrive.p;
+    k_reduce<<<blocks_for(n, 128), 128, 0, st>>>(A);
+    RL_LAUNCH_CHECK();
+}
+
+void dump_tree(Ctx& c, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax, uint32_t* cnt_exc,
+               uint32_t* cnt_inh, double* pos_exc, double* pos_inh) {
+    const uint32_t m = c.tree.num_nodes;
+    cudaStream_t st = c.stream;
+    std::vector<uint2> topo(m);
+    std::vector<double4> r0(m), r1(m);
+    std::vector<double> b[6];
+    RL_CUDA_TRY(cudaMemcpyAsync(topo.data(), c.tree.topo.p, m * sizeof(uint2), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaMemcpyAsync(r0.data(), c.tree.rec[0].p, m * sizeof(double4), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaMemcpyAsync(r1.data(), c.tree.rec[1].p, m * sizeof(double4), cudaMemcpyDeviceToHost, st));
+    for (int a = 0; a < 3; ++a) {
+        b[a].resize(m);
+        b[3 + a].resize(m);
+        RL_CUDA_TRY(cudaMemcpyAsync(b[a].data(), c.tree.bmin[a].p, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        RL_CUDA_TRY(cudaMemcpyAsync(b[3 + a].data(), c.tree.bmax[a].p, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    const double nan = __builtin_nan("");
+    for (uint32_t i = 0; i < m; ++i) {
+        const bool leaf = topo_leaf(topo[i].y);
+        if (level) level[i] = (int32_t)topo_level(topo[i].y);
+        if (neuron) neuron[i] = leaf ? (int32_t)topo[i].x : -1;
+        if (child_mask) child_mask[i] = (uint8_t)topo_mask(topo[i].y);
+        if (first_child) first_child[i] = leaf ? -1 : (int32_t)topo[i].x;
+        for (int a = 0; a < 3; ++a) {
+            if (bmin) bmin[3 * (size_t)i + a] = b[a][i];
+            if (bmax) bmax[3 * (size_t)i + a] = b[3 + a][i];
+        }
+        uint64_t ce, ci;
+        __builtin_memcpy(&ce, &r0[i].w, 8);
+        __builtin_memcpy(&ci, &r1[i].w, 8);
+        if (cnt_exc) cnt_exc[i] = (uint32_t)ce;
+        if (cnt_inh) cnt_inh[i] = (uint32_t)ci;
+        const bool he = leaf || (uint32_t)ce > 0;
+        const bool hi = leaf || (uint32_t)ci > 0;
+        if (pos_exc) {
+            pos_exc[3 * (size_t)i] = he ? r0[i].x : nan;
+            pos_exc[3 * (size_t)i + 1] = he ? r0[i].y : nan;
+            pos_exc[3 * (size_t)i + 2] = he ? r0[i].z : nan;
+        }
+        if (pos_inh) {
+            pos_inh[3 * (size_t)i] = hi ? r1[i].x : nan;
+            pos_inh[3 * (size_t)i + 1] = hi ? r1[i].y : nan;
+            pos_inh[3 * (size_t)i + 2] = hi ? r1[i].z : nan;
+        }
+    }
+}
+
+}  // namespace rl

@@ -1,0 +1,125 @@
+// Device-resident state of one network (one rl_ctx).
+#pragma once
+
+#include "rl_internal.cuh"
+
+namespace rl {
+
+// Octree levels encoded in the two key words (3 bits per level, 21 per word).
+constexpr int kLevelsPerWord = 21;
+constexpr int kMaxLevels = 2 * kLevelsPerWord;  // deepest leaf level + 1 representable
+
+// Node topology word y: child mask (bits 0-7), leaf flag (bit 8), level (bits 16-31).
+__host__ __device__ __forceinline__ uint32_t topo_mask(uint32_t y) { return y & 0xFFu; }
+__host__ __device__ __forceinline__ bool topo_leaf(uint32_t y) { return (y >> 8) & 1u; }
+__host__ __device__ __forceinline__ uint32_t topo_level(uint32_t y) { return y >> 16; }
+
+#if defined(__CUDACC__)
+// Read-only 32-byte record load through the non-coherent path.
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+#endif
+
+// The octree in breadth-first order (root first; within a level, Morton order).
+struct Tree {
+    uint32_t num_nodes = 0;
+    uint32_t max_level = 0;
+    bool root_is_leaf = false;
+    uint32_t root_neuron = 0;
+    DBuf<double4> rec[2];     // per dendrite type: centroid (x, y, z), w = count bits (low 32)
+    DBuf<uint2> topo;         // x: first child (inner) or neuron id (leaf); y: see topo_*
+    DBuf<double> maxdim;      // BoundingBox::get_maximum_difference of the cell
+    DBuf<double> bmin[3], bmax[3];
+    DBuf<int32_t> parent;
+    DBuf<uint32_t> first_key;  // Morton rank of the first neuron under the node
+    DBuf<uint32_t> leaf_of;    // neuron -> node
+    DBuf<uint32_t> morton;     // Morton rank -> neuron
+    DBuf<uint32_t> arrive;     // bottom-up arrival counters
+};
+
+struct Neurons {
+    DBuf<double> px, py, pz;    // positions (SoA)
+    DBuf<uint8_t> signal;       // 0 excitatory, 1 inhibitory
+    DBuf<uint8_t> enabled;      // NeuronsExtraInfo disable flags (1 = enabled)
+    DBuf<uint8_t> update;       // takes part in plasticity
+    DBuf<double> x, u, calcium, target, input;
+    DBuf<uint8_t> fired[2];     // double-buffered fired flags
+    int cur = 0;                // fired[cur] holds the last step's flags
+    DBuf<double> grown[3], delta[3];
+    DBuf<uint32_t> connected[3], vacant[3];
+    DBuf<uint32_t> search_vacant;  // vacant axons handed to the next search
+};
+
+// Synapse list kept as CSR over targets (one entry per synapse, weight +-1 or
+// an aggregated integer weight) plus an append buffer for the current update.
+struct Graph {
+    uint64_t num_edges = 0;
+    DBuf<uint32_t> offsets;  // n + 1
+    DBuf<uint32_t> src;
+    DBuf<int32_t> weight;
+    DBuf<uint32_t> new_tgt, new_src;
+    DBuf<int32_t> new_w;
+    uint64_t num_new = 0;
+};
+
+struct Search {
+    DBuf<uint32_t> counts;   // per Morton rank, per type
+    DBuf<uint32_t> src, jj;  // search list: exc segment then inh segment
+    DBuf<int32_t> target;    // result per search (-1 failure)
+    DBuf<uint32_t> first_fail;   // per neuron: smallest failing j
+    DBuf<uint32_t> req_count;    // per neuron: valid requests
+    DBuf<uint32_t> req_off;      // per neuron: output offset
+    DBuf<uint32_t> req_tgt, req_src, req_j, req_sig;  // requests in (source, j) order
+    uint64_t num_searches = 0;
+    uint64_t num_exc = 0;
+    uint64_t num_requests = 0;
+    // connector
+    DBuf<uint64_t> ckey;
+    DBuf<uint32_t> cidx;
+    DBuf<uint32_t> gkey;
+    DBuf<uint32_t> accepted;
+    DBuf<uint32_t> rank;
+    DBuf<uint32_t> flags;
+};
+
+struct Ctx {
+    rl_config cfg{};
+    uint32_t n = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    bool positions_set = false;
+    Tree tree;
+    Neurons nr;
+    Graph graph;
+    Search search;
+    PrimScratch prim;
+    DBuf<uint32_t> err;       // device error word
+    DBuf<uint64_t> counters;  // device counters
+    rl_stats stats{};
+};
+
+// octree.cu
+void build_octree(Ctx& c, const double* h_xyz);
+void update_tree(Ctx& c);  // leaf counts from nr.vacant[1..2] and nr.update, then the reduction
+void dump_tree(Ctx& c, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax, uint32_t* cnt_exc,
+               uint32_t* cnt_inh, double* pos_exc, double* pos_inh);
+
+// bh_search.cu
+void run_search(Ctx& c, uint32_t step);  // fills search.req_* (requests in (source, j) order)
+
+// connector.cu
+uint64_t run_connector(Ctx& c, uint32_t step);  // accepts requests, updates elements, appends new edges
+void rebuild_graph(Ctx& c);                     // merge new edges into the CSR
+void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w);
+
+// activity.cu
+void run_activity_step(Ctx& c, uint32_t step);
+uint64_t run_commit(Ctx& c);  // returns bound elements to delete
+
+void check_device_error(Ctx& c, const char* phase);
+
+}  // namespace rl

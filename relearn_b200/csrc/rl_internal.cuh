@@ -1,0 +1,121 @@
+// Internal declarations shared by the translation units of librelearn_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/relearn_b200.h"
+
+namespace rl {
+
+// ------------------------------------------------------------------ errors
+struct Error {
+    rl_status status;
+    std::string message;
+};
+
+#define RL_CUDA_TRY(expr)                                                                              \
+    do {                                                                                               \
+        cudaError_t _e = (expr);                                                                       \
+        if (_e != cudaSuccess) {                                                                       \
+            throw ::rl::Error{ _e == cudaErrorMemoryAllocation ? RL_ERR_OOM : RL_ERR_DEVICE,           \
+                               std::string(#expr) + ": " + cudaGetErrorString(_e) };                   \
+        }                                                                                              \
+    } while (0)
+
+#define RL_CHECK(cond, status, msg)                        \
+    do {                                                   \
+        if (!(cond)) {                                     \
+            throw ::rl::Error{ (status), std::string(msg) }; \
+        }                                                  \
+    } while (0)
+
+// Every kernel launch of the library goes through this counter.
+extern uint64_t g_launches;
+
+#define RL_LAUNCH_CHECK()                          \
+    do {                                           \
+        ++::rl::g_launches;                        \
+        RL_CUDA_TRY(cudaPeekAtLastError());        \
+    } while (0)
+
+constexpr int kSmCount = 148;
+
+inline unsigned blocks_for(uint64_t n, unsigned threads) {
+    uint64_t b = (n + threads - 1) / threads;
+    if (b == 0) {
+        b = 1;
+    }
+    return (unsigned)b;
+}
+
+// Device error word bits (written by kernels, read by the host after a phase).
+enum DeviceError : uint32_t {
+    DERR_NONE = 0,
+    DERR_OUT_OF_BOX = 1u << 0,      // a position outside the root cell
+    DERR_DUPLICATE = 1u << 1,       // two positions share all key levels
+    DERR_STACK = 1u << 2,           // traversal stack overflow
+    DERR_NO_CROSSING = 1u << 3,     // pick scan found no crossing
+    DERR_CAPACITY = 1u << 4,        // a device buffer was too small
+    DERR_CONNECT = 1u << 5,         // connector bookkeeping underflow
+    DERR_TIMEOUT = 1u << 6,         // bounded wait ran out
+};
+
+// ------------------------------------------------------------- device buffer
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        if (count == 0) {
+            count = 1;
+        }
+        RL_CUDA_TRY(cudaMalloc((void**)&p, count * sizeof(T)));
+        n = count;
+    }
+    void ensure(size_t count) {
+        if (count > n || p == nullptr) {
+            size_t c = n ? n : 1;
+            while (c < count) {
+                c *= 2;
+            }
+            alloc(c);
+        }
+    }
+    void release() {
+        if (p) {
+            cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+};
+
+// ------------------------------------------------------------- primitives
+// Scratch for the primitives; grows on demand.
+struct PrimScratch {
+    DBuf<uint32_t> a, b, c;
+    DBuf<uint64_t> k64;
+    DBuf<uint32_t> v32;
+};
+
+// out[i] = sum_{j<i} in[i]; returns the total (synchronous read of one word).
+// in and out may alias.
+uint32_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n, PrimScratch& s, cudaStream_t st);
+// Same without the host read: returns a device pointer to the total.
+uint32_t* exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint64_t n, PrimScratch& s, cudaStream_t st);
+
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of the
+// keys.  keys/vals are sorted in place (ping-pong through the scratch).
+void radix_sort_u64(uint64_t* keys, uint32_t* vals, uint64_t n, int bits, PrimScratch& s, cudaStream_t st);
+void radix_sort_u32(uint32_t* keys, uint32_t* vals, uint64_t n, int bits, PrimScratch& s, cudaStream_t st);
+
+}  // namespace rl

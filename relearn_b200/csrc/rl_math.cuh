@@ -1,0 +1,311 @@
+// Shared arithmetic for the structural-plasticity hot path.
+//
+// Every function here is __host__ __device__ and uses only IEEE-754 binary64
+// additions, multiplications, divisions and square roots (each correctly
+// rounded on both sides) plus integer bit manipulation.  The translation units
+// that include this header are compiled without multiply-add contraction
+// (nvcc -fmad=false, g++ -ffp-contract=off), so host and device produce the
+// same bits for the same inputs.  That is what makes the FP64 path bit-exact
+// against the CPU oracle.
+//
+// Contents
+//   * rl_philox4x32_10 : Philox4x32-10 counter-based generator (Salmon, Moraes,
+//     Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11).  It
+//     replaces the reference's thread_local std::mt19937 draws
+//     (relearn/source/util/Random.h:245-283) by a stream keyed on
+//     (seed, step, neuron, sub-index, stream/depth).
+//   * rl_exp, rl_log   : exponential and natural log written from the
+//     mathematics (Cody-Waite argument reduction + Taylor / atanh series).
+//     They stand in for std::exp in GaussianDistributionKernel::get_probability
+//     (relearn/source/algorithm/Kernel/Gaussian.h:62-68) and
+//     gaussian_growth_curve (relearn/source/neurons/synaptic_elements/GrowthCurves.h:30-53).
+//   * rl_hypot3        : the three-argument hypot of libstdc++ (scale by the
+//     largest magnitude, then sqrt of the sum of scaled squares), which the
+//     reference reaches through Vec3::calculate_2_norm
+//     (relearn/external/cpp-utility/data-structure/Vec3.hpp:549-551).
+//   * rl_normal_quantile: Wichura's AS241 (PPND16) rational approximation of
+//     the standard normal quantile (Applied Statistics 37 (1988) 477-484); one
+//     uniform per normal draw, replacing boost::random::normal_distribution
+//     (relearn/source/util/Random.h:128-140).
+#pragma once
+
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define RL_HD __host__ __device__ __forceinline__
+#else
+#define RL_HD inline
+#endif
+
+namespace rl {
+
+// ---------------------------------------------------------------- bit casts
+RL_HD uint64_t as_u64(double x) {
+#if defined(__CUDA_ARCH__)
+    return (uint64_t)__double_as_longlong(x);
+#else
+    uint64_t u;
+    __builtin_memcpy(&u, &x, sizeof(u));
+    return u;
+#endif
+}
+
+RL_HD double as_f64(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)u);
+#else
+    double x;
+    __builtin_memcpy(&x, &u, sizeof(x));
+    return x;
+#endif
+}
+
+// ------------------------------------------------------------------ Philox
+struct u32x4 {
+    uint32_t x, y, z, w;
+};
+
+RL_HD void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+    const uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
+// Philox4x32 with 10 rounds.  Round function and constants as published:
+// multipliers 0xD2511F53 / 0xCD9E8D57, Weyl key increments 0x9E3779B9 /
+// 0xBB67AE85.
+RL_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+        c = u32x4{ hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0 };
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Stream identifiers (upper byte of the fourth counter word).
+enum Stream : uint32_t {
+    STREAM_BH_PICK = 1,    // Barnes-Hut weighted pick (per descent)
+    STREAM_CONNECTOR = 2,  // connector shuffle key (per request)
+    STREAM_NOISE = 3,      // normal background input (per neuron-step)
+    STREAM_DELETION = 4,   // synapse deletion picks
+};
+
+// Draw the four words keyed on (seed, step, neuron, sub, stream, depth).
+RL_HD u32x4 draw(uint64_t seed, uint32_t step, uint32_t neuron, uint32_t sub, uint32_t stream, uint32_t depth) {
+    const u32x4 ctr{ step, neuron, sub, (stream << 24) | (depth & 0xFFFFFFu) };
+    return philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// 53 random bits from two words.
+RL_HD uint64_t bits53(const u32x4& r) {
+    return ((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11);
+}
+
+// Uniform double in [0, 1).
+RL_HD double uniform01(const u32x4& r) {
+    return (double)bits53(r) * 1.1102230246251565404e-16;  // 2^-53
+}
+
+// Uniform double in the open interval (0, 1).
+RL_HD double uniform_open01(const u32x4& r) {
+    return ((double)bits53(r) + 0.5) * 1.1102230246251565404e-16;
+}
+
+// 64-bit key (connector shuffle).
+RL_HD uint64_t bits64(const u32x4& r) {
+    return ((uint64_t)r.x << 32) | (uint64_t)r.y;
+}
+
+// -------------------------------------------------------------- exp / log
+// ln 2 split so that k * LN2_HI is exact for |k| < 2^20.
+#define RL_LN2_HI 0.6931467056274414
+#define RL_LN2_LO 4.7493250390316726e-07
+#define RL_INV_LN2 1.4426950408889634
+
+// y * 2^k for y in [0.5, 2) and k in [-1080, 1030]; one rounding at most.
+RL_HD double scale_pow2(double y, int k) {
+    if (k > 1023) {
+        y = y * as_f64((uint64_t)(1023 + 1023) << 52);
+        k -= 1023;
+        if (k > 1023) {
+            k = 1023;
+        }
+        return y * as_f64((uint64_t)(k + 1023) << 52);
+    }
+    if (k < -1021) {
+        // exact move into the normal range, then a single rounding into the subnormals
+        const double t = y * as_f64((uint64_t)(k + 54 + 1023) << 52);
+        return t * as_f64((uint64_t)(-54 + 1023) << 52);
+    }
+    return y * as_f64((uint64_t)(k + 1023) << 52);
+}
+
+// exp(x): x = k ln2 + r with |r| <= ln2/2, exp(r) from its Taylor series to
+// degree 13 (truncation error < 5e-18), result scaled by 2^k.
+RL_HD double rl_exp(double x) {
+    if (x != x) {
+        return x;
+    }
+    if (x > 709.782712893384) {
+        return as_f64(0x7FF0000000000000ull);
+    }
+    if (x < -745.1332191019412) {
+        return 0.0;
+    }
+    const double kd = floor(x * RL_INV_LN2 + 0.5);
+    const double r = (x - kd * RL_LN2_HI) - kd * RL_LN2_LO;
+    // p = sum_{n=2..13} r^(n-2) / n!
+    double p = 1.6059043836821614599e-10;   // 1/13!
+    p = p * r + 2.0876756987868098979e-09;  // 1/12!
+    p = p * r + 2.5052108385441718775e-08;  // 1/11!
+    p = p * r + 2.7557319223985890653e-07;  // 1/10!
+    p = p * r + 2.7557319223985890653e-06;  // 1/9!
+    p = p * r + 2.4801587301587301587e-05;  // 1/8!
+    p = p * r + 1.9841269841269841270e-04;  // 1/7!
+    p = p * r + 1.3888888888888888889e-03;  // 1/6!
+    p = p * r + 8.3333333333333333333e-03;  // 1/5!
+    p = p * r + 4.1666666666666666667e-02;  // 1/4!
+    p = p * r + 1.6666666666666666667e-01;  // 1/3!
+    p = p * r + 0.5;                        // 1/2!
+    const double y = 1.0 + (r + (r * r) * p);
+    return scale_pow2(y, (int)kd);
+}
+
+// log(x) for finite x > 0 (normal range): x = m 2^e with m in
+// [sqrt(2)/2, sqrt(2)), log(m) = 2 atanh(s), s = (m-1)/(m+1), odd series in s.
+RL_HD double rl_log(double x) {
+    uint64_t b = as_u64(x);
+    int e = (int)((b >> 52) & 0x7FF) - 1023;
+    double m = as_f64((b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull);
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    const double f = m - 1.0;
+    const double s = f / (2.0 + f);
+    const double z = s * s;
+    double R = 1.0 / 23.0;
+    R = R * z + 1.0 / 21.0;
+    R = R * z + 1.0 / 19.0;
+    R = R * z + 1.0 / 17.0;
+    R = R * z + 1.0 / 15.0;
+    R = R * z + 1.0 / 13.0;
+    R = R * z + 1.0 / 11.0;
+    R = R * z + 1.0 / 9.0;
+    R = R * z + 1.0 / 7.0;
+    R = R * z + 1.0 / 5.0;
+    R = R * z + 1.0 / 3.0;
+    R = R * z;
+    const double two_s = 2.0 * s;
+    const double logm = two_s + two_s * R;
+    const double ed = (double)e;
+    return ed * RL_LN2_HI + (logm + ed * RL_LN2_LO);
+}
+
+// ----------------------------------------------------------------- hypot3
+RL_HD double rl_hypot3(double x, double y, double z) {
+    x = fabs(x);
+    y = fabs(y);
+    z = fabs(z);
+    const double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+    if (a == 0.0) {
+        return 0.0;
+    }
+    const double xs = x / a;
+    const double ys = y / a;
+    const double zs = z / a;
+    return a * sqrt(xs * xs + ys * ys + zs * zs);
+}
+
+// std::nextafter(total, total + 1e-5) for finite total > 0
+// (ProbabilityPicker.h:108 of the reference).
+RL_HD double next_up_eps(double total) {
+    const double toward = total + 1e-5;
+    if (toward > total) {
+        return as_f64(as_u64(total) + 1);
+    }
+    return total;
+}
+
+// ------------------------------------------------------ normal quantile
+// AS241 / PPND16: standard normal quantile for p in (0, 1).
+RL_HD double normal_quantile(double p) {
+    const double q = p - 0.5;
+    if (fabs(q) <= 0.425) {
+        const double r = 0.180625 - q * q;
+        double num = 2.5090809287301226727e+3;
+        num = num * r + 3.3430575583588128105e+4;
+        num = num * r + 6.7265770927008700853e+4;
+        num = num * r + 4.5921953931549871457e+4;
+        num = num * r + 1.3731693765509461125e+4;
+        num = num * r + 1.9715909503065514427e+3;
+        num = num * r + 1.3314166789178437745e+2;
+        num = num * r + 3.3871328727963666080e+0;
+        double den = 5.2264952788528545610e+3;
+        den = den * r + 2.8729085735721942674e+4;
+        den = den * r + 3.9307895800092710610e+4;
+        den = den * r + 2.1213794301586595867e+4;
+        den = den * r + 5.3941960214247511077e+3;
+        den = den * r + 6.8718700749205790830e+2;
+        den = den * r + 4.2313330701600911252e+1;
+        den = den * r + 1.0;
+        return (num * q) / den;
+    }
+    double r = q < 0.0 ? p : 1.0 - p;
+    r = sqrt(-rl_log(r));
+    double num;
+    double den;
+    if (r <= 5.0) {
+        r = r - 1.6;
+        num = 7.7454501427834140764e-4;
+        num = num * r + 2.2723844989269184583e-2;
+        num = num * r + 2.4178072517745061177e-1;
+        num = num * r + 1.2704582524523683826e+0;
+        num = num * r + 3.6478483247632046050e+0;
+        num = num * r + 5.7694972214606914055e+0;
+        num = num * r + 4.6303378461565452959e+0;
+        num = num * r + 1.4234371107496835773e+0;
+        den = 1.0507500716444168432e-9;
+        den = den * r + 5.4759380849953449460e-4;
+        den = den * r + 1.5198666563616457197e-2;
+        den = den * r + 1.4810397642748007459e-1;
+        den = den * r + 6.8976733498510000455e-1;
+        den = den * r + 1.6763848301838038494e+0;
+        den = den * r + 2.0531916266377588219e+0;
+        den = den * r + 1.0;
+    } else {
+        r = r - 5.0;
+        num = 2.0103343992922881327e-7;
+        num = num * r + 2.7115555687434875782e-5;
+        num = num * r + 1.2426609473880784386e-3;
+        num = num * r + 2.6532189526576123093e-2;
+        num = num * r + 2.9656057182850489123e-1;
+        num = num * r + 1.7848265399172913358e+0;
+        num = num * r + 5.4637849111641143699e+0;
+        num = num * r + 6.6579046435011037772e+0;
+        den = 2.0442631033899397856e-15;
+        den = den * r + 1.4215117583164458887e-7;
+        den = den * r + 1.8463183175100546818e-5;
+        den = den * r + 7.8686913114561325910e-4;
+        den = den * r + 1.4875361290850614853e-2;
+        den = den * r + 1.3692988092273580531e-1;
+        den = den * r + 5.9983220655588793769e-1;
+        den = den * r + 1.0;
+    }
+    const double x = num / den;
+    return q < 0.0 ? -x : x;
+}
+
+// Normal(mean, stddev) background draw for (seed, step, neuron).
+RL_HD double background_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
+    const u32x4 r = draw(seed, step, neuron, 0u, STREAM_NOISE, 0u);
+    return mean + stddev * normal_quantile(uniform_open01(r));
+}
+
+}  // namespace rl

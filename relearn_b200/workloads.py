@@ -1,0 +1,64 @@
+"""Seeded synthetic networks with the shapes of the benchmark configurations.
+
+The reference places ``--num-neurons`` neurons on a jittered grid shuffled by
+a fixed seed (sim/random/BoxBasedRandomSubdomainAssignment.cpp:26-131); the
+workloads here instead draw positions from a seeded generator and hand them
+over as a position list, which the reference also accepts (a positions file,
+io/NeuronIO.cpp:229-270).  Signal types are 80 % excitatory / 20 % inhibitory
+after a seeded shuffle.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def uniform_cube(n: int, side: float, seed: int) -> np.ndarray:
+    """n positions uniform in [0, side)^3."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.0, side, size=(n, 3))
+
+
+def gaussian_mixture(n: int, side: float, seed: int, components: int = 64, std: float = 200.0) -> np.ndarray:
+    """n positions from an isotropic Gaussian mixture (centres uniform in the
+    cube, component std `std`), samples outside the cube rejected."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.0, side, size=(components, 3))
+    out = np.empty((0, 3))
+    while len(out) < n:
+        k = rng.integers(0, components, size=2 * n)
+        p = centres[k] + rng.normal(0.0, std, size=(2 * n, 3))
+        ok = np.all((p >= 0.0) & (p < side), axis=1)
+        out = np.concatenate([out, p[ok]])
+    return np.ascontiguousarray(out[:n])
+
+
+def signal_types(n: int, seed: int, inhibitory_fraction: float = 0.2) -> np.ndarray:
+    """0 = excitatory, 1 = inhibitory; round(n * fraction) inhibitory after a seeded shuffle."""
+    rng = np.random.default_rng(seed + 7919)
+    sig = np.zeros(n, np.uint8)
+    k = int(round(n * inhibitory_fraction))
+    sig[rng.permutation(n)[:k]] = 1
+    return sig
+
+
+def initial_elements(n: int, seed: int, lower: float, upper: float) -> list:
+    """Initial grown elements per type uniform in [lower, upper] (the reference's
+    --synaptic-elements-lower-bound / --synaptic-elements-upper-bound,
+    relearn.cpp:620-624, 1179-1185).  Returns [(grown, vacant)] for axon,
+    excitatory dendrite and inhibitory dendrite; vacant = floor(grown) as in
+    ElementBaseBase::init_values (ElementBaseBase.h:390-420) with nothing
+    connected."""
+    rng = np.random.default_rng(seed + 104729)
+    out = []
+    for _ in range(3):
+        g = rng.uniform(lower, upper, size=n) if upper > lower else np.full(n, float(lower))
+        out.append((g, np.floor(g).astype(np.uint32)))
+    return out
+
+
+def ensure_distinct(pos: np.ndarray) -> np.ndarray:
+    """The point-region octree needs pairwise distinct positions."""
+    u = np.unique(pos, axis=0)
+    if len(u) != len(pos):
+        raise ValueError("positions are not pairwise distinct")
+    return pos

@@ -1,0 +1,21 @@
+// Host build of the product's shared arithmetic header, for the agreement
+// test against the oracle (compiled with g++ -ffp-contract=off).
+#include "../../relearn_b200/csrc/rl_math.cuh"
+
+extern "C" {
+double probe_exp(double x) { return rl::rl_exp(x); }
+double probe_log(double x) { return rl::rl_log(x); }
+double probe_hypot3(double x, double y, double z) { return rl::rl_hypot3(x, y, z); }
+double probe_quantile(double p) { return rl::normal_quantile(p); }
+double probe_normal(unsigned long long seed, unsigned step, unsigned neuron, double mean, double sd) {
+    return rl::background_normal(seed, step, neuron, mean, sd);
+}
+void probe_philox(unsigned c0, unsigned c1, unsigned c2, unsigned c3, unsigned k0, unsigned k1, unsigned* out) {
+    const rl::u32x4 r = rl::philox4x32_10(rl::u32x4{ c0, c1, c2, c3 }, k0, k1);
+    out[0] = r.x;
+    out[1] = r.y;
+    out[2] = r.z;
+    out[3] = r.w;
+}
+double probe_next_up(double t) { return rl::next_up_eps(t); }
+}

@@ -1,0 +1,132 @@
+"""CPU checks of the C-ABI boundary and of the host-side code: the library
+loads and exports every entry point declared in include/relearn_b200.h, the
+ctypes mirror matches the C struct layout, and the product's shared arithmetic
+header agrees bit for bit with the oracle's statement of it."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "relearn_b200.h")
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from relearn_b200 import build
+
+    return build.build()
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"RL_API\s+[\w\s\*]+?\b(rl_\w+)\s*\(", text)))
+
+
+def test_header_and_mirror_agree():
+    import relearn_b200
+
+    assert declared_functions() == sorted(relearn_b200.ABI_FUNCTIONS)
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\sT\s(rl_\w+)", out))
+    missing = [f for f in declared_functions() if f not in exported]
+    assert not missing, missing
+    lib = C.CDLL(built_lib)
+    for f in declared_functions():
+        assert hasattr(lib, f)
+
+
+def test_struct_layout(tmp_path):
+    import relearn_b200 as R
+
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), os.path.join(ROOT, "tests", "helpers", "abi_layout.c")], check=True)
+    lines = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if l)
+    assert int(lines["rl_config"]) == C.sizeof(R.RlConfig)
+    assert int(lines["rl_stats"]) == C.sizeof(R.RlStats)
+    assert int(lines["rl_request"]) == R.REQUEST_DTYPE.itemsize
+    assert int(lines["rl_synapse"]) == R.SYNAPSE_DTYPE.itemsize
+    for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device"):
+        assert int(lines[f"rl_config.{f}"]) == getattr(R.RlConfig, f).offset
+    assert int(lines["rl_stats.max_level"]) == R.RlStats.max_level.offset
+
+
+def test_host_only_entry_points(built_lib):
+    import relearn_b200 as R
+
+    L = R.load_library()
+    assert L.rl_abi_version() == 1
+    cfg = R.RlConfig()
+    L.rl_config_default(C.byref(cfg), 2000, 1000.0)
+    # reference defaults: Parameters.h:123-130, CalciumCalculatorBase.h:206-210, Gaussian.h:38-39
+    assert (cfg.iz_a, cfg.iz_b, cfg.iz_c, cfg.iz_d) == (0.1, 0.2, -65.0, 2.0)
+    assert (cfg.beta, cfg.tau_c, cfg.target_calcium, cfg.h_calcium) == (0.001, 10000.0, 0.7, 10)
+    assert (cfg.sigma, cfg.mu, cfg.theta, cfg.plasticity_interval) == (750.0, 0.0, 0.3, 100)
+    assert L.rl_status_string(1) == b"invalid argument or state"
+
+
+def test_create_without_device_fails_cleanly(built_lib):
+    from conftest import has_gpu
+
+    if has_gpu():
+        pytest.skip("a device is present")
+    import relearn_b200 as R
+
+    with pytest.raises(R.RelearnError) as e:
+        R.Network(R.default_params(10, 100.0))
+    assert e.value.status == 3  # RL_ERR_DEVICE
+
+
+def test_invalid_config_is_rejected(built_lib):
+    import relearn_b200 as R
+
+    p = R.default_params(10, 100.0)
+    p["theta"] = 0.7  # above Constants::bh_max_theta
+    with pytest.raises(R.RelearnError) as e:
+        R.Network(p)
+    assert e.value.status in (1, 3)
+
+
+@pytest.fixture(scope="module")
+def probe(tmp_path_factory):
+    so = tmp_path_factory.mktemp("probe") / "probe.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(so),
+                    os.path.join(ROOT, "tests", "helpers", "math_probe.cpp")], check=True)
+    L = C.CDLL(str(so))
+    for name in ("probe_exp", "probe_log", "probe_quantile", "probe_next_up"):
+        getattr(L, name).restype = C.c_double
+        getattr(L, name).argtypes = [C.c_double]
+    L.probe_hypot3.restype = C.c_double
+    L.probe_hypot3.argtypes = [C.c_double] * 3
+    L.probe_normal.restype = C.c_double
+    L.probe_normal.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double]
+    L.probe_philox.argtypes = [C.c_uint32] * 6 + [C.c_void_p]
+    return L
+
+
+def test_shared_math_bitwise_agreement(probe, oracle_mod):
+    O = oracle_mod.lib()
+    rng = np.random.default_rng(8)
+    for x in np.concatenate([rng.uniform(-746, 710, 30000), rng.uniform(-2, 2, 10000), [-745.0, -740.0, 0.0, 709.7]]):
+        assert probe.probe_exp(float(x)) == O.orc_exp(float(x)) or (np.isnan(probe.probe_exp(float(x))))
+    for y in np.exp(rng.uniform(-37, 0, 20000)):
+        assert probe.probe_log(float(y)) == O.orc_log(float(y))
+    for p in rng.uniform(0, 1, 20000):
+        assert probe.probe_quantile(float(p)) == O.orc_quantile(float(p))
+    for v in rng.uniform(-1e4, 1e4, (5000, 3)):
+        assert probe.probe_hypot3(*map(float, v)) == O.orc_hypot3(*map(float, v))
+    for s in range(1, 4):
+        for i in range(2000):
+            assert probe.probe_normal(42, s, i, 5.0, 2.0) == O.orc_normal(42, s, i, 5.0, 2.0)
+    out = np.zeros(4, np.uint32)
+    for c in rng.integers(0, 2**32, (500, 6), dtype=np.uint64):
+        probe.probe_philox(*map(int, c), out.ctypes.data_as(C.c_void_p))
+        assert list(out) == oracle_mod.philox(*map(int, c))
+    for t in rng.uniform(1e-3, 1e6, 1000):
+        assert probe.probe_next_up(float(t)) == np.nextafter(float(t), float(t) + 1e-5)

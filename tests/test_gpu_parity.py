@@ -1,0 +1,215 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Integer and index results (octree structure, counts, requests, synapses,
+fired flags) must be bit-identical; FP64 results (potentials, calcium,
+centroids, growth) are compared bit for bit as well, which is stricter than
+the 1e-12 relative bound the path promises (RTOL below)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import oracle_params, seed_elements, small_network
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12  # promised bound for FP64 state; the assertions below are exact
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def same_f64(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def assert_tree_equal(g, o, with_values=True):
+    for k in ("level", "neuron", "child_mask", "first_child"):
+        assert np.array_equal(g[k], o[k]), k
+    for k in ("bmin", "bmax"):
+        assert same_f64(g[k], o[k]), k
+    if with_values:
+        for k in ("cnt_exc", "cnt_inh"):
+            assert np.array_equal(g[k], o[k]), k
+        for k in ("pos_exc", "pos_inh"):
+            assert same_f64(g[k], o[k]), k
+
+
+def net_and_oracle(n, side, seed, mixture=False):
+    from oracle import oracle as O
+    from relearn_b200 import Network
+
+    params, pos, sig = small_network(n, side, seed, mixture)
+    net = Network(params)
+    net.set_positions(pos, sig)
+    sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    return net, sim, params, pos, sig
+
+
+@pytest.mark.parametrize("n,mixture", [(1, False), (2, False), (3, False), (100, False), (2000, False), (3000, True), (60000, False),
+                                       (60000, True)])
+def test_octree_and_reduction(n, mixture):
+    net, sim, *_ = net_and_oracle(n, 1000.0 * (n / 2000) ** (1 / 3) + 10.0, 31 + n, mixture)
+    assert_tree_equal(net.tree(), sim.tree(), with_values=False)
+    rng = np.random.default_rng(n)
+    ve = rng.integers(0, 4, n).astype(np.uint32)
+    vi = rng.integers(0, 3, n).astype(np.uint32)
+    ve[rng.random(n) < 0.3] = 0
+    net.prepare_update_connectivity(np.zeros(n, np.uint32), ve, vi)
+    sim.update_tree(ve, vi)
+    assert_tree_equal(net.tree(), sim.tree())
+
+
+@pytest.mark.parametrize("n,mixture,lower,upper", [(2000, False, 0.0, 3.0), (2000, True, 0.0, 2.0), (30000, False, 1.0, 1.0),
+                                                   (20000, True, 0.0, 4.0)])
+def test_search_requests(n, mixture, lower, upper):
+    net, sim, params, pos, sig = net_and_oracle(n, 1000.0 * (n / 2000) ** (1 / 3), 41 + n, mixture)
+    seed_elements(sim, n, 5, lower, upper)
+    seed_elements(net, n, 5, lower, upper)
+    va, ve, vi = (sim.get_elements(t)["vacant"] for t in range(3))
+    sim.update_tree(ve, vi)
+    net.prepare_update_connectivity(va, ve, vi)
+    for step in (100, 200):
+        g = net.find_targets(step)
+        o = sim.find_targets(step)
+        assert len(g) == len(o) > 0
+        for k in ("target", "source", "j", "signal"):
+            assert np.array_equal(g[k], o[k]), k
+
+
+def test_connector_and_edges():
+    n = 3000
+    net, sim, *_ = net_and_oracle(n, 1100.0, 51)
+    seed_elements(sim, n, 6, 0.0, 4.0)
+    seed_elements(net, n, 6, 0.0, 4.0)
+    va, ve, vi = (sim.get_elements(t)["vacant"] for t in range(3))
+    sim.update_tree(ve, vi)
+    net.prepare_update_connectivity(va, ve, vi)
+    req = sim.find_targets(300)
+    created_o, acc = sim.connect(300, len(req))
+    syn = net.update_connectivity(300)
+    assert len(syn) == created_o
+    got = sorted(zip(syn["target"].tolist(), syn["source"].tolist(), syn["weight"].tolist()))
+    r = req[acc.astype(bool)]
+    exp = sorted(zip(r["target"].tolist(), r["source"].tolist(), np.where(r["signal"] == 1, -1, 1).tolist()))
+    assert got == exp
+    for t in range(3):
+        eg, eo = net.get_elements(t), sim.get_elements(t)
+        assert np.array_equal(eg["connected"], eo["connected"])
+        assert np.array_equal(eg["vacant"], eo["vacant"])
+    for a, b in zip(net.edges(), sim.edges()):
+        assert np.array_equal(a, b)
+
+
+def compare_state(net, sim, n):
+    g, o = net.neurons(), sim.neurons()
+    for k in ("x", "u", "calcium", "input"):
+        assert same_f64(g[k], o[k]), k
+    assert np.array_equal(g["fired"], o["fired"])
+    for t in range(3):
+        eg, eo = net.get_elements(t), sim.get_elements(t)
+        assert same_f64(eg["grown"], eo["grown"]), ("grown", t)
+        assert same_f64(eg["delta"], eo["delta"]), ("delta", t)
+        assert np.array_equal(eg["connected"], eo["connected"]), ("connected", t)
+        assert np.array_equal(eg["vacant"], eo["vacant"]), ("vacant", t)
+    for a, b in zip(net.edges(), sim.edges()):
+        assert np.array_equal(a, b)
+
+
+def test_activity_steps_bitwise():
+    n = 2000
+    net, sim, *_ = net_and_oracle(n, 1000.0, 61)
+    net.activity_block(1, 99)
+    for s in range(1, 100):
+        sim.activity_step(s)
+    compare_state(net, sim, n)
+
+
+def test_seeded_vacancy_simulation():
+    n = 2000
+    net, sim, *_ = net_and_oracle(n, 1000.0, 71)
+    seed_elements(sim, n, 7, 0.0, 3.0)
+    seed_elements(net, n, 7, 0.0, 3.0)
+    net.simulate(1, 1001)
+    sim.simulate(1, 1001)
+    compare_state(net, sim, n)
+    st = net.stats()
+    assert st["synapses_created"] == sim.stats()["created"] > 0
+
+
+def test_config0_organic_20001_steps():
+    """2,000 neurons in a 1000 um cube, reference parameters, 20,001 steps
+    (Simulation::simulate runs number_steps + 1)."""
+    n = 2000
+    net, sim, *_ = net_and_oracle(n, 1000.0, 1)
+    net.simulate(1, 20001)
+    sim.simulate(1, 20001)
+    compare_state(net, sim, n)
+
+
+@pytest.mark.parametrize("name", ["golden_uniform_300.npz", "golden_mixture_400.npz"])
+def test_golden_fixtures(name):
+    from relearn_b200 import Network, default_params
+
+    z = np.load(os.path.join(GOLDEN, name))
+    n = len(z["signal"])
+    params = default_params(n, float(z["side"]))
+    params["seed"] = int(z["seed"])
+    net = Network(params)
+    net.set_positions(z["positions"], z["signal"])
+    seed_elements(net, n, int(z["seed"]) - 1000, float(z["lower"]), float(z["upper"]))
+    va, ve, vi = (net.get_elements(t)["vacant"] for t in range(3))
+    net.prepare_update_connectivity(va, ve, vi)
+    t = net.tree()
+    for k in ("level", "neuron", "child_mask", "first_child", "cnt_exc", "cnt_inh"):
+        assert np.array_equal(t[k], z["tree_" + k]), k
+    for k in ("bmin", "bmax", "pos_exc", "pos_inh"):
+        assert same_f64(t[k], z["tree_" + k]), k
+    req = net.find_targets(100)
+    for k in ("target", "source", "j", "signal"):
+        assert np.array_equal(req[k], z["requests"][k]), k
+    syn = net.update_connectivity(100)
+    e = net.edges()
+    assert np.array_equal(e[0], z["edges_target"]) and np.array_equal(e[1], z["edges_source"]) and np.array_equal(e[2], z["edges_weight"])
+    net2 = Network(params)
+    net2.set_positions(z["positions"], z["signal"])
+    seed_elements(net2, n, int(z["seed"]) - 1000, float(z["lower"]), float(z["upper"]))
+    net2.simulate(1, int(z["steps"]))
+    nr = net2.neurons()
+    for k in ("x", "u", "calcium", "input"):
+        assert same_f64(nr[k], z["final_" + k]), k
+    assert np.array_equal(nr["fired"], z["final_fired"])
+    for tpe in range(3):
+        el = net2.get_elements(tpe)
+        for k in ("grown", "delta"):
+            assert same_f64(el[k], z[f"final_el{tpe}_{k}"]), (tpe, k)
+        for k in ("connected", "vacant"):
+            assert np.array_equal(el[k], z[f"final_el{tpe}_{k}"]), (tpe, k)
+    e = net2.edges()
+    assert np.array_equal(e[0], z["final_edges_target"]) and np.array_equal(e[2], z["final_edges_weight"])
+
+
+def test_search_properties_at_1m():
+    """1M neurons, uniform in a 10,000 um cube, one vacant axon and one vacant
+    dendrite of each type per neuron (the reference benchmark's setting,
+    benchmark/benchmark_barnes_hut_cuda.cpp:53-77): every request targets
+    another neuron, the tree counts add up, and two runs agree."""
+    from relearn_b200 import Network, default_params, workloads
+
+    n = 1_000_000
+    pos = workloads.uniform_cube(n, 10000.0, 3)
+    sig = workloads.signal_types(n, 3)
+    params = default_params(n, 10000.0)
+    net = Network(params)
+    net.set_positions(pos, sig)
+    one = np.ones(n, np.uint32)
+    net.prepare_update_connectivity(one, one, one)
+    t = net.tree()
+    assert t["cnt_exc"][0] == n and t["cnt_inh"][0] == n
+    assert np.sum(t["neuron"] >= 0) == n and len(np.unique(t["neuron"][t["neuron"] >= 0])) == n
+    r1 = net.find_targets(100)
+    r2 = net.find_targets(100)
+    assert len(r1) == n
+    assert np.array_equal(r1["target"], r2["target"])
+    assert np.all(r1["target"] != r1["source"])
+    assert np.array_equal(r1["signal"], sig[r1["source"]])
