@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the structural-plasticity hot path on B200.
+
+Workload (one bench step): one plasticity period of a 1,000,000-neuron
+network — 100 activity steps (input + Izhikevich + calcium + growth, one fused
+kernel each) followed by one plasticity update (commit, octree update,
+Barnes-Hut search, connector, graph rebuild) — with the reference parameters
+(Izhikevich a=0.02 b=0.2 c=-65 d=8, normal(5,2) input, conductance 3,
+sigma 750 um, theta 0.3, growth 1e-4, target calcium 0.7), neurons uniform in
+a 10,000 um cube, FP64.  Metric: neuron-steps/s = N * 100 * K / device time.
+
+A second figure, Barnes-Hut searches/s, is measured on the reference
+benchmark's search snapshot: one vacant axon and one vacant excitatory and
+inhibitory dendrite per neuron (benchmark/benchmark_barnes_hut_cuda.cpp:53-77),
+i.e. 1,000,000 searches per plasticity update.
+
+`--impl reference` times the CPU restatement of the reference's barnes-hut +
+izhikevich path (the oracle) on all host cores for the same metric.
+Multi-GPU: independent replicas (one network per GPU, no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 1_000_000
+SIDE_DEFAULT = 10_000.0
+PERIOD = 100
+# algorithmic bytes of the fused activity kernel per neuron-step (FP64 SoA):
+# reads enabled 1 + x 8 + u 8 + calcium 8 + target 8 + 3 deltas 24 = 57,
+# writes input 8 + x 8 + u 8 + fired 1 + calcium 8 + 3 deltas 24 = 57
+ACT_BYTES_PER_NEURON = 114
+ACT_BYTES_PER_EDGE = 9  # pull over in-edges: source id 4 + weight 4 + fired flag 1
+ACT_BYTES_CSR_ROW = 8   # two row offsets when the graph is not empty
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_network(n, side, seed, placement):
+    from relearn_b200 import Network, default_params, workloads
+
+    params = default_params(n, side)
+    params["seed"] = seed
+    pos = workloads.uniform_cube(n, side, seed) if placement == "uniform" else workloads.gaussian_mixture(n, side, seed)
+    sig = workloads.signal_types(n, seed)
+    return params, pos, sig
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    import relearn_b200 as R
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    n, side = args.neurons, args.side
+    params, pos, sig = build_network(n, side, args.seed + rank, args.placement)
+    params["device"] = local
+    net = R.Network(params)
+    stream = torch.cuda.current_stream(dev)
+    net.set_stream(stream.cuda_stream)
+    net.set_positions(pos, sig)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    step = 1
+    for _ in range(args.warmup):
+        net.simulate(step, PERIOD)
+        step += PERIOD
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = net.stats()["gpu_launches"]
+    net.phase_times()
+    net.set_profiling(True)
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            net.simulate(step, PERIOD)
+            e1.record(stream)
+            step += PERIOD
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize(dev)
+    phases = net.phase_times()
+    net.set_profiling(False)
+    launches = net.stats()["gpu_launches"] - launches0
+    total_ms = float(sum(times))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * PERIOD * args.steps / (total_ms / 1e3)
+
+    # roofline of the dominant kernel (the fused activity kernel)
+    act_ms, act_cnt = phases["activity_kernel"]
+    edges = int(net.stats().get("synapses_created", 0))
+    bytes_per_launch = ACT_BYTES_PER_NEURON * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)
+    hbm, peak_kind = peaks()
+    achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+
+    # e2e through the public C ABI with host buffers: every bench step uploads
+    # the enable flags (a per-step host input of Simulation::simulate's
+    # interrupts) and reads back calcium and fired flags
+    enabled = torch.ones(n, dtype=torch.uint8).pin_memory().numpy()
+    ca = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    fired = torch.empty(n, dtype=torch.uint8).pin_memory().numpy()
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        net.set_enabled(enabled)
+        net.simulate(step, PERIOD)
+        step += PERIOD
+        net.lib.rl_get_neurons(net.h, None, None, ca.ctypes.data, fired.ctypes.data, None)
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    e2e_val = world * n * PERIOD * e2e_steps / e2e_s
+
+    # Barnes-Hut searches on the reference benchmark's snapshot
+    bh = bh_snapshot(net, n, stream, step) if not args.skip_bh else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, params, pos, sig)
+    clocks = clk.summary()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return None
+    line = {
+        "metric": "neuron-steps/s",
+        "value": value,
+        "unit": "neuron-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded positions, reference parameters)",
+        "config": {"workload": f"{n} Izhikevich neurons {args.placement} in a {side:g} um cube, FP64 drop-in; one bench step = "
+                               f"{PERIOD} activity steps + 1 plasticity update", "neurons": n, "placement": args.placement,
+                   "period": PERIOD, "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "kernel": "k_activity", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind,
+                     "bytes_per_launch": bytes_per_launch, "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None},
+        "phases_ms": {k: v[0] for k, v in phases.items()},
+        "e2e": {"value": e2e_val, "unit": "neuron-steps/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 9 * n,
+                "api": "rl_set_enabled + rl_simulate + rl_get_neurons (pinned host buffers)"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if bh:
+        line["bh_search"] = bh
+    if cpu:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+def bh_snapshot(net, n, stream, step):
+    import torch
+
+    one = np.ones(n, np.uint32)
+    grown = np.full(n, 1.5)
+    reps = 3
+    search_ms = []
+    update_ms = []
+    for r in range(reps + 1):
+        for t in range(3):
+            net.set_elements(t, grown, np.zeros(n), np.zeros(n, np.uint32), one)
+        net.set_profiling(True)
+        net.phase_times()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        net.prepare_update_connectivity(one, one, one)
+        net.find_targets(step)
+        e1.record(stream)
+        e1.synchronize()
+        ph = net.phase_times()
+        net.set_profiling(False)
+        if r > 0:
+            search_ms.append(ph["search_kernel"][0])
+            update_ms.append(e0.elapsed_time(e1))
+    searches = n
+    st = net.stats()
+    return {"metric": "BH searches/s", "value": searches / (min(search_ms) / 1e3), "unit": "searches/s",
+            "with_tree_update_and_copies": searches / (min(update_ms) / 1e3), "searches_per_update": searches,
+            "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron"}
+
+
+def cpu_baseline(args, params, pos, sig, activity_steps=None, searches=20000):
+    """The oracle (C++ restatement of the reference's CPU path, OpenMP) on all
+    host cores: a bounded sample of the same workload."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    p = dict(params)
+    p.pop("device", None)
+    p["use_libm"] = 0
+    sim = O.OracleSim(p, pos, sig, threads=threads)
+    steps = activity_steps or PERIOD
+    t0 = time.perf_counter()
+    sim.simulate(1, steps)  # includes the plasticity update at step 100
+    dt = time.perf_counter() - t0
+    n = params["num_neurons"]
+    out = {"value": n * steps / dt, "unit": "neuron-steps/s", "cores": threads, "kind": "port",
+           "sample": f"{n} neurons, {steps} activity steps incl. 1 plasticity update ({dt:.1f} s)"}
+    # search snapshot on a subset of sources
+    one = np.ones(n, np.uint32)
+    sel = np.zeros(n, np.uint32)
+    rng = np.random.default_rng(0)
+    sel[rng.choice(n, size=min(searches, n), replace=False)] = 1
+    for t in range(3):
+        sim.set_elements(t, np.full(n, 1.5), np.zeros(n), np.zeros(n, np.uint32), sel if t == 0 else one)
+    sim.update_tree(one, one)
+    t0 = time.perf_counter()
+    req = sim.find_targets(step := 100)
+    ds = time.perf_counter() - t0
+    out["bh_searches_per_s"] = int(sel.sum()) / ds
+    out["bh_sample"] = f"{int(sel.sum())} searches on the snapshot ({ds:.1f} s)"
+    return out
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    p = dict(params)
+    p.pop("device", None)
+    p["use_libm"] = 0
+    sim = O.OracleSim(p, pos, sig, threads=threads)
+    # each step is a bounded sample: 10 activity steps, plus the plasticity
+    # update every 10th sample step (keeping the 100:1 ratio)
+    sample_steps = 10
+    step = 1
+    for _ in range(args.warmup):
+        sim.simulate(step, sample_steps)
+        step += sample_steps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.simulate(step, sample_steps)
+        step += sample_steps
+    dt = time.perf_counter() - t0
+    value = args.neurons * sample_steps * args.steps / dt
+    return {
+        "impl": "reference",
+        "metric": "neuron-steps/s",
+        "value": value,
+        "unit": "neuron-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded positions, reference parameters)",
+        "config": {"workload": f"{args.neurons} Izhikevich neurons {args.placement} in a {args.side:g} um cube, FP64",
+                   "neurons": args.neurons, "placement": args.placement, "sample_steps_per_step": sample_steps},
+        "cpu_baseline": {"value": value, "unit": "neuron-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample_steps} activity steps of {args.neurons} neurons per step (plasticity update every 100 steps)"},
+        "e2e": {"value": value, "unit": "neuron-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--neurons", type=int, default=N_DEFAULT)
+    ap.add_argument("--side", type=float, default=SIDE_DEFAULT)
+    ap.add_argument("--placement", choices=["uniform", "mixture"], default="uniform")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-bh", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_b200(args, world, rank, local)
+    if line is not None and rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

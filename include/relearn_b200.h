@@ -120,6 +120,18 @@ typedef struct rl_stats {
     uint32_t reserved;
 } rl_stats;
 
+/* Phases timed with CUDA events when profiling is on (rl_set_profiling). */
+enum {
+    RL_PHASE_ACTIVITY_KERNEL = 0, /* the fused activity kernel */
+    RL_PHASE_COMMIT = 1,          /* commit of the synaptic elements */
+    RL_PHASE_TREE_UPDATE = 2,     /* leaf update + bottom-up reduction */
+    RL_PHASE_SEARCH_KERNEL = 3,   /* the Barnes-Hut search kernels */
+    RL_PHASE_SEARCH = 4,          /* search including list building and request compaction */
+    RL_PHASE_CONNECTOR = 5,       /* connector */
+    RL_PHASE_GRAPH = 6,           /* synapse graph rebuild */
+    RL_NUM_PHASES = 7
+};
+
 /* Fill *cfg with the reference defaults for n neurons in the given cube. */
 RL_API void rl_config_default(rl_config* cfg, uint32_t num_neurons, double side);
 
@@ -207,6 +219,17 @@ RL_API rl_status rl_simulate(void* ctx, uint32_t first_step, uint32_t nsteps);
 RL_API rl_status rl_synchronize(void* ctx);
 
 RL_API rl_status rl_get_stats(void* ctx, rl_stats* out);
+
+/* Issue all work of the context on `cuda_stream` (a cudaStream_t of the
+ * context's device), or on the context's own stream when NULL. */
+RL_API rl_status rl_set_stream(void* ctx, void* cuda_stream);
+
+/* Turn per-phase CUDA-event timing on (1) or off (0). */
+RL_API rl_status rl_set_profiling(void* ctx, int enable);
+
+/* Accumulated device milliseconds and invocation counts per phase since the
+ * last call (arrays of RL_NUM_PHASES entries); resets the accumulators. */
+RL_API rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts);
 
 #ifdef __cplusplus
 }

@@ -95,8 +95,9 @@ ABI_FUNCTIONS = [
     "rl_set_positions", "rl_tree_info", "rl_dump_tree", "rl_prepare_update_connectivity", "rl_find_targets",
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
-    "rl_get_stats",
+    "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times",
 ]
+PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
 _lib = None
 
@@ -160,6 +161,12 @@ def load_library(path: str = LIB_PATH):
     L.rl_synchronize.argtypes = [vp]
     L.rl_get_stats.restype = st
     L.rl_get_stats.argtypes = [vp, P(RlStats)]
+    L.rl_set_stream.restype = st
+    L.rl_set_stream.argtypes = [vp, vp]
+    L.rl_set_profiling.restype = st
+    L.rl_set_profiling.argtypes = [vp, C.c_int]
+    L.rl_get_phase_times.restype = st
+    L.rl_get_phase_times.argtypes = [vp, vp, vp]
     _lib = L
     return L
 
@@ -330,6 +337,18 @@ class Network:
 
     def synchronize(self):
         self._check(self.lib.rl_synchronize(self.h))
+
+    def set_stream(self, cuda_stream: int):
+        """Issue the context's work on an external cudaStream_t (e.g. torch's)."""
+        self._check(self.lib.rl_set_stream(self.h, C.c_void_p(cuda_stream)))
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.rl_set_profiling(self.h, int(on)))
+
+    def phase_times(self) -> dict:
+        ms = np.zeros(len(PHASES)); cnt = np.zeros(len(PHASES), np.uint64)
+        self._check(self.lib.rl_get_phase_times(self.h, _p(ms), _p(cnt)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(PHASES)}
 
     def stats(self) -> dict:
         s = RlStats()

@@ -223,8 +223,11 @@ void run_activity_step(Ctx& c, uint32_t step) {
         A.eta[t] = k.min_calcium[t];
         A.nu[t] = k.growth_rate[t];
     }
-    k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
-    RL_LAUNCH_CHECK();
+    {
+        PhaseScope ps(c, PH_ACTIVITY_KERNEL);
+        k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
+        RL_LAUNCH_CHECK();
+    }
     c.nr.cur ^= 1;
     c.stats.activity_steps += 1;
 }

@@ -506,6 +506,7 @@ void run_search(Ctx& c, uint32_t step) {
                 }
                 const uint64_t warps = (A.end - A.begin + 31) / 32;
                 const unsigned blocks = (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
+                PhaseScope ps(c, PH_SEARCH_KERNEL);
                 k_search<<<blocks, kWarpsPerBlock * 32, 0, st>>>(A);
                 RL_LAUNCH_CHECK();
             }

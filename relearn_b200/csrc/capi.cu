@@ -8,6 +8,48 @@
 
 namespace rl {
 
+PhaseScope::PhaseScope(Ctx& ctx, int ph) : c(&ctx), phase(ph) {
+    if (!c->timer.on) {
+        c = nullptr;
+        return;
+    }
+    auto take = [&]() {
+        cudaEvent_t e;
+        if (!c->timer.free_events.empty()) {
+            e = c->timer.free_events.back();
+            c->timer.free_events.pop_back();
+        } else {
+            RL_CUDA_TRY(cudaEventCreate(&e));
+        }
+        return e;
+    };
+    cudaEvent_t start = take();
+    end = take();
+    RL_CUDA_TRY(cudaEventRecord(start, c->stream));
+    c->timer.pending[phase].emplace_back(start, end);
+}
+
+PhaseScope::~PhaseScope() {
+    if (c) {
+        cudaEventRecord(end, c->stream);
+    }
+}
+
+static void resolve_timers(Ctx& c) {
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    for (int p = 0; p < PH_COUNT; ++p) {
+        for (auto& pr : c.timer.pending[p]) {
+            float ms = 0.f;
+            RL_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            c.timer.ms[p] += ms;
+            c.timer.count[p] += 1;
+            c.timer.free_events.push_back(pr.first);
+            c.timer.free_events.push_back(pr.second);
+        }
+        c.timer.pending[p].clear();
+    }
+}
+
 void check_device_error(Ctx& c, const char* phase) {
     uint32_t h = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&h, c.err.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
@@ -94,7 +136,8 @@ void create(Ctx& c, const rl_config& k) {
     RL_CUDA_TRY(cudaGetDeviceCount(&count));
     RL_CHECK(k.device >= 0 && k.device < count, RL_ERR_DEVICE, "no such CUDA device");
     RL_CUDA_TRY(cudaSetDevice(k.device));
-    RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
+    c.stream = c.own_stream;
     const size_t n = c.n;
     Neurons& N = c.nr;
     N.px.alloc(n);
@@ -149,14 +192,29 @@ void require_tree(Ctx& c) {
 void plasticity_update(Ctx& c, uint32_t step) {
     require_tree(c);
     // SynapseDeletionFinderCPU::delete_synapses: commit the three element types
-    run_commit(c);
+    {
+        PhaseScope ps(c, PH_COMMIT);
+        run_commit(c);
+    }
     // Neurons::create_synapses: search from the committed vacant axons
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
-    update_tree(c);
-    run_search(c, step);
-    run_connector(c, step);
-    rebuild_graph(c);
+    {
+        PhaseScope ps(c, PH_TREE_UPDATE);
+        update_tree(c);
+    }
+    {
+        PhaseScope ps(c, PH_SEARCH);
+        run_search(c, step);
+    }
+    {
+        PhaseScope ps(c, PH_CONNECTOR);
+        run_connector(c, step);
+    }
+    {
+        PhaseScope ps(c, PH_GRAPH);
+        rebuild_graph(c);
+    }
     c.stats.plasticity_updates += 1;
 }
 
@@ -275,7 +333,18 @@ rl_status rl_ctx_destroy(void* ctx) {
     cudaSetDevice(c->device);
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
-        cudaStreamDestroy(c->stream);
+    }
+    for (int p = 0; p < rl::PH_COUNT; ++p) {
+        for (auto& pr : c->timer.pending[p]) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    }
+    for (auto e : c->timer.free_events) {
+        cudaEventDestroy(e);
+    }
+    if (c->own_stream) {
+        cudaStreamDestroy(c->own_stream);
     }
     delete c;
     return RL_OK;
@@ -514,6 +583,29 @@ rl_status rl_synchronize(void* ctx) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
         rl::check_device_error(c, "synchronize");
+    });
+}
+
+rl_status rl_set_stream(void* ctx, void* cuda_stream) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        c.stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c.own_stream;
+    });
+}
+
+rl_status rl_set_profiling(void* ctx, int enable) {
+    return rl::guarded(ctx, [&](Ctx& c) { c.timer.on = enable != 0; });
+}
+
+rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::resolve_timers(c);
+        for (int p = 0; p < rl::PH_COUNT; ++p) {
+            if (ms) ms[p] = c.timer.ms[p];
+            if (counts) counts[p] = c.timer.count[p];
+            c.timer.ms[p] = 0.0;
+            c.timer.count[p] = 0;
+        }
     });
 }
 

@@ -85,11 +85,43 @@ struct Search {
     DBuf<uint32_t> flags;
 };
 
+// Per-phase device time, measured with CUDA events on the context's stream.
+enum Phase : int {
+    PH_ACTIVITY_KERNEL = RL_PHASE_ACTIVITY_KERNEL,
+    PH_COMMIT = RL_PHASE_COMMIT,
+    PH_TREE_UPDATE = RL_PHASE_TREE_UPDATE,
+    PH_SEARCH_KERNEL = RL_PHASE_SEARCH_KERNEL,
+    PH_SEARCH = RL_PHASE_SEARCH,
+    PH_CONNECTOR = RL_PHASE_CONNECTOR,
+    PH_GRAPH = RL_PHASE_GRAPH,
+    PH_COUNT = RL_NUM_PHASES,
+};
+
+struct PhaseTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> free_events;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[PH_COUNT];
+    double ms[PH_COUNT] = {};
+    uint64_t count[PH_COUNT] = {};
+};
+
+struct Ctx;
+// Records an event pair around a scope when profiling is on.
+struct PhaseScope {
+    Ctx* c;
+    int phase;
+    cudaEvent_t end = nullptr;
+    PhaseScope(Ctx& ctx, int ph);
+    ~PhaseScope();
+};
+
 struct Ctx {
     rl_config cfg{};
     uint32_t n = 0;
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream all work is issued on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    PhaseTimer timer;
     std::string last_error;
     bool positions_set = false;
     Tree tree;
