@@ -354,6 +354,28 @@ def run_reference(args, world, rank):
     }
 
 
+def run_case(args):
+    """Small cases for kernel profiles: `activity` runs 4 activity steps of a
+    network of --neurons neurons (no octree needed); `search` runs the search
+    snapshot (one vacant axon and dendrite of each type per neuron) once."""
+    import relearn_b200 as R
+
+    params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
+    net = R.Network(params)
+    if args.case == "activity":
+        net.activity_block(1, 4)
+    else:
+        net.set_positions(pos, sig)
+        one = np.ones(args.neurons, np.uint32)
+        for t in range(3):
+            net.set_elements(t, np.full(args.neurons, 1.5), np.zeros(args.neurons), np.zeros(args.neurons, np.uint32), one)
+        net.prepare_update_connectivity(one, one, one)
+        req = net.find_targets(100)
+        print(json.dumps({"case": "search", "searches": args.neurons, "requests": int(len(req))}))
+    net.synchronize()
+    print(json.dumps({"case": args.case, "neurons": args.neurons, "stats": net.stats()}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -366,8 +388,13 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-bh", action="store_true")
+    ap.add_argument("--case", choices=["activity", "search"], default=None,
+                    help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.case:
+        run_case(args)
+        return
     if args.impl == "reference":
         line = run_reference(args, world, rank)
     else:

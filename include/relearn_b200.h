@@ -112,6 +112,7 @@ typedef struct rl_stats {
     uint64_t requests;           /* requests emitted by the searches */
     uint64_t synapses_created;   /* requests accepted by the connector */
     uint64_t bound_to_delete;    /* bound elements the commits asked to delete */
+    uint64_t synapses_deleted;   /* synapses removed by the deletion passes */
     uint64_t activity_steps;     /* activity steps run */
     uint64_t plasticity_updates; /* plasticity updates run */
     uint64_t gpu_launches;       /* kernels this library launched */

@@ -236,9 +236,10 @@ class OracleSim:
         lib().orc_add_edges(self.h, len(t), _p(t), _p(s), _p(w))
 
     def stats(self) -> dict:
-        out = np.zeros(5, np.uint64)
+        out = np.zeros(6, np.uint64)
         lib().orc_stats(self.h, _p(out))
-        return dict(created=int(out[0]), to_delete=int(out[1]), searches=int(out[2]), nodes_touched=int(out[3]), descents=int(out[4]))
+        return dict(created=int(out[0]), to_delete=int(out[1]), searches=int(out[2]), nodes_touched=int(out[3]), descents=int(out[4]),
+                    deleted=int(out[5]))
 
 
 # ---- element-level helpers for the known-answer tests -------------------

@@ -324,6 +324,7 @@ struct Sim {
     std::vector<uint8_t> last_accepted;
     uint64_t total_created = 0;
     uint64_t total_deleted_requests = 0;
+    uint64_t total_deleted = 0;
     uint64_t searches = 0;
     uint64_t nodes_touched = 0;
     uint64_t descents = 0;
@@ -647,6 +648,105 @@ uint32_t commit_element(Elements& e, uint32_t i, double retract) {
     return (uint32_t)(conn - new_conn);
 }
 
+// RandomHolder::get_random_uniform_indices (util/Random.h:99-115): `count`
+// distinct uniform indices below `total`, redrawing duplicates; the draws come
+// from the injected stream keyed on (step, neuron, pass, k, attempt).
+std::vector<uint32_t> draw_indices(uint64_t seed, uint32_t step, uint32_t neuron, uint32_t pass, uint32_t count, uint32_t total) {
+    std::vector<uint32_t> chosen;
+    chosen.reserve(count);
+    for (uint32_t k = 0; k < count; ++k) {
+        for (uint32_t attempt = 0;; ++attempt) {
+            const oracle::Words r = oracle::stream_draw(seed, step, neuron, (pass << 24) | k, oracle::S_DELETE, attempt);
+            const uint32_t idx = (uint32_t)(((unsigned __int128)oracle::take64(r) * total) >> 64);
+            if (std::find(chosen.begin(), chosen.end(), idx) == chosen.end()) {
+                chosen.push_back(idx);
+                break;
+            }
+        }
+    }
+    return chosen;
+}
+
+void add_weight(Sim& s, uint32_t target, uint32_t source, int32_t w) {
+    auto& edges = s.in_edges[target];
+    auto it = edges.find(source);
+    if (it == edges.end()) {
+        edges.emplace(source, w);
+    } else {
+        it->second += w;
+        if (it->second == 0) {
+            edges.erase(it);
+        }
+    }
+}
+
+// SynapseDeletionFinderCPU::find_synapses_to_delete + commit_deletions
+// (neurons/helper/SynapseDeletionFinderCPU.cpp:93-237) with the random
+// finder (SynapseDeletionFinder.cpp:52-68, register_synapses
+// SynapseDeletionFinderBase.cpp:52-110) for one element type.  The synapse
+// list of a neuron holds each partner |weight| times; here it is ordered by
+// partner id (the reference's order is the insertion order of its edge
+// vectors, which only relabels the uniform choice).
+uint64_t delete_synapses(Sim& s, uint32_t step, int pass, const std::vector<uint32_t>& to_delete) {
+    const uint32_t n = s.n;
+    std::vector<std::vector<std::pair<uint32_t, int32_t>>> out_edges;
+    if (pass == 0) {
+        out_edges.assign(n, {});
+        for (uint32_t t = 0; t < n; ++t) {
+            for (const auto& [src, w] : s.in_edges[t]) {
+                out_edges[src].emplace_back(t, w);
+            }
+        }
+    }
+    std::vector<std::pair<uint32_t, uint32_t>> requests;  // (initiator, partner)
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t d = to_delete[i];
+        if (d == 0 || !s.enabled[i]) {
+            continue;
+        }
+        std::vector<uint32_t> partners;
+        if (pass == 0) {
+            for (const auto& [tg, w] : out_edges[i]) {
+                for (int32_t k = 0; k < std::abs(w); ++k) {
+                    partners.push_back(tg);
+                }
+            }
+        } else {
+            const bool exc = pass == 1;
+            for (const auto& [src, w] : s.in_edges[i]) {
+                if ((exc && w < 0) || (!exc && w > 0)) {
+                    continue;
+                }
+                for (int32_t k = 0; k < std::abs(w); ++k) {
+                    partners.push_back(src);
+                }
+            }
+        }
+        if (d > partners.size()) {
+            s.error = 3;  // the reference throws: more deletions than synapses
+            continue;
+        }
+        for (uint32_t idx : draw_indices(s.cfg.seed, step, i, (uint32_t)pass, d, (uint32_t)partners.size())) {
+            requests.emplace_back(i, partners[idx]);
+        }
+    }
+    for (const auto& [i, p] : requests) {
+        const int signal = pass == 0 ? s.signal[i] : pass - 1;
+        const int32_t weight = signal == 0 ? -1 : 1;
+        if (pass == 0) {
+            add_weight(s, p, i, weight);
+            Elements& den = s.el[1 + signal];  // ElementBaseBase::disconnect_elements (ElementBaseBase.h:311-319)
+            den.connected[p] -= 1;
+            den.vacant[p] += 1;
+        } else {
+            add_weight(s, i, p, weight);
+            s.el[0].connected[p] -= 1;
+            s.el[0].vacant[p] += 1;
+        }
+    }
+    return requests.size();
+}
+
 // One activity step, in the order of Simulation::simulate
 // (sim/Simulation.cpp:443-453): input, Izhikevich, calcium, growth deltas.
 void activity_step(Sim& s, uint32_t step) {
@@ -736,15 +836,19 @@ void activity_step(Sim& s, uint32_t step) {
 // (OctreeAlgorithm.h:100-238), search, connector, edge insertion.
 void plasticity_step(Sim& s, uint32_t step) {
     const uint32_t n = s.n;
+    // SynapseDeletionFinderCPU::delete_synapses (SynapseDeletionFinderCPU.cpp:27-92):
+    // per element type (axon, excitatory, inhibitory dendrite) commit, then delete
+    std::vector<uint32_t> to_delete(n);
     for (int t = 0; t < 3; ++t) {
-        uint64_t to_delete = 0;
+        uint64_t sum = 0;
         for (uint32_t i = 0; i < n; ++i) {
-            if (!s.enabled[i]) {
-                continue;
-            }
-            to_delete += commit_element(s.el[t], i, s.cfg.retract_ratio[t]);
+            to_delete[i] = s.enabled[i] ? commit_element(s.el[t], i, s.cfg.retract_ratio[t]) : 0u;
+            sum += to_delete[i];
         }
-        s.total_deleted_requests += to_delete;
+        s.total_deleted_requests += sum;
+        if (sum) {
+            s.total_deleted += delete_synapses(s, step, t, to_delete);
+        }
     }
     // update_leaf_nodes (OctreeAlgorithm.h:154-238)
     for (uint32_t i = 0; i < n; ++i) {
@@ -1014,6 +1118,7 @@ void orc_stats(void* h, uint64_t* out) {
     out[2] = s->searches;
     out[3] = s->nodes_touched;
     out[4] = s->descents;
+    out[5] = s->total_deleted;
 }
 
 // ---- element-level functions for known-answer tests -------------------

@@ -81,7 +81,7 @@ class RlConfig(C.Structure):
 
 
 class RlStats(C.Structure):
-    _fields_ = [(k, C.c_uint64) for k in ("searches", "requests", "synapses_created", "bound_to_delete", "activity_steps",
+    _fields_ = [(k, C.c_uint64) for k in ("searches", "requests", "synapses_created", "bound_to_delete", "synapses_deleted", "activity_steps",
                                            "plasticity_updates", "gpu_launches", "num_nodes")] + [("max_level", C.c_uint32),
                                                                                                   ("reserved", C.c_uint32)]
 

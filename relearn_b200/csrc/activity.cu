@@ -129,53 +129,57 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A) {
 struct CommitArgs {
     uint32_t n;
     const uint8_t* enabled;
-    double* grown[3];
-    double* delta[3];
-    uint32_t* connected[3];
-    uint32_t* vacant[3];
-    double retract[3];
-    unsigned long long* to_delete;
+    double* grown;
+    double* delta;
+    uint32_t* connected;
+    uint32_t* vacant;
+    double retract;
+    uint32_t* to_delete;
+    unsigned long long* total;
 };
 
+// ElementBaseBase::update for one element type.
 __global__ void k_commit(CommitArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n || !A.enabled[i]) {
+    if (i >= A.n) {
         return;
     }
-    uint32_t del_total = 0;
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const double current_count = A.grown[t][i];
-        const double current_delta = A.delta[t][i];
-        const uint32_t conn_int = A.connected[t][i];
-        const double conn = (double)conn_int;
-        const double current_vacant = current_count - conn;
-        const double new_vacant = current_vacant + current_delta;
-        const double keep = 1.0 - A.retract[t];
-        if (new_vacant >= 0.0) {
-            const double after = keep * new_vacant;
-            A.grown[t][i] = after + conn;
-            A.delta[t][i] = 0.0;
-            A.vacant[t][i] = (uint32_t)after;
-        } else if (current_count + current_delta <= 0.0) {
-            A.grown[t][i] = 0.0;
-            A.delta[t][i] = 0.0;
-            A.vacant[t][i] = 0u;
-            A.connected[t][i] = 0u;
-            del_total += conn_int;
-        } else {
-            const double new_count = current_count + current_delta;
-            const double new_conn = floor(new_count);
-            const double num_vacant = new_count - new_conn;
-            A.grown[t][i] = (keep * num_vacant) + new_conn;
-            A.delta[t][i] = 0.0;
-            A.vacant[t][i] = 0u;
-            A.connected[t][i] = (uint32_t)new_conn;
-            del_total += (uint32_t)(conn - new_conn);
-        }
+    if (!A.enabled[i]) {
+        A.to_delete[i] = 0u;
+        return;
     }
-    if (del_total) {
-        atomicAdd(A.to_delete, (unsigned long long)del_total);
+    const double current_count = A.grown[i];
+    const double current_delta = A.delta[i];
+    const uint32_t conn_int = A.connected[i];
+    const double conn = (double)conn_int;
+    const double current_vacant = current_count - conn;
+    const double new_vacant = current_vacant + current_delta;
+    const double keep = 1.0 - A.retract;
+    uint32_t del = 0;
+    if (new_vacant >= 0.0) {
+        const double after = keep * new_vacant;
+        A.grown[i] = after + conn;
+        A.delta[i] = 0.0;
+        A.vacant[i] = (uint32_t)after;
+    } else if (current_count + current_delta <= 0.0) {
+        A.grown[i] = 0.0;
+        A.delta[i] = 0.0;
+        A.vacant[i] = 0u;
+        A.connected[i] = 0u;
+        del = conn_int;
+    } else {
+        const double new_count = current_count + current_delta;
+        const double new_conn = floor(new_count);
+        const double num_vacant = new_count - new_conn;
+        A.grown[i] = (keep * num_vacant) + new_conn;
+        A.delta[i] = 0.0;
+        A.vacant[i] = 0u;
+        A.connected[i] = (uint32_t)new_conn;
+        del = (uint32_t)(conn - new_conn);
+    }
+    A.to_delete[i] = del;
+    if (del) {
+        atomicAdd(A.total, (unsigned long long)del);
     }
 }
 
@@ -232,20 +236,19 @@ void run_activity_step(Ctx& c, uint32_t step) {
     c.stats.activity_steps += 1;
 }
 
-uint64_t run_commit(Ctx& c) {
+uint64_t run_commit(Ctx& c, int type) {
     CommitArgs A;
     A.n = c.n;
     A.enabled = c.nr.enabled.p;
-    for (int t = 0; t < 3; ++t) {
-        A.grown[t] = c.nr.grown[t].p;
-        A.delta[t] = c.nr.delta[t].p;
-        A.connected[t] = c.nr.connected[t].p;
-        A.vacant[t] = c.nr.vacant[t].p;
-        A.retract[t] = c.cfg.retract_ratio[t];
-    }
+    A.grown = c.nr.grown[type].p;
+    A.delta = c.nr.delta[type].p;
+    A.connected = c.nr.connected[type].p;
+    A.vacant = c.nr.vacant[type].p;
+    A.retract = c.cfg.retract_ratio[type];
+    A.to_delete = c.to_delete.p;
     unsigned long long* d_del = reinterpret_cast<unsigned long long*>(c.counters.p) + 1;
     RL_CUDA_TRY(cudaMemsetAsync(d_del, 0, sizeof(unsigned long long), c.stream));
-    A.to_delete = d_del;
+    A.total = d_del;
     k_commit<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
     RL_LAUNCH_CHECK();
     unsigned long long h = 0;

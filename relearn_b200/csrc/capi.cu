@@ -178,6 +178,7 @@ void create(Ctx& c, const rl_config& k) {
     fill(N.input, n, 0.0, c.stream);
     c.graph.offsets.alloc(n + 1);
     RL_CUDA_TRY(cudaMemsetAsync(c.graph.offsets.p, 0, (n + 1) * sizeof(uint32_t), c.stream));
+    c.to_delete.alloc(n);
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.counters.alloc(4);
@@ -193,8 +194,14 @@ void plasticity_update(Ctx& c, uint32_t step) {
     require_tree(c);
     // SynapseDeletionFinderCPU::delete_synapses: commit the three element types
     {
+        // SynapseDeletionFinderCPU::delete_synapses (neurons/helper/SynapseDeletionFinderCPU.cpp:27-92):
+        // commit axons, delete; commit excitatory dendrites, delete; commit inhibitory dendrites, delete
         PhaseScope ps(c, PH_COMMIT);
-        run_commit(c);
+        for (int t = 0; t < 3; ++t) {
+            if (run_commit(c, t) > 0) {
+                c.stats.synapses_deleted += run_deletion(c, step, t);
+            }
+        }
     }
     // Neurons::create_synapses: search from the committed vacant axons
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));

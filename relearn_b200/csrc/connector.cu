@@ -110,17 +110,7 @@ __global__ void k_emit_edges(uint64_t m, const uint32_t* __restrict__ accepted, 
     ew[o] = sig[i] ? -1 : 1;
 }
 
-// ---- graph rebuild
-__global__ void k_csr_expand(uint32_t n, const uint32_t* __restrict__ off, uint32_t* __restrict__ tgt) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) {
-        return;
-    }
-    for (uint32_t e = off[t]; e < off[t + 1]; ++e) {
-        tgt[e] = t;
-    }
-}
-
+// ---- graph
 __global__ void k_iota(uint64_t m, uint32_t* __restrict__ p) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
@@ -128,20 +118,166 @@ __global__ void k_iota(uint64_t m, uint32_t* __restrict__ p) {
     }
 }
 
-__global__ void k_count_targets(uint64_t m, const uint32_t* __restrict__ tgt, uint32_t* __restrict__ cnt) {
+__global__ void k_pair_keys(uint64_t m, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint64_t* __restrict__ key,
+                            uint32_t* __restrict__ idx) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
-        atomicAdd(&cnt[tgt[i]], 1u);
+        key[i] = ((uint64_t)hi[i] << 32) | lo[i];
+        idx[i] = (uint32_t)i;
     }
 }
 
-__global__ void k_gather_edges(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ s_in, const int32_t* __restrict__ w_in,
-                               uint32_t* __restrict__ s_out, int32_t* __restrict__ w_out) {
+__global__ void k_count_u32(uint64_t m, const uint32_t* __restrict__ v, uint32_t* __restrict__ cnt) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
-        s_out[i] = s_in[perm[i]];
-        w_out[i] = w_in[perm[i]];
+        atomicAdd(&cnt[v[i]], 1u);
     }
+}
+
+__global__ void k_gather_edges(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ t_in, const uint32_t* __restrict__ s_in,
+                               const int32_t* __restrict__ w_in, uint32_t* __restrict__ t_out, uint32_t* __restrict__ s_out, int32_t* __restrict__ w_out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        const uint32_t k = perm[i];
+        t_out[i] = t_in[k];
+        s_out[i] = s_in[k];
+        w_out[i] = w_in[k];
+    }
+}
+
+__global__ void k_keep_flags(uint64_t m, const int32_t* __restrict__ w, uint32_t* __restrict__ keep) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        keep[i] = w[i] != 0 ? 1u : 0u;
+    }
+}
+
+__global__ void k_compact_edges(uint64_t m, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ pos, const uint32_t* __restrict__ t_in,
+                                const uint32_t* __restrict__ s_in, const int32_t* __restrict__ w_in, uint32_t* __restrict__ t_out,
+                                uint32_t* __restrict__ s_out, int32_t* __restrict__ w_out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m && keep[i]) {
+        const uint32_t o = pos[i];
+        t_out[o] = t_in[i];
+        s_out[o] = s_in[i];
+        w_out[o] = w_in[i];
+    }
+}
+
+struct DeleteArgs {
+    uint32_t n;
+    int type;  // 0 axon, 1 excitatory dendrite, 2 inhibitory dendrite
+    uint32_t step;
+    uint64_t seed;
+    const uint32_t* to_delete;
+    const uint8_t* signal;
+    const uint8_t* enabled;
+    const uint32_t* in_off;
+    const uint32_t* out_off;
+    const uint32_t* out_perm;
+    const uint32_t* etgt;
+    const uint32_t* esrc;
+    int32_t* ew;
+    uint32_t* connected[3];
+    uint32_t* vacant[3];
+    unsigned long long* deleted;
+    uint32_t* err;
+};
+
+constexpr uint32_t kMaxDeletePerNeuron = 64;
+
+// Random synapse deletion for one element type (SynapseDeletionFinderCPU
+// find_synapses_to_delete + commit_deletions, neurons/helper/
+// SynapseDeletionFinderCPU.cpp:93-237; RandomSynapseDeletionFinder
+// SynapseDeletionFinder.cpp:52-68).  A neuron's synapse list holds every
+// partner |weight| times, ordered by partner id; d distinct indices are drawn
+// (redrawing duplicates, util/Random.h:99-115).  Every synapse belongs to the
+// list of exactly one neuron in a pass, so the weight updates need no atomics;
+// the partners' elements are disconnected with atomics (integer, order free).
+__global__ void k_delete(DeleteArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    const uint32_t d = A.to_delete[i];
+    if (d == 0 || !A.enabled[i]) {
+        return;
+    }
+    const bool axon = A.type == 0;
+    const int signal = axon ? (int)A.signal[i] : A.type - 1;
+    const uint32_t r0 = axon ? A.out_off[i] : A.in_off[i];
+    const uint32_t r1 = axon ? A.out_off[i + 1] : A.in_off[i + 1];
+    auto edge_at = [&](uint32_t r) { return axon ? A.out_perm[r] : r; };
+    auto matches = [&](int32_t w) { return axon || (signal == 0 ? w > 0 : w < 0); };
+    uint32_t total = 0;
+    for (uint32_t r = r0; r < r1; ++r) {
+        const int32_t w = A.ew[edge_at(r)];
+        if (matches(w)) {
+            total += (uint32_t)(w < 0 ? -w : w);
+        }
+    }
+    if (d > total || d > kMaxDeletePerNeuron) {
+        atomicOr(A.err, (uint32_t)DERR_CONNECT);
+        return;
+    }
+    uint32_t chosen[kMaxDeletePerNeuron];
+    for (uint32_t k = 0; k < d; ++k) {
+        uint32_t idx = 0;
+        bool ok = false;
+        for (uint32_t attempt = 0; attempt < (1u << 20) && !ok; ++attempt) {
+            const u32x4 w = draw(A.seed, A.step, i, ((uint32_t)A.type << 24) | k, STREAM_DELETION, attempt);
+            idx = (uint32_t)__umul64hi(bits64(w), (uint64_t)total);
+            ok = true;
+            for (uint32_t q = 0; q < k; ++q) {
+                if (chosen[q] == idx) {
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        if (!ok) {
+            atomicOr(A.err, (uint32_t)DERR_TIMEOUT);
+            return;
+        }
+        chosen[k] = idx;
+    }
+    // sort the chosen list indices, then walk the row once over the original
+    // multiplicities: entry e covers list indices [acc, acc + |w_e|)
+    for (uint32_t a = 1; a < d; ++a) {
+        const uint32_t v = chosen[a];
+        uint32_t b = a;
+        while (b > 0 && chosen[b - 1] > v) {
+            chosen[b] = chosen[b - 1];
+            --b;
+        }
+        chosen[b] = v;
+    }
+    uint32_t acc = 0;
+    uint32_t q = 0;
+    for (uint32_t r = r0; r < r1 && q < d; ++r) {
+        const uint32_t e = edge_at(r);
+        const int32_t w = A.ew[e];
+        if (!matches(w)) {
+            continue;
+        }
+        const uint32_t mult = (uint32_t)(w < 0 ? -w : w);
+        uint32_t hits = 0;
+        while (q < d && chosen[q] < acc + mult) {
+            ++hits;
+            ++q;
+        }
+        acc += mult;
+        if (hits == 0) {
+            continue;
+        }
+        A.ew[e] = w < 0 ? w + (int32_t)hits : w - (int32_t)hits;
+        const uint32_t partner = axon ? A.etgt[e] : A.esrc[e];
+        // ElementBaseBase::disconnect_elements (ElementBaseBase.h:311-319) on the partner
+        const int pt = axon ? 1 + signal : 0;
+        atomicSub(&A.connected[pt][partner], hits);
+        atomicAdd(&A.vacant[pt][partner], hits);
+    }
+    atomicAdd(A.deleted, (unsigned long long)d);
 }
 
 }  // namespace
@@ -236,6 +372,49 @@ uint64_t run_connector(Ctx& c, uint32_t step) {
     return created;
 }
 
+namespace {
+
+int bits_for(uint64_t v) {
+    int b = 1;
+    while (b < 32 && ((uint64_t)1 << b) <= v) {
+        ++b;
+    }
+    return b;
+}
+
+// In-CSR offsets and the out-CSR of the sorted edge list.
+void finish_graph(Ctx& c, uint64_t m) {
+    Graph& G = c.graph;
+    cudaStream_t st = c.stream;
+    const uint32_t n = c.n;
+    G.num_edges = m;
+    G.offsets.ensure((size_t)n + 1);
+    G.out_off.ensure((size_t)n + 1);
+    DBuf<uint32_t> cnt;
+    cnt.alloc((size_t)n + 1);
+    RL_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, ((size_t)n + 1) * sizeof(uint32_t), st));
+    if (m) {
+        k_count_u32<<<blocks_for(m, 256), 256, 0, st>>>(m, G.tgt.p, cnt.p);
+        RL_LAUNCH_CHECK();
+    }
+    exclusive_scan_u32(cnt.p, G.offsets.p, (uint64_t)n + 1, c.prim, st);
+    RL_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, ((size_t)n + 1) * sizeof(uint32_t), st));
+    G.out_perm.ensure(m ? m : 1);
+    if (m) {
+        k_count_u32<<<blocks_for(m, 256), 256, 0, st>>>(m, G.src.p, cnt.p);
+        RL_LAUNCH_CHECK();
+        DBuf<uint64_t> key;
+        key.alloc(m);
+        k_pair_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, G.src.p, G.tgt.p, key.p, G.out_perm.p);
+        RL_LAUNCH_CHECK();
+        radix_sort_u64(key.p, G.out_perm.p, m, 32 + bits_for(n), c.prim, st);
+    }
+    exclusive_scan_u32(cnt.p, G.out_off.p, (uint64_t)n + 1, c.prim, st);
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+
 void rebuild_graph(Ctx& c) {
     Graph& G = c.graph;
     if (G.num_new == 0) {
@@ -246,41 +425,96 @@ void rebuild_graph(Ctx& c) {
     const uint64_t old = G.num_edges;
     const uint64_t m = old + G.num_new;
     RL_CHECK(m < 0xFFFFFFFFull, RL_ERR_OVERFLOW, "synapse count exceeds 2^32");
-    DBuf<uint32_t> tgt, perm, srcs, cnt;
+    DBuf<uint32_t> tgt, srcs, perm;
     DBuf<int32_t> ws;
+    DBuf<uint64_t> key;
     tgt.alloc(m);
-    perm.alloc(m);
     srcs.alloc(m);
     ws.alloc(m);
-    cnt.alloc((size_t)n + 1);
+    perm.alloc(m);
+    key.alloc(m);
     if (old) {
-        k_csr_expand<<<blocks_for(n, 256), 256, 0, st>>>(n, G.offsets.p, tgt.p);
-        RL_LAUNCH_CHECK();
+        RL_CUDA_TRY(cudaMemcpyAsync(tgt.p, G.tgt.p, old * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
         RL_CUDA_TRY(cudaMemcpyAsync(srcs.p, G.src.p, old * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
         RL_CUDA_TRY(cudaMemcpyAsync(ws.p, G.weight.p, old * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     }
     RL_CUDA_TRY(cudaMemcpyAsync(tgt.p + old, G.new_tgt.p, G.num_new * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     RL_CUDA_TRY(cudaMemcpyAsync(srcs.p + old, G.new_src.p, G.num_new * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     RL_CUDA_TRY(cudaMemcpyAsync(ws.p + old, G.new_w.p, G.num_new * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-    RL_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, ((size_t)n + 1) * sizeof(uint32_t), st));
-    k_count_targets<<<blocks_for(m, 256), 256, 0, st>>>(m, tgt.p, cnt.p);
+    // canonical order: (target, source), equal pairs in insertion order
+    k_pair_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, tgt.p, srcs.p, key.p, perm.p);
     RL_LAUNCH_CHECK();
-    G.offsets.ensure((size_t)n + 1);
-    exclusive_scan_u32(cnt.p, G.offsets.p, (uint64_t)n + 1, c.prim, st);
-    k_iota<<<blocks_for(m, 256), 256, 0, st>>>(m, perm.p);
-    RL_LAUNCH_CHECK();
-    int bits = 1;
-    while (bits < 32 && ((uint64_t)1 << bits) <= n) {
-        ++bits;
-    }
-    radix_sort_u32(tgt.p, perm.p, m, bits, c.prim, st);
+    radix_sort_u64(key.p, perm.p, m, 32 + bits_for(n), c.prim, st);
+    G.tgt.ensure(m);
     G.src.ensure(m);
     G.weight.ensure(m);
-    k_gather_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, perm.p, srcs.p, ws.p, G.src.p, G.weight.p);
+    k_gather_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, perm.p, tgt.p, srcs.p, ws.p, G.tgt.p, G.src.p, G.weight.p);
     RL_LAUNCH_CHECK();
-    RL_CUDA_TRY(cudaStreamSynchronize(st));
-    G.num_edges = m;
     G.num_new = 0;
+    finish_graph(c, m);
+}
+
+uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
+    Graph& G = c.graph;
+    cudaStream_t st = c.stream;
+    rebuild_graph(c);
+    if (G.num_edges == 0) {
+        // nothing to delete: the elements say otherwise only if the state was set inconsistently
+        RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), st));
+    }
+    unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(c.counters.p) + 2;
+    RL_CUDA_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st));
+    DeleteArgs A;
+    A.n = c.n;
+    A.type = type;
+    A.step = step;
+    A.seed = c.cfg.seed;
+    A.to_delete = c.to_delete.p;
+    A.signal = c.nr.signal.p;
+    A.enabled = c.nr.enabled.p;
+    A.in_off = G.offsets.p;
+    A.out_off = G.out_off.p;
+    A.out_perm = G.out_perm.p;
+    A.etgt = G.tgt.p;
+    A.esrc = G.src.p;
+    A.ew = G.weight.p;
+    for (int t = 0; t < 3; ++t) {
+        A.connected[t] = c.nr.connected[t].p;
+        A.vacant[t] = c.nr.vacant[t].p;
+    }
+    A.deleted = d_cnt;
+    A.err = c.err.p;
+    k_delete<<<blocks_for(c.n, 128), 128, 0, st>>>(A);
+    RL_LAUNCH_CHECK();
+    check_device_error(c, "synapse deletion");
+    unsigned long long deleted = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&deleted, d_cnt, sizeof(deleted), cudaMemcpyDeviceToHost, st));
+    // drop entries whose weight reached zero
+    const uint64_t m = G.num_edges;
+    if (m) {
+        DBuf<uint32_t> keep, pos, t2, s2;
+        DBuf<int32_t> w2;
+        keep.alloc(m);
+        pos.alloc(m);
+        k_keep_flags<<<blocks_for(m, 256), 256, 0, st>>>(m, G.weight.p, keep.p);
+        RL_LAUNCH_CHECK();
+        const uint64_t kept = exclusive_scan_u32(keep.p, pos.p, m, c.prim, st);
+        t2.alloc(kept ? kept : 1);
+        s2.alloc(kept ? kept : 1);
+        w2.alloc(kept ? kept : 1);
+        k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, pos.p, G.tgt.p, G.src.p, G.weight.p, t2.p, s2.p, w2.p);
+        RL_LAUNCH_CHECK();
+        RL_CUDA_TRY(cudaStreamSynchronize(st));
+        std::swap(G.tgt.p, t2.p);
+        std::swap(G.tgt.n, t2.n);
+        std::swap(G.src.p, s2.p);
+        std::swap(G.src.n, s2.n);
+        std::swap(G.weight.p, w2.p);
+        std::swap(G.weight.n, w2.n);
+        finish_graph(c, kept);
+    }
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    return deleted;
 }
 
 void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w) {

@@ -53,13 +53,18 @@ struct Neurons {
     DBuf<uint32_t> search_vacant;  // vacant axons handed to the next search
 };
 
-// Synapse list kept as CSR over targets (one entry per synapse, weight +-1 or
-// an aggregated integer weight) plus an append buffer for the current update.
+// Synapse list: one entry per (target, source) synapse group with an integer
+// weight (+1 per excitatory, -1 per inhibitory synapse), sorted by
+// (target, source); in-CSR over targets and out-CSR (a permutation sorted by
+// (source, target)) over sources.  New synapses of a plasticity update are
+// appended to the new_* buffers and merged by rebuild_graph.
 struct Graph {
     uint64_t num_edges = 0;
-    DBuf<uint32_t> offsets;  // n + 1
-    DBuf<uint32_t> src;
+    DBuf<uint32_t> offsets;  // in-CSR, n + 1
+    DBuf<uint32_t> tgt, src;
     DBuf<int32_t> weight;
+    DBuf<uint32_t> out_off;   // out-CSR, n + 1
+    DBuf<uint32_t> out_perm;  // edge indices in (source, target) order
     DBuf<uint32_t> new_tgt, new_src;
     DBuf<int32_t> new_w;
     uint64_t num_new = 0;
@@ -129,6 +134,7 @@ struct Ctx {
     Graph graph;
     Search search;
     PrimScratch prim;
+    DBuf<uint32_t> to_delete;  // per neuron, bound elements to delete in the current pass
     DBuf<uint32_t> err;       // device error word
     DBuf<uint64_t> counters;  // device counters
     rl_stats stats{};
@@ -146,11 +152,12 @@ void run_search(Ctx& c, uint32_t step);  // fills search.req_* (requests in (sou
 // connector.cu
 uint64_t run_connector(Ctx& c, uint32_t step);  // accepts requests, updates elements, appends new edges
 void rebuild_graph(Ctx& c);                     // merge new edges into the CSR
+uint64_t run_deletion(Ctx& c, uint32_t step, int type);  // delete to_delete[] synapses per neuron for one element type
 void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w);
 
 // activity.cu
 void run_activity_step(Ctx& c, uint32_t step);
-uint64_t run_commit(Ctx& c);  // returns bound elements to delete
+uint64_t run_commit(Ctx& c, int type);  // commit one element type; to_delete[] per neuron, returns the sum
 
 void check_device_error(Ctx& c, const char* phase);
 

@@ -134,7 +134,9 @@ def test_seeded_vacancy_simulation():
     sim.simulate(1, 1001)
     compare_state(net, sim, n)
     st = net.stats()
-    assert st["synapses_created"] == sim.stats()["created"] > 0
+    so = sim.stats()
+    assert st["synapses_created"] == so["created"] > 0
+    assert st["synapses_deleted"] == so["deleted"]
 
 
 def test_config0_organic_20001_steps():
