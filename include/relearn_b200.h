@@ -225,6 +225,23 @@ RL_API rl_status rl_get_stats(void* ctx, rl_stats* out);
  * context's device), or on the context's own stream when NULL. */
 RL_API rl_status rl_set_stream(void* ctx, void* cuda_stream);
 
+/* Allocation-free form of the tree part of rl_prepare_update_connectivity
+ * (leaf counts + bottom-up reduction).  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory when they update the
+ * octree (a runtime that hands out all device memory from its own pool or
+ * budget, or a host that must not touch the allocator once set-up is done).
+ * Inputs are DEVICE arrays of n entries (vacant excitatory and inhibitory
+ * dendrites, optional plasticity flags); the result goes to the context's
+ * octree.  The call allocates nothing: its scratch (one counter per octree
+ * node) is a file-scope device array of 2,097,152 counters (8 MiB) that every
+ * GPU loading the library holds until exit; larger trees are rejected with
+ * RL_ERR_OVERFLOW.  All calls share that array, so calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's device address
+ * and should come before any stream capture.  Work is enqueued on cuda_stream
+ * (NULL: the context's stream); the caller synchronizes before reading. */
+RL_API rl_status rl_prepare_update_connectivity_noalloc(void* ctx, const uint32_t* d_vacant_exc, const uint32_t* d_vacant_inh,
+                                                        const uint8_t* d_update, void* cuda_stream);
+
 /* Turn per-phase CUDA-event timing on (1) or off (0). */
 RL_API rl_status rl_set_profiling(void* ctx, int enable);
 

@@ -95,7 +95,7 @@ ABI_FUNCTIONS = [
     "rl_set_positions", "rl_tree_info", "rl_dump_tree", "rl_prepare_update_connectivity", "rl_find_targets",
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
-    "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times",
+    "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -167,6 +167,8 @@ def load_library(path: str = LIB_PATH):
     L.rl_set_profiling.argtypes = [vp, C.c_int]
     L.rl_get_phase_times.restype = st
     L.rl_get_phase_times.argtypes = [vp, vp, vp]
+    L.rl_prepare_update_connectivity_noalloc.restype = st
+    L.rl_prepare_update_connectivity_noalloc.argtypes = [vp, vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -341,6 +343,12 @@ class Network:
     def set_stream(self, cuda_stream: int):
         """Issue the context's work on an external cudaStream_t (e.g. torch's)."""
         self._check(self.lib.rl_set_stream(self.h, C.c_void_p(cuda_stream)))
+
+    def prepare_update_connectivity_noalloc(self, d_vacant_exc: int, d_vacant_inh: int, d_update: int = 0, cuda_stream: int = 0):
+        """Tree update from DEVICE arrays (addresses), allocating nothing; see
+        rl_prepare_update_connectivity_noalloc in include/relearn_b200.h."""
+        self._check(self.lib.rl_prepare_update_connectivity_noalloc(self.h, C.c_void_p(d_vacant_exc), C.c_void_p(d_vacant_inh),
+                                                                    C.c_void_p(d_update or None), C.c_void_p(cuda_stream or None)))
 
     def set_profiling(self, on: bool = True):
         self._check(self.lib.rl_set_profiling(self.h, int(on)))

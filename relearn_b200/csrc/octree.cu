@@ -572,6 +572,35 @@ void update_tree(Ctx& c) {
     RL_LAUNCH_CHECK();
 }
 
+void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_t* d_vac_inh, const uint8_t* d_update, uint32_t* arrive,
+                                cudaStream_t st) {
+    const uint32_t n = c.n;
+    Tree& T = c.tree;
+    k_leaf_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, T.leaf_of.p, c.nr.enabled.p, d_update ? d_update : c.nr.enabled.p, d_vac_exc, d_vac_inh,
+                                                      T.rec[0].p, T.rec[1].p);
+    RL_LAUNCH_CHECK();
+    if (T.root_is_leaf) {
+        return;
+    }
+    RL_CUDA_TRY(cudaMemsetAsync(arrive, 0, T.num_nodes * sizeof(uint32_t), st));
+    ReduceArgs A;
+    A.n = n;
+    A.leaf_of = T.leaf_of.p;
+    A.parent = T.parent.p;
+    A.topo = T.topo.p;
+    A.bx0 = T.bmin[0].p;
+    A.by0 = T.bmin[1].p;
+    A.bz0 = T.bmin[2].p;
+    A.bx1 = T.bmax[0].p;
+    A.by1 = T.bmax[1].p;
+    A.bz1 = T.bmax[2].p;
+    A.rec0 = T.rec[0].p;
+    A.rec1 = T.rec[1].p;
+    A.arrive = arrive;
+    k_reduce<<<blocks_for(n, 128), 128, 0, st>>>(A);
+    RL_LAUNCH_CHECK();
+}
+
 void dump_tree(Ctx& c, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax, uint32_t* cnt_exc,
                uint32_t* cnt_inh, double* pos_exc, double* pos_inh) {
     const uint32_t m = c.tree.num_nodes;

@@ -143,6 +143,10 @@ struct Ctx {
 // octree.cu
 void build_octree(Ctx& c, const double* h_xyz);
 void update_tree(Ctx& c);  // leaf counts from nr.vacant[1..2] and nr.update, then the reduction
+// Leaf update + reduction with caller-given device vacancy arrays and an
+// external arrival-counter buffer of at least tree.num_nodes words.
+void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_t* d_vac_inh, const uint8_t* d_update, uint32_t* arrive,
+                                cudaStream_t st);
 void dump_tree(Ctx& c, int32_t* level, int32_t* neuron, uint8_t* child_mask, int32_t* first_child, double* bmin, double* bmax, uint32_t* cnt_exc,
                uint32_t* cnt_inh, double* pos_exc, double* pos_inh);
 
