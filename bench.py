@@ -119,28 +119,23 @@ def build_network(n, side, seed, placement):
     return params, pos, sig
 
 
-def run_b200(args, world, rank, local):
+ACT_BYTES_FP32 = 62  # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes input 4 + x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12
+
+
+def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None):
+    """Warm up and time args.steps plasticity periods of one network in the
+    given precision form; returns the figures of that form."""
     import torch
 
     import relearn_b200 as R
 
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    n, side = args.neurons, args.side
-    params, pos, sig = build_network(n, side, args.seed + rank, args.placement)
-    params["device"] = local
-    net = R.Network(params)
-    stream = torch.cuda.current_stream(dev)
+    n = args.neurons
+    p = dict(params)
+    p["precision"] = precision
+    net = R.Network(p)
     net.set_stream(stream.cuda_stream)
     net.set_positions(pos, sig)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
-
     step = 1
     for _ in range(args.warmup):
         net.simulate(step, PERIOD)
@@ -152,7 +147,8 @@ def run_b200(args, world, rank, local):
     net.phase_times()
     net.set_profiling(True)
     times = []
-    with ClockSampler(local) as clk:
+    ctx = clk if clk is not None else _Null()
+    with ctx:
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -173,13 +169,45 @@ def run_b200(args, world, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * n * PERIOD * args.steps / (total_ms / 1e3)
-
-    # roofline of the dominant kernel (the fused activity kernel)
     act_ms, act_cnt = phases["activity_kernel"]
     edges = int(net.stats().get("synapses_created", 0))
-    bytes_per_launch = ACT_BYTES_PER_NEURON * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)
+    per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
+    bytes_per_launch = per_neuron * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+    roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch,
+            "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
+    return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof)
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    n, side = args.neurons, args.side
+    params, pos, sig = build_network(n, side, args.seed + rank, args.placement)
+    params["device"] = local
+    stream = torch.cuda.current_stream(dev)
+    main_prec = 1 if args.precision == "fp32" else 0
+    clk = ClockSampler(local)
+    m = measure_form(args, main_prec, dev, stream, world, pos, sig, params, clk)
+    net, step = m["net"], m["step"]
 
     # e2e through the public C ABI with host buffers: every bench step uploads
     # the enable flags (a per-step host input of Simulation::simulate's
@@ -199,8 +227,19 @@ def run_b200(args, world, rank, local):
     e2e_s = time.perf_counter() - t0
     e2e_val = world * n * PERIOD * e2e_steps / e2e_s
 
-    # Barnes-Hut searches on the reference benchmark's snapshot
     bh = bh_snapshot(net, n, stream, step) if not args.skip_bh else None
+    net.close()
+    other = None
+    if not args.skip_fp32 and main_prec == 0:
+        o = measure_form(args, 1, dev, stream, world, pos, sig, params)
+        bh32 = bh_snapshot(o["net"], n, stream, o["step"]) if not args.skip_bh else None
+        other = {"precision": "fp32", "value": o["value"], "unit": "neuron-steps/s", "ms_per_step": o["total_ms"] / args.steps,
+                 "vs_fp64_drop_in": o["value"] / m["value"], "roofline": o["roofline"], "phases_ms": o["phases"]}
+        if bh32:
+            other["bh_search"] = bh32
+            if bh:
+                other["bh_search"]["vs_fp64_drop_in"] = bh32["value"] / bh["value"]
+        o["net"].close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -213,31 +252,32 @@ def run_b200(args, world, rank, local):
         return None
     line = {
         "metric": "neuron-steps/s",
-        "value": value,
+        "value": m["value"],
         "unit": "neuron-steps/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps,
+        "ms_per_step": m["total_ms"] / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if main_prec == 0 else "f32",
         "data": "synthetic (seeded positions, reference parameters)",
-        "config": {"workload": f"{n} Izhikevich neurons {args.placement} in a {side:g} um cube, FP64 drop-in; one bench step = "
-                               f"{PERIOD} activity steps + 1 plasticity update", "neurons": n, "placement": args.placement,
-                   "period": PERIOD, "l2": "256 MB buffer written between timed steps", "parallelism": f"replicas{world}"},
-        "roofline": {"bound": "hbm", "kernel": "k_activity", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind,
-                     "bytes_per_launch": bytes_per_launch, "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None},
-        "phases_ms": {k: v[0] for k, v in phases.items()},
+        "config": {"workload": f"{n} Izhikevich neurons {args.placement} in a {side:g} um cube, "
+                               f"{'FP64 drop-in' if main_prec == 0 else 'FP32 form'}; one bench step = {PERIOD} activity steps + 1 plasticity update",
+                   "neurons": n, "placement": args.placement, "period": PERIOD, "l2": "256 MB buffer written between timed steps",
+                   "parallelism": f"replicas{world}"},
+        "roofline": m["roofline"],
+        "phases_ms": m["phases"],
         "e2e": {"value": e2e_val, "unit": "neuron-steps/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 9 * n,
                 "api": "rl_set_enabled + rl_simulate + rl_get_neurons (pinned host buffers)"},
-        "gpu_launches": launches,
+        "gpu_launches": m["launches"],
         "clocks": clocks,
     }
     if bh:
         line["bh_search"] = bh
+    if other:
+        line["fp32_form"] = other
     if cpu:
         line["cpu_baseline"] = cpu
     return line
@@ -388,6 +428,8 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-bh", action="store_true")
+    ap.add_argument("--skip-fp32", action="store_true", help="do not measure the FP32 form beside the FP64 drop-in")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="form of the headline figure")
     ap.add_argument("--case", choices=["activity", "search"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()

@@ -86,8 +86,14 @@ typedef struct rl_config {
     double noise_mean;            /* normal background input mean */
     double noise_stddev;          /* normal background input stddev */
     int32_t device;               /* CUDA device ordinal */
-    int32_t reserved;
+    int32_t precision;            /* RL_PRECISION_FP64 (drop-in, bit-exact) or RL_PRECISION_FP32 */
 } rl_config;
+
+/* Precision forms.  FP64: the drop-in; every FP64 operation in the reference's
+ * order, bit-exact against the oracle.  FP32: membrane, input, growth and
+ * attraction arithmetic in FP32 with Kahan-compensated attraction sums; calcium
+ * integrated in FP64; octree centroids reduced in FP64 and read as FP32. */
+enum { RL_PRECISION_FP64 = 0, RL_PRECISION_FP32 = 1 };
 
 /* One synapse creation request (SynapseCreationRequest,
  * neurons/helper/SynapseCreationRequests.h) plus the vacant-axon index j. */
@@ -241,6 +247,14 @@ RL_API rl_status rl_set_stream(void* ctx, void* cuda_stream);
  * (NULL: the context's stream); the caller synchronizes before reading. */
 RL_API rl_status rl_prepare_update_connectivity_noalloc(void* ctx, const uint32_t* d_vacant_exc, const uint32_t* d_vacant_inh,
                                                         const uint8_t* d_update, void* cuda_stream);
+
+/* Diagnostic: the candidates of the first descent (from the root) of a search
+ * by `source`, in visiting order, with their unnormalised attraction weights
+ * evaluated in `precision` (RL_PRECISION_FP64 or RL_PRECISION_FP32) on the
+ * current octree (after rl_prepare_update_connectivity).  *count receives the
+ * number of candidates; at most `capacity` are copied. */
+RL_API rl_status rl_candidate_weights(void* ctx, uint32_t source, int precision, uint32_t* nodes, double* weights, uint64_t capacity,
+                                      uint64_t* count);
 
 /* Turn per-phase CUDA-event timing on (1) or off (0). */
 RL_API rl_status rl_set_profiling(void* ctx, int enable);

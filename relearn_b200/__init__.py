@@ -76,8 +76,11 @@ class RlConfig(C.Structure):
         ("noise_mean", C.c_double),
         ("noise_stddev", C.c_double),
         ("device", C.c_int32),
-        ("reserved", C.c_int32),
+        ("precision", C.c_int32),
     ]
+
+
+PRECISION_FP64, PRECISION_FP32 = 0, 1
 
 
 class RlStats(C.Structure):
@@ -96,6 +99,7 @@ ABI_FUNCTIONS = [
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
+    "rl_candidate_weights",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -167,6 +171,8 @@ def load_library(path: str = LIB_PATH):
     L.rl_set_profiling.argtypes = [vp, C.c_int]
     L.rl_get_phase_times.restype = st
     L.rl_get_phase_times.argtypes = [vp, vp, vp]
+    L.rl_candidate_weights.restype = st
+    L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
     L.rl_prepare_update_connectivity_noalloc.argtypes = [vp, vp, vp, vp, vp]
     _lib = L
@@ -189,7 +195,7 @@ def default_params(num_neurons: int, side: float) -> dict:
                 iz_a=0.02, iz_b=0.2, iz_c=-65.0, iz_d=8.0, iz_v_spike=30.0, iz_k1=0.04, iz_k2=5.0, iz_k3=140.0,
                 beta=0.001, tau_c=10000.0, target_calcium=0.7, initial_calcium=0.0,
                 growth_rate=(1e-4, 1e-4, 1e-4), min_calcium=(0.4, 0.1, 0.0), retract_ratio=(0.0, 0.0, 0.0),
-                conductance=3.0, noise_mean=5.0, noise_stddev=2.0, device=0)
+                conductance=3.0, noise_mean=5.0, noise_stddev=2.0, device=0, precision=PRECISION_FP64)
 
 
 def make_config(params: dict) -> RlConfig:
@@ -264,6 +270,7 @@ class Network:
     # ---- algorithm surface
     def prepare_update_connectivity(self, vacant_axons, vacant_exc, vacant_inh, signal=None, update=None):
         va = np.ascontiguousarray(vacant_axons, np.uint32)
+        self._search_capacity = int(va.astype(np.uint64).sum())
         ve = np.ascontiguousarray(vacant_exc, np.uint32)
         vi = np.ascontiguousarray(vacant_inh, np.uint32)
         sg = None if signal is None else np.ascontiguousarray(signal, np.uint8)
@@ -271,10 +278,15 @@ class Network:
         self._check(self.lib.rl_prepare_update_connectivity(self.h, _p(sg), _p(va), _p(ve), _p(vi), _p(up)))
 
     def find_targets(self, step: int) -> np.ndarray:
+        cap = getattr(self, "_search_capacity", None)
+        if cap is None:
+            cap = int(self.get_elements(AXON)["vacant"].astype(np.uint64).sum())
+        out = np.zeros(max(int(cap), 1), REQUEST_DTYPE)
         cnt = C.c_uint64()
-        self._check(self.lib.rl_find_targets(self.h, step, None, 0, C.byref(cnt)))
-        out = np.zeros(max(int(cnt.value), 1), REQUEST_DTYPE)
         self._check(self.lib.rl_find_targets(self.h, step, _p(out), len(out), C.byref(cnt)))
+        if int(cnt.value) > len(out):  # the vacancy changed since the last prepare: run again with room
+            out = np.zeros(int(cnt.value), REQUEST_DTYPE)
+            self._check(self.lib.rl_find_targets(self.h, step, _p(out), len(out), C.byref(cnt)))
         return out[: int(cnt.value)]
 
     def update_connectivity(self, step: int, capacity: Optional[int] = None) -> np.ndarray:
@@ -349,6 +361,15 @@ class Network:
         rl_prepare_update_connectivity_noalloc in include/relearn_b200.h."""
         self._check(self.lib.rl_prepare_update_connectivity_noalloc(self.h, C.c_void_p(d_vacant_exc), C.c_void_p(d_vacant_inh),
                                                                     C.c_void_p(d_update or None), C.c_void_p(cuda_stream or None)))
+
+    def candidate_weights(self, source: int, precision: int = PRECISION_FP64):
+        """Descent-0 candidates (visiting order) and raw weights of a search by `source`."""
+        cnt = C.c_uint64()
+        self._check(self.lib.rl_candidate_weights(self.h, source, precision, None, None, 0, C.byref(cnt)))
+        m = int(cnt.value)
+        nodes = np.zeros(max(m, 1), np.uint32); w = np.zeros(max(m, 1))
+        self._check(self.lib.rl_candidate_weights(self.h, source, precision, _p(nodes), _p(w), m, C.byref(cnt)))
+        return nodes[:m], w[:m]
 
     def set_profiling(self, on: bool = True):
         self._check(self.lib.rl_set_profiling(self.h, int(on)))

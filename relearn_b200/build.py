@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librelearn_b200.so")
-SOURCES = ["prims.cu", "octree.cu", "bh_search.cu", "connector.cu", "activity.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["prims.cu", "octree.cu", "bh_search.cu", "connector.cu", "activity.cu", "capi.cu", "noalloc.cu", "fp32.cu"]
 HEADERS = ["rl_internal.cuh", "rl_context.cuh", "rl_math.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include", "relearn_b200.h")
 

@@ -186,6 +186,10 @@ __global__ void k_commit(CommitArgs A) {
 }  // namespace
 
 void run_activity_step(Ctx& c, uint32_t step) {
+    if (is_fp32(c)) {
+        run_activity_step_f32(c, step);
+        return;
+    }
     const rl_config& k = c.cfg;
     ActArgs A;
     A.n = c.n;
@@ -237,6 +241,9 @@ void run_activity_step(Ctx& c, uint32_t step) {
 }
 
 uint64_t run_commit(Ctx& c, int type) {
+    if (is_fp32(c)) {
+        return run_commit_f32(c, type);
+    }
     CommitArgs A;
     A.n = c.n;
     A.enabled = c.nr.enabled.p;

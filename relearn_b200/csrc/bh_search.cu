@@ -497,11 +497,18 @@ void run_search(Ctx& c, uint32_t step) {
             A.step = step;
             A.err = c.err.p;
             A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
+            if (is_fp32(c)) {
+                pack_tree_f32(c);
+            }
             for (int t = 0; t < 2; ++t) {
                 A.rec = c.tree.rec[t].p;
                 A.begin = t == 0 ? 0 : num_exc;
                 A.end = t == 0 ? num_exc : m;
                 if (A.end <= A.begin) {
+                    continue;
+                }
+                if (is_fp32(c)) {
+                    launch_search_f32(c, t, A.begin, A.end, step);
                     continue;
                 }
                 const uint64_t warps = (A.end - A.begin + 31) / 32;

@@ -121,6 +121,7 @@ void validate(const rl_config& k) {
     RL_CHECK(k.h_model >= 1 && k.h_model <= 1000, RL_ERR_INVALID, "h_model must lie in [1, 1000]");
     RL_CHECK(k.h_calcium >= 1 && k.h_calcium <= 1000, RL_ERR_INVALID, "h_calcium must lie in [1, 1000]");
     RL_CHECK(k.noise_stddev > 0.0, RL_ERR_INVALID, "noise_stddev must be positive");
+    RL_CHECK(k.precision == RL_PRECISION_FP64 || k.precision == RL_PRECISION_FP32, RL_ERR_INVALID, "precision must be FP64 or FP32");
     for (int a = 0; a < 3; ++a) {
         RL_CHECK(k.box_min[a] <= k.box_max[a], RL_ERR_INVALID, "box_min must not exceed box_max");
         RL_CHECK(k.retract_ratio[a] >= 0.0 && k.retract_ratio[a] <= 1.0, RL_ERR_INVALID, "retract ratio must lie in [0, 1]");
@@ -183,6 +184,9 @@ void create(Ctx& c, const rl_config& k) {
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
+    if (is_fp32(c)) {
+        alloc_fp32(c);
+    }
     RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
 }
 
@@ -460,10 +464,16 @@ rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* out, uint
 rl_status rl_set_elements(void* ctx, int type, const double* grown, const double* delta, const uint32_t* connected, const uint32_t* vacant) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(type >= 0 && type < 3, RL_ERR_INVALID, "element type must be 0, 1 or 2");
+        if (rl::is_fp32(c)) {
+            rl::f64_from_f32(c);
+        }
         if (grown) rl::upload(c.nr.grown[type], grown, c.n, c.stream);
         if (delta) rl::upload(c.nr.delta[type], delta, c.n, c.stream);
         if (connected) rl::upload(c.nr.connected[type], connected, c.n, c.stream);
         if (vacant) rl::upload(c.nr.vacant[type], vacant, c.n, c.stream);
+        if (rl::is_fp32(c)) {
+            rl::f32_from_f64(c);
+        }
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
     });
 }
@@ -471,6 +481,9 @@ rl_status rl_set_elements(void* ctx, int type, const double* grown, const double
 rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uint32_t* connected, uint32_t* vacant) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(type >= 0 && type < 3, RL_ERR_INVALID, "element type must be 0, 1 or 2");
+        if (rl::is_fp32(c)) {
+            rl::f64_from_f32(c);
+        }
         if (grown) rl::download(grown, c.nr.grown[type], c.n, c.stream);
         if (delta) rl::download(delta, c.nr.delta[type], c.n, c.stream);
         if (connected) rl::download(connected, c.nr.connected[type], c.n, c.stream);
@@ -481,16 +494,25 @@ rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uin
 
 rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const double* calcium, const uint8_t* fired) {
     return rl::guarded(ctx, [&](Ctx& c) {
+        if (rl::is_fp32(c)) {
+            rl::f64_from_f32(c);
+        }
         if (x) rl::upload(c.nr.x, x, c.n, c.stream);
         if (u) rl::upload(c.nr.u, u, c.n, c.stream);
         if (calcium) rl::upload(c.nr.calcium, calcium, c.n, c.stream);
         if (fired) rl::upload(c.nr.fired[c.nr.cur], fired, c.n, c.stream);
+        if (rl::is_fp32(c)) {
+            rl::f32_from_f64(c);
+        }
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
     });
 }
 
 rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input) {
     return rl::guarded(ctx, [&](Ctx& c) {
+        if (rl::is_fp32(c)) {
+            rl::f64_from_f32(c);
+        }
         if (x) rl::download(x, c.nr.x, c.n, c.stream);
         if (u) rl::download(u, c.nr.u, c.n, c.stream);
         if (calcium) rl::download(calcium, c.nr.calcium, c.n, c.stream);
@@ -590,6 +612,22 @@ rl_status rl_synchronize(void* ctx) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
         rl::check_device_error(c, "synchronize");
+    });
+}
+
+rl_status rl_candidate_weights(void* ctx, uint32_t source, int precision, uint32_t* nodes, double* weights, uint64_t capacity, uint64_t* count) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::require_tree(c);
+        RL_CHECK(precision == RL_PRECISION_FP64 || precision == RL_PRECISION_FP32, RL_ERR_INVALID, "precision must be FP64 or FP32");
+        std::vector<uint32_t> nd;
+        std::vector<double> w;
+        rl::candidate_weights(c, source, precision, nd, w);
+        if (count) *count = nd.size();
+        const uint64_t k = nd.size() < capacity ? nd.size() : capacity;
+        for (uint64_t i = 0; i < k; ++i) {
+            if (nodes) nodes[i] = nd[i];
+            if (weights) weights[i] = w[i];
+        }
     });
 }
 

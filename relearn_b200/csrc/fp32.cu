@@ -1,0 +1,809 @@
+// FP32 precision form of the activity update and of the Barnes-Hut search.
+//
+// Same algorithms as the FP64 drop-in (activity.cu, bh_search.cu) with
+// different arithmetic, as the precision form specifies:
+//   * membrane (Izhikevich), input (normal background) and growth-curve
+//     arithmetic in FP32, state x, u, growth deltas stored as FP32;
+//   * calcium integrated in FP64.  The h Euler substeps of
+//     CalciumCalculatorCPU::update_current_calcium (calcium/CalciumCalculatorCPU.cpp:61-68)
+//     form the linear recurrence c <- c*A + s*beta*fired with A = 1 + s/(-tau);
+//     h substeps are applied at once as c*A^h + s*beta*fired*(A^(h-1)+...+1)
+//     with both factors precomputed in FP64;
+//   * octree counts and centroids reduced in FP64 (octree.cu), then read by
+//     the search as FP32 records (16 B instead of 32 B);
+//   * attraction weights exp(-(d-mu)^2/sigma^2)*count in FP32, summed per lane in
+//     visiting order with Kahan compensation; the pick compares the
+//     compensated running sum with r.
+// Errors against the FP64 form are measured, not assumed (bench.py
+// --precision-report): selection probabilities, calcium drift, distances of
+// formed synapses.
+#include "rl_context.cuh"
+#include "rl_math.cuh"
+
+namespace rl {
+
+bool is_fp32(const Ctx& c) {
+    return c.cfg.precision == RL_PRECISION_FP32;
+}
+
+namespace {
+
+__global__ void k_d2f(uint32_t n, const double* __restrict__ a, float* __restrict__ b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        b[i] = (float)a[i];
+    }
+}
+
+__global__ void k_f2d(uint32_t n, const float* __restrict__ a, double* __restrict__ b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        b[i] = (double)a[i];
+    }
+}
+
+// ----------------------------------------------------------- activity
+struct Act32 {
+    uint32_t n, step;
+    uint64_t seed;
+    const uint8_t* enabled;
+    const uint32_t* csr_off;
+    const uint32_t* csr_src;
+    const int32_t* csr_w;
+    const uint8_t* fired_prev;
+    uint8_t* fired_cur;
+    float* x;
+    float* u;
+    float* input;
+    double* calcium;
+    float* delta[3];
+    float conductance, noise_mean, noise_stddev;
+    uint32_t h_model;
+    float a, ab, c, d, v_spike, k1, k2, k3, scale_m;
+    double ca_mul, ca_add;  // calcium: c <- c*ca_mul + fired*ca_add
+    float xi[3], inv_zeta[3], nu[3];
+    int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
+    float eta[3];
+    int has_edges;
+};
+
+// AS241 in FP32 (Wichura 1988, PPND7 accuracy), own log via __logf.
+__device__ __forceinline__ float normal_quantile_f32(float p) {
+    const float q = p - 0.5f;
+    if (fabsf(q) <= 0.425f) {
+        const float r = 0.180625f - q * q;
+        float num = 2.5090809287301226727e+3f;
+        num = fmaf(num, r, 3.3430575583588128105e+4f);
+        num = fmaf(num, r, 6.7265770927008700853e+4f);
+        num = fmaf(num, r, 4.5921953931549871457e+4f);
+        num = fmaf(num, r, 1.3731693765509461125e+4f);
+        num = fmaf(num, r, 1.9715909503065514427e+3f);
+        num = fmaf(num, r, 1.3314166789178437745e+2f);
+        num = fmaf(num, r, 3.3871328727963666080e+0f);
+        float den = 5.2264952788528545610e+3f;
+        den = fmaf(den, r, 2.8729085735721942674e+4f);
+        den = fmaf(den, r, 3.9307895800092710610e+4f);
+        den = fmaf(den, r, 2.1213794301586595867e+4f);
+        den = fmaf(den, r, 5.3941960214247511077e+3f);
+        den = fmaf(den, r, 6.8718700749205790830e+2f);
+        den = fmaf(den, r, 4.2313330701600911252e+1f);
+        den = fmaf(den, r, 1.0f);
+        return __fdividef(num * q, den);
+    }
+    float r = q < 0.0f ? p : 1.0f - p;
+    r = sqrtf(-__logf(r));
+    float num, den;
+    if (r <= 5.0f) {
+        r -= 1.6f;
+        num = 7.7454501427834140764e-4f;
+        num = fmaf(num, r, 2.2723844989269184583e-2f);
+        num = fmaf(num, r, 2.4178072517745061177e-1f);
+        num = fmaf(num, r, 1.2704582524523683826e+0f);
+        num = fmaf(num, r, 3.6478483247632046050e+0f);
+        num = fmaf(num, r, 5.7694972214606914055e+0f);
+        num = fmaf(num, r, 4.6303378461565452959e+0f);
+        num = fmaf(num, r, 1.4234371107496835773e+0f);
+        den = 1.0507500716444168432e-9f;
+        den = fmaf(den, r, 5.4759380849953449460e-4f);
+        den = fmaf(den, r, 1.5198666563616457197e-2f);
+        den = fmaf(den, r, 1.4810397642748007459e-1f);
+        den = fmaf(den, r, 6.8976733498510000455e-1f);
+        den = fmaf(den, r, 1.6763848301838038494e+0f);
+        den = fmaf(den, r, 2.0531916266377588219e+0f);
+        den = fmaf(den, r, 1.0f);
+    } else {
+        r -= 5.0f;
+        num = 2.0103343992922881327e-7f;
+        num = fmaf(num, r, 2.7115555687434875782e-5f);
+        num = fmaf(num, r, 1.2426609473880784386e-3f);
+        num = fmaf(num, r, 2.6532189526576123093e-2f);
+        num = fmaf(num, r, 2.9656057182850489123e-1f);
+        num = fmaf(num, r, 1.7848265399172913358e+0f);
+        num = fmaf(num, r, 5.4637849111641143699e+0f);
+        num = fmaf(num, r, 6.6579046435011037772e+0f);
+        den = 2.0442631033899397856e-15f;
+        den = fmaf(den, r, 1.4215117583164458887e-7f);
+        den = fmaf(den, r, 1.8463183175100546818e-5f);
+        den = fmaf(den, r, 7.8686913114561325910e-4f);
+        den = fmaf(den, r, 1.4875361290850614853e-2f);
+        den = fmaf(den, r, 1.3692988092273580531e-1f);
+        den = fmaf(den, r, 5.9983220655588793769e-1f);
+        den = fmaf(den, r, 1.0f);
+    }
+    const float x = __fdividef(num, den);
+    return q < 0.0f ? -x : x;
+}
+
+__global__ void __launch_bounds__(256) k_activity_f32(Act32 A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    if (!A.enabled[i]) {
+        A.input[i] = 0.0f;
+        A.fired_cur[i] = A.fired_prev[i];
+        return;
+    }
+    int isum = 0;
+    if (A.has_edges) {
+        const uint32_t e0 = A.csr_off[i], e1 = A.csr_off[i + 1];
+        for (uint32_t e = e0; e < e1; ++e) {
+            if (A.fired_prev[A.csr_src[e]]) {
+                isum += A.csr_w[e];
+            }
+        }
+    }
+    // the same Philox draw as the FP64 form, 24 bits of it
+    const u32x4 w = draw(A.seed, A.step, i, 0u, STREAM_NOISE, 0u);
+    const float p = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-8f;  // 2^-24
+    const float input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_quantile_f32(p), A.noise_mean));
+    A.input[i] = input;
+
+    float xv = A.x[i];
+    float uv = A.u[i];
+    uint8_t spiked = 0;
+    for (uint32_t it = 0; it < A.h_model; ++it) {
+        const float x_inc = fmaf(A.k1 * xv, xv, fmaf(A.k2, xv, A.k3)) - uv + input;
+        const float u_inc = fmaf(A.ab, xv, -A.a * uv);
+        xv = fmaf(x_inc, A.scale_m, xv);
+        uv = fmaf(u_inc, A.scale_m, uv);
+        if (xv >= A.v_spike) {
+            xv = A.c;
+            uv += A.d;
+            spiked = 1;
+            break;
+        }
+    }
+    A.x[i] = xv;
+    A.u[i] = uv;
+    A.fired_cur[i] = spiked;
+
+    const double ca = fma(A.calcium[i], A.ca_mul, spiked ? A.ca_add : 0.0);
+    A.calcium[i] = ca;
+    const float caf = (float)ca;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        float dz;
+        if (A.flat[t]) {
+            dz = caf == A.eta[t] ? 0.0f : -1.0f;
+        } else {
+            const float q = (caf - A.xi[t]) * A.inv_zeta[t];
+            dz = fmaf(2.0f, __expf(-q * q), -1.0f);
+        }
+        A.delta[t][i] = fmaf(dz, A.nu[t], A.delta[t][i]);
+    }
+}
+
+// ElementBaseBase::update with an FP32 delta.
+__global__ void k_commit_f32(uint32_t n, const uint8_t* __restrict__ enabled, double* grown, float* delta, uint32_t* connected, uint32_t* vacant,
+                             double retract, uint32_t* to_delete, unsigned long long* total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    if (!enabled[i]) {
+        to_delete[i] = 0u;
+        return;
+    }
+    const double current_count = grown[i];
+    const double current_delta = (double)delta[i];
+    const uint32_t conn_int = connected[i];
+    const double conn = (double)conn_int;
+    const double new_vacant = (current_count - conn) + current_delta;
+    const double keep = 1.0 - retract;
+    uint32_t del = 0;
+    if (new_vacant >= 0.0) {
+        const double after = keep * new_vacant;
+        grown[i] = after + conn;
+        vacant[i] = (uint32_t)after;
+    } else if (current_count + current_delta <= 0.0) {
+        grown[i] = 0.0;
+        vacant[i] = 0u;
+        connected[i] = 0u;
+        del = conn_int;
+    } else {
+        const double new_count = current_count + current_delta;
+        const double new_conn = floor(new_count);
+        grown[i] = keep * (new_count - new_conn) + new_conn;
+        vacant[i] = 0u;
+        connected[i] = (uint32_t)new_conn;
+        del = (uint32_t)(conn - new_conn);
+    }
+    delta[i] = 0.0f;
+    to_delete[i] = del;
+    if (del) {
+        atomicAdd(total, (unsigned long long)del);
+    }
+}
+
+__global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4* __restrict__ r1, const double* __restrict__ md, float4* __restrict__ o0,
+                       float4* __restrict__ o1, float* __restrict__ omd) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) {
+        return;
+    }
+    const double4 a = r0[i];
+    const double4 b = r1[i];
+    o0[i] = make_float4((float)a.x, (float)a.y, (float)a.z, __uint_as_float((uint32_t)__double_as_longlong(a.w)));
+    o1[i] = make_float4((float)b.x, (float)b.y, (float)b.z, __uint_as_float((uint32_t)__double_as_longlong(b.w)));
+    omd[i] = (float)md[i];
+}
+
+// ----------------------------------------------------------- search
+constexpr int kWarps = 4;
+constexpr int kStack = kMaxLevels + 4;
+enum : int { S_DISCARD = 0, S_EXPAND = 1, S_ACCEPT = 2 };
+
+struct Search32 {
+    const float4* rec;
+    const uint2* topo;
+    const float* maxdim;
+    const double *px, *py, *pz;
+    const uint32_t* list_src;
+    const uint32_t* list_j;
+    uint64_t begin, end;
+    int32_t* target;
+    float theta, mu, inv_sigma2;
+    uint64_t seed;
+    uint32_t step;
+    uint32_t* err;
+};
+
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void add(float x) {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+struct E32 {
+    int status;
+    float w;
+};
+
+__device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float sx, float sy, float sz, uint32_t source, const Search32& A, bool fb) {
+    E32 e{ S_DISCARD, 0.0f };
+    const uint32_t cnt = __float_as_uint(r.w);
+    if (cnt == 0) {
+        return e;
+    }
+    const float dx = r.x - sx, dy = r.y - sy, dz = r.z - sz;
+    const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    if (d == 0.0f) {
+        return e;
+    }
+    const bool leaf = topo_leaf(t.y);
+    if (!leaf && !(md < A.theta * d)) {
+        e.status = S_EXPAND;
+        return e;
+    }
+    e.status = S_ACCEPT;
+    if (leaf && t.x == source) {
+        e.w = 0.0f;
+    } else if (!fb) {
+        const float dm = d - A.mu;
+        e.w = __expf(-(dm * dm) * A.inv_sigma2) * (float)cnt;
+    } else {
+        e.w = __fdividef((float)cnt, d);
+    }
+    return e;
+}
+
+__device__ __forceinline__ uint32_t child_of(uint2 t, int oct) {
+    return t.x + (uint32_t)__popc(topo_mask(t.y) & ((1u << oct) - 1u));
+}
+
+__device__ __forceinline__ float threshold32(float total, const Search32& A, uint32_t source, uint32_t j, uint32_t depth) {
+    const u32x4 w = draw(A.seed, A.step, source, j, STREAM_BH_PICK, depth);
+    float r = (float)(w.x >> 8) * 5.9604644775390625e-8f * total;  // [0, total)
+    return r > 0.0f ? r : 1.0e-38f;
+}
+
+struct Walk32 {
+    KSum sum;
+    int32_t picked;
+    bool overflow;
+};
+
+__device__ Walk32 lane_walk32(const Search32& A, uint32_t sub, bool include_root, KSum start, bool pick, float r, float sx, float sy, float sz,
+                              uint32_t source, bool fb) {
+    Walk32 res{ start, -1, false };
+    uint32_t fnode[kStack];
+    uint32_t frem[kStack];
+    if (include_root) {
+        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sx, sy, sz, source, A, fb);
+        if (e.status == S_ACCEPT) {
+            res.sum.add(e.w);
+            if (pick && res.sum.s >= r) {
+                res.picked = (int32_t)sub;
+            }
+            return res;
+        }
+        if (e.status == S_DISCARD) {
+            return res;
+        }
+    }
+    fnode[0] = sub;
+    frem[0] = topo_mask(A.topo[sub].y);
+    int depth = 1;
+    while (depth > 0) {
+        const int top = depth - 1;
+        const uint32_t rem = frem[top];
+        if (rem == 0) {
+            --depth;
+            continue;
+        }
+        const int oct = 31 - __clz(rem);
+        frem[top] = rem & ~(1u << oct);
+        const uint32_t child = child_of(A.topo[fnode[top]], oct);
+        const uint2 tt = A.topo[child];
+        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sx, sy, sz, source, A, fb);
+        if (e.status == S_ACCEPT) {
+            res.sum.add(e.w);
+            if (pick && res.sum.s >= r) {
+                res.picked = (int32_t)child;
+                return res;
+            }
+        } else if (e.status == S_EXPAND) {
+            if (depth >= kStack) {
+                res.overflow = true;
+                return res;
+            }
+            fnode[depth] = child;
+            frem[depth] = topo_mask(tt.y);
+            ++depth;
+        }
+    }
+    return res;
+}
+
+__device__ KSum packet32(const Search32& A, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb, float2* cp, uint32_t* s_node,
+                         uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
+    const int lane = threadIdx.x & 31;
+    const bool me = (lanes >> lane) & 1u;
+    KSum sum{ 0.0f, 0.0f };
+    if (lane == 0) {
+        s_node[0] = 0;
+        s_rem[0] = topo_mask(A.topo[0].y);
+        s_act[0] = lanes;
+    }
+    __syncwarp();
+    int depth = 1;
+    while (depth > 0) {
+        const int top = depth - 1;
+        const uint32_t rem = s_rem[top];
+        if (rem == 0) {
+            --depth;
+            continue;
+        }
+        const uint32_t node = s_node[top];
+        const uint32_t act = s_act[top];
+        const int oct = 31 - __clz(rem);
+        __syncwarp();
+        if (lane == 0) {
+            s_rem[top] = rem & ~(1u << oct);
+        }
+        if (depth == 1 && me) {
+            cp[oct * 32] = make_float2(sum.s, sum.c);
+        }
+        const uint32_t child = child_of(A.topo[node], oct);
+        const float4 rr = A.rec[child];
+        const uint2 tt = A.topo[child];
+        const float md = A.maxdim[child];
+        int status = S_DISCARD;
+        if ((act >> lane) & 1u) {
+            const E32 e = eval32(rr, tt, md, sx, sy, sz, source, A, fb);
+            status = e.status;
+            if (e.status == S_ACCEPT) {
+                sum.add(e.w);
+            }
+        }
+        const uint32_t expand = __ballot_sync(0xFFFFFFFFu, status == S_EXPAND);
+        __syncwarp();
+        if (expand) {
+            if (depth >= kStack) {
+                overflow = true;
+                break;
+            }
+            if (lane == 0) {
+                s_node[depth] = child;
+                s_rem[depth] = topo_mask(tt.y);
+                s_act[depth] = expand;
+            }
+            ++depth;
+        }
+        __syncwarp();
+    }
+    __syncwarp();
+    return sum;
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
+    __shared__ uint32_t s_node[kWarps][kStack];
+    __shared__ uint32_t s_rem[kWarps][kStack];
+    __shared__ uint32_t s_act[kWarps][kStack];
+    __shared__ float2 s_cp[kWarps][8 * 32];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint64_t warp_global = (uint64_t)blockIdx.x * kWarps + wib;
+    if (A.begin + warp_global * 32 >= A.end) {
+        return;
+    }
+    const uint64_t idx = A.begin + warp_global * 32 + lane;
+    const bool active = idx < A.end;
+    const uint32_t source = active ? A.list_src[idx] : 0u;
+    const uint32_t j = active ? A.list_j[idx] : 0u;
+    const float sx = active ? (float)A.px[source] : 0.0f;
+    const float sy = active ? (float)A.py[source] : 0.0f;
+    const float sz = active ? (float)A.pz[source] : 0.0f;
+    float2* cp = &s_cp[wib][lane];
+    bool overflow = false;
+    const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
+    KSum total = packet32(A, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
+    bool fb = false;
+    const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total.s == 0.0f);
+    if (need_fb) {
+        const KSum t2 = packet32(A, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
+        if ((need_fb >> lane) & 1u) {
+            total = t2;
+            fb = true;
+        }
+    }
+    int32_t result = -1;
+    bool done = !active || total.s == 0.0f;
+    uint32_t sub = 0;
+    if (!done) {
+        const float r = threshold32(total.s, A, source, j, 0);
+        const uint2 root = A.topo[0];
+        const uint32_t mask = topo_mask(root.y);
+        int cstar = -1;
+        for (int oct = 7; oct >= 0; --oct) {
+            if ((mask >> oct) & 1u) {
+                if (cp[oct * 32].x < r) {
+                    cstar = oct;
+                } else {
+                    break;
+                }
+            }
+        }
+        if (cstar < 0) {
+            done = true;
+        } else {
+            const float2 c0 = cp[cstar * 32];
+            const Walk32 wr = lane_walk32(A, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
+            overflow |= wr.overflow;
+            if (wr.picked < 0) {
+                done = true;  // rounding left the crossing past the last candidate: no pick
+            } else {
+                sub = (uint32_t)wr.picked;
+            }
+        }
+    }
+    for (uint32_t depth = 1; !done; ++depth) {
+        if (depth > (uint32_t)kStack) {
+            overflow = true;
+            break;
+        }
+        const uint2 st = A.topo[sub];
+        if (topo_leaf(st.y)) {
+            result = (int32_t)st.x;
+            break;
+        }
+        Walk32 s1 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
+        bool f = false;
+        if (s1.sum.s == 0.0f) {
+            s1 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
+            f = true;
+        }
+        overflow |= s1.overflow;
+        if (s1.sum.s == 0.0f) {
+            break;
+        }
+        const float r = threshold32(s1.sum.s, A, source, j, depth);
+        const Walk32 s2 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
+        if (s2.picked < 0) {
+            break;
+        }
+        sub = (uint32_t)s2.picked;
+    }
+    if (overflow) {
+        atomicOr(A.err, (uint32_t)DERR_STACK);
+        result = -1;
+    }
+    if (active) {
+        A.target[idx] = result;
+    }
+}
+
+// ----------------------------------------------------------- diagnostic
+__global__ void k_candidates(const double4* rec64, const float4* rec32, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
+                             double sz, uint32_t source, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
+                             uint64_t capacity, unsigned long long* count, uint32_t* err) {
+    uint32_t fnode[kStack];
+    uint32_t frem[kStack];
+    int depth = 1;
+    fnode[0] = 0;
+    frem[0] = topo_mask(topo[0].y);
+    uint64_t k = 0;
+    const double scale = -1.0 / (sigma * sigma);
+    const float inv_s2 = (float)(1.0 / (sigma * sigma));
+    while (depth > 0) {
+        const int top = depth - 1;
+        const uint32_t rem = frem[top];
+        if (rem == 0) {
+            --depth;
+            continue;
+        }
+        const int oct = 31 - __clz(rem);
+        frem[top] = rem & ~(1u << oct);
+        const uint32_t child = child_of(topo[fnode[top]], oct);
+        const uint2 tt = topo[child];
+        const bool leaf = topo_leaf(tt.y);
+        int status = S_DISCARD;
+        double weight = 0.0;
+        if (precision == RL_PRECISION_FP64) {
+            const double4 r = rec64[child];
+            const uint32_t cnt = (uint32_t)__double_as_longlong(r.w);
+            if (cnt) {
+                const double d = rl_hypot3(r.x - sx, r.y - sy, r.z - sz);
+                if (d != 0.0) {
+                    if (!leaf && !(md64[child] < theta * d)) {
+                        status = S_EXPAND;
+                    } else {
+                        status = S_ACCEPT;
+                        weight = (leaf && tt.x == source) ? 0.0 : (rl_exp(((d - mu) * (d - mu)) * scale) * 1.0) * (double)cnt;
+                    }
+                }
+            }
+        } else {
+            const float4 r = rec32[child];
+            const uint32_t cnt = __float_as_uint(r.w);
+            if (cnt) {
+                const float dx = r.x - (float)sx, dy = r.y - (float)sy, dz = r.z - (float)sz;
+                const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                if (d != 0.0f) {
+                    if (!leaf && !(md32[child] < (float)theta * d)) {
+                        status = S_EXPAND;
+                    } else {
+                        status = S_ACCEPT;
+                        const float dm = d - (float)mu;
+                        weight = (leaf && tt.x == source) ? 0.0 : (double)(__expf(-(dm * dm) * inv_s2) * (float)cnt);
+                    }
+                }
+            }
+        }
+        if (status == S_ACCEPT) {
+            if (k < capacity) {
+                nodes[k] = child;
+                w[k] = weight;
+            }
+            ++k;
+        } else if (status == S_EXPAND) {
+            if (depth >= kStack) {
+                atomicOr(err, (uint32_t)DERR_STACK);
+                break;
+            }
+            fnode[depth] = child;
+            frem[depth] = topo_mask(tt.y);
+            ++depth;
+        }
+    }
+    *count = k;
+}
+
+}  // namespace
+
+void alloc_fp32(Ctx& c) {
+    const size_t n = c.n;
+    c.nr.x32.alloc(n);
+    c.nr.u32.alloc(n);
+    c.nr.input32.alloc(n);
+    for (int t = 0; t < 3; ++t) {
+        c.nr.delta32[t].alloc(n);
+    }
+    f32_from_f64(c);
+}
+
+void f32_from_f64(Ctx& c) {
+    const uint32_t n = c.n;
+    const unsigned b = blocks_for(n, 256);
+    k_d2f<<<b, 256, 0, c.stream>>>(n, c.nr.x.p, c.nr.x32.p);
+    RL_LAUNCH_CHECK();
+    k_d2f<<<b, 256, 0, c.stream>>>(n, c.nr.u.p, c.nr.u32.p);
+    RL_LAUNCH_CHECK();
+    k_d2f<<<b, 256, 0, c.stream>>>(n, c.nr.input.p, c.nr.input32.p);
+    RL_LAUNCH_CHECK();
+    for (int t = 0; t < 3; ++t) {
+        k_d2f<<<b, 256, 0, c.stream>>>(n, c.nr.delta[t].p, c.nr.delta32[t].p);
+        RL_LAUNCH_CHECK();
+    }
+}
+
+void f64_from_f32(Ctx& c) {
+    const uint32_t n = c.n;
+    const unsigned b = blocks_for(n, 256);
+    k_f2d<<<b, 256, 0, c.stream>>>(n, c.nr.x32.p, c.nr.x.p);
+    RL_LAUNCH_CHECK();
+    k_f2d<<<b, 256, 0, c.stream>>>(n, c.nr.u32.p, c.nr.u.p);
+    RL_LAUNCH_CHECK();
+    k_f2d<<<b, 256, 0, c.stream>>>(n, c.nr.input32.p, c.nr.input.p);
+    RL_LAUNCH_CHECK();
+    for (int t = 0; t < 3; ++t) {
+        k_f2d<<<b, 256, 0, c.stream>>>(n, c.nr.delta32[t].p, c.nr.delta[t].p);
+        RL_LAUNCH_CHECK();
+    }
+}
+
+void run_activity_step_f32(Ctx& c, uint32_t step) {
+    const rl_config& k = c.cfg;
+    Act32 A;
+    A.n = c.n;
+    A.step = step;
+    A.seed = k.seed;
+    A.enabled = c.nr.enabled.p;
+    A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
+    A.csr_off = c.graph.offsets.p;
+    A.csr_src = c.graph.src.p;
+    A.csr_w = c.graph.weight.p;
+    A.fired_prev = c.nr.fired[c.nr.cur].p;
+    A.fired_cur = c.nr.fired[c.nr.cur ^ 1].p;
+    A.x = c.nr.x32.p;
+    A.u = c.nr.u32.p;
+    A.input = c.nr.input32.p;
+    A.calcium = c.nr.calcium.p;
+    for (int t = 0; t < 3; ++t) {
+        A.delta[t] = c.nr.delta32[t].p;
+    }
+    A.conductance = (float)k.conductance;
+    A.noise_mean = (float)k.noise_mean;
+    A.noise_stddev = (float)k.noise_stddev;
+    A.h_model = k.h_model;
+    A.a = (float)k.iz_a;
+    A.ab = (float)(k.iz_a * k.iz_b);
+    A.c = (float)k.iz_c;
+    A.d = (float)k.iz_d;
+    A.v_spike = (float)k.iz_v_spike;
+    A.k1 = (float)k.iz_k1;
+    A.k2 = (float)k.iz_k2;
+    A.k3 = (float)k.iz_k3;
+    A.scale_m = (float)(1.0 / (double)k.h_model);
+    // h calcium substeps c <- c*a + b at once
+    const long double s = 1.0L / (long double)k.h_calcium;
+    const long double a = 1.0L + s * (-1.0L / (long double)k.tau_c);
+    long double an = 1.0L, geo = 0.0L;
+    for (uint32_t it = 0; it < k.h_calcium; ++it) {
+        geo += an;
+        an *= a;
+    }
+    A.ca_mul = (double)an;
+    A.ca_add = (double)(s * (long double)k.beta * geo);
+    const double factor_inv = 1.0 / 1.6651092223153955127063292897904020952611777045288814583336582344;
+    for (int t = 0; t < 3; ++t) {
+        const double eta = k.min_calcium[t];
+        const double eps = k.target_calcium < eta ? eta : k.target_calcium;
+        A.flat[t] = eta == eps;
+        A.eta[t] = (float)eta;
+        A.xi[t] = (float)((eta + eps) * 0.5);
+        A.inv_zeta[t] = A.flat[t] ? 0.0f : (float)(1.0 / ((eta - eps) * factor_inv));
+        A.nu[t] = (float)k.growth_rate[t];
+    }
+    {
+        PhaseScope ps(c, PH_ACTIVITY_KERNEL);
+        k_activity_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
+        RL_LAUNCH_CHECK();
+    }
+    c.nr.cur ^= 1;
+    c.stats.activity_steps += 1;
+}
+
+uint64_t run_commit_f32(Ctx& c, int type) {
+    unsigned long long* d_del = reinterpret_cast<unsigned long long*>(c.counters.p) + 1;
+    RL_CUDA_TRY(cudaMemsetAsync(d_del, 0, sizeof(unsigned long long), c.stream));
+    k_commit_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(c.n, c.nr.enabled.p, c.nr.grown[type].p, c.nr.delta32[type].p, c.nr.connected[type].p,
+                                                             c.nr.vacant[type].p, c.cfg.retract_ratio[type], c.to_delete.p, d_del);
+    RL_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&h, d_del, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    c.stats.bound_to_delete += h;
+    return h;
+}
+
+void pack_tree_f32(Ctx& c) {
+    Tree& T = c.tree;
+    const uint32_t m = T.num_nodes;
+    T.rec32[0].ensure(m);
+    T.rec32[1].ensure(m);
+    T.maxdim32.ensure(m);
+    k_pack<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, T.rec[0].p, T.rec[1].p, T.maxdim.p, T.rec32[0].p, T.rec32[1].p, T.maxdim32.p);
+    RL_LAUNCH_CHECK();
+}
+
+void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t step) {
+    Search32 A;
+    A.rec = c.tree.rec32[type].p;
+    A.topo = c.tree.topo.p;
+    A.maxdim = c.tree.maxdim32.p;
+    A.px = c.nr.px.p;
+    A.py = c.nr.py.p;
+    A.pz = c.nr.pz.p;
+    A.list_src = c.search.src.p;
+    A.list_j = c.search.jj.p;
+    A.begin = begin;
+    A.end = end;
+    A.target = c.search.target.p;
+    A.theta = (float)c.cfg.theta;
+    A.mu = (float)c.cfg.mu;
+    A.inv_sigma2 = (float)(1.0 / (c.cfg.sigma * c.cfg.sigma));
+    A.seed = c.cfg.seed;
+    A.step = step;
+    A.err = c.err.p;
+    const uint64_t warps = (end - begin + 31) / 32;
+    const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
+    PhaseScope ps(c, PH_SEARCH_KERNEL);
+    k_search_f32<<<blocks, kWarps * 32, 0, c.stream>>>(A);
+    RL_LAUNCH_CHECK();
+}
+
+void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w) {
+    RL_CHECK(source < c.n, RL_ERR_INVALID, "source out of range");
+    RL_CHECK(!c.tree.root_is_leaf, RL_ERR_INVALID, "the octree has a single neuron");
+    if (precision == RL_PRECISION_FP32) {
+        pack_tree_f32(c);
+    }
+    uint8_t sig = 0;
+    double pos[3];
+    RL_CUDA_TRY(cudaMemcpyAsync(&sig, c.nr.signal.p + source, 1, cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaMemcpyAsync(&pos[0], c.nr.px.p + source, 8, cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaMemcpyAsync(&pos[1], c.nr.py.p + source, 8, cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaMemcpyAsync(&pos[2], c.nr.pz.p + source, 8, cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    const uint64_t cap = 1u << 16;
+    DBuf<uint32_t> dn;
+    DBuf<double> dw;
+    DBuf<unsigned long long> dc;
+    dn.alloc(cap);
+    dw.alloc(cap);
+    dc.alloc(1);
+    k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.rec32[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
+                                        precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, precision,
+                                        c.cfg.theta, c.cfg.mu, c.cfg.sigma, dn.p, dw.p, cap, dc.p, c.err.p);
+    RL_LAUNCH_CHECK();
+    unsigned long long k = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&k, dc.p, sizeof(k), cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    check_device_error(c, "candidate weights");
+    RL_CHECK(k <= cap, RL_ERR_OVERFLOW, "more than 65536 candidates");
+    nodes.resize(k);
+    w.resize(k);
+    if (k) {
+        RL_CUDA_TRY(cudaMemcpyAsync(nodes.data(), dn.p, k * 4, cudaMemcpyDeviceToHost, c.stream));
+        RL_CUDA_TRY(cudaMemcpyAsync(w.data(), dw.p, k * 8, cudaMemcpyDeviceToHost, c.stream));
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    }
+}
+
+}  // namespace rl

@@ -38,6 +38,9 @@ struct Tree {
     DBuf<uint32_t> leaf_of;    // neuron -> node
     DBuf<uint32_t> morton;     // Morton rank -> neuron
     DBuf<uint32_t> arrive;     // bottom-up arrival counters
+    // FP32 form: records (centroid, count bits in w) and cell lengths as FP32
+    DBuf<float4> rec32[2];
+    DBuf<float> maxdim32;
 };
 
 struct Neurons {
@@ -51,6 +54,8 @@ struct Neurons {
     DBuf<double> grown[3], delta[3];
     DBuf<uint32_t> connected[3], vacant[3];
     DBuf<uint32_t> search_vacant;  // vacant axons handed to the next search
+    // FP32 form: authoritative membrane / growth state in FP32
+    DBuf<float> x32, u32, input32, delta32[3];
 };
 
 // Synapse list: one entry per (target, source) synapse group with an integer
@@ -158,6 +163,17 @@ uint64_t run_connector(Ctx& c, uint32_t step);  // accepts requests, updates ele
 void rebuild_graph(Ctx& c);                     // merge new edges into the CSR
 uint64_t run_deletion(Ctx& c, uint32_t step, int type);  // delete to_delete[] synapses per neuron for one element type
 void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w);
+
+// fp32.cu (precision form)
+bool is_fp32(const Ctx& c);
+void alloc_fp32(Ctx& c);
+void f32_from_f64(Ctx& c);  // state arrays FP64 -> FP32 (after a host upload)
+void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download)
+void run_activity_step_f32(Ctx& c, uint32_t step);
+uint64_t run_commit_f32(Ctx& c, int type);
+void pack_tree_f32(Ctx& c);
+void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t step);
+void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu
 void run_activity_step(Ctx& c, uint32_t step);

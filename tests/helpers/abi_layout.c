@@ -17,6 +17,7 @@ int main(void) {
     F(rl_config, growth_rate);
     F(rl_config, conductance);
     F(rl_config, device);
+    F(rl_config, precision);
     F(rl_stats, max_level);
     return 0;
 }

@@ -52,7 +52,7 @@ def test_struct_layout(tmp_path):
     assert int(lines["rl_stats"]) == C.sizeof(R.RlStats)
     assert int(lines["rl_request"]) == R.REQUEST_DTYPE.itemsize
     assert int(lines["rl_synapse"]) == R.SYNAPSE_DTYPE.itemsize
-    for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device"):
+    for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device", "precision"):
         assert int(lines[f"rl_config.{f}"]) == getattr(R.RlConfig, f).offset
     assert int(lines["rl_stats.max_level"]) == R.RlStats.max_level.offset
 

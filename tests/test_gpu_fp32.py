@@ -1,0 +1,83 @@
+"""FP32 precision form against the FP64 drop-in on the same seed.
+
+Tolerances (stated here, measured at scale by bench.py --precision-report):
+* one activity step from the same state: x and u within 2e-5 relative for
+  neurons that spike in neither form; calcium within 1e-12 relative;
+* selection probabilities of the first descent: within 1e-5 relative for every
+  candidate with probability >= 1e-6 in the FP64 form;
+* a seeded FP32 run keeps the element and synapse bookkeeping consistent."""
+import numpy as np
+import pytest
+
+from conftest import seed_elements, small_network
+
+pytestmark = pytest.mark.gpu
+
+
+def make(n, side, seed, precision, mixture=False):
+    from relearn_b200 import Network
+
+    params, pos, sig = small_network(n, side, seed, mixture)
+    params["precision"] = precision
+    net = Network(params)
+    net.set_positions(pos, sig)
+    return net, params, pos, sig
+
+
+def test_one_step_close_to_fp64():
+    n = 20000
+    a, *_ = make(n, 2000.0, 5, 0)
+    b, *_ = make(n, 2000.0, 5, 1)
+    rng = np.random.default_rng(1)
+    x0 = rng.uniform(-70.0, -50.0, n)
+    u0 = rng.uniform(-14.0, -10.0, n)
+    ca0 = rng.uniform(0.0, 1.0, n)
+    for net in (a, b):
+        net.set_neurons(x=x0, u=u0, calcium=ca0)
+        net.activity_block(7, 1)
+    ga, gb = a.neurons(), b.neurons()
+    quiet = (ga["fired"] == 0) & (gb["fired"] == 0)
+    assert quiet.mean() > 0.5
+    for k in ("x", "u"):
+        rel = np.abs(ga[k][quiet] - gb[k][quiet]) / np.maximum(np.abs(ga[k][quiet]), 1.0)
+        assert rel.max() < 2e-5, (k, rel.max())
+    both = ga["fired"] == gb["fired"]
+    assert both.mean() > 0.999
+    rel_ca = np.abs(ga["calcium"][both] - gb["calcium"][both]) / np.abs(ga["calcium"][both])
+    assert rel_ca.max() < 1e-12
+
+
+@pytest.mark.parametrize("mixture", [False, True])
+def test_selection_probabilities(mixture):
+    n = 50000
+    net, *_ = make(n, 3700.0, 9, 1, mixture)
+    one = np.ones(n, np.uint32)
+    net.prepare_update_connectivity(one, one, one)
+    rng = np.random.default_rng(3)
+    worst = 0.0
+    for s in rng.choice(n, 40, replace=False):
+        n64, w64 = net.candidate_weights(int(s), 0)
+        n32, w32 = net.candidate_weights(int(s), 1)
+        p64 = dict(zip(n64.tolist(), (w64 / w64.sum()).tolist()))
+        p32 = dict(zip(n32.tolist(), (w32 / w32.sum()).tolist()))
+        for node, p in p64.items():
+            if p >= 1e-6:
+                worst = max(worst, abs(p32.get(node, 0.0) - p) / p)
+    assert worst <= 1e-5, worst
+
+
+def test_seeded_fp32_run_bookkeeping():
+    n = 4000
+    net, *_ = make(n, 1260.0, 11, 1)
+    seed_elements(net, n, 4, 0.0, 3.0)
+    net.simulate(1, 1001)
+    st = net.stats()
+    assert st["synapses_created"] > 0
+    t, s, w = net.edges()
+    ax = net.get_elements(0)["connected"]
+    ex = net.get_elements(1)["connected"]
+    ih = net.get_elements(2)["connected"]
+    # every synapse is counted once on each side
+    assert ax.sum() == np.abs(w).sum() == ex.sum() + ih.sum()
+    out_deg = np.bincount(s, weights=np.abs(w), minlength=n)
+    assert np.array_equal(out_deg.astype(np.uint32), ax)
