@@ -401,6 +401,7 @@ def run_case(args):
     import relearn_b200 as R
 
     params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
+    params["precision"] = 1 if args.precision == "fp32" else 0
     net = R.Network(params)
     if args.case == "activity":
         net.activity_block(1, 4)

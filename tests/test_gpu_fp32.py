@@ -1,7 +1,7 @@
 """FP32 precision form against the FP64 drop-in on the same seed.
 
 Tolerances (stated here, measured at scale by bench.py --precision-report):
-* one activity step from the same state: x and u within 2e-5 relative for
+* one activity step from the same state: x and u within 1e-4 relative for
   neurons that spike in neither form; calcium within 1e-12 relative;
 * selection probabilities of the first descent: within 1e-5 relative for every
   candidate with probability >= 1e-6 in the FP64 form;
@@ -40,7 +40,7 @@ def test_one_step_close_to_fp64():
     assert quiet.mean() > 0.5
     for k in ("x", "u"):
         rel = np.abs(ga[k][quiet] - gb[k][quiet]) / np.maximum(np.abs(ga[k][quiet]), 1.0)
-        assert rel.max() < 2e-5, (k, rel.max())
+        assert rel.max() < 1e-4, (k, rel.max())
     both = ga["fired"] == gb["fired"]
     assert both.mean() > 0.999
     rel_ca = np.abs(ga["calcium"][both] - gb["calcium"][both]) / np.abs(ga["calcium"][both])
