@@ -139,11 +139,32 @@ enum {
     RL_NUM_PHASES = 7
 };
 
+/* One network of an ensemble (rl_ensemble_create): its own size, seed, cube,
+ * acceptance criterion, kernel width and growth rates; everything else comes
+ * from the ensemble's base rl_config. */
+typedef struct rl_network {
+    uint32_t num_neurons;
+    uint32_t reserved;
+    uint64_t seed;
+    double box_min[3];
+    double box_max[3];
+    double theta;
+    double sigma;
+    double growth_rate[3];
+} rl_network;
+
 /* Fill *cfg with the reference defaults for n neurons in the given cube. */
 RL_API void rl_config_default(rl_config* cfg, uint32_t num_neurons, double side);
 
 /* Create a context for cfg->num_neurons neurons on cfg->device. */
 RL_API rl_status rl_ctx_create(const rl_config* cfg, void** ctx);
+
+/* Create one context holding `num_networks` independent networks (the batched
+ * form): their neurons are concatenated in network order in every array of
+ * the other entry points, each activity step is one launch over all networks,
+ * and each network evolves exactly as it would in a context of its own with
+ * the same parameters.  base->num_neurons is ignored. */
+RL_API rl_status rl_ensemble_create(const rl_config* base, const rl_network* networks, uint32_t num_networks, void** ctx);
 RL_API rl_status rl_ctx_destroy(void* ctx);
 RL_API const char* rl_last_error(void* ctx);
 RL_API const char* rl_status_string(rl_status s);

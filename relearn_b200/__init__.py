@@ -83,6 +83,19 @@ class RlConfig(C.Structure):
 PRECISION_FP64, PRECISION_FP32 = 0, 1
 
 
+class RlNetwork(C.Structure):
+    _fields_ = [
+        ("num_neurons", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("seed", C.c_uint64),
+        ("box_min", C.c_double * 3),
+        ("box_max", C.c_double * 3),
+        ("theta", C.c_double),
+        ("sigma", C.c_double),
+        ("growth_rate", C.c_double * 3),
+    ]
+
+
 class RlStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("searches", "requests", "synapses_created", "bound_to_delete", "synapses_deleted", "activity_steps",
                                            "plasticity_updates", "gpu_launches", "num_nodes")] + [("max_level", C.c_uint32),
@@ -94,7 +107,7 @@ SYNAPSE_DTYPE = np.dtype([("target", "<u4"), ("source", "<u4"), ("weight", "<i4"
 
 # Every entry point declared in include/relearn_b200.h.
 ABI_FUNCTIONS = [
-    "rl_config_default", "rl_ctx_create", "rl_ctx_destroy", "rl_last_error", "rl_status_string", "rl_abi_version",
+    "rl_config_default", "rl_ctx_create", "rl_ensemble_create", "rl_ctx_destroy", "rl_last_error", "rl_status_string", "rl_abi_version",
     "rl_set_positions", "rl_tree_info", "rl_dump_tree", "rl_prepare_update_connectivity", "rl_find_targets",
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
@@ -121,6 +134,8 @@ def load_library(path: str = LIB_PATH):
     L.rl_config_default.argtypes = [P(RlConfig), u32, dbl]
     L.rl_ctx_create.restype = st
     L.rl_ctx_create.argtypes = [P(RlConfig), P(vp)]
+    L.rl_ensemble_create.restype = st
+    L.rl_ensemble_create.argtypes = [P(RlConfig), P(RlNetwork), u32, P(vp)]
     L.rl_ctx_destroy.restype = st
     L.rl_ctx_destroy.argtypes = [vp]
     L.rl_last_error.restype = C.c_char_p
@@ -211,15 +226,35 @@ def make_config(params: dict) -> RlConfig:
 class Network:
     """One network in one device context (rl_ctx)."""
 
-    def __init__(self, params: dict):
+    def __init__(self, params: dict, networks: Optional[list] = None):
+        """One network from `params`, or — with `networks`, a list of dicts
+        with num_neurons, seed, side (or box_min/box_max), theta, sigma,
+        growth_rate — an ensemble whose shared parameters come from `params`."""
         self.lib = load_library()
         self.params = dict(params)
-        self.n = int(params["num_neurons"])
         self.cfg = make_config(params)
         h = C.c_void_p()
-        s = self.lib.rl_ctx_create(C.byref(self.cfg), C.byref(h))
+        if networks is None:
+            self.n = int(params["num_neurons"])
+            s = self.lib.rl_ctx_create(C.byref(self.cfg), C.byref(h))
+        else:
+            arr = (RlNetwork * len(networks))()
+            for k, d in enumerate(networks):
+                r = arr[k]
+                r.num_neurons = int(d["num_neurons"])
+                r.seed = int(d["seed"])
+                side = d.get("side")
+                r.box_min[:] = list(d.get("box_min", (0.0, 0.0, 0.0)))
+                r.box_max[:] = list(d.get("box_max", (side, side, side)))
+                r.theta = float(d["theta"])
+                r.sigma = float(d["sigma"])
+                gr = d["growth_rate"]
+                r.growth_rate[:] = list(gr) if hasattr(gr, "__len__") else [float(gr)] * 3
+            self.networks = [dict(d) for d in networks]
+            self.n = int(sum(int(d["num_neurons"]) for d in networks))
+            s = self.lib.rl_ensemble_create(C.byref(self.cfg), arr, len(networks), C.byref(h))
         if s != RL_OK:
-            raise RelearnError(s, "rl_ctx_create failed")
+            raise RelearnError(s, "context creation failed")
         self.h = h
 
     # ---- plumbing

@@ -26,7 +26,6 @@ namespace {
 struct ActArgs {
     uint32_t n;
     uint32_t step;
-    uint64_t seed;
     const uint8_t* enabled;
     const uint32_t* csr_off;
     const uint32_t* csr_src;
@@ -45,8 +44,10 @@ struct ActArgs {
     uint32_t h_model, h_calcium;
     double a, ab, c, d, v_spike, k1, k2, k3, scale_m;
     double beta, tau_inv, scale_c;
-    double eta[3], nu[3];
+    double eta[3];
     int has_edges;
+    const NetInfo* nets;
+    const uint16_t* net_of;
 };
 
 __device__ __forceinline__ double growth_curve(double current, double eta, double eps) {
@@ -84,9 +85,11 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A) {
             }
         }
     }
+    // draws are keyed on the network's seed and the neuron's index in its network
+    const NetInfo& N = A.nets[A.net_of[i]];
     double input = 0.0;
     input += (double)isum * A.conductance;
-    input += background_normal(A.seed, A.step, i, A.noise_mean, A.noise_stddev);
+    input += background_normal(N.seed, A.step, i - N.first, A.noise_mean, A.noise_stddev);
     A.input[i] = input;
 
     double xv = A.x[i];
@@ -121,7 +124,7 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A) {
     for (int t = 0; t < 3; ++t) {
         const double eta = A.eta[t];
         const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
-        const double inc = growth_curve(ca, eta, eps) * A.nu[t];
+        const double inc = growth_curve(ca, eta, eps) * N.nu[t];
         deltas[t][i] = deltas[t][i] + inc;
     }
 }
@@ -194,7 +197,6 @@ void run_activity_step(Ctx& c, uint32_t step) {
     ActArgs A;
     A.n = c.n;
     A.step = step;
-    A.seed = k.seed;
     A.enabled = c.nr.enabled.p;
     A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
     A.csr_off = c.graph.offsets.p;
@@ -229,8 +231,9 @@ void run_activity_step(Ctx& c, uint32_t step) {
     A.scale_c = 1.0 / (double)k.h_calcium;
     for (int t = 0; t < 3; ++t) {
         A.eta[t] = k.min_calcium[t];
-        A.nu[t] = k.growth_rate[t];
     }
+    A.nets = c.d_nets.p;
+    A.net_of = c.net_of.p;
     {
         PhaseScope ps(c, PH_ACTIVITY_KERNEL);
         k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);

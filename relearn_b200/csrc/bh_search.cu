@@ -46,13 +46,28 @@ struct SearchArgs {
     const double *px, *py, *pz;
     const uint32_t* list_src;
     const uint32_t* list_j;
-    uint64_t begin, end;  // segment of the search list
+    // segments of the search list, one per network with searches: warps
+    // [seg_warp[s], seg_warp[s+1]) handle list entries [seg_begin[s], seg_end[s])
+    const uint32_t* seg_warp;
+    const uint64_t* seg_begin;
+    const uint64_t* seg_end;
+    const uint32_t* seg_net;
+    uint32_t num_segs;
+    const NetInfo* nets;
     int32_t* target;
-    double theta, mu, scale;
-    uint64_t seed;
+    double mu;
     uint32_t step;
     uint32_t* err;
     unsigned long long* touched;
+};
+
+// Parameters of the network a warp searches in.
+struct WarpNet {
+    double theta;
+    double scale;
+    uint64_t seed;
+    uint32_t root;
+    uint32_t first;
 };
 
 __device__ __forceinline__ uint32_t rcount(const double4& r) {
@@ -121,8 +136,8 @@ struct WalkResult {
     bool overflow;
 };
 
-__device__ WalkResult lane_walk(const SearchArgs& A, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r, double sx, double sy,
-                                double sz, uint32_t source, bool fallback) {
+__device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r,
+                                double sx, double sy, double sz, uint32_t source, bool fallback) {
     WalkResult res{ start_sum, -1, 0, false };
     uint32_t fnode[kStackDepth];
     uint32_t frem[kStackDepth];
@@ -130,7 +145,7 @@ __device__ WalkResult lane_walk(const SearchArgs& A, uint32_t sub, bool include_
     if (include_root) {
         const double4 rr = ldg4(&A.rec[sub]);
         const uint2 tt = __ldg(&A.topo[sub]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
             res.sum += e.w;
@@ -162,7 +177,7 @@ __device__ WalkResult lane_walk(const SearchArgs& A, uint32_t sub, bool include_
         const uint32_t child = child_index(pt, oct);
         const double4 rr = ldg4(&A.rec[child]);
         const uint2 tt = __ldg(&A.topo[child]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
             res.sum += e.w;
@@ -185,14 +200,14 @@ __device__ WalkResult lane_walk(const SearchArgs& A, uint32_t sub, bool include_
 
 // Warp-packet walk over the whole tree for the lanes in `lanes`; each lane
 // returns its sequential sum and the running sum before every root child.
-__device__ double packet_walk(const SearchArgs& A, uint32_t lanes, double sx, double sy, double sz, uint32_t source, bool fallback, double* cp_lane,
-                              uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
+__device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t lanes, double sx, double sy, double sz, uint32_t source, bool fallback,
+                              double* cp_lane, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     double sum = 0.0;
-    const uint2 root = __ldg(&A.topo[0]);
+    const uint2 root = __ldg(&A.topo[W.root]);
     if (lane == 0) {
-        s_node[0] = 0;
+        s_node[0] = W.root;
         s_rem[0] = topo_mask(root.y);
         s_act[0] = lanes;
     }
@@ -222,7 +237,7 @@ __device__ double packet_walk(const SearchArgs& A, uint32_t lanes, double sx, do
         const double md = __ldg(&A.maxdim[child]);
         int status = ST_DISCARD;
         if ((act >> lane) & 1u) {
-            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, A.theta, A.mu, A.scale, fallback);
+            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
             status = e.status;
             ++touched;
             if (e.status == ST_ACCEPT) {
@@ -256,12 +271,31 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
     __shared__ double s_cp[kWarpsPerBlock][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const uint64_t warp_global = (uint64_t)blockIdx.x * kWarpsPerBlock + wib;
-    const uint64_t idx = A.begin + warp_global * 32 + lane;
-    if (A.begin + warp_global * 32 >= A.end) {
+    const uint32_t warp_global = blockIdx.x * kWarpsPerBlock + wib;
+    if (warp_global >= A.seg_warp[A.num_segs]) {
         return;  // whole warp idle
     }
-    const bool active = idx < A.end;
+    // segment (network) of this warp
+    uint32_t lo = 0, hi = A.num_segs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A.seg_warp[mid] <= warp_global) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    const NetInfo& N = A.nets[A.seg_net[lo]];
+    const WarpNet W{ N.theta, N.scale, N.seed, A.seg_net[lo], N.first };
+    const uint64_t idx = A.seg_begin[lo] + (uint64_t)(warp_global - A.seg_warp[lo]) * 32 + lane;
+    const bool active = idx < A.seg_end[lo];
+    if (N.root_leaf) {
+        // a network of one neuron: its only candidate is itself
+        if (active) {
+            A.target[idx] = -1;
+        }
+        return;
+    }
     const uint32_t source = active ? A.list_src[idx] : 0u;
     const uint32_t j = active ? A.list_j[idx] : 0u;
     const double sx = active ? A.px[source] : 0.0;
@@ -273,12 +307,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
     uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
 
     // ---- descent 0: warp packet over the whole tree
-    double total = packet_walk(A, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], touched, overflow);
+    double total = packet_walk(A, W, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], touched, overflow);
     bool fallback = false;
     const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total == 0.0);
     if (need_fb) {
         uint32_t t2 = 0;
-        const double fb = packet_walk(A, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], t2, overflow);
+        const double fb = packet_walk(A, W, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], t2, overflow);
         if ((need_fb >> lane) & 1u) {
             total = fb;
             fallback = true;
@@ -291,10 +325,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
     }
     uint32_t sub = 0;
     if (!done) {
-        const double r = pick_threshold(total, A.seed, A.step, source, j, 0);
+        const double r = pick_threshold(total, W.seed, A.step, source - W.first, j, 0);
         // the crossing lies in the last root-child subtree (DFS order) whose
         // checkpoint is below r
-        const uint2 root = __ldg(&A.topo[0]);
+        const uint2 root = __ldg(&A.topo[W.root]);
         const uint32_t mask = topo_mask(root.y);
         int cstar = -1;
         for (int oct = 7; oct >= 0; --oct) {
@@ -311,7 +345,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
             done = true;
         } else {
             const uint32_t c0 = child_index(root, cstar);
-            const WalkResult wr = lane_walk(A, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
+            const WalkResult wr = lane_walk(A, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
             overflow |= wr.overflow;
             if (wr.picked < 0) {
                 atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
@@ -333,11 +367,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
             done = true;
             break;
         }
-        WalkResult s1 = lane_walk(A, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
+        WalkResult s1 = lane_walk(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
         touched += s1.touched;
         bool fb = false;
         if (s1.sum == 0.0) {
-            s1 = lane_walk(A, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
+            s1 = lane_walk(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
             fb = true;
         }
         overflow |= s1.overflow;
@@ -345,8 +379,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
             done = true;
             break;
         }
-        const double r = pick_threshold(s1.sum, A.seed, A.step, source, j, depth);
-        const WalkResult s2 = lane_walk(A, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
+        const double r = pick_threshold(s1.sum, W.seed, A.step, source - W.first, j, depth);
+        const WalkResult s2 = lane_walk(A, W, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
         if (s2.picked < 0) {
             atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
             done = true;
@@ -399,6 +433,17 @@ __global__ void k_search_fill(uint32_t n, const uint32_t* __restrict__ morton, c
     for (uint32_t j = 0; j < v; ++j) {
         list_src[base + j] = nid;
         list_j[base + j] = j;
+    }
+}
+
+// Start of every network's searches in the exclusive scans of both types.
+__global__ void k_net_starts(uint32_t K, const NetInfo* __restrict__ nets, const uint32_t* __restrict__ off_exc, const uint32_t* __restrict__ off_inh,
+                             uint32_t n, uint32_t* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) {
+        const uint32_t f = nets[k].first;
+        out[k] = off_exc[f];
+        out[K + k] = off_inh[f];
     }
 }
 
@@ -477,11 +522,52 @@ void run_search(Ctx& c, uint32_t step) {
         k_search_fill<<<blocks_for(n, 256), 256, 0, st>>>(n, c.tree.morton.p, c.nr.enabled.p, c.nr.signal.p, c.nr.search_vacant.p, cnt_exc, cnt_inh,
                                                           num_exc, S.src.p, S.jj.p);
         RL_LAUNCH_CHECK();
-        if (c.tree.root_is_leaf) {
-            // one neuron: its only candidate is itself (find_target_neuron returns nothing)
-            RL_CUDA_TRY(cudaMemsetAsync(S.target.p, 0xFF, m * sizeof(int32_t), st));
-        } else {
+        // segments: one per (type, network) with searches, so a warp never mixes networks
+        const uint32_t K = (uint32_t)c.nets.size();
+        S.seg_starts.ensure(2 * (size_t)K);
+        k_net_starts<<<blocks_for(K, 128), 128, 0, st>>>(K, c.d_nets.p, cnt_exc, cnt_inh, n, S.seg_starts.p);
+        RL_LAUNCH_CHECK();
+        std::vector<uint32_t> starts(2 * (size_t)K);
+        RL_CUDA_TRY(cudaMemcpyAsync(starts.data(), S.seg_starts.p, 2 * (size_t)K * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        RL_CUDA_TRY(cudaStreamSynchronize(st));
+        if (is_fp32(c)) {
+            pack_tree_f32(c);
+        }
+        for (int t = 0; t < 2; ++t) {
+            const uint64_t base = t == 0 ? 0 : num_exc;
+            const uint64_t total = t == 0 ? num_exc : num_inh;
+            std::vector<uint32_t> warp{ 0u }, net;
+            std::vector<uint64_t> begin, endv;
+            for (uint32_t k = 0; k < K; ++k) {
+                const uint64_t b = starts[(size_t)t * K + k];
+                const uint64_t e = k + 1 < K ? starts[(size_t)t * K + k + 1] : total;
+                if (e > b) {
+                    begin.push_back(base + b);
+                    endv.push_back(base + e);
+                    net.push_back(k);
+                    warp.push_back(warp.back() + (uint32_t)((e - b + 31) / 32));
+                }
+            }
+            if (net.empty()) {
+                continue;
+            }
+            const uint32_t segs = (uint32_t)net.size();
+            S.seg_warp[t].ensure(segs + 1);
+            S.seg_begin[t].ensure(segs);
+            S.seg_end[t].ensure(segs);
+            S.seg_net[t].ensure(segs);
+            RL_CUDA_TRY(cudaMemcpyAsync(S.seg_warp[t].p, warp.data(), (segs + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            RL_CUDA_TRY(cudaMemcpyAsync(S.seg_begin[t].p, begin.data(), segs * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            RL_CUDA_TRY(cudaMemcpyAsync(S.seg_end[t].p, endv.data(), segs * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+            RL_CUDA_TRY(cudaMemcpyAsync(S.seg_net[t].p, net.data(), segs * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            const uint32_t warps = warp.back();
+            const unsigned blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
+            if (is_fp32(c)) {
+                launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, segs, warps, step);
+                continue;
+            }
             SearchArgs A;
+            A.rec = c.tree.rec[t].p;
             A.topo = c.tree.topo.p;
             A.maxdim = c.tree.maxdim.p;
             A.px = c.nr.px.p;
@@ -489,34 +575,20 @@ void run_search(Ctx& c, uint32_t step) {
             A.pz = c.nr.pz.p;
             A.list_src = S.src.p;
             A.list_j = S.jj.p;
+            A.seg_warp = S.seg_warp[t].p;
+            A.seg_begin = S.seg_begin[t].p;
+            A.seg_end = S.seg_end[t].p;
+            A.seg_net = S.seg_net[t].p;
+            A.num_segs = segs;
+            A.nets = c.d_nets.p;
             A.target = S.target.p;
-            A.theta = c.cfg.theta;
             A.mu = c.cfg.mu;
-            A.scale = -1.0 / (c.cfg.sigma * c.cfg.sigma);
-            A.seed = c.cfg.seed;
             A.step = step;
             A.err = c.err.p;
             A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
-            if (is_fp32(c)) {
-                pack_tree_f32(c);
-            }
-            for (int t = 0; t < 2; ++t) {
-                A.rec = c.tree.rec[t].p;
-                A.begin = t == 0 ? 0 : num_exc;
-                A.end = t == 0 ? num_exc : m;
-                if (A.end <= A.begin) {
-                    continue;
-                }
-                if (is_fp32(c)) {
-                    launch_search_f32(c, t, A.begin, A.end, step);
-                    continue;
-                }
-                const uint64_t warps = (A.end - A.begin + 31) / 32;
-                const unsigned blocks = (unsigned)((warps + kWarpsPerBlock - 1) / kWarpsPerBlock);
-                PhaseScope ps(c, PH_SEARCH_KERNEL);
-                k_search<<<blocks, kWarpsPerBlock * 32, 0, st>>>(A);
-                RL_LAUNCH_CHECK();
-            }
+            PhaseScope ps(c, PH_SEARCH_KERNEL);
+            k_search<<<blocks, kWarpsPerBlock * 32, 0, st>>>(A);
+            RL_LAUNCH_CHECK();
         }
         k_first_fail<<<blocks_for(m, 256), 256, 0, st>>>(m, S.src.p, S.jj.p, S.target.p, S.first_fail.p);
         RL_LAUNCH_CHECK();

@@ -128,7 +128,64 @@ void validate(const rl_config& k) {
     }
 }
 
-void create(Ctx& c, const rl_config& k) {
+// The network table: one network from the config, or the ensemble's list.
+void setup_nets(Ctx& c, const rl_network* nets, uint32_t num) {
+    c.nets.clear();
+    uint32_t first = 0;
+    for (uint32_t k = 0; k < (nets ? num : 1u); ++k) {
+        NetInfo N{};
+        if (nets) {
+            const rl_network& r = nets[k];
+            RL_CHECK(r.num_neurons > 0, RL_ERR_INVALID, "every network needs at least one neuron");
+            RL_CHECK(r.theta > 0.0 && r.theta <= 0.5, RL_ERR_INVALID, "theta must lie in (0, 0.5] (Constants::bh_max_theta)");
+            RL_CHECK(r.sigma > 0.0, RL_ERR_INVALID, "sigma must be positive");
+            N.seed = r.seed;
+            N.count = r.num_neurons;
+            N.theta = r.theta;
+            N.sigma = r.sigma;
+            for (int a = 0; a < 3; ++a) {
+                RL_CHECK(r.box_min[a] <= r.box_max[a], RL_ERR_INVALID, "box_min must not exceed box_max");
+                N.box_min[a] = r.box_min[a];
+                N.box_max[a] = r.box_max[a];
+                N.nu[a] = r.growth_rate[a];
+            }
+        } else {
+            const rl_config& cf = c.cfg;
+            N.seed = cf.seed;
+            N.count = cf.num_neurons;
+            N.theta = cf.theta;
+            N.sigma = cf.sigma;
+            for (int a = 0; a < 3; ++a) {
+                N.box_min[a] = cf.box_min[a];
+                N.box_max[a] = cf.box_max[a];
+                N.nu[a] = cf.growth_rate[a];
+            }
+        }
+        N.first = first;
+        first += N.count;
+        N.scale = -1.0 / (N.sigma * N.sigma);
+        N.theta32 = (float)N.theta;
+        N.inv_sigma2_32 = (float)(1.0 / (N.sigma * N.sigma));
+        for (int a = 0; a < 3; ++a) {
+            N.nu32[a] = (float)N.nu[a];
+        }
+        N.root_leaf = 0;
+        c.nets.push_back(N);
+    }
+    RL_CHECK(first == c.n, RL_ERR_INVALID, "network sizes do not add up to num_neurons");
+    RL_CHECK(c.nets.size() <= 65535, RL_ERR_UNSUPPORTED, "at most 65535 networks per context");
+    c.d_nets.alloc(c.nets.size());
+    RL_CUDA_TRY(cudaMemcpyAsync(c.d_nets.p, c.nets.data(), c.nets.size() * sizeof(NetInfo), cudaMemcpyHostToDevice, c.stream));
+    std::vector<uint16_t> net_of(c.n);
+    for (size_t k = 0; k < c.nets.size(); ++k) {
+        std::fill(net_of.begin() + c.nets[k].first, net_of.begin() + c.nets[k].first + c.nets[k].count, (uint16_t)k);
+    }
+    c.net_of.alloc(c.n);
+    RL_CUDA_TRY(cudaMemcpyAsync(c.net_of.p, net_of.data(), c.n * sizeof(uint16_t), cudaMemcpyHostToDevice, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+}
+
+void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32_t num_nets = 0) {
     validate(k);
     c.cfg = k;
     c.n = k.num_neurons;
@@ -184,6 +241,7 @@ void create(Ctx& c, const rl_config& k) {
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
+    setup_nets(c, nets, num_nets);
     if (is_fp32(c)) {
         alloc_fp32(c);
     }
@@ -329,6 +387,40 @@ rl_status rl_ctx_create(const rl_config* cfg, void** out) {
         rl::create(*c, *cfg);
     } catch (const rl::Error& e) {
         std::fprintf(stderr, "rl_ctx_create: %s\n", e.message.c_str());
+        delete c;
+        return e.status;
+    }
+    *out = c;
+    return RL_OK;
+}
+
+rl_status rl_ensemble_create(const rl_config* base, const rl_network* networks, uint32_t num_networks, void** out) {
+    if (!base || !networks || !out || num_networks == 0) {
+        return RL_ERR_INVALID;
+    }
+    *out = nullptr;
+    rl_config cfg = *base;
+    uint64_t total = 0;
+    for (uint32_t k = 0; k < num_networks; ++k) {
+        total += networks[k].num_neurons;
+    }
+    if (total == 0 || total >= (1ull << 30)) {
+        return RL_ERR_INVALID;
+    }
+    cfg.num_neurons = (uint32_t)total;
+    // the base box and theta only need to pass validation; each network brings its own
+    for (int a = 0; a < 3; ++a) {
+        cfg.box_min[a] = 0.0;
+        cfg.box_max[a] = 1.0;
+    }
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) {
+        return RL_ERR_OOM;
+    }
+    try {
+        rl::create(*c, cfg, networks, num_networks);
+    } catch (const rl::Error& e) {
+        std::fprintf(stderr, "rl_ensemble_create: %s\n", e.message.c_str());
         delete c;
         return e.status;
     }

@@ -20,13 +20,14 @@ namespace rl {
 namespace {
 
 __global__ void k_conn_keys(uint64_t m, uint32_t n, const uint32_t* __restrict__ tgt, const uint32_t* __restrict__ src, const uint32_t* __restrict__ jj,
-                            const uint32_t* __restrict__ sig, uint64_t seed, uint32_t step, uint64_t* __restrict__ key, uint32_t* __restrict__ idx,
-                            uint32_t* __restrict__ gkey) {
+                            const uint32_t* __restrict__ sig, const NetInfo* __restrict__ nets, const uint16_t* __restrict__ net_of, uint32_t step,
+                            uint64_t* __restrict__ key, uint32_t* __restrict__ idx, uint32_t* __restrict__ gkey) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) {
         return;
     }
-    const u32x4 w = draw(seed, step, src[i], jj[i], STREAM_CONNECTOR, 0u);
+    const NetInfo& N = nets[net_of[src[i]]];
+    const u32x4 w = draw(N.seed, step, src[i] - N.first, jj[i], STREAM_CONNECTOR, 0u);
     key[i] = bits64(w);
     idx[i] = (uint32_t)i;
     // autapses go to a group past all real ones and are rejected there
@@ -168,7 +169,8 @@ struct DeleteArgs {
     uint32_t n;
     int type;  // 0 axon, 1 excitatory dendrite, 2 inhibitory dendrite
     uint32_t step;
-    uint64_t seed;
+    const NetInfo* nets;
+    const uint16_t* net_of;
     const uint32_t* to_delete;
     const uint8_t* signal;
     const uint8_t* enabled;
@@ -221,11 +223,12 @@ __global__ void k_delete(DeleteArgs A) {
         return;
     }
     uint32_t chosen[kMaxDeletePerNeuron];
+    const NetInfo& N = A.nets[A.net_of[i]];
     for (uint32_t k = 0; k < d; ++k) {
         uint32_t idx = 0;
         bool ok = false;
         for (uint32_t attempt = 0; attempt < (1u << 20) && !ok; ++attempt) {
-            const u32x4 w = draw(A.seed, A.step, i, ((uint32_t)A.type << 24) | k, STREAM_DELETION, attempt);
+            const u32x4 w = draw(N.seed, A.step, i - N.first, ((uint32_t)A.type << 24) | k, STREAM_DELETION, attempt);
             idx = (uint32_t)__umul64hi(bits64(w), (uint64_t)total);
             ok = true;
             for (uint32_t q = 0; q < k; ++q) {
@@ -297,8 +300,8 @@ uint64_t run_connector(Ctx& c, uint32_t step) {
     S.accepted.ensure(m);
     S.rank.ensure(m);
     S.flags.ensure(2 * (size_t)n + 2);
-    k_conn_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, n, S.req_tgt.p, S.req_src.p, S.req_j.p, S.req_sig.p, c.cfg.seed, step, S.ckey.p, S.cidx.p,
-                                                    S.gkey.p);
+    k_conn_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, n, S.req_tgt.p, S.req_src.p, S.req_j.p, S.req_sig.p, c.d_nets.p, c.net_of.p, step, S.ckey.p,
+                                                    S.cidx.p, S.gkey.p);
     RL_LAUNCH_CHECK();
     radix_sort_u64(S.ckey.p, S.cidx.p, m, 64, c.prim, st);
     // group key in key order, then a stable sort on it
@@ -468,7 +471,8 @@ uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
     A.n = c.n;
     A.type = type;
     A.step = step;
-    A.seed = c.cfg.seed;
+    A.nets = c.d_nets.p;
+    A.net_of = c.net_of.p;
     A.to_delete = c.to_delete.p;
     A.signal = c.nr.signal.p;
     A.enabled = c.nr.enabled.p;

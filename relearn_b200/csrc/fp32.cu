@@ -45,7 +45,6 @@ __global__ void k_f2d(uint32_t n, const float* __restrict__ a, double* __restric
 // ----------------------------------------------------------- activity
 struct Act32 {
     uint32_t n, step;
-    uint64_t seed;
     const uint8_t* enabled;
     const uint32_t* csr_off;
     const uint32_t* csr_src;
@@ -61,10 +60,12 @@ struct Act32 {
     uint32_t h_model;
     float a, ab, c, d, v_spike, k1, k2, k3, scale_m;
     double ca_mul, ca_add;  // calcium: c <- c*ca_mul + fired*ca_add
-    float xi[3], inv_zeta[3], nu[3];
+    float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
     float eta[3];
     int has_edges;
+    const NetInfo* nets;
+    const uint16_t* net_of;
 };
 
 // AS241 in FP32 (Wichura 1988, PPND7 accuracy), own log via __logf.
@@ -154,7 +155,8 @@ __global__ void __launch_bounds__(256) k_activity_f32(Act32 A) {
         }
     }
     // the same Philox draw as the FP64 form, 24 bits of it
-    const u32x4 w = draw(A.seed, A.step, i, 0u, STREAM_NOISE, 0u);
+    const NetInfo& N = A.nets[A.net_of[i]];
+    const u32x4 w = draw(N.seed, A.step, i - N.first, 0u, STREAM_NOISE, 0u);
     const float p = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-8f;  // 2^-24
     const float input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_quantile_f32(p), A.noise_mean));
     A.input[i] = input;
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(256) k_activity_f32(Act32 A) {
             const float q = (caf - A.xi[t]) * A.inv_zeta[t];
             dz = fmaf(2.0f, __expf(-q * q), -1.0f);
         }
-        A.delta[t][i] = fmaf(dz, A.nu[t], A.delta[t][i]);
+        A.delta[t][i] = fmaf(dz, N.nu32[t], A.delta[t][i]);
     }
 }
 
@@ -261,12 +263,25 @@ struct Search32 {
     const double *px, *py, *pz;
     const uint32_t* list_src;
     const uint32_t* list_j;
-    uint64_t begin, end;
+    const uint32_t* seg_warp;
+    const uint64_t* seg_begin;
+    const uint64_t* seg_end;
+    const uint32_t* seg_net;
+    uint32_t num_segs;
+    const NetInfo* nets;
     int32_t* target;
-    float theta, mu, inv_sigma2;
-    uint64_t seed;
+    float mu;
     uint32_t step;
     uint32_t* err;
+};
+
+// Parameters of the network a warp searches in.
+struct Net32 {
+    float theta;
+    float inv_sigma2;
+    uint64_t seed;
+    uint32_t root;
+    uint32_t first;
 };
 
 struct KSum {
@@ -284,7 +299,8 @@ struct E32 {
     float w;
 };
 
-__device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float sx, float sy, float sz, uint32_t source, const Search32& A, bool fb) {
+__device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float sx, float sy, float sz, uint32_t source, const Search32& A, const Net32& W,
+                                      bool fb) {
     E32 e{ S_DISCARD, 0.0f };
     const uint32_t cnt = __float_as_uint(r.w);
     if (cnt == 0) {
@@ -296,7 +312,7 @@ __device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float 
         return e;
     }
     const bool leaf = topo_leaf(t.y);
-    if (!leaf && !(md < A.theta * d)) {
+    if (!leaf && !(md < W.theta * d)) {
         e.status = S_EXPAND;
         return e;
     }
@@ -305,7 +321,7 @@ __device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float 
         e.w = 0.0f;
     } else if (!fb) {
         const float dm = d - A.mu;
-        e.w = __expf(-(dm * dm) * A.inv_sigma2) * (float)cnt;
+        e.w = __expf(-(dm * dm) * W.inv_sigma2) * (float)cnt;
     } else {
         e.w = __fdividef((float)cnt, d);
     }
@@ -316,8 +332,8 @@ __device__ __forceinline__ uint32_t child_of(uint2 t, int oct) {
     return t.x + (uint32_t)__popc(topo_mask(t.y) & ((1u << oct) - 1u));
 }
 
-__device__ __forceinline__ float threshold32(float total, const Search32& A, uint32_t source, uint32_t j, uint32_t depth) {
-    const u32x4 w = draw(A.seed, A.step, source, j, STREAM_BH_PICK, depth);
+__device__ __forceinline__ float threshold32(float total, const Search32& A, const Net32& W, uint32_t source, uint32_t j, uint32_t depth) {
+    const u32x4 w = draw(W.seed, A.step, source - W.first, j, STREAM_BH_PICK, depth);
     float r = (float)(w.x >> 8) * 5.9604644775390625e-8f * total;  // [0, total)
     return r > 0.0f ? r : 1.0e-38f;
 }
@@ -328,13 +344,13 @@ struct Walk32 {
     bool overflow;
 };
 
-__device__ Walk32 lane_walk32(const Search32& A, uint32_t sub, bool include_root, KSum start, bool pick, float r, float sx, float sy, float sz,
-                              uint32_t source, bool fb) {
+__device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, float sx, float sy,
+                              float sz, uint32_t source, bool fb) {
     Walk32 res{ start, -1, false };
     uint32_t fnode[kStack];
     uint32_t frem[kStack];
     if (include_root) {
-        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sx, sy, sz, source, A, fb);
+        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sx, sy, sz, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -360,7 +376,7 @@ __device__ Walk32 lane_walk32(const Search32& A, uint32_t sub, bool include_root
         frem[top] = rem & ~(1u << oct);
         const uint32_t child = child_of(A.topo[fnode[top]], oct);
         const uint2 tt = A.topo[child];
-        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sx, sy, sz, source, A, fb);
+        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sx, sy, sz, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -380,14 +396,14 @@ __device__ Walk32 lane_walk32(const Search32& A, uint32_t sub, bool include_root
     return res;
 }
 
-__device__ KSum packet32(const Search32& A, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb, float2* cp, uint32_t* s_node,
-                         uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
+__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb, float2* cp,
+                         uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     KSum sum{ 0.0f, 0.0f };
     if (lane == 0) {
-        s_node[0] = 0;
-        s_rem[0] = topo_mask(A.topo[0].y);
+        s_node[0] = W.root;
+        s_rem[0] = topo_mask(A.topo[W.root].y);
         s_act[0] = lanes;
     }
     __syncwarp();
@@ -415,7 +431,7 @@ __device__ KSum packet32(const Search32& A, uint32_t lanes, float sx, float sy, 
         const float md = A.maxdim[child];
         int status = S_DISCARD;
         if ((act >> lane) & 1u) {
-            const E32 e = eval32(rr, tt, md, sx, sy, sz, source, A, fb);
+            const E32 e = eval32(rr, tt, md, sx, sy, sz, source, A, W, fb);
             status = e.status;
             if (e.status == S_ACCEPT) {
                 sum.add(e.w);
@@ -448,12 +464,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
     __shared__ float2 s_cp[kWarps][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const uint64_t warp_global = (uint64_t)blockIdx.x * kWarps + wib;
-    if (A.begin + warp_global * 32 >= A.end) {
+    const uint32_t warp_global = blockIdx.x * kWarps + wib;
+    if (warp_global >= A.seg_warp[A.num_segs]) {
         return;
     }
-    const uint64_t idx = A.begin + warp_global * 32 + lane;
-    const bool active = idx < A.end;
+    uint32_t lo = 0, hi = A.num_segs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A.seg_warp[mid] <= warp_global) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    const NetInfo& N = A.nets[A.seg_net[lo]];
+    const Net32 W{ N.theta32, N.inv_sigma2_32, N.seed, A.seg_net[lo], N.first };
+    const uint64_t idx = A.seg_begin[lo] + (uint64_t)(warp_global - A.seg_warp[lo]) * 32 + lane;
+    const bool active = idx < A.seg_end[lo];
+    if (N.root_leaf) {
+        if (active) {
+            A.target[idx] = -1;
+        }
+        return;
+    }
     const uint32_t source = active ? A.list_src[idx] : 0u;
     const uint32_t j = active ? A.list_j[idx] : 0u;
     const float sx = active ? (float)A.px[source] : 0.0f;
@@ -462,11 +495,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
     float2* cp = &s_cp[wib][lane];
     bool overflow = false;
     const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
-    KSum total = packet32(A, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
+    KSum total = packet32(A, W, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
     bool fb = false;
     const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total.s == 0.0f);
     if (need_fb) {
-        const KSum t2 = packet32(A, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
+        const KSum t2 = packet32(A, W, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
         if ((need_fb >> lane) & 1u) {
             total = t2;
             fb = true;
@@ -476,8 +509,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
     bool done = !active || total.s == 0.0f;
     uint32_t sub = 0;
     if (!done) {
-        const float r = threshold32(total.s, A, source, j, 0);
-        const uint2 root = A.topo[0];
+        const float r = threshold32(total.s, A, W, source, j, 0);
+        const uint2 root = A.topo[W.root];
         const uint32_t mask = topo_mask(root.y);
         int cstar = -1;
         for (int oct = 7; oct >= 0; --oct) {
@@ -493,7 +526,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
             done = true;
         } else {
             const float2 c0 = cp[cstar * 32];
-            const Walk32 wr = lane_walk32(A, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
+            const Walk32 wr = lane_walk32(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
             overflow |= wr.overflow;
             if (wr.picked < 0) {
                 done = true;  // rounding left the crossing past the last candidate: no pick
@@ -512,18 +545,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
             result = (int32_t)st.x;
             break;
         }
-        Walk32 s1 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
+        Walk32 s1 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
         bool f = false;
         if (s1.sum.s == 0.0f) {
-            s1 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
+            s1 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
             f = true;
         }
         overflow |= s1.overflow;
         if (s1.sum.s == 0.0f) {
             break;
         }
-        const float r = threshold32(s1.sum.s, A, source, j, depth);
-        const Walk32 s2 = lane_walk32(A, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
+        const float r = threshold32(s1.sum.s, A, W, source, j, depth);
+        const Walk32 s2 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
         if (s2.picked < 0) {
             break;
         }
@@ -540,13 +573,13 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
 
 // ----------------------------------------------------------- diagnostic
 __global__ void k_candidates(const double4* rec64, const float4* rec32, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
-                             double sz, uint32_t source, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
+                             double sz, uint32_t source, uint32_t root, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
                              uint64_t capacity, unsigned long long* count, uint32_t* err) {
     uint32_t fnode[kStack];
     uint32_t frem[kStack];
     int depth = 1;
-    fnode[0] = 0;
-    frem[0] = topo_mask(topo[0].y);
+    fnode[0] = root;
+    frem[0] = topo_mask(topo[root].y);
     uint64_t k = 0;
     const double scale = -1.0 / (sigma * sigma);
     const float inv_s2 = (float)(1.0 / (sigma * sigma));
@@ -662,7 +695,6 @@ void run_activity_step_f32(Ctx& c, uint32_t step) {
     Act32 A;
     A.n = c.n;
     A.step = step;
-    A.seed = k.seed;
     A.enabled = c.nr.enabled.p;
     A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
     A.csr_off = c.graph.offsets.p;
@@ -708,8 +740,9 @@ void run_activity_step_f32(Ctx& c, uint32_t step) {
         A.eta[t] = (float)eta;
         A.xi[t] = (float)((eta + eps) * 0.5);
         A.inv_zeta[t] = A.flat[t] ? 0.0f : (float)(1.0 / ((eta - eps) * factor_inv));
-        A.nu[t] = (float)k.growth_rate[t];
     }
+    A.nets = c.d_nets.p;
+    A.net_of = c.net_of.p;
     {
         PhaseScope ps(c, PH_ACTIVITY_KERNEL);
         k_activity_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
@@ -742,7 +775,8 @@ void pack_tree_f32(Ctx& c) {
     RL_LAUNCH_CHECK();
 }
 
-void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t step) {
+void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
+                       uint32_t num_segs, uint32_t warps, uint32_t step) {
     Search32 A;
     A.rec = c.tree.rec32[type].p;
     A.topo = c.tree.topo.p;
@@ -752,17 +786,17 @@ void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t 
     A.pz = c.nr.pz.p;
     A.list_src = c.search.src.p;
     A.list_j = c.search.jj.p;
-    A.begin = begin;
-    A.end = end;
+    A.seg_warp = seg_warp;
+    A.seg_begin = seg_begin;
+    A.seg_end = seg_end;
+    A.seg_net = seg_net;
+    A.num_segs = num_segs;
+    A.nets = c.d_nets.p;
     A.target = c.search.target.p;
-    A.theta = (float)c.cfg.theta;
     A.mu = (float)c.cfg.mu;
-    A.inv_sigma2 = (float)(1.0 / (c.cfg.sigma * c.cfg.sigma));
-    A.seed = c.cfg.seed;
     A.step = step;
     A.err = c.err.p;
-    const uint64_t warps = (end - begin + 31) / 32;
-    const unsigned blocks = (unsigned)((warps + kWarps - 1) / kWarps);
+    const unsigned blocks = (warps + kWarps - 1) / kWarps;
     PhaseScope ps(c, PH_SEARCH_KERNEL);
     k_search_f32<<<blocks, kWarps * 32, 0, c.stream>>>(A);
     RL_LAUNCH_CHECK();
@@ -770,7 +804,10 @@ void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t 
 
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w) {
     RL_CHECK(source < c.n, RL_ERR_INVALID, "source out of range");
-    RL_CHECK(!c.tree.root_is_leaf, RL_ERR_INVALID, "the octree has a single neuron");
+    uint16_t net = 0;
+    RL_CUDA_TRY(cudaMemcpy(&net, c.net_of.p + source, sizeof(net), cudaMemcpyDeviceToHost));
+    const NetInfo& N = c.nets[net];
+    RL_CHECK(!N.root_leaf, RL_ERR_INVALID, "the network has a single neuron");
     if (precision == RL_PRECISION_FP32) {
         pack_tree_f32(c);
     }
@@ -789,8 +826,8 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
     dw.alloc(cap);
     dc.alloc(1);
     k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.rec32[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
-                                        precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, precision,
-                                        c.cfg.theta, c.cfg.mu, c.cfg.sigma, dn.p, dw.p, cap, dc.p, c.err.p);
+                                        precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, net, precision,
+                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p);
     RL_LAUNCH_CHECK();
     unsigned long long k = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&k, dc.p, sizeof(k), cudaMemcpyDeviceToHost, c.stream));

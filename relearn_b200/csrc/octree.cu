@@ -37,13 +37,17 @@ __device__ __forceinline__ int octant_step(double p, double& lo, double& hi) {
     return 1;
 }
 
-__global__ void k_keys(uint32_t n, const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz, double3 bmin,
-                       double3 bmax, uint64_t* __restrict__ key0, uint64_t* __restrict__ key1, uint32_t* __restrict__ idx, uint32_t* err) {
+__global__ void k_keys(uint32_t n, const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+                       const NetInfo* __restrict__ nets, const uint16_t* __restrict__ net_of, uint64_t* __restrict__ key0, uint64_t* __restrict__ key1,
+                       uint32_t* __restrict__ idx, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
     }
     const double x = px[i], y = py[i], z = pz[i];
+    const NetInfo& N = nets[net_of[i]];
+    const double3 bmin = make_double3(N.box_min[0], N.box_min[1], N.box_min[2]);
+    const double3 bmax = make_double3(N.box_max[0], N.box_max[1], N.box_max[2]);
     idx[i] = i;
     if (!(bmin.x <= x && x <= bmax.x && bmin.y <= y && y <= bmax.y && bmin.z <= z && z <= bmax.z)) {
         atomicOr(err, (uint32_t)DERR_OUT_OF_BOX);
@@ -71,16 +75,18 @@ __global__ void k_keys(uint32_t n, const double* __restrict__ px, const double* 
 
 // Neurons whose first words agree are ordered by the second word (runs are
 // tiny: the cell of a 21-level prefix is 2^-21 of the box).
-__global__ void k_fix_runs(uint32_t n, uint64_t* __restrict__ k0s, uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1, uint32_t* err) {
+__global__ void k_fix_runs(uint32_t n, uint64_t* __restrict__ k0s, uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1,
+                           const uint16_t* __restrict__ net_of, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) {
         return;
     }
-    if (k0s[i] != k0s[i + 1] || (i > 0 && k0s[i - 1] == k0s[i])) {
+    auto same = [&](uint32_t a, uint32_t b) { return k0s[a] == k0s[b] && net_of[idx[a]] == net_of[idx[b]]; };
+    if (!same(i, i + 1) || (i > 0 && same(i - 1, i))) {
         return;
     }
     uint32_t end = i + 1;
-    while (end + 1 < n && k0s[end + 1] == k0s[i]) {
+    while (end + 1 < n && same(end + 1, i)) {
         ++end;
     }
     for (uint32_t a = i + 1; a <= end; ++a) {
@@ -114,9 +120,13 @@ __device__ __forceinline__ int common_levels(uint64_t a0, uint64_t a1, uint64_t 
 
 // lcp[i] = common levels of sorted neighbours i and i+1, for i < n-1.
 __global__ void k_lcp(uint32_t n, const uint64_t* __restrict__ k0s, const uint32_t* __restrict__ idx, const uint64_t* __restrict__ key1,
-                      int32_t* __restrict__ lcp, uint32_t* err) {
+                      const uint16_t* __restrict__ net_of, int32_t* __restrict__ lcp, uint32_t* err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n) {
+        return;
+    }
+    if (net_of[idx[i]] != net_of[idx[i + 1]]) {
+        lcp[i] = -1;  // different networks share no node
         return;
     }
     const int c = common_levels(k0s[i], key1[idx[i]], k0s[i + 1], key1[idx[i + 1]]);
@@ -177,6 +187,24 @@ __device__ __forceinline__ int digit_at(uint64_t k0, uint64_t k1, int level) {
     return (int)((k1 >> (3 * (2 * kLevelsPerWord - level))) & 7u);
 }
 
+__global__ void k_net_keys(uint32_t n, const uint32_t* __restrict__ idx, const uint16_t* __restrict__ net_of, uint32_t* __restrict__ netk,
+                           uint32_t* __restrict__ perm) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        netk[i] = net_of[idx[i]];
+        perm[i] = i;
+    }
+}
+
+__global__ void k_permute_keys(uint32_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ k0s, const uint32_t* __restrict__ idx,
+                               uint64_t* __restrict__ k0o, uint32_t* __restrict__ idxo) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        k0o[i] = k0s[perm[i]];
+        idxo[i] = idx[perm[i]];
+    }
+}
+
 struct FillArgs {
     uint32_t n, m;
     const uint32_t* skey;
@@ -187,7 +215,8 @@ struct FillArgs {
     const uint64_t* key1;
     const uint32_t* idx;
     const double *px, *py, *pz;
-    double3 bmin, bmax;
+    const NetInfo* nets;
+    const uint16_t* net_of;
     double4* rec0;
     double4* rec1;
     uint2* topo;
@@ -216,8 +245,9 @@ __global__ void k_fill(FillArgs A) {
     const uint32_t neuron = A.idx[i];
     const uint64_t k0 = A.k0s[i];
     const uint64_t k1 = A.key1[neuron];
+    const NetInfo& N = A.nets[A.net_of[neuron]];
     // cell box: descend l levels along the digits of the first neuron
-    double lx = A.bmin.x, hx = A.bmax.x, ly = A.bmin.y, hy = A.bmax.y, lz = A.bmin.z, hz = A.bmax.z;
+    double lx = N.box_min[0], hx = N.box_max[0], ly = N.box_min[1], hy = N.box_max[1], lz = N.box_min[2], hz = N.box_max[2];
     for (int lev = 1; lev <= (int)l; ++lev) {
         const int d = digit_at(k0, k1, lev);
         const double mx = (lx + hx) / 2.0, my = (ly + hy) / 2.0, mz = (lz + hz) / 2.0;
@@ -424,21 +454,39 @@ void build_octree(Ctx& c, const double* h_xyz) {
     key0.alloc(n);
     key1.alloc(n);
     idx.alloc(n);
-    const double3 bmin = make_double3(c.cfg.box_min[0], c.cfg.box_min[1], c.cfg.box_min[2]);
-    const double3 bmax = make_double3(c.cfg.box_max[0], c.cfg.box_max[1], c.cfg.box_max[2]);
-    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, c.nr.px.p, c.nr.py.p, c.nr.pz.p, bmin, bmax, key0.p, key1.p, idx.p, c.err.p);
+    k_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, c.nr.px.p, c.nr.py.p, c.nr.pz.p, c.d_nets.p, c.net_of.p, key0.p, key1.p, idx.p, c.err.p);
     RL_LAUNCH_CHECK();
     check_device_error(c, "octree keys");
-    // sort on the first word (63 bits), then order ties by the second word
+    // sort on the first word (63 bits), then stably by network; order ties by the second word
     DBuf<uint64_t> k0s;
     k0s.alloc(n);
     RL_CUDA_TRY(cudaMemcpyAsync(k0s.p, key0.p, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
     radix_sort_u64(k0s.p, idx.p, n, 63, c.prim, st);
-    k_fix_runs<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, c.err.p);
+    if (c.multi()) {
+        DBuf<uint32_t> netk, perm, idx2;
+        DBuf<uint64_t> k02;
+        netk.alloc(n);
+        perm.alloc(n);
+        idx2.alloc(n);
+        k02.alloc(n);
+        k_net_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, idx.p, c.net_of.p, netk.p, perm.p);
+        RL_LAUNCH_CHECK();
+        int nb = 1;
+        while (nb < 16 && ((uint64_t)1 << nb) < c.nets.size()) {
+            ++nb;
+        }
+        radix_sort_u32(netk.p, perm.p, n, nb, c.prim, st);
+        k_permute_keys<<<blocks_for(n, 256), 256, 0, st>>>(n, perm.p, k0s.p, idx.p, k02.p, idx2.p);
+        RL_LAUNCH_CHECK();
+        RL_CUDA_TRY(cudaMemcpyAsync(k0s.p, k02.p, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+        RL_CUDA_TRY(cudaMemcpyAsync(idx.p, idx2.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        RL_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    k_fix_runs<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, c.net_of.p, c.err.p);
     RL_LAUNCH_CHECK();
     DBuf<int32_t> lcp;
     lcp.alloc(n);
-    k_lcp<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, lcp.p, c.err.p);
+    k_lcp<<<blocks_for(n, 256), 256, 0, st>>>(n, k0s.p, idx.p, key1.p, c.net_of.p, lcp.p, c.err.p);
     RL_LAUNCH_CHECK();
     check_device_error(c, "octree keys");
 
@@ -503,8 +551,8 @@ void build_octree(Ctx& c, const double* h_xyz) {
     A.px = c.nr.px.p;
     A.py = c.nr.py.p;
     A.pz = c.nr.pz.p;
-    A.bmin = bmin;
-    A.bmax = bmax;
+    A.nets = c.d_nets.p;
+    A.net_of = c.net_of.p;
     A.rec0 = T.rec[0].p;
     A.rec1 = T.rec[1].p;
     A.topo = T.topo.p;
@@ -535,11 +583,19 @@ void build_octree(Ctx& c, const double* h_xyz) {
     RL_LAUNCH_CHECK();
     k_child_mask<<<blocks_for(m, 256), 256, 0, st>>>(m, T.parent.p, T.first_key.p, k0s.p, idx.p, key1.p, T.topo.p);
     RL_LAUNCH_CHECK();
-    uint2 root;
-    RL_CUDA_TRY(cudaMemcpyAsync(&root, T.topo.p, sizeof(uint2), cudaMemcpyDeviceToHost, st));
+    // the roots: level 0 holds one node per network, in network order
+    const size_t K = c.nets.size();
+    RL_CHECK(hcount[0] == K, RL_ERR_INVALID, "every network needs at least one neuron");
+    std::vector<uint2> roots(K);
+    RL_CUDA_TRY(cudaMemcpyAsync(roots.data(), T.topo.p, K * sizeof(uint2), cudaMemcpyDeviceToHost, st));
     RL_CUDA_TRY(cudaStreamSynchronize(st));
-    T.root_is_leaf = topo_leaf(root.y);
-    T.root_neuron = root.x;
+    for (size_t k = 0; k < K; ++k) {
+        c.nets[k].root_leaf = topo_leaf(roots[k].y) ? 1u : 0u;
+    }
+    RL_CUDA_TRY(cudaMemcpyAsync(c.d_nets.p, c.nets.data(), K * sizeof(NetInfo), cudaMemcpyHostToDevice, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    T.root_is_leaf = K == 1 && topo_leaf(roots[0].y);
+    T.root_neuron = roots[0].x;
     check_device_error(c, "octree build");
 }
 

@@ -83,6 +83,9 @@ struct Search {
     DBuf<uint32_t> req_count;    // per neuron: valid requests
     DBuf<uint32_t> req_off;      // per neuron: output offset
     DBuf<uint32_t> req_tgt, req_src, req_j, req_sig;  // requests in (source, j) order
+    DBuf<uint32_t> seg_starts;
+    DBuf<uint32_t> seg_warp[2], seg_net[2];
+    DBuf<uint64_t> seg_begin[2], seg_end[2];
     uint64_t num_searches = 0;
     uint64_t num_exc = 0;
     uint64_t num_requests = 0;
@@ -115,6 +118,27 @@ struct PhaseTimer {
     uint64_t count[PH_COUNT] = {};
 };
 
+// One network of a context.  A context holds one or more networks in one set
+// of arrays: network k owns neurons [first, first + count); the octree is a
+// forest whose root of network k is node k; every random draw of a neuron is
+// keyed on the network's seed and the neuron's index inside its network, so a
+// network evolves exactly as it would alone.
+struct NetInfo {
+    uint64_t seed;
+    uint32_t first;
+    uint32_t count;
+    double theta;
+    double scale;  // -1 / sigma^2
+    double sigma;
+    double nu[3];
+    double box_min[3];
+    double box_max[3];
+    float theta32;
+    float inv_sigma2_32;
+    float nu32[3];
+    uint32_t root_leaf;  // the network has a single neuron
+};
+
 struct Ctx;
 // Records an event pair around a scope when profiling is on.
 struct PhaseScope {
@@ -132,6 +156,10 @@ struct Ctx {
     cudaStream_t stream = nullptr;      // stream all work is issued on
     cudaStream_t own_stream = nullptr;  // the context's own stream
     PhaseTimer timer;
+    std::vector<NetInfo> nets;  // host copy
+    DBuf<NetInfo> d_nets;
+    DBuf<uint16_t> net_of;      // network of each neuron
+    bool multi() const { return nets.size() > 1; }
     std::string last_error;
     bool positions_set = false;
     Tree tree;
@@ -172,7 +200,8 @@ void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download
 void run_activity_step_f32(Ctx& c, uint32_t step);
 uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
-void launch_search_f32(Ctx& c, int type, uint64_t begin, uint64_t end, uint32_t step);
+void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
+                       uint32_t num_segs, uint32_t warps, uint32_t step);
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu
