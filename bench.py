@@ -203,7 +203,10 @@ def run_b200(args, world, rank, local):
     n, side = args.neurons, args.side
     params, pos, sig = build_network(n, side, args.seed + rank, args.placement)
     params["device"] = local
-    stream = torch.cuda.current_stream(dev)
+    # a stream of its own: the library captures the 100-step activity blocks as
+    # CUDA graphs, which the legacy default stream does not allow
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     main_prec = 1 if args.precision == "fp32" else 0
     clk = ClockSampler(local)
     m = measure_form(args, main_prec, dev, stream, world, pos, sig, params, clk)
@@ -241,6 +244,12 @@ def run_b200(args, world, rank, local):
                 other["bh_search"]["vs_fp64_drop_in"] = bh32["value"] / bh["value"]
         o["net"].close()
 
+    ens = None
+    if not args.skip_ensemble:
+        ens = ensemble_figure(args, dev, stream, world, rank)
+    prec = None
+    if rank == 0 and world == 1 and args.precision_report:
+        prec = precision_report(args, dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, params, pos, sig)
@@ -278,9 +287,149 @@ def run_b200(args, world, rank, local):
         line["bh_search"] = bh
     if other:
         line["fp32_form"] = other
+    if ens:
+        line["ensemble"] = ens
+    if prec:
+        line["precision_report"] = prec
     if cpu:
         line["cpu_baseline"] = cpu
     return line
+
+
+def ensemble_spec(count, seed):
+    """The batched configuration: `count` networks with sizes log-uniform in
+    5,000-250,000 neurons, growth rates log-uniform in 1e-5-1e-3, theta from
+    {0.2, 0.3, 0.5}, sigma from {500, 750, 1000} um, uniform placement at one
+    neuron per 1000 um^3."""
+    rng = np.random.default_rng(seed)
+    nets = []
+    for k in range(count):
+        n = int(np.exp(rng.uniform(np.log(5_000), np.log(250_000))))
+        nets.append(dict(num_neurons=n, seed=seed * 100_003 + k, side=(1000.0 * n) ** (1.0 / 3.0), theta=float(rng.choice([0.2, 0.3, 0.5])),
+                         sigma=float(rng.choice([500.0, 750.0, 1000.0])), growth_rate=float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-3))))))
+    return nets
+
+
+def ensemble_figure(args, dev, stream, world, rank, periods=None):
+    """128 networks in one FP32 context: one launch per activity step over all
+    networks, 100-step blocks replayed as CUDA graphs, plasticity updates over
+    all networks at once."""
+    import torch
+
+    import relearn_b200 as R
+    from relearn_b200 import workloads
+
+    nets = ensemble_spec(args.ensemble_networks, 7 + rank)
+    base = R.default_params(1, 1.0)
+    base["precision"] = 1
+    base["device"] = dev.index
+    total = sum(d["num_neurons"] for d in nets)
+    pos = np.concatenate([workloads.uniform_cube(d["num_neurons"], d["side"], 900 + k) for k, d in enumerate(nets)])
+    sig = np.concatenate([workloads.signal_types(d["num_neurons"], 900 + k) for k, d in enumerate(nets)])
+    ens = R.Network(base, networks=nets)
+    ens.set_stream(stream.cuda_stream)
+    ens.set_positions(pos, sig)
+    step = 1
+    for _ in range(args.warmup):
+        ens.simulate(step, PERIOD)
+        step += PERIOD
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    periods = periods or max(args.steps, 3)
+    ens.phase_times()
+    ens.set_profiling(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(periods):
+        ens.simulate(step, PERIOD)
+        step += PERIOD
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ph = ens.phase_times()
+    ens.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    act_ms, act_cnt = ph["activity_kernel"]
+    hbm, peak_kind = peaks()
+    bytes_per_launch = ACT_BYTES_FP32 * total
+    achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+    ens.close()
+    return {"metric": "neuron-steps/s", "value": world * total * PERIOD * periods / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),
+            "neurons": total, "periods": periods, "precision": "fp32", "launches_per_step": 1, "graphs": "100-step activity blocks",
+            "roofline": {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None},
+            "phases_ms": {k: v[0] for k, v in ph.items()}}
+
+
+def precision_report(args, dev, stream, n=4_000_000, side=16_000.0, steps=1000, sources=64):
+    """The precision form against the FP64 drop-in on the same seed: 4M neurons
+    uniform in a 16,000 um cube, 1,000 steps.  Reports selection-probability
+    error, calcium drift and the chi-square of the formed-synapse distance
+    histograms of one search per neuron on the same snapshot."""
+    import torch
+
+    import relearn_b200 as R
+
+    params, pos, sig = build_network(n, side, 11, "uniform")
+    params["device"] = dev.index
+    out = {"neurons": n, "side_um": side, "steps": steps}
+    nets = []
+    for prec in (0, 1):
+        p = dict(params)
+        p["precision"] = prec
+        net = R.Network(p)
+        net.set_stream(stream.cuda_stream)
+        net.set_positions(pos, sig)
+        net.simulate(1, steps)
+        nets.append(net)
+    ca64 = nets[0].neurons()["calcium"]
+    ca32 = nets[1].neurons()["calcium"]
+    rel = np.abs(ca32 - ca64) / np.maximum(np.abs(ca64), 1e-300)
+    fired_rate = [float(x.neurons()["fired"].mean()) for x in nets]
+    out["calcium_drift"] = {"max_rel": float(rel.max()), "mean_rel": float(rel.mean()), "mean_fp64": float(ca64.mean()), "mean_fp32": float(ca32.mean()),
+                            "mean_rel_of_means": float(abs(ca32.mean() - ca64.mean()) / ca64.mean())}
+    out["last_step_fired_fraction"] = fired_rate
+    # same snapshot in both forms: one vacant axon and dendrite of each type
+    one = np.ones(n, np.uint32)
+    for net in nets:
+        for t in range(3):
+            net.set_elements(t, np.full(n, 1.5), np.zeros(n), np.zeros(n, np.uint32), one)
+        net.prepare_update_connectivity(one, one, one)
+    rng = np.random.default_rng(5)
+    worst, tv = 0.0, 0.0
+    for src in rng.choice(n, sources, replace=False):
+        n64, w64 = nets[0].candidate_weights(int(src), 0)
+        n32, w32 = nets[1].candidate_weights(int(src), 1)
+        p64 = dict(zip(n64.tolist(), (w64 / w64.sum()).tolist()))
+        p32 = dict(zip(n32.tolist(), (w32 / w32.sum()).tolist()))
+        keys = set(p64) | set(p32)
+        tv = max(tv, 0.5 * sum(abs(p64.get(k, 0.0) - p32.get(k, 0.0)) for k in keys))
+        for k, v in p64.items():
+            if v >= 1e-6:
+                worst = max(worst, abs(p32.get(k, 0.0) - v) / v)
+    out["selection_probability"] = {"max_rel_err_p_ge_1e-6": worst, "max_total_variation": tv, "sources": sources, "descent": "first (from the root)"}
+    hist = []
+    edges = np.linspace(0.0, 3 * 750.0, 46)
+    for net in nets:
+        req = net.find_targets(100)
+        d = np.linalg.norm(pos[req["source"]] - pos[req["target"]], axis=1)
+        h, _ = np.histogram(d, bins=edges)
+        hist.append(h.astype(np.float64))
+    a, b = hist
+    m = (a + b) > 0
+    chi2 = float(np.sum((a[m] - b[m]) ** 2 / (a[m] + b[m])))
+    from scipy.stats import chi2 as chi2_dist
+
+    out["distance_histogram"] = {"bins": int(m.sum()), "chi2": chi2, "dof": int(m.sum()) - 1, "p_value": float(chi2_dist.sf(chi2, int(m.sum()) - 1)),
+                                 "synapses": [int(a.sum()), int(b.sum())], "bin_um": float(edges[1] - edges[0])}
+    for net in nets:
+        net.close()
+    return out
 
 
 def bh_snapshot(net, n, stream, step):
@@ -431,6 +580,9 @@ def main():
     ap.add_argument("--skip-bh", action="store_true")
     ap.add_argument("--skip-fp32", action="store_true", help="do not measure the FP32 form beside the FP64 drop-in")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="form of the headline figure")
+    ap.add_argument("--skip-ensemble", action="store_true", help="do not measure the batched form (128 networks)")
+    ap.add_argument("--ensemble-networks", type=int, default=128)
+    ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
     ap.add_argument("--case", choices=["activity", "search"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()

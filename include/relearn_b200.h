@@ -277,6 +277,11 @@ RL_API rl_status rl_prepare_update_connectivity_noalloc(void* ctx, const uint32_
 RL_API rl_status rl_candidate_weights(void* ctx, uint32_t source, int precision, uint32_t* nodes, double* weights, uint64_t capacity,
                                       uint64_t* count);
 
+/* Run each full plasticity interval of activity steps as one captured CUDA
+ * graph (1, the default) or as separate launches (0).  Graphs are used only on
+ * a stream other than the legacy default stream. */
+RL_API rl_status rl_set_graphs(void* ctx, int enable);
+
 /* Turn per-phase CUDA-event timing on (1) or off (0). */
 RL_API rl_status rl_set_profiling(void* ctx, int enable);
 

@@ -112,7 +112,7 @@ ABI_FUNCTIONS = [
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
-    "rl_candidate_weights",
+    "rl_candidate_weights", "rl_set_graphs",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -186,6 +186,8 @@ def load_library(path: str = LIB_PATH):
     L.rl_set_profiling.argtypes = [vp, C.c_int]
     L.rl_get_phase_times.restype = st
     L.rl_get_phase_times.argtypes = [vp, vp, vp]
+    L.rl_set_graphs.restype = st
+    L.rl_set_graphs.argtypes = [vp, C.c_int]
     L.rl_candidate_weights.restype = st
     L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
@@ -405,6 +407,9 @@ class Network:
         nodes = np.zeros(max(m, 1), np.uint32); w = np.zeros(max(m, 1))
         self._check(self.lib.rl_candidate_weights(self.h, source, precision, _p(nodes), _p(w), m, C.byref(cnt)))
         return nodes[:m], w[:m]
+
+    def set_graphs(self, on: bool = True):
+        self._check(self.lib.rl_set_graphs(self.h, int(on)))
 
     def set_profiling(self, on: bool = True):
         self._check(self.lib.rl_set_profiling(self.h, int(on)))

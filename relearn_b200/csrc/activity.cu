@@ -25,11 +25,7 @@ namespace {
 
 struct ActArgs {
     uint32_t n;
-    uint32_t step;
     const uint8_t* enabled;
-    const uint32_t* csr_off;
-    const uint32_t* csr_src;
-    const int32_t* csr_w;
     const uint8_t* fired_prev;
     uint8_t* fired_cur;
     double* x;
@@ -45,7 +41,6 @@ struct ActArgs {
     double a, ab, c, d, v_spike, k1, k2, k3, scale_m;
     double beta, tau_inv, scale_c;
     double eta[3];
-    int has_edges;
     const NetInfo* nets;
     const uint16_t* net_of;
 };
@@ -63,11 +58,12 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
-__global__ void __launch_bounds__(256) k_activity(ActArgs A) {
+__global__ void __launch_bounds__(256) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) {
         return;
     }
+    const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
         A.input[i] = 0.0;
         A.fired_cur[i] = A.fired_prev[i];
@@ -77,11 +73,14 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A) {
         return;
     }
     long long isum = 0;
-    if (A.has_edges) {
-        const uint32_t e0 = A.csr_off[i], e1 = A.csr_off[i + 1];
+    if (D->has_edges) {
+        const uint32_t* __restrict__ off = D->off;
+        const uint32_t* __restrict__ src = D->src;
+        const int32_t* __restrict__ wt = D->w;
+        const uint32_t e0 = off[i], e1 = off[i + 1];
         for (uint32_t e = e0; e < e1; ++e) {
-            if (A.fired_prev[A.csr_src[e]]) {
-                isum += A.csr_w[e];
+            if (A.fired_prev[src[e]]) {
+                isum += wt[e];
             }
         }
     }
@@ -89,7 +88,7 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A) {
     const NetInfo& N = A.nets[A.net_of[i]];
     double input = 0.0;
     input += (double)isum * A.conductance;
-    input += background_normal(N.seed, A.step, i - N.first, A.noise_mean, A.noise_stddev);
+    input += background_normal(N.seed, step, i - N.first, A.noise_mean, A.noise_stddev);
     A.input[i] = input;
 
     double xv = A.x[i];
@@ -188,22 +187,15 @@ __global__ void k_commit(CommitArgs A) {
 
 }  // namespace
 
-void run_activity_step(Ctx& c, uint32_t step) {
-    if (is_fp32(c)) {
-        run_activity_step_f32(c, step);
-        return;
-    }
+namespace {
+
+void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
     const rl_config& k = c.cfg;
     ActArgs A;
     A.n = c.n;
-    A.step = step;
     A.enabled = c.nr.enabled.p;
-    A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
-    A.csr_off = c.graph.offsets.p;
-    A.csr_src = c.graph.src.p;
-    A.csr_w = c.graph.weight.p;
-    A.fired_prev = c.nr.fired[c.nr.cur].p;
-    A.fired_cur = c.nr.fired[c.nr.cur ^ 1].p;
+    A.fired_prev = fired_prev;
+    A.fired_cur = fired_cur;
     A.x = c.nr.x.p;
     A.u = c.nr.u.p;
     A.calcium = c.nr.calcium.p;
@@ -234,13 +226,84 @@ void run_activity_step(Ctx& c, uint32_t step) {
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
-    {
-        PhaseScope ps(c, PH_ACTIVITY_KERNEL);
-        k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
-        RL_LAUNCH_CHECK();
+    k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    RL_LAUNCH_CHECK();
+}
+
+__global__ void k_set_desc(ActDesc* D, ActDesc v) {
+    *D = v;
+}
+
+void launch_step(Ctx& c, uint32_t kstep) {
+    const int p = (c.nr.cur + (int)kstep) & 1;
+    if (is_fp32(c)) {
+        launch_activity_f32(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p);
+    } else {
+        launch_activity_fp64(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p);
     }
-    c.nr.cur ^= 1;
-    c.stats.activity_steps += 1;
+}
+
+}  // namespace
+
+void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
+    if (nsteps == 0) {
+        return;
+    }
+    const ActDesc v{ first_step, c.graph.num_edges > 0 ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p };
+    k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
+    RL_LAUNCH_CHECK();
+    const bool graph = c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
+    if (graph) {
+        const int p = c.nr.cur & 1;
+        if (c.act_graph[p] == nullptr || c.act_graph_len != nsteps) {
+            for (auto& g : c.act_graph) {
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+            }
+            // capture one interval of activity kernels for this parity
+            cudaGraph_t gr = nullptr;
+            const bool timer = c.timer.on;
+            c.timer.on = false;
+            const uint64_t launches = g_launches;
+            RL_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+            c.capturing = true;
+            try {
+                for (uint32_t k = 0; k < nsteps; ++k) {
+                    launch_step(c, k);
+                }
+            } catch (...) {
+                c.capturing = false;
+                cudaStreamEndCapture(c.stream, &gr);
+                if (gr) {
+                    cudaGraphDestroy(gr);
+                }
+                c.timer.on = timer;
+                throw;
+            }
+            c.capturing = false;
+            RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &gr));
+            c.timer.on = timer;
+            g_launches = launches;
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+            cudaGraphDestroy(gr);
+            RL_CUDA_TRY(e);
+            c.act_graph[p] = ex;
+            c.act_graph_len = nsteps;
+        }
+        PhaseScope ps(c, PH_ACTIVITY_KERNEL, nsteps);
+        RL_CUDA_TRY(cudaGraphLaunch(c.act_graph[p], c.stream));
+        g_launches += nsteps;
+    } else {
+        for (uint32_t k = 0; k < nsteps; ++k) {
+            PhaseScope ps(c, PH_ACTIVITY_KERNEL);
+            launch_step(c, k);
+        }
+    }
+    c.nr.cur ^= (int)(nsteps & 1u);
+    c.stats.activity_steps += nsteps;
 }
 
 uint64_t run_commit(Ctx& c, int type) {

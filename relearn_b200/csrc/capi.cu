@@ -8,8 +8,8 @@
 
 namespace rl {
 
-PhaseScope::PhaseScope(Ctx& ctx, int ph) : c(&ctx), phase(ph) {
-    if (!c->timer.on) {
+PhaseScope::PhaseScope(Ctx& ctx, int ph, uint32_t weight) : c(&ctx), phase(ph) {
+    if (!c->timer.on || c->capturing) {
         c = nullptr;
         return;
     }
@@ -26,7 +26,7 @@ PhaseScope::PhaseScope(Ctx& ctx, int ph) : c(&ctx), phase(ph) {
     cudaEvent_t start = take();
     end = take();
     RL_CUDA_TRY(cudaEventRecord(start, c->stream));
-    c->timer.pending[phase].emplace_back(start, end);
+    c->timer.pending[phase].push_back(PendingTimer{ start, end, weight });
 }
 
 PhaseScope::~PhaseScope() {
@@ -40,11 +40,11 @@ static void resolve_timers(Ctx& c) {
     for (int p = 0; p < PH_COUNT; ++p) {
         for (auto& pr : c.timer.pending[p]) {
             float ms = 0.f;
-            RL_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+            RL_CUDA_TRY(cudaEventElapsedTime(&ms, pr.start, pr.end));
             c.timer.ms[p] += ms;
-            c.timer.count[p] += 1;
-            c.timer.free_events.push_back(pr.first);
-            c.timer.free_events.push_back(pr.second);
+            c.timer.count[p] += pr.weight;
+            c.timer.free_events.push_back(pr.start);
+            c.timer.free_events.push_back(pr.end);
         }
         c.timer.pending[p].clear();
     }
@@ -237,6 +237,7 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     c.graph.offsets.alloc(n + 1);
     RL_CUDA_TRY(cudaMemsetAsync(c.graph.offsets.p, 0, (n + 1) * sizeof(uint32_t), c.stream));
     c.to_delete.alloc(n);
+    c.act_desc.alloc(1);
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.counters.alloc(4);
@@ -439,12 +440,17 @@ rl_status rl_ctx_destroy(void* ctx) {
     }
     for (int p = 0; p < rl::PH_COUNT; ++p) {
         for (auto& pr : c->timer.pending[p]) {
-            cudaEventDestroy(pr.first);
-            cudaEventDestroy(pr.second);
+            cudaEventDestroy(pr.start);
+            cudaEventDestroy(pr.end);
         }
     }
     for (auto e : c->timer.free_events) {
         cudaEventDestroy(e);
+    }
+    for (auto& g : c->act_graph) {
+        if (g) {
+            cudaGraphExecDestroy(g);
+        }
     }
     if (c->own_stream) {
         cudaStreamDestroy(c->own_stream);
@@ -675,9 +681,7 @@ rl_status rl_get_edges(void* ctx, uint32_t* target, uint32_t* source, int32_t* w
 rl_status rl_activity_block(void* ctx, uint32_t first_step, uint32_t nsteps) {
     return rl::guarded(ctx, [&](Ctx& c) {
         rl::rebuild_graph(c);
-        for (uint32_t s = 0; s < nsteps; ++s) {
-            rl::run_activity_step(c, first_step + s);
-        }
+        rl::run_activity_block(c, first_step, nsteps);
     });
 }
 
@@ -690,12 +694,22 @@ rl_status rl_simulate(void* ctx, uint32_t first_step, uint32_t nsteps) {
         rl::require_tree(c);
         rl::rebuild_graph(c);
         const uint32_t interval = c.cfg.plasticity_interval;
-        for (uint32_t s = 0; s < nsteps; ++s) {
-            const uint32_t step = first_step + s;
-            rl::run_activity_step(c, step);
-            if (interval > 0 && step % interval == 0) {
-                rl::plasticity_update(c, step);
+        const uint64_t end = (uint64_t)first_step + nsteps;  // exclusive
+        uint64_t step = first_step;
+        while (step < end) {
+            // activity up to and including the next plasticity step, then the update
+            uint64_t stop = end;
+            if (interval > 0) {
+                const uint64_t next = ((step + interval - 1) / interval) * interval;  // first multiple >= step
+                if (next < end) {
+                    stop = next + 1;
+                }
             }
+            rl::run_activity_block(c, (uint32_t)step, (uint32_t)(stop - step));
+            if (interval > 0 && (stop - 1) % interval == 0 && stop - 1 >= step) {
+                rl::plasticity_update(c, (uint32_t)(stop - 1));
+            }
+            step = stop;
         }
     });
 }
@@ -728,6 +742,10 @@ rl_status rl_set_stream(void* ctx, void* cuda_stream) {
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
         c.stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c.own_stream;
     });
+}
+
+rl_status rl_set_graphs(void* ctx, int enable) {
+    return rl::guarded(ctx, [&](Ctx& c) { c.use_graphs = enable != 0; });
 }
 
 rl_status rl_set_profiling(void* ctx, int enable) {

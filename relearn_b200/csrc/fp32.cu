@@ -2,7 +2,8 @@
 //
 // Same algorithms as the FP64 drop-in (activity.cu, bh_search.cu) with
 // different arithmetic, as the precision form specifies:
-//   * membrane (Izhikevich), input (normal background) and growth-curve
+//   * membrane (Izhikevich), input (normal background, the same Philox draw
+//     as the FP64 form mapped through an FP32 erfinv) and growth-curve
 //     arithmetic in FP32, state x, u, growth deltas stored as FP32;
 //   * calcium integrated in FP64.  The h Euler substeps of
 //     CalciumCalculatorCPU::update_current_calcium (calcium/CalciumCalculatorCPU.cpp:61-68)
@@ -44,11 +45,8 @@ __global__ void k_f2d(uint32_t n, const float* __restrict__ a, double* __restric
 
 // ----------------------------------------------------------- activity
 struct Act32 {
-    uint32_t n, step;
+    uint32_t n;
     const uint8_t* enabled;
-    const uint32_t* csr_off;
-    const uint32_t* csr_src;
-    const int32_t* csr_w;
     const uint8_t* fired_prev;
     uint8_t* fired_cur;
     float* x;
@@ -63,108 +61,80 @@ struct Act32 {
     float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
     float eta[3];
-    int has_edges;
     const NetInfo* nets;
     const uint16_t* net_of;
 };
 
-// AS241 in FP32 (Wichura 1988, PPND7 accuracy), own log via __logf.
-__device__ __forceinline__ float normal_quantile_f32(float p) {
-    const float q = p - 0.5f;
-    if (fabsf(q) <= 0.425f) {
-        const float r = 0.180625f - q * q;
-        float num = 2.5090809287301226727e+3f;
-        num = fmaf(num, r, 3.3430575583588128105e+4f);
-        num = fmaf(num, r, 6.7265770927008700853e+4f);
-        num = fmaf(num, r, 4.5921953931549871457e+4f);
-        num = fmaf(num, r, 1.3731693765509461125e+4f);
-        num = fmaf(num, r, 1.9715909503065514427e+3f);
-        num = fmaf(num, r, 1.3314166789178437745e+2f);
-        num = fmaf(num, r, 3.3871328727963666080e+0f);
-        float den = 5.2264952788528545610e+3f;
-        den = fmaf(den, r, 2.8729085735721942674e+4f);
-        den = fmaf(den, r, 3.9307895800092710610e+4f);
-        den = fmaf(den, r, 2.1213794301586595867e+4f);
-        den = fmaf(den, r, 5.3941960214247511077e+3f);
-        den = fmaf(den, r, 6.8718700749205790830e+2f);
-        den = fmaf(den, r, 4.2313330701600911252e+1f);
-        den = fmaf(den, r, 1.0f);
-        return __fdividef(num * q, den);
-    }
-    float r = q < 0.0f ? p : 1.0f - p;
-    r = sqrtf(-__logf(r));
-    float num, den;
-    if (r <= 5.0f) {
-        r -= 1.6f;
-        num = 7.7454501427834140764e-4f;
-        num = fmaf(num, r, 2.2723844989269184583e-2f);
-        num = fmaf(num, r, 2.4178072517745061177e-1f);
-        num = fmaf(num, r, 1.2704582524523683826e+0f);
-        num = fmaf(num, r, 3.6478483247632046050e+0f);
-        num = fmaf(num, r, 5.7694972214606914055e+0f);
-        num = fmaf(num, r, 4.6303378461565452959e+0f);
-        num = fmaf(num, r, 1.4234371107496835773e+0f);
-        den = 1.0507500716444168432e-9f;
-        den = fmaf(den, r, 5.4759380849953449460e-4f);
-        den = fmaf(den, r, 1.5198666563616457197e-2f);
-        den = fmaf(den, r, 1.4810397642748007459e-1f);
-        den = fmaf(den, r, 6.8976733498510000455e-1f);
-        den = fmaf(den, r, 1.6763848301838038494e+0f);
-        den = fmaf(den, r, 2.0531916266377588219e+0f);
-        den = fmaf(den, r, 1.0f);
+// Standard normal quantile of u = (k + 0.5) 2^-24 in FP32 as sqrt(2) erfinv(2u - 1),
+// with the single-precision erfinv approximation of M. Giles ("Approximating
+// the erfinv function", GPU Computing Gems Jade Edition, 2011): the central
+// branch covers 99.7 % of the draws, so warps rarely diverge.
+__device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
+    const float x = (float)((int)(2u * k24 + 1u) - (1 << 24)) * 5.9604644775390625e-8f;  // 2u - 1, exact
+    float w = -__logf((1.0f - x) * (1.0f + x));
+    float p;
+    if (w < 5.0f) {
+        w -= 2.5f;
+        p = 2.81022636e-08f;
+        p = fmaf(p, w, 3.43273939e-07f);
+        p = fmaf(p, w, -3.5233877e-06f);
+        p = fmaf(p, w, -4.39150654e-06f);
+        p = fmaf(p, w, 0.00021858087f);
+        p = fmaf(p, w, -0.00125372503f);
+        p = fmaf(p, w, -0.00417768164f);
+        p = fmaf(p, w, 0.246640727f);
+        p = fmaf(p, w, 1.50140941f);
     } else {
-        r -= 5.0f;
-        num = 2.0103343992922881327e-7f;
-        num = fmaf(num, r, 2.7115555687434875782e-5f);
-        num = fmaf(num, r, 1.2426609473880784386e-3f);
-        num = fmaf(num, r, 2.6532189526576123093e-2f);
-        num = fmaf(num, r, 2.9656057182850489123e-1f);
-        num = fmaf(num, r, 1.7848265399172913358e+0f);
-        num = fmaf(num, r, 5.4637849111641143699e+0f);
-        num = fmaf(num, r, 6.6579046435011037772e+0f);
-        den = 2.0442631033899397856e-15f;
-        den = fmaf(den, r, 1.4215117583164458887e-7f);
-        den = fmaf(den, r, 1.8463183175100546818e-5f);
-        den = fmaf(den, r, 7.8686913114561325910e-4f);
-        den = fmaf(den, r, 1.4875361290850614853e-2f);
-        den = fmaf(den, r, 1.3692988092273580531e-1f);
-        den = fmaf(den, r, 5.9983220655588793769e-1f);
-        den = fmaf(den, r, 1.0f);
+        w = sqrtf(w) - 3.0f;
+        p = -0.000200214257f;
+        p = fmaf(p, w, 0.000100950558f);
+        p = fmaf(p, w, 0.00134934322f);
+        p = fmaf(p, w, -0.00367342844f);
+        p = fmaf(p, w, 0.00573950773f);
+        p = fmaf(p, w, -0.0076224613f);
+        p = fmaf(p, w, 0.00943887047f);
+        p = fmaf(p, w, 1.00167406f);
+        p = fmaf(p, w, 2.83297682f);
     }
-    const float x = __fdividef(num, den);
-    return q < 0.0f ? -x : x;
+    return 1.41421356237f * (p * x);
 }
 
-__global__ void __launch_bounds__(256) k_activity_f32(Act32 A) {
+template <int H>
+__global__ void __launch_bounds__(256) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) {
         return;
     }
+    const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
         A.input[i] = 0.0f;
         A.fired_cur[i] = A.fired_prev[i];
         return;
     }
     int isum = 0;
-    if (A.has_edges) {
-        const uint32_t e0 = A.csr_off[i], e1 = A.csr_off[i + 1];
+    if (D->has_edges) {
+        const uint32_t* __restrict__ off = D->off;
+        const uint32_t* __restrict__ src = D->src;
+        const int32_t* __restrict__ wt = D->w;
+        const uint32_t e0 = off[i], e1 = off[i + 1];
         for (uint32_t e = e0; e < e1; ++e) {
-            if (A.fired_prev[A.csr_src[e]]) {
-                isum += A.csr_w[e];
+            if (A.fired_prev[src[e]]) {
+                isum += wt[e];
             }
         }
     }
     // the same Philox draw as the FP64 form, 24 bits of it
     const NetInfo& N = A.nets[A.net_of[i]];
-    const u32x4 w = draw(N.seed, A.step, i - N.first, 0u, STREAM_NOISE, 0u);
-    const float p = ((float)(w.x >> 8) + 0.5f) * 5.9604644775390625e-8f;  // 2^-24
-    const float input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_quantile_f32(p), A.noise_mean));
+    const u32x4 w = draw(N.seed, step, i - N.first, 0u, STREAM_NOISE, 0u);
+    const float input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(w.x >> 8), A.noise_mean));
     A.input[i] = input;
 
     float xv = A.x[i];
     float uv = A.u[i];
     uint8_t spiked = 0;
-    for (uint32_t it = 0; it < A.h_model; ++it) {
+    const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
+#pragma unroll
+    for (uint32_t it = 0; it < h; ++it) {
         const float x_inc = fmaf(A.k1 * xv, xv, fmaf(A.k2, xv, A.k3)) - uv + input;
         const float u_inc = fmaf(A.ab, xv, -A.a * uv);
         xv = fmaf(x_inc, A.scale_m, xv);
@@ -690,18 +660,13 @@ void f64_from_f32(Ctx& c) {
     }
 }
 
-void run_activity_step_f32(Ctx& c, uint32_t step) {
+void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
     const rl_config& k = c.cfg;
     Act32 A;
     A.n = c.n;
-    A.step = step;
     A.enabled = c.nr.enabled.p;
-    A.has_edges = c.graph.num_edges > 0 ? 1 : 0;
-    A.csr_off = c.graph.offsets.p;
-    A.csr_src = c.graph.src.p;
-    A.csr_w = c.graph.weight.p;
-    A.fired_prev = c.nr.fired[c.nr.cur].p;
-    A.fired_cur = c.nr.fired[c.nr.cur ^ 1].p;
+    A.fired_prev = fired_prev;
+    A.fired_cur = fired_cur;
     A.x = c.nr.x32.p;
     A.u = c.nr.u32.p;
     A.input = c.nr.input32.p;
@@ -743,13 +708,12 @@ void run_activity_step_f32(Ctx& c, uint32_t step) {
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
-    {
-        PhaseScope ps(c, PH_ACTIVITY_KERNEL);
-        k_activity_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
-        RL_LAUNCH_CHECK();
+    if (k.h_model == 10) {
+        k_activity_f32<10><<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    } else {
+        k_activity_f32<0><<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
     }
-    c.nr.cur ^= 1;
-    c.stats.activity_steps += 1;
+    RL_LAUNCH_CHECK();
 }
 
 uint64_t run_commit_f32(Ctx& c, int type) {

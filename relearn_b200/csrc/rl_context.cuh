@@ -110,10 +110,16 @@ enum Phase : int {
     PH_COUNT = RL_NUM_PHASES,
 };
 
+struct PendingTimer {
+    cudaEvent_t start;
+    cudaEvent_t end;
+    uint32_t weight;  // kernel launches the interval stands for
+};
+
 struct PhaseTimer {
     bool on = false;
     std::vector<cudaEvent_t> free_events;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[PH_COUNT];
+    std::vector<PendingTimer> pending[PH_COUNT];
     double ms[PH_COUNT] = {};
     uint64_t count[PH_COUNT] = {};
 };
@@ -145,8 +151,18 @@ struct PhaseScope {
     Ctx* c;
     int phase;
     cudaEvent_t end = nullptr;
-    PhaseScope(Ctx& ctx, int ph);
+    PhaseScope(Ctx& ctx, int ph, uint32_t weight = 1);
     ~PhaseScope();
+};
+
+// Per-block values of the activity kernels, read from device memory so that a
+// captured 100-step graph stays valid when the synapse graph is rebuilt.
+struct ActDesc {
+    uint32_t base_step;
+    uint32_t has_edges;
+    const uint32_t* off;
+    const uint32_t* src;
+    const int32_t* w;
 };
 
 struct Ctx {
@@ -156,6 +172,11 @@ struct Ctx {
     cudaStream_t stream = nullptr;      // stream all work is issued on
     cudaStream_t own_stream = nullptr;  // the context's own stream
     PhaseTimer timer;
+    DBuf<ActDesc> act_desc;
+    cudaGraphExec_t act_graph[2] = { nullptr, nullptr };  // per fired-buffer parity
+    uint32_t act_graph_len = 0;
+    bool use_graphs = true;
+    bool capturing = false;
     std::vector<NetInfo> nets;  // host copy
     DBuf<NetInfo> d_nets;
     DBuf<uint16_t> net_of;      // network of each neuron
@@ -197,7 +218,7 @@ bool is_fp32(const Ctx& c);
 void alloc_fp32(Ctx& c);
 void f32_from_f64(Ctx& c);  // state arrays FP64 -> FP32 (after a host upload)
 void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download)
-void run_activity_step_f32(Ctx& c, uint32_t step);
+void launch_activity_f32(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur);
 uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
@@ -205,7 +226,9 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu
-void run_activity_step(Ctx& c, uint32_t step);
+// Activity steps first..first+nsteps-1 (one fused kernel per step; a full
+// plasticity interval runs as a captured CUDA graph).
+void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps);
 uint64_t run_commit(Ctx& c, int type);  // commit one element type; to_delete[] per neuron, returns the sum
 
 void check_device_error(Ctx& c, const char* phase);
