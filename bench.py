@@ -135,6 +135,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     net = R.Network(p)
     net.set_stream(stream.cuda_stream)
     net.set_positions(pos, sig)
+    net.autotune(1)  # launch shapes timed during the warm-up
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     step = 1
     for _ in range(args.warmup):
@@ -178,7 +179,8 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch,
             "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
-    return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof)
+    return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof,
+                tuning=net.tuning())
 
 
 class _Null:
@@ -237,7 +239,7 @@ def run_b200(args, world, rank, local):
         o = measure_form(args, 1, dev, stream, world, pos, sig, params)
         bh32 = bh_snapshot(o["net"], n, stream, o["step"]) if not args.skip_bh else None
         other = {"precision": "fp32", "value": o["value"], "unit": "neuron-steps/s", "ms_per_step": o["total_ms"] / args.steps,
-                 "vs_fp64_drop_in": o["value"] / m["value"], "roofline": o["roofline"], "phases_ms": o["phases"]}
+                 "vs_fp64_drop_in": o["value"] / m["value"], "roofline": o["roofline"], "phases_ms": o["phases"], "tuning": o["tuning"]}
         if bh32:
             other["bh_search"] = bh32
             if bh:
@@ -250,6 +252,9 @@ def run_b200(args, world, rank, local):
     prec = None
     if rank == 0 and world == 1 and args.precision_report:
         prec = precision_report(args, dev, stream)
+    serve = None
+    if rank == 0 and world == 1 and not args.skip_serve:
+        serve = serve_figure(args, dev)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, params, pos, sig)
@@ -281,6 +286,7 @@ def run_b200(args, world, rank, local):
         "e2e": {"value": e2e_val, "unit": "neuron-steps/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 9 * n,
                 "api": "rl_set_enabled + rl_simulate + rl_get_neurons (pinned host buffers)"},
         "gpu_launches": m["launches"],
+        "tuning": m["tuning"],
         "clocks": clocks,
     }
     if bh:
@@ -291,6 +297,8 @@ def run_b200(args, world, rank, local):
         line["ensemble"] = ens
     if prec:
         line["precision_report"] = prec
+    if serve:
+        line["serving"] = serve
     if cpu:
         line["cpu_baseline"] = cpu
     return line
@@ -329,6 +337,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     ens = R.Network(base, networks=nets)
     ens.set_stream(stream.cuda_stream)
     ens.set_positions(pos, sig)
+    ens.autotune(1)  # launch shapes timed during the warm-up
     step = 1
     for _ in range(args.warmup):
         ens.simulate(step, PERIOD)
@@ -355,6 +364,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     act_ms, act_cnt = ph["activity_kernel"]
+    tuning = ens.tuning()
     hbm, peak_kind = peaks()
     bytes_per_launch = ACT_BYTES_FP32 * total
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
@@ -363,7 +373,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
             "neurons": total, "periods": periods, "precision": "fp32", "launches_per_step": 1, "graphs": "100-step activity blocks",
             "roofline": {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None},
-            "phases_ms": {k: v[0] for k, v in ph.items()}}
+            "phases_ms": {k: v[0] for k, v in ph.items()}, "tuning": tuning}
 
 
 def precision_report(args, dev, stream, n=4_000_000, side=16_000.0, steps=1000, sources=64):
@@ -432,6 +442,74 @@ def precision_report(args, dev, stream, n=4_000_000, side=16_000.0, steps=1000, 
     return out
 
 
+def serve_figure(args, dev):
+    """The serving form: a seeded Poisson stream of sweep requests (20 per
+    second; each one network of log-uniform 2,000-1,000,000 neurons with its own
+    seed, growth rate log-uniform 1e-5-1e-3 and theta uniform 0.2-0.5, run for
+    5,000 steps) submitted in real time to the native request loop, which admits
+    them against a 150 GB HBM budget as slots free up, overlaps them on the GPU
+    and packs small pending ones into batched contexts.  Reports p50 / p99
+    completion latency (submission to result) and aggregate neuron-steps/s."""
+    import relearn_b200 as R
+    from relearn_b200 import workloads
+    from relearn_b200.serving import Server, latency_summary
+
+    prec = 1 if args.serve_precision == "fp32" else 0
+    params = R.default_params(1, 1.0)
+    params["precision"] = prec
+    params["device"] = dev.index
+    reqs = workloads.serving_stream(args.seed + 17, args.serve_rate, args.serve_seconds, steps=args.serve_steps)
+    budget = 150e9
+    done, max_running, max_reserved, max_pending, lag = [], 0, 0, 0, 0.0
+    with Server(params, hbm_budget_bytes=budget, slots=args.serve_slots, pack_networks=16, pack_max_neurons=65_536) as srv:
+        t0 = time.perf_counter()
+        for t_arr, net in reqs:
+            pos, sig = workloads.request_inputs(net)
+            while True:
+                wait = t_arr - (time.perf_counter() - t0)
+                if wait <= 0:
+                    break
+                done += srv.poll(wait_ms=max(1, int(min(wait, 0.05) * 1e3)))
+            lag = max(lag, time.perf_counter() - t0 - t_arr)
+            srv.submit(net, pos, sig, net["steps"])
+            p, r, b = srv.load()
+            max_pending, max_running, max_reserved = max(max_pending, p), max(max_running, r), max(max_reserved, b)
+        while len(done) < len(reqs):
+            done += srv.poll(wait_ms=200)
+            p, r, b = srv.load()
+            max_pending, max_running, max_reserved = max(max_pending, p), max(max_running, r), max(max_reserved, b)
+    # capacity: the same requests submitted at once, so the GPU never waits for arrivals
+    burst = []
+    with Server(params, hbm_budget_bytes=budget, slots=args.serve_slots, pack_networks=16, pack_max_neurons=65_536) as srv:
+        for _, net in reqs:
+            pos, sig = workloads.request_inputs(net)
+            srv.submit(net, pos, sig, net["steps"])
+        while len(burst) < len(reqs):
+            burst += srv.poll(wait_ms=200)
+    cap = latency_summary(burst)
+    bad = [d for d in done + burst if d["status"] != 0]
+    summ = latency_summary(done)
+    hbm, peak_kind = peaks()
+    per_ns = ACT_BYTES_FP32 if prec else ACT_BYTES_PER_NEURON
+    achieved = summ["neuron_steps_per_s"] * per_ns / 1e9
+    offered = sum(d["num_neurons"] * d["steps"] for _, d in reqs) / args.serve_seconds
+    packs = [d["pack_size"] for d in done]
+    return {"metric": "p50/p99 completion latency; aggregate neuron-steps/s", "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
+            "max_s": summ["max_s"], "value": summ["neuron_steps_per_s"], "unit": "neuron-steps/s", "requests": len(done), "failed": len(bad),
+            "precision": "fp32" if prec else "fp64", "arrivals": f"Poisson {args.serve_rate:g}/s over {args.serve_seconds:g} s (seeded)",
+            "sample": f"the first {args.serve_seconds:g} s of the 600 s stream", "steps_per_request": args.serve_steps,
+            "offered_neuron_steps_per_s": offered, "span_s": summ["span_s"], "mean_queue_s": summ["mean_queue_s"], "p99_queue_s": summ["p99_queue_s"],
+            "slots": args.serve_slots, "hbm_budget_bytes": budget, "max_running": max_running, "max_pending": max_pending,
+            "max_reserved_bytes": max_reserved, "mean_pack_size": float(np.mean(packs)), "max_pack_size": int(max(packs)),
+            "max_peak_over_footprint": max(d["device_peak_bytes"] / d["footprint_bytes"] for d in done if d["pack_size"] == 1)
+            if any(d["pack_size"] == 1 for d in done) else None,
+            "max_submit_lag_s": lag,
+            "capacity": {"neuron_steps_per_s": cap["neuron_steps_per_s"], "span_s": cap["span_s"],
+                         "how": "the same requests submitted at once; aggregate over first submission to last result"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "bytes_per_neuron_step": per_ns}}
+
+
 def bh_snapshot(net, n, stream, step):
     import torch
 
@@ -458,10 +536,11 @@ def bh_snapshot(net, n, stream, step):
             search_ms.append(ph["search_kernel"][0])
             update_ms.append(e0.elapsed_time(e1))
     searches = n
-    st = net.stats()
+    t = net.tuning()
     return {"metric": "BH searches/s", "value": searches / (min(search_ms) / 1e3), "unit": "searches/s",
             "with_tree_update_and_copies": searches / (min(update_ms) / 1e3), "searches_per_update": searches,
-            "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron"}
+            "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron",
+            "search_shape": {"warps_per_block": t["search_warps"], "stack": t["search_stack"], "packet": t["search_packet"], "timed_ms": t["search_ms"]}}
 
 
 def cpu_baseline(args, params, pos, sig, activity_steps=None, searches=20000):
@@ -546,7 +625,9 @@ def run_reference(args, world, rank):
 def run_case(args):
     """Small cases for kernel profiles: `activity` runs 4 activity steps of a
     network of --neurons neurons (no octree needed); `search` runs the search
-    snapshot (one vacant axon and dendrite of each type per neuron) once."""
+    snapshot (one vacant axon and dendrite of each type per neuron) once;
+    `plasticity` seeds 0-3 elements per type and runs two plasticity periods
+    (100 activity steps + 1 plasticity update each)."""
     import relearn_b200 as R
 
     params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
@@ -554,6 +635,13 @@ def run_case(args):
     net = R.Network(params)
     if args.case == "activity":
         net.activity_block(1, 4)
+    elif args.case == "plasticity":
+        from relearn_b200 import workloads
+
+        net.set_positions(pos, sig)
+        for t, (g, v) in enumerate(workloads.initial_elements(args.neurons, 3, 0.0, 3.0)):
+            net.set_elements(t, g, np.zeros(args.neurons), np.zeros(args.neurons, np.uint32), v)
+        net.simulate(1, 200)
     else:
         net.set_positions(pos, sig)
         one = np.ones(args.neurons, np.uint32)
@@ -583,7 +671,13 @@ def main():
     ap.add_argument("--skip-ensemble", action="store_true", help="do not measure the batched form (128 networks)")
     ap.add_argument("--ensemble-networks", type=int, default=128)
     ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
-    ap.add_argument("--case", choices=["activity", "search"], default=None,
+    ap.add_argument("--skip-serve", action="store_true", help="do not measure the serving form")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the Poisson request stream (the full one is 600 s)")
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-steps", type=int, default=5000)
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-precision", choices=["fp64", "fp32"], default="fp32")
+    ap.add_argument("--case", choices=["activity", "search", "plasticity"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -289,6 +289,129 @@ RL_API rl_status rl_set_profiling(void* ctx, int enable);
  * last call (arrays of RL_NUM_PHASES entries); resets the accumulators. */
 RL_API rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts);
 
+/* Launch shapes of the hot kernels.  The search kernels walk the octree with
+ * `search_warps` warps per block, `search_stack` frames per walk and
+ * `search_packet` lanes (sources) walking the descent from the root together;
+ * the activity kernel runs `act_block` threads per block, and with
+ * `act_persistent` one resident wave of blocks strides over the neurons.  No
+ * counterpart in the reference (its CPU loops have no launch shape). */
+typedef struct rl_tuning {
+    int32_t search_warps;    /* 2, 4 or 8 */
+    int32_t search_stack;    /* 24 or 48 (at least the octree depth + 2) */
+    int32_t search_packet;   /* 32 or 16 */
+    int32_t act_block;       /* 128, 256 or 512 */
+    int32_t act_persistent;  /* 0 or 1 */
+    int32_t tuned;           /* bit 0: search shape timed or recalled, bit 1: activity shape */
+} rl_tuning;
+
+/* Candidates the tuner times, in the order of the times rl_get_tuning returns:
+ * search: packet 32 then 16, stack 24 then 48, warps 2, 4, 8 (12 shapes);
+ * activity: persistent 0 then 1, block 128, 256, 512 (6 shapes). */
+#define RL_NUM_SEARCH_SHAPES 12
+#define RL_NUM_ACT_SHAPES 6
+
+/* Autotuning: 0 keeps the current shapes; 1 times the candidates on the
+ * context's own data at the next activity block and the next search (a search
+ * shape needs a stack of at least the octree depth + 2) and keeps the fastest,
+ * reusing a result the process already has for the same precision, form and
+ * size class (power of two of the neuron count); 2 times them again even then.
+ * Timing runs the kernels on the current state and restores it, so results do
+ * not depend on tuning. */
+RL_API rl_status rl_autotune(void* ctx, int mode);
+
+/* Shapes in use; search_ms / act_ms (NULL to skip) receive the timed
+ * milliseconds per candidate (0 for a candidate not timed). */
+RL_API rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_ms);
+
+/* Set the shapes by hand (`tuned` is ignored); RL_ERR_INVALID for a shape that
+ * is not a candidate. */
+RL_API rl_status rl_set_tuning(void* ctx, const rl_tuning* t);
+
+/* Device memory the context holds now and at most since creation (bytes). */
+RL_API rl_status rl_ctx_memory(void* ctx, uint64_t* current, uint64_t* peak);
+
+/* ------------------------------------------------------------------ serving
+ * A request loop for sweep runs.  No counterpart in the reference, whose
+ * Simulation (sim/Simulation.cpp) runs one network per process; a sweep there
+ * is one mpirun per parameter set.  Here one process serves a stream of runs
+ * on one GPU: each request is one network (rl_network: its size, seed, box,
+ * theta, sigma and growth rates; the model parameters come from the server's
+ * base rl_config) simulated for steps 1..steps exactly as rl_simulate does in a
+ * context of its own.
+ *
+ * Admission is continuous: `slots` worker threads each run one context on a
+ * stream of their own, so the work of running requests overlaps on the GPU,
+ * and a pending request is admitted as soon as a slot is free and its device
+ * footprint (rl_serve_footprint) fits into what is left of the HBM budget.
+ * Pending requests are taken in arrival order; a request that does not fit
+ * lets later ones pass at most 2*slots times before admission waits for it.
+ * When several small requests are pending, one slot takes up to
+ * `pack_networks` of them (each of at most `pack_max_neurons` neurons, all with
+ * the same number of steps) into one batched context (rl_ensemble_create), so
+ * they share every launch.  Results do not depend on how requests were
+ * grouped or overlapped: each network evolves bit for bit as in a context of
+ * its own. */
+typedef struct rl_serve_config {
+    uint64_t hbm_budget_bytes;  /* device bytes that admitted requests may hold together */
+    uint64_t pack_max_neurons;  /* requests up to this size may share a batched context */
+    int32_t slots;              /* runs on the GPU at a time (worker threads, one stream each) */
+    int32_t pack_networks;      /* most requests in one batched context (1 = never pack) */
+    int32_t use_graphs;         /* capture activity intervals as CUDA graphs (rl_set_graphs) */
+    int32_t autotune;           /* rl_autotune mode of every context (shapes reused per size class) */
+} rl_serve_config;
+
+typedef struct rl_serve_request {
+    rl_network net;             /* the network; net.num_neurons > 0 */
+    const double* xyz;          /* 3*num_neurons positions, copied at submission */
+    const uint8_t* signal;      /* num_neurons signal types (1 = inhibitory), copied */
+    const double* grown[3];     /* initial grown elements per type, or NULL for 0; copied */
+    uint32_t steps;             /* simulate steps 1..steps */
+    uint32_t keep_state;        /* 1: keep the final state for rl_serve_fetch */
+} rl_serve_request;
+
+typedef struct rl_serve_done {
+    uint64_t id;
+    int32_t status;             /* rl_status of the run */
+    uint32_t pack_size;         /* requests that shared its context */
+    double t_submit;            /* seconds since the server was created */
+    double t_admit;
+    double t_finish;
+    uint64_t num_neurons;
+    uint64_t num_synapses;      /* synapses of this network after the last step */
+    uint64_t footprint_bytes;   /* what admission reserved for it */
+    uint64_t device_peak_bytes; /* peak bytes of the context it ran in */
+    uint64_t neuron_steps;      /* num_neurons * steps */
+} rl_serve_done;
+
+/* Device bytes admission reserves for a request: an upper bound on what its
+ * context holds at any time, from its size, the initial axons and the most
+ * the axons can grow in `steps` steps (growth_rate[0] per step). */
+RL_API rl_status rl_serve_footprint(const rl_config* base, const rl_network* net, double initial_axons, uint32_t steps, uint64_t* bytes);
+
+RL_API rl_status rl_serve_create(const rl_config* base, const rl_serve_config* sc, void** server);
+
+/* Queue a request; *id receives its number.  Requests whose footprint exceeds
+ * the whole budget are refused with RL_ERR_OOM. */
+RL_API rl_status rl_serve_submit(void* server, const rl_serve_request* req, uint64_t* id);
+
+/* Finished requests in completion order: up to `capacity` records, waiting up
+ * to wait_ms milliseconds for the first one (0: do not wait). */
+RL_API rl_status rl_serve_poll(void* server, rl_serve_done* out, uint64_t capacity, uint64_t* count, int32_t wait_ms);
+
+/* The kept final state of a finished request (keep_state = 1): x, u, calcium
+ * (num_neurons each), connected elements (3*num_neurons, type-major) and its
+ * synapses (network-local ids, sorted by target then source); NULL pointers
+ * are skipped.  The record is released afterwards. */
+RL_API rl_status rl_serve_fetch(void* server, uint64_t id, double* x, double* u, double* calcium, uint32_t* connected,
+                                rl_synapse* synapses, uint64_t capacity);
+
+/* Requests queued, running, and device bytes reserved now. */
+RL_API rl_status rl_serve_load(void* server, uint64_t* pending, uint64_t* running, uint64_t* reserved_bytes);
+
+/* Let every queued and running request finish, then stop the workers and free
+ * the server with the results nobody fetched. */
+RL_API rl_status rl_serve_destroy(void* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,31 @@ class RlStats(C.Structure):
                                                                                                   ("reserved", C.c_uint32)]
 
 
+class RlTuning(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("search_warps", "search_stack", "search_packet", "act_block", "act_persistent", "tuned")]
+
+
+NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 12, 6
+SEARCH_SHAPES = [(w, s, p) for p in (32, 16) for s in (24, 48) for w in (2, 4, 8)]  # (warps, stack, packet) in timing order
+ACT_SHAPES = [(b, p) for p in (0, 1) for b in (128, 256, 512)]  # (block, persistent)
+
+
+class RlServeConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("pack_max_neurons", C.c_uint64), ("slots", C.c_int32), ("pack_networks", C.c_int32),
+                ("use_graphs", C.c_int32), ("autotune", C.c_int32)]
+
+
+class RlServeRequest(C.Structure):
+    _fields_ = [("net", RlNetwork), ("xyz", C.c_void_p), ("signal", C.c_void_p), ("grown", C.c_void_p * 3), ("steps", C.c_uint32),
+                ("keep_state", C.c_uint32)]
+
+
+class RlServeDone(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("pack_size", C.c_uint32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_finish", C.c_double), ("num_neurons", C.c_uint64), ("num_synapses", C.c_uint64), ("footprint_bytes", C.c_uint64),
+                ("device_peak_bytes", C.c_uint64), ("neuron_steps", C.c_uint64)]
+
+
 REQUEST_DTYPE = np.dtype([("target", "<u4"), ("source", "<u4"), ("j", "<u4"), ("signal", "<u4")])
 SYNAPSE_DTYPE = np.dtype([("target", "<u4"), ("source", "<u4"), ("weight", "<i4"), ("reserved", "<u4")])
 
@@ -112,7 +137,8 @@ ABI_FUNCTIONS = [
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
-    "rl_candidate_weights", "rl_set_graphs",
+    "rl_candidate_weights", "rl_set_graphs", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
+    "rl_serve_fetch", "rl_serve_load", "rl_serve_destroy", "rl_autotune", "rl_get_tuning", "rl_set_tuning",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -192,6 +218,28 @@ def load_library(path: str = LIB_PATH):
     L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
     L.rl_prepare_update_connectivity_noalloc.argtypes = [vp, vp, vp, vp, vp]
+    L.rl_autotune.restype = st
+    L.rl_autotune.argtypes = [vp, C.c_int]
+    L.rl_get_tuning.restype = st
+    L.rl_get_tuning.argtypes = [vp, P(RlTuning), vp, vp]
+    L.rl_set_tuning.restype = st
+    L.rl_set_tuning.argtypes = [vp, P(RlTuning)]
+    L.rl_ctx_memory.restype = st
+    L.rl_ctx_memory.argtypes = [vp, P(u64), P(u64)]
+    L.rl_serve_footprint.restype = st
+    L.rl_serve_footprint.argtypes = [P(RlConfig), P(RlNetwork), dbl, u32, P(u64)]
+    L.rl_serve_create.restype = st
+    L.rl_serve_create.argtypes = [P(RlConfig), P(RlServeConfig), P(vp)]
+    L.rl_serve_submit.restype = st
+    L.rl_serve_submit.argtypes = [vp, P(RlServeRequest), P(u64)]
+    L.rl_serve_poll.restype = st
+    L.rl_serve_poll.argtypes = [vp, P(RlServeDone), u64, P(u64), i32]
+    L.rl_serve_fetch.restype = st
+    L.rl_serve_fetch.argtypes = [vp, u64, vp, vp, vp, vp, vp, u64]
+    L.rl_serve_load.restype = st
+    L.rl_serve_load.argtypes = [vp, P(u64), P(u64), P(u64)]
+    L.rl_serve_destroy.restype = st
+    L.rl_serve_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -225,6 +273,21 @@ def make_config(params: dict) -> RlConfig:
     return cfg
 
 
+def fill_network(r: RlNetwork, d: dict) -> RlNetwork:
+    """rl_network from a dict with num_neurons, seed, side (or box_min /
+    box_max), theta, sigma and growth_rate (one rate or three)."""
+    r.num_neurons = int(d["num_neurons"])
+    r.seed = int(d["seed"])
+    side = d.get("side")
+    r.box_min[:] = list(d.get("box_min", (0.0, 0.0, 0.0)))
+    r.box_max[:] = list(d.get("box_max", (side, side, side)))
+    r.theta = float(d["theta"])
+    r.sigma = float(d["sigma"])
+    gr = d["growth_rate"]
+    r.growth_rate[:] = list(gr) if hasattr(gr, "__len__") else [float(gr)] * 3
+    return r
+
+
 class Network:
     """One network in one device context (rl_ctx)."""
 
@@ -242,16 +305,7 @@ class Network:
         else:
             arr = (RlNetwork * len(networks))()
             for k, d in enumerate(networks):
-                r = arr[k]
-                r.num_neurons = int(d["num_neurons"])
-                r.seed = int(d["seed"])
-                side = d.get("side")
-                r.box_min[:] = list(d.get("box_min", (0.0, 0.0, 0.0)))
-                r.box_max[:] = list(d.get("box_max", (side, side, side)))
-                r.theta = float(d["theta"])
-                r.sigma = float(d["sigma"])
-                gr = d["growth_rate"]
-                r.growth_rate[:] = list(gr) if hasattr(gr, "__len__") else [float(gr)] * 3
+                fill_network(arr[k], d)
             self.networks = [dict(d) for d in networks]
             self.n = int(sum(int(d["num_neurons"]) for d in networks))
             s = self.lib.rl_ensemble_create(C.byref(self.cfg), arr, len(networks), C.byref(h))
@@ -418,6 +472,32 @@ class Network:
         ms = np.zeros(len(PHASES)); cnt = np.zeros(len(PHASES), np.uint64)
         self._check(self.lib.rl_get_phase_times(self.h, _p(ms), _p(cnt)))
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(PHASES)}
+
+    def autotune(self, mode: int = 1):
+        """Time the launch shapes of the search and activity kernels on this
+        context's data at the next search and activity block (mode 1 reuses the
+        process's result for the same size class, mode 2 always times)."""
+        self._check(self.lib.rl_autotune(self.h, int(mode)))
+
+    def tuning(self) -> dict:
+        t = RlTuning()
+        sm = (C.c_float * NUM_SEARCH_SHAPES)()
+        am = (C.c_float * NUM_ACT_SHAPES)()
+        self._check(self.lib.rl_get_tuning(self.h, C.byref(t), sm, am))
+        d = {f: getattr(t, f) for f, _ in RlTuning._fields_}
+        d["search_ms"] = {f"w{w}_s{st}_p{p}": float(sm[k]) for k, (w, st, p) in enumerate(SEARCH_SHAPES) if sm[k] > 0}
+        d["act_ms"] = {f"b{b}_{'persistent' if p else 'grid'}": float(am[k]) for k, (b, p) in enumerate(ACT_SHAPES) if am[k] > 0}
+        return d
+
+    def set_tuning(self, search_warps=4, search_stack=48, search_packet=32, act_block=256, act_persistent=0):
+        t = RlTuning(search_warps, search_stack, search_packet, act_block, act_persistent, 0)
+        self._check(self.lib.rl_set_tuning(self.h, C.byref(t)))
+
+    def memory(self) -> tuple:
+        """Device bytes the context holds now and at its peak."""
+        cur, peak = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.rl_ctx_memory(self.h, C.byref(cur), C.byref(peak)))
+        return int(cur.value), int(peak.value)
 
     def stats(self) -> dict:
         s = RlStats()

@@ -4,11 +4,12 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librelearn_b200.so")
-SOURCES = ["prims.cu", "octree.cu", "bh_search.cu", "connector.cu", "activity.cu", "capi.cu", "noalloc.cu", "fp32.cu"]
+SOURCES = ["prims.cu", "octree.cu", "bh_search.cu", "connector.cu", "activity.cu", "capi.cu", "noalloc.cu", "fp32.cu", "serve.cpp"]
 HEADERS = ["rl_internal.cuh", "rl_context.cuh", "rl_math.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include", "relearn_b200.h")
 
@@ -40,15 +41,17 @@ def stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
+    objs = [os.path.join(CSRC, os.path.splitext(src)[0] + ".o") for src in SOURCES]
+    cmds = [[nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj] for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs]
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for res in pool.map(lambda cmd: subprocess.run(cmd, capture_output=True, text=True), cmds):
+            if res.returncode != 0:
+                sys.stderr.write(res.stdout + res.stderr)
+                raise subprocess.CalledProcessError(res.returncode, res.args)
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-pthread", "-o", LIB, *objs]
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)

@@ -17,6 +17,8 @@
 //     plasticity update.
 // All state is structure-of-arrays in HBM; one thread per neuron reads and
 // writes each of its words once per step.
+#include <memory>
+
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -58,11 +60,7 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
-__global__ void __launch_bounds__(256) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) {
-        return;
-    }
+__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
     const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
         A.input[i] = 0.0;
@@ -128,6 +126,16 @@ __global__ void __launch_bounds__(256) k_activity(ActArgs A, const ActDesc* __re
     }
 }
 
+// One thread per neuron; with fewer blocks than neurons / BLOCK (the
+// persistent shape) each thread strides over the neurons.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
+        activity_neuron(A, D, k, i);
+    }
+}
+
 struct CommitArgs {
     uint32_t n;
     const uint8_t* enabled;
@@ -187,9 +195,7 @@ __global__ void k_commit(CommitArgs A) {
 
 }  // namespace
 
-namespace {
-
-void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
+void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
     const rl_config& k = c.cfg;
     ActArgs A;
     A.n = c.n;
@@ -226,24 +232,139 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
-    k_activity<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    switch (v.block) {
+        case 128:
+            k_activity<128><<<act_grid(c, v, (const void*)&k_activity<128>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+        case 512:
+            k_activity<512><<<act_grid(c, v, (const void*)&k_activity<512>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+        default:
+            k_activity<256><<<act_grid(c, v, (const void*)&k_activity<256>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+    }
     RL_LAUNCH_CHECK();
 }
+
+namespace {
 
 __global__ void k_set_desc(ActDesc* D, ActDesc v) {
     *D = v;
 }
 
-void launch_step(Ctx& c, uint32_t kstep) {
+void launch_step(Ctx& c, uint32_t kstep, const ActVariant& v) {
     const int p = (c.nr.cur + (int)kstep) & 1;
     if (is_fp32(c)) {
-        launch_activity_f32(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p);
+        launch_activity_f32(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p, v);
     } else {
-        launch_activity_fp64(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p);
+        launch_activity_fp64(c, kstep, c.nr.fired[p].p, c.nr.fired[p ^ 1].p, v);
     }
 }
 
+void launch_step(Ctx& c, uint32_t kstep) {
+    launch_step(c, kstep, c.tune.act);
+}
+
+// Copies of the state one activity step writes, so that the tuner can run
+// steps and put everything back.
+struct ActSnapshot {
+    std::vector<std::pair<void*, size_t>> bufs;
+    std::vector<std::unique_ptr<DBuf<uint8_t>>> copies;
+    explicit ActSnapshot(Ctx& c) {
+        Neurons& N = c.nr;
+        const size_t n = c.n;
+        if (is_fp32(c)) {
+            bufs = { { N.x32.p, 4 * n }, { N.u32.p, 4 * n }, { N.input32.p, 4 * n }, { N.calcium.p, 8 * n } };
+            for (int t = 0; t < 3; ++t) {
+                bufs.push_back({ N.delta32[t].p, 4 * n });
+            }
+        } else {
+            bufs = { { N.x.p, 8 * n }, { N.u.p, 8 * n }, { N.input.p, 8 * n }, { N.calcium.p, 8 * n } };
+            for (int t = 0; t < 3; ++t) {
+                bufs.push_back({ N.delta[t].p, 8 * n });
+            }
+        }
+        bufs.push_back({ N.fired[0].p, n });
+        bufs.push_back({ N.fired[1].p, n });
+        for (size_t b = 0; b < bufs.size(); ++b) {
+            copies.push_back(std::make_unique<DBuf<uint8_t>>());
+            copies[b]->alloc(bufs[b].second);
+            RL_CUDA_TRY(cudaMemcpyAsync(copies[b]->p, bufs[b].first, bufs[b].second, cudaMemcpyDeviceToDevice, c.stream));
+        }
+    }
+    void restore(Ctx& c) {
+        for (size_t b = 0; b < bufs.size(); ++b) {
+            RL_CUDA_TRY(cudaMemcpyAsync(bufs[b].first, copies[b]->p, bufs[b].second, cudaMemcpyDeviceToDevice, c.stream));
+        }
+    }
+};
+
+// Times every activity variant on two steps from the current state (the
+// second is timed) and keeps the fastest; the state is restored after each.
+void tune_activity(Ctx& c) {
+    ActSnapshot snap(c);
+    cudaEvent_t e0, e1;
+    RL_CUDA_TRY(cudaEventCreate(&e0));
+    RL_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    ActVariant pick = c.tune.act;
+    for (const ActVariant& v : act_variants()) {
+        launch_step(c, 0, v);
+        RL_CUDA_TRY(cudaEventRecord(e0, c.stream));
+        launch_step(c, 1, v);
+        RL_CUDA_TRY(cudaEventRecord(e1, c.stream));
+        RL_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        RL_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        c.tune.act_ms.push_back(ms);
+        if (ms < best) {
+            best = ms;
+            pick = v;
+        }
+        snap.restore(c);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    c.tune.act = pick;
+}
+
 }  // namespace
+
+const std::vector<ActVariant>& act_variants() {
+    static const std::vector<ActVariant> v = [] {
+        std::vector<ActVariant> out;
+        for (int p : { 0, 1 }) {
+            for (int b : { 128, 256, 512 }) {
+                out.push_back(ActVariant{ b, p });
+            }
+        }
+        return out;
+    }();
+    return v;
+}
+
+unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel) {
+    const unsigned full = blocks_for(c.n, (unsigned)v.block);
+    if (!v.persistent) {
+        return full;
+    }
+    int per_sm = 0;
+    RL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, v.block, 0));
+    int sms = 0;
+    RL_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+    const unsigned wave = (unsigned)(per_sm > 0 ? per_sm : 1) * (unsigned)sms;
+    return full < wave ? full : wave;
+}
+
+void drop_activity_graphs(Ctx& c) {
+    for (auto& g : c.act_graph) {
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    }
+}
 
 void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     if (nsteps == 0) {
@@ -252,6 +373,14 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     const ActDesc v{ first_step, c.graph.num_edges > 0 ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p };
     k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
     RL_LAUNCH_CHECK();
+    if (c.tune.act_state == TUNE_REQUESTED) {
+        if (c.tune.force || !recall_act_tuning(c)) {
+            tune_activity(c);
+            remember_act_tuning(c);
+        }
+        c.tune.act_state = TUNE_DONE;
+        drop_activity_graphs(c);
+    }
     const bool graph = c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
     if (graph) {
         const int p = c.nr.cur & 1;
@@ -266,7 +395,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
             cudaGraph_t gr = nullptr;
             const bool timer = c.timer.on;
             c.timer.on = false;
-            const uint64_t launches = g_launches;
+            const uint64_t launches = c.launches;
             RL_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
             c.capturing = true;
             try {
@@ -285,7 +414,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
             c.capturing = false;
             RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &gr));
             c.timer.on = timer;
-            g_launches = launches;
+            c.launches = launches;
             cudaGraphExec_t ex = nullptr;
             const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
             cudaGraphDestroy(gr);
@@ -295,7 +424,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         }
         PhaseScope ps(c, PH_ACTIVITY_KERNEL, nsteps);
         RL_CUDA_TRY(cudaGraphLaunch(c.act_graph[p], c.stream));
-        g_launches += nsteps;
+        c.launches += nsteps;
     } else {
         for (uint32_t k = 0; k < nsteps; ++k) {
             PhaseScope ps(c, PH_ACTIVITY_KERNEL);

@@ -34,8 +34,6 @@
 namespace rl {
 namespace {
 
-constexpr int kWarpsPerBlock = 4;
-constexpr int kStackDepth = kMaxLevels + 4;
 
 enum : int { ST_DISCARD = 0, ST_EXPAND = 1, ST_ACCEPT = 2 };
 
@@ -136,11 +134,12 @@ struct WalkResult {
     bool overflow;
 };
 
+template <int SD>
 __device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r,
                                 double sx, double sy, double sz, uint32_t source, bool fallback) {
     WalkResult res{ start_sum, -1, 0, false };
-    uint32_t fnode[kStackDepth];
-    uint32_t frem[kStackDepth];
+    uint32_t fnode[SD];
+    uint32_t frem[SD];
     int depth = 0;
     if (include_root) {
         const double4 rr = ldg4(&A.rec[sub]);
@@ -186,7 +185,7 @@ __device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t 
                 return res;
             }
         } else if (e.status == ST_EXPAND) {
-            if (depth >= kStackDepth) {
+            if (depth >= SD) {
                 res.overflow = true;
                 return res;
             }
@@ -198,20 +197,24 @@ __device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t 
     return res;
 }
 
-// Warp-packet walk over the whole tree for the lanes in `lanes`; each lane
-// returns its sequential sum and the running sum before every root child.
-__device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t lanes, double sx, double sy, double sz, uint32_t source, bool fallback,
-                              double* cp_lane, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
+// Packet walk over the whole tree: the lanes of packet mask `pm` (a warp or
+// an aligned part of it) walk one shared depth-first stack; `lanes` are the
+// packet's active lanes.  Each lane returns its sequential sum and the running
+// sum before every root child.
+template <int SD>
+__device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz, uint32_t source,
+                              bool fallback, double* cp_lane, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
     const int lane = threadIdx.x & 31;
+    const bool leader = lane == __ffs(pm) - 1;
     const bool me = (lanes >> lane) & 1u;
     double sum = 0.0;
     const uint2 root = __ldg(&A.topo[W.root]);
-    if (lane == 0) {
+    if (leader) {
         s_node[0] = W.root;
         s_rem[0] = topo_mask(root.y);
         s_act[0] = lanes;
     }
-    __syncwarp();
+    __syncwarp(pm);
     int depth = 1;
     while (depth > 0) {
         const int top = depth - 1;
@@ -223,8 +226,8 @@ __device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t la
         const uint32_t node = s_node[top];
         const uint32_t act = s_act[top];
         const int oct = 31 - __clz(rem);
-        __syncwarp();
-        if (lane == 0) {
+        __syncwarp(pm);
+        if (leader) {
             s_rem[top] = rem & ~(1u << oct);
         }
         if (depth == 1 && me) {
@@ -244,34 +247,40 @@ __device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t la
                 sum += e.w;
             }
         }
-        const uint32_t expand = __ballot_sync(0xFFFFFFFFu, status == ST_EXPAND);
-        __syncwarp();
+        const uint32_t expand = __ballot_sync(pm, status == ST_EXPAND);
+        __syncwarp(pm);
         if (expand) {
-            if (depth >= kStackDepth) {
+            if (depth >= SD) {
                 overflow = true;
                 break;
             }
-            if (lane == 0) {
+            if (leader) {
                 s_node[depth] = child;
                 s_rem[depth] = topo_mask(tt.y);
                 s_act[depth] = expand;
             }
             ++depth;
         }
-        __syncwarp();
+        __syncwarp(pm);
     }
-    __syncwarp();
+    __syncwarp(pm);
     return sum;
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
-    __shared__ uint32_t s_node[kWarpsPerBlock][kStackDepth];
-    __shared__ uint32_t s_rem[kWarpsPerBlock][kStackDepth];
-    __shared__ uint32_t s_act[kWarpsPerBlock][kStackDepth];
-    __shared__ double s_cp[kWarpsPerBlock][8 * 32];
+// One warp handles 32 consecutive entries of the search list (Morton-adjacent
+// sources) as 32/PW packets of PW lanes.  WPB warps per block, SD stack frames.
+template <int WPB, int SD, int PW>
+__global__ void __launch_bounds__(WPB * 32) k_search(SearchArgs A) {
+    constexpr int kPackets = 32 / PW;
+    __shared__ uint32_t s_node[WPB][kPackets][SD];
+    __shared__ uint32_t s_rem[WPB][kPackets][SD];
+    __shared__ uint32_t s_act[WPB][kPackets][SD];
+    __shared__ double s_cp[WPB][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const uint32_t warp_global = blockIdx.x * kWarpsPerBlock + wib;
+    const int pk = lane / PW;
+    const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
+    const uint32_t warp_global = blockIdx.x * WPB + wib;
     if (warp_global >= A.seg_warp[A.num_segs]) {
         return;  // whole warp idle
     }
@@ -304,60 +313,62 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
     double* cp = &s_cp[wib][lane];
     uint32_t touched = 0;
     bool overflow = false;
-    uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
-
-    // ---- descent 0: warp packet over the whole tree
-    double total = packet_walk(A, W, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], touched, overflow);
-    bool fallback = false;
-    const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total == 0.0);
-    if (need_fb) {
-        uint32_t t2 = 0;
-        const double fb = packet_walk(A, W, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], t2, overflow);
-        if ((need_fb >> lane) & 1u) {
-            total = fb;
-            fallback = true;
-        }
-    }
+    const uint32_t lanes = __ballot_sync(pm, active);
     int32_t result = -1;
     bool done = !active;
-    if (active && total == 0.0) {
-        done = true;  // no candidate: the search fails
-    }
     uint32_t sub = 0;
-    if (!done) {
-        const double r = pick_threshold(total, W.seed, A.step, source - W.first, j, 0);
-        // the crossing lies in the last root-child subtree (DFS order) whose
-        // checkpoint is below r
-        const uint2 root = __ldg(&A.topo[W.root]);
-        const uint32_t mask = topo_mask(root.y);
-        int cstar = -1;
-        for (int oct = 7; oct >= 0; --oct) {
-            if ((mask >> oct) & 1u) {
-                if (cp[oct * 32] < r) {
-                    cstar = oct;
-                } else {
-                    break;
-                }
+    if (lanes) {
+        // ---- descent 0: packet walk over the whole tree
+        double total = packet_walk<SD>(A, W, pm, lanes, sx, sy, sz, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], touched, overflow);
+        bool fallback = false;
+        const uint32_t need_fb = __ballot_sync(pm, active && total == 0.0);
+        if (need_fb) {
+            uint32_t t2 = 0;
+            const double fb =
+                packet_walk<SD>(A, W, pm, need_fb, sx, sy, sz, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], t2, overflow);
+            if ((need_fb >> lane) & 1u) {
+                total = fb;
+                fallback = true;
             }
         }
-        if (cstar < 0) {
-            atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
-            done = true;
-        } else {
-            const uint32_t c0 = child_index(root, cstar);
-            const WalkResult wr = lane_walk(A, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
-            overflow |= wr.overflow;
-            if (wr.picked < 0) {
+        if (active && total == 0.0) {
+            done = true;  // no candidate: the search fails
+        }
+        if (!done) {
+            const double r = pick_threshold(total, W.seed, A.step, source - W.first, j, 0);
+            // the crossing lies in the last root-child subtree (DFS order) whose
+            // checkpoint is below r
+            const uint2 root = __ldg(&A.topo[W.root]);
+            const uint32_t mask = topo_mask(root.y);
+            int cstar = -1;
+            for (int oct = 7; oct >= 0; --oct) {
+                if ((mask >> oct) & 1u) {
+                    if (cp[oct * 32] < r) {
+                        cstar = oct;
+                    } else {
+                        break;
+                    }
+                }
+            }
+            if (cstar < 0) {
                 atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
                 done = true;
             } else {
-                sub = (uint32_t)wr.picked;
+                const uint32_t c0 = child_index(root, cstar);
+                const WalkResult wr = lane_walk<SD>(A, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
+                overflow |= wr.overflow;
+                if (wr.picked < 0) {
+                    atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
+                    done = true;
+                } else {
+                    sub = (uint32_t)wr.picked;
+                }
             }
         }
     }
     // ---- deeper descents, per lane
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > (uint32_t)kStackDepth) {
+        if (depth > (uint32_t)SD) {
             overflow = true;  // a descent always moves one level down; cannot recur this often
             break;
         }
@@ -367,11 +378,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
             done = true;
             break;
         }
-        WalkResult s1 = lane_walk(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
+        WalkResult s1 = lane_walk<SD>(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
         touched += s1.touched;
         bool fb = false;
         if (s1.sum == 0.0) {
-            s1 = lane_walk(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
+            s1 = lane_walk<SD>(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
             fb = true;
         }
         overflow |= s1.overflow;
@@ -380,7 +391,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
             break;
         }
         const double r = pick_threshold(s1.sum, W.seed, A.step, source - W.first, j, depth);
-        const WalkResult s2 = lane_walk(A, W, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
+        const WalkResult s2 = lane_walk<SD>(A, W, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
         if (s2.picked < 0) {
             atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
             done = true;
@@ -403,6 +414,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_search(SearchArgs A) {
     if (lane == 0) {
         atomicAdd(A.touched, t);
     }
+}
+
+using SearchKernel = void (*)(SearchArgs);
+
+// The search variants the tuner chooses from, indexed by SearchVariant.
+template <int WPB, int SD, int PW>
+constexpr SearchKernel search_kernel() {
+    return &k_search<WPB, SD, PW>;
+}
+
+SearchKernel fp64_search_kernel(const SearchVariant& v) {
+#define RL_SV(w, s, p)                                  \
+    if (v.warps == w && v.stack == s && v.packet == p) { \
+        return search_kernel<w, s, p>();                 \
+    }
+    RL_SV(2, 24, 32) RL_SV(4, 24, 32) RL_SV(8, 24, 32) RL_SV(2, 48, 32) RL_SV(4, 48, 32) RL_SV(8, 48, 32)
+    RL_SV(2, 24, 16) RL_SV(4, 24, 16) RL_SV(8, 24, 16) RL_SV(2, 48, 16) RL_SV(4, 48, 16) RL_SV(8, 48, 16)
+#undef RL_SV
+    return nullptr;
 }
 
 // ---------------------------------------------------------- search list
@@ -496,6 +526,60 @@ __global__ void k_req_scatter(uint64_t m, const uint32_t* __restrict__ list_src,
 
 }  // namespace
 
+// Times every search variant that fits the octree on the current search list
+// and keeps the fastest.  Each variant runs twice (the second run is timed);
+// the searches are deterministic, so the variants leave the same targets, and
+// the touched-node counter is restored afterwards.
+template <typename F>
+void tune_search(Ctx& c, F&& launch_all) {
+    cudaStream_t st = c.stream;
+    std::vector<uint64_t> saved(4);
+    RL_CUDA_TRY(cudaMemcpyAsync(saved.data(), c.counters.p, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaEvent_t e0, e1;
+    RL_CUDA_TRY(cudaEventCreate(&e0));
+    RL_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    SearchVariant pick = c.tune.search;
+    for (const SearchVariant& v : search_variants()) {
+        if ((uint32_t)v.stack < c.tree.max_level + 2) {
+            continue;  // the stacks must hold a walk from the root to the deepest leaf
+        }
+        launch_all(v);
+        RL_CUDA_TRY(cudaEventRecord(e0, st));
+        launch_all(v);
+        RL_CUDA_TRY(cudaEventRecord(e1, st));
+        RL_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        RL_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        c.tune.search_ms.push_back(ms);
+        if (ms < best) {
+            best = ms;
+            pick = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    RL_CUDA_TRY(cudaMemcpyAsync(c.counters.p, saved.data(), 4 * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    c.tune.search = pick;
+}
+
+const std::vector<SearchVariant>& search_variants() {
+    static const std::vector<SearchVariant> v = [] {
+        std::vector<SearchVariant> out;
+        for (int p : { 32, 16 }) {
+            for (int s : { 24, 48 }) {
+                for (int w : { 2, 4, 8 }) {
+                    out.push_back(SearchVariant{ w, s, p });
+                }
+            }
+        }
+        return out;
+    }();
+    return v;
+}
+
 void run_search(Ctx& c, uint32_t step) {
     const uint32_t n = c.n;
     cudaStream_t st = c.stream;
@@ -533,6 +617,13 @@ void run_search(Ctx& c, uint32_t step) {
         if (is_fp32(c)) {
             pack_tree_f32(c);
         }
+        struct SearchLaunch {
+            bool on = false;
+            uint32_t warps = 0;
+            uint32_t segs = 0;
+        };
+        SearchLaunch launches[2];
+        SearchArgs args[2];
         for (int t = 0; t < 2; ++t) {
             const uint64_t base = t == 0 ? 0 : num_exc;
             const uint64_t total = t == 0 ? num_exc : num_inh;
@@ -561,12 +652,14 @@ void run_search(Ctx& c, uint32_t step) {
             RL_CUDA_TRY(cudaMemcpyAsync(S.seg_end[t].p, endv.data(), segs * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
             RL_CUDA_TRY(cudaMemcpyAsync(S.seg_net[t].p, net.data(), segs * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
             const uint32_t warps = warp.back();
-            const unsigned blocks = (warps + kWarpsPerBlock - 1) / kWarpsPerBlock;
+            SearchLaunch& L = launches[t];
+            L.on = true;
+            L.warps = warps;
+            L.segs = segs;
             if (is_fp32(c)) {
-                launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, segs, warps, step);
                 continue;
             }
-            SearchArgs A;
+            SearchArgs& A = args[t];
             A.rec = c.tree.rec[t].p;
             A.topo = c.tree.topo.p;
             A.maxdim = c.tree.maxdim.p;
@@ -586,9 +679,33 @@ void run_search(Ctx& c, uint32_t step) {
             A.step = step;
             A.err = c.err.p;
             A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
+        }
+        auto launch_all = [&](const SearchVariant& v) {
+            for (int t = 0; t < 2; ++t) {
+                if (!launches[t].on) {
+                    continue;
+                }
+                if (is_fp32(c)) {
+                    launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, launches[t].segs, launches[t].warps, step, v);
+                } else {
+                    const SearchKernel kern = fp64_search_kernel(v);
+                    RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");
+                    const unsigned blocks = (launches[t].warps + v.warps - 1) / v.warps;
+                    kern<<<blocks, v.warps * 32, 0, st>>>(args[t]);
+                    RL_LAUNCH_CHECK();
+                }
+            }
+        };
+        if (c.tune.search_state == TUNE_REQUESTED) {
+            if (c.tune.force || !recall_search_tuning(c)) {
+                tune_search(c, launch_all);
+                remember_search_tuning(c);
+            }
+            c.tune.search_state = TUNE_DONE;
+        }
+        {
             PhaseScope ps(c, PH_SEARCH_KERNEL);
-            k_search<<<blocks, kWarpsPerBlock * 32, 0, st>>>(A);
-            RL_LAUNCH_CHECK();
+            launch_all(c.tune.search);
         }
         k_first_fail<<<blocks_for(m, 256), 256, 0, st>>>(m, S.src.p, S.jj.p, S.target.p, S.first_fail.p);
         RL_LAUNCH_CHECK();

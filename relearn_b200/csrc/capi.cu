@@ -1,4 +1,8 @@
 // C ABI of librelearn_b200 (declared in include/relearn_b200.h).
+#include <atomic>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -7,6 +11,11 @@
 #include "rl_context.cuh"
 
 namespace rl {
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_live[kMaxDevices];  // contexts alive per device
+}  // namespace
 
 PhaseScope::PhaseScope(Ctx& ctx, int ph, uint32_t weight) : c(&ctx), phase(ph) {
     if (!c->timer.on || c->capturing) {
@@ -196,6 +205,17 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     RL_CUDA_TRY(cudaSetDevice(k.device));
     RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
     c.stream = c.own_stream;
+    g_bind = Binding{ c.stream, &c.launches, &c.device_bytes, &c.device_peak };
+    RL_CHECK(k.device < kMaxDevices, RL_ERR_DEVICE, "device ordinal above what this build tracks");
+    {
+        // keep freed device memory in the pool for the next context or buffer
+        cudaMemPool_t pool;
+        RL_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, k.device));
+        uint64_t keep = UINT64_MAX;
+        RL_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    g_live[k.device].fetch_add(1);
+    c.counted = true;
     const size_t n = c.n;
     Neurons& N = c.nr;
     N.px.alloc(n);
@@ -288,9 +308,66 @@ void plasticity_update(Ctx& c, uint32_t step) {
     c.stats.plasticity_updates += 1;
 }
 
+}  // namespace
+
+// ------------------------------------------------------------ tuning cache
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, SearchVariant> g_search_shapes;
+std::map<std::tuple<int, int, int>, ActVariant> g_act_shapes;
+
+std::tuple<int, int, int> tune_key(const Ctx& c) {
+    int lg = 0;
+    while (lg < 40 && (1ull << (lg + 1)) <= (uint64_t)c.n) {
+        ++lg;
+    }
+    return std::make_tuple(c.cfg.precision, c.multi() ? 1 : 0, lg);
+}
+}  // namespace
+
+void remember_search_tuning(const Ctx& c) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_search_shapes[tune_key(c)] = c.tune.search;
+}
+
+bool recall_search_tuning(Ctx& c) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_search_shapes.find(tune_key(c));
+    if (it == g_search_shapes.end() || (uint32_t)it->second.stack < c.tree.max_level + 2) {
+        return false;
+    }
+    c.tune.search = it->second;
+    return true;
+}
+
+void remember_act_tuning(const Ctx& c) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_act_shapes[tune_key(c)] = c.tune.act;
+}
+
+bool recall_act_tuning(Ctx& c) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_act_shapes.find(tune_key(c));
+    if (it == g_act_shapes.end()) {
+        return false;
+    }
+    c.tune.act = it->second;
+    return true;
+}
+
+namespace {
+
 Ctx* as_ctx(void* p) {
     return static_cast<Ctx*>(p);
 }
+
+// Binds a context to the calling thread for one entry point.
+struct Bind {
+    explicit Bind(Ctx& c) { g_bind = Binding{ c.stream, &c.launches, &c.device_bytes, &c.device_peak }; }
+    ~Bind() { g_bind = Binding{}; }
+    Bind(const Bind&) = delete;
+    Bind& operator=(const Bind&) = delete;
+};
 
 template <typename F>
 rl_status guarded(void* ctx, F&& f) {
@@ -298,6 +375,7 @@ rl_status guarded(void* ctx, F&& f) {
         return RL_ERR_INVALID;
     }
     Ctx& c = *as_ctx(ctx);
+    Bind bind(c);
     try {
         RL_CUDA_TRY(cudaSetDevice(c.device));
         f(c);
@@ -388,9 +466,10 @@ rl_status rl_ctx_create(const rl_config* cfg, void** out) {
         rl::create(*c, *cfg);
     } catch (const rl::Error& e) {
         std::fprintf(stderr, "rl_ctx_create: %s\n", e.message.c_str());
-        delete c;
+        rl::discard(c);
         return e.status;
     }
+    rl::g_bind = rl::Binding{};
     *out = c;
     return RL_OK;
 }
@@ -422,9 +501,10 @@ rl_status rl_ensemble_create(const rl_config* base, const rl_network* networks, 
         rl::create(*c, cfg, networks, num_networks);
     } catch (const rl::Error& e) {
         std::fprintf(stderr, "rl_ensemble_create: %s\n", e.message.c_str());
-        delete c;
+        rl::discard(c);
         return e.status;
     }
+    rl::g_bind = rl::Binding{};
     *out = c;
     return RL_OK;
 }
@@ -433,8 +513,17 @@ rl_status rl_ctx_destroy(void* ctx) {
     if (!ctx) {
         return RL_ERR_INVALID;
     }
-    Ctx* c = static_cast<Ctx*>(ctx);
+    rl::discard(static_cast<Ctx*>(ctx));
+    return RL_OK;
+}
+
+}  // extern "C"
+
+namespace rl {
+
+void discard(Ctx* c) {
     cudaSetDevice(c->device);
+    g_bind = Binding{ c->stream, &c->launches, &c->device_bytes, &c->device_peak };
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
     }
@@ -452,12 +541,33 @@ rl_status rl_ctx_destroy(void* ctx) {
             cudaGraphExecDestroy(g);
         }
     }
-    if (c->own_stream) {
-        cudaStreamDestroy(c->own_stream);
-    }
+    // device buffers are freed on their streams; the context's own stream
+    // goes last
+    cudaStream_t own = c->own_stream;
+    cudaStream_t last = c->stream;
+    const int dev = c->device;
+    const bool counted = c->counted;
     delete c;
-    return RL_OK;
+    g_bind = Binding{};
+    if (last) {
+        cudaStreamSynchronize(last);
+    }
+    if (own) {
+        cudaStreamDestroy(own);
+    }
+    // the pool keeps freed memory for the next context; give it back to the
+    // device when the last context of the device is gone
+    if (counted && dev >= 0 && dev < kMaxDevices && g_live[dev].fetch_sub(1) == 1) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            cudaMemPoolTrimTo(pool, 0);
+        }
+    }
 }
+
+}  // namespace rl
+
+extern "C" {
 
 const char* rl_last_error(void* ctx) {
     return ctx ? static_cast<Ctx*>(ctx)->last_error.c_str() : "null context";
@@ -764,11 +874,77 @@ rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts) {
     });
 }
 
+rl_status rl_autotune(void* ctx, int mode) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(mode >= 0 && mode <= 2, RL_ERR_INVALID, "autotune mode must be 0, 1 or 2");
+        c.tune.force = mode == 2;
+        const int st = mode == 0 ? rl::TUNE_OFF : rl::TUNE_REQUESTED;
+        c.tune.search_state = st;
+        c.tune.act_state = st;
+        if (mode != 0) {
+            c.tune.search_ms.clear();
+            c.tune.act_ms.clear();
+        }
+    });
+}
+
+rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_ms) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(out != nullptr, RL_ERR_INVALID, "null output");
+        out->search_warps = c.tune.search.warps;
+        out->search_stack = c.tune.search.stack;
+        out->search_packet = c.tune.search.packet;
+        out->act_block = c.tune.act.block;
+        out->act_persistent = c.tune.act.persistent;
+        out->tuned = (c.tune.search_state == rl::TUNE_DONE ? 1 : 0) | (c.tune.act_state == rl::TUNE_DONE ? 2 : 0);
+        // times are recorded for the shapes that fit, in candidate order
+        if (search_ms) {
+            size_t k = 0;
+            for (size_t v = 0; v < rl::search_variants().size(); ++v) {
+                const bool fits = (uint32_t)rl::search_variants()[v].stack >= c.tree.max_level + 2;
+                search_ms[v] = fits && k < c.tune.search_ms.size() ? c.tune.search_ms[k++] : 0.0f;
+            }
+        }
+        if (act_ms) {
+            for (size_t v = 0; v < rl::act_variants().size(); ++v) {
+                act_ms[v] = v < c.tune.act_ms.size() ? c.tune.act_ms[v] : 0.0f;
+            }
+        }
+    });
+}
+
+rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(t != nullptr, RL_ERR_INVALID, "null tuning");
+        bool s_ok = false, a_ok = false;
+        for (const auto& v : rl::search_variants()) {
+            s_ok = s_ok || (v.warps == t->search_warps && v.stack == t->search_stack && v.packet == t->search_packet);
+        }
+        for (const auto& v : rl::act_variants()) {
+            a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent);
+        }
+        RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
+        RL_CHECK(!c.positions_set || (uint32_t)t->search_stack >= c.tree.max_level + 2, RL_ERR_INVALID, "search stack shallower than the octree");
+        c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet };
+        c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent };
+        c.tune.search_state = rl::TUNE_OFF;
+        c.tune.act_state = rl::TUNE_OFF;
+        rl::drop_activity_graphs(c);
+    });
+}
+
+rl_status rl_ctx_memory(void* ctx, uint64_t* current, uint64_t* peak) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        if (current) *current = (uint64_t)c.device_bytes;
+        if (peak) *peak = (uint64_t)c.device_peak;
+    });
+}
+
 rl_status rl_get_stats(void* ctx, rl_stats* out) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(out != nullptr, RL_ERR_INVALID, "null output");
         *out = c.stats;
-        out->gpu_launches = rl::g_launches;
+        out->gpu_launches = c.launches;
         out->num_nodes = c.tree.num_nodes;
         out->max_level = c.tree.max_level;
     });

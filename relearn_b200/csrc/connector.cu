@@ -358,13 +358,9 @@ uint64_t run_connector(Ctx& c, uint32_t step) {
             RL_CUDA_TRY(cudaMemcpyAsync(s2.p, G.new_src.p, G.num_new * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
             RL_CUDA_TRY(cudaMemcpyAsync(w2.p, G.new_w.p, G.num_new * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
         }
-        RL_CUDA_TRY(cudaStreamSynchronize(st));
-        std::swap(G.new_tgt.p, t2.p);
-        std::swap(G.new_tgt.n, t2.n);
-        std::swap(G.new_src.p, s2.p);
-        std::swap(G.new_src.n, s2.n);
-        std::swap(G.new_w.p, w2.p);
-        std::swap(G.new_w.n, w2.n);
+        G.new_tgt.swap(t2);
+        G.new_src.swap(s2);
+        G.new_w.swap(w2);
     }
     k_emit_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, S.accepted.p, pos.p, S.cidx.p, S.req_tgt.p, S.req_src.p, S.req_sig.p, G.num_new, G.new_tgt.p,
                                                      G.new_src.p, G.new_w.p);
@@ -508,13 +504,9 @@ uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
         w2.alloc(kept ? kept : 1);
         k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, pos.p, G.tgt.p, G.src.p, G.weight.p, t2.p, s2.p, w2.p);
         RL_LAUNCH_CHECK();
-        RL_CUDA_TRY(cudaStreamSynchronize(st));
-        std::swap(G.tgt.p, t2.p);
-        std::swap(G.tgt.n, t2.n);
-        std::swap(G.src.p, s2.p);
-        std::swap(G.src.n, s2.n);
-        std::swap(G.weight.p, w2.p);
-        std::swap(G.weight.n, w2.n);
+        G.tgt.swap(t2);
+        G.src.swap(s2);
+        G.weight.swap(w2);
         finish_graph(c, kept);
     }
     RL_CUDA_TRY(cudaStreamSynchronize(st));
@@ -545,12 +537,9 @@ void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, co
     RL_CUDA_TRY(cudaMemcpyAsync(s2.p + G.num_new, s, m * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     RL_CUDA_TRY(cudaMemcpyAsync(w2.p + G.num_new, w, m * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     RL_CUDA_TRY(cudaStreamSynchronize(st));
-    std::swap(G.new_tgt.p, t2.p);
-    std::swap(G.new_tgt.n, t2.n);
-    std::swap(G.new_src.p, s2.p);
-    std::swap(G.new_src.n, s2.n);
-    std::swap(G.new_w.p, w2.p);
-    std::swap(G.new_w.n, w2.n);
+    G.new_tgt.swap(t2);
+    G.new_src.swap(s2);
+    G.new_w.swap(w2);
     G.num_new = need;
     rebuild_graph(c);
 }

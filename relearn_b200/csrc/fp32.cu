@@ -56,7 +56,10 @@ struct Act32 {
     float* delta[3];
     float conductance, noise_mean, noise_stddev;
     uint32_t h_model;
-    float a, ab, c, d, v_spike, k1, k2, k3, scale_m;
+    // one Euler substep with s = 1/h, rearranged to five FP32 operations:
+    //   x' = x (1 + s k2 + s k1 x) + s (k3 + I) - s u
+    //   u' = u (1 - s a) + s a b x
+    float c, d, v_spike, s, sk1, one_sk2, sk3, sab, one_sa;
     double ca_mul, ca_add;  // calcium: c <- c*ca_mul + fired*ca_add
     float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
@@ -100,11 +103,7 @@ __device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
 }
 
 template <int H>
-__global__ void __launch_bounds__(256) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) {
-        return;
-    }
+__device__ __forceinline__ void activity_neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
     const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
         A.input[i] = 0.0f;
@@ -133,12 +132,13 @@ __global__ void __launch_bounds__(256) k_activity_f32(Act32 A, const ActDesc* __
     float uv = A.u[i];
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
+    const float sI = fmaf(A.s, input, A.sk3);
+    const float ms = -A.s;
 #pragma unroll
     for (uint32_t it = 0; it < h; ++it) {
-        const float x_inc = fmaf(A.k1 * xv, xv, fmaf(A.k2, xv, A.k3)) - uv + input;
-        const float u_inc = fmaf(A.ab, xv, -A.a * uv);
-        xv = fmaf(x_inc, A.scale_m, xv);
-        uv = fmaf(u_inc, A.scale_m, uv);
+        const float xn = fmaf(xv, fmaf(A.sk1, xv, A.one_sk2), fmaf(ms, uv, sI));
+        uv = fmaf(A.sab, xv, uv * A.one_sa);
+        xv = xn;
         if (xv >= A.v_spike) {
             xv = A.c;
             uv += A.d;
@@ -163,6 +163,16 @@ __global__ void __launch_bounds__(256) k_activity_f32(Act32 A, const ActDesc* __
             dz = fmaf(2.0f, __expf(-q * q), -1.0f);
         }
         A.delta[t][i] = fmaf(dz, N.nu32[t], A.delta[t][i]);
+    }
+}
+
+// H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
+// block, striding over the neurons when the grid is one resident wave.
+template <int H, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
+        activity_neuron_f32<H>(A, D, k, i);
     }
 }
 
@@ -222,8 +232,7 @@ __global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4
 }
 
 // ----------------------------------------------------------- search
-constexpr int kWarps = 4;
-constexpr int kStack = kMaxLevels + 4;
+constexpr int kStack = kMaxLevels + 4;  // the diagnostic walk
 enum : int { S_DISCARD = 0, S_EXPAND = 1, S_ACCEPT = 2 };
 
 struct Search32 {
@@ -314,11 +323,12 @@ struct Walk32 {
     bool overflow;
 };
 
+template <int SD>
 __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, float sx, float sy,
                               float sz, uint32_t source, bool fb) {
     Walk32 res{ start, -1, false };
-    uint32_t fnode[kStack];
-    uint32_t frem[kStack];
+    uint32_t fnode[SD];
+    uint32_t frem[SD];
     if (include_root) {
         const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sx, sy, sz, source, A, W, fb);
         if (e.status == S_ACCEPT) {
@@ -354,7 +364,7 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
                 return res;
             }
         } else if (e.status == S_EXPAND) {
-            if (depth >= kStack) {
+            if (depth >= SD) {
                 res.overflow = true;
                 return res;
             }
@@ -366,17 +376,20 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
     return res;
 }
 
-__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb, float2* cp,
-                         uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
+// Packet walk of the lanes in packet mask `pm` (see the FP64 search).
+template <int SD>
+__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb,
+                         float2* cp, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
     const int lane = threadIdx.x & 31;
+    const bool leader = lane == __ffs(pm) - 1;
     const bool me = (lanes >> lane) & 1u;
     KSum sum{ 0.0f, 0.0f };
-    if (lane == 0) {
+    if (leader) {
         s_node[0] = W.root;
         s_rem[0] = topo_mask(A.topo[W.root].y);
         s_act[0] = lanes;
     }
-    __syncwarp();
+    __syncwarp(pm);
     int depth = 1;
     while (depth > 0) {
         const int top = depth - 1;
@@ -388,8 +401,8 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t lanes, floa
         const uint32_t node = s_node[top];
         const uint32_t act = s_act[top];
         const int oct = 31 - __clz(rem);
-        __syncwarp();
-        if (lane == 0) {
+        __syncwarp(pm);
+        if (leader) {
             s_rem[top] = rem & ~(1u << oct);
         }
         if (depth == 1 && me) {
@@ -407,34 +420,38 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t lanes, floa
                 sum.add(e.w);
             }
         }
-        const uint32_t expand = __ballot_sync(0xFFFFFFFFu, status == S_EXPAND);
-        __syncwarp();
+        const uint32_t expand = __ballot_sync(pm, status == S_EXPAND);
+        __syncwarp(pm);
         if (expand) {
-            if (depth >= kStack) {
+            if (depth >= SD) {
                 overflow = true;
                 break;
             }
-            if (lane == 0) {
+            if (leader) {
                 s_node[depth] = child;
                 s_rem[depth] = topo_mask(tt.y);
                 s_act[depth] = expand;
             }
             ++depth;
         }
-        __syncwarp();
+        __syncwarp(pm);
     }
-    __syncwarp();
+    __syncwarp(pm);
     return sum;
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
-    __shared__ uint32_t s_node[kWarps][kStack];
-    __shared__ uint32_t s_rem[kWarps][kStack];
-    __shared__ uint32_t s_act[kWarps][kStack];
-    __shared__ float2 s_cp[kWarps][8 * 32];
+template <int WPB, int SD, int PW>
+__global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
+    constexpr int kPackets = 32 / PW;
+    __shared__ uint32_t s_node[WPB][kPackets][SD];
+    __shared__ uint32_t s_rem[WPB][kPackets][SD];
+    __shared__ uint32_t s_act[WPB][kPackets][SD];
+    __shared__ float2 s_cp[WPB][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const uint32_t warp_global = blockIdx.x * kWarps + wib;
+    const int pk = lane / PW;
+    const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
+    const uint32_t warp_global = blockIdx.x * WPB + wib;
     if (warp_global >= A.seg_warp[A.num_segs]) {
         return;
     }
@@ -464,49 +481,52 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
     const float sz = active ? (float)A.pz[source] : 0.0f;
     float2* cp = &s_cp[wib][lane];
     bool overflow = false;
-    const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, active);
-    KSum total = packet32(A, W, lanes, sx, sy, sz, source, false, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
-    bool fb = false;
-    const uint32_t need_fb = __ballot_sync(0xFFFFFFFFu, active && total.s == 0.0f);
-    if (need_fb) {
-        const KSum t2 = packet32(A, W, need_fb, sx, sy, sz, source, true, cp, s_node[wib], s_rem[wib], s_act[wib], overflow);
-        if ((need_fb >> lane) & 1u) {
-            total = t2;
-            fb = true;
-        }
-    }
+    const uint32_t lanes = __ballot_sync(pm, active);
     int32_t result = -1;
-    bool done = !active || total.s == 0.0f;
+    bool done = !active;
     uint32_t sub = 0;
-    if (!done) {
-        const float r = threshold32(total.s, A, W, source, j, 0);
-        const uint2 root = A.topo[W.root];
-        const uint32_t mask = topo_mask(root.y);
-        int cstar = -1;
-        for (int oct = 7; oct >= 0; --oct) {
-            if ((mask >> oct) & 1u) {
-                if (cp[oct * 32].x < r) {
-                    cstar = oct;
-                } else {
-                    break;
-                }
+    if (lanes) {
+        KSum total = packet32<SD>(A, W, pm, lanes, sx, sy, sz, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+        bool fb = false;
+        const uint32_t need_fb = __ballot_sync(pm, active && total.s == 0.0f);
+        if (need_fb) {
+            const KSum t2 = packet32<SD>(A, W, pm, need_fb, sx, sy, sz, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+            if ((need_fb >> lane) & 1u) {
+                total = t2;
+                fb = true;
             }
         }
-        if (cstar < 0) {
-            done = true;
-        } else {
-            const float2 c0 = cp[cstar * 32];
-            const Walk32 wr = lane_walk32(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
-            overflow |= wr.overflow;
-            if (wr.picked < 0) {
-                done = true;  // rounding left the crossing past the last candidate: no pick
+        done = done || total.s == 0.0f;
+        if (!done) {
+            const float r = threshold32(total.s, A, W, source, j, 0);
+            const uint2 root = A.topo[W.root];
+            const uint32_t mask = topo_mask(root.y);
+            int cstar = -1;
+            for (int oct = 7; oct >= 0; --oct) {
+                if ((mask >> oct) & 1u) {
+                    if (cp[oct * 32].x < r) {
+                        cstar = oct;
+                    } else {
+                        break;
+                    }
+                }
+            }
+            if (cstar < 0) {
+                done = true;
             } else {
-                sub = (uint32_t)wr.picked;
+                const float2 c0 = cp[cstar * 32];
+                const Walk32 wr = lane_walk32<SD>(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
+                overflow |= wr.overflow;
+                if (wr.picked < 0) {
+                    done = true;  // rounding left the crossing past the last candidate: no pick
+                } else {
+                    sub = (uint32_t)wr.picked;
+                }
             }
         }
     }
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > (uint32_t)kStack) {
+        if (depth > (uint32_t)SD) {
             overflow = true;
             break;
         }
@@ -515,10 +535,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
             result = (int32_t)st.x;
             break;
         }
-        Walk32 s1 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
+        Walk32 s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
         bool f = false;
         if (s1.sum.s == 0.0f) {
-            s1 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
+            s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
             f = true;
         }
         overflow |= s1.overflow;
@@ -526,7 +546,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
             break;
         }
         const float r = threshold32(s1.sum.s, A, W, source, j, depth);
-        const Walk32 s2 = lane_walk32(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
+        const Walk32 s2 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
         if (s2.picked < 0) {
             break;
         }
@@ -539,6 +559,19 @@ __global__ void __launch_bounds__(kWarps * 32) k_search_f32(Search32 A) {
     if (active) {
         A.target[idx] = result;
     }
+}
+
+using Search32Kernel = void (*)(Search32);
+
+Search32Kernel fp32_search_kernel(const SearchVariant& v) {
+#define RL_SV(w, s, p)                                  \
+    if (v.warps == w && v.stack == s && v.packet == p) { \
+        return &k_search_f32<w, s, p>;                   \
+    }
+    RL_SV(2, 24, 32) RL_SV(4, 24, 32) RL_SV(8, 24, 32) RL_SV(2, 48, 32) RL_SV(4, 48, 32) RL_SV(8, 48, 32)
+    RL_SV(2, 24, 16) RL_SV(4, 24, 16) RL_SV(8, 24, 16) RL_SV(2, 48, 16) RL_SV(4, 48, 16) RL_SV(8, 48, 16)
+#undef RL_SV
+    return nullptr;
 }
 
 // ----------------------------------------------------------- diagnostic
@@ -660,7 +693,27 @@ void f64_from_f32(Ctx& c) {
     }
 }
 
-void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
+template <int H, int BLOCK>
+void launch_act32(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
+    k_activity_f32<H, BLOCK><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+}
+
+template <int H>
+void launch_act32_h(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
+    switch (v.block) {
+        case 128:
+            launch_act32<H, 128>(c, v, A, kstep);
+            break;
+        case 512:
+            launch_act32<H, 512>(c, v, A, kstep);
+            break;
+        default:
+            launch_act32<H, 256>(c, v, A, kstep);
+            break;
+    }
+}
+
+void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
     const rl_config& k = c.cfg;
     Act32 A;
     A.n = c.n;
@@ -678,15 +731,16 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     A.noise_mean = (float)k.noise_mean;
     A.noise_stddev = (float)k.noise_stddev;
     A.h_model = k.h_model;
-    A.a = (float)k.iz_a;
-    A.ab = (float)(k.iz_a * k.iz_b);
+    const double sm = 1.0 / (double)k.h_model;
+    A.s = (float)sm;
+    A.sk1 = (float)(sm * k.iz_k1);
+    A.one_sk2 = (float)(1.0 + sm * k.iz_k2);
+    A.sk3 = (float)(sm * k.iz_k3);
+    A.sab = (float)(sm * k.iz_a * k.iz_b);
+    A.one_sa = (float)(1.0 - sm * k.iz_a);
     A.c = (float)k.iz_c;
     A.d = (float)k.iz_d;
     A.v_spike = (float)k.iz_v_spike;
-    A.k1 = (float)k.iz_k1;
-    A.k2 = (float)k.iz_k2;
-    A.k3 = (float)k.iz_k3;
-    A.scale_m = (float)(1.0 / (double)k.h_model);
     // h calcium substeps c <- c*a + b at once
     const long double s = 1.0L / (long double)k.h_calcium;
     const long double a = 1.0L + s * (-1.0L / (long double)k.tau_c);
@@ -709,9 +763,9 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
     if (k.h_model == 10) {
-        k_activity_f32<10><<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+        launch_act32_h<10>(c, v, A, kstep);
     } else {
-        k_activity_f32<0><<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+        launch_act32_h<0>(c, v, A, kstep);
     }
     RL_LAUNCH_CHECK();
 }
@@ -740,7 +794,7 @@ void pack_tree_f32(Ctx& c) {
 }
 
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
-                       uint32_t num_segs, uint32_t warps, uint32_t step) {
+                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v) {
     Search32 A;
     A.rec = c.tree.rec32[type].p;
     A.topo = c.tree.topo.p;
@@ -760,9 +814,10 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     A.mu = (float)c.cfg.mu;
     A.step = step;
     A.err = c.err.p;
-    const unsigned blocks = (warps + kWarps - 1) / kWarps;
-    PhaseScope ps(c, PH_SEARCH_KERNEL);
-    k_search_f32<<<blocks, kWarps * 32, 0, c.stream>>>(A);
+    const Search32Kernel kern = fp32_search_kernel(v);
+    RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");
+    const unsigned blocks = (warps + v.warps - 1) / v.warps;
+    kern<<<blocks, v.warps * 32, 0, c.stream>>>(A);
     RL_LAUNCH_CHECK();
 }
 

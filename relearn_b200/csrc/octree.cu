@@ -403,9 +403,33 @@ struct ReduceArgs {
     uint32_t* arrive;
 };
 
+// One level of the bottom-up reduction: one thread per node of the level; an
+// inner node is computed from its children (the next level, finished by the
+// previous launch), read in octant order as the reference sums them.  The
+// children of a node are contiguous, so neighbouring threads read neighbouring
+// records.
+__global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
+    const uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= hi) {
+        return;
+    }
+    const uint2 t = A.topo[node];
+    if (topo_leaf(t.y)) {
+        return;
+    }
+    const uint32_t mask = topo_mask(t.y);
+    const double lx = A.bx0[node], ly = A.by0[node], lz = A.bz0[node];
+    const double hx = A.bx1[node], hy = A.by1[node], hz = A.bz1[node];
+    const double4 r0 = update_type(A.rec0, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
+    const double4 r1 = update_type(A.rec1, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
+    stcg4(&A.rec0[node], r0);
+    stcg4(&A.rec1[node], r1);
+}
+
 // One thread per leaf walks up; the last child to arrive at a node computes
 // it (reading all children in octant order), so every node is computed once
-// and in the reference's summation order.
+// and in the reference's summation order.  Used by the allocation-free entry
+// point, whose only scratch is the arrival counters.
 __global__ void k_reduce(ReduceArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) {
@@ -532,7 +556,6 @@ void build_octree(Ctx& c, const double* h_xyz) {
     T.first_key.alloc(m);
     T.leaf_of.alloc(n);
     T.morton.alloc(n);
-    T.arrive.alloc(m);
     RL_CUDA_TRY(cudaMemcpyAsync(T.morton.p, idx.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
 
     DBuf<uint32_t> level_count;
@@ -576,6 +599,7 @@ void build_octree(Ctx& c, const double* h_xyz) {
     for (int l = 0; l < kMaxLevels + 2; ++l) {
         hoff[l + 1] = hoff[l] + hcount[l];
     }
+    T.level_off = hoff;
     DBuf<uint32_t> level_off;
     level_off.alloc(hoff.size());
     RL_CUDA_TRY(cudaMemcpyAsync(level_off.p, hoff.data(), hoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -609,7 +633,6 @@ void update_tree(Ctx& c) {
     if (T.root_is_leaf) {
         return;
     }
-    RL_CUDA_TRY(cudaMemsetAsync(T.arrive.p, 0, T.num_nodes * sizeof(uint32_t), st));
     ReduceArgs A;
     A.n = n;
     A.leaf_of = T.leaf_of.p;
@@ -623,9 +646,19 @@ void update_tree(Ctx& c) {
     A.bz1 = T.bmax[2].p;
     A.rec0 = T.rec[0].p;
     A.rec1 = T.rec[1].p;
-    A.arrive = T.arrive.p;
-    k_reduce<<<blocks_for(n, 128), 128, 0, st>>>(A);
-    RL_LAUNCH_CHECK();
+    A.arrive = nullptr;
+    // bottom-up, one launch per level; the deepest non-empty level holds leaves only
+    int deepest = (int)T.level_off.size() - 2;
+    while (deepest > 0 && T.level_off[deepest + 1] == T.level_off[deepest]) {
+        --deepest;
+    }
+    for (int l = deepest - 1; l >= 0; --l) {
+        const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
+        if (hi > lo) {
+            k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(A, lo, hi);
+            RL_LAUNCH_CHECK();
+        }
+    }
 }
 
 void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_t* d_vac_inh, const uint8_t* d_update, uint32_t* arrive,

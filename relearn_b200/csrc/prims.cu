@@ -11,7 +11,7 @@
 
 namespace rl {
 
-uint64_t g_launches = 0;
+thread_local Binding g_bind;
 
 
 namespace {

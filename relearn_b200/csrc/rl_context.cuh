@@ -37,7 +37,7 @@ struct Tree {
     DBuf<uint32_t> first_key;  // Morton rank of the first neuron under the node
     DBuf<uint32_t> leaf_of;    // neuron -> node
     DBuf<uint32_t> morton;     // Morton rank -> neuron
-    DBuf<uint32_t> arrive;     // bottom-up arrival counters
+    std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
     // FP32 form: records (centroid, count bits in w) and cell lengths as FP32
     DBuf<float4> rec32[2];
     DBuf<float> maxdim32;
@@ -165,6 +165,35 @@ struct ActDesc {
     const int32_t* w;
 };
 
+// Launch shape of the Barnes-Hut search kernels.
+struct SearchVariant {
+    int warps = 4;    // warps per block
+    int stack = 48;   // frames of the per-lane and per-packet stacks
+    int packet = 32;  // lanes (sources) that walk the descent from the root together
+};
+
+// Launch shape of the activity kernel.
+struct ActVariant {
+    int block = 256;     // threads per block
+    int persistent = 0;  // 1: one resident wave of blocks looping over the neurons
+};
+
+enum : int { TUNE_OFF = 0, TUNE_REQUESTED = 1, TUNE_DONE = 2 };
+
+// Launch shapes in use and the tuner's state.
+struct Tuning {
+    SearchVariant search;
+    ActVariant act;
+    int search_state = TUNE_OFF;
+    int act_state = TUNE_OFF;
+    bool force = false;            // time again even when the process has a result for this shape
+    std::vector<float> search_ms;  // per variant tried, in search_variants() order
+    std::vector<float> act_ms;     // per variant tried, in act_variants() order
+};
+
+const std::vector<SearchVariant>& search_variants();
+const std::vector<ActVariant>& act_variants();
+
 struct Ctx {
     rl_config cfg{};
     uint32_t n = 0;
@@ -192,7 +221,23 @@ struct Ctx {
     DBuf<uint32_t> err;       // device error word
     DBuf<uint64_t> counters;  // device counters
     rl_stats stats{};
+    uint64_t launches = 0;     // kernels launched for this context
+    int64_t device_bytes = 0;  // device memory held now
+    int64_t device_peak = 0;   // and at most so far
+    bool counted = false;      // counted among the device's live contexts
+    Tuning tune;
 };
+
+// Tuning results shared by the contexts of a process, keyed by precision,
+// batched or not, and the neuron count's power of two.
+void remember_search_tuning(const Ctx& c);
+bool recall_search_tuning(Ctx& c);
+void remember_act_tuning(const Ctx& c);
+bool recall_act_tuning(Ctx& c);
+// Releases the captured activity intervals (they are captured again on use).
+void drop_activity_graphs(Ctx& c);
+// Blocks of an activity launch of variant v of `kernel`.
+unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel);
 
 // octree.cu
 void build_octree(Ctx& c, const double* h_xyz);
@@ -218,17 +263,20 @@ bool is_fp32(const Ctx& c);
 void alloc_fp32(Ctx& c);
 void f32_from_f64(Ctx& c);  // state arrays FP64 -> FP32 (after a host upload)
 void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download)
-void launch_activity_f32(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur);
+void launch_activity_f32(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);
+void launch_activity_fp64(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);
 uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
-                       uint32_t num_segs, uint32_t warps, uint32_t step);
+                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v);
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu
 // Activity steps first..first+nsteps-1 (one fused kernel per step; a full
 // plasticity interval runs as a captured CUDA graph).
 void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps);
+// Frees a context and everything it holds (after its stream has drained).
+void discard(Ctx* c);
 uint64_t run_commit(Ctx& c, int type);  // commit one element type; to_delete[] per neuron, returns the sum
 
 void check_device_error(Ctx& c, const char* phase);

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/relearn_b200.h"
@@ -33,12 +34,24 @@ struct Error {
         }                                                  \
     } while (0)
 
-// Every kernel launch of the library goes through this counter.
-extern uint64_t g_launches;
+// The context an entry point works for, bound to the calling thread for the
+// duration of the call: the stream its device memory is ordered on and its
+// launch and device-memory counters.  Contexts driven from different host
+// threads therefore share no mutable state in the library.
+struct Binding {
+    cudaStream_t stream = nullptr;
+    uint64_t* launches = nullptr;
+    int64_t* bytes = nullptr;
+    int64_t* peak = nullptr;
+};
+extern thread_local Binding g_bind;
 
+// Every kernel launch of the library goes through this counter.
 #define RL_LAUNCH_CHECK()                          \
     do {                                           \
-        ++::rl::g_launches;                        \
+        if (::rl::g_bind.launches) {               \
+            ++*::rl::g_bind.launches;              \
+        }                                          \
         RL_CUDA_TRY(cudaPeekAtLastError());        \
     } while (0)
 
@@ -65,6 +78,19 @@ enum DeviceError : uint32_t {
 };
 
 // ------------------------------------------------------------- device buffer
+// Device memory is stream ordered (cudaMallocAsync / cudaFreeAsync from the
+// device's memory pool) on the bound context's stream, so contexts that run
+// side by side never synchronise the device by allocating or freeing, and the
+// bytes each context holds are counted.
+inline void account(int64_t delta) {
+    if (g_bind.bytes) {
+        *g_bind.bytes += delta;
+        if (g_bind.peak && *g_bind.bytes > *g_bind.peak) {
+            *g_bind.peak = *g_bind.bytes;
+        }
+    }
+}
+
 template <typename T>
 struct DBuf {
     T* p = nullptr;
@@ -74,8 +100,9 @@ struct DBuf {
         if (count == 0) {
             count = 1;
         }
-        RL_CUDA_TRY(cudaMalloc((void**)&p, count * sizeof(T)));
+        RL_CUDA_TRY(cudaMallocAsync((void**)&p, count * sizeof(T), g_bind.stream));
         n = count;
+        account((int64_t)(n * sizeof(T)));
     }
     void ensure(size_t count) {
         if (count > n || p == nullptr) {
@@ -88,10 +115,19 @@ struct DBuf {
     }
     void release() {
         if (p) {
-            cudaFree(p);
+            if (g_bind.stream) {
+                cudaFreeAsync(p, g_bind.stream);
+            } else {
+                cudaFree(p);
+            }
+            account(-(int64_t)(n * sizeof(T)));
         }
         p = nullptr;
         n = 0;
+    }
+    void swap(DBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
     }
     ~DBuf() { release(); }
     DBuf() = default;

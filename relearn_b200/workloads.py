@@ -62,3 +62,36 @@ def ensure_distinct(pos: np.ndarray) -> np.ndarray:
     if len(u) != len(pos):
         raise ValueError("positions are not pairwise distinct")
     return pos
+
+
+def serving_stream(seed: int, rate: float, duration: float, lo: int = 2_000, hi: int = 1_000_000, steps: int = 5_000,
+                   theta=(0.2, 0.5), growth=(1e-5, 1e-3), sigma: float = 750.0, density_um3: float = 1000.0) -> list:
+    """The serving workload: Poisson arrivals at `rate` per second over
+    `duration` seconds; each request one network of log-uniform lo..hi neurons
+    with its own seed, growth rate (log-uniform, the same for all element
+    types) and theta (uniform), placed uniformly at one neuron per
+    `density_um3` cubic micrometres, run for `steps` steps.  Returns
+    [(arrival time, network dict)] in arrival order; positions and signal
+    types come from :func:`request_inputs`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    k = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        net = dict(num_neurons=n, seed=int(seed) * 1_000_003 + k, side=(density_um3 * n) ** (1.0 / 3.0),
+                   theta=float(rng.uniform(*theta)), sigma=float(sigma), growth_rate=float(np.exp(rng.uniform(np.log(growth[0]), np.log(growth[1])))),
+                   steps=int(steps))
+        out.append((t, net))
+        k += 1
+    return out
+
+
+def request_inputs(net: dict) -> tuple:
+    """Positions and signal types of a serving request, seeded by its seed."""
+    n = int(net["num_neurons"])
+    s = int(net["seed"]) % (2**31)
+    return uniform_cube(n, float(net["side"]), s), signal_types(n, s)

@@ -23,6 +23,13 @@ def has_gpu() -> bool:
 
 
 @pytest.fixture(scope="session")
+def built_lib():
+    from relearn_b200 import build
+
+    return build.build()
+
+
+@pytest.fixture(scope="session")
 def oracle_mod():
     from oracle import oracle
 

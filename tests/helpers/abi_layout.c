@@ -19,5 +19,22 @@ int main(void) {
     F(rl_config, device);
     F(rl_config, precision);
     F(rl_stats, max_level);
+    printf("rl_network %zu\n", sizeof(rl_network));
+    printf("rl_tuning %zu\n", sizeof(rl_tuning));
+    printf("RL_NUM_SEARCH_SHAPES %d\n", RL_NUM_SEARCH_SHAPES);
+    printf("RL_NUM_ACT_SHAPES %d\n", RL_NUM_ACT_SHAPES);
+    printf("rl_serve_config %zu\n", sizeof(rl_serve_config));
+    printf("rl_serve_request %zu\n", sizeof(rl_serve_request));
+    printf("rl_serve_done %zu\n", sizeof(rl_serve_done));
+    F(rl_network, growth_rate);
+    F(rl_serve_config, slots);
+    F(rl_serve_config, use_graphs);
+    F(rl_serve_request, xyz);
+    F(rl_serve_request, grown);
+    F(rl_serve_request, steps);
+    F(rl_serve_request, keep_state);
+    F(rl_serve_done, t_submit);
+    F(rl_serve_done, num_synapses);
+    F(rl_serve_done, neuron_steps);
     return 0;
 }

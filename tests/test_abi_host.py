@@ -14,13 +14,6 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "relearn_b200.h")
 
 
-@pytest.fixture(scope="module")
-def built_lib():
-    from relearn_b200 import build
-
-    return build.build()
-
-
 def declared_functions():
     text = open(HEADER).read()
     return sorted(set(re.findall(r"RL_API\s+[\w\s\*]+?\b(rl_\w+)\s*\(", text)))
@@ -55,6 +48,18 @@ def test_struct_layout(tmp_path):
     for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device", "precision"):
         assert int(lines[f"rl_config.{f}"]) == getattr(R.RlConfig, f).offset
     assert int(lines["rl_stats.max_level"]) == R.RlStats.max_level.offset
+    assert int(lines["RL_NUM_SEARCH_SHAPES"]) == R.NUM_SEARCH_SHAPES == len(R.SEARCH_SHAPES)
+    assert int(lines["RL_NUM_ACT_SHAPES"]) == R.NUM_ACT_SHAPES == len(R.ACT_SHAPES)
+    for name, cls in (("rl_tuning", R.RlTuning), ("rl_network", R.RlNetwork), ("rl_serve_config", R.RlServeConfig), ("rl_serve_request", R.RlServeRequest),
+                      ("rl_serve_done", R.RlServeDone)):
+        assert int(lines[name]) == C.sizeof(cls), name
+    assert int(lines["rl_network.growth_rate"]) == R.RlNetwork.growth_rate.offset
+    for f in ("slots", "use_graphs"):
+        assert int(lines[f"rl_serve_config.{f}"]) == getattr(R.RlServeConfig, f).offset
+    for f in ("xyz", "grown", "steps", "keep_state"):
+        assert int(lines[f"rl_serve_request.{f}"]) == getattr(R.RlServeRequest, f).offset
+    for f in ("t_submit", "num_synapses", "neuron_steps"):
+        assert int(lines[f"rl_serve_done.{f}"]) == getattr(R.RlServeDone, f).offset
 
 
 def test_host_only_entry_points(built_lib):

@@ -1,0 +1,87 @@
+"""Autotuned launch shapes: every candidate shape of the search and activity
+kernels computes the same results (bit for bit), so tuning never changes what
+a run produces; the tuner times the candidates that fit the octree."""
+import numpy as np
+import pytest
+
+from conftest import seed_elements, small_network
+
+pytestmark = pytest.mark.gpu
+
+
+def make(n, side, seed, precision):
+    from relearn_b200 import Network
+
+    params, pos, sig = small_network(n, side, seed)
+    params["precision"] = precision
+    net = Network(params)
+    net.set_positions(pos, sig)
+    return net
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_search_shape_finds_the_same_targets(precision):
+    from relearn_b200 import SEARCH_SHAPES
+
+    n = 30000
+    net = make(n, 3100.0, 21, precision)
+    one = np.full(n, 2, np.uint32)
+    net.prepare_update_connectivity(one, one, one)
+    depth = net.tree_info()[1]
+    ref = None
+    tried = 0
+    for w, st, p in SEARCH_SHAPES:
+        if st < depth + 2:
+            continue
+        net.set_tuning(search_warps=w, search_stack=st, search_packet=p)
+        req = net.find_targets(100)
+        if ref is None:
+            ref = req
+        else:
+            assert np.array_equal(req, ref), (w, st, p)
+        tried += 1
+    assert tried >= 6 and len(ref) > 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_activity_shape_gives_the_same_state(precision):
+    from relearn_b200 import ACT_SHAPES
+
+    n = 50000
+    ref = None
+    for b, p in ACT_SHAPES:
+        net = make(n, 3700.0, 8, precision)
+        net.set_tuning(act_block=b, act_persistent=p)
+        net.activity_block(1, 37)
+        a = net.neurons()
+        got = [a["x"].view(np.uint64), a["u"].view(np.uint64), a["calcium"].view(np.uint64), a["fired"]]
+        if ref is None:
+            ref = got
+        else:
+            for g, r in zip(got, ref):
+                assert np.array_equal(g, r), (b, p)
+        net.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_tuned_run_equals_untuned(precision):
+    n = 6000
+    runs = []
+    for tune in (False, True):
+        net = make(n, 1820.0, 13, precision)
+        seed_elements(net, n, 5, 0.0, 3.0)
+        if tune:
+            net.autotune(2)
+        net.simulate(1, 401)
+        a = net.neurons()
+        runs.append((a["x"].view(np.uint64), a["calcium"].view(np.uint64), net.edges()))
+        if tune:
+            t = net.tuning()
+            assert t["tuned"] == 3
+            assert len(t["act_ms"]) == 6 and len(t["search_ms"]) >= 6
+        net.close()
+    (x0, c0, e0), (x1, c1, e1) = runs
+    assert np.array_equal(x0, x1) and np.array_equal(c0, c1)
+    for a, b in zip(e0, e1):
+        assert np.array_equal(a, b)
+    assert len(e0[0]) > 0
