@@ -292,7 +292,8 @@ RL_API rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts);
 /* Launch shapes of the hot kernels.  The search kernels walk the octree with
  * `search_warps` warps per block, `search_stack` frames per walk and
  * `search_packet` lanes (sources) walking the descent from the root together;
- * the activity kernel runs `act_block` threads per block, and with
+ * the activity kernel runs `act_block` threads per block with `act_vec`
+ * neurons per thread (vector loads and stores; the FP64 form runs 1), and with
  * `act_persistent` one resident wave of blocks strides over the neurons.  No
  * counterpart in the reference (its CPU loops have no launch shape). */
 typedef struct rl_tuning {
@@ -301,14 +302,15 @@ typedef struct rl_tuning {
     int32_t search_packet;   /* 32 or 16 */
     int32_t act_block;       /* 128, 256 or 512 */
     int32_t act_persistent;  /* 0 or 1 */
+    int32_t act_vec;         /* 1, 2 or 4 */
     int32_t tuned;           /* bit 0: search shape timed or recalled, bit 1: activity shape */
 } rl_tuning;
 
 /* Candidates the tuner times, in the order of the times rl_get_tuning returns:
  * search: packet 32 then 16, stack 24 then 48, warps 2, 4, 8 (12 shapes);
- * activity: persistent 0 then 1, block 128, 256, 512 (6 shapes). */
+ * activity: persistent 0 then 1, block 128, 256, 512, vec 1, 2, 4 (18 shapes). */
 #define RL_NUM_SEARCH_SHAPES 12
-#define RL_NUM_ACT_SHAPES 6
+#define RL_NUM_ACT_SHAPES 18
 
 /* Autotuning: 0 keeps the current shapes; 1 times the candidates on the
  * context's own data at the next activity block and the next search (a search

@@ -30,12 +30,32 @@ def nvcc() -> str:
     return "nvcc"
 
 
+HOST = os.path.join(HERE, "host")
+BIN = os.path.join(HERE, "bin")
+HOST_PROGRAMS = ["relearn_b200_run", "host_selftest"]
+
+
 def stale() -> bool:
-    if not os.path.exists(LIB):
+    outs = [LIB] + [os.path.join(BIN, p) for p in HOST_PROGRAMS]
+    if not all(os.path.exists(o) for o in outs):
         return True
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(o) for o in outs)
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [INCLUDE, __file__]
+    deps += [os.path.join(HOST, f) for f in os.listdir(HOST)]
     return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_host(verbose: bool = False) -> None:
+    """The C++ host programs over the C ABI (C++20, linked to the library in
+    this directory through an rpath)."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = os.environ.get("CXX", "g++")
+    for prog in HOST_PROGRAMS:
+        cmd = [cxx, "-std=c++20", "-O2", "-Wall", "-Wextra", "-o", os.path.join(BIN, prog), os.path.join(HOST, prog + ".cpp"), "-L" + HERE,
+               "-lrelearn_b200", "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -55,6 +75,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
+    build_host(verbose)
     return LIB
 
 

@@ -146,12 +146,22 @@ struct CommitArgs {
     double retract;
     uint32_t* to_delete;
     unsigned long long* total;
+    const unsigned long long* guard;  // counts of the earlier types of this update
+    int guard_n;                      // how many of them; any nonzero count skips the commit
 };
+
+__device__ __forceinline__ bool commit_guarded(const unsigned long long* guard, int guard_n) {
+    unsigned long long g = 0;
+    for (int t = 0; t < guard_n; ++t) {
+        g += guard[t];
+    }
+    return g != 0;
+}
 
 // ElementBaseBase::update for one element type.
 __global__ void k_commit(CommitArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) {
+    if (i >= A.n || commit_guarded(A.guard, A.guard_n)) {
         return;
     }
     if (!A.enabled[i]) {
@@ -299,8 +309,9 @@ struct ActSnapshot {
     }
 };
 
-// Times every activity variant on two steps from the current state (the
-// second is timed) and keeps the fastest; the state is restored after each.
+// Times every activity variant on four steps from the current state (the
+// last three are timed) and keeps the fastest; the state is restored after
+// each.
 void tune_activity(Ctx& c) {
     ActSnapshot snap(c);
     cudaEvent_t e0, e1;
@@ -309,9 +320,15 @@ void tune_activity(Ctx& c) {
     float best = 1e30f;
     ActVariant pick = c.tune.act;
     for (const ActVariant& v : act_variants()) {
+        if (!is_fp32(c) && v.vec != 1) {
+            c.tune.act_ms.push_back(0.0f);  // the FP64 kernel runs one neuron per thread
+            continue;
+        }
         launch_step(c, 0, v);
         RL_CUDA_TRY(cudaEventRecord(e0, c.stream));
-        launch_step(c, 1, v);
+        for (uint32_t k = 1; k <= 3; ++k) {
+            launch_step(c, k, v);
+        }
         RL_CUDA_TRY(cudaEventRecord(e1, c.stream));
         RL_CUDA_TRY(cudaEventSynchronize(e1));
         float ms = 0.0f;
@@ -336,7 +353,9 @@ const std::vector<ActVariant>& act_variants() {
         std::vector<ActVariant> out;
         for (int p : { 0, 1 }) {
             for (int b : { 128, 256, 512 }) {
-                out.push_back(ActVariant{ b, p });
+                for (int v : { 1, 2, 4 }) {
+                    out.push_back(ActVariant{ b, p, v });
+                }
             }
         }
         return out;
@@ -345,7 +364,9 @@ const std::vector<ActVariant>& act_variants() {
 }
 
 unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel) {
-    const unsigned full = blocks_for(c.n, (unsigned)v.block);
+    const uint32_t groups = c.n / (uint32_t)v.vec;
+    const uint32_t tail = c.n - groups * (uint32_t)v.vec;
+    const unsigned full = blocks_for(groups > tail ? groups : tail, (unsigned)v.block);
     if (!v.persistent) {
         return full;
     }
@@ -435,6 +456,28 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     c.stats.activity_steps += nsteps;
 }
 
+void launch_commit_guarded(Ctx& c, int type) {
+    unsigned long long* cnt = c.commit_cnt.p;
+    if (is_fp32(c)) {
+        launch_commit_f32(c, type, cnt + type, cnt, type);
+        return;
+    }
+    CommitArgs A;
+    A.n = c.n;
+    A.enabled = c.nr.enabled.p;
+    A.grown = c.nr.grown[type].p;
+    A.delta = c.nr.delta[type].p;
+    A.connected = c.nr.connected[type].p;
+    A.vacant = c.nr.vacant[type].p;
+    A.retract = c.cfg.retract_ratio[type];
+    A.to_delete = c.to_delete.p;
+    A.total = cnt + type;
+    A.guard = cnt;
+    A.guard_n = type;
+    k_commit<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
+    RL_LAUNCH_CHECK();
+}
+
 uint64_t run_commit(Ctx& c, int type) {
     if (is_fp32(c)) {
         return run_commit_f32(c, type);
@@ -451,6 +494,8 @@ uint64_t run_commit(Ctx& c, int type) {
     unsigned long long* d_del = reinterpret_cast<unsigned long long*>(c.counters.p) + 1;
     RL_CUDA_TRY(cudaMemsetAsync(d_del, 0, sizeof(unsigned long long), c.stream));
     A.total = d_del;
+    A.guard = nullptr;
+    A.guard_n = 0;
     k_commit<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(A);
     RL_LAUNCH_CHECK();
     unsigned long long h = 0;

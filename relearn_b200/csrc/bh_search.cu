@@ -589,11 +589,22 @@ void run_search(Ctx& c, uint32_t step) {
     uint32_t* cnt_inh = S.counts.p + n;
     k_search_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, c.tree.morton.p, c.nr.enabled.p, c.nr.signal.p, c.nr.search_vacant.p, cnt_exc, cnt_inh);
     RL_LAUNCH_CHECK();
-    const uint64_t num_exc = exclusive_scan_u32(cnt_exc, cnt_exc, n, c.prim, st);
-    const uint64_t num_inh = exclusive_scan_u32(cnt_inh, cnt_inh, n, c.prim, st);
-    const uint64_t m = num_exc + num_inh;
+    // one scan over both halves: excitatory offsets, then inhibitory offsets
+    // counted on from the last excitatory search
+    const uint32_t* dtot = exclusive_scan_u32_async(S.counts.p, S.counts.p, 2 * (uint64_t)n, c.prim, st);
+    uint32_t h[2] = { 0, 0 };
+    RL_CUDA_TRY(cudaMemcpyAsync(&h[0], cnt_inh, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaMemcpyAsync(&h[1], dtot, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    const uint64_t num_exc = h[0];
+    const uint64_t m = h[1];
+    const uint64_t num_inh = m - num_exc;
     S.num_searches = m;
     S.num_exc = num_exc;
+    if (m == 0) {
+        S.num_requests = 0;  // nothing searches: no requests, nothing else to run
+        return;
+    }
     S.first_fail.ensure(n);
     S.req_count.ensure(n);
     S.req_off.ensure(n);
@@ -604,16 +615,21 @@ void run_search(Ctx& c, uint32_t step) {
         S.jj.ensure(m);
         S.target.ensure(m);
         k_search_fill<<<blocks_for(n, 256), 256, 0, st>>>(n, c.tree.morton.p, c.nr.enabled.p, c.nr.signal.p, c.nr.search_vacant.p, cnt_exc, cnt_inh,
-                                                          num_exc, S.src.p, S.jj.p);
+                                                          0, S.src.p, S.jj.p);
         RL_LAUNCH_CHECK();
         // segments: one per (type, network) with searches, so a warp never mixes networks
         const uint32_t K = (uint32_t)c.nets.size();
-        S.seg_starts.ensure(2 * (size_t)K);
-        k_net_starts<<<blocks_for(K, 128), 128, 0, st>>>(K, c.d_nets.p, cnt_exc, cnt_inh, n, S.seg_starts.p);
-        RL_LAUNCH_CHECK();
-        std::vector<uint32_t> starts(2 * (size_t)K);
-        RL_CUDA_TRY(cudaMemcpyAsync(starts.data(), S.seg_starts.p, 2 * (size_t)K * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        RL_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<uint32_t> starts(2 * (size_t)K, 0u);
+        if (K > 1) {
+            S.seg_starts.ensure(2 * (size_t)K);
+            k_net_starts<<<blocks_for(K, 128), 128, 0, st>>>(K, c.d_nets.p, cnt_exc, cnt_inh, n, S.seg_starts.p);
+            RL_LAUNCH_CHECK();
+            RL_CUDA_TRY(cudaMemcpyAsync(starts.data(), S.seg_starts.p, 2 * (size_t)K * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            RL_CUDA_TRY(cudaStreamSynchronize(st));
+            for (uint32_t k = 0; k < K; ++k) {
+                starts[K + k] -= (uint32_t)num_exc;  // inhibitory starts relative to the first inhibitory search
+            }
+        }
         if (is_fp32(c)) {
             pack_tree_f32(c);
         }

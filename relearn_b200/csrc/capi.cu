@@ -260,6 +260,7 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     c.act_desc.alloc(1);
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
+    c.commit_cnt.alloc(3);
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
     setup_nets(c, nets, num_nets);
@@ -279,10 +280,28 @@ void plasticity_update(Ctx& c, uint32_t step) {
     {
         // SynapseDeletionFinderCPU::delete_synapses (neurons/helper/SynapseDeletionFinderCPU.cpp:27-92):
         // commit axons, delete; commit excitatory dendrites, delete; commit inhibitory dendrites, delete
+        // The commit of a type reads the connected counts that the deletion
+        // of an earlier type changes, so types are committed in order with the
+        // deletions between them.  Usually nothing is deleted: the three
+        // commits go out at once, each skipping itself on the device when an
+        // earlier one left deletions, and a single read says where the
+        // sequential path has to take over.
         PhaseScope ps(c, PH_COMMIT);
+        RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 3 * sizeof(unsigned long long), c.stream));
         for (int t = 0; t < 3; ++t) {
-            if (run_commit(c, t) > 0) {
-                c.stats.synapses_deleted += run_deletion(c, step, t);
+            launch_commit_guarded(c, t);
+        }
+        unsigned long long h[3] = { 0, 0, 0 };
+        RL_CUDA_TRY(cudaMemcpyAsync(h, c.commit_cnt.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        c.stats.bound_to_delete += h[0] + h[1] + h[2];
+        const int first = h[0] ? 0 : (h[1] ? 1 : (h[2] ? 2 : 3));
+        if (first < 3) {
+            c.stats.synapses_deleted += run_deletion(c, step, first);
+            for (int t = first + 1; t < 3; ++t) {
+                if (run_commit(c, t) > 0) {
+                    c.stats.synapses_deleted += run_deletion(c, step, t);
+                }
             }
         }
     }
@@ -896,6 +915,7 @@ rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_
         out->search_packet = c.tune.search.packet;
         out->act_block = c.tune.act.block;
         out->act_persistent = c.tune.act.persistent;
+        out->act_vec = c.tune.act.vec;
         out->tuned = (c.tune.search_state == rl::TUNE_DONE ? 1 : 0) | (c.tune.act_state == rl::TUNE_DONE ? 2 : 0);
         // times are recorded for the shapes that fit, in candidate order
         if (search_ms) {
@@ -921,12 +941,13 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
             s_ok = s_ok || (v.warps == t->search_warps && v.stack == t->search_stack && v.packet == t->search_packet);
         }
         for (const auto& v : rl::act_variants()) {
-            a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent);
+            a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent && v.vec == t->act_vec);
         }
         RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
+        RL_CHECK(rl::is_fp32(c) || t->act_vec == 1, RL_ERR_INVALID, "the FP64 activity kernel runs one neuron per thread");
         RL_CHECK(!c.positions_set || (uint32_t)t->search_stack >= c.tree.max_level + 2, RL_ERR_INVALID, "search stack shallower than the octree");
         c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet };
-        c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent };
+        c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent, t->act_vec };
         c.tune.search_state = rl::TUNE_OFF;
         c.tune.act_state = rl::TUNE_OFF;
         rl::drop_activity_graphs(c);

@@ -102,12 +102,14 @@ __device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
     return 1.41421356237f * (p * x);
 }
 
+// One neuron's activity step on registers: `x`, `u`, `ca` and the three
+// deltas are read and updated in place; `input` and `fired` are outputs.
 template <int H>
-__device__ __forceinline__ void activity_neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
-    const uint32_t step = D->base_step + k;
-    if (!A.enabled[i]) {
-        A.input[i] = 0.0f;
-        A.fired_cur[i] = A.fired_prev[i];
+__device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, bool enabled, uint8_t fired_prev,
+                                           uint16_t net, float& x, float& u, double& ca, float (&delta)[3], float& input, uint8_t& fired) {
+    if (!enabled) {
+        input = 0.0f;
+        fired = fired_prev;
         return;
     }
     int isum = 0;
@@ -123,13 +125,12 @@ __device__ __forceinline__ void activity_neuron_f32(const Act32& A, const ActDes
         }
     }
     // the same Philox draw as the FP64 form, 24 bits of it
-    const NetInfo& N = A.nets[A.net_of[i]];
+    const NetInfo& N = A.nets[net];
     const u32x4 w = draw(N.seed, step, i - N.first, 0u, STREAM_NOISE, 0u);
-    const float input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(w.x >> 8), A.noise_mean));
-    A.input[i] = input;
+    input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(w.x >> 8), A.noise_mean));
 
-    float xv = A.x[i];
-    float uv = A.u[i];
+    float xv = x;
+    float uv = u;
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
     const float sI = fmaf(A.s, input, A.sk3);
@@ -146,12 +147,10 @@ __device__ __forceinline__ void activity_neuron_f32(const Act32& A, const ActDes
             break;
         }
     }
-    A.x[i] = xv;
-    A.u[i] = uv;
-    A.fired_cur[i] = spiked;
-
-    const double ca = fma(A.calcium[i], A.ca_mul, spiked ? A.ca_add : 0.0);
-    A.calcium[i] = ca;
+    x = xv;
+    u = uv;
+    fired = spiked;
+    ca = fma(ca, A.ca_mul, spiked ? A.ca_add : 0.0);
     const float caf = (float)ca;
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
@@ -162,26 +161,159 @@ __device__ __forceinline__ void activity_neuron_f32(const Act32& A, const ActDes
             const float q = (caf - A.xi[t]) * A.inv_zeta[t];
             dz = fmaf(2.0f, __expf(-q * q), -1.0f);
         }
-        A.delta[t][i] = fmaf(dz, N.nu32[t], A.delta[t][i]);
+        delta[t] = fmaf(dz, N.nu32[t], delta[t]);
     }
 }
 
+// Vector loads and stores of V consecutive entries (V = 1, 2, 4); the
+// caller's index is a multiple of V, so every access is aligned to its width.
+template <int V>
+__device__ __forceinline__ void ld_f(const float* p, float (&v)[V]) {
+    if constexpr (V == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+    } else if constexpr (V == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        v[0] = t.x, v[1] = t.y;
+    } else {
+        v[0] = *p;
+    }
+}
+template <int V>
+__device__ __forceinline__ void st_f(float* p, const float (&v)[V]) {
+    if constexpr (V == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (V == 2) {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    } else {
+        *p = v[0];
+    }
+}
+template <int V>
+__device__ __forceinline__ void ld_d(const double* p, double (&v)[V]) {
+    if constexpr (V >= 2) {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            const double2 t = *reinterpret_cast<const double2*>(p + k);
+            v[k] = t.x, v[k + 1] = t.y;
+        }
+    } else {
+        v[0] = *p;
+    }
+}
+template <int V>
+__device__ __forceinline__ void st_d(double* p, const double (&v)[V]) {
+    if constexpr (V >= 2) {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            *reinterpret_cast<double2*>(p + k) = make_double2(v[k], v[k + 1]);
+        }
+    } else {
+        *p = v[0];
+    }
+}
+template <int V>
+__device__ __forceinline__ void ld_b(const uint8_t* p, uint8_t (&v)[V]) {
+    if constexpr (V == 4) {
+        const uint32_t t = *reinterpret_cast<const uint32_t*>(p);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[k] = (uint8_t)(t >> (8 * k));
+        }
+    } else if constexpr (V == 2) {
+        const uint16_t t = *reinterpret_cast<const uint16_t*>(p);
+        v[0] = (uint8_t)t, v[1] = (uint8_t)(t >> 8);
+    } else {
+        v[0] = *p;
+    }
+}
+template <int V>
+__device__ __forceinline__ void st_b(uint8_t* p, const uint8_t (&v)[V]) {
+    if constexpr (V == 4) {
+        *reinterpret_cast<uint32_t*>(p) = (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+    } else if constexpr (V == 2) {
+        *reinterpret_cast<uint16_t*>(p) = (uint16_t)(v[0] | (v[1] << 8));
+    } else {
+        *p = v[0];
+    }
+}
+template <int V>
+__device__ __forceinline__ void ld_h(const uint16_t* p, uint16_t (&v)[V]) {
+    if constexpr (V == 4) {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        v[0] = (uint16_t)t.x, v[1] = (uint16_t)(t.x >> 16), v[2] = (uint16_t)t.y, v[3] = (uint16_t)(t.y >> 16);
+    } else if constexpr (V == 2) {
+        const uint32_t t = *reinterpret_cast<const uint32_t*>(p);
+        v[0] = (uint16_t)t, v[1] = (uint16_t)(t >> 16);
+    } else {
+        v[0] = *p;
+    }
+}
+
+// V consecutive neurons from index i (a multiple of V): all loads first, so
+// that each thread keeps its whole footprint in flight, then the updates,
+// then the stores.
+template <int H, int V>
+__device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i) {
+    uint8_t en[V], fp[V], fired[V];
+    uint16_t net[V];
+    float x[V], u[V], d0[V], d1[V], d2[V], input[V];
+    double ca[V];
+    ld_b<V>(A.enabled + i, en);
+    ld_b<V>(A.fired_prev + i, fp);
+    ld_h<V>(A.net_of + i, net);
+    ld_f<V>(A.x + i, x);
+    ld_f<V>(A.u + i, u);
+    ld_d<V>(A.calcium + i, ca);
+    ld_f<V>(A.delta[0] + i, d0);
+    ld_f<V>(A.delta[1] + i, d1);
+    ld_f<V>(A.delta[2] + i, d2);
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        float d[3] = { d0[k], d1[k], d2[k] };
+        neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], net[k], x[k], u[k], ca[k], d, input[k], fired[k]);
+        d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
+    }
+    st_f<V>(A.input + i, input);
+    st_b<V>(A.fired_cur + i, fired);
+    st_f<V>(A.x + i, x);
+    st_f<V>(A.u + i, u);
+    st_d<V>(A.calcium + i, ca);
+    st_f<V>(A.delta[0] + i, d0);
+    st_f<V>(A.delta[1] + i, d1);
+    st_f<V>(A.delta[2] + i, d2);
+}
+
 // H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
-// block, striding over the neurons when the grid is one resident wave.
-template <int H, int BLOCK>
+// block, V neurons per thread, striding over the neurons when the grid is one
+// resident wave.  The last n % V neurons go one per thread.
+template <int H, int BLOCK, int V>
 __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
+    const uint32_t step = D->base_step + k;
+    const uint32_t groups = A.n / V;
+    const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     const uint32_t stride = gridDim.x * BLOCK;
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        activity_neuron_f32<H>(A, D, k, i);
+    for (uint32_t g = tid; g < groups; g += stride) {
+        neurons_f32<H, V>(A, D, step, g * V);
+    }
+    if (V > 1 && tid < A.n - groups * V) {
+        neurons_f32<H, 1>(A, D, step, groups * V + tid);
     }
 }
 
 // ElementBaseBase::update with an FP32 delta.
 __global__ void k_commit_f32(uint32_t n, const uint8_t* __restrict__ enabled, double* grown, float* delta, uint32_t* connected, uint32_t* vacant,
-                             double retract, uint32_t* to_delete, unsigned long long* total) {
+                             double retract, uint32_t* to_delete, unsigned long long* total, const unsigned long long* guard, int guard_n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
+    }
+    unsigned long long g = 0;
+    for (int t = 0; t < guard_n; ++t) {
+        g += guard[t];
+    }
+    if (g != 0) {
+        return;  // an earlier type of this update left synapses to delete first
     }
     if (!enabled[i]) {
         to_delete[i] = 0u;
@@ -693,22 +825,37 @@ void f64_from_f32(Ctx& c) {
     }
 }
 
-template <int H, int BLOCK>
+template <int H, int BLOCK, int V>
 void launch_act32(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
-    k_activity_f32<H, BLOCK><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    k_activity_f32<H, BLOCK, V><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+}
+
+template <int H, int BLOCK>
+void launch_act32_b(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
+    switch (v.vec) {
+        case 4:
+            launch_act32<H, BLOCK, 4>(c, v, A, kstep);
+            break;
+        case 2:
+            launch_act32<H, BLOCK, 2>(c, v, A, kstep);
+            break;
+        default:
+            launch_act32<H, BLOCK, 1>(c, v, A, kstep);
+            break;
+    }
 }
 
 template <int H>
 void launch_act32_h(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
     switch (v.block) {
         case 128:
-            launch_act32<H, 128>(c, v, A, kstep);
+            launch_act32_b<H, 128>(c, v, A, kstep);
             break;
         case 512:
-            launch_act32<H, 512>(c, v, A, kstep);
+            launch_act32_b<H, 512>(c, v, A, kstep);
             break;
         default:
-            launch_act32<H, 256>(c, v, A, kstep);
+            launch_act32_b<H, 256>(c, v, A, kstep);
             break;
     }
 }
@@ -770,11 +917,17 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     RL_LAUNCH_CHECK();
 }
 
+void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n) {
+    k_commit_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(c.n, c.nr.enabled.p, c.nr.grown[type].p, c.nr.delta32[type].p, c.nr.connected[type].p,
+                                                             c.nr.vacant[type].p, c.cfg.retract_ratio[type], c.to_delete.p, total, guard, guard_n);
+    RL_LAUNCH_CHECK();
+}
+
 uint64_t run_commit_f32(Ctx& c, int type) {
     unsigned long long* d_del = reinterpret_cast<unsigned long long*>(c.counters.p) + 1;
     RL_CUDA_TRY(cudaMemsetAsync(d_del, 0, sizeof(unsigned long long), c.stream));
     k_commit_f32<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(c.n, c.nr.enabled.p, c.nr.grown[type].p, c.nr.delta32[type].p, c.nr.connected[type].p,
-                                                             c.nr.vacant[type].p, c.cfg.retract_ratio[type], c.to_delete.p, d_del);
+                                                             c.nr.vacant[type].p, c.cfg.retract_ratio[type], c.to_delete.p, d_del, nullptr, 0);
     RL_LAUNCH_CHECK();
     unsigned long long h = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&h, d_del, sizeof(h), cudaMemcpyDeviceToHost, c.stream));

@@ -358,6 +358,22 @@ __device__ __forceinline__ void stcg4(double4* p, const double4& v) {
     __stcg(reinterpret_cast<double2*>(p) + 1, make_double2(v.z, v.w));
 }
 
+// Centroid = count-weighted sum / total count, clipped to the cell; NaN
+// centroid and count 0 for a cell without vacant elements.
+__device__ __forceinline__ double4 finish_centroid(double ax, double ay, double az, uint32_t total, double lx, double ly, double lz, double hx, double hy,
+                                                   double hz) {
+    if (total == 0) {
+        const double nan = __longlong_as_double(0x7FF8000000000000ll);
+        return make_double4(nan, nan, nan, 0.0);
+    }
+    const double td = (double)total;
+    double x = ax / td, y = ay / td, z = az / td;
+    x = x < lx ? lx : (hx < x ? hx : x);
+    y = y < ly ? ly : (hy < y ? hy : y);
+    z = z < lz ? lz : (hz < z ? hz : z);
+    return make_double4(x, y, z, __longlong_as_double((long long)total));
+}
+
 // OctreeNodeUpdater::update_node for one dendrite type.
 __device__ __forceinline__ double4 update_type(const double4* rec, const uint2* topo, uint32_t base, uint32_t mask, double lx, double ly, double lz,
                                                double hx, double hy, double hz) {
@@ -380,16 +396,7 @@ __device__ __forceinline__ double4 update_type(const double4* rec, const uint2* 
             az = az + r.z * kd;
         }
     }
-    if (total == 0) {
-        const double nan = __longlong_as_double(0x7FF8000000000000ll);
-        return make_double4(nan, nan, nan, 0.0);
-    }
-    const double td = (double)total;
-    double x = ax / td, y = ay / td, z = az / td;
-    x = x < lx ? lx : (hx < x ? hx : x);
-    y = y < ly ? ly : (hy < y ? hy : y);
-    z = z < lz ? lz : (hz < z ? hz : z);
-    return make_double4(x, y, z, __longlong_as_double((long long)total));
+    return finish_centroid(ax, ay, az, total, lx, ly, lz, hx, hy, hz);
 }
 
 struct ReduceArgs {
@@ -401,13 +408,28 @@ struct ReduceArgs {
     double4* rec0;
     double4* rec1;
     uint32_t* arrive;
+    // leaf counts: vacant dendrites of the neurons that take part
+    const uint8_t* enabled;
+    const uint8_t* update;
+    const uint32_t* vac_exc;
+    const uint32_t* vac_inh;
 };
 
-// One level of the bottom-up reduction: one thread per node of the level; an
-// inner node is computed from its children (the next level, finished by the
-// previous launch), read in octant order as the reference sums them.  The
-// children of a node are contiguous, so neighbouring threads read neighbouring
-// records.
+__device__ __forceinline__ void set_leaf_counts(const ReduceArgs& A, uint32_t node, uint32_t nid, uint32_t& c0, uint32_t& c1) {
+    const bool on = A.enabled[nid] && A.update[nid];
+    c0 = on ? A.vac_exc[nid] : 0u;
+    c1 = on ? A.vac_inh[nid] : 0u;
+    reinterpret_cast<long long*>(&A.rec0[node])[3] = (long long)c0;
+    reinterpret_cast<long long*>(&A.rec1[node])[3] = (long long)c1;
+}
+
+// One level of the bottom-up reduction: one thread per node of the level.  An
+// inner node first refreshes the vacant counts of its leaf children
+// (OctreeAlgorithm::update_leaf_nodes) and then sums its children, read in
+// octant order as the reference sums them (inner children come from the
+// previous launch, one level deeper).  The children of a node are contiguous,
+// so neighbouring threads read and write neighbouring records.  A leaf at
+// level 0 (a network of one neuron) refreshes its own counts.
 __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
     const uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= hi) {
@@ -415,15 +437,51 @@ __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
     }
     const uint2 t = A.topo[node];
     if (topo_leaf(t.y)) {
+        if (topo_level(t.y) == 0) {
+            uint32_t c0, c1;
+            set_leaf_counts(A, node, t.x, c0, c1);
+        }
         return;
     }
     const uint32_t mask = topo_mask(t.y);
+    double ax0 = 0.0, ay0 = 0.0, az0 = 0.0, ax1 = 0.0, ay1 = 0.0, az1 = 0.0;
+    uint32_t tot0 = 0, tot1 = 0;
+    uint32_t k = 0;
+    for (int oct = 0; oct < 8; ++oct) {
+        if (!((mask >> oct) & 1u)) {
+            continue;
+        }
+        const uint32_t child = t.x + k++;
+        const uint2 tc = A.topo[child];
+        const bool leaf = topo_leaf(tc.y);
+        const double4 r0 = ldcg4(&A.rec0[child]);
+        const double4 r1 = ldcg4(&A.rec1[child]);
+        uint32_t c0, c1;
+        if (leaf) {
+            set_leaf_counts(A, child, tc.x, c0, c1);
+        } else {
+            c0 = rec_count(r0);
+            c1 = rec_count(r1);
+        }
+        tot0 += c0;
+        tot1 += c1;
+        if (leaf || c0 > 0) {
+            const double kd = (double)c0;
+            ax0 = ax0 + r0.x * kd;
+            ay0 = ay0 + r0.y * kd;
+            az0 = az0 + r0.z * kd;
+        }
+        if (leaf || c1 > 0) {
+            const double kd = (double)c1;
+            ax1 = ax1 + r1.x * kd;
+            ay1 = ay1 + r1.y * kd;
+            az1 = az1 + r1.z * kd;
+        }
+    }
     const double lx = A.bx0[node], ly = A.by0[node], lz = A.bz0[node];
     const double hx = A.bx1[node], hy = A.by1[node], hz = A.bz1[node];
-    const double4 r0 = update_type(A.rec0, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
-    const double4 r1 = update_type(A.rec1, A.topo, t.x, mask, lx, ly, lz, hx, hy, hz);
-    stcg4(&A.rec0[node], r0);
-    stcg4(&A.rec1[node], r1);
+    stcg4(&A.rec0[node], finish_centroid(ax0, ay0, az0, tot0, lx, ly, lz, hx, hy, hz));
+    stcg4(&A.rec1[node], finish_centroid(ax1, ay1, az1, tot1, lx, ly, lz, hx, hy, hz));
 }
 
 // One thread per leaf walks up; the last child to arrive at a node computes
@@ -461,6 +519,7 @@ void build_octree(Ctx& c, const double* h_xyz) {
     const uint32_t n = c.n;
     cudaStream_t st = c.stream;
     Tree& T = c.tree;
+    T.drop_graph();
     // positions to SoA on the host side of the copy
     std::vector<double> hx(n), hy(n), hz(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -625,12 +684,11 @@ void build_octree(Ctx& c, const double* h_xyz) {
 
 void update_tree(Ctx& c) {
     const uint32_t n = c.n;
-    cudaStream_t st = c.stream;
     Tree& T = c.tree;
-    k_leaf_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, T.leaf_of.p, c.nr.enabled.p, c.nr.update.p, c.nr.vacant[1].p, c.nr.vacant[2].p, T.rec[0].p,
-                                                      T.rec[1].p);
-    RL_LAUNCH_CHECK();
     if (T.root_is_leaf) {
+        // a single network of one neuron: the root is its leaf
+        k_leaf_counts<<<1, 32, 0, c.stream>>>(n, T.leaf_of.p, c.nr.enabled.p, c.nr.update.p, c.nr.vacant[1].p, c.nr.vacant[2].p, T.rec[0].p, T.rec[1].p);
+        RL_LAUNCH_CHECK();
         return;
     }
     ReduceArgs A;
@@ -647,18 +705,58 @@ void update_tree(Ctx& c) {
     A.rec0 = T.rec[0].p;
     A.rec1 = T.rec[1].p;
     A.arrive = nullptr;
-    // bottom-up, one launch per level; the deepest non-empty level holds leaves only
+    A.enabled = c.nr.enabled.p;
+    A.update = c.nr.update.p;
+    A.vac_exc = c.nr.vacant[1].p;
+    A.vac_inh = c.nr.vacant[2].p;
+    // bottom-up, one launch per level from the deepest level with inner nodes
     int deepest = (int)T.level_off.size() - 2;
     while (deepest > 0 && T.level_off[deepest + 1] == T.level_off[deepest]) {
         --deepest;
     }
-    for (int l = deepest - 1; l >= 0; --l) {
-        const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
-        if (hi > lo) {
-            k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(A, lo, hi);
-            RL_LAUNCH_CHECK();
+    auto enqueue = [&](cudaStream_t st) {
+        uint32_t kernels = 0;
+        for (int l = deepest > 0 ? deepest - 1 : 0; l >= 0; --l) {
+            const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
+            if (hi > lo) {
+                k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(A, lo, hi);
+                RL_LAUNCH_CHECK();
+                ++kernels;
+            }
         }
+        return kernels;
+    };
+    if (!c.use_graphs || c.stream == nullptr || c.capturing) {
+        enqueue(c.stream);
+        return;
     }
+    // the launches depend only on the octree's shape: captured once per build
+    if (T.update_graph == nullptr) {
+        const uint64_t launches = c.launches;
+        cudaGraph_t gr = nullptr;
+        RL_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        c.capturing = true;
+        try {
+            T.update_graph_kernels = enqueue(c.stream);
+        } catch (...) {
+            c.capturing = false;
+            cudaStreamEndCapture(c.stream, &gr);
+            if (gr) {
+                cudaGraphDestroy(gr);
+            }
+            throw;
+        }
+        c.capturing = false;
+        RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &gr));
+        c.launches = launches;
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        RL_CUDA_TRY(e);
+        T.update_graph = ex;
+    }
+    RL_CUDA_TRY(cudaGraphLaunch(T.update_graph, c.stream));
+    c.launches += T.update_graph_kernels;
 }
 
 void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_t* d_vac_inh, const uint8_t* d_update, uint32_t* arrive,

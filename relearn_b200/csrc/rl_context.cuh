@@ -38,6 +38,15 @@ struct Tree {
     DBuf<uint32_t> leaf_of;    // neuron -> node
     DBuf<uint32_t> morton;     // Morton rank -> neuron
     std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
+    cudaGraphExec_t update_graph = nullptr;  // the bottom-up update of this octree, captured once
+    uint32_t update_graph_kernels = 0;
+    void drop_graph() {
+        if (update_graph) {
+            cudaGraphExecDestroy(update_graph);
+            update_graph = nullptr;
+        }
+    }
+    ~Tree() { drop_graph(); }
     // FP32 form: records (centroid, count bits in w) and cell lengths as FP32
     DBuf<float4> rec32[2];
     DBuf<float> maxdim32;
@@ -176,6 +185,7 @@ struct SearchVariant {
 struct ActVariant {
     int block = 256;     // threads per block
     int persistent = 0;  // 1: one resident wave of blocks looping over the neurons
+    int vec = 1;         // neurons per thread (vector loads and stores; FP32 form)
 };
 
 enum : int { TUNE_OFF = 0, TUNE_REQUESTED = 1, TUNE_DONE = 2 };
@@ -220,6 +230,7 @@ struct Ctx {
     DBuf<uint32_t> to_delete;  // per neuron, bound elements to delete in the current pass
     DBuf<uint32_t> err;       // device error word
     DBuf<uint64_t> counters;  // device counters
+    DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
     int64_t device_bytes = 0;  // device memory held now
@@ -277,7 +288,12 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
 void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps);
 // Frees a context and everything it holds (after its stream has drained).
 void discard(Ctx* c);
-uint64_t run_commit(Ctx& c, int type);  // commit one element type; to_delete[] per neuron, returns the sum
+uint64_t run_commit(Ctx& c, int type);
+// Commit of `type` that does nothing when an earlier type of the same update
+// (its count in commit_cnt) left bound elements to delete; counts into
+// commit_cnt[type].  The three are launched back to back and read once.
+void launch_commit_guarded(Ctx& c, int type);
+void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n);  // commit one element type; to_delete[] per neuron, returns the sum
 
 void check_device_error(Ctx& c, const char* phase);
 

@@ -1,0 +1,400 @@
+// C++ host side of relearn-b200: the reference's plugin interfaces for the
+// structural-plasticity path, implemented over the C ABI of
+// include/relearn_b200.h (every call goes to the sm_100a kernels of
+// librelearn_b200.so; there is no CPU fallback).
+//
+// Names, argument meaning and error behaviour follow the reference (paths
+// relative to relearn/source of tuda-hpclab/relearn):
+//   * Algorithm (algorithm/Algorithm.h:48-197): init, prepare_update_connectivity
+//     with spans of signal types and vacant element counts, update_connectivity
+//     returning a ConnectivityUpdateResult, get_algorithm_type; BarnesHut is the
+//     --algorithm barnes-hut implementation.
+//   * NeuronModel (neurons/models/NeuronModelBase.h): update_electrical_activity
+//     per step and the per-neuron getters; IzhikevichModel is --neuron-model
+//     izhikevich (with the calcium and synaptic-element updates Neurons drives
+//     every step, neurons/Neurons.cpp:351-384).
+//   * Simulation::simulate (sim/Simulation.cpp:388-480): steps 1 .. number_steps + 1,
+//     plasticity every plasticity_update_step steps.
+//   * RelearnException::check / fail (util/RelearnException.h): every non-OK
+//     status becomes a RelearnException carrying the library's message.
+#pragma once
+
+#include <cstdint>
+#include <fstream>
+#include <memory>
+#include <span>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/relearn_b200.h"
+
+namespace relearn_b200 {
+
+class RelearnException : public std::runtime_error {
+public:
+    explicit RelearnException(const std::string& what, rl_status status = RL_ERR_INVALID)
+        : std::runtime_error(what), status_(status) { }
+
+    static void check(bool condition, const std::string& message) {
+        if (!condition) {
+            throw RelearnException(message);
+        }
+    }
+
+    [[noreturn]] static void fail(const std::string& message) { throw RelearnException(message); }
+
+    rl_status status() const { return status_; }
+
+private:
+    rl_status status_;
+};
+
+enum class SignalType : uint8_t { Excitatory = RL_EXCITATORY, Inhibitory = RL_INHIBITORY };
+enum class ElementType : int { Axon = RL_AXON, DendriteExcitatory = RL_DENDRITE_EXC, DendriteInhibitory = RL_DENDRITE_INH };
+enum class AlgorithmEnum { BarnesHut };
+enum class NeuronModelEnum { Izhikevich };
+
+using number_neurons_type = uint64_t;
+using counter_type = uint32_t;  // RelearnTypes::counter_type
+using step_type = uint32_t;
+
+namespace detail {
+inline void check_status(rl_status s, void* ctx, const char* what) {
+    if (s != RL_OK) {
+        std::string msg = std::string(what) + ": " + rl_status_string(s);
+        if (ctx) {
+            msg += " (" + std::string(rl_last_error(ctx)) + ")";
+        }
+        throw RelearnException(msg, s);
+    }
+}
+}  // namespace detail
+
+// Model parameters of one network; the reference defaults come from
+// rl_config_default.
+struct Parameters {
+    rl_config cfg{};
+
+    static Parameters defaults(uint32_t number_neurons, double side) {
+        Parameters p;
+        rl_config_default(&p.cfg, number_neurons, side);
+        return p;
+    }
+};
+
+// One network on one GPU: owns the library context.
+class Context {
+public:
+    explicit Context(const Parameters& p) {
+        void* h = nullptr;
+        detail::check_status(rl_ctx_create(&p.cfg, &h), nullptr, "rl_ctx_create");
+        ctx_ = h;
+        n_ = p.cfg.num_neurons;
+        interval_ = p.cfg.plasticity_interval;
+    }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
+    Context(Context&& o) noexcept : ctx_(std::exchange(o.ctx_, nullptr)), n_(o.n_), interval_(o.interval_) { }
+    ~Context() {
+        if (ctx_) {
+            rl_ctx_destroy(ctx_);
+        }
+    }
+
+    void* handle() const { return ctx_; }
+    number_neurons_type size() const { return n_; }
+    uint32_t plasticity_interval() const { return interval_; }
+    void check(rl_status s, const char* what) const { detail::check_status(s, ctx_, what); }
+
+    rl_stats stats() const {
+        rl_stats st{};
+        check(rl_get_stats(ctx_, &st), "rl_get_stats");
+        return st;
+    }
+
+private:
+    void* ctx_ = nullptr;
+    number_neurons_type n_ = 0;
+    uint32_t interval_ = 100;
+};
+
+struct SynapseCreationRequest {
+    uint32_t target;
+    uint32_t source;
+    SignalType signal_type;
+};
+
+struct PlasticLocalSynapse {
+    uint32_t target;
+    uint32_t source;
+    int32_t weight;
+};
+
+struct ConnectivityUpdateResult {
+    uint64_t number_synapses_created = 0;
+    std::vector<PlasticLocalSynapse> local_synapses;
+};
+
+// Algorithm: the connectivity update of the structural-plasticity model.
+class Algorithm {
+public:
+    virtual ~Algorithm() = default;
+    virtual void init(number_neurons_type number_neurons) = 0;
+    virtual void prepare_update_connectivity(std::span<const SignalType> signal_types, std::span<const counter_type> vacant_axons,
+                                             std::span<const counter_type> vacant_excitatory_dendrites,
+                                             std::span<const counter_type> vacant_inhibitory_dendrites) = 0;
+    [[nodiscard]] virtual ConnectivityUpdateResult update_connectivity(number_neurons_type number_neurons) = 0;
+    [[nodiscard]] virtual AlgorithmEnum get_algorithm_type() const = 0;
+};
+
+// --algorithm barnes-hut on the GPU.
+class BarnesHut final : public Algorithm {
+public:
+    // positions: 3 * n coordinates (x, y, z per neuron) in the simulation box.
+    BarnesHut(Context& ctx, std::span<const double> positions, std::span<const SignalType> signal_types)
+        : ctx_(ctx), positions_(positions.begin(), positions.end()), signal_(signal_types.size()) {
+        for (size_t i = 0; i < signal_types.size(); ++i) {
+            signal_[i] = static_cast<uint8_t>(signal_types[i]);
+        }
+    }
+
+    void init(number_neurons_type number_neurons) override {
+        RelearnException::check(number_neurons == ctx_.size(), "BarnesHut::init: number of neurons does not match the context");
+        RelearnException::check(positions_.size() == 3 * number_neurons && signal_.size() == number_neurons,
+                                "BarnesHut::init: positions or signal types have the wrong size");
+        ctx_.check(rl_set_positions(ctx_.handle(), positions_.data(), signal_.data()), "rl_set_positions");
+    }
+
+    void prepare_update_connectivity(std::span<const SignalType> signal_types, std::span<const counter_type> vacant_axons,
+                                     std::span<const counter_type> vacant_excitatory_dendrites,
+                                     std::span<const counter_type> vacant_inhibitory_dendrites) override {
+        const size_t n = ctx_.size();
+        RelearnException::check(signal_types.size() == n && vacant_axons.size() == n && vacant_excitatory_dendrites.size() == n &&
+                                    vacant_inhibitory_dendrites.size() == n,
+                                "BarnesHut::prepare_update_connectivity: spans must have one entry per neuron");
+        std::vector<uint8_t> sig(n);
+        for (size_t i = 0; i < n; ++i) {
+            sig[i] = static_cast<uint8_t>(signal_types[i]);
+        }
+        ctx_.check(rl_prepare_update_connectivity(ctx_.handle(), sig.data(), vacant_axons.data(), vacant_excitatory_dendrites.data(),
+                                                  vacant_inhibitory_dendrites.data(), nullptr),
+                   "rl_prepare_update_connectivity");
+        pending_axons_ = 0;
+        for (counter_type v : vacant_axons) {
+            pending_axons_ += v;
+        }
+    }
+
+    // Searches for every vacant axon of the last prepare_update_connectivity
+    // and connects the accepted requests (the caller's step number keys the
+    // random stream).
+    ConnectivityUpdateResult update_connectivity_at(step_type step) {
+        std::vector<rl_synapse> out(pending_axons_ ? pending_axons_ : 1);
+        uint64_t created = 0;
+        ctx_.check(rl_update_connectivity(ctx_.handle(), step, out.data(), out.size(), &created), "rl_update_connectivity");
+        ConnectivityUpdateResult r;
+        r.number_synapses_created = created;
+        r.local_synapses.reserve(created);
+        for (uint64_t k = 0; k < created && k < out.size(); ++k) {
+            r.local_synapses.push_back({ out[k].target, out[k].source, out[k].weight });
+        }
+        return r;
+    }
+
+    ConnectivityUpdateResult update_connectivity(number_neurons_type number_neurons) override {
+        RelearnException::check(number_neurons == ctx_.size(), "BarnesHut::update_connectivity: number of neurons does not match the context");
+        return update_connectivity_at(step_);
+    }
+
+    // The requests of one search pass without connecting them
+    // (BarnesHut::find_target_neurons).
+    std::vector<SynapseCreationRequest> find_target_neurons(step_type step) {
+        std::vector<rl_request> out(pending_axons_ ? pending_axons_ : 1);
+        uint64_t count = 0;
+        ctx_.check(rl_find_targets(ctx_.handle(), step, out.data(), out.size(), &count), "rl_find_targets");
+        std::vector<SynapseCreationRequest> r;
+        r.reserve(count);
+        for (uint64_t k = 0; k < count && k < out.size(); ++k) {
+            r.push_back({ out[k].target, out[k].source, out[k].signal ? SignalType::Inhibitory : SignalType::Excitatory });
+        }
+        return r;
+    }
+
+    void set_step(step_type step) { step_ = step; }
+
+    AlgorithmEnum get_algorithm_type() const override { return AlgorithmEnum::BarnesHut; }
+
+private:
+    Context& ctx_;
+    std::vector<double> positions_;
+    std::vector<uint8_t> signal_;
+    uint64_t pending_axons_ = 0;
+    step_type step_ = 0;
+};
+
+// NeuronModel: the electrical activity between plasticity updates.
+class NeuronModel {
+public:
+    virtual ~NeuronModel() = default;
+    virtual void update_electrical_activity(step_type step) = 0;
+    [[nodiscard]] virtual std::vector<double> get_x() const = 0;
+    [[nodiscard]] virtual std::vector<uint8_t> get_fired() const = 0;
+    [[nodiscard]] virtual NeuronModelEnum get_model_type() const = 0;
+};
+
+// --neuron-model izhikevich with the calcium and growth updates of each step.
+class IzhikevichModel final : public NeuronModel {
+public:
+    explicit IzhikevichModel(Context& ctx) : ctx_(ctx) { }
+
+    void update_electrical_activity(step_type step) override {
+        ctx_.check(rl_activity_block(ctx_.handle(), step, 1), "rl_activity_block");
+    }
+
+    // Steps first .. first + count - 1 at once (one launch each, or one CUDA
+    // graph per full plasticity interval).
+    void update_electrical_activity_block(step_type first, uint32_t count) {
+        ctx_.check(rl_activity_block(ctx_.handle(), first, count), "rl_activity_block");
+    }
+
+    std::vector<double> get_x() const override { return neurons().x; }
+    std::vector<uint8_t> get_fired() const override { return neurons().fired; }
+    std::vector<double> get_calcium() const { return neurons().calcium; }
+    NeuronModelEnum get_model_type() const override { return NeuronModelEnum::Izhikevich; }
+
+    struct State {
+        std::vector<double> x, u, calcium, input;
+        std::vector<uint8_t> fired;
+    };
+
+    State neurons() const {
+        const size_t n = ctx_.size();
+        State s{ std::vector<double>(n), std::vector<double>(n), std::vector<double>(n), std::vector<double>(n), std::vector<uint8_t>(n) };
+        ctx_.check(rl_get_neurons(ctx_.handle(), s.x.data(), s.u.data(), s.calcium.data(), s.fired.data(), s.input.data()), "rl_get_neurons");
+        return s;
+    }
+
+private:
+    Context& ctx_;
+};
+
+// Simulation::simulate on one GPU.
+class Simulation {
+public:
+    Simulation(const Parameters& params, std::span<const double> positions, std::span<const SignalType> signal_types,
+               const std::string& algorithm = "barnes-hut", const std::string& neuron_model = "izhikevich")
+        : ctx_(checked(params, algorithm, neuron_model)), algorithm_(ctx_, positions, signal_types), model_(ctx_) {
+        algorithm_.init(ctx_.size());
+    }
+
+    // Initial grown elements of one type (--synaptic-elements-lower-bound /
+    // --synaptic-elements-upper-bound draw these); vacant = floor(grown).
+    void set_initial_elements(ElementType type, std::span<const double> grown) {
+        const size_t n = ctx_.size();
+        RelearnException::check(grown.size() == n, "Simulation::set_initial_elements: one value per neuron");
+        std::vector<double> delta(n, 0.0);
+        std::vector<uint32_t> connected(n, 0u), vacant(n);
+        for (size_t i = 0; i < n; ++i) {
+            vacant[i] = static_cast<uint32_t>(grown[i]);
+        }
+        ctx_.check(rl_set_elements(ctx_.handle(), static_cast<int>(type), grown.data(), delta.data(), connected.data(), vacant.data()),
+                   "rl_set_elements");
+    }
+
+    // Runs number_steps + 1 steps, as the reference does.
+    void simulate(step_type number_steps) {
+        const uint32_t count = number_steps + 1;
+        ctx_.check(rl_simulate(ctx_.handle(), step_, count), "rl_simulate");
+        step_ += count;
+    }
+
+    struct Synapses {
+        std::vector<uint32_t> target, source;
+        std::vector<int32_t> weight;
+    };
+
+    Synapses synapses() const {
+        uint64_t m = 0;
+        ctx_.check(rl_get_edges(ctx_.handle(), nullptr, nullptr, nullptr, 0, &m), "rl_get_edges");
+        Synapses s{ std::vector<uint32_t>(m), std::vector<uint32_t>(m), std::vector<int32_t>(m) };
+        ctx_.check(rl_get_edges(ctx_.handle(), s.target.data(), s.source.data(), s.weight.data(), m, &m), "rl_get_edges");
+        return s;
+    }
+
+    std::vector<uint32_t> connected(ElementType type) const {
+        std::vector<uint32_t> c(ctx_.size());
+        ctx_.check(rl_get_elements(ctx_.handle(), static_cast<int>(type), nullptr, nullptr, c.data(), nullptr), "rl_get_elements");
+        return c;
+    }
+
+    Context& context() { return ctx_; }
+    BarnesHut& algorithm() { return algorithm_; }
+    IzhikevichModel& neuron_model() { return model_; }
+    step_type current_step() const { return step_; }
+
+private:
+    static const Parameters& checked(const Parameters& p, const std::string& algorithm, const std::string& neuron_model) {
+        if (algorithm != "barnes-hut") {
+            throw RelearnException("algorithm '" + algorithm + "' is not built here (have barnes-hut)", RL_ERR_UNSUPPORTED);
+        }
+        if (neuron_model != "izhikevich") {
+            throw RelearnException("neuron model '" + neuron_model + "' is not built here (have izhikevich)", RL_ERR_UNSUPPORTED);
+        }
+        return p;
+    }
+
+    Context ctx_;
+    BarnesHut algorithm_;
+    IzhikevichModel model_;
+    step_type step_ = 1;
+};
+
+}  // namespace relearn_b200
+
+namespace relearn_b200 {
+
+// A positions file in the reference's format (NeuronIO::read_neuron_positions_and_signals,
+// io/NeuronIO.cpp:229-300): '#' comment lines, then one neuron per line as
+// "id x y z signal" with ids 1, 2, ... in order, non-negative coordinates and
+// signal "in" for inhibitory (anything else excitatory).
+struct LoadedNeurons {
+    std::vector<double> positions;  // x, y, z per neuron
+    std::vector<SignalType> signal_types;
+    double maximum[3] = { 0.0, 0.0, 0.0 };
+};
+
+inline LoadedNeurons read_neuron_positions_and_signals(const std::string& path) {
+    std::ifstream file(path);
+    RelearnException::check(file.good(), "read_neuron_positions_and_signals: cannot open '" + path + "'");
+    LoadedNeurons out;
+    uint64_t expected = 0;
+    std::string line;
+    while (std::getline(file, line)) {
+        if (line.empty() || line[0] == '#') {
+            continue;
+        }
+        std::istringstream ss(line);
+        uint64_t id = 0;
+        double x = 0, y = 0, z = 0;
+        std::string signal;
+        if (!(ss >> id >> x >> y >> z >> signal)) {
+            continue;  // the reference skips lines it cannot parse
+        }
+        RelearnException::check(x >= 0 && y >= 0 && z >= 0, "read_neuron_positions_and_signals: negative position of neuron " + std::to_string(id));
+        RelearnException::check(id >= 1, "read_neuron_positions_and_signals: neuron id is too small");
+        RelearnException::check(id - 1 == expected, "read_neuron_positions_and_signals: loaded neuron " + std::to_string(id - 1) + " but expected " +
+                                                        std::to_string(expected));
+        ++expected;
+        out.positions.insert(out.positions.end(), { x, y, z });
+        out.signal_types.push_back(signal == "in" ? SignalType::Inhibitory : SignalType::Excitatory);
+        out.maximum[0] = x > out.maximum[0] ? x : out.maximum[0];
+        out.maximum[1] = y > out.maximum[1] ? y : out.maximum[1];
+        out.maximum[2] = z > out.maximum[2] ? z : out.maximum[2];
+    }
+    return out;
+}
+
+}  // namespace relearn_b200
