@@ -92,7 +92,8 @@ typedef struct rl_config {
 /* Precision forms.  FP64: the drop-in; every FP64 operation in the reference's
  * order, bit-exact against the oracle.  FP32: membrane, input, growth and
  * attraction arithmetic in FP32 with Kahan-compensated attraction sums; calcium
- * integrated in FP64; octree centroids reduced in FP64 and read as FP32. */
+ * integrated in FP64; octree centroids reduced in FP64 and read by the search
+ * in 32-bit fixed point. */
 enum { RL_PRECISION_FP64 = 0, RL_PRECISION_FP32 = 1 };
 
 /* One synapse creation request (SynapseCreationRequest,

@@ -179,9 +179,24 @@ void setup_nets(Ctx& c, const rl_network* nets, uint32_t num) {
             N.nu32[a] = (float)N.nu[a];
         }
         N.root_leaf = 0;
+        // fixed-point frame of the FP32 search
+        const double extent = std::max(N.box_max[0] - N.box_min[0], std::max(N.box_max[1] - N.box_min[1], N.box_max[2] - N.box_min[2]));
+        double quantum = 1.0;
+        while (quantum * 1073741824.0 < extent) {
+            quantum *= 2.0;
+        }
+        while (quantum * 0.5 * 1073741824.0 >= extent && quantum > 1e-30) {
+            quantum *= 0.5;
+        }
+        for (int a = 0; a < 3; ++a) {
+            N.frame.origin[a] = N.box_min[a];
+        }
+        N.frame.quantum = (float)quantum;
+        N.frame.inv_quantum = 1.0 / quantum;
         c.nets.push_back(N);
     }
     RL_CHECK(first == c.n, RL_ERR_INVALID, "network sizes do not add up to num_neurons");
+
     RL_CHECK(c.nets.size() <= 65535, RL_ERR_UNSUPPORTED, "at most 65535 networks per context");
     c.d_nets.alloc(c.nets.size());
     RL_CUDA_TRY(cudaMemcpyAsync(c.d_nets.p, c.nets.data(), c.nets.size() * sizeof(NetInfo), cudaMemcpyHostToDevice, c.stream));

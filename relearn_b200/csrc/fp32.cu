@@ -11,7 +11,11 @@
 //     h substeps are applied at once as c*A^h + s*beta*fired*(A^(h-1)+...+1)
 //     with both factors precomputed in FP64;
 //   * octree counts and centroids reduced in FP64 (octree.cu), then read by
-//     the search as FP32 records (16 B instead of 32 B);
+//     the search as 16-byte records with the centroid in 32-bit fixed point
+//     (QFrame): a coordinate difference is exact in the integers and rounds
+//     once when it becomes a float, so distances keep FP32 relative precision
+//     even between cells far from the origin (FP32 coordinates would round
+//     each coordinate to its own magnitude);
 //   * attraction weights exp(-(d-mu)^2/sigma^2)*count in FP32, summed per lane in
 //     visiting order with Kahan compensation; the pick compares the
 //     compensated running sum with r.
@@ -56,10 +60,15 @@ struct Act32 {
     float* delta[3];
     float conductance, noise_mean, noise_stddev;
     uint32_t h_model;
-    // one Euler substep with s = 1/h, rearranged to five FP32 operations:
-    //   x' = x (1 + s k2 + s k1 x) + s (k3 + I) - s u
-    //   u' = u (1 - s a) + s a b x
-    float c, d, v_spike, s, sk1, one_sk2, sk3, sab, one_sa;
+    // one Euler substep with s = 1/h as two increments, each rounded at its own
+    // (small) magnitude before it is added:
+    //   x' = x + [x (s k1 x + s k2) + (s k3 + s I) - s u]
+    //   u' = u + [s a b x - s a u]
+    // (folding the 1 into the factor, x' = x (1 + s k2 + s k1 x) + ..., saves
+    // one operation but rounds at the magnitude of x twice and biased the
+    // firing rate by +2.4e-5 against FP64 in a 200,000-neuron, 1,000-step
+    // check; this form: +2.5e-6)
+    float c, d, v_spike, s, sk1, sk2, sk3, sab, sa;
     double ca_mul, ca_add;  // calcium: c <- c*ca_mul + fired*ca_add
     float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
@@ -133,13 +142,13 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     float uv = u;
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
-    const float sI = fmaf(A.s, input, A.sk3);
+    const float sc = fmaf(A.s, input, A.sk3);
     const float ms = -A.s;
 #pragma unroll
     for (uint32_t it = 0; it < h; ++it) {
-        const float xn = fmaf(xv, fmaf(A.sk1, xv, A.one_sk2), fmaf(ms, uv, sI));
-        uv = fmaf(A.sab, xv, uv * A.one_sa);
-        xv = xn;
+        const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
+        uv = uv + fmaf(A.sab, xv, -A.sa * uv);
+        xv = xv + inc;
         if (xv >= A.v_spike) {
             xv = A.c;
             uv += A.d;
@@ -350,16 +359,18 @@ __global__ void k_commit_f32(uint32_t n, const uint8_t* __restrict__ enabled, do
     }
 }
 
-__global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4* __restrict__ r1, const double* __restrict__ md, float4* __restrict__ o0,
-                       float4* __restrict__ o1, float* __restrict__ omd) {
+// FP64 records -> fixed-point records (in the frame of the node's network,
+// found through the first neuron under the node) and FP32 cell lengths.
+__global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4* __restrict__ r1, const double* __restrict__ md, uint4* __restrict__ o0,
+                       uint4* __restrict__ o1, float* __restrict__ omd, const uint32_t* __restrict__ first_key, const uint32_t* __restrict__ morton,
+                       const uint16_t* __restrict__ net_of, const NetInfo* __restrict__ nets) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) {
         return;
     }
-    const double4 a = r0[i];
-    const double4 b = r1[i];
-    o0[i] = make_float4((float)a.x, (float)a.y, (float)a.z, __uint_as_float((uint32_t)__double_as_longlong(a.w)));
-    o1[i] = make_float4((float)b.x, (float)b.y, (float)b.z, __uint_as_float((uint32_t)__double_as_longlong(b.w)));
+    const QFrame& f = nets[net_of[morton[first_key[i]]]].frame;
+    o0[i] = quantize_record(r0[i], f);
+    o1[i] = quantize_record(r1[i], f);
     omd[i] = (float)md[i];
 }
 
@@ -368,7 +379,7 @@ constexpr int kStack = kMaxLevels + 4;  // the diagnostic walk
 enum : int { S_DISCARD = 0, S_EXPAND = 1, S_ACCEPT = 2 };
 
 struct Search32 {
-    const float4* rec;
+    const uint4* rec;
     const uint2* topo;
     const float* maxdim;
     const double *px, *py, *pz;
@@ -393,6 +404,7 @@ struct Net32 {
     uint64_t seed;
     uint32_t root;
     uint32_t first;
+    float quantum;
 };
 
 struct KSum {
@@ -410,14 +422,23 @@ struct E32 {
     float w;
 };
 
-__device__ __forceinline__ E32 eval32(const float4& r, uint2 t, float md, float sx, float sy, float sz, uint32_t source, const Search32& A, const Net32& W,
-                                      bool fb) {
+// Source position in the fixed-point frame.
+struct QPos {
+    uint32_t x, y, z;
+};
+
+__device__ __forceinline__ float qdiff(uint32_t a, uint32_t b, float quantum) {
+    return (float)(int32_t)(a - b) * quantum;
+}
+
+__device__ __forceinline__ E32 eval32(const uint4& r, uint2 t, float md, const QPos& s, uint32_t source, const Search32& A, const Net32& W, bool fb) {
     E32 e{ S_DISCARD, 0.0f };
-    const uint32_t cnt = __float_as_uint(r.w);
+    const uint32_t cnt = r.w;
     if (cnt == 0) {
         return e;
     }
-    const float dx = r.x - sx, dy = r.y - sy, dz = r.z - sz;
+    const float q = W.quantum;
+    const float dx = qdiff(r.x, s.x, q), dy = qdiff(r.y, s.y, q), dz = qdiff(r.z, s.z, q);
     const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
     if (d == 0.0f) {
         return e;
@@ -456,13 +477,13 @@ struct Walk32 {
 };
 
 template <int SD>
-__device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, float sx, float sy,
-                              float sz, uint32_t source, bool fb) {
+__device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, const QPos& sp,
+                              uint32_t source, bool fb) {
     Walk32 res{ start, -1, false };
     uint32_t fnode[SD];
     uint32_t frem[SD];
     if (include_root) {
-        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sx, sy, sz, source, A, W, fb);
+        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -488,7 +509,7 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
         frem[top] = rem & ~(1u << oct);
         const uint32_t child = child_of(A.topo[fnode[top]], oct);
         const uint2 tt = A.topo[child];
-        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sx, sy, sz, source, A, W, fb);
+        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -510,8 +531,8 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
 
 // Packet walk of the lanes in packet mask `pm` (see the FP64 search).
 template <int SD>
-__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, float sx, float sy, float sz, uint32_t source, bool fb,
-                         float2* cp, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
+__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb, float2* cp,
+                         uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
     const int lane = threadIdx.x & 31;
     const bool leader = lane == __ffs(pm) - 1;
     const bool me = (lanes >> lane) & 1u;
@@ -541,12 +562,12 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_
             cp[oct * 32] = make_float2(sum.s, sum.c);
         }
         const uint32_t child = child_of(A.topo[node], oct);
-        const float4 rr = A.rec[child];
+        const uint4 rr = A.rec[child];
         const uint2 tt = A.topo[child];
         const float md = A.maxdim[child];
         int status = S_DISCARD;
         if ((act >> lane) & 1u) {
-            const E32 e = eval32(rr, tt, md, sx, sy, sz, source, A, W, fb);
+            const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
             status = e.status;
             if (e.status == S_ACCEPT) {
                 sum.add(e.w);
@@ -597,7 +618,7 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
         }
     }
     const NetInfo& N = A.nets[A.seg_net[lo]];
-    const Net32 W{ N.theta32, N.inv_sigma2_32, N.seed, A.seg_net[lo], N.first };
+    const Net32 W{ N.theta32, N.inv_sigma2_32, N.seed, A.seg_net[lo], N.first, N.frame.quantum };
     const uint64_t idx = A.seg_begin[lo] + (uint64_t)(warp_global - A.seg_warp[lo]) * 32 + lane;
     const bool active = idx < A.seg_end[lo];
     if (N.root_leaf) {
@@ -608,9 +629,10 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
     }
     const uint32_t source = active ? A.list_src[idx] : 0u;
     const uint32_t j = active ? A.list_j[idx] : 0u;
-    const float sx = active ? (float)A.px[source] : 0.0f;
-    const float sy = active ? (float)A.py[source] : 0.0f;
-    const float sz = active ? (float)A.pz[source] : 0.0f;
+    const QFrame& F = N.frame;
+    const QPos sp = active ? QPos{ quantize(A.px[source], F.origin[0], F.inv_quantum), quantize(A.py[source], F.origin[1], F.inv_quantum),
+                                   quantize(A.pz[source], F.origin[2], F.inv_quantum) }
+                           : QPos{ 0u, 0u, 0u };
     float2* cp = &s_cp[wib][lane];
     bool overflow = false;
     const uint32_t lanes = __ballot_sync(pm, active);
@@ -618,11 +640,11 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
-        KSum total = packet32<SD>(A, W, pm, lanes, sx, sy, sz, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+        KSum total = packet32<SD>(A, W, pm, lanes, sp, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
         bool fb = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total.s == 0.0f);
         if (need_fb) {
-            const KSum t2 = packet32<SD>(A, W, pm, need_fb, sx, sy, sz, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+            const KSum t2 = packet32<SD>(A, W, pm, need_fb, sp, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
             if ((need_fb >> lane) & 1u) {
                 total = t2;
                 fb = true;
@@ -647,7 +669,7 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
                 done = true;
             } else {
                 const float2 c0 = cp[cstar * 32];
-                const Walk32 wr = lane_walk32<SD>(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sx, sy, sz, source, fb);
+                const Walk32 wr = lane_walk32<SD>(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sp, source, fb);
                 overflow |= wr.overflow;
                 if (wr.picked < 0) {
                     done = true;  // rounding left the crossing past the last candidate: no pick
@@ -667,10 +689,10 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
             result = (int32_t)st.x;
             break;
         }
-        Walk32 s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, false);
+        Walk32 s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, false);
         bool f = false;
         if (s1.sum.s == 0.0f) {
-            s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sx, sy, sz, source, true);
+            s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, true);
             f = true;
         }
         overflow |= s1.overflow;
@@ -678,7 +700,7 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
             break;
         }
         const float r = threshold32(s1.sum.s, A, W, source, j, depth);
-        const Walk32 s2 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sx, sy, sz, source, f);
+        const Walk32 s2 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sp, source, f);
         if (s2.picked < 0) {
             break;
         }
@@ -707,9 +729,10 @@ Search32Kernel fp32_search_kernel(const SearchVariant& v) {
 }
 
 // ----------------------------------------------------------- diagnostic
-__global__ void k_candidates(const double4* rec64, const float4* rec32, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
+__global__ void k_candidates(const double4* rec64, const uint4* recq, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
                              double sz, uint32_t source, uint32_t root, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
-                             uint64_t capacity, unsigned long long* count, uint32_t* err) {
+                             uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f) {
+    const QPos sp{ quantize(sx, f.origin[0], f.inv_quantum), quantize(sy, f.origin[1], f.inv_quantum), quantize(sz, f.origin[2], f.inv_quantum) };
     uint32_t fnode[kStack];
     uint32_t frem[kStack];
     int depth = 1;
@@ -747,10 +770,10 @@ __global__ void k_candidates(const double4* rec64, const float4* rec32, const ui
                 }
             }
         } else {
-            const float4 r = rec32[child];
-            const uint32_t cnt = __float_as_uint(r.w);
+            const uint4 r = recq[child];
+            const uint32_t cnt = r.w;
             if (cnt) {
-                const float dx = r.x - (float)sx, dy = r.y - (float)sy, dz = r.z - (float)sz;
+                const float dx = qdiff(r.x, sp.x, f.quantum), dy = qdiff(r.y, sp.y, f.quantum), dz = qdiff(r.z, sp.z, f.quantum);
                 const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
                 if (d != 0.0f) {
                     if (!leaf && !(md32[child] < (float)theta * d)) {
@@ -881,10 +904,10 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     const double sm = 1.0 / (double)k.h_model;
     A.s = (float)sm;
     A.sk1 = (float)(sm * k.iz_k1);
-    A.one_sk2 = (float)(1.0 + sm * k.iz_k2);
+    A.sk2 = (float)(sm * k.iz_k2);
     A.sk3 = (float)(sm * k.iz_k3);
     A.sab = (float)(sm * k.iz_a * k.iz_b);
-    A.one_sa = (float)(1.0 - sm * k.iz_a);
+    A.sa = (float)(sm * k.iz_a);
     A.c = (float)k.iz_c;
     A.d = (float)k.iz_d;
     A.v_spike = (float)k.iz_v_spike;
@@ -938,18 +961,23 @@ uint64_t run_commit_f32(Ctx& c, int type) {
 
 void pack_tree_f32(Ctx& c) {
     Tree& T = c.tree;
+    if (T.recq_valid) {
+        return;  // kept in step by the incremental octree update
+    }
     const uint32_t m = T.num_nodes;
-    T.rec32[0].ensure(m);
-    T.rec32[1].ensure(m);
+    T.recq[0].ensure(m);
+    T.recq[1].ensure(m);
     T.maxdim32.ensure(m);
-    k_pack<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, T.rec[0].p, T.rec[1].p, T.maxdim.p, T.rec32[0].p, T.rec32[1].p, T.maxdim32.p);
+    k_pack<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, T.rec[0].p, T.rec[1].p, T.maxdim.p, T.recq[0].p, T.recq[1].p, T.maxdim32.p, T.first_key.p,
+                                                     T.morton.p, c.net_of.p, c.d_nets.p);
     RL_LAUNCH_CHECK();
+    T.recq_valid = true;
 }
 
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
                        uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v) {
     Search32 A;
-    A.rec = c.tree.rec32[type].p;
+    A.rec = c.tree.recq[type].p;
     A.topo = c.tree.topo.p;
     A.maxdim = c.tree.maxdim32.p;
     A.px = c.nr.px.p;
@@ -997,9 +1025,9 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
     dn.alloc(cap);
     dw.alloc(cap);
     dc.alloc(1);
-    k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.rec32[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
+    k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.recq[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
                                         precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, net, precision,
-                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p);
+                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame);
     RL_LAUNCH_CHECK();
     unsigned long long k = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&k, dc.p, sizeof(k), cudaMemcpyDeviceToHost, c.stream));

@@ -408,41 +408,66 @@ struct ReduceArgs {
     double4* rec0;
     double4* rec1;
     uint32_t* arrive;
+    // incremental update: nodes to recompute, and the leaf counts of the last update
+    uint8_t* dirty;
+    uint2* last;
     // leaf counts: vacant dendrites of the neurons that take part
     const uint8_t* enabled;
     const uint8_t* update;
     const uint32_t* vac_exc;
     const uint32_t* vac_inh;
+    int force;  // every leaf counts as changed
+    // FP32 form: fixed-point records kept in step (null otherwise)
+    uint4* recq0;
+    uint4* recq1;
+    const uint32_t* first_key;
+    const uint32_t* morton;
+    const uint16_t* net_of;
+    const NetInfo* nets;
 };
 
-__device__ __forceinline__ void set_leaf_counts(const ReduceArgs& A, uint32_t node, uint32_t nid, uint32_t& c0, uint32_t& c1) {
-    const bool on = A.enabled[nid] && A.update[nid];
-    c0 = on ? A.vac_exc[nid] : 0u;
-    c1 = on ? A.vac_inh[nid] : 0u;
-    reinterpret_cast<long long*>(&A.rec0[node])[3] = (long long)c0;
-    reinterpret_cast<long long*>(&A.rec1[node])[3] = (long long)c1;
+// Leaf pass of the incremental update (OctreeAlgorithm::update_leaf_nodes):
+// one thread per neuron; a leaf whose vacant counts differ from the last
+// update gets the new counts and marks its parent for recomputation.
+__global__ void k_leaf_update(ReduceArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    const bool on = A.enabled[i] && A.update[i];
+    const uint2 now = make_uint2(on ? A.vac_exc[i] : 0u, on ? A.vac_inh[i] : 0u);
+    const uint2 was = A.last[i];
+    if (!A.force && now.x == was.x && now.y == was.y) {
+        return;
+    }
+    A.last[i] = now;
+    const uint32_t leaf = A.leaf_of[i];
+    reinterpret_cast<long long*>(&A.rec0[leaf])[3] = (long long)now.x;
+    reinterpret_cast<long long*>(&A.rec1[leaf])[3] = (long long)now.y;
+    if (A.recq0) {
+        A.recq0[leaf].w = now.x;
+        A.recq1[leaf].w = now.y;
+    }
+    const int32_t p = A.parent[leaf];
+    if (p >= 0) {
+        A.dirty[p] = 1;
+    }
 }
 
-// One level of the bottom-up reduction: one thread per node of the level.  An
-// inner node first refreshes the vacant counts of its leaf children
-// (OctreeAlgorithm::update_leaf_nodes) and then sums its children, read in
-// octant order as the reference sums them (inner children come from the
-// previous launch, one level deeper).  The children of a node are contiguous,
-// so neighbouring threads read and write neighbouring records.  A leaf at
-// level 0 (a network of one neuron) refreshes its own counts.
+// One level of the bottom-up reduction: one thread per node of the level; a
+// node marked dirty is recomputed from its children (leaves refreshed by the
+// leaf pass, inner children by the previous launch, one level deeper), read in
+// octant order as the reference sums them (OctreeNodeUpdater::update_node),
+// and marks its parent.  Recomputing only the nodes above changed leaves gives
+// the same records as recomputing all.  The children of a node are contiguous,
+// so neighbouring threads read neighbouring records.
 __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
     const uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= hi) {
+    if (node >= hi || !A.dirty[node]) {
         return;
     }
+    A.dirty[node] = 0;
     const uint2 t = A.topo[node];
-    if (topo_leaf(t.y)) {
-        if (topo_level(t.y) == 0) {
-            uint32_t c0, c1;
-            set_leaf_counts(A, node, t.x, c0, c1);
-        }
-        return;
-    }
     const uint32_t mask = topo_mask(t.y);
     double ax0 = 0.0, ay0 = 0.0, az0 = 0.0, ax1 = 0.0, ay1 = 0.0, az1 = 0.0;
     uint32_t tot0 = 0, tot1 = 0;
@@ -452,17 +477,10 @@ __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
             continue;
         }
         const uint32_t child = t.x + k++;
-        const uint2 tc = A.topo[child];
-        const bool leaf = topo_leaf(tc.y);
+        const bool leaf = topo_leaf(A.topo[child].y);
         const double4 r0 = ldcg4(&A.rec0[child]);
         const double4 r1 = ldcg4(&A.rec1[child]);
-        uint32_t c0, c1;
-        if (leaf) {
-            set_leaf_counts(A, child, tc.x, c0, c1);
-        } else {
-            c0 = rec_count(r0);
-            c1 = rec_count(r1);
-        }
+        const uint32_t c0 = rec_count(r0), c1 = rec_count(r1);
         tot0 += c0;
         tot1 += c1;
         if (leaf || c0 > 0) {
@@ -480,8 +498,19 @@ __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
     }
     const double lx = A.bx0[node], ly = A.by0[node], lz = A.bz0[node];
     const double hx = A.bx1[node], hy = A.by1[node], hz = A.bz1[node];
-    stcg4(&A.rec0[node], finish_centroid(ax0, ay0, az0, tot0, lx, ly, lz, hx, hy, hz));
-    stcg4(&A.rec1[node], finish_centroid(ax1, ay1, az1, tot1, lx, ly, lz, hx, hy, hz));
+    const double4 n0 = finish_centroid(ax0, ay0, az0, tot0, lx, ly, lz, hx, hy, hz);
+    const double4 n1 = finish_centroid(ax1, ay1, az1, tot1, lx, ly, lz, hx, hy, hz);
+    stcg4(&A.rec0[node], n0);
+    stcg4(&A.rec1[node], n1);
+    if (A.recq0) {
+        const QFrame& f = A.nets[A.net_of[A.morton[A.first_key[node]]]].frame;
+        A.recq0[node] = quantize_record(n0, f);
+        A.recq1[node] = quantize_record(n1, f);
+    }
+    const int32_t p = A.parent[node];
+    if (p >= 0) {
+        A.dirty[p] = 1;
+    }
 }
 
 // One thread per leaf walks up; the last child to arrive at a node computes
@@ -520,6 +549,8 @@ void build_octree(Ctx& c, const double* h_xyz) {
     cudaStream_t st = c.stream;
     Tree& T = c.tree;
     T.drop_graph();
+    T.force_full = true;
+    T.recq_valid = false;
     // positions to SoA on the host side of the copy
     std::vector<double> hx(n), hy(n), hz(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -612,6 +643,9 @@ void build_octree(Ctx& c, const double* h_xyz) {
         T.bmax[a].alloc(m);
     }
     T.parent.alloc(m);
+    T.dirty.alloc(m);
+    RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m, st));
+    T.last_counts.alloc(n);
     T.first_key.alloc(m);
     T.leaf_of.alloc(n);
     T.morton.alloc(n);
@@ -685,12 +719,6 @@ void build_octree(Ctx& c, const double* h_xyz) {
 void update_tree(Ctx& c) {
     const uint32_t n = c.n;
     Tree& T = c.tree;
-    if (T.root_is_leaf) {
-        // a single network of one neuron: the root is its leaf
-        k_leaf_counts<<<1, 32, 0, c.stream>>>(n, T.leaf_of.p, c.nr.enabled.p, c.nr.update.p, c.nr.vacant[1].p, c.nr.vacant[2].p, T.rec[0].p, T.rec[1].p);
-        RL_LAUNCH_CHECK();
-        return;
-    }
     ReduceArgs A;
     A.n = n;
     A.leaf_of = T.leaf_of.p;
@@ -705,39 +733,64 @@ void update_tree(Ctx& c) {
     A.rec0 = T.rec[0].p;
     A.rec1 = T.rec[1].p;
     A.arrive = nullptr;
+    A.dirty = T.dirty.p;
+    A.last = T.last_counts.p;
     A.enabled = c.nr.enabled.p;
     A.update = c.nr.update.p;
     A.vac_exc = c.nr.vacant[1].p;
     A.vac_inh = c.nr.vacant[2].p;
+    // the FP32 form's fixed-point records follow the update once they exist
+    const bool keep_q = is_fp32(c) && T.recq_valid;
+    if (!keep_q) {
+        T.recq_valid = false;
+    }
+    A.recq0 = keep_q ? T.recq[0].p : nullptr;
+    A.recq1 = keep_q ? T.recq[1].p : nullptr;
+    A.first_key = T.first_key.p;
+    A.morton = T.morton.p;
+    A.net_of = c.net_of.p;
+    A.nets = c.d_nets.p;
     // bottom-up, one launch per level from the deepest level with inner nodes
     int deepest = (int)T.level_off.size() - 2;
     while (deepest > 0 && T.level_off[deepest + 1] == T.level_off[deepest]) {
         --deepest;
     }
-    auto enqueue = [&](cudaStream_t st) {
-        uint32_t kernels = 0;
-        for (int l = deepest > 0 ? deepest - 1 : 0; l >= 0; --l) {
+    auto enqueue = [&](cudaStream_t st, int force) {
+        ReduceArgs a = A;
+        a.force = force;
+        k_leaf_update<<<blocks_for(n, 256), 256, 0, st>>>(a);
+        RL_LAUNCH_CHECK();
+        uint32_t kernels = 1;
+        for (int l = deepest - 1; l >= 0; --l) {
             const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
             if (hi > lo) {
-                k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(A, lo, hi);
+                k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(a, lo, hi);
                 RL_LAUNCH_CHECK();
                 ++kernels;
             }
         }
         return kernels;
     };
-    if (!c.use_graphs || c.stream == nullptr || c.capturing) {
-        enqueue(c.stream);
+    // the first update after a build (or after an update outside this path)
+    // takes every leaf as changed
+    const int force = T.force_full ? 1 : 0;
+    T.force_full = false;
+    if (force || !c.use_graphs || c.stream == nullptr || c.capturing) {
+        enqueue(c.stream, force);
         return;
+    }
+    if (T.update_graph != nullptr && keep_q != T.graph_keeps_q) {
+        T.drop_graph();
     }
     // the launches depend only on the octree's shape: captured once per build
     if (T.update_graph == nullptr) {
+        T.graph_keeps_q = keep_q;
         const uint64_t launches = c.launches;
         cudaGraph_t gr = nullptr;
         RL_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
         c.capturing = true;
         try {
-            T.update_graph_kernels = enqueue(c.stream);
+            T.update_graph_kernels = enqueue(c.stream, 0);
         } catch (...) {
             c.capturing = false;
             cudaStreamEndCapture(c.stream, &gr);
@@ -763,6 +816,9 @@ void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_
                                 cudaStream_t st) {
     const uint32_t n = c.n;
     Tree& T = c.tree;
+    // this update bypasses the incremental bookkeeping: the next regular one is complete
+    T.force_full = true;
+    T.recq_valid = false;
     k_leaf_counts<<<blocks_for(n, 256), 256, 0, st>>>(n, T.leaf_of.p, c.nr.enabled.p, d_update ? d_update : c.nr.enabled.p, d_vac_exc, d_vac_inh,
                                                       T.rec[0].p, T.rec[1].p);
     RL_LAUNCH_CHECK();

@@ -38,6 +38,11 @@ struct Tree {
     DBuf<uint32_t> leaf_of;    // neuron -> node
     DBuf<uint32_t> morton;     // Morton rank -> neuron
     std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
+    DBuf<uint8_t> dirty;        // nodes to recompute in the running update
+    DBuf<uint2> last_counts;    // per neuron: leaf counts (exc, inh) of the last update
+    bool force_full = true;     // next update takes every leaf as changed
+    bool recq_valid = false;    // fixed-point records match the FP64 records
+    bool graph_keeps_q = false; // the captured update also maintains them
     cudaGraphExec_t update_graph = nullptr;  // the bottom-up update of this octree, captured once
     uint32_t update_graph_kernels = 0;
     void drop_graph() {
@@ -48,7 +53,7 @@ struct Tree {
     }
     ~Tree() { drop_graph(); }
     // FP32 form: records (centroid, count bits in w) and cell lengths as FP32
-    DBuf<float4> rec32[2];
+    DBuf<uint4> recq[2];  // centroid in fixed point (QFrame), w = count
     DBuf<float> maxdim32;
 };
 
@@ -138,6 +143,31 @@ struct PhaseTimer {
 // forest whose root of network k is node k; every random draw of a neuron is
 // keyed on the network's seed and the neuron's index inside its network, so a
 // network evolves exactly as it would alone.
+// Fixed-point frame of a network for the FP32 search: a coordinate x is stored
+// as the integer round((x - origin) / quantum) in [0, 2^30], origin = the
+// network's box_min, quantum = the smallest power of two that maps the box's
+// longest edge into 2^30 steps.  The difference of two stored coordinates
+// converts to micrometres exactly up to the float rounding of the difference
+// itself (distances keep their relative precision however far from the origin
+// the cells lie), and each network's frame depends on its own box only.
+struct QFrame {
+    double origin[3] = { 0.0, 0.0, 0.0 };
+    double inv_quantum = 1.0;  // 1 / quantum
+    float quantum = 1.0f;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t quantize(double x, double origin, double inv_quantum) {
+    const double q = (x - origin) * inv_quantum;
+    return q > 0.0 ? (uint32_t)__double2uint_rn(q) : 0u;  // also 0 for the NaN centroid of an empty cell
+}
+
+__device__ __forceinline__ uint4 quantize_record(const double4& r, const QFrame& f) {
+    return make_uint4(quantize(r.x, f.origin[0], f.inv_quantum), quantize(r.y, f.origin[1], f.inv_quantum), quantize(r.z, f.origin[2], f.inv_quantum),
+                      (uint32_t)__double_as_longlong(r.w));
+}
+#endif
+
 struct NetInfo {
     uint64_t seed;
     uint32_t first;
@@ -152,6 +182,7 @@ struct NetInfo {
     float inv_sigma2_32;
     float nu32[3];
     uint32_t root_leaf;  // the network has a single neuron
+    QFrame frame;
 };
 
 struct Ctx;

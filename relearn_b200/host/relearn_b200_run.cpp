@@ -8,7 +8,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <random>
 #include <string>
 #include <vector>
 
@@ -17,6 +16,21 @@
 using namespace relearn_b200;
 
 namespace {
+
+// SplitMix64 (Steele, Lea and Flood, OOPSLA 2014): the driver's generator for
+// positions without --file and for the initial elements, simple enough to be
+// reproduced exactly by other tools (the tests do).
+struct SplitMix64 {
+    uint64_t x;
+    uint64_t next() {
+        x += 0x9E3779B97F4A7C15ull;
+        uint64_t z = x;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+    double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }  // [0, 1)
+};
 
 struct Options {
     uint32_t num_neurons = 2000;
@@ -146,10 +160,10 @@ int main(int argc, char** argv) {
         } else {
             // uniform in a cube at one neuron per 1000 um^3, 20 % inhibitory
             const double side = o.side > 0 ? o.side : std::cbrt(1000.0 * o.num_neurons);
-            std::mt19937_64 gen(o.cfg.seed);
-            std::uniform_real_distribution<double> pos(0.0, side);
+            SplitMix64 gen{ o.cfg.seed };
             for (uint32_t i = 0; i < o.num_neurons; ++i) {
-                neurons.positions.insert(neurons.positions.end(), { pos(gen), pos(gen), pos(gen) });
+                const double x = side * gen.uniform(), y = side * gen.uniform(), z = side * gen.uniform();
+                neurons.positions.insert(neurons.positions.end(), { x, y, z });
                 neurons.signal_types.push_back(i % 5 == 4 ? SignalType::Inhibitory : SignalType::Excitatory);
             }
             neurons.maximum[0] = neurons.maximum[1] = neurons.maximum[2] = side;
@@ -172,12 +186,13 @@ int main(int argc, char** argv) {
 
         Simulation sim(p, neurons.positions, neurons.signal_types, o.algorithm, o.neuron_model);
         if (o.upper > 0.0) {
-            std::mt19937_64 gen(o.cfg.seed + 17);
-            std::uniform_real_distribution<double> u(o.lower, o.upper);
+            // grown elements lower + (upper - lower) * u per type and neuron, in that order
+            RelearnException::check(o.lower <= o.upper, "--synaptic-elements-lower-bound must not exceed the upper bound");
+            SplitMix64 gen{ o.cfg.seed + 17 };
             for (int t = 0; t < 3; ++t) {
                 std::vector<double> grown(o.num_neurons);
                 for (auto& g : grown) {
-                    g = u(gen);
+                    g = o.lower + (o.upper - o.lower) * gen.uniform();
                 }
                 sim.set_initial_elements(static_cast<ElementType>(t), grown);
             }

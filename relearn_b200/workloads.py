@@ -95,3 +95,37 @@ def request_inputs(net: dict) -> tuple:
     n = int(net["num_neurons"])
     s = int(net["seed"]) % (2**31)
     return uniform_cube(n, float(net["side"]), s), signal_types(n, s)
+
+
+def write_positions_file(path: str, positions: np.ndarray, signal: np.ndarray) -> None:
+    """Positions in the reference's positions-file format (read by
+    NeuronIO::read_neuron_positions_and_signals, io/NeuronIO.cpp:229-300): one
+    line "id x y z signal" per neuron, ids from 1, signal "in" or "ex";
+    coordinates with 17 significant digits, so they read back bit for bit."""
+    with open(path, "w") as f:
+        f.write("# id x y z signal_type\n")
+        for i, (p, s) in enumerate(zip(np.asarray(positions, np.float64), np.asarray(signal))):
+            f.write(f"{i + 1} {float(p[0]):.17g} {float(p[1]):.17g} {float(p[2]):.17g} {'in' if s else 'ex'}\n")
+
+
+def read_positions_file(path: str) -> tuple:
+    """Positions and signal types (0 excitatory, 1 inhibitory) from a file in
+    the reference's positions-file format; comment lines start with '#', lines
+    that do not parse are skipped, ids must run 1, 2, ... in order."""
+    pos, sig = [], []
+    with open(path) as f:
+        for line in f:
+            if not line.strip() or line.startswith("#"):
+                continue
+            parts = line.split()
+            try:
+                nid, x, y, z, s = int(parts[0]), float(parts[1]), float(parts[2]), float(parts[3]), parts[4]
+            except (ValueError, IndexError):
+                continue
+            if min(x, y, z) < 0:
+                raise ValueError(f"negative position of neuron {nid}")
+            if nid != len(pos) + 1:
+                raise ValueError(f"loaded neuron {nid - 1} but expected {len(pos)}")
+            pos.append((x, y, z))
+            sig.append(1 if s == "in" else 0)
+    return np.array(pos, np.float64).reshape(-1, 3), np.array(sig, np.uint8)

@@ -1,7 +1,8 @@
 """The C++ driver (relearn_b200/host/relearn_b200_run.cpp, Simulation over the
-C ABI) reproduces the oracle on config[0]'s network: positions written in the
-reference's positions-file format, 20,001 steps, final calcium and synapses
-bit for bit."""
+C ABI) reproduces the oracle on a 2,000-neuron network with config[0]'s
+parameters: positions written in the reference's positions-file format,
+initial elements from the driver's SplitMix64 stream (restated here), 3,001
+steps, final calcium and synapses bit for bit."""
 import os
 import subprocess
 
@@ -14,30 +15,46 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def write_positions(path, pos, sig):
-    with open(path, "w") as f:
-        f.write("# positions of a seeded synthetic network\n")
-        for i, (p, s) in enumerate(zip(pos, sig)):
-            f.write(f"{i + 1} {p[0]!r} {p[1]!r} {p[2]!r} {'in' if s else 'ex'}\n")
+M64 = (1 << 64) - 1
+
+
+def splitmix64_uniform(seed, count):
+    """The driver's SplitMix64 draws as doubles in [0, 1)."""
+    x = seed & M64
+    out = np.empty(count)
+    for k in range(count):
+        x = (x + 0x9E3779B97F4A7C15) & M64
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+        z ^= z >> 31
+        out[k] = float(z >> 11) * 2.0**-53
+    return out
 
 
 def test_driver_matches_oracle(tmp_path):
     from oracle import oracle as O
+    from relearn_b200.workloads import write_positions_file
 
     n, side, seed = 2000, 1000.0, 3
     params, pos, sig = small_network(n, side, seed)
     path = str(tmp_path / "positions.txt")
-    write_positions(path, pos, sig)
+    write_positions_file(path, pos, sig)
     prefix = str(tmp_path / "run")
-    args = [os.path.join(ROOT, "relearn_b200", "bin", "relearn_b200_run"), "--file", path, "-s", "20000", "-r", str(params["seed"]), "--side",
+    args = [os.path.join(ROOT, "relearn_b200", "bin", "relearn_b200_run"), "--file", path, "-s", "3000", "-r", str(params["seed"]), "--side",
             repr(side), "--izhikevich-a", "0.02", "--izhikevich-d", "8", "--synapse-conductance", "3", "--growth-rate-axon", "1e-4",
-            "--growth-rate-dendrite-exc", "1e-4", "--growth-rate-dendrite-inh", "1e-4", "--output-prefix", prefix]
+            "--growth-rate-dendrite-exc", "1e-4", "--growth-rate-dendrite-inh", "1e-4", "--synaptic-elements-lower-bound", "0",
+            "--synaptic-elements-upper-bound", "3", "--output-prefix", prefix]
     r = subprocess.run(args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     ca = np.loadtxt(prefix + "_calcium.txt", dtype=np.float64)
     syn = np.loadtxt(prefix + "_synapses.txt", dtype=np.int64, ndmin=2)
     sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
-    sim.simulate(1, 20001)
+    u = splitmix64_uniform(params["seed"] + 17, 3 * n).reshape(3, n)
+    for t in range(3):
+        g = 0.0 + (3.0 - 0.0) * u[t]
+        sim.set_elements(t, g, np.zeros(n), np.zeros(n, np.uint32), np.floor(g).astype(np.uint32))
+    sim.simulate(1, 3001)
     o = sim.neurons()
     assert np.array_equal(ca.view(np.uint64), o["calcium"].view(np.uint64))
     t, s, w = sim.edges()

@@ -4,6 +4,7 @@ driver's command line, without a GPU."""
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -38,3 +39,18 @@ def test_driver_without_device_fails_cleanly(built_lib):
         pytest.skip("a device is present")
     r = subprocess.run([os.path.join(BIN, "relearn_b200_run"), "--num-neurons", "100", "-s", "10"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 2 and "rl_ctx_create" in r.stderr
+
+
+def test_positions_file_round_trip(tmp_path):
+    from relearn_b200 import workloads
+
+    pos = workloads.uniform_cube(500, 1234.5, 7)
+    sig = workloads.signal_types(500, 7)
+    path = str(tmp_path / "p.txt")
+    workloads.write_positions_file(path, pos, sig)
+    p2, s2 = workloads.read_positions_file(path)
+    assert np.array_equal(p2.view(np.uint64), pos.view(np.uint64)) and np.array_equal(s2, sig)
+    with open(path, "a") as f:
+        f.write("not a neuron line\n502 1 1 1 ex\n")
+    with pytest.raises(ValueError):
+        workloads.read_positions_file(path)
