@@ -135,7 +135,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     net = R.Network(p)
     net.set_stream(stream.cuda_stream)
     net.set_positions(pos, sig)
-    net.autotune(1)  # launch shapes timed during the warm-up
+    apply_shapes(args, net, precision)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     step = 1
     for _ in range(args.warmup):
@@ -189,6 +189,26 @@ class _Null:
 
     def __exit__(self, *exc):
         return False
+
+
+def apply_shapes(args, net, precision):
+    """Launch shapes: timed during the warm-up (default), or set by hand with
+    --act-shape / --search-shape (profiling runs, where timing under the
+    profiler would pick shapes at random)."""
+    if args.act_shape or args.search_shape:
+        b, p, v = (int(x) for x in (args.act_shape or "256,0,1").split(","))
+        w, st, pk = (int(x) for x in (args.search_shape or "4,48,32").split(","))
+        net.set_tuning(search_warps=w, search_stack=st, search_packet=pk, act_block=b, act_persistent=p, act_vec=v if precision else 1)
+    else:
+        net.autotune(1)
+
+
+def bench_config(args, world, precision):
+    """The workload of one bench step, the same for both arms."""
+    return {"workload": f"{args.neurons} Izhikevich neurons {args.placement} in a {args.side:g} um cube, "
+                        f"{'FP64 drop-in' if precision == 0 else 'FP32 form'}; one bench step = {PERIOD} activity steps + 1 plasticity update",
+            "neurons": args.neurons, "placement": args.placement, "period": PERIOD, "l2": "256 MB buffer written between timed steps (GPU arm)",
+            "parallelism": f"replicas{world}"}
 
 
 def run_b200(args, world, rank, local):
@@ -277,10 +297,7 @@ def run_b200(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64" if main_prec == 0 else "f32",
         "data": "synthetic (seeded positions, reference parameters)",
-        "config": {"workload": f"{n} Izhikevich neurons {args.placement} in a {side:g} um cube, "
-                               f"{'FP64 drop-in' if main_prec == 0 else 'FP32 form'}; one bench step = {PERIOD} activity steps + 1 plasticity update",
-                   "neurons": n, "placement": args.placement, "period": PERIOD, "l2": "256 MB buffer written between timed steps",
-                   "parallelism": f"replicas{world}"},
+        "config": bench_config(args, world, main_prec),
         "roofline": m["roofline"],
         "phases_ms": m["phases"],
         "e2e": {"value": e2e_val, "unit": "neuron-steps/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 9 * n,
@@ -587,9 +604,9 @@ def run_reference(args, world, rank):
     p.pop("device", None)
     p["use_libm"] = 0
     sim = O.OracleSim(p, pos, sig, threads=threads)
-    # each step is a bounded sample: 10 activity steps, plus the plasticity
-    # update every 10th sample step (keeping the 100:1 ratio)
-    sample_steps = 10
+    # each step is the bench step itself: 100 activity steps and the
+    # plasticity update at the end of them
+    sample_steps = PERIOD
     step = 1
     for _ in range(args.warmup):
         sim.simulate(step, sample_steps)
@@ -614,10 +631,10 @@ def run_reference(args, world, rank):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded positions, reference parameters)",
-        "config": {"workload": f"{args.neurons} Izhikevich neurons {args.placement} in a {args.side:g} um cube, FP64",
-                   "neurons": args.neurons, "placement": args.placement, "sample_steps_per_step": sample_steps},
+        "config": bench_config(args, world, 1 if args.precision == "fp32" else 0),
         "cpu_baseline": {"value": value, "unit": "neuron-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample_steps} activity steps of {args.neurons} neurons per step (plasticity update every 100 steps)"},
+                         "sample": f"the bench step itself: {sample_steps} activity steps of {args.neurons} neurons and 1 plasticity update, "
+                                   f"{args.steps} timed after {args.warmup} warm-up"},
         "e2e": {"value": value, "unit": "neuron-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -672,6 +689,8 @@ def main():
     ap.add_argument("--ensemble-networks", type=int, default=128)
     ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
     ap.add_argument("--skip-serve", action="store_true", help="do not measure the serving form")
+    ap.add_argument("--act-shape", default=None, help="activity launch shape 'block,persistent,vec' instead of the tuner's")
+    ap.add_argument("--search-shape", default=None, help="search launch shape 'warps,stack,packet' instead of the tuner's")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the Poisson request stream (the full one is 600 s)")
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-steps", type=int, default=5000)

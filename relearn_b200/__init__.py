@@ -422,6 +422,23 @@ class Network:
         w = np.ascontiguousarray(weight, np.int32)
         self._check(self.lib.rl_add_edges(self.h, len(t), _p(t), _p(s), _p(w)))
 
+    def load_network(self, target, source, weight):
+        """Add synapses as the reference loads a network file
+        (Neurons::init_synaptic_elements, neurons/Neurons.cpp:105-127): each
+        adds |weight| connected and grown elements to its source's axons and to
+        its target's excitatory (weight > 0) or inhibitory dendrites."""
+        t = np.ascontiguousarray(target, np.uint32)
+        s = np.ascontiguousarray(source, np.uint32)
+        w = np.ascontiguousarray(weight, np.int32)
+        self.add_edges(t, s, w)
+        a = np.abs(w).astype(np.uint32)
+        adds = [np.bincount(s, weights=a, minlength=self.n), np.bincount(t[w > 0], weights=a[w > 0], minlength=self.n),
+                np.bincount(t[w < 0], weights=a[w < 0], minlength=self.n)]
+        for typ in range(3):
+            el = self.get_elements(typ)
+            add = adds[typ].astype(np.uint32)
+            self.set_elements(typ, el["grown"] + add, el["delta"], el["connected"] + add, el["vacant"])
+
     def edges(self):
         cnt = C.c_uint64()
         self._check(self.lib.rl_get_edges(self.h, None, None, None, 0, C.byref(cnt)))

@@ -60,6 +60,8 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
+// H > 0: h_model and h_calcium are both H, fixed at compile time.
+template <int H>
 __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
     const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
@@ -92,7 +94,9 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
     double xv = A.x[i];
     double uv = A.u[i];
     uint8_t spiked = 0;
-    for (uint32_t it = 0; it < A.h_model; ++it) {
+    const uint32_t hm = H > 0 ? (uint32_t)H : A.h_model;
+#pragma unroll
+    for (uint32_t it = 0; it < hm; ++it) {
         const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
         const double u_inc = (A.ab * xv) - (A.a * uv);
         xv += x_inc * A.scale_m;
@@ -109,9 +113,20 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
     A.fired_cur[i] = spiked;
 
     double ca = A.calcium[i];
-    const double local_beta = A.beta * (double)(spiked ? 1 : 0);
-    for (uint32_t it = 0; it < A.h_calcium; ++it) {
-        ca += A.scale_c * (ca * A.tau_inv + local_beta);
+    const uint32_t hc = H > 0 ? (uint32_t)H : A.h_calcium;
+    if (spiked) {
+        const double local_beta = A.beta * 1.0;
+#pragma unroll
+        for (uint32_t it = 0; it < hc; ++it) {
+            ca += A.scale_c * (ca * A.tau_inv + local_beta);
+        }
+    } else {
+        // local_beta is +0: x + 0 = x for x != 0, and where ca * tau_inv is a
+        // signed zero the sign is lost again when the scaled term is added to ca
+#pragma unroll
+        for (uint32_t it = 0; it < hc; ++it) {
+            ca += A.scale_c * (ca * A.tau_inv);
+        }
     }
     A.calcium[i] = ca;
 
@@ -128,11 +143,11 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
 // persistent shape) each thread strides over the neurons.
-template <int BLOCK>
+template <int BLOCK, int H>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        activity_neuron(A, D, k, i);
+        activity_neuron<H>(A, D, k, i);
     }
 }
 
@@ -203,7 +218,51 @@ __global__ void k_commit(CommitArgs A) {
     }
 }
 
+// Sum of v[i] over enabled neurons (the vacant axons the next search will
+// start from), one atomic per block.
+__global__ void k_sum_enabled(uint32_t n, const uint8_t* __restrict__ enabled, const uint32_t* __restrict__ v, unsigned long long* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t x = (i < n && enabled[i]) ? v[i] : 0u;
+    for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+    }
+    __shared__ uint32_t part[32];
+    if ((threadIdx.x & 31) == 0) {
+        part[threadIdx.x >> 5] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned long long y = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0u;
+        for (int o = 16; o > 0; o >>= 1) {
+            y += __shfl_down_sync(0xFFFFFFFFu, y, o);
+        }
+        if (threadIdx.x == 0 && y) {
+            atomicAdd(out, y);
+        }
+    }
+}
+
 }  // namespace
+
+void launch_vacant_axon_count(Ctx& c, unsigned long long* out) {
+    k_sum_enabled<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(c.n, c.nr.enabled.p, c.nr.vacant[0].p, out);
+    RL_LAUNCH_CHECK();
+}
+
+template <int H>
+void launch_act64(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+    switch (v.block) {
+        case 128:
+            k_activity<128, H><<<act_grid(c, v, (const void*)&k_activity<128, H>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+        case 512:
+            k_activity<512, H><<<act_grid(c, v, (const void*)&k_activity<512, H>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+        default:
+            k_activity<256, H><<<act_grid(c, v, (const void*)&k_activity<256, H>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+    }
+}
 
 void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
     const rl_config& k = c.cfg;
@@ -242,16 +301,10 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
-    switch (v.block) {
-        case 128:
-            k_activity<128><<<act_grid(c, v, (const void*)&k_activity<128>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
-            break;
-        case 512:
-            k_activity<512><<<act_grid(c, v, (const void*)&k_activity<512>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
-            break;
-        default:
-            k_activity<256><<<act_grid(c, v, (const void*)&k_activity<256>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
-            break;
+    if (k.h_model == 10 && k.h_calcium == 10) {
+        launch_act64<10>(c, v, A, kstep);
+    } else {
+        launch_act64<0>(c, v, A, kstep);
     }
     RL_LAUNCH_CHECK();
 }

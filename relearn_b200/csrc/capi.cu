@@ -275,7 +275,7 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     c.act_desc.alloc(1);
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
-    c.commit_cnt.alloc(3);
+    c.commit_cnt.alloc(4);
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
     setup_nets(c, nets, num_nets);
@@ -302,15 +302,19 @@ void plasticity_update(Ctx& c, uint32_t step) {
         // earlier one left deletions, and a single read says where the
         // sequential path has to take over.
         PhaseScope ps(c, PH_COMMIT);
-        RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 3 * sizeof(unsigned long long), c.stream));
+        RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 4 * sizeof(unsigned long long), c.stream));
         for (int t = 0; t < 3; ++t) {
             launch_commit_guarded(c, t);
         }
-        unsigned long long h[3] = { 0, 0, 0 };
+        // the same read says whether the search will have anything to do
+        launch_vacant_axon_count(c, c.commit_cnt.p + 3);
+        unsigned long long h[4] = { 0, 0, 0, 0 };
         RL_CUDA_TRY(cudaMemcpyAsync(h, c.commit_cnt.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
         c.stats.bound_to_delete += h[0] + h[1] + h[2];
         const int first = h[0] ? 0 : (h[1] ? 1 : (h[2] ? 2 : 3));
+        // deletions change vacant axons: then the search counts them itself
+        c.no_searches = first == 3 && h[3] == 0;
         if (first < 3) {
             c.stats.synapses_deleted += run_deletion(c, step, first);
             for (int t = first + 1; t < 3; ++t) {
@@ -329,7 +333,13 @@ void plasticity_update(Ctx& c, uint32_t step) {
     }
     {
         PhaseScope ps(c, PH_SEARCH);
-        run_search(c, step);
+        if (c.no_searches) {
+            c.search.num_searches = 0;  // no enabled neuron has a vacant axon
+            c.search.num_requests = 0;
+        } else {
+            run_search(c, step);
+        }
+        c.no_searches = false;
     }
     {
         PhaseScope ps(c, PH_CONNECTOR);

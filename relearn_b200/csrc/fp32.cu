@@ -60,21 +60,25 @@ struct Act32 {
     float* delta[3];
     float conductance, noise_mean, noise_stddev;
     uint32_t h_model;
-    // one Euler substep with s = 1/h as two increments, each rounded at its own
-    // (small) magnitude before it is added:
-    //   x' = x + [x (s k1 x + s k2) + (s k3 + s I) - s u]
-    //   u' = u + [s a b x - s a u]
-    // (folding the 1 into the factor, x' = x (1 + s k2 + s k1 x) + ..., saves
-    // one operation but rounds at the magnitude of x twice and biased the
-    // firing rate by +2.4e-5 against FP64 in a 200,000-neuron, 1,000-step
-    // check; this form: +2.5e-6)
-    float c, d, v_spike, s, sk1, sk2, sk3, sab, sa;
+    // one Euler substep with s = 1/h, each increment rounded at its own (small)
+    // magnitude before it meets the state:
+    //   x' = x + [x (s k1 x + s k2) + (s k3 + s I) - s u]      (3 FMA + 1 add)
+    //   u' = u + s a (b x - u)                                  (2 FMA)
+    // Folding the 1 into the factor, x' = x (1 + s k2 + s k1 x) + ..., saves an
+    // operation but rounds at the magnitude of x twice per substep, which
+    // shifts the resting point and biased the firing rate by +2.4e-5 against
+    // FP64 in a 200,000-neuron, 1,000-step check; this form: +2.1e-6.
+    float c, d, v_spike, s, sk1, sk2, sk3, sa, b;
     double ca_mul, ca_add;  // calcium: c <- c*ca_mul + fired*ca_add
     float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
     float eta[3];
     const NetInfo* nets;
     const uint16_t* net_of;
+    // a context with one network: its seed and growth rates, so that the
+    // kernel reads no network table
+    uint64_t seed1;
+    float nu1[3];
 };
 
 // Standard normal quantile of u = (k + 0.5) 2^-24 in FP32 as sqrt(2) erfinv(2u - 1),
@@ -115,7 +119,8 @@ __device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
 // deltas are read and updated in place; `input` and `fired` are outputs.
 template <int H>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, bool enabled, uint8_t fired_prev,
-                                           uint16_t net, float& x, float& u, double& ca, float (&delta)[3], float& input, uint8_t& fired) {
+                                           uint64_t seed, uint32_t local, const float* nu, float& x, float& u, double& ca, float (&delta)[3],
+                                           float& input, uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
         fired = fired_prev;
@@ -134,8 +139,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
         }
     }
     // the same Philox draw as the FP64 form, 24 bits of it
-    const NetInfo& N = A.nets[net];
-    const u32x4 w = draw(N.seed, step, i - N.first, 0u, STREAM_NOISE, 0u);
+    const u32x4 w = draw(seed, step, local, 0u, STREAM_NOISE, 0u);
     input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(w.x >> 8), A.noise_mean));
 
     float xv = x;
@@ -147,7 +151,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
 #pragma unroll
     for (uint32_t it = 0; it < h; ++it) {
         const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
-        uv = uv + fmaf(A.sab, xv, -A.sa * uv);
+        uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
         xv = xv + inc;
         if (xv >= A.v_spike) {
             xv = A.c;
@@ -170,7 +174,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
             const float q = (caf - A.xi[t]) * A.inv_zeta[t];
             dz = fmaf(2.0f, __expf(-q * q), -1.0f);
         }
-        delta[t] = fmaf(dz, N.nu32[t], delta[t]);
+        delta[t] = fmaf(dz, nu[t], delta[t]);
     }
 }
 
@@ -262,7 +266,7 @@ __device__ __forceinline__ void ld_h(const uint16_t* p, uint16_t (&v)[V]) {
 // V consecutive neurons from index i (a multiple of V): all loads first, so
 // that each thread keeps its whole footprint in flight, then the updates,
 // then the stores.
-template <int H, int V>
+template <int H, int V, bool MULTI>
 __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i) {
     uint8_t en[V], fp[V], fired[V];
     uint16_t net[V];
@@ -270,7 +274,9 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     double ca[V];
     ld_b<V>(A.enabled + i, en);
     ld_b<V>(A.fired_prev + i, fp);
-    ld_h<V>(A.net_of + i, net);
+    if (MULTI) {
+        ld_h<V>(A.net_of + i, net);
+    }
     ld_f<V>(A.x + i, x);
     ld_f<V>(A.u + i, u);
     ld_d<V>(A.calcium + i, ca);
@@ -280,7 +286,13 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         float d[3] = { d0[k], d1[k], d2[k] };
-        neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], net[k], x[k], u[k], ca[k], d, input[k], fired[k]);
+        if (MULTI) {
+            // draws are keyed on the network's seed and the neuron's index in its network
+            const NetInfo& N = A.nets[net[k]];
+            neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], N.seed, i + k - N.first, N.nu32, x[k], u[k], ca[k], d, input[k], fired[k]);
+        } else {
+            neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], A.seed1, i + k, A.nu1, x[k], u[k], ca[k], d, input[k], fired[k]);
+        }
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     st_f<V>(A.input + i, input);
@@ -296,17 +308,17 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 // H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
 // block, V neurons per thread, striding over the neurons when the grid is one
 // resident wave.  The last n % V neurons go one per thread.
-template <int H, int BLOCK, int V>
+template <int H, int BLOCK, int V, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
     const uint32_t step = D->base_step + k;
     const uint32_t groups = A.n / V;
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t g = tid; g < groups; g += stride) {
-        neurons_f32<H, V>(A, D, step, g * V);
+        neurons_f32<H, V, MULTI>(A, D, step, g * V);
     }
     if (V > 1 && tid < A.n - groups * V) {
-        neurons_f32<H, 1>(A, D, step, groups * V + tid);
+        neurons_f32<H, 1, MULTI>(A, D, step, groups * V + tid);
     }
 }
 
@@ -850,7 +862,12 @@ void f64_from_f32(Ctx& c) {
 
 template <int H, int BLOCK, int V>
 void launch_act32(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
-    k_activity_f32<H, BLOCK, V><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    if (c.multi()) {
+        k_activity_f32<H, BLOCK, V, true><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, true>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    } else {
+        k_activity_f32<H, BLOCK, V, false>
+            <<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, false>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+    }
 }
 
 template <int H, int BLOCK>
@@ -906,8 +923,8 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     A.sk1 = (float)(sm * k.iz_k1);
     A.sk2 = (float)(sm * k.iz_k2);
     A.sk3 = (float)(sm * k.iz_k3);
-    A.sab = (float)(sm * k.iz_a * k.iz_b);
     A.sa = (float)(sm * k.iz_a);
+    A.b = (float)k.iz_b;
     A.c = (float)k.iz_c;
     A.d = (float)k.iz_d;
     A.v_spike = (float)k.iz_v_spike;
@@ -932,6 +949,10 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
+    A.seed1 = c.nets[0].seed;
+    for (int t = 0; t < 3; ++t) {
+        A.nu1[t] = c.nets[0].nu32[t];
+    }
     if (k.h_model == 10) {
         launch_act32_h<10>(c, v, A, kstep);
     } else {

@@ -261,7 +261,8 @@ struct Ctx {
     DBuf<uint32_t> to_delete;  // per neuron, bound elements to delete in the current pass
     DBuf<uint32_t> err;       // device error word
     DBuf<uint64_t> counters;  // device counters
-    DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update
+    DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update, then vacant axons
+    bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
     int64_t device_bytes = 0;  // device memory held now
@@ -324,6 +325,8 @@ uint64_t run_commit(Ctx& c, int type);
 // (its count in commit_cnt) left bound elements to delete; counts into
 // commit_cnt[type].  The three are launched back to back and read once.
 void launch_commit_guarded(Ctx& c, int type);
+// Adds the vacant axons of the enabled neurons to *out.
+void launch_vacant_axon_count(Ctx& c, unsigned long long* out);
 void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n);  // commit one element type; to_delete[] per neuron, returns the sum
 
 void check_device_error(Ctx& c, const char* phase);

@@ -217,10 +217,20 @@ RL_HD double rl_hypot3(double x, double y, double z) {
     if (a == 0.0) {
         return 0.0;
     }
-    const double xs = x / a;
-    const double ys = y / a;
-    const double zs = z / a;
-    return a * sqrt(xs * xs + ys * ys + zs * zs);
+    // The largest component divided by a is exactly 1, so only the other two
+    // are divided (an FP64 division is a long sequence on the GPU); the terms
+    // are still added in x, y, z order, so the result is the same bits.
+    const bool zmax = a == z;
+    const bool ymax = !zmax && a == y;
+    const double p = zmax || ymax ? x : y;  // first component that is not the maximum
+    const double q = zmax ? y : z;          // second one
+    const double ps = p / a;
+    const double qs = q / a;
+    const double p2 = ps * ps, q2 = qs * qs;
+    const double t0 = zmax || ymax ? p2 : 1.0;
+    const double t1 = zmax ? q2 : (ymax ? 1.0 : p2);
+    const double t2 = zmax ? 1.0 : q2;
+    return a * sqrt(t0 + t1 + t2);
 }
 
 // std::nextafter(total, total + 1e-5) for finite total > 0

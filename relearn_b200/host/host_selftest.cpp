@@ -62,6 +62,26 @@ int main(int argc, char** argv) {
     EXPECT(throws([&] { read_neuron_positions_and_signals(neg); }) == RL_ERR_INVALID);
     EXPECT(throws([&] { read_neuron_positions_and_signals(dir + "/does_not_exist.txt"); }) == RL_ERR_INVALID);
 
+    // network files: write, read back, refuse what one GPU does not run
+    {
+        NetworkSynapses s{ { 2, 0, 1, 2 }, { 1, 2, 2, 0 }, { 1, -1, 2, 1 } };
+        write_network_files(dir, 3, s);
+        const NetworkSynapses r = read_in_network(dir + "/rank_0_in_network.txt", 3);
+        EXPECT(r.target.size() == 4);
+        // sorted by (target, source)
+        EXPECT(r.target[0] == 0 && r.source[0] == 2 && r.weight[0] == -1);
+        EXPECT(r.target[1] == 1 && r.source[1] == 2 && r.weight[1] == 2);
+        EXPECT(r.target[3] == 2 && r.source[3] == 1 && r.weight[3] == 1);
+        const NetworkSynapses o = read_in_network(dir + "/rank_0_out_network.txt", 3);
+        EXPECT(o.target.size() == 4 && o.source[0] == 0 && o.target[0] == 2);
+        std::ofstream(dir + "/static.txt") << "0 1 0 2 1 0\n";
+        EXPECT(throws([&] { read_in_network(dir + "/static.txt", 3); }) == RL_ERR_UNSUPPORTED);
+        std::ofstream(dir + "/rank1.txt") << "1 1 0 2 1 1\n";
+        EXPECT(throws([&] { read_in_network(dir + "/rank1.txt", 3); }) == RL_ERR_INVALID);
+        std::ofstream(dir + "/range.txt") << "0 4 0 2 1 1\n";
+        EXPECT(throws([&] { read_in_network(dir + "/range.txt", 3); }) == RL_ERR_INVALID);
+    }
+
     // plugin names the reference offers but this path does not build
     Parameters p = Parameters::defaults(3, 100.0);
     EXPECT(p.cfg.plasticity_interval == 100 && p.cfg.theta == 0.3 && p.cfg.sigma == 750.0);

@@ -398,3 +398,99 @@ inline LoadedNeurons read_neuron_positions_and_signals(const std::string& path) 
 }
 
 }  // namespace relearn_b200
+
+#include <algorithm>
+#include <numeric>
+#include <tuple>
+
+namespace relearn_b200 {
+
+// Plastic synapses of one rank in the reference's network files
+// (NeuronIO::read_in_synapses / write_in_synapses, io/NeuronIO.cpp:793-860 and
+// 935-1030): '#' comment lines, then "target_rank target_id source_rank
+// source_id weight plastic" with ids from 1.  This path runs one rank and
+// plastic synapses only: other ranks and static synapses are refused.
+struct NetworkSynapses {
+    std::vector<uint32_t> target, source;
+    std::vector<int32_t> weight;
+};
+
+inline NetworkSynapses read_in_network(const std::string& path, number_neurons_type number_neurons) {
+    std::ifstream file(path);
+    RelearnException::check(file.good(), "read_in_network: cannot open '" + path + "'");
+    NetworkSynapses out;
+    std::string line;
+    while (std::getline(file, line)) {
+        if (line.empty() || line[0] == '#') {
+            continue;
+        }
+        std::istringstream ss(line);
+        int64_t target_rank = 0, source_rank = 0, weight = 0;
+        uint64_t target_id = 0, source_id = 0;
+        int plastic = 0;
+        if (!(ss >> target_rank >> target_id >> source_rank >> source_id >> weight >> plastic)) {
+            continue;  // the reference skips lines it cannot parse
+        }
+        RelearnException::check(target_rank == 0 && source_rank == 0, "read_in_network: synapses of other ranks are not supported on one GPU");
+        RelearnException::check(target_id >= 1 && target_id <= number_neurons && source_id >= 1 && source_id <= number_neurons,
+                                "read_in_network: neuron id out of range in '" + line + "'");
+        RelearnException::check(weight != 0, "read_in_network: weight was 0");
+        if (!plastic) {
+            throw RelearnException("read_in_network: static synapses are not supported by this path", RL_ERR_UNSUPPORTED);
+        }
+        out.target.push_back((uint32_t)(target_id - 1));
+        out.source.push_back((uint32_t)(source_id - 1));
+        out.weight.push_back((int32_t)weight);
+    }
+    return out;
+}
+
+// rank_0_in_network.txt (sorted by target, then source) and
+// rank_0_out_network.txt (sorted by source, then target) in `directory`.
+inline void write_network_files(const std::string& directory, number_neurons_type number_neurons, const NetworkSynapses& s) {
+    std::vector<size_t> order(s.target.size());
+    std::iota(order.begin(), order.end(), size_t{ 0 });
+    for (int side = 0; side < 2; ++side) {
+        const bool in = side == 0;
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            return in ? std::tie(s.target[a], s.source[a]) < std::tie(s.target[b], s.source[b])
+                      : std::tie(s.source[a], s.target[a]) < std::tie(s.source[b], s.target[b]);
+        });
+        const std::string path = directory + (in ? "/rank_0_in_network.txt" : "/rank_0_out_network.txt");
+        std::ofstream f(path);
+        RelearnException::check(f.good(), "write_network_files: cannot write '" + path + "'");
+        f << "# " << number_neurons << "\n# <target rank> <target neuron id>\t<source rank> <source neuron id>\t<weight>\t<plastic>\n";
+        for (size_t k : order) {
+            f << "0 " << s.target[k] + 1 << "\t0 " << s.source[k] + 1 << "\t" << s.weight[k] << "\t1\n";
+        }
+    }
+}
+
+// Loads synapses into a simulation as Neurons::init_synaptic_elements does
+// (neurons/Neurons.cpp:105-127): every synapse adds |weight| connected and
+// grown elements to its source's axons and to its target's excitatory or
+// inhibitory dendrites (by the weight's sign).
+inline void load_network(Simulation& sim, const NetworkSynapses& s) {
+    Context& ctx = sim.context();
+    const size_t n = ctx.size();
+    const size_t m = s.target.size();
+    ctx.check(rl_add_edges(ctx.handle(), m, s.target.data(), s.source.data(), s.weight.data()), "rl_add_edges");
+    std::vector<uint32_t> add[3] = { std::vector<uint32_t>(n, 0u), std::vector<uint32_t>(n, 0u), std::vector<uint32_t>(n, 0u) };
+    for (size_t k = 0; k < m; ++k) {
+        const uint32_t a = (uint32_t)(s.weight[k] < 0 ? -s.weight[k] : s.weight[k]);
+        add[RL_AXON][s.source[k]] += a;
+        add[s.weight[k] < 0 ? RL_DENDRITE_INH : RL_DENDRITE_EXC][s.target[k]] += a;
+    }
+    for (int t = 0; t < 3; ++t) {
+        std::vector<double> grown(n), delta(n);
+        std::vector<uint32_t> connected(n), vacant(n);
+        ctx.check(rl_get_elements(ctx.handle(), t, grown.data(), delta.data(), connected.data(), vacant.data()), "rl_get_elements");
+        for (size_t i = 0; i < n; ++i) {
+            connected[i] += add[t][i];
+            grown[i] += (double)add[t][i];
+        }
+        ctx.check(rl_set_elements(ctx.handle(), t, grown.data(), delta.data(), connected.data(), vacant.data()), "rl_set_elements");
+    }
+}
+
+}  // namespace relearn_b200

@@ -42,6 +42,8 @@ struct Options {
     double lower = 0.0, upper = 0.0;
     std::string precision = "fp64";
     std::string output_prefix;
+    std::string graph;           // directory with rank_0_in_network.txt
+    std::string output_network;  // directory for the final network files
     rl_config cfg{};
 };
 
@@ -54,8 +56,10 @@ void usage() {
         "    --growth-rate-axon, --growth-rate-dendrite-exc, --growth-rate-dendrite-inh, --min-calcium-axons,\n"
         "    --min-calcium-excitatory-dendrites, --min-calcium-inhibitory-dendrites, --retract-ratio,\n"
         "    --synaptic-elements-lower-bound, --synaptic-elements-upper-bound\n"
+        "    -g/--graph DIR (rank_0_in_network.txt with plastic synapses)\n"
         "  added here: --izhikevich-a/-b/-c/-d, --side UM (cube edge; default: the largest coordinate),\n"
-        "    --precision fp64|fp32, --output-prefix P (final calcium and synapses as text)\n");
+        "    --precision fp64|fp32, --output-prefix P (final calcium and synapses as text),\n"
+        "    --output-network DIR (final rank_0_in_network.txt and rank_0_out_network.txt)\n");
 }
 
 bool parse(int argc, char** argv, Options& o) {
@@ -138,6 +142,10 @@ bool parse(int argc, char** argv, Options& o) {
             o.precision = next();
         } else if (a == "--output-prefix") {
             o.output_prefix = next();
+        } else if (a == "--graph" || a == "-g") {
+            o.graph = next();
+        } else if (a == "--output-network") {
+            o.output_network = next();
         } else {
             throw RelearnException("unknown option " + a);
         }
@@ -197,6 +205,9 @@ int main(int argc, char** argv) {
                 sim.set_initial_elements(static_cast<ElementType>(t), grown);
             }
         }
+        if (!o.graph.empty()) {
+            load_network(sim, read_in_network(o.graph + "/rank_0_in_network.txt", o.num_neurons));
+        }
         const auto t0 = std::chrono::steady_clock::now();
         sim.simulate(o.steps);
         const auto calcium = sim.neuron_model().get_calcium();
@@ -214,6 +225,9 @@ int main(int argc, char** argv) {
             o.num_neurons, o.steps + 1, secs, (double)o.num_neurons * (o.steps + 1) / secs, mean_ca, syn.target.size(),
             (unsigned long long)st.synapses_created, (unsigned long long)st.synapses_deleted, (unsigned long long)st.searches,
             (unsigned long long)st.plasticity_updates);
+        if (!o.output_network.empty()) {
+            write_network_files(o.output_network, o.num_neurons, NetworkSynapses{ syn.target, syn.source, syn.weight });
+        }
         if (!o.output_prefix.empty()) {
             FILE* f = std::fopen((o.output_prefix + "_calcium.txt").c_str(), "w");
             RelearnException::check(f != nullptr, "cannot write " + o.output_prefix + "_calcium.txt");

@@ -129,3 +129,47 @@ def read_positions_file(path: str) -> tuple:
             pos.append((x, y, z))
             sig.append(1 if s == "in" else 0)
     return np.array(pos, np.float64).reshape(-1, 3), np.array(sig, np.uint8)
+
+
+NETWORK_HEADER = "# <target rank> <target neuron id>\t<source rank> <source neuron id>\t<weight>\t<plastic>\n"
+
+
+def write_network_files(directory: str, num_neurons: int, target, source, weight) -> None:
+    """rank_0_in_network.txt (sorted by target, source) and
+    rank_0_out_network.txt (sorted by source, target) in the reference's
+    network-file format (NeuronIO::write_in_synapses / write_out_synapses,
+    io/NeuronIO.cpp:935-1030): "target_rank target_id source_rank source_id
+    weight plastic", ids from 1, all synapses plastic on rank 0."""
+    t, s, w = (np.asarray(a) for a in (target, source, weight))
+    for name, order in (("rank_0_in_network.txt", np.lexsort((s, t))), ("rank_0_out_network.txt", np.lexsort((t, s)))):
+        with open(f"{directory}/{name}", "w") as f:
+            f.write(f"# {num_neurons}\n" + NETWORK_HEADER)
+            for k in order:
+                f.write(f"0 {int(t[k]) + 1}\t0 {int(s[k]) + 1}\t{int(w[k])}\t1\n")
+
+
+def read_in_network_file(path: str, num_neurons: int) -> tuple:
+    """(target, source, weight) of the plastic synapses in a network file of
+    the reference's format; one rank, plastic synapses only."""
+    t, s, w = [], [], []
+    with open(path) as f:
+        for line in f:
+            if not line.strip() or line.startswith("#"):
+                continue
+            parts = line.split()
+            try:
+                tr, ti, sr, si, wt, pl = (int(x) for x in parts[:6])
+            except (ValueError, IndexError):
+                continue
+            if tr != 0 or sr != 0:
+                raise ValueError("synapses of other ranks are not supported on one GPU")
+            if not (1 <= ti <= num_neurons and 1 <= si <= num_neurons):
+                raise ValueError(f"neuron id out of range: {line.strip()}")
+            if wt == 0:
+                raise ValueError("weight was 0")
+            if not pl:
+                raise ValueError("static synapses are not supported by this path")
+            t.append(ti - 1)
+            s.append(si - 1)
+            w.append(wt)
+    return np.array(t, np.uint32), np.array(s, np.uint32), np.array(w, np.int32)

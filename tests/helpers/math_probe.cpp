@@ -1,11 +1,14 @@
 // Host build of the product's shared arithmetic header, for the agreement
 // test against the oracle (compiled with g++ -ffp-contract=off).
+#include <cmath>
 #include "../../relearn_b200/csrc/rl_math.cuh"
 
 extern "C" {
 double probe_exp(double x) { return rl::rl_exp(x); }
 double probe_log(double x) { return rl::rl_log(x); }
 double probe_hypot3(double x, double y, double z) { return rl::rl_hypot3(x, y, z); }
+// libstdc++'s own three-argument std::hypot, which the reference calls
+double probe_std_hypot3(double x, double y, double z) { return std::hypot(x, y, z); }
 double probe_quantile(double p) { return rl::normal_quantile(p); }
 double probe_normal(unsigned long long seed, unsigned step, unsigned neuron, double mean, double sd) {
     return rl::background_normal(seed, step, neuron, mean, sd);

@@ -107,8 +107,9 @@ def probe(tmp_path_factory):
     for name in ("probe_exp", "probe_log", "probe_quantile", "probe_next_up"):
         getattr(L, name).restype = C.c_double
         getattr(L, name).argtypes = [C.c_double]
-    L.probe_hypot3.restype = C.c_double
-    L.probe_hypot3.argtypes = [C.c_double] * 3
+    for name in ("probe_hypot3", "probe_std_hypot3"):
+        getattr(L, name).restype = C.c_double
+        getattr(L, name).argtypes = [C.c_double] * 3
     L.probe_normal.restype = C.c_double
     L.probe_normal.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double]
     L.probe_philox.argtypes = [C.c_uint32] * 6 + [C.c_void_p]
@@ -124,8 +125,12 @@ def test_shared_math_bitwise_agreement(probe, oracle_mod):
         assert probe.probe_log(float(y)) == O.orc_log(float(y))
     for p in rng.uniform(0, 1, 20000):
         assert probe.probe_quantile(float(p)) == O.orc_quantile(float(p))
-    for v in rng.uniform(-1e4, 1e4, (5000, 3)):
-        assert probe.probe_hypot3(*map(float, v)) == O.orc_hypot3(*map(float, v))
+    vs = rng.uniform(-1e4, 1e4, (5000, 3))
+    ties = rng.choice([-3.5, 0.0, 2.0, 7.25, 1e-300], (600, 3))  # equal magnitudes, zeros, tiny values
+    for v in np.concatenate([vs, ties]):
+        h = probe.probe_hypot3(*map(float, v))
+        # the restatement, the oracle's and libstdc++'s std::hypot(x, y, z) agree bit for bit
+        assert h == O.orc_hypot3(*map(float, v)) == probe.probe_std_hypot3(*map(float, v)), v
     for s in range(1, 4):
         for i in range(2000):
             assert probe.probe_normal(42, s, i, 5.0, 2.0) == O.orc_normal(42, s, i, 5.0, 2.0)

@@ -54,3 +54,23 @@ def test_positions_file_round_trip(tmp_path):
         f.write("not a neuron line\n502 1 1 1 ex\n")
     with pytest.raises(ValueError):
         workloads.read_positions_file(path)
+
+
+def test_network_file_round_trip(tmp_path):
+    from relearn_b200 import workloads
+
+    rng = np.random.default_rng(4)
+    t = rng.integers(0, 50, 200).astype(np.uint32)
+    s = rng.integers(0, 50, 200).astype(np.uint32)
+    w = rng.choice([-2, -1, 1, 3], 200).astype(np.int32)
+    workloads.write_network_files(str(tmp_path), 50, t, s, w)
+    t2, s2, w2 = workloads.read_in_network_file(str(tmp_path / "rank_0_in_network.txt"), 50)
+    order = np.lexsort((s, t))
+    assert np.array_equal(t2, t[order]) and np.array_equal(s2, s[order]) and np.array_equal(w2, w[order])
+    t3, s3, _ = workloads.read_in_network_file(str(tmp_path / "rank_0_out_network.txt"), 50)
+    assert np.all(np.diff(s3.astype(np.int64)) >= 0)
+    bad = tmp_path / "bad.txt"
+    for line in ("0 1 0 2 1 0\n", "1 1 0 2 1 1\n", "0 51 0 2 1 1\n", "0 1 0 2 0 1\n"):
+        bad.write_text(line)
+        with pytest.raises(ValueError):
+            workloads.read_in_network_file(str(bad), 50)
