@@ -650,6 +650,8 @@ def run_case(args):
     params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
     params["precision"] = 1 if args.precision == "fp32" else 0
     net = R.Network(params)
+    if args.act_shape or args.search_shape:
+        apply_shapes(args, net, params["precision"])
     if args.case == "activity":
         net.activity_block(1, 4)
     elif args.case == "plasticity":

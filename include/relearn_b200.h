@@ -221,6 +221,13 @@ RL_API rl_status rl_get_elements(void* ctx, int type, double* grown, double* del
 RL_API rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const double* calcium, const uint8_t* fired);
 RL_API rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input);
 
+/* Target calcium per neuron (the target function CalciumIO builds from a
+ * --file-calcium, io/CalciumIO.cpp:27-130; otherwise every neuron has
+ * rl_config.target_calcium).  The FP32 form runs one target for all neurons of
+ * a context: there, targets that are not all equal give RL_ERR_UNSUPPORTED. */
+RL_API rl_status rl_set_target_calcium(void* ctx, const double* target);
+RL_API rl_status rl_get_target_calcium(void* ctx, double* target);
+
 /* Enable flags (NeuronsExtraInfo disable flags): 1 enabled, 0 disabled. */
 RL_API rl_status rl_set_enabled(void* ctx, const uint8_t* enabled);
 

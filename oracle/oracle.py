@@ -98,6 +98,7 @@ def lib():
         L.orc_plasticity_step.argtypes = [vp, u32]
         L.orc_get_neurons.argtypes = [vp] * 6
         L.orc_set_neurons.argtypes = [vp] * 5
+        L.orc_set_targets.argtypes = [vp, vp]
         L.orc_num_edges.restype = u64
         L.orc_num_edges.argtypes = [vp]
         L.orc_get_edges.argtypes = [vp, vp, vp, vp]
@@ -222,6 +223,10 @@ class OracleSim:
         for v, dt in ((x, np.float64), (u, np.float64), (calcium, np.float64), (fired, np.uint8)):
             arrs.append(None if v is None else np.ascontiguousarray(v, dt))
         lib().orc_set_neurons(self.h, *[None if a is None else _p(a) for a in arrs])
+
+    def set_targets(self, target):
+        t = np.ascontiguousarray(target, np.float64)
+        lib().orc_set_targets(self.h, _p(t))
 
     def edges(self):
         m = int(lib().orc_num_edges(self.h))

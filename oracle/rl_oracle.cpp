@@ -1071,6 +1071,12 @@ void orc_set_neurons(void* h, const double* x, const double* u, const double* ca
     if (fired) std::copy(fired, fired + s->n, s->fired.begin());
 }
 
+// Per-neuron target calcium (CalciumIO's target function, io/CalciumIO.cpp:27-130).
+void orc_set_targets(void* h, const double* target) {
+    Sim* s = static_cast<Sim*>(h);
+    std::copy(target, target + s->n, s->target.begin());
+}
+
 // Number of distinct (target, source) pairs with non-zero weight.
 uint64_t orc_num_edges(void* h) {
     const Sim* s = static_cast<Sim*>(h);

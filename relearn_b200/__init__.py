@@ -139,6 +139,7 @@ ABI_FUNCTIONS = [
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
     "rl_candidate_weights", "rl_set_graphs", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
     "rl_serve_fetch", "rl_serve_load", "rl_serve_destroy", "rl_autotune", "rl_get_tuning", "rl_set_tuning",
+    "rl_set_target_calcium", "rl_get_target_calcium",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -218,6 +219,10 @@ def load_library(path: str = LIB_PATH):
     L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
     L.rl_prepare_update_connectivity_noalloc.argtypes = [vp, vp, vp, vp, vp]
+    L.rl_set_target_calcium.restype = st
+    L.rl_set_target_calcium.argtypes = [vp, vp]
+    L.rl_get_target_calcium.restype = st
+    L.rl_get_target_calcium.argtypes = [vp, vp]
     L.rl_autotune.restype = st
     L.rl_autotune.argtypes = [vp, C.c_int]
     L.rl_get_tuning.restype = st
@@ -421,6 +426,16 @@ class Network:
         t = np.ascontiguousarray(target, np.uint32); s = np.ascontiguousarray(source, np.uint32)
         w = np.ascontiguousarray(weight, np.int32)
         self._check(self.lib.rl_add_edges(self.h, len(t), _p(t), _p(s), _p(w)))
+
+    def set_target_calcium(self, target):
+        """Target calcium per neuron (the reference's --file-calcium targets)."""
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(target, np.float64), (self.n,)))
+        self._check(self.lib.rl_set_target_calcium(self.h, _p(t)))
+
+    def target_calcium(self) -> np.ndarray:
+        t = np.zeros(self.n)
+        self._check(self.lib.rl_get_target_calcium(self.h, _p(t)))
+        return t
 
     def load_network(self, target, source, weight):
         """Add synapses as the reference loads a network file

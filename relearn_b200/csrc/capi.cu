@@ -760,6 +760,30 @@ rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const doub
     });
 }
 
+rl_status rl_set_target_calcium(void* ctx, const double* target) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(target != nullptr, RL_ERR_INVALID, "null target");
+        if (rl::is_fp32(c)) {
+            // the FP32 kernel folds one target into its growth-curve constants
+            for (uint32_t i = 1; i < c.n; ++i) {
+                RL_CHECK(target[i] == target[0], RL_ERR_UNSUPPORTED, "the FP32 form runs one target calcium for all neurons");
+            }
+            c.cfg.target_calcium = target[0];
+        }
+        rl::drop_activity_graphs(c);  // captured intervals hold the growth-curve constants
+        rl::upload(c.nr.target, target, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+rl_status rl_get_target_calcium(void* ctx, double* target) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(target != nullptr, RL_ERR_INVALID, "null target");
+        rl::download(target, c.nr.target, c.n, c.stream);
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
 rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input) {
     return rl::guarded(ctx, [&](Ctx& c) {
         if (rl::is_fp32(c)) {

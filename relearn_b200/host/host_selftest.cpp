@@ -82,6 +82,21 @@ int main(int argc, char** argv) {
         EXPECT(throws([&] { read_in_network(dir + "/range.txt", 3); }) == RL_ERR_INVALID);
     }
 
+    // calcium files
+    {
+        std::ofstream(dir + "/calcium.txt") << "# comment\ndefault 0.1 0.7\n0:2;-1:4 0.3 0.9\n0:1 0.0 0.5\n";
+        const CalciumValues v = read_calcium_file(dir + "/calcium.txt", 5);
+        EXPECT(v.initial[0] == 0.0 && v.target[0] == 0.5);
+        EXPECT(v.initial[1] == 0.3 && v.target[1] == 0.9 && v.initial[3] == 0.3 && v.target[3] == 0.9);
+        EXPECT(v.initial[2] == 0.1 && v.target[2] == 0.7 && v.initial[4] == 0.1);
+        std::ofstream(dir + "/calcium_twice.txt") << "default 0 0.7\n0:1 0 1\n0:1 0 1\n";
+        EXPECT(throws([&] { read_calcium_file(dir + "/calcium_twice.txt", 5); }) == RL_ERR_INVALID);
+        std::ofstream(dir + "/calcium_nodefault.txt") << "0:1 0 1\n";
+        EXPECT(throws([&] { read_calcium_file(dir + "/calcium_nodefault.txt", 5); }) == RL_ERR_INVALID);
+        std::ofstream(dir + "/calcium_group.txt") << "default 0 0.7\nexcitatory 0 1\n";
+        EXPECT(throws([&] { read_calcium_file(dir + "/calcium_group.txt", 5); }) == RL_ERR_INVALID);
+    }
+
     // plugin names the reference offers but this path does not build
     Parameters p = Parameters::defaults(3, 100.0);
     EXPECT(p.cfg.plasticity_interval == 100 && p.cfg.theta == 0.3 && p.cfg.sigma == 750.0);

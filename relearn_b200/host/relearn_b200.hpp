@@ -494,3 +494,75 @@ inline void load_network(Simulation& sim, const NetworkSynapses& s) {
 }
 
 }  // namespace relearn_b200
+
+namespace relearn_b200 {
+
+// Initial and target calcium per neuron from a calcium file of the reference
+// (CalciumIO::load_initial_and_target_function, io/CalciumIO.cpp:27-130):
+// lines "<description> <initial> <target>", the description "default" (at most
+// once) or ';'-separated "<rank>:<neuron id>" with 1-based ids (rank -1 = this
+// rank; one rank here).  A neuron gets at most one pair; the others take the
+// default.  Neuron groups are not supported.
+struct CalciumValues {
+    std::vector<double> initial, target;
+};
+
+inline CalciumValues read_calcium_file(const std::string& path, number_neurons_type number_neurons) {
+    std::ifstream file(path);
+    RelearnException::check(file.good(), "read_calcium_file: cannot open '" + path + "'");
+    CalciumValues v{ std::vector<double>(number_neurons, 0.0), std::vector<double>(number_neurons, 0.0) };
+    std::vector<uint8_t> seen(number_neurons, 0);
+    bool has_default = false;
+    double def_initial = 0.0, def_target = 0.0;
+    std::string line;
+    while (std::getline(file, line)) {
+        if (!line.empty() && line[0] == '#') {
+            continue;
+        }
+        std::istringstream ss(line);
+        std::string description;
+        double initial = 0.0, target = 0.0;
+        if (!(ss >> description >> initial >> target)) {
+            continue;
+        }
+        if (description == "default") {
+            RelearnException::check(!has_default, "read_calcium_file: more than one default");
+            has_default = true;
+            def_initial = initial;
+            def_target = target;
+            continue;
+        }
+        std::istringstream items(description);
+        std::string item;
+        while (std::getline(items, item, ';')) {
+            const auto colon = item.find(':');
+            RelearnException::check(colon != std::string::npos, "read_calcium_file: neuron groups are not supported: " + item);
+            const long rank = std::stol(item.substr(0, colon));
+            const long long id = std::stoll(item.substr(colon + 1));
+            RelearnException::check(rank == 0 || rank == -1, "read_calcium_file: one rank only: " + item);
+            RelearnException::check(id >= 1 && (uint64_t)id <= number_neurons, "read_calcium_file: neuron id out of range (ids are 1-based): " + item);
+            RelearnException::check(!seen[id - 1], "read_calcium_file: neuron " + std::to_string(id) + " assigned twice");
+            seen[id - 1] = 1;
+            v.initial[id - 1] = initial;
+            v.target[id - 1] = target;
+        }
+    }
+    for (size_t i = 0; i < number_neurons; ++i) {
+        if (!seen[i]) {
+            RelearnException::check(has_default, "read_calcium_file: neurons without values and no default");
+            v.initial[i] = def_initial;
+            v.target[i] = def_target;
+        }
+    }
+    return v;
+}
+
+// Applies a calcium file's values: the calcium state starts at `initial`, the
+// growth curves use `target`.
+inline void set_calcium(Simulation& sim, const CalciumValues& v) {
+    Context& ctx = sim.context();
+    ctx.check(rl_set_neurons(ctx.handle(), nullptr, nullptr, v.initial.data(), nullptr), "rl_set_neurons");
+    ctx.check(rl_set_target_calcium(ctx.handle(), v.target.data()), "rl_set_target_calcium");
+}
+
+}  // namespace relearn_b200

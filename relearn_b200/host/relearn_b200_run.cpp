@@ -43,6 +43,7 @@ struct Options {
     std::string precision = "fp64";
     std::string output_prefix;
     std::string graph;           // directory with rank_0_in_network.txt
+    std::string file_calcium;    // initial and target calcium per neuron
     std::string output_network;  // directory for the final network files
     rl_config cfg{};
 };
@@ -56,7 +57,7 @@ void usage() {
         "    --growth-rate-axon, --growth-rate-dendrite-exc, --growth-rate-dendrite-inh, --min-calcium-axons,\n"
         "    --min-calcium-excitatory-dendrites, --min-calcium-inhibitory-dendrites, --retract-ratio,\n"
         "    --synaptic-elements-lower-bound, --synaptic-elements-upper-bound\n"
-        "    -g/--graph DIR (rank_0_in_network.txt with plastic synapses)\n"
+        "    -g/--graph DIR (rank_0_in_network.txt with plastic synapses), --file-calcium FILE\n"
         "  added here: --izhikevich-a/-b/-c/-d, --side UM (cube edge; default: the largest coordinate),\n"
         "    --precision fp64|fp32, --output-prefix P (final calcium and synapses as text),\n"
         "    --output-network DIR (final rank_0_in_network.txt and rank_0_out_network.txt)\n");
@@ -144,6 +145,8 @@ bool parse(int argc, char** argv, Options& o) {
             o.output_prefix = next();
         } else if (a == "--graph" || a == "-g") {
             o.graph = next();
+        } else if (a == "--file-calcium") {
+            o.file_calcium = next();
         } else if (a == "--output-network") {
             o.output_network = next();
         } else {
@@ -207,6 +210,9 @@ int main(int argc, char** argv) {
         }
         if (!o.graph.empty()) {
             load_network(sim, read_in_network(o.graph + "/rank_0_in_network.txt", o.num_neurons));
+        }
+        if (!o.file_calcium.empty()) {
+            set_calcium(sim, read_calcium_file(o.file_calcium, o.num_neurons));
         }
         const auto t0 = std::chrono::steady_clock::now();
         sim.simulate(o.steps);

@@ -173,3 +173,50 @@ def read_in_network_file(path: str, num_neurons: int) -> tuple:
             s.append(si - 1)
             w.append(wt)
     return np.array(t, np.uint32), np.array(s, np.uint32), np.array(w, np.int32)
+
+
+def read_calcium_file(path: str, num_neurons: int) -> tuple:
+    """Initial and target calcium per neuron from a calcium file of the
+    reference (CalciumIO::load_initial_and_target_function,
+    io/CalciumIO.cpp:27-130): lines "<description> <initial> <target>", where
+    the description is "default" (at most once) or ';'-separated
+    "<rank>:<neuron id>" with 1-based ids (rank -1 meaning this rank; one rank
+    here).  Every neuron gets at most one pair; neurons without one take the
+    default.  Neuron groups are not supported."""
+    initial = np.full(num_neurons, np.nan)
+    target = np.full(num_neurons, np.nan)
+    default = None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#"):
+                continue
+            parts = line.split()
+            if len(parts) < 3:
+                continue
+            try:
+                ini, tgt = float(parts[1]), float(parts[2])
+            except ValueError:
+                continue
+            if parts[0] == "default":
+                if default is not None:
+                    raise ValueError("more than one default")
+                default = (ini, tgt)
+                continue
+            for item in parts[0].split(";"):
+                if ":" not in item:
+                    raise ValueError(f"neuron groups are not supported: {item!r}")
+                rank, nid = item.split(":", 1)
+                rank, nid = int(rank), int(nid)
+                if rank not in (0, -1):
+                    raise ValueError(f"rank {rank}: one rank only")
+                if nid < 1 or nid > num_neurons:
+                    raise ValueError(f"neuron id {nid} out of range (ids are 1-based)")
+                if not np.isnan(initial[nid - 1]):
+                    raise ValueError(f"neuron {nid} assigned twice")
+                initial[nid - 1], target[nid - 1] = ini, tgt
+    missing = np.isnan(initial)
+    if missing.any():
+        if default is None:
+            raise ValueError("neurons without values and no default")
+        initial[missing], target[missing] = default
+    return initial, target

@@ -63,10 +63,11 @@ def test_driver_matches_oracle(tmp_path):
 
 
 def test_driver_loads_network(tmp_path):
-    """-g DIR: the driver loads plastic synapses from the reference's network
-    file format (connected and grown elements follow them, as
-    Neurons::init_synaptic_elements does) and the run matches the oracle
-    started from the same network."""
+    """-g DIR and --file-calcium: the driver loads plastic synapses from the
+    reference's network file format (connected and grown elements follow them,
+    as Neurons::init_synaptic_elements does) and initial / target calcium from
+    a calcium file, and the run matches the oracle started from the same
+    state."""
     from oracle import oracle as O
     from relearn_b200.workloads import write_network_files, write_positions_file
 
@@ -79,16 +80,23 @@ def test_driver_loads_network(tmp_path):
     t, s = pairs[:, 0].astype(np.uint32), pairs[:, 1].astype(np.uint32)
     w = np.where(sig[s] == 1, -1, 1).astype(np.int32)
     write_network_files(str(tmp_path), n, t, s, w)
+    (tmp_path / "calcium.txt").write_text("# initial and target\ndefault 0.05 0.7\n" + ";".join(f"0:{k}" for k in range(1, n, 7)) + " 0.2 0.3\n")
     prefix = str(tmp_path / "run")
     args = [os.path.join(ROOT, "relearn_b200", "bin", "relearn_b200_run"), "--file", str(tmp_path / "positions.txt"), "-g", str(tmp_path), "-s",
             "1000", "-r", str(params["seed"]), "--side", repr(side), "--izhikevich-a", "0.02", "--izhikevich-d", "8", "--synapse-conductance", "3",
             "--growth-rate-axon", "1e-4", "--growth-rate-dendrite-exc", "1e-4", "--growth-rate-dendrite-inh", "1e-4",
-            "--synaptic-elements-lower-bound", "0", "--synaptic-elements-upper-bound", "2", "--output-prefix", prefix]
+            "--synaptic-elements-lower-bound", "0", "--synaptic-elements-upper-bound", "2", "--file-calcium", str(tmp_path / "calcium.txt"),
+            "--output-prefix", prefix]
     r = subprocess.run(args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     ca = np.loadtxt(prefix + "_calcium.txt", dtype=np.float64)
     syn = np.loadtxt(prefix + "_synapses.txt", dtype=np.int64, ndmin=2)
+    from relearn_b200.workloads import read_calcium_file
+
+    ini, tgt = read_calcium_file(str(tmp_path / "calcium.txt"), n)
     sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    sim.set_neurons(calcium=ini)
+    sim.set_targets(tgt)
     u = splitmix64_uniform(params["seed"] + 17, 3 * n).reshape(3, n)
     grown = [2.0 * u[k] for k in range(3)]
     a = np.abs(w).astype(np.float64)

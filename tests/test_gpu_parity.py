@@ -215,3 +215,31 @@ def test_search_properties_at_1m():
     assert np.array_equal(r1["target"], r2["target"])
     assert np.all(r1["target"] != r1["source"])
     assert np.array_equal(r1["signal"], sig[r1["source"]])
+
+
+def test_per_neuron_target_calcium():
+    """Targets from a calcium file (per neuron) steer growth as in the oracle;
+    the FP32 form refuses targets that differ between neurons."""
+    from relearn_b200 import Network, RelearnError
+
+    n = 2000
+    net, sim, params, *_ = net_and_oracle(n, 1000.0, 77)
+    rng = np.random.default_rng(2)
+    target = rng.choice([0.05, 0.3, 0.7], n)
+    initial = rng.uniform(0.0, 0.2, n)
+    net.set_target_calcium(target)
+    net.set_neurons(calcium=initial)
+    sim.set_targets(target)
+    sim.set_neurons(calcium=initial)
+    seed_elements(net, n, 3, 0.0, 2.0)
+    seed_elements(sim, n, 3, 0.0, 2.0)
+    net.simulate(1, 1001)
+    sim.simulate(1, 1001)
+    assert np.array_equal(net.target_calcium(), target)
+    compare_state(net, sim, n)
+    p32 = dict(params)
+    p32["precision"] = 1
+    f = Network(p32)
+    f.set_target_calcium(np.full(n, 0.5))
+    with pytest.raises(RelearnError):
+        f.set_target_calcium(target)

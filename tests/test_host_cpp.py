@@ -74,3 +74,17 @@ def test_network_file_round_trip(tmp_path):
         bad.write_text(line)
         with pytest.raises(ValueError):
             workloads.read_in_network_file(str(bad), 50)
+
+
+def test_calcium_file(tmp_path):
+    from relearn_b200 import workloads
+
+    p = tmp_path / "calcium.txt"
+    p.write_text("# initial and target calcium\ndefault 0.1 0.7\n0:2;-1:4 0.3 0.9\n0:1 0.0 0.5\n")
+    ini, tgt = workloads.read_calcium_file(str(p), 5)
+    assert list(ini) == [0.0, 0.3, 0.1, 0.3, 0.1] and list(tgt) == [0.5, 0.9, 0.7, 0.9, 0.7]
+    for text in ("default 0 0.7\n0:1 0 1\n0:1 0 1\n", "0:1 0 1\n", "default 0 0.7\nexcitatory 0 1\n", "default 0 0.7\n0:6 0 1\n",
+                 "default 0 0.7\n2:1 0 1\n", "default 0 1\ndefault 0 1\n"):
+        p.write_text(text)
+        with pytest.raises(ValueError):
+            workloads.read_calcium_file(str(p), 5)
