@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RL_ABI_VERSION 1
+#define RL_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define RL_API __attribute__((visibility("default")))
@@ -87,7 +87,21 @@ typedef struct rl_config {
     double noise_stddev;          /* normal background input stddev */
     int32_t device;               /* CUDA device ordinal */
     int32_t precision;            /* RL_PRECISION_FP64 (drop-in, bit-exact) or RL_PRECISION_FP32 */
+    int32_t kernel_type;          /* [RL_KERNEL_GAUSSIAN] probability kernel (--kernel-type) */
+    int32_t reserved;
+    double kernel_k;              /* [1] shape of the gamma / Weibull kernel (--gamma-k, --weibull-k) */
+    double kernel_scale;          /* [1] gamma theta / Weibull b (--gamma-theta, --weibull-b) */
+    double linear_cutoff;         /* [+inf] cut-off of the linear kernel (--linear-cutoff) */
 } rl_config;
+
+/* Probability kernels of the search (algorithm/Kernel/KernelType.h): the
+ * attraction of a cell at distance d, times its vacant count, is
+ *   Gaussian: exp((d - mu)^2 * (-1 / sigma^2))              (Gaussian.h:62-68)
+ *   gamma:    1 / (Gamma(k) theta^k) * d^(k-1) * exp(-d / theta) (Gamma.h)
+ *   linear:   1 - d / cutoff for d <= cutoff, else 0; 1 for an infinite cutoff (Linear.h)
+ *   Weibull:  b k * d^(k-1) * exp(-b d^(k-1) d)             (Weibull.h)
+ * sigma is per network in a batched context; the other parameters are shared. */
+enum { RL_KERNEL_GAUSSIAN = 0, RL_KERNEL_GAMMA = 1, RL_KERNEL_LINEAR = 2, RL_KERNEL_WEIBULL = 3 };
 
 /* Precision forms.  FP64: the drop-in; every FP64 operation in the reference's
  * order, bit-exact against the oracle.  FP32: membrane, input, growth and

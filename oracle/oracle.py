@@ -57,7 +57,10 @@ class OrcConfig(C.Structure):
         ("noise_mean", C.c_double),
         ("noise_stddev", C.c_double),
         ("use_libm", C.c_int32),
-        ("reserved", C.c_int32),
+        ("kernel_type", C.c_int32),
+        ("kernel_k", C.c_double),
+        ("kernel_scale", C.c_double),
+        ("linear_cutoff", C.c_double),
     ]
 
 
@@ -99,6 +102,8 @@ def lib():
         L.orc_get_neurons.argtypes = [vp] * 6
         L.orc_set_neurons.argtypes = [vp] * 5
         L.orc_set_targets.argtypes = [vp, vp]
+        L.orc_kernel_prob.restype = C.c_double
+        L.orc_kernel_prob.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_num_edges.restype = u64
         L.orc_num_edges.argtypes = [vp]
         L.orc_get_edges.argtypes = [vp, vp, vp, vp]

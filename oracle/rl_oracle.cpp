@@ -50,7 +50,10 @@ typedef struct orc_config {
     double conductance;       // synaptic_equally_weighted conductance
     double noise_mean, noise_stddev;
     int32_t use_libm;  // 1: std::exp/std::log instead of the shared exp/log
-    int32_t reserved;
+    int32_t kernel_type;    // 0 Gaussian, 1 gamma, 2 linear, 3 Weibull (KernelType.h)
+    double kernel_k;        // gamma / Weibull shape
+    double kernel_scale;    // gamma theta / Weibull b
+    double linear_cutoff;   // linear cut-off (+inf: constant 1)
 } orc_config;
 
 typedef struct orc_request {
@@ -436,9 +439,46 @@ long pick_index(const double* p, long size, double r) {
     return counter - 1;
 }
 
+// KernelBase::get_probability(distance) of the configured kernel:
+// GaussianDistributionKernel (Gaussian.h:62-68), GammaDistributionKernel
+// (Gamma.h: gamma_divisor_inv * pow(d, k - 1) * exp(d * theta_divisor)),
+// LinearDistributionKernel (Linear.h) and WeibullDistributionKernel (Weibull.h:
+// b k * pow(d, k - 1) * exp(-b * pow(d, k - 1) * d)); pow(d, y) is exact for
+// y = 0 and 1 and exp(y log d) otherwise.
+double kernel_probability(const Sim& s, double d, double scale) {
+    const orc_config& c = s.cfg;
+    auto pw = [&](double y) { return y == 0.0 ? 1.0 : (y == 1.0 ? d : s.ex(y * s.lg(d))); };
+    if (c.kernel_type == 1) {
+        const double gamma_divisor_inv = 1.0 / (std::tgamma(c.kernel_k) * std::pow(c.kernel_scale, c.kernel_k));
+        const double theta_divisor = -1.0 / c.kernel_scale;
+        const double f1 = pw(c.kernel_k - 1.0);
+        const double f2 = s.ex(d * theta_divisor);
+        return gamma_divisor_inv * f1 * f2;
+    }
+    if (c.kernel_type == 2) {
+        if (std::isinf(c.linear_cutoff)) {
+            return 1.0;
+        }
+        if (d > c.linear_cutoff) {
+            return 0.0;
+        }
+        const double factor = d / c.linear_cutoff;
+        return 1 - factor;
+    }
+    if (c.kernel_type == 3) {
+        const double f1 = c.kernel_scale * c.kernel_k;
+        const double f2 = pw(c.kernel_k - 1.0);
+        const double exponent = -c.kernel_scale * f2 * d;
+        const double f3 = s.ex(exponent);
+        return f1 * f2 * f3;
+    }
+    const double num = (d - s.cfg.mu) * (d - s.cfg.mu);
+    return s.ex(num * scale);
+}
+
 // Kernel::pick_target + create_probability_interval (Kernel.h:90-173) with
-// GaussianDistributionKernel::get_probability (Gaussian.h:62-68) and
-// ProbabilityPicker::pick_target(values, key) (ProbabilityPicker.h:97-112).
+// the kernel's get_probability and ProbabilityPicker::pick_target(values, key)
+// (ProbabilityPicker.h:97-112).
 int pick_candidate(const Sim& s, const std::vector<int>& cand, uint32_t source, const V3& src, int t, uint32_t step, uint32_t j, uint32_t depth, std::vector<double>& w) {
     if (cand.empty()) {
         return -1;
@@ -452,8 +492,7 @@ int pick_candidate(const Sim& s, const std::vector<int>& cand, uint32_t source, 
         if (!(!nd.parent && nd.neuron == (int32_t)source)) {
             const V3& tp = nd.dpos[t];
             const double d = hypot3(tp.x - src.x, tp.y - src.y, tp.z - src.z);
-            const double num = (d - s.cfg.mu) * (d - s.cfg.mu);
-            const double e = s.ex(num * scale);
+            const double e = kernel_probability(s, d, scale);
             prob = (e * 1.0) * (double)nd.cnt[t];
         }
         w[i] = prob;
@@ -1069,6 +1108,20 @@ void orc_set_neurons(void* h, const double* x, const double* u, const double* ca
     if (u) std::copy(u, u + s->n, s->u.begin());
     if (calcium) std::copy(calcium, calcium + s->n, s->calcium.begin());
     if (fired) std::copy(fired, fired + s->n, s->fired.begin());
+}
+
+// The kernel probability of distance d (for the agreement test of the shared
+// formula): a Gaussian / gamma / linear / Weibull kernel with the shared exp / log.
+double orc_kernel_prob(int type, double d, double mu, double sigma, double k, double scale, double cutoff) {
+    Sim s{};
+    s.cfg.kernel_type = type;
+    s.cfg.mu = mu;
+    s.cfg.sigma = sigma;
+    s.cfg.kernel_k = k;
+    s.cfg.kernel_scale = scale;
+    s.cfg.linear_cutoff = cutoff;
+    s.cfg.use_libm = 0;
+    return kernel_probability(s, d, -1.0 / (sigma * sigma));
 }
 
 // Per-neuron target calcium (CalciumIO's target function, io/CalciumIO.cpp:27-130).

@@ -77,10 +77,17 @@ class RlConfig(C.Structure):
         ("noise_stddev", C.c_double),
         ("device", C.c_int32),
         ("precision", C.c_int32),
+        ("kernel_type", C.c_int32),
+        ("reserved", C.c_int32),
+        ("kernel_k", C.c_double),
+        ("kernel_scale", C.c_double),
+        ("linear_cutoff", C.c_double),
     ]
 
 
 PRECISION_FP64, PRECISION_FP32 = 0, 1
+KERNEL_GAUSSIAN, KERNEL_GAMMA, KERNEL_LINEAR, KERNEL_WEIBULL = 0, 1, 2, 3
+KERNELS = {"gaussian": KERNEL_GAUSSIAN, "gamma": KERNEL_GAMMA, "linear": KERNEL_LINEAR, "weibull": KERNEL_WEIBULL}
 
 
 class RlNetwork(C.Structure):
@@ -265,7 +272,8 @@ def default_params(num_neurons: int, side: float) -> dict:
                 iz_a=0.02, iz_b=0.2, iz_c=-65.0, iz_d=8.0, iz_v_spike=30.0, iz_k1=0.04, iz_k2=5.0, iz_k3=140.0,
                 beta=0.001, tau_c=10000.0, target_calcium=0.7, initial_calcium=0.0,
                 growth_rate=(1e-4, 1e-4, 1e-4), min_calcium=(0.4, 0.1, 0.0), retract_ratio=(0.0, 0.0, 0.0),
-                conductance=3.0, noise_mean=5.0, noise_stddev=2.0, device=0, precision=PRECISION_FP64)
+                conductance=3.0, noise_mean=5.0, noise_stddev=2.0, device=0, precision=PRECISION_FP64,
+                kernel_type=KERNEL_GAUSSIAN, kernel_k=1.0, kernel_scale=1.0, linear_cutoff=float("inf"))
 
 
 def make_config(params: dict) -> RlConfig:

@@ -57,6 +57,7 @@ struct SearchArgs {
     uint32_t step;
     uint32_t* err;
     unsigned long long* touched;
+    KernelParams kernel;
 };
 
 // Parameters of the network a warp searches in.
@@ -79,7 +80,7 @@ struct Eval {
 
 // test_acceptance_criterion + calculate_attractiveness_to_connect for one node.
 __device__ __forceinline__ Eval evaluate(const double4& r, uint2 t, double md, double sx, double sy, double sz, uint32_t source, double theta, double mu,
-                                         double scale, bool fallback) {
+                                         double scale, bool fallback, const KernelParams& K) {
     Eval e{ ST_DISCARD, 0.0 };
     const uint32_t cnt = rcount(r);
     if (cnt == 0) {
@@ -98,8 +99,7 @@ __device__ __forceinline__ Eval evaluate(const double4& r, uint2 t, double md, d
     if (leaf && t.x == source) {
         e.w = 0.0;  // a neuron never connects to itself
     } else if (!fallback) {
-        const double num = (d - mu) * (d - mu);
-        e.w = (rl_exp(num * scale) * 1.0) * (double)cnt;
+        e.w = (rl_kernel_prob(K.type, d, mu, scale, K.k_minus_1, K.a, K.b, K.cutoff, K.cutoff_inf) * 1.0) * (double)cnt;
     } else {
         e.w = (double)cnt / d;
     }
@@ -144,7 +144,7 @@ __device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t 
     if (include_root) {
         const double4 rr = ldg4(&A.rec[sub]);
         const uint2 tt = __ldg(&A.topo[sub]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
             res.sum += e.w;
@@ -176,7 +176,7 @@ __device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t 
         const uint32_t child = child_index(pt, oct);
         const double4 rr = ldg4(&A.rec[child]);
         const uint2 tt = __ldg(&A.topo[child]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
+        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
             res.sum += e.w;
@@ -240,7 +240,7 @@ __device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t pm
         const double md = __ldg(&A.maxdim[child]);
         int status = ST_DISCARD;
         if ((act >> lane) & 1u) {
-            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback);
+            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
             status = e.status;
             ++touched;
             if (e.status == ST_ACCEPT) {
@@ -695,6 +695,7 @@ void run_search(Ctx& c, uint32_t step) {
             A.step = step;
             A.err = c.err.p;
             A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
+            A.kernel = c.kernel;
         }
         auto launch_all = [&](const SearchVariant& v) {
             for (int t = 0; t < 2; ++t) {

@@ -4,6 +4,7 @@
 #include <mutex>
 #include <map>
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -131,10 +132,33 @@ void validate(const rl_config& k) {
     RL_CHECK(k.h_calcium >= 1 && k.h_calcium <= 1000, RL_ERR_INVALID, "h_calcium must lie in [1, 1000]");
     RL_CHECK(k.noise_stddev > 0.0, RL_ERR_INVALID, "noise_stddev must be positive");
     RL_CHECK(k.precision == RL_PRECISION_FP64 || k.precision == RL_PRECISION_FP32, RL_ERR_INVALID, "precision must be FP64 or FP32");
+    RL_CHECK(k.kernel_type >= RL_KERNEL_GAUSSIAN && k.kernel_type <= RL_KERNEL_WEIBULL, RL_ERR_INVALID, "unknown kernel type");
+    // GammaDistributionKernel / WeibullDistributionKernel / LinearDistributionKernel constructors
+    RL_CHECK(k.kernel_type != RL_KERNEL_GAMMA || (k.kernel_k > 0.0 && k.kernel_scale > 0.0), RL_ERR_INVALID, "gamma k and theta must be positive");
+    RL_CHECK(k.kernel_type != RL_KERNEL_WEIBULL || (k.kernel_k > 0.0 && k.kernel_scale > 0.0), RL_ERR_INVALID, "Weibull k and b must be positive");
+    RL_CHECK(k.kernel_type != RL_KERNEL_LINEAR || k.linear_cutoff >= 0.0, RL_ERR_INVALID, "the linear cut-off must not be negative");
     for (int a = 0; a < 3; ++a) {
         RL_CHECK(k.box_min[a] <= k.box_max[a], RL_ERR_INVALID, "box_min must not exceed box_max");
         RL_CHECK(k.retract_ratio[a] >= 0.0 && k.retract_ratio[a] <= 1.0, RL_ERR_INVALID, "retract ratio must lie in [0, 1]");
     }
+}
+
+// Constants of the probability kernel, as the kernels' constructors compute
+// them (algorithm/Kernel/Gamma.h, Weibull.h, Linear.h).
+KernelParams make_kernel(const rl_config& k) {
+    KernelParams p;
+    p.type = k.kernel_type;
+    p.k_minus_1 = k.kernel_k - 1.0;
+    if (k.kernel_type == RL_KERNEL_GAMMA) {
+        p.a = 1.0 / (std::tgamma(k.kernel_k) * std::pow(k.kernel_scale, k.kernel_k));  // gamma_divisor_inv
+        p.b = -1.0 / k.kernel_scale;                                                   // theta_divisor
+    } else if (k.kernel_type == RL_KERNEL_WEIBULL) {
+        p.a = k.kernel_scale * k.kernel_k;  // factor_1 = b * k
+        p.b = k.kernel_scale;               // b
+    }
+    p.cutoff = k.linear_cutoff;
+    p.cutoff_inf = std::isinf(k.linear_cutoff) ? 1 : 0;
+    return p;
 }
 
 // The network table: one network from the config, or the ensemble's list.
@@ -212,6 +236,7 @@ void setup_nets(Ctx& c, const rl_network* nets, uint32_t num) {
 void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32_t num_nets = 0) {
     validate(k);
     c.cfg = k;
+    c.kernel = make_kernel(k);
     c.n = k.num_neurons;
     c.device = k.device;
     int count = 0;
@@ -495,6 +520,10 @@ void rl_config_default(rl_config* k, uint32_t num_neurons, double side) {
     k->noise_mean = 5.0;
     k->noise_stddev = 2.0;
     k->device = 0;
+    k->kernel_type = RL_KERNEL_GAUSSIAN;
+    k->kernel_k = 1.0;
+    k->kernel_scale = 1.0;
+    k->linear_cutoff = INFINITY;
 }
 
 rl_status rl_ctx_create(const rl_config* cfg, void** out) {

@@ -390,6 +390,29 @@ __global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4
 constexpr int kStack = kMaxLevels + 4;  // the diagnostic walk
 enum : int { S_DISCARD = 0, S_EXPAND = 1, S_ACCEPT = 2 };
 
+// The probability kernel's constants in FP32 (KernelParams).
+struct Kernel32 {
+    int type;
+    int cutoff_inf;
+    float k_minus_1, a, b, cutoff;
+};
+
+__device__ __forceinline__ float pow_pos32(float d, float y) {
+    return y == 0.0f ? 1.0f : (y == 1.0f ? d : exp2f(y * __log2f(d)));
+}
+
+// Attraction of a cell at distance d (FP32) for the non-Gaussian kernels.
+__device__ __forceinline__ float kernel_prob32(const Kernel32& K, float d) {
+    if (K.type == RL_KERNEL_GAMMA) {
+        return K.a * pow_pos32(d, K.k_minus_1) * __expf(d * K.b);
+    }
+    if (K.type == RL_KERNEL_LINEAR) {
+        return K.cutoff_inf ? 1.0f : (d > K.cutoff ? 0.0f : 1.0f - __fdividef(d, K.cutoff));
+    }
+    const float f2 = pow_pos32(d, K.k_minus_1);  // Weibull
+    return K.a * f2 * __expf(-K.b * f2 * d);
+}
+
 struct Search32 {
     const uint4* rec;
     const uint2* topo;
@@ -407,6 +430,7 @@ struct Search32 {
     float mu;
     uint32_t step;
     uint32_t* err;
+    Kernel32 kernel;
 };
 
 // Parameters of the network a warp searches in.
@@ -464,8 +488,12 @@ __device__ __forceinline__ E32 eval32(const uint4& r, uint2 t, float md, const Q
     if (leaf && t.x == source) {
         e.w = 0.0f;
     } else if (!fb) {
-        const float dm = d - A.mu;
-        e.w = __expf(-(dm * dm) * W.inv_sigma2) * (float)cnt;
+        if (A.kernel.type == RL_KERNEL_GAUSSIAN) {
+            const float dm = d - A.mu;
+            e.w = __expf(-(dm * dm) * W.inv_sigma2) * (float)cnt;
+        } else {
+            e.w = kernel_prob32(A.kernel, d) * (float)cnt;
+        }
     } else {
         e.w = __fdividef((float)cnt, d);
     }
@@ -743,7 +771,8 @@ Search32Kernel fp32_search_kernel(const SearchVariant& v) {
 // ----------------------------------------------------------- diagnostic
 __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
                              double sz, uint32_t source, uint32_t root, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
-                             uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f) {
+                             uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f, KernelParams K) {
+    const Kernel32 K32{ K.type, K.cutoff_inf, (float)K.k_minus_1, (float)K.a, (float)K.b, (float)K.cutoff };
     const QPos sp{ quantize(sx, f.origin[0], f.inv_quantum), quantize(sy, f.origin[1], f.inv_quantum), quantize(sz, f.origin[2], f.inv_quantum) };
     uint32_t fnode[kStack];
     uint32_t frem[kStack];
@@ -777,7 +806,9 @@ __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint
                         status = S_EXPAND;
                     } else {
                         status = S_ACCEPT;
-                        weight = (leaf && tt.x == source) ? 0.0 : (rl_exp(((d - mu) * (d - mu)) * scale) * 1.0) * (double)cnt;
+                        weight = (leaf && tt.x == source) ? 0.0
+                                                          : (rl_kernel_prob(K.type, d, mu, scale, K.k_minus_1, K.a, K.b, K.cutoff, K.cutoff_inf) * 1.0) *
+                                                                (double)cnt;
                     }
                 }
             }
@@ -793,7 +824,8 @@ __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint
                     } else {
                         status = S_ACCEPT;
                         const float dm = d - (float)mu;
-                        weight = (leaf && tt.x == source) ? 0.0 : (double)(__expf(-(dm * dm) * inv_s2) * (float)cnt);
+                        const float kp = K.type == RL_KERNEL_GAUSSIAN ? __expf(-(dm * dm) * inv_s2) : kernel_prob32(K32, d);
+                        weight = (leaf && tt.x == source) ? 0.0 : (double)(kp * (float)cnt);
                     }
                 }
             }
@@ -1016,6 +1048,7 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     A.mu = (float)c.cfg.mu;
     A.step = step;
     A.err = c.err.p;
+    A.kernel = Kernel32{ c.kernel.type, c.kernel.cutoff_inf, (float)c.kernel.k_minus_1, (float)c.kernel.a, (float)c.kernel.b, (float)c.kernel.cutoff };
     const Search32Kernel kern = fp32_search_kernel(v);
     RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");
     const unsigned blocks = (warps + v.warps - 1) / v.warps;
@@ -1048,7 +1081,7 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
     dc.alloc(1);
     k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.recq[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
                                         precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, net, precision,
-                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame);
+                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame, c.kernel);
     RL_LAUNCH_CHECK();
     unsigned long long k = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&k, dc.p, sizeof(k), cudaMemcpyDeviceToHost, c.stream));

@@ -185,6 +185,18 @@ struct NetInfo {
     QFrame frame;
 };
 
+// Probability kernel of the search: `type` is an RL_KERNEL_* value; a and b
+// are the kernel's constants (gamma: 1/(Gamma(k) theta^k) and -1/theta;
+// Weibull: b k and b); k_minus_1 the exponent of d; the linear cut-off.
+struct KernelParams {
+    int type = RL_KERNEL_GAUSSIAN;
+    int cutoff_inf = 1;
+    double k_minus_1 = 0.0;
+    double a = 0.0;
+    double b = 0.0;
+    double cutoff = 0.0;
+};
+
 struct Ctx;
 // Records an event pair around a scope when profiling is on.
 struct PhaseScope {
@@ -269,6 +281,7 @@ struct Ctx {
     int64_t device_peak = 0;   // and at most so far
     bool counted = false;      // counted among the device's live contexts
     Tuning tune;
+    KernelParams kernel;
 };
 
 // Tuning results shared by the contexts of a process, keyed by precision,

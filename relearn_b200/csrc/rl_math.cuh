@@ -233,6 +233,48 @@ RL_HD double rl_hypot3(double x, double y, double z) {
     return a * sqrt(t0 + t1 + t2);
 }
 
+// d^y for d > 0 (the std::pow(distance, k - 1) of the gamma and Weibull
+// kernels): exact for y = 0 and y = 1, exp(y log d) with the shared exp / log
+// otherwise, so that host and device agree bit for bit.
+RL_HD double rl_pow_pos(double d, double y) {
+    if (y == 0.0) {
+        return 1.0;
+    }
+    if (y == 1.0) {
+        return d;
+    }
+    return rl_exp(y * rl_log(d));
+}
+
+// Attraction of a cell at distance d > 0 for the kernel `type`
+// (KernelBase::get_probability(distance)): Gaussian scale = -1/sigma^2 and mu;
+// gamma a = 1/(Gamma(k) theta^k), b = -1/theta; Weibull a = b k, b = b;
+// linear cut-off.  Operation order as in the reference's kernels.
+RL_HD double rl_kernel_prob(int type, double d, double mu, double scale, double k_minus_1, double a, double b, double cutoff, int cutoff_inf) {
+    if (type == 1) {  // gamma (Gamma.h)
+        const double f1 = rl_pow_pos(d, k_minus_1);
+        const double f2 = rl_exp(d * b);
+        return a * f1 * f2;
+    }
+    if (type == 2) {  // linear (Linear.h)
+        if (cutoff_inf) {
+            return 1.0;
+        }
+        if (d > cutoff) {
+            return 0.0;
+        }
+        return 1 - d / cutoff;
+    }
+    if (type == 3) {  // Weibull (Weibull.h)
+        const double f2 = rl_pow_pos(d, k_minus_1);
+        const double exponent = -b * f2 * d;
+        const double f3 = rl_exp(exponent);
+        return a * f2 * f3;
+    }
+    const double num = (d - mu) * (d - mu);  // Gaussian (Gaussian.h:62-68)
+    return rl_exp(num * scale);
+}
+
 // std::nextafter(total, total + 1e-5) for finite total > 0
 // (ProbabilityPicker.h:108 of the reference).
 RL_HD double next_up_eps(double total) {

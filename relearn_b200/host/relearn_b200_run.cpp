@@ -52,6 +52,8 @@ void usage() {
     std::printf(
         "usage: relearn_b200_run [--num-neurons N | --file POSITIONS] -s STEPS [options]\n"
         "  reference options: --algorithm barnes-hut, --neuron-model izhikevich, -t/--theta, --gaussian-sigma,\n"
+        "    --gaussian-mu, --kernel-type gaussian|gamma|linear|weibull, --gamma-k, --gamma-theta, --linear-cutoff,\n"
+        "    --weibull-k, --weibull-b,\n"
         "    -r/--random-seed, --plasticity-update-step, --synapse-conductance, --background-activity-mean,\n"
         "    --background-activity-stddev, --beta, --calcium-decay, --target-ca, --initial-ca,\n"
         "    --growth-rate-axon, --growth-rate-dendrite-exc, --growth-rate-dendrite-inh, --min-calcium-axons,\n"
@@ -92,6 +94,27 @@ bool parse(int argc, char** argv, Options& o) {
             c.theta = num();
         } else if (a == "--gaussian-sigma") {
             c.sigma = num();
+        } else if (a == "--gaussian-mu") {
+            c.mu = num();
+        } else if (a == "--kernel-type") {
+            const std::string t = next();
+            if (t == "gaussian") {
+                c.kernel_type = RL_KERNEL_GAUSSIAN;
+            } else if (t == "gamma") {
+                c.kernel_type = RL_KERNEL_GAMMA;
+            } else if (t == "linear") {
+                c.kernel_type = RL_KERNEL_LINEAR;
+            } else if (t == "weibull") {
+                c.kernel_type = RL_KERNEL_WEIBULL;
+            } else {
+                throw RelearnException("unknown kernel type " + t + " (gaussian, gamma, linear, weibull)");
+            }
+        } else if (a == "--gamma-k" || a == "--weibull-k") {
+            c.kernel_k = num();
+        } else if (a == "--gamma-theta" || a == "--weibull-b") {
+            c.kernel_scale = num();
+        } else if (a == "--linear-cutoff") {
+            c.linear_cutoff = num();
         } else if (a == "--random-seed" || a == "-r") {
             c.seed = std::stoull(next());
         } else if (a == "--plasticity-update-step") {

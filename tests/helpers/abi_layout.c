@@ -18,6 +18,10 @@ int main(void) {
     F(rl_config, conductance);
     F(rl_config, device);
     F(rl_config, precision);
+    F(rl_config, kernel_type);
+    F(rl_config, kernel_k);
+    F(rl_config, kernel_scale);
+    F(rl_config, linear_cutoff);
     F(rl_stats, max_level);
     printf("rl_network %zu\n", sizeof(rl_network));
     printf("rl_tuning %zu\n", sizeof(rl_tuning));

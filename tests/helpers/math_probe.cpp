@@ -21,4 +21,7 @@ void probe_philox(unsigned c0, unsigned c1, unsigned c2, unsigned c3, unsigned k
     out[3] = r.w;
 }
 double probe_next_up(double t) { return rl::next_up_eps(t); }
+double probe_kernel_prob(int type, double d, double mu, double scale, double km1, double a, double b, double cutoff, int inf) {
+    return rl::rl_kernel_prob(type, d, mu, scale, km1, a, b, cutoff, inf);
+}
 }

@@ -45,7 +45,8 @@ def test_struct_layout(tmp_path):
     assert int(lines["rl_stats"]) == C.sizeof(R.RlStats)
     assert int(lines["rl_request"]) == R.REQUEST_DTYPE.itemsize
     assert int(lines["rl_synapse"]) == R.SYNAPSE_DTYPE.itemsize
-    for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device", "precision"):
+    for f in ("seed", "box_min", "theta", "growth_rate", "conductance", "device", "precision", "kernel_type", "kernel_k", "kernel_scale",
+              "linear_cutoff"):
         assert int(lines[f"rl_config.{f}"]) == getattr(R.RlConfig, f).offset
     assert int(lines["rl_stats.max_level"]) == R.RlStats.max_level.offset
     assert int(lines["RL_NUM_SEARCH_SHAPES"]) == R.NUM_SEARCH_SHAPES == len(R.SEARCH_SHAPES)
@@ -66,7 +67,7 @@ def test_host_only_entry_points(built_lib):
     import relearn_b200 as R
 
     L = R.load_library()
-    assert L.rl_abi_version() == 1
+    assert L.rl_abi_version() == 2
     cfg = R.RlConfig()
     L.rl_config_default(C.byref(cfg), 2000, 1000.0)
     # reference defaults: Parameters.h:123-130, CalciumCalculatorBase.h:206-210, Gaussian.h:38-39
@@ -110,6 +111,8 @@ def probe(tmp_path_factory):
     for name in ("probe_hypot3", "probe_std_hypot3"):
         getattr(L, name).restype = C.c_double
         getattr(L, name).argtypes = [C.c_double] * 3
+    L.probe_kernel_prob.restype = C.c_double
+    L.probe_kernel_prob.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
     L.probe_normal.restype = C.c_double
     L.probe_normal.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_double, C.c_double]
     L.probe_philox.argtypes = [C.c_uint32] * 6 + [C.c_void_p]
@@ -140,3 +143,27 @@ def test_shared_math_bitwise_agreement(probe, oracle_mod):
         assert list(out) == oracle_mod.philox(*map(int, c))
     for t in rng.uniform(1e-3, 1e6, 1000):
         assert probe.probe_next_up(float(t)) == np.nextafter(float(t), float(t) + 1e-5)
+
+
+@pytest.mark.parametrize("kernel", [(1, 2.0, 400.0, 0.0), (1, 1.0, 300.0, 0.0), (2, 1.0, 1.0, 1500.0), (2, 1.0, 1.0, float("inf")),
+                                    (3, 1.5, 0.002, 0.0), (3, 1.0, 0.001, 0.0), (0, 1.0, 1.0, 0.0)])
+def test_kernel_probability_agrees_with_oracle(probe, oracle_mod, kernel):
+    """The shared kernel formula (product) and the oracle's restatement of the
+    reference's kernels give the same bits for every kernel type."""
+    import math
+
+    kt, k, sc, cut = kernel
+    O = oracle_mod.lib()
+    a = b = 0.0
+    if kt == 1:
+        a = 1.0 / (math.gamma(k) * sc**k)
+        b = -1.0 / sc
+    elif kt == 3:
+        a = sc * k
+        b = sc
+    sigma = 750.0
+    rng = np.random.default_rng(kt)
+    for d in np.concatenate([rng.uniform(0.5, 4000.0, 3000), [1.0, 1499.99, 1500.0, 1500.01]]):
+        mine = probe.probe_kernel_prob(kt, float(d), 0.0, -1.0 / (sigma * sigma), k - 1.0, a, b, cut, 1 if math.isinf(cut) else 0)
+        ref = O.orc_kernel_prob(kt, float(d), 0.0, sigma, k, sc, cut)
+        assert mine == ref, (kernel, d, mine, ref)

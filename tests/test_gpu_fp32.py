@@ -81,3 +81,31 @@ def test_seeded_fp32_run_bookkeeping():
     assert ax.sum() == np.abs(w).sum() == ex.sum() + ih.sum()
     out_deg = np.bincount(s, weights=np.abs(w), minlength=n)
     assert np.array_equal(out_deg.astype(np.uint32), ax)
+
+
+@pytest.mark.parametrize("kernel", [dict(kernel_type=1, kernel_k=2.0, kernel_scale=400.0), dict(kernel_type=2, linear_cutoff=1500.0),
+                                    dict(kernel_type=3, kernel_k=1.5, kernel_scale=0.002)])
+def test_selection_probabilities_other_kernels(kernel):
+    """Gamma, linear and Weibull kernels in FP32 (powers through log2 / exp2):
+    selection probabilities within 1e-4 relative of the FP64 form for every
+    candidate with probability >= 1e-6."""
+    from relearn_b200 import Network
+
+    n = 20000
+    params, pos, sig = small_network(n, 2700.0, 12)
+    params.update(kernel)
+    params["precision"] = 1
+    net = Network(params)
+    net.set_positions(pos, sig)
+    one = np.ones(n, np.uint32)
+    net.prepare_update_connectivity(one, one, one)
+    worst = 0.0
+    for s in np.random.default_rng(4).choice(n, 20, replace=False):
+        n64, w64 = net.candidate_weights(int(s), 0)
+        n32, w32 = net.candidate_weights(int(s), 1)
+        p64 = dict(zip(n64.tolist(), (w64 / w64.sum()).tolist()))
+        p32 = dict(zip(n32.tolist(), (w32 / w32.sum()).tolist()))
+        for node, p in p64.items():
+            if p >= 1e-6:
+                worst = max(worst, abs(p32.get(node, 0.0) - p) / p)
+    assert worst <= 1e-4, worst

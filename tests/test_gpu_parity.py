@@ -243,3 +243,33 @@ def test_per_neuron_target_calcium():
     f.set_target_calcium(np.full(n, 0.5))
     with pytest.raises(RelearnError):
         f.set_target_calcium(target)
+
+
+KERNELS = [("gamma", dict(kernel_type=1, kernel_k=2.0, kernel_scale=400.0)), ("gamma_k1", dict(kernel_type=1, kernel_k=1.0, kernel_scale=300.0)),
+           ("linear", dict(kernel_type=2, linear_cutoff=1500.0)), ("linear_inf", dict(kernel_type=2)),
+           ("weibull", dict(kernel_type=3, kernel_k=1.5, kernel_scale=0.002))]
+
+
+@pytest.mark.parametrize("name,kernel", KERNELS)
+def test_search_requests_other_kernels(name, kernel):
+    """--kernel-type gamma / linear / weibull (algorithm/Kernel/*.h): requests
+    bit for bit against the oracle."""
+    from oracle import oracle as O
+    from relearn_b200 import Network
+
+    n = 4000
+    params, pos, sig = small_network(n, 1260.0, 91)
+    params.update(kernel)
+    net = Network(params)
+    net.set_positions(pos, sig)
+    sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    seed_elements(sim, n, 5, 0.0, 3.0)
+    seed_elements(net, n, 5, 0.0, 3.0)
+    va, ve, vi = (sim.get_elements(t)["vacant"] for t in range(3))
+    sim.update_tree(ve, vi)
+    net.prepare_update_connectivity(va, ve, vi)
+    g = net.find_targets(100)
+    o = sim.find_targets(100)
+    assert len(g) == len(o) > 0
+    for k in ("target", "source", "j", "signal"):
+        assert np.array_equal(g[k], o[k]), (name, k)
