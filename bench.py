@@ -119,6 +119,10 @@ def build_network(n, side, seed, placement):
     return params, pos, sig
 
 
+# dram__bytes_read.sum + dram__bytes_write.sum of one activity launch at 1M
+# neurons (ncu --set full, see profiles/): FP64 59.0 + 4.0 MB, FP32 30.0 + 0.1 MB
+PROFILED_TRAFFIC = {0: 63.0e6, 1: 30.1e6}
+
 ACT_BYTES_FP32 = 62  # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes input 4 + x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12
 
 
@@ -176,9 +180,13 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     bytes_per_launch = per_neuron * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+    # DRAM bytes per launch from one ncu capture of the same kernel on this
+    # workload (profiles/k_activity_f32_1M.md, k_activity_fp64_1M.md): reads
+    # equal the algorithmic read bytes, writes stay in L2 during the launch
+    traffic = PROFILED_TRAFFIC.get(precision) if (n == 1_000_000 and args.placement == "uniform" and not edges) else None
     roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if hbm else None, "traffic": None, "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch,
-            "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
+            "frac": achieved / hbm if hbm else None, "traffic": traffic, "traffic_unit": "bytes per launch (ncu dram read + write)",
+            "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
     return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof,
                 tuning=net.tuning())
 
