@@ -92,7 +92,22 @@ typedef struct rl_config {
     double kernel_k;              /* [1] shape of the gamma / Weibull kernel (--gamma-k, --weibull-k) */
     double kernel_scale;          /* [1] gamma theta / Weibull b (--gamma-theta, --weibull-b) */
     double linear_cutoff;         /* [+inf] cut-off of the linear kernel (--linear-cutoff) */
+    int32_t neuron_model;         /* [RL_MODEL_IZHIKEVICH] --neuron-model */
+    uint32_t poisson_refractory;  /* [4] Poisson: steps without spiking after a spike */
+    double poisson_x0;            /* [0.05] Poisson: resting potential */
+    double poisson_tau_x;         /* [5] Poisson: decay of the potential */
+    double fhn_a, fhn_b, fhn_phi; /* [0.7, 0.8, 0.08] FitzHugh-Nagumo */
+    double fhn_init_x, fhn_init_w;  /* [-1.2, -0.6] FitzHugh-Nagumo initial x and w */
+    double aeif_C, aeif_g_L, aeif_E_L, aeif_V_T, aeif_d_T;  /* [281, 30, -70.6, -50.4, 2] AEIF */
+    double aeif_tau_w, aeif_a, aeif_b, aeif_V_spike;          /* [144, 4, 0.0805, 20] AEIF */
 } rl_config;
+
+/* Neuron models (--neuron-model; the classes under neurons/models), defaults of their
+ * Parameters.h.  The second state variable (rl_get_neurons' u) is the
+ * Izhikevich recovery u, the FitzHugh-Nagumo and AEIF adaptation w, or the
+ * Poisson model's refractory steps left.  The FP32 form runs the Izhikevich
+ * model only. */
+enum { RL_MODEL_IZHIKEVICH = 0, RL_MODEL_POISSON = 1, RL_MODEL_FITZHUGH_NAGUMO = 2, RL_MODEL_AEIF = 3 };
 
 /* Probability kernels of the search (algorithm/Kernel/KernelType.h): the
  * attraction of a cell at distance d, times its vacant count, is

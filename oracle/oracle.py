@@ -61,6 +61,24 @@ class OrcConfig(C.Structure):
         ("kernel_k", C.c_double),
         ("kernel_scale", C.c_double),
         ("linear_cutoff", C.c_double),
+        ("neuron_model", C.c_int32),
+        ("poisson_refractory", C.c_uint32),
+        ("poisson_x0", C.c_double),
+        ("poisson_tau_x", C.c_double),
+        ("fhn_a", C.c_double),
+        ("fhn_b", C.c_double),
+        ("fhn_phi", C.c_double),
+        ("fhn_init_x", C.c_double),
+        ("fhn_init_w", C.c_double),
+        ("aeif_C", C.c_double),
+        ("aeif_g_L", C.c_double),
+        ("aeif_E_L", C.c_double),
+        ("aeif_V_T", C.c_double),
+        ("aeif_d_T", C.c_double),
+        ("aeif_tau_w", C.c_double),
+        ("aeif_a", C.c_double),
+        ("aeif_b", C.c_double),
+        ("aeif_V_spike", C.c_double),
     ]
 
 
@@ -102,6 +120,8 @@ def lib():
         L.orc_get_neurons.argtypes = [vp] * 6
         L.orc_set_neurons.argtypes = [vp] * 5
         L.orc_set_targets.argtypes = [vp, vp]
+        L.orc_model_step.restype = C.c_int
+        L.orc_model_step.argtypes = [P(OrcConfig), P(dbl), P(dbl), dbl, u32, u32]
         L.orc_kernel_prob.restype = C.c_double
         L.orc_kernel_prob.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_num_edges.restype = u64
@@ -267,6 +287,15 @@ def izhikevich(x: float, u: float, inp: float, h: int, a, b, c, d, v_spike=30.0,
 
 def growth_curve(current: float, eta: float, epsilon: float, use_libm: bool = False) -> float:
     return float(lib().orc_growth_curve(current, eta, epsilon, int(use_libm)))
+
+
+def model_step(params: dict, x: float, u: float, inp: float, step: int = 1, neuron: int = 0):
+    """One update_activity of the configured neuron model for one neuron:
+    returns (x, u, fired)."""
+    cfg = make_config(params)
+    xc, uc = C.c_double(x), C.c_double(u)
+    f = lib().orc_model_step(C.byref(cfg), C.byref(xc), C.byref(uc), inp, step, neuron)
+    return xc.value, uc.value, bool(f)
 
 
 def calcium(c: float, fired: bool, beta: float, tau: float, h: int) -> float:

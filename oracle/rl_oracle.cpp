@@ -54,6 +54,11 @@ typedef struct orc_config {
     double kernel_k;        // gamma / Weibull shape
     double kernel_scale;    // gamma theta / Weibull b
     double linear_cutoff;   // linear cut-off (+inf: constant 1)
+    int32_t neuron_model;   // 0 Izhikevich, 1 Poisson, 2 FitzHugh-Nagumo, 3 AEIF
+    uint32_t poisson_refractory;
+    double poisson_x0, poisson_tau_x;
+    double fhn_a, fhn_b, fhn_phi, fhn_init_x, fhn_init_w;
+    double aeif_C, aeif_g_L, aeif_E_L, aeif_V_T, aeif_d_T, aeif_tau_w, aeif_a, aeif_b, aeif_V_spike;
 } orc_config;
 
 typedef struct orc_request {
@@ -786,14 +791,84 @@ uint64_t delete_synapses(Sim& s, uint32_t step, int pass, const std::vector<uint
     return requests.size();
 }
 
+// One neuron's update_activity for the configured model, on x and the second
+// state variable u (Izhikevich u, FitzHugh-Nagumo / AEIF w, Poisson refractory
+// steps left); returns the fired flag.
+uint8_t model_step(const Sim& s, double& xv, double& uv, double input, uint32_t step, uint32_t neuron) {
+    const orc_config& c = s.cfg;
+    const double scale_m = 1.0 / (double)c.h_model;
+    const double ab = c.iz_a * c.iz_b;
+    uint8_t spiked = 0;
+    if (c.neuron_model == 1) {
+        // PoissonModelCPU::update_activity (models/poisson/PoissonModelCPU.cpp):
+        // u counts the refractory steps left; the threshold is
+        // RandomHolder::get_random_uniform_double(PoissonModel, 0, 1) from the shared stream
+        const double tau_x_inverse = 1.0 / c.poisson_tau_x;
+        for (uint32_t it = 0; it < c.h_model; ++it) {
+            xv += ((c.poisson_x0 - xv) * tau_x_inverse + input) * scale_m;
+        }
+        if (uv == 0.0) {
+            const double threshold = oracle::unit_closed_open(oracle::stream_draw(c.seed, step, neuron, 0, oracle::S_POISSON, 0));
+            if (xv >= threshold) {
+                spiked = 1;
+                uv = (double)c.poisson_refractory;
+            }
+        } else {
+            uv -= 1.0;
+        }
+    } else if (c.neuron_model == 2) {
+        // FitzHughNagumoModelCPU::update_activity (models/fitzhughnagumo/FitzHughNagumoModelCPU.cpp)
+        const double third = 1.0 / 3.0;
+        for (uint32_t it = 0; it < c.h_model; ++it) {
+            const double x_increase = xv - (xv * xv * xv * third) - uv + input;
+            const double w_increase = c.fhn_phi * (xv + c.fhn_a - c.fhn_b * uv);
+            xv += x_increase * scale_m;
+            uv += w_increase * scale_m;
+        }
+        spiked = (uv > xv - xv * xv * xv * third && xv > 1.0) ? 1 : 0;
+    } else if (c.neuron_model == 3) {
+        // AEIFModelCPU::update_activity (models/aeif/AEIFModelCPU.cpp)
+        const double d_T_inverse = 1.0 / c.aeif_d_T;
+        const double tau_w_inverse = 1.0 / c.aeif_tau_w;
+        const double C_inverse = 1.0 / c.aeif_C;
+        for (uint32_t it = 0; it < c.h_model; ++it) {
+            const double linear_part = -c.aeif_g_L * (xv - c.aeif_E_L);
+            const double exp_part = c.aeif_g_L * c.aeif_d_T * s.ex((xv - c.aeif_V_T) * d_T_inverse);
+            const double x_increase = (linear_part + exp_part - uv + input) * C_inverse;
+            const double w_increase = (c.aeif_a * (xv - c.aeif_E_L) - uv) * tau_w_inverse;
+            xv += x_increase * scale_m;
+            uv += w_increase * scale_m;
+            if (xv >= c.aeif_V_spike) {
+                xv = c.aeif_E_L;
+                uv += c.aeif_b;
+                spiked = 1;
+                break;
+            }
+        }
+    } else {
+        // IzhikevichModelCPU::update_activity (IzhikevichModelCPU.cpp:75-125)
+        for (uint32_t it = 0; it < c.h_model; ++it) {
+            const double x_inc = (c.iz_k1 * xv * xv) + (c.iz_k2 * xv) + c.iz_k3 - uv + input;
+            const double u_inc = (ab * xv) - (c.iz_a * uv);
+            xv += x_inc * scale_m;
+            uv += u_inc * scale_m;
+            if (xv >= c.iz_v_spike) {
+                xv = c.iz_c;
+                uv += c.iz_d;
+                spiked = 1;
+                break;
+            }
+        }
+    }
+    return spiked;
+}
+
 // One activity step, in the order of Simulation::simulate
-// (sim/Simulation.cpp:443-453): input, Izhikevich, calcium, growth deltas.
+// (sim/Simulation.cpp:443-453): input, the neuron model, calcium, growth deltas.
 void activity_step(Sim& s, uint32_t step) {
     const orc_config& c = s.cfg;
     const uint32_t n = s.n;
     s.fired_prev = s.fired;
-    const double scale_m = 1.0 / (double)c.h_model;
-    const double ab = c.iz_a * c.iz_b;
     const double scale_c = 1.0 / (double)c.h_calcium;
     const double tau_inv = -1.0 / c.tau_c;
     const double factor_inv = 1.0 / 1.6651092223153955127063292897904020952611777045288814583336582344;
@@ -822,22 +897,9 @@ void activity_step(Sim& s, uint32_t step) {
         const double z = oracle::as241(oracle::unit_open(r), [&](double v) { return s.lg(v); });
         input += c.noise_mean + c.noise_stddev * z;
         s.input[i] = input;
-        // IzhikevichModelCPU::update_activity (IzhikevichModelCPU.cpp:75-125)
         double xv = s.x[i];
         double uv = s.u[i];
-        uint8_t spiked = 0;
-        for (uint32_t it = 0; it < c.h_model; ++it) {
-            const double x_inc = (c.iz_k1 * xv * xv) + (c.iz_k2 * xv) + c.iz_k3 - uv + input;
-            const double u_inc = (ab * xv) - (c.iz_a * uv);
-            xv += x_inc * scale_m;
-            uv += u_inc * scale_m;
-            if (xv >= c.iz_v_spike) {
-                xv = c.iz_c;
-                uv += c.iz_d;
-                spiked = 1;
-                break;
-            }
-        }
+        const uint8_t spiked = model_step(s, xv, uv, input, step, (uint32_t)i);
         s.x[i] = xv;
         s.u[i] = uv;
         s.fired[i] = spiked;
@@ -932,8 +994,20 @@ void* orc_create(const orc_config* cfg, const double* pos_xyz, const uint8_t* si
     }
     s->tree.index_leaves(n);
     // IzhikevichModelBase::init_neurons (IzhikevichModelBase.cpp:59-66)
-    s->x.assign(n, cfg->iz_c);
-    s->u.assign(n, 0.0);
+    // init_neurons of the model (IzhikevichModelBase, FitzHughNagumoModelBase,
+    // AEIFModelBase); NeuronModel::init and PoissonModelBase::init: x = 0, no
+    // refractory steps
+    double x0 = cfg->iz_c, u0 = 0.0;
+    if (cfg->neuron_model == 1) {
+        x0 = 0.0;
+    } else if (cfg->neuron_model == 2) {
+        x0 = cfg->fhn_init_x;
+        u0 = cfg->fhn_init_w;
+    } else if (cfg->neuron_model == 3) {
+        x0 = cfg->aeif_E_L;
+    }
+    s->x.assign(n, x0);
+    s->u.assign(n, u0);
     s->input.assign(n, 0.0);
     s->fired.assign(n, 0);
     s->fired_prev.assign(n, 0);
@@ -1122,6 +1196,14 @@ double orc_kernel_prob(int type, double d, double mu, double sigma, double k, do
     s.cfg.linear_cutoff = cutoff;
     s.cfg.use_libm = 0;
     return kernel_probability(s, d, -1.0 / (sigma * sigma));
+}
+
+// One model update (h substeps) of a single neuron for the pins of the neuron
+// models: *x, *u in and out, returns the fired flag.
+int orc_model_step(const orc_config* cfg, double* x, double* u, double input, uint32_t step, uint32_t neuron) {
+    Sim s{};
+    s.cfg = *cfg;
+    return model_step(s, *x, *u, input, step, neuron);
 }
 
 // Per-neuron target calcium (CalciumIO's target function, io/CalciumIO.cpp:27-130).

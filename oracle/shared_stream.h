@@ -56,7 +56,7 @@ inline Words philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t
     return Words{ { c[0], c[1], c[2], c[3] } };
 }
 
-enum : uint32_t { S_BH = 1, S_CONNECT = 2, S_NOISE = 3, S_DELETE = 4 };
+enum : uint32_t { S_BH = 1, S_CONNECT = 2, S_NOISE = 3, S_DELETE = 4, S_POISSON = 5 };
 
 inline Words stream_draw(uint64_t seed, uint32_t step, uint32_t neuron, uint32_t sub, uint32_t stream, uint32_t depth) {
     return philox(step, neuron, sub, (stream << 24) | (depth & 0xFFFFFFu), (uint32_t)seed, (uint32_t)(seed >> 32));

@@ -28,7 +28,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librelearn_b200.so")
 
 ALGORITHMS = {"barnes-hut": "BarnesHut"}
-NEURON_MODELS = {"izhikevich": "IzhikevichModel"}
+NEURON_MODELS = {"izhikevich": 0, "poisson": 1, "fitzhughnagumo": 2, "aeif": 3}
 
 RL_OK = 0
 STATUS_NAMES = {0: "RL_OK", 1: "RL_ERR_INVALID", 2: "RL_ERR_OOM", 3: "RL_ERR_DEVICE", 4: "RL_ERR_TIMEOUT", 5: "RL_ERR_OVERFLOW",
@@ -82,11 +82,30 @@ class RlConfig(C.Structure):
         ("kernel_k", C.c_double),
         ("kernel_scale", C.c_double),
         ("linear_cutoff", C.c_double),
+        ("neuron_model", C.c_int32),
+        ("poisson_refractory", C.c_uint32),
+        ("poisson_x0", C.c_double),
+        ("poisson_tau_x", C.c_double),
+        ("fhn_a", C.c_double),
+        ("fhn_b", C.c_double),
+        ("fhn_phi", C.c_double),
+        ("fhn_init_x", C.c_double),
+        ("fhn_init_w", C.c_double),
+        ("aeif_C", C.c_double),
+        ("aeif_g_L", C.c_double),
+        ("aeif_E_L", C.c_double),
+        ("aeif_V_T", C.c_double),
+        ("aeif_d_T", C.c_double),
+        ("aeif_tau_w", C.c_double),
+        ("aeif_a", C.c_double),
+        ("aeif_b", C.c_double),
+        ("aeif_V_spike", C.c_double),
     ]
 
 
 PRECISION_FP64, PRECISION_FP32 = 0, 1
 KERNEL_GAUSSIAN, KERNEL_GAMMA, KERNEL_LINEAR, KERNEL_WEIBULL = 0, 1, 2, 3
+MODEL_IZHIKEVICH, MODEL_POISSON, MODEL_FITZHUGH_NAGUMO, MODEL_AEIF = 0, 1, 2, 3
 KERNELS = {"gaussian": KERNEL_GAUSSIAN, "gamma": KERNEL_GAMMA, "linear": KERNEL_LINEAR, "weibull": KERNEL_WEIBULL}
 
 
@@ -273,7 +292,11 @@ def default_params(num_neurons: int, side: float) -> dict:
                 beta=0.001, tau_c=10000.0, target_calcium=0.7, initial_calcium=0.0,
                 growth_rate=(1e-4, 1e-4, 1e-4), min_calcium=(0.4, 0.1, 0.0), retract_ratio=(0.0, 0.0, 0.0),
                 conductance=3.0, noise_mean=5.0, noise_stddev=2.0, device=0, precision=PRECISION_FP64,
-                kernel_type=KERNEL_GAUSSIAN, kernel_k=1.0, kernel_scale=1.0, linear_cutoff=float("inf"))
+                kernel_type=KERNEL_GAUSSIAN, kernel_k=1.0, kernel_scale=1.0, linear_cutoff=float("inf"),
+                neuron_model=MODEL_IZHIKEVICH, poisson_refractory=4, poisson_x0=0.05, poisson_tau_x=5.0,
+                fhn_a=0.7, fhn_b=0.8, fhn_phi=0.08, fhn_init_x=-1.2, fhn_init_w=-0.6,
+                aeif_C=281.0, aeif_g_L=30.0, aeif_E_L=-70.6, aeif_V_T=-50.4, aeif_d_T=2.0, aeif_tau_w=144.0, aeif_a=4.0, aeif_b=0.0805,
+                aeif_V_spike=20.0)
 
 
 def make_config(params: dict) -> RlConfig:
@@ -585,12 +608,16 @@ class BarnesHut:
         return self.algorithm_type
 
 
-class IzhikevichModel:
-    """The ``izhikevich`` NeuronModel plugin with the calcium and growth updates
-    that Neurons runs after it every step."""
+class NeuronModel:
+    """A NeuronModel plugin (neurons/models/NeuronModelBase.h) with the calcium
+    and growth updates that Neurons runs after it every step; the model is the
+    network's ``neuron_model`` parameter."""
+
+    name = "izhikevich"
 
     def __init__(self, network: Network):
         self.net = network
+        self.name = {v: k for k, v in NEURON_MODELS.items()}[int(network.params.get("neuron_model", 0))]
 
     def update_electrical_activity(self, step: int):
         self.net.activity_block(step, 1)
@@ -600,6 +627,25 @@ class IzhikevichModel:
 
     def get_fired(self):
         return self.net.neurons()["fired"]
+
+    def get_model_type(self) -> str:
+        return self.name
+
+
+class IzhikevichModel(NeuronModel):
+    """--neuron-model izhikevich (models/izhikevich)."""
+
+
+class PoissonModel(NeuronModel):
+    """--neuron-model poisson (models/poisson); u holds the refractory steps left."""
+
+
+class FitzHughNagumoModel(NeuronModel):
+    """--neuron-model fitzhughnagumo (models/fitzhughnagumo); u holds w."""
+
+
+class AEIFModel(NeuronModel):
+    """--neuron-model aeif (models/aeif); u holds the adaptation w."""
 
 
 class Simulation:
@@ -612,10 +658,12 @@ class Simulation:
             raise RelearnError(6, f"algorithm {algorithm!r} is not built here (have {sorted(ALGORITHMS)})")
         if neuron_model not in NEURON_MODELS:
             raise RelearnError(6, f"neuron model {neuron_model!r} is not built here (have {sorted(NEURON_MODELS)})")
+        params = dict(params)
+        params["neuron_model"] = NEURON_MODELS[neuron_model]
         self.net = Network(params)
         self.net.set_positions(positions, signal)
         self.algorithm = BarnesHut(params, self.net)
-        self.model = IzhikevichModel(self.net)
+        self.model = {"izhikevich": IzhikevichModel, "poisson": PoissonModel, "fitzhughnagumo": FitzHughNagumoModel, "aeif": AEIFModel}[neuron_model](self.net)
         self.step = 1
 
     def simulate(self, number_steps: int):
@@ -626,5 +674,5 @@ class Simulation:
 
 from . import workloads  # noqa: E402  (re-export)
 
-__all__ = ["Network", "BarnesHut", "IzhikevichModel", "Simulation", "ConnectivityUpdateResult", "RelearnError", "default_params",
+__all__ = ["Network", "BarnesHut", "NeuronModel", "IzhikevichModel", "PoissonModel", "FitzHughNagumoModel", "AEIFModel", "Simulation", "ConnectivityUpdateResult", "RelearnError", "default_params",
            "make_config", "load_library", "workloads", "REQUEST_DTYPE", "SYNAPSE_DTYPE", "ABI_FUNCTIONS"]

@@ -45,6 +45,11 @@ struct ActArgs {
     double eta[3];
     const NetInfo* nets;
     const uint16_t* net_of;
+    // other neuron models (neurons/models/*)
+    double p_x0, p_tau_inv;  // Poisson
+    uint32_t p_refractory;
+    double f_a, f_b, f_phi;  // FitzHugh-Nagumo
+    double e_g_L, e_E_L, e_V_T, e_d_T, e_d_T_inv, e_tau_w_inv, e_C_inv, e_a, e_b, e_V_spike;  // AEIF
 };
 
 __device__ __forceinline__ double growth_curve(double current, double eta, double eps) {
@@ -60,8 +65,9 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
-// H > 0: h_model and h_calcium are both H, fixed at compile time.
-template <int H>
+// H > 0: h_model and h_calcium are both H, fixed at compile time.  MODEL is
+// the neuron model (RL_MODEL_*).
+template <int H, int MODEL>
 __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
     const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
@@ -95,17 +101,62 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
     double uv = A.u[i];
     uint8_t spiked = 0;
     const uint32_t hm = H > 0 ? (uint32_t)H : A.h_model;
+    if (MODEL == RL_MODEL_IZHIKEVICH) {
+        // IzhikevichModelCPU::update_activity (IzhikevichModelCPU.cpp:75-125)
 #pragma unroll
-    for (uint32_t it = 0; it < hm; ++it) {
-        const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
-        const double u_inc = (A.ab * xv) - (A.a * uv);
-        xv += x_inc * A.scale_m;
-        uv += u_inc * A.scale_m;
-        if (xv >= A.v_spike) {
-            xv = A.c;
-            uv += A.d;
-            spiked = 1;
-            break;
+        for (uint32_t it = 0; it < hm; ++it) {
+            const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
+            const double u_inc = (A.ab * xv) - (A.a * uv);
+            xv += x_inc * A.scale_m;
+            uv += u_inc * A.scale_m;
+            if (xv >= A.v_spike) {
+                xv = A.c;
+                uv += A.d;
+                spiked = 1;
+                break;
+            }
+        }
+    } else if (MODEL == RL_MODEL_POISSON) {
+        // PoissonModelCPU::update_activity (models/poisson/PoissonModelCPU.cpp):
+        // u holds the refractory steps left
+        for (uint32_t it = 0; it < hm; ++it) {
+            xv += ((A.p_x0 - xv) * A.p_tau_inv + input) * A.scale_m;
+        }
+        if (uv == 0.0) {
+            const double threshold = uniform01(draw(N.seed, step, i - N.first, 0u, STREAM_POISSON, 0u));
+            if (xv >= threshold) {
+                spiked = 1;
+                uv = (double)A.p_refractory;
+            }
+        } else {
+            uv -= 1.0;
+        }
+    } else if (MODEL == RL_MODEL_FITZHUGH_NAGUMO) {
+        // FitzHughNagumoModelCPU::update_activity (models/fitzhughnagumo/FitzHughNagumoModelCPU.cpp):
+        // no reset; the spike test follows the h substeps
+        const double third = 1.0 / 3.0;
+        for (uint32_t it = 0; it < hm; ++it) {
+            const double x_inc = xv - (xv * xv * xv * third) - uv + input;
+            const double w_inc = A.f_phi * (xv + A.f_a - A.f_b * uv);
+            xv += x_inc * A.scale_m;
+            uv += w_inc * A.scale_m;
+        }
+        spiked = (uv > xv - xv * xv * xv * third && xv > 1.0) ? 1 : 0;
+    } else {
+        // AEIFModelCPU::update_activity (models/aeif/AEIFModelCPU.cpp)
+        for (uint32_t it = 0; it < hm; ++it) {
+            const double linear_part = -A.e_g_L * (xv - A.e_E_L);
+            const double exp_part = A.e_g_L * A.e_d_T * rl_exp((xv - A.e_V_T) * A.e_d_T_inv);
+            const double x_inc = (linear_part + exp_part - uv + input) * A.e_C_inv;
+            const double w_inc = (A.e_a * (xv - A.e_E_L) - uv) * A.e_tau_w_inv;
+            xv += x_inc * A.scale_m;
+            uv += w_inc * A.scale_m;
+            if (xv >= A.e_V_spike) {
+                xv = A.e_E_L;
+                uv += A.e_b;
+                spiked = 1;
+                break;
+            }
         }
     }
     A.x[i] = xv;
@@ -143,11 +194,11 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
 // persistent shape) each thread strides over the neurons.
-template <int BLOCK, int H>
+template <int BLOCK, int H, int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        activity_neuron<H>(A, D, k, i);
+        activity_neuron<H, MODEL>(A, D, k, i);
     }
 }
 
@@ -249,17 +300,35 @@ void launch_vacant_axon_count(Ctx& c, unsigned long long* out) {
     RL_LAUNCH_CHECK();
 }
 
-template <int H>
-void launch_act64(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+template <int H, int MODEL>
+void launch_act64_m(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
     switch (v.block) {
         case 128:
-            k_activity<128, H><<<act_grid(c, v, (const void*)&k_activity<128, H>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            k_activity<128, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<128, H, MODEL>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
             break;
         case 512:
-            k_activity<512, H><<<act_grid(c, v, (const void*)&k_activity<512, H>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            k_activity<512, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<512, H, MODEL>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
             break;
         default:
-            k_activity<256, H><<<act_grid(c, v, (const void*)&k_activity<256, H>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            k_activity<256, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<256, H, MODEL>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            break;
+    }
+}
+
+template <int H>
+void launch_act64(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+    switch (c.cfg.neuron_model) {
+        case RL_MODEL_POISSON:
+            launch_act64_m<H, RL_MODEL_POISSON>(c, v, A, kstep);
+            break;
+        case RL_MODEL_FITZHUGH_NAGUMO:
+            launch_act64_m<H, RL_MODEL_FITZHUGH_NAGUMO>(c, v, A, kstep);
+            break;
+        case RL_MODEL_AEIF:
+            launch_act64_m<H, RL_MODEL_AEIF>(c, v, A, kstep);
+            break;
+        default:
+            launch_act64_m<H, RL_MODEL_IZHIKEVICH>(c, v, A, kstep);
             break;
     }
 }
@@ -301,6 +370,22 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
+    A.p_x0 = k.poisson_x0;
+    A.p_tau_inv = 1.0 / k.poisson_tau_x;
+    A.p_refractory = k.poisson_refractory;
+    A.f_a = k.fhn_a;
+    A.f_b = k.fhn_b;
+    A.f_phi = k.fhn_phi;
+    A.e_g_L = k.aeif_g_L;
+    A.e_E_L = k.aeif_E_L;
+    A.e_V_T = k.aeif_V_T;
+    A.e_d_T = k.aeif_d_T;
+    A.e_d_T_inv = 1.0 / k.aeif_d_T;
+    A.e_tau_w_inv = 1.0 / k.aeif_tau_w;
+    A.e_C_inv = 1.0 / k.aeif_C;
+    A.e_a = k.aeif_a;
+    A.e_b = k.aeif_b;
+    A.e_V_spike = k.aeif_V_spike;
     if (k.h_model == 10 && k.h_calcium == 10) {
         launch_act64<10>(c, v, A, kstep);
     } else {

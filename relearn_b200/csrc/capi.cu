@@ -133,6 +133,12 @@ void validate(const rl_config& k) {
     RL_CHECK(k.noise_stddev > 0.0, RL_ERR_INVALID, "noise_stddev must be positive");
     RL_CHECK(k.precision == RL_PRECISION_FP64 || k.precision == RL_PRECISION_FP32, RL_ERR_INVALID, "precision must be FP64 or FP32");
     RL_CHECK(k.kernel_type >= RL_KERNEL_GAUSSIAN && k.kernel_type <= RL_KERNEL_WEIBULL, RL_ERR_INVALID, "unknown kernel type");
+    RL_CHECK(k.neuron_model >= RL_MODEL_IZHIKEVICH && k.neuron_model <= RL_MODEL_AEIF, RL_ERR_INVALID, "unknown neuron model");
+    RL_CHECK(k.precision == RL_PRECISION_FP64 || k.neuron_model == RL_MODEL_IZHIKEVICH, RL_ERR_UNSUPPORTED,
+             "the FP32 form runs the Izhikevich model only");
+    RL_CHECK(k.neuron_model != RL_MODEL_POISSON || k.poisson_tau_x > 0.0, RL_ERR_INVALID, "Poisson tau_x must be positive");
+    RL_CHECK(k.neuron_model != RL_MODEL_AEIF || (k.aeif_C > 0.0 && k.aeif_d_T > 0.0 && k.aeif_tau_w > 0.0), RL_ERR_INVALID,
+             "AEIF C, d_T and tau_w must be positive");
     // GammaDistributionKernel / WeibullDistributionKernel / LinearDistributionKernel constructors
     RL_CHECK(k.kernel_type != RL_KERNEL_GAMMA || (k.kernel_k > 0.0 && k.kernel_scale > 0.0), RL_ERR_INVALID, "gamma k and theta must be positive");
     RL_CHECK(k.kernel_type != RL_KERNEL_WEIBULL || (k.kernel_k > 0.0 && k.kernel_scale > 0.0), RL_ERR_INVALID, "Weibull k and b must be positive");
@@ -288,9 +294,21 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     RL_CUDA_TRY(cudaMemsetAsync(N.update.p, 1, n, c.stream));
     RL_CUDA_TRY(cudaMemsetAsync(N.fired[0].p, 0, n, c.stream));
     RL_CUDA_TRY(cudaMemsetAsync(N.fired[1].p, 0, n, c.stream));
-    // IzhikevichModelBase::init_neurons (models/izhikevich/IzhikevichModelBase.cpp:59-66)
-    fill(N.x, n, k.iz_c, c.stream);
-    fill(N.u, n, 0.0, c.stream);
+    // initial x and second state variable per model: init_neurons of
+    // IzhikevichModelBase (models/izhikevich/IzhikevichModelBase.cpp:59-66),
+    // FitzHughNagumoModelBase and AEIFModelBase; NeuronModel::init and
+    // PoissonModelBase::init: x = 0, no refractory steps
+    double x0 = k.iz_c, u0 = 0.0;
+    if (k.neuron_model == RL_MODEL_POISSON) {
+        x0 = 0.0;
+    } else if (k.neuron_model == RL_MODEL_FITZHUGH_NAGUMO) {
+        x0 = k.fhn_init_x;
+        u0 = k.fhn_init_w;
+    } else if (k.neuron_model == RL_MODEL_AEIF) {
+        x0 = k.aeif_E_L;
+    }
+    fill(N.x, n, x0, c.stream);
+    fill(N.u, n, u0, c.stream);
     fill(N.calcium, n, k.initial_calcium, c.stream);
     fill(N.target, n, k.target_calcium, c.stream);
     fill(N.input, n, 0.0, c.stream);
@@ -524,6 +542,25 @@ void rl_config_default(rl_config* k, uint32_t num_neurons, double side) {
     k->kernel_k = 1.0;
     k->kernel_scale = 1.0;
     k->linear_cutoff = INFINITY;
+    // neurons/models/*/Parameters.h defaults
+    k->neuron_model = RL_MODEL_IZHIKEVICH;
+    k->poisson_refractory = 4;
+    k->poisson_x0 = 0.05;
+    k->poisson_tau_x = 5.0;
+    k->fhn_a = 0.7;
+    k->fhn_b = 0.8;
+    k->fhn_phi = 0.08;
+    k->fhn_init_x = -1.2;
+    k->fhn_init_w = -0.6;
+    k->aeif_C = 281.0;
+    k->aeif_g_L = 30.0;
+    k->aeif_E_L = -70.6;
+    k->aeif_V_T = -50.4;
+    k->aeif_d_T = 2.0;
+    k->aeif_tau_w = 144.0;
+    k->aeif_a = 4.0;
+    k->aeif_b = 0.0805;
+    k->aeif_V_spike = 20.0;
 }
 
 rl_status rl_ctx_create(const rl_config* cfg, void** out) {

@@ -94,6 +94,7 @@ enum Stream : uint32_t {
     STREAM_CONNECTOR = 2,  // connector shuffle key (per request)
     STREAM_NOISE = 3,      // normal background input (per neuron-step)
     STREAM_DELETION = 4,   // synapse deletion picks
+    STREAM_POISSON = 5,    // Poisson model spike thresholds (per neuron-step)
 };
 
 // Draw the four words keyed on (seed, step, neuron, sub, stream, depth).

@@ -101,7 +101,7 @@ int main(int argc, char** argv) {
     Parameters p = Parameters::defaults(3, 100.0);
     EXPECT(p.cfg.plasticity_interval == 100 && p.cfg.theta == 0.3 && p.cfg.sigma == 750.0);
     EXPECT(throws([&] { Simulation s(p, n.positions, n.signal_types, "naive"); }) == RL_ERR_UNSUPPORTED);
-    EXPECT(throws([&] { Simulation s(p, n.positions, n.signal_types, "barnes-hut", "poisson"); }) == RL_ERR_UNSUPPORTED);
+    EXPECT(throws([&] { Simulation s(p, n.positions, n.signal_types, "barnes-hut", "hodgkin-huxley"); }) == RL_ERR_UNSUPPORTED);
 
     // without a device the context cannot be created: the status comes back as an exception
     if (argc > 2 && std::string(argv[2]) == "--no-device") {

@@ -10,9 +10,10 @@
 //     returning a ConnectivityUpdateResult, get_algorithm_type; BarnesHut is the
 //     --algorithm barnes-hut implementation.
 //   * NeuronModel (neurons/models/NeuronModelBase.h): update_electrical_activity
-//     per step and the per-neuron getters; IzhikevichModel is --neuron-model
-//     izhikevich (with the calcium and synaptic-element updates Neurons drives
-//     every step, neurons/Neurons.cpp:351-384).
+//     per step and the per-neuron getters; ActivityModel runs the --neuron-model
+//     of the context (izhikevich, poisson, fitzhughnagumo, aeif) with the
+//     calcium and synaptic-element updates Neurons drives every step
+//     (neurons/Neurons.cpp:351-384).
 //   * Simulation::simulate (sim/Simulation.cpp:388-480): steps 1 .. number_steps + 1,
 //     plasticity every plasticity_update_step steps.
 //   * RelearnException::check / fail (util/RelearnException.h): every non-OK
@@ -55,7 +56,12 @@ private:
 enum class SignalType : uint8_t { Excitatory = RL_EXCITATORY, Inhibitory = RL_INHIBITORY };
 enum class ElementType : int { Axon = RL_AXON, DendriteExcitatory = RL_DENDRITE_EXC, DendriteInhibitory = RL_DENDRITE_INH };
 enum class AlgorithmEnum { BarnesHut };
-enum class NeuronModelEnum { Izhikevich };
+enum class NeuronModelEnum : int {
+    Izhikevich = RL_MODEL_IZHIKEVICH,
+    Poisson = RL_MODEL_POISSON,
+    FitzHughNagumo = RL_MODEL_FITZHUGH_NAGUMO,
+    AEIF = RL_MODEL_AEIF
+};
 
 using number_neurons_type = uint64_t;
 using counter_type = uint32_t;  // RelearnTypes::counter_type
@@ -245,10 +251,11 @@ public:
     [[nodiscard]] virtual NeuronModelEnum get_model_type() const = 0;
 };
 
-// --neuron-model izhikevich with the calcium and growth updates of each step.
-class IzhikevichModel final : public NeuronModel {
+// The --neuron-model chosen for the context (izhikevich, poisson,
+// fitzhughnagumo or aeif) with the calcium and growth updates of each step.
+class ActivityModel final : public NeuronModel {
 public:
-    explicit IzhikevichModel(Context& ctx) : ctx_(ctx) { }
+    ActivityModel(Context& ctx, NeuronModelEnum type) : ctx_(ctx), type_(type) { }
 
     void update_electrical_activity(step_type step) override {
         ctx_.check(rl_activity_block(ctx_.handle(), step, 1), "rl_activity_block");
@@ -263,7 +270,7 @@ public:
     std::vector<double> get_x() const override { return neurons().x; }
     std::vector<uint8_t> get_fired() const override { return neurons().fired; }
     std::vector<double> get_calcium() const { return neurons().calcium; }
-    NeuronModelEnum get_model_type() const override { return NeuronModelEnum::Izhikevich; }
+    NeuronModelEnum get_model_type() const override { return type_; }
 
     struct State {
         std::vector<double> x, u, calcium, input;
@@ -279,6 +286,7 @@ public:
 
 private:
     Context& ctx_;
+    NeuronModelEnum type_;
 };
 
 // Simulation::simulate on one GPU.
@@ -286,7 +294,8 @@ class Simulation {
 public:
     Simulation(const Parameters& params, std::span<const double> positions, std::span<const SignalType> signal_types,
                const std::string& algorithm = "barnes-hut", const std::string& neuron_model = "izhikevich")
-        : ctx_(checked(params, algorithm, neuron_model)), algorithm_(ctx_, positions, signal_types), model_(ctx_) {
+        : ctx_(checked(params, algorithm, neuron_model)), algorithm_(ctx_, positions, signal_types),
+          model_(ctx_, static_cast<NeuronModelEnum>(checked(params, algorithm, neuron_model).cfg.neuron_model)) {
         algorithm_.init(ctx_.size());
     }
 
@@ -332,23 +341,34 @@ public:
 
     Context& context() { return ctx_; }
     BarnesHut& algorithm() { return algorithm_; }
-    IzhikevichModel& neuron_model() { return model_; }
+    ActivityModel& neuron_model() { return model_; }
     step_type current_step() const { return step_; }
 
 private:
-    static const Parameters& checked(const Parameters& p, const std::string& algorithm, const std::string& neuron_model) {
+    // The parameters with the --neuron-model chosen by name (relearn.cpp:326-333).
+    static Parameters checked(const Parameters& p, const std::string& algorithm, const std::string& neuron_model) {
         if (algorithm != "barnes-hut") {
             throw RelearnException("algorithm '" + algorithm + "' is not built here (have barnes-hut)", RL_ERR_UNSUPPORTED);
         }
-        if (neuron_model != "izhikevich") {
-            throw RelearnException("neuron model '" + neuron_model + "' is not built here (have izhikevich)", RL_ERR_UNSUPPORTED);
+        Parameters q = p;
+        if (neuron_model == "izhikevich") {
+            q.cfg.neuron_model = RL_MODEL_IZHIKEVICH;
+        } else if (neuron_model == "poisson") {
+            q.cfg.neuron_model = RL_MODEL_POISSON;
+        } else if (neuron_model == "fitzhughnagumo") {
+            q.cfg.neuron_model = RL_MODEL_FITZHUGH_NAGUMO;
+        } else if (neuron_model == "aeif") {
+            q.cfg.neuron_model = RL_MODEL_AEIF;
+        } else {
+            throw RelearnException("neuron model '" + neuron_model + "' is not built here (have aeif, fitzhughnagumo, izhikevich, poisson)",
+                                   RL_ERR_UNSUPPORTED);
         }
-        return p;
+        return q;
     }
 
     Context ctx_;
     BarnesHut algorithm_;
-    IzhikevichModel model_;
+    ActivityModel model_;
     step_type step_ = 1;
 };
 

@@ -273,3 +273,38 @@ def test_search_requests_other_kernels(name, kernel):
     assert len(g) == len(o) > 0
     for k in ("target", "source", "j", "signal"):
         assert np.array_equal(g[k], o[k]), (name, k)
+
+
+@pytest.mark.parametrize("model", [1, 2, 3])
+def test_other_neuron_models(model):
+    """--neuron-model poisson / fitzhughnagumo / aeif (neurons/models/*) through
+    activity, plasticity and synapse formation, bit for bit against the oracle."""
+    from oracle import oracle as O
+    from relearn_b200 import Network
+
+    n = 2000
+    params, pos, sig = small_network(n, 1000.0, 61 + model)
+    params["neuron_model"] = model
+    if model == 3:
+        params["noise_mean"] = 600.0  # pA: enough drive for the AEIF neuron to spike
+        params["noise_stddev"] = 200.0
+    net = Network(params)
+    net.set_positions(pos, sig)
+    sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    seed_elements(net, n, 9, 0.0, 3.0)
+    seed_elements(sim, n, 9, 0.0, 3.0)
+    net.simulate(1, 1001)
+    sim.simulate(1, 1001)
+    compare_state(net, sim, n)
+    assert net.neurons()["fired"].sum() > 0 or model == 2
+    assert len(net.edges()[0]) > 0
+
+
+def test_fp32_form_runs_izhikevich_only():
+    from relearn_b200 import Network, RelearnError
+
+    params, _, _ = small_network(100, 200.0, 1)
+    params["precision"] = 1
+    params["neuron_model"] = 2
+    with pytest.raises(RelearnError):
+        Network(params)

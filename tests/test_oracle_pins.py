@@ -197,3 +197,75 @@ def test_hypot3_matches_libstdcxx_rule(oracle_mod):
         expect = a * math.sqrt((x / a) * (x / a) + (y / a) * (y / a) + (z / a) * (z / a))
         assert L.orc_hypot3(*map(float, v)) == expect
     assert L.orc_hypot3(0.0, 0.0, 0.0) == 0.0
+
+
+def _model_params(model, **kw):
+    from relearn_b200 import default_params
+
+    p = default_params(1, 1.0)
+    p["neuron_model"] = model
+    p.update(kw)
+    return p
+
+
+def test_aeif_formula(oracle_mod):
+    """AEIF update_activity against the formula of the reference's model test
+    (test/neuron_models_gpu/test_neuron_models_gpu.cpp:186-254): parameters
+    (C 281, g_L 30, E_L -70.6, V_T -50.4, d_T 2, tau_w 144, a 4, b 80.5,
+    V_spike -40), h = 10, a resting and a driven neuron."""
+    import math
+
+    prm = dict(aeif_C=281.0, aeif_g_L=30.0, aeif_E_L=-70.6, aeif_V_T=-50.4, aeif_d_T=2.0, aeif_tau_w=144.0, aeif_a=4.0, aeif_b=80.5,
+               aeif_V_spike=-40.0, h_model=10)
+    p = _model_params(3, **prm)
+    for x0, w0, inp in ((-70.6, 0.0, 0.0), (-60.0, 5.0, 200.0)):
+        x, w, fired = oracle_mod.model_step(p, x0, w0, inp)
+        # the test's reference formula, step by step
+        ex, ew, ef = x0, w0, False
+        for _ in range(10):
+            lin = -prm["aeif_g_L"] * (ex - prm["aeif_E_L"])
+            expp = prm["aeif_g_L"] * prm["aeif_d_T"] * math.exp((ex - prm["aeif_V_T"]) * (1.0 / prm["aeif_d_T"]))
+            xi = (lin + expp - ew + inp) * (1.0 / prm["aeif_C"])
+            wi = (prm["aeif_a"] * (ex - prm["aeif_E_L"]) - ew) * (1.0 / prm["aeif_tau_w"])
+            ex += xi * 0.1
+            ew += wi * 0.1
+            if ex >= prm["aeif_V_spike"]:
+                ex, ew, ef = prm["aeif_E_L"], ew + prm["aeif_b"], True
+                break
+        assert fired == ef
+        assert abs(x - ex) <= 1e-12 * max(1.0, abs(ex)) and abs(w - ew) <= 1e-12 * max(1.0, abs(ew))
+
+
+def test_fitzhugh_nagumo_formula(oracle_mod):
+    """FitzHugh-Nagumo update_activity of the CPU model
+    (models/fitzhughnagumo/FitzHughNagumoModelCPU.cpp: cubic term x^3 / 3, spike
+    test after the h substeps) with the parameters and inputs of the reference's
+    model test (test_neuron_models_gpu.cpp:256-310; that test's own formula
+    writes the cubic coefficient as 1/2, the CPU model uses 1/3)."""
+    p = _model_params(2, fhn_a=0.7, fhn_b=0.8, fhn_phi=0.08, h_model=10)
+    for x0, w0, inp in ((-1.2, -0.6, 0.0), (0.5, 0.2, 1.5), (1.8, -1.0, 2.0)):
+        x, w, fired = oracle_mod.model_step(p, x0, w0, inp)
+        ex, ew = x0, w0
+        for _ in range(10):
+            xi = ex - (ex * ex * ex * (1.0 / 3.0)) - ew + inp
+            wi = 0.08 * (ex + 0.7 - 0.8 * ew)
+            ex += xi * 0.1
+            ew += wi * 0.1
+        assert (x, w) == (ex, ew)
+        assert fired == (ew > ex - ex * ex * ex * (1.0 / 3.0) and ex > 1.0)
+
+
+def test_poisson_refractory_and_firing(oracle_mod):
+    """Poisson model contract of the reference's tests
+    (test_neuron_models_gpu.cpp:316-365): a refractory neuron never fires and
+    counts down; a potential far above any threshold in [0, 1) always fires and
+    starts the refractory period."""
+    p = _model_params(1, poisson_x0=0.0, poisson_tau_x=1000.0, poisson_refractory=5, h_model=1)
+    x, r, fired = oracle_mod.model_step(p, 1e6, 3.0, 0.0)
+    assert not fired and r == 2.0
+    for step in range(1, 50):
+        x, r, fired = oracle_mod.model_step(p, 1e6, 0.0, 0.0, step=step, neuron=step)
+        assert fired and r == 5.0
+    # below every threshold: never fires
+    x, r, fired = oracle_mod.model_step(p, -1.0, 0.0, 0.0)
+    assert not fired and r == 0.0
