@@ -337,6 +337,7 @@ typedef struct rl_tuning {
     int32_t search_warps;    /* 2, 4 or 8 */
     int32_t search_stack;    /* 24 or 48 (at least the octree depth + 2) */
     int32_t search_packet;   /* 32 or 16 */
+    int32_t search_cap;      /* 1: registers capped at 64 (more resident warps), 0: as compiled */
     int32_t act_block;       /* 128, 256 or 512 */
     int32_t act_persistent;  /* 0 or 1 */
     int32_t act_vec;         /* 1, 2 or 4 */
@@ -344,9 +345,9 @@ typedef struct rl_tuning {
 } rl_tuning;
 
 /* Candidates the tuner times, in the order of the times rl_get_tuning returns:
- * search: packet 32 then 16, stack 24 then 48, warps 2, 4, 8 (12 shapes);
+ * search: cap 0 then 1, packet 32 then 16, stack 24 then 48, warps 2, 4, 8 (24 shapes);
  * activity: persistent 0 then 1, block 128, 256, 512, vec 1, 2, 4 (18 shapes). */
-#define RL_NUM_SEARCH_SHAPES 12
+#define RL_NUM_SEARCH_SHAPES 24
 #define RL_NUM_ACT_SHAPES 18
 
 /* Autotuning: 0 keeps the current shapes; 1 times the candidates on the

@@ -269,8 +269,10 @@ __device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t pm
 
 // One warp handles 32 consecutive entries of the search list (Morton-adjacent
 // sources) as 32/PW packets of PW lanes.  WPB warps per block, SD stack frames.
-template <int WPB, int SD, int PW>
-__global__ void __launch_bounds__(WPB * 32) k_search(SearchArgs A) {
+// CAP = 1 caps the registers at 64 (a resident block count of 32 / WPB), for
+// more warps in flight at the price of a few spills.
+template <int WPB, int SD, int PW, int CAP>
+__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchArgs A) {
     constexpr int kPackets = 32 / PW;
     __shared__ uint32_t s_node[WPB][kPackets][SD];
     __shared__ uint32_t s_rem[WPB][kPackets][SD];
@@ -419,18 +421,16 @@ __global__ void __launch_bounds__(WPB * 32) k_search(SearchArgs A) {
 using SearchKernel = void (*)(SearchArgs);
 
 // The search variants the tuner chooses from, indexed by SearchVariant.
-template <int WPB, int SD, int PW>
-constexpr SearchKernel search_kernel() {
-    return &k_search<WPB, SD, PW>;
-}
 
 SearchKernel fp64_search_kernel(const SearchVariant& v) {
-#define RL_SV(w, s, p)                                  \
-    if (v.warps == w && v.stack == s && v.packet == p) { \
-        return search_kernel<w, s, p>();                 \
+#define RL_SV(w, s, p, c)                                                 \
+    if (v.warps == w && v.stack == s && v.packet == p && v.cap == c) {    \
+        return &k_search<w, s, p, c>;                                    \
     }
-    RL_SV(2, 24, 32) RL_SV(4, 24, 32) RL_SV(8, 24, 32) RL_SV(2, 48, 32) RL_SV(4, 48, 32) RL_SV(8, 48, 32)
-    RL_SV(2, 24, 16) RL_SV(4, 24, 16) RL_SV(8, 24, 16) RL_SV(2, 48, 16) RL_SV(4, 48, 16) RL_SV(8, 48, 16)
+#define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
+    RL_SV2(2, 24, 32) RL_SV2(4, 24, 32) RL_SV2(8, 24, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
+    RL_SV2(2, 24, 16) RL_SV2(4, 24, 16) RL_SV2(8, 24, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+#undef RL_SV2
 #undef RL_SV
     return nullptr;
 }
@@ -568,10 +568,12 @@ void tune_search(Ctx& c, F&& launch_all) {
 const std::vector<SearchVariant>& search_variants() {
     static const std::vector<SearchVariant> v = [] {
         std::vector<SearchVariant> out;
-        for (int p : { 32, 16 }) {
-            for (int s : { 24, 48 }) {
-                for (int w : { 2, 4, 8 }) {
-                    out.push_back(SearchVariant{ w, s, p });
+        for (int cap : { 0, 1 }) {
+            for (int p : { 32, 16 }) {
+                for (int s : { 24, 48 }) {
+                    for (int w : { 2, 4, 8 }) {
+                        out.push_back(SearchVariant{ w, s, p, cap });
+                    }
                 }
             }
         }

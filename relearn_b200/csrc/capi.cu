@@ -1028,6 +1028,7 @@ rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_
         out->search_warps = c.tune.search.warps;
         out->search_stack = c.tune.search.stack;
         out->search_packet = c.tune.search.packet;
+        out->search_cap = c.tune.search.cap;
         out->act_block = c.tune.act.block;
         out->act_persistent = c.tune.act.persistent;
         out->act_vec = c.tune.act.vec;
@@ -1053,7 +1054,7 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
         RL_CHECK(t != nullptr, RL_ERR_INVALID, "null tuning");
         bool s_ok = false, a_ok = false;
         for (const auto& v : rl::search_variants()) {
-            s_ok = s_ok || (v.warps == t->search_warps && v.stack == t->search_stack && v.packet == t->search_packet);
+            s_ok = s_ok || (v.warps == t->search_warps && v.stack == t->search_stack && v.packet == t->search_packet && v.cap == t->search_cap);
         }
         for (const auto& v : rl::act_variants()) {
             a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent && v.vec == t->act_vec);
@@ -1061,7 +1062,7 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
         RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
         RL_CHECK(rl::is_fp32(c) || t->act_vec == 1, RL_ERR_INVALID, "the FP64 activity kernel runs one neuron per thread");
         RL_CHECK(!c.positions_set || (uint32_t)t->search_stack >= c.tree.max_level + 2, RL_ERR_INVALID, "search stack shallower than the octree");
-        c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet };
+        c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet, t->search_cap };
         c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent, t->act_vec };
         c.tune.search_state = rl::TUNE_OFF;
         c.tune.act_state = rl::TUNE_OFF;

@@ -633,8 +633,8 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_
     return sum;
 }
 
-template <int WPB, int SD, int PW>
-__global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
+template <int WPB, int SD, int PW, int CAP>
+__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Search32 A) {
     constexpr int kPackets = 32 / PW;
     __shared__ uint32_t s_node[WPB][kPackets][SD];
     __shared__ uint32_t s_rem[WPB][kPackets][SD];
@@ -758,12 +758,14 @@ __global__ void __launch_bounds__(WPB * 32) k_search_f32(Search32 A) {
 using Search32Kernel = void (*)(Search32);
 
 Search32Kernel fp32_search_kernel(const SearchVariant& v) {
-#define RL_SV(w, s, p)                                  \
-    if (v.warps == w && v.stack == s && v.packet == p) { \
-        return &k_search_f32<w, s, p>;                   \
+#define RL_SV(w, s, p, c)                                                 \
+    if (v.warps == w && v.stack == s && v.packet == p && v.cap == c) {    \
+        return &k_search_f32<w, s, p, c>;                                    \
     }
-    RL_SV(2, 24, 32) RL_SV(4, 24, 32) RL_SV(8, 24, 32) RL_SV(2, 48, 32) RL_SV(4, 48, 32) RL_SV(8, 48, 32)
-    RL_SV(2, 24, 16) RL_SV(4, 24, 16) RL_SV(8, 24, 16) RL_SV(2, 48, 16) RL_SV(4, 48, 16) RL_SV(8, 48, 16)
+#define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
+    RL_SV2(2, 24, 32) RL_SV2(4, 24, 32) RL_SV2(8, 24, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
+    RL_SV2(2, 24, 16) RL_SV2(4, 24, 16) RL_SV2(8, 24, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+#undef RL_SV2
 #undef RL_SV
     return nullptr;
 }

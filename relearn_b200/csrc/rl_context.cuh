@@ -222,6 +222,7 @@ struct SearchVariant {
     int warps = 4;    // warps per block
     int stack = 48;   // frames of the per-lane and per-packet stacks
     int packet = 32;  // lanes (sources) that walk the descent from the root together
+    int cap = 0;      // 1: registers capped at 64 for more resident warps
 };
 
 // Launch shape of the activity kernel.

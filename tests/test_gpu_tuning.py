@@ -30,17 +30,17 @@ def test_every_search_shape_finds_the_same_targets(precision):
     depth = net.tree_info()[1]
     ref = None
     tried = 0
-    for w, st, p in SEARCH_SHAPES:
+    for w, st, p, cp in SEARCH_SHAPES:
         if st < depth + 2:
             continue
-        net.set_tuning(search_warps=w, search_stack=st, search_packet=p)
+        net.set_tuning(search_warps=w, search_stack=st, search_packet=p, search_cap=cp)
         req = net.find_targets(100)
         if ref is None:
             ref = req
         else:
-            assert np.array_equal(req, ref), (w, st, p)
+            assert np.array_equal(req, ref), (w, st, p, cp)
         tried += 1
-    assert tried >= 6 and len(ref) > 0
+    assert tried >= 12 and len(ref) > 0
 
 
 @pytest.mark.parametrize("precision", [0, 1])
