@@ -353,8 +353,9 @@ typedef struct rl_tuning {
 /* Autotuning: 0 keeps the current shapes; 1 times the candidates on the
  * context's own data at the next activity block and the next search (a search
  * shape needs a stack of at least the octree depth + 2) and keeps the fastest,
- * reusing a result the process already has for the same precision, form and
- * size class (power of two of the neuron count); 2 times them again even then.
+ * reusing a result the process already has for the same precision, form, size
+ * class (power of two of the neuron count), neuron model and kernel; 2 times them
+ * again even then.
  * Timing runs the kernels on the current state and restores it, so results do
  * not depend on tuning. */
 RL_API rl_status rl_autotune(void* ctx, int mode);

@@ -400,15 +400,17 @@ void plasticity_update(Ctx& c, uint32_t step) {
 // ------------------------------------------------------------ tuning cache
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int>, SearchVariant> g_search_shapes;
-std::map<std::tuple<int, int, int>, ActVariant> g_act_shapes;
+using TuneKey = std::tuple<int, int, int, int, int>;
+std::map<TuneKey, SearchVariant> g_search_shapes;
+std::map<TuneKey, ActVariant> g_act_shapes;
 
-std::tuple<int, int, int> tune_key(const Ctx& c) {
+// precision, batched or not, power of two of the neuron count, neuron model, kernel
+TuneKey tune_key(const Ctx& c) {
     int lg = 0;
     while (lg < 40 && (1ull << (lg + 1)) <= (uint64_t)c.n) {
         ++lg;
     }
-    return std::make_tuple(c.cfg.precision, c.multi() ? 1 : 0, lg);
+    return std::make_tuple(c.cfg.precision, c.multi() ? 1 : 0, lg, c.cfg.neuron_model, c.cfg.kernel_type);
 }
 }  // namespace
 
