@@ -102,6 +102,24 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest of the ranks' values (device time of the timed region): the
+    job is as slow as its slowest replica.  NCCL on the GPU, gloo on the CPU."""
+    if world <= 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, units_per_rank: float, max_ms: float) -> float:
+    """Whole-job throughput of independent replicas: the units all ranks
+    processed over the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -168,12 +186,8 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     phases = net.phase_times()
     net.set_profiling(False)
     launches = net.stats()["gpu_launches"] - launches0
-    total_ms = float(sum(times))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * n * PERIOD * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(float(sum(times)), world, dev)
+    value = replica_value(world, n * PERIOD * args.steps, total_ms)
     act_ms, act_cnt = phases["activity_kernel"]
     edges = int(net.stats().get("synapses_created", 0))
     per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
@@ -384,10 +398,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     ms = e0.elapsed_time(e1)
     ph = ens.phase_times()
     ens.set_profiling(False)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, dev)
     act_ms, act_cnt = ph["activity_kernel"]
     tuning = ens.tuning()
     hbm, peak_kind = peaks()
