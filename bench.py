@@ -219,7 +219,7 @@ def apply_shapes(args, net, precision):
     profiler would pick shapes at random)."""
     if args.act_shape or args.search_shape:
         b, p, v = (int(x) for x in (args.act_shape or "256,0,1").split(","))
-        w, st, pk, cp = (int(x) for x in ((args.search_shape or "4,48,32") + ",0").split(",")[:4])
+        w, st, pk, cp = (int(x) for x in ((args.search_shape or "4,0,32") + ",1").split(",")[:4])
         net.set_tuning(search_warps=w, search_stack=st, search_packet=pk, search_cap=cp, act_block=b, act_persistent=p, act_vec=v if precision else 1)
     else:
         net.autotune(1)

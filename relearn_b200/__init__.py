@@ -134,7 +134,7 @@ class RlTuning(C.Structure):
 
 
 NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 24, 18
-SEARCH_SHAPES = [(w, s, p, c) for c in (0, 1) for p in (32, 16) for s in (24, 48) for w in (2, 4, 8)]  # (warps, stack, packet, cap), timing order
+SEARCH_SHAPES = [(w, s, p, c) for c in (0, 1) for p in (32, 16) for s in (0, 48) for w in (2, 4, 8)]  # (warps, stack (0: none), packet, cap), timing order
 ACT_SHAPES = [(b, p, v) for p in (0, 1) for b in (128, 256, 512) for v in (1, 2, 4)]  # (block, persistent, neurons per thread)
 
 
@@ -553,7 +553,7 @@ class Network:
         d["act_ms"] = {f"b{b}_v{v}_{'persistent' if p else 'grid'}": float(am[k]) for k, (b, p, v) in enumerate(ACT_SHAPES) if am[k] > 0}
         return d
 
-    def set_tuning(self, search_warps=4, search_stack=48, search_packet=32, act_block=256, act_persistent=0, act_vec=1, search_cap=0):
+    def set_tuning(self, search_warps=4, search_stack=0, search_packet=32, act_block=256, act_persistent=0, act_vec=1, search_cap=1):
         t = RlTuning(search_warps, search_stack, search_packet, search_cap, act_block, act_persistent, act_vec, 0)
         self._check(self.lib.rl_set_tuning(self.h, C.byref(t)))
 

@@ -41,6 +41,8 @@ struct SearchArgs {
     const double4* rec;  // records of the searched dendrite type
     const uint2* topo;
     const double* maxdim;
+    const uint4* meta;     // topo, escape link, FP32 cell length (k_meta)
+    uint32_t num_nodes;
     const double *px, *py, *pz;
     const uint32_t* list_src;
     const uint32_t* list_j;
@@ -267,16 +269,138 @@ __device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t pm
     return sum;
 }
 
+// Walks without a stack: the depth-first order is followed through the
+// escape links (after a node that is not expanded, the walk continues at
+// skip[node]; after an expanded node, at its last child), so a walk keeps one
+// node index instead of a stack of frames.  The order of visits, and with it
+// every sum, is that of the stack walks above.  Every walk visits a node at
+// most once; a walk that leaves the node range or runs longer than the node
+// count reports DERR_WALK instead of looping.
+__device__ __forceinline__ uint32_t last_child(uint2 t) {
+    return t.x + (uint32_t)__popc(topo_mask(t.y)) - 1u;
+}
+
+__device__ WalkResult lane_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r,
+                                   double sx, double sy, double sz, uint32_t source, bool fallback, bool& bad) {
+    WalkResult res{ start_sum, -1, 0, false };
+    const uint4 ms = __ldg(&A.meta[sub]);
+    const uint2 ts = make_uint2(ms.x, ms.y);
+    if (include_root) {
+        const double4 rr = ldg4(&A.rec[sub]);
+        const Eval e = evaluate(rr, ts, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
+        ++res.touched;
+        if (e.status == ST_ACCEPT) {
+            res.sum += e.w;
+            if (pick_mode && res.sum >= r) {
+                res.picked = (int32_t)sub;
+            }
+            return res;
+        }
+        if (e.status == ST_DISCARD) {
+            return res;
+        }
+    }
+    const uint32_t end = ms.z;
+    uint32_t node = last_child(ts);
+    for (uint32_t guard = 0; node != end; ++guard) {
+        if (node >= A.num_nodes || guard >= A.num_nodes) {
+            bad = true;
+            return res;
+        }
+        const double4 rr = ldg4(&A.rec[node]);
+        const uint4 mm = __ldg(&A.meta[node]);
+        const double md = __ldg(&A.maxdim[node]);
+        const uint2 tt = make_uint2(mm.x, mm.y);
+        const uint32_t sk = mm.z;
+        const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
+        ++res.touched;
+        if (e.status == ST_ACCEPT) {
+            res.sum += e.w;
+            if (pick_mode && res.sum >= r) {
+                res.picked = (int32_t)node;
+                return res;
+            }
+        }
+        node = e.status == ST_EXPAND ? last_child(tt) : sk;
+    }
+    return res;
+}
+
+// Packet walk without a stack.  A lane that does not expand a node the packet
+// expands sits out the node's subtree: it records the node's escape link and
+// joins again when the walk arrives there.  The root's children are visited
+// in descending octant order; the running sum before each is the lane's
+// checkpoint for that octant.
+__device__ double packet_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz, uint32_t source,
+                                 bool fallback, double* cp_lane, uint32_t& touched, bool& bad) {
+    const int lane = threadIdx.x & 31;
+    const bool me = (lanes >> lane) & 1u;
+    double sum = 0.0;
+    const uint2 root = __ldg(&A.topo[W.root]);
+    const uint32_t first = root.x;
+    const uint32_t nrc = (uint32_t)__popc(topo_mask(root.y));
+    uint32_t rc_left = topo_mask(root.y);  // root children not reached yet
+    uint32_t node = last_child(root);
+    bool act = me;
+    uint32_t resume = kNoNode;
+    for (uint32_t guard = 0; node != kNoNode; ++guard) {
+        if (node >= A.num_nodes || guard >= A.num_nodes) {
+            bad = true;
+            break;
+        }
+        if (!act && node == resume) {
+            act = true;
+            resume = kNoNode;
+        }
+        if (node - first < nrc) {
+            const int oct = 31 - __clz(rc_left);
+            rc_left &= ~(1u << oct);
+            if (me) {
+                cp_lane[oct * 32] = sum;  // running sum before the subtree of root child `oct`
+            }
+        }
+        const double4 rr = ldg4(&A.rec[node]);
+        const uint4 mm = __ldg(&A.meta[node]);
+        const double md = __ldg(&A.maxdim[node]);
+        const uint2 tt = make_uint2(mm.x, mm.y);
+        const uint32_t sk = mm.z;
+        int status = ST_DISCARD;
+        if (act) {
+            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
+            status = e.status;
+            ++touched;
+            if (e.status == ST_ACCEPT) {
+                sum += e.w;
+            }
+        }
+        const uint32_t expand = __ballot_sync(pm, status == ST_EXPAND);
+        if (expand) {
+            if (act && status != ST_EXPAND) {
+                act = false;
+                resume = sk;
+            }
+            node = last_child(tt);
+        } else {
+            node = sk;
+        }
+    }
+    __syncwarp(pm);
+    return sum;
+}
+
 // One warp handles 32 consecutive entries of the search list (Morton-adjacent
-// sources) as 32/PW packets of PW lanes.  WPB warps per block, SD stack frames.
+// sources) as 32/PW packets of PW lanes.  WPB warps per block; SD stack frames,
+// or walks without a stack for SD = 0.
 // CAP = 1 caps the registers at 64 (a resident block count of 32 / WPB), for
 // more warps in flight at the price of a few spills.
 template <int WPB, int SD, int PW, int CAP>
 __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchArgs A) {
     constexpr int kPackets = 32 / PW;
-    __shared__ uint32_t s_node[WPB][kPackets][SD];
-    __shared__ uint32_t s_rem[WPB][kPackets][SD];
-    __shared__ uint32_t s_act[WPB][kPackets][SD];
+    constexpr int kFrames = SD > 0 ? SD : 1;
+    constexpr uint32_t kDescents = SD > 0 ? (uint32_t)SD : (uint32_t)kMaxLevels + 2u;
+    __shared__ uint32_t s_node[WPB][kPackets][kFrames];
+    __shared__ uint32_t s_rem[WPB][kPackets][kFrames];
+    __shared__ uint32_t s_act[WPB][kPackets][kFrames];
     __shared__ double s_cp[WPB][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -315,19 +439,34 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     double* cp = &s_cp[wib][lane];
     uint32_t touched = 0;
     bool overflow = false;
+    bool bad = false;
     const uint32_t lanes = __ballot_sync(pm, active);
+    // the walks of this shape (SD = 0: without a stack)
+    auto packet = [&](uint32_t ls, bool fb, uint32_t& t) -> double {
+        if constexpr (SD == 0) {
+            return packet_walk_sl(A, W, pm, ls, sx, sy, sz, source, fb, cp, t, bad);
+        } else {
+            return packet_walk<SD>(A, W, pm, ls, sx, sy, sz, source, fb, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], t, overflow);
+        }
+    };
+    auto walk = [&](uint32_t sub, bool include_root, double start, bool pick_mode, double r, bool fb) -> WalkResult {
+        if constexpr (SD == 0) {
+            return lane_walk_sl(A, W, sub, include_root, start, pick_mode, r, sx, sy, sz, source, fb, bad);
+        } else {
+            return lane_walk<SD>(A, W, sub, include_root, start, pick_mode, r, sx, sy, sz, source, fb);
+        }
+    };
     int32_t result = -1;
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
         // ---- descent 0: packet walk over the whole tree
-        double total = packet_walk<SD>(A, W, pm, lanes, sx, sy, sz, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], touched, overflow);
+        double total = packet(lanes, false, touched);
         bool fallback = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total == 0.0);
         if (need_fb) {
             uint32_t t2 = 0;
-            const double fb =
-                packet_walk<SD>(A, W, pm, need_fb, sx, sy, sz, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], t2, overflow);
+            const double fb = packet(need_fb, true, t2);
             if ((need_fb >> lane) & 1u) {
                 total = fb;
                 fallback = true;
@@ -357,7 +496,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
                 done = true;
             } else {
                 const uint32_t c0 = child_index(root, cstar);
-                const WalkResult wr = lane_walk<SD>(A, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback);
+                const WalkResult wr = walk(c0, true, cp[cstar * 32], true, r, fallback);
                 overflow |= wr.overflow;
                 if (wr.picked < 0) {
                     atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
@@ -370,7 +509,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     }
     // ---- deeper descents, per lane
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > (uint32_t)SD) {
+        if (depth > kDescents) {
             overflow = true;  // a descent always moves one level down; cannot recur this often
             break;
         }
@@ -380,11 +519,11 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
             done = true;
             break;
         }
-        WalkResult s1 = lane_walk<SD>(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false);
+        WalkResult s1 = walk(sub, false, 0.0, false, 0.0, false);
         touched += s1.touched;
         bool fb = false;
         if (s1.sum == 0.0) {
-            s1 = lane_walk<SD>(A, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true);
+            s1 = walk(sub, false, 0.0, false, 0.0, true);
             fb = true;
         }
         overflow |= s1.overflow;
@@ -393,7 +532,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
             break;
         }
         const double r = pick_threshold(s1.sum, W.seed, A.step, source - W.first, j, depth);
-        const WalkResult s2 = lane_walk<SD>(A, W, sub, false, 0.0, true, r, sx, sy, sz, source, fb);
+        const WalkResult s2 = walk(sub, false, 0.0, true, r, fb);
         if (s2.picked < 0) {
             atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
             done = true;
@@ -403,6 +542,10 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     }
     if (overflow) {
         atomicOr(A.err, (uint32_t)DERR_STACK);
+        result = -1;
+    }
+    if (bad) {
+        atomicOr(A.err, (uint32_t)DERR_WALK);
         result = -1;
     }
     if (active) {
@@ -428,8 +571,8 @@ SearchKernel fp64_search_kernel(const SearchVariant& v) {
         return &k_search<w, s, p, c>;                                    \
     }
 #define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
-    RL_SV2(2, 24, 32) RL_SV2(4, 24, 32) RL_SV2(8, 24, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
-    RL_SV2(2, 24, 16) RL_SV2(4, 24, 16) RL_SV2(8, 24, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+    RL_SV2(2, 0, 32) RL_SV2(4, 0, 32) RL_SV2(8, 0, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
+    RL_SV2(2, 0, 16) RL_SV2(4, 0, 16) RL_SV2(8, 0, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;
@@ -542,7 +685,7 @@ void tune_search(Ctx& c, F&& launch_all) {
     float best = 1e30f;
     SearchVariant pick = c.tune.search;
     for (const SearchVariant& v : search_variants()) {
-        if ((uint32_t)v.stack < c.tree.max_level + 2) {
+        if (!stack_fits(v, c.tree)) {
             continue;  // the stacks must hold a walk from the root to the deepest leaf
         }
         launch_all(v);
@@ -570,7 +713,7 @@ const std::vector<SearchVariant>& search_variants() {
         std::vector<SearchVariant> out;
         for (int cap : { 0, 1 }) {
             for (int p : { 32, 16 }) {
-                for (int s : { 24, 48 }) {
+                for (int s : { 0, 48 }) {
                     for (int w : { 2, 4, 8 }) {
                         out.push_back(SearchVariant{ w, s, p, cap });
                     }
@@ -681,6 +824,8 @@ void run_search(Ctx& c, uint32_t step) {
             A.rec = c.tree.rec[t].p;
             A.topo = c.tree.topo.p;
             A.maxdim = c.tree.maxdim.p;
+            A.meta = c.tree.meta.p;
+            A.num_nodes = c.tree.num_nodes;
             A.px = c.nr.px.p;
             A.py = c.nr.py.p;
             A.pz = c.nr.pz.p;

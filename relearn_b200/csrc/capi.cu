@@ -82,6 +82,9 @@ void check_device_error(Ctx& c, const char* phase) {
         msg += " [traversal stack overflow]";
         st = RL_ERR_OVERFLOW;
     }
+    if (h & DERR_WALK) {
+        msg += " [octree walk left the node range]";
+    }
     if (h & DERR_NO_CROSSING) {
         msg += " [pick found no crossing]";
     }
@@ -422,7 +425,7 @@ void remember_search_tuning(const Ctx& c) {
 bool recall_search_tuning(Ctx& c) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_search_shapes.find(tune_key(c));
-    if (it == g_search_shapes.end() || (uint32_t)it->second.stack < c.tree.max_level + 2) {
+    if (it == g_search_shapes.end() || !stack_fits(it->second, c.tree)) {
         return false;
     }
     c.tune.search = it->second;
@@ -1039,7 +1042,7 @@ rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_
         if (search_ms) {
             size_t k = 0;
             for (size_t v = 0; v < rl::search_variants().size(); ++v) {
-                const bool fits = (uint32_t)rl::search_variants()[v].stack >= c.tree.max_level + 2;
+                const bool fits = rl::stack_fits(rl::search_variants()[v], c.tree);
                 search_ms[v] = fits && k < c.tune.search_ms.size() ? c.tune.search_ms[k++] : 0.0f;
             }
         }
@@ -1063,7 +1066,8 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
         }
         RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
         RL_CHECK(rl::is_fp32(c) || t->act_vec == 1, RL_ERR_INVALID, "the FP64 activity kernel runs one neuron per thread");
-        RL_CHECK(!c.positions_set || (uint32_t)t->search_stack >= c.tree.max_level + 2, RL_ERR_INVALID, "search stack shallower than the octree");
+        RL_CHECK(!c.positions_set || rl::stack_fits(rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet, t->search_cap }, c.tree),
+                 RL_ERR_INVALID, "search stack shallower than the octree");
         c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet, t->search_cap };
         c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent, t->act_vec };
         c.tune.search_state = rl::TUNE_OFF;

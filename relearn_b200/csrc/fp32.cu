@@ -374,7 +374,7 @@ __global__ void k_commit_f32(uint32_t n, const uint8_t* __restrict__ enabled, do
 // FP64 records -> fixed-point records (in the frame of the node's network,
 // found through the first neuron under the node) and FP32 cell lengths.
 __global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4* __restrict__ r1, const double* __restrict__ md, uint4* __restrict__ o0,
-                       uint4* __restrict__ o1, float* __restrict__ omd, const uint32_t* __restrict__ first_key, const uint32_t* __restrict__ morton,
+                       uint4* __restrict__ o1, const uint32_t* __restrict__ first_key, const uint32_t* __restrict__ morton,
                        const uint16_t* __restrict__ net_of, const NetInfo* __restrict__ nets) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) {
@@ -383,7 +383,6 @@ __global__ void k_pack(uint32_t m, const double4* __restrict__ r0, const double4
     const QFrame& f = nets[net_of[morton[first_key[i]]]].frame;
     o0[i] = quantize_record(r0[i], f);
     o1[i] = quantize_record(r1[i], f);
-    omd[i] = (float)md[i];
 }
 
 // ----------------------------------------------------------- search
@@ -415,8 +414,8 @@ __device__ __forceinline__ float kernel_prob32(const Kernel32& K, float d) {
 
 struct Search32 {
     const uint4* rec;
-    const uint2* topo;
-    const float* maxdim;
+    const uint4* meta;  // topo, escape link, FP32 cell length (k_meta)
+    uint32_t num_nodes;
     const double *px, *py, *pz;
     const uint32_t* list_src;
     const uint32_t* list_j;
@@ -458,6 +457,22 @@ struct E32 {
     float w;
 };
 
+// A node's topology and FP32 cell length from its meta entry.
+__device__ __forceinline__ uint2 mtopo(const uint4& m) {
+    return make_uint2(m.x, m.y);
+}
+__device__ __forceinline__ float mmaxdim(const uint4& m) {
+    return __uint_as_float(m.w);
+}
+
+// Euclidean length in FP32 as d2 * rsqrt(d2) (MUFU.RSQ, relative error below
+// 2e-7); 0 for a zero vector.  The precision form's error budget (1e-5 on
+// selection probabilities) leaves room for it.
+__device__ __forceinline__ float dist32(float dx, float dy, float dz) {
+    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    return d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;
+}
+
 // Source position in the fixed-point frame.
 struct QPos {
     uint32_t x, y, z;
@@ -475,7 +490,7 @@ __device__ __forceinline__ E32 eval32(const uint4& r, uint2 t, float md, const Q
     }
     const float q = W.quantum;
     const float dx = qdiff(r.x, s.x, q), dy = qdiff(r.y, s.y, q), dz = qdiff(r.z, s.z, q);
-    const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    const float d = dist32(dx, dy, dz);
     if (d == 0.0f) {
         return e;
     }
@@ -523,7 +538,8 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
     uint32_t fnode[SD];
     uint32_t frem[SD];
     if (include_root) {
-        const E32 e = eval32(A.rec[sub], A.topo[sub], A.maxdim[sub], sp, source, A, W, fb);
+        const uint4 ms = A.meta[sub];
+        const E32 e = eval32(A.rec[sub], mtopo(ms), mmaxdim(ms), sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -536,7 +552,7 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
         }
     }
     fnode[0] = sub;
-    frem[0] = topo_mask(A.topo[sub].y);
+    frem[0] = A.meta[sub].y & 0xFFu;
     int depth = 1;
     while (depth > 0) {
         const int top = depth - 1;
@@ -547,9 +563,10 @@ __device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, b
         }
         const int oct = 31 - __clz(rem);
         frem[top] = rem & ~(1u << oct);
-        const uint32_t child = child_of(A.topo[fnode[top]], oct);
-        const uint2 tt = A.topo[child];
-        const E32 e = eval32(A.rec[child], tt, A.maxdim[child], sp, source, A, W, fb);
+        const uint32_t child = child_of(mtopo(A.meta[fnode[top]]), oct);
+        const uint4 mc = A.meta[child];
+        const uint2 tt = mtopo(mc);
+        const E32 e = eval32(A.rec[child], tt, mmaxdim(mc), sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -579,7 +596,7 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_
     KSum sum{ 0.0f, 0.0f };
     if (leader) {
         s_node[0] = W.root;
-        s_rem[0] = topo_mask(A.topo[W.root].y);
+        s_rem[0] = topo_mask(A.meta[W.root].y);
         s_act[0] = lanes;
     }
     __syncwarp(pm);
@@ -601,10 +618,11 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_
         if (depth == 1 && me) {
             cp[oct * 32] = make_float2(sum.s, sum.c);
         }
-        const uint32_t child = child_of(A.topo[node], oct);
+        const uint32_t child = child_of(mtopo(A.meta[node]), oct);
         const uint4 rr = A.rec[child];
-        const uint2 tt = A.topo[child];
-        const float md = A.maxdim[child];
+        const uint4 mc = A.meta[child];
+        const uint2 tt = mtopo(mc);
+        const float md = mmaxdim(mc);
         int status = S_DISCARD;
         if ((act >> lane) & 1u) {
             const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
@@ -633,12 +651,119 @@ __device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_
     return sum;
 }
 
+// Walks without a stack through the escape links (see the FP64 search): the
+// same visiting order as the stack walks above.
+__device__ __forceinline__ uint32_t last_child32(uint2 t) {
+    return t.x + (uint32_t)__popc(topo_mask(t.y)) - 1u;
+}
+
+__device__ Walk32 lane_walk32_sl(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, const QPos& sp,
+                                 uint32_t source, bool fb, bool& bad) {
+    Walk32 res{ start, -1, false };
+    const uint4 ms = A.meta[sub];
+    const uint2 ts = mtopo(ms);
+    if (include_root) {
+        const E32 e = eval32(A.rec[sub], ts, mmaxdim(ms), sp, source, A, W, fb);
+        if (e.status == S_ACCEPT) {
+            res.sum.add(e.w);
+            if (pick && res.sum.s >= r) {
+                res.picked = (int32_t)sub;
+            }
+            return res;
+        }
+        if (e.status == S_DISCARD) {
+            return res;
+        }
+    }
+    const uint32_t end = ms.z;
+    uint32_t node = last_child32(ts);
+    for (uint32_t guard = 0; node != end; ++guard) {
+        if (node >= A.num_nodes || guard >= A.num_nodes) {
+            bad = true;
+            return res;
+        }
+        const uint4 rr = A.rec[node];
+        const uint4 mm = A.meta[node];
+        const uint2 tt = mtopo(mm);
+        const float md = mmaxdim(mm);
+        const uint32_t sk = mm.z;
+        const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
+        if (e.status == S_ACCEPT) {
+            res.sum.add(e.w);
+            if (pick && res.sum.s >= r) {
+                res.picked = (int32_t)node;
+                return res;
+            }
+        }
+        node = e.status == S_EXPAND ? last_child32(tt) : sk;
+    }
+    return res;
+}
+
+__device__ KSum packet32_sl(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb, float2* cp,
+                            bool& bad) {
+    const int lane = threadIdx.x & 31;
+    const bool me = (lanes >> lane) & 1u;
+    KSum sum{ 0.0f, 0.0f };
+    const uint2 root = mtopo(A.meta[W.root]);
+    const uint32_t first = root.x;
+    const uint32_t nrc = (uint32_t)__popc(topo_mask(root.y));
+    uint32_t rc_left = topo_mask(root.y);
+    uint32_t node = last_child32(root);
+    bool act = me;
+    uint32_t resume = kNoNode;
+    for (uint32_t guard = 0; node != kNoNode; ++guard) {
+        if (node >= A.num_nodes || guard >= A.num_nodes) {
+            bad = true;
+            break;
+        }
+        if (!act && node == resume) {
+            act = true;
+            resume = kNoNode;
+        }
+        if (node - first < nrc) {
+            const int oct = 31 - __clz(rc_left);
+            rc_left &= ~(1u << oct);
+            if (me) {
+                cp[oct * 32] = make_float2(sum.s, sum.c);
+            }
+        }
+        const uint4 rr = A.rec[node];
+        const uint4 mm = A.meta[node];
+        const uint2 tt = mtopo(mm);
+        const float md = mmaxdim(mm);
+        const uint32_t sk = mm.z;
+        int status = S_DISCARD;
+        if (act) {
+            const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
+            status = e.status;
+            if (e.status == S_ACCEPT) {
+                sum.add(e.w);
+            }
+        }
+        const uint32_t expand = __ballot_sync(pm, status == S_EXPAND);
+        if (expand) {
+            if (act && status != S_EXPAND) {
+                act = false;
+                resume = sk;
+            }
+            node = last_child32(tt);
+        } else {
+            node = sk;
+        }
+    }
+    __syncwarp(pm);
+    return sum;
+}
+
 template <int WPB, int SD, int PW, int CAP>
 __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Search32 A) {
     constexpr int kPackets = 32 / PW;
-    __shared__ uint32_t s_node[WPB][kPackets][SD];
-    __shared__ uint32_t s_rem[WPB][kPackets][SD];
-    __shared__ uint32_t s_act[WPB][kPackets][SD];
+    constexpr int kFrames = SD > 0 ? SD : 1;
+    constexpr uint32_t kDescents = SD > 0 ? (uint32_t)SD : (uint32_t)kMaxLevels + 2u;
+    __shared__ uint32_t s_node[WPB][kPackets][kFrames];
+    __shared__ uint32_t s_rem[WPB][kPackets][kFrames];
+    __shared__ uint32_t s_act[WPB][kPackets][kFrames];
     __shared__ float2 s_cp[WPB][8 * 32];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -675,16 +800,32 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
                            : QPos{ 0u, 0u, 0u };
     float2* cp = &s_cp[wib][lane];
     bool overflow = false;
+    bool bad = false;
     const uint32_t lanes = __ballot_sync(pm, active);
+    // the walks of this shape (SD = 0: without a stack)
+    auto packet = [&](uint32_t ls, bool f) -> KSum {
+        if constexpr (SD == 0) {
+            return packet32_sl(A, W, pm, ls, sp, source, f, cp, bad);
+        } else {
+            return packet32<SD>(A, W, pm, ls, sp, source, f, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+        }
+    };
+    auto walk = [&](uint32_t sub, bool include_root, KSum start, bool pick, float r, bool f) -> Walk32 {
+        if constexpr (SD == 0) {
+            return lane_walk32_sl(A, W, sub, include_root, start, pick, r, sp, source, f, bad);
+        } else {
+            return lane_walk32<SD>(A, W, sub, include_root, start, pick, r, sp, source, f);
+        }
+    };
     int32_t result = -1;
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
-        KSum total = packet32<SD>(A, W, pm, lanes, sp, source, false, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+        KSum total = packet(lanes, false);
         bool fb = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total.s == 0.0f);
         if (need_fb) {
-            const KSum t2 = packet32<SD>(A, W, pm, need_fb, sp, source, true, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
+            const KSum t2 = packet(need_fb, true);
             if ((need_fb >> lane) & 1u) {
                 total = t2;
                 fb = true;
@@ -693,7 +834,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
         done = done || total.s == 0.0f;
         if (!done) {
             const float r = threshold32(total.s, A, W, source, j, 0);
-            const uint2 root = A.topo[W.root];
+            const uint2 root = mtopo(A.meta[W.root]);
             const uint32_t mask = topo_mask(root.y);
             int cstar = -1;
             for (int oct = 7; oct >= 0; --oct) {
@@ -709,7 +850,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
                 done = true;
             } else {
                 const float2 c0 = cp[cstar * 32];
-                const Walk32 wr = lane_walk32<SD>(A, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sp, source, fb);
+                const Walk32 wr = walk(child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, fb);
                 overflow |= wr.overflow;
                 if (wr.picked < 0) {
                     done = true;  // rounding left the crossing past the last candidate: no pick
@@ -720,19 +861,19 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
         }
     }
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > (uint32_t)SD) {
+        if (depth > kDescents) {
             overflow = true;
             break;
         }
-        const uint2 st = A.topo[sub];
+        const uint2 st = mtopo(A.meta[sub]);
         if (topo_leaf(st.y)) {
             result = (int32_t)st.x;
             break;
         }
-        Walk32 s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, false);
+        Walk32 s1 = walk(sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, false);
         bool f = false;
         if (s1.sum.s == 0.0f) {
-            s1 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, true);
+            s1 = walk(sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, true);
             f = true;
         }
         overflow |= s1.overflow;
@@ -740,7 +881,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
             break;
         }
         const float r = threshold32(s1.sum.s, A, W, source, j, depth);
-        const Walk32 s2 = lane_walk32<SD>(A, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sp, source, f);
+        const Walk32 s2 = walk(sub, false, KSum{ 0.0f, 0.0f }, true, r, f);
         if (s2.picked < 0) {
             break;
         }
@@ -748,6 +889,10 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
     }
     if (overflow) {
         atomicOr(A.err, (uint32_t)DERR_STACK);
+        result = -1;
+    }
+    if (bad) {
+        atomicOr(A.err, (uint32_t)DERR_WALK);
         result = -1;
     }
     if (active) {
@@ -763,15 +908,15 @@ Search32Kernel fp32_search_kernel(const SearchVariant& v) {
         return &k_search_f32<w, s, p, c>;                                    \
     }
 #define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
-    RL_SV2(2, 24, 32) RL_SV2(4, 24, 32) RL_SV2(8, 24, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
-    RL_SV2(2, 24, 16) RL_SV2(4, 24, 16) RL_SV2(8, 24, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+    RL_SV2(2, 0, 32) RL_SV2(4, 0, 32) RL_SV2(8, 0, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
+    RL_SV2(2, 0, 16) RL_SV2(4, 0, 16) RL_SV2(8, 0, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;
 }
 
 // ----------------------------------------------------------- diagnostic
-__global__ void k_candidates(const double4* rec64, const uint4* recq, const uint2* topo, const double* md64, const float* md32, double sx, double sy,
+__global__ void k_candidates(const double4* rec64, const uint4* recq, const uint2* topo, const double* md64, const uint4* meta, double sx, double sy,
                              double sz, uint32_t source, uint32_t root, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
                              uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f, KernelParams K) {
     const Kernel32 K32{ K.type, K.cutoff_inf, (float)K.k_minus_1, (float)K.a, (float)K.b, (float)K.cutoff };
@@ -819,9 +964,9 @@ __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint
             const uint32_t cnt = r.w;
             if (cnt) {
                 const float dx = qdiff(r.x, sp.x, f.quantum), dy = qdiff(r.y, sp.y, f.quantum), dz = qdiff(r.z, sp.z, f.quantum);
-                const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                const float d = dist32(dx, dy, dz);
                 if (d != 0.0f) {
-                    if (!leaf && !(md32[child] < (float)theta * d)) {
+                    if (!leaf && !(mmaxdim(meta[child]) < (float)theta * d)) {
                         status = S_EXPAND;
                     } else {
                         status = S_ACCEPT;
@@ -1022,8 +1167,7 @@ void pack_tree_f32(Ctx& c) {
     const uint32_t m = T.num_nodes;
     T.recq[0].ensure(m);
     T.recq[1].ensure(m);
-    T.maxdim32.ensure(m);
-    k_pack<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, T.rec[0].p, T.rec[1].p, T.maxdim.p, T.recq[0].p, T.recq[1].p, T.maxdim32.p, T.first_key.p,
+    k_pack<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, T.rec[0].p, T.rec[1].p, T.maxdim.p, T.recq[0].p, T.recq[1].p, T.first_key.p,
                                                      T.morton.p, c.net_of.p, c.d_nets.p);
     RL_LAUNCH_CHECK();
     T.recq_valid = true;
@@ -1033,8 +1177,8 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
                        uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v) {
     Search32 A;
     A.rec = c.tree.recq[type].p;
-    A.topo = c.tree.topo.p;
-    A.maxdim = c.tree.maxdim32.p;
+    A.meta = c.tree.meta.p;
+    A.num_nodes = c.tree.num_nodes;
     A.px = c.nr.px.p;
     A.py = c.nr.py.p;
     A.pz = c.nr.pz.p;
@@ -1082,7 +1226,7 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
     dw.alloc(cap);
     dc.alloc(1);
     k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.recq[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
-                                        precision == RL_PRECISION_FP32 ? c.tree.maxdim32.p : nullptr, pos[0], pos[1], pos[2], source, net, precision,
+                                        c.tree.meta.p, pos[0], pos[1], pos[2], source, net, precision,
                                         N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame, c.kernel);
     RL_LAUNCH_CHECK();
     unsigned long long k = 0;

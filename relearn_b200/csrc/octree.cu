@@ -328,6 +328,41 @@ __global__ void k_child_mask(uint32_t m, const int32_t* __restrict__ parent, con
     atomicOr(&topo[p].y, 1u << d);
 }
 
+// Escape link of every node for walks without a stack.  The reference's walk
+// (BarnesHutBase::get_nodes_to_consider, BarnesHutBase.h:129-206) pushes the
+// children of an expanded node in octant order 0..7 onto a LIFO stack, so it
+// visits them 7..0; children are contiguous in octant order here, so after the
+// subtree of node v the walk continues at v - 1 unless v is its parent's first
+// child, in which case it continues wherever the parent's subtree is left.
+// kNoNode after the last node of a tree (the roots have no parent).  Written
+// into the node's meta entry with its topology and FP32 cell length.
+__global__ void k_meta(uint32_t m, const int32_t* __restrict__ parent, const uint2* __restrict__ topo, const double* __restrict__ maxdim,
+                       uint4* __restrict__ meta, uint32_t* __restrict__ err) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m) {
+        return;
+    }
+    uint32_t skip = kNoNode;
+    uint32_t v = b;
+    int up = 0;
+    for (; up <= kMaxLevels; ++up) {
+        const int32_t p = parent[v];
+        if (p < 0) {
+            break;
+        }
+        if (v != topo[p].x) {
+            skip = v - 1;
+            break;
+        }
+        v = (uint32_t)p;
+    }
+    if (up > kMaxLevels) {
+        atomicOr(err, (uint32_t)DERR_WALK);  // deeper than any octree built here
+    }
+    const uint2 t = topo[b];
+    meta[b] = make_uint4(t.x, t.y, skip, __float_as_uint((float)maxdim[b]));
+}
+
 // ------------------------------------------------------------ aggregation
 __global__ void k_leaf_counts(uint32_t n, const uint32_t* __restrict__ leaf_of, const uint8_t* __restrict__ enabled, const uint8_t* __restrict__ update,
                               const uint32_t* __restrict__ vac_exc, const uint32_t* __restrict__ vac_inh, double4* rec0, double4* rec1) {
@@ -643,6 +678,7 @@ void build_octree(Ctx& c, const double* h_xyz) {
         T.bmax[a].alloc(m);
     }
     T.parent.alloc(m);
+    T.meta.alloc(m);
     T.dirty.alloc(m);
     RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m, st));
     T.last_counts.alloc(n);
@@ -699,6 +735,8 @@ void build_octree(Ctx& c, const double* h_xyz) {
     k_parent_search<<<blocks_for(m, 256), 256, 0, st>>>(m, level_off.p, T.first_key.p, T.topo.p, T.parent.p);
     RL_LAUNCH_CHECK();
     k_child_mask<<<blocks_for(m, 256), 256, 0, st>>>(m, T.parent.p, T.first_key.p, k0s.p, idx.p, key1.p, T.topo.p);
+    RL_LAUNCH_CHECK();
+    k_meta<<<blocks_for(m, 256), 256, 0, st>>>(m, T.parent.p, T.topo.p, T.maxdim.p, T.meta.p, c.err.p);
     RL_LAUNCH_CHECK();
     // the roots: level 0 holds one node per network, in network order
     const size_t K = c.nets.size();

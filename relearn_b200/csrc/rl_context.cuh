@@ -13,6 +13,8 @@ constexpr int kMaxLevels = 2 * kLevelsPerWord;  // deepest leaf level + 1 repres
 __host__ __device__ __forceinline__ uint32_t topo_mask(uint32_t y) { return y & 0xFFu; }
 __host__ __device__ __forceinline__ bool topo_leaf(uint32_t y) { return (y >> 8) & 1u; }
 __host__ __device__ __forceinline__ uint32_t topo_level(uint32_t y) { return y >> 16; }
+// Escape link past the last node of a tree.
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;
 
 #if defined(__CUDACC__)
 // Read-only 32-byte record load through the non-coherent path.
@@ -31,6 +33,10 @@ struct Tree {
     uint32_t root_neuron = 0;
     DBuf<double4> rec[2];     // per dendrite type: centroid (x, y, z), w = count bits (low 32)
     DBuf<uint2> topo;         // x: first child (inner) or neuron id (leaf); y: see topo_*
+    // what a walk reads of a node besides its record, in one 16-byte load:
+    // topo.x, topo.y, the escape link (the node a depth-first walk visits after
+    // this node's subtree; kNoNode after the last) and maxdim as FP32 bits
+    DBuf<uint4> meta;
     DBuf<double> maxdim;      // BoundingBox::get_maximum_difference of the cell
     DBuf<double> bmin[3], bmax[3];
     DBuf<int32_t> parent;
@@ -52,9 +58,8 @@ struct Tree {
         }
     }
     ~Tree() { drop_graph(); }
-    // FP32 form: records (centroid, count bits in w) and cell lengths as FP32
+    // FP32 form: records (centroid, count bits in w); cell lengths are in meta
     DBuf<uint4> recq[2];  // centroid in fixed point (QFrame), w = count
-    DBuf<float> maxdim32;
 };
 
 struct Neurons {
@@ -220,9 +225,9 @@ struct ActDesc {
 // Launch shape of the Barnes-Hut search kernels.
 struct SearchVariant {
     int warps = 4;    // warps per block
-    int stack = 48;   // frames of the per-lane and per-packet stacks
+    int stack = 0;    // frames of the per-lane and per-packet stacks; 0 = walks without a stack
     int packet = 32;  // lanes (sources) that walk the descent from the root together
-    int cap = 0;      // 1: registers capped at 64 for more resident warps
+    int cap = 1;      // 1: registers capped at 64 for more resident warps
 };
 
 // Launch shape of the activity kernel.
@@ -246,6 +251,11 @@ struct Tuning {
 };
 
 const std::vector<SearchVariant>& search_variants();
+// A shape with a stack needs frames for a walk from the root to the deepest
+// leaf; stack 0 walks without a stack and fits every octree.
+inline bool stack_fits(const SearchVariant& v, const Tree& t) {
+    return v.stack == 0 || (uint32_t)v.stack >= t.max_level + 2;
+}
 const std::vector<ActVariant>& act_variants();
 
 struct Ctx {

@@ -75,6 +75,7 @@ enum DeviceError : uint32_t {
     DERR_CAPACITY = 1u << 4,        // a device buffer was too small
     DERR_CONNECT = 1u << 5,         // connector bookkeeping underflow
     DERR_TIMEOUT = 1u << 6,         // bounded wait ran out
+    DERR_WALK = 1u << 7,            // a walk left the node range or its bound
 };
 
 // ------------------------------------------------------------- device buffer
