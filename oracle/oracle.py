@@ -21,7 +21,7 @@ def build(force: bool = False) -> str:
     """Compile the oracle with g++ (no FMA contraction, OpenMP)."""
     stale = not os.path.exists(LIB_PATH) or any(os.path.getmtime(s) > os.path.getmtime(LIB_PATH) for s in SOURCES)
     if force or stale:
-        cmd = ["g++", "-O2", "-std=c++20", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-o", LIB_PATH, SOURCES[0]]
+        cmd = ["g++", "-O2", "-std=c++20", "-ffp-contract=off", "-mfma", "-fopenmp", "-fPIC", "-shared", "-o", LIB_PATH, SOURCES[0]]
         subprocess.run(cmd, check=True)
     return LIB_PATH
 

@@ -13,7 +13,10 @@
 //   * hypot of three arguments as libstdc++ evaluates it
 //     (Vec3.hpp:549-551 -> std::hypot(x, y, z)).
 //   * Wichura AS241 normal quantile for the background input.
-// Build with -ffp-contract=off: no multiply-add contraction.
+// Build with -ffp-contract=off: no multiply-add contraction.  The polynomials of
+// exp, log and the quantile use explicit std::fma (one rounding, as on the
+// device); the reference's own formulas never do.  Built with -mfma so that
+// std::fma is a single instruction.
 #pragma once
 
 #include <cmath>
@@ -105,7 +108,7 @@ inline double own_exp(double x) {
     const double ln2_hi = 0.6931467056274414;      // ln 2, low 32 mantissa bits cleared
     const double ln2_lo = 4.7493250390316726e-07;  // ln 2 - ln2_hi
     const double k = std::floor(x * 1.4426950408889634 + 0.5);
-    const double r = (x - k * ln2_hi) - k * ln2_lo;
+    const double r = std::fma(-k, ln2_lo, x - k * ln2_hi);
     // 1/n! for n = 13 .. 2
     static const double inv_fact[12] = { 1.6059043836821614599e-10, 2.0876756987868098979e-09, 2.5052108385441718775e-08,
                                          2.7557319223985890653e-07, 2.7557319223985890653e-06, 2.4801587301587301587e-05,
@@ -113,9 +116,9 @@ inline double own_exp(double x) {
                                          4.1666666666666666667e-02, 1.6666666666666666667e-01, 0.5 };
     double p = inv_fact[0];
     for (int i = 1; i < 12; ++i) {
-        p = p * r + inv_fact[i];
+        p = std::fma(p, r, inv_fact[i]);
     }
-    const double y = 1.0 + (r + (r * r) * p);
+    const double y = 1.0 + std::fma(r * r, p, r);
     return times_pow2(y, (int)k);
 }
 
@@ -132,13 +135,13 @@ inline double own_log(double x) {
     const double z = s * s;
     double R = 1.0 / 23.0;
     for (int d = 21; d >= 3; d -= 2) {
-        R = R * z + 1.0 / (double)d;
+        R = std::fma(R, z, 1.0 / (double)d);
     }
     R = R * z;
     const double two_s = 2.0 * s;
-    const double logm = two_s + two_s * R;
+    const double logm = std::fma(two_s, R, two_s);
     const double ed = (double)e;
-    return ed * 0.6931467056274414 + (logm + ed * 4.7493250390316726e-07);
+    return ed * 0.6931467056274414 + std::fma(ed, 4.7493250390316726e-07, logm);
 }
 
 // libstdc++ <cmath> three-argument hypot: a = max(|x|,|y|,|z|),
@@ -167,10 +170,10 @@ inline double as241(double p, Log lg) {
         double num = A[0];
         double den = B[0];
         for (int i = 1; i < 8; ++i) {
-            num = num * r + A[i];
+            num = std::fma(num, r, A[i]);
         }
         for (int i = 1; i < 8; ++i) {
-            den = den * r + B[i];
+            den = std::fma(den, r, B[i]);
         }
         return (num * q) / den;
     }
@@ -187,10 +190,10 @@ inline double as241(double p, Log lg) {
         num = C[0];
         den = D[0];
         for (int i = 1; i < 8; ++i) {
-            num = num * r + C[i];
+            num = std::fma(num, r, C[i]);
         }
         for (int i = 1; i < 8; ++i) {
-            den = den * r + D[i];
+            den = std::fma(den, r, D[i]);
         }
     } else {
         r = r - 5.0;
@@ -201,10 +204,10 @@ inline double as241(double p, Log lg) {
         num = E[0];
         den = F[0];
         for (int i = 1; i < 8; ++i) {
-            num = num * r + E[i];
+            num = std::fma(num, r, E[i]);
         }
         for (int i = 1; i < 8; ++i) {
-            den = den * r + F[i];
+            den = std::fma(den, r, F[i]);
         }
     }
     const double x = num / den;

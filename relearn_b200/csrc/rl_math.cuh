@@ -1,12 +1,14 @@
 // Shared arithmetic for the structural-plasticity hot path.
 //
 // Every function here is __host__ __device__ and uses only IEEE-754 binary64
-// additions, multiplications, divisions and square roots (each correctly
-// rounded on both sides) plus integer bit manipulation.  The translation units
-// that include this header are compiled without multiply-add contraction
-// (nvcc -fmad=false, g++ -ffp-contract=off), so host and device produce the
-// same bits for the same inputs.  That is what makes the FP64 path bit-exact
-// against the CPU oracle.
+// additions, multiplications, divisions, square roots and explicit fused
+// multiply-adds (each correctly rounded on both sides) plus integer bit
+// manipulation.  The translation units that include this header are compiled
+// without multiply-add contraction (nvcc -fmad=false, g++ -ffp-contract=off),
+// so host and device produce the same bits for the same inputs.  That is what
+// makes the FP64 path bit-exact against the CPU oracle.  The fused
+// multiply-adds are only in the functions written here (the polynomials of
+// exp, log and the normal quantile), never in the reference's own formulas.
 //
 // Contents
 //   * rl_philox4x32_10 : Philox4x32-10 counter-based generator (Salmon, Moraes,
@@ -123,6 +125,15 @@ RL_HD uint64_t bits64(const u32x4& r) {
     return ((uint64_t)r.x << 32) | (uint64_t)r.y;
 }
 
+// a * b + c with one rounding (fma on both sides).
+RL_HD double rl_fma(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return __builtin_fma(a, b, c);
+#endif
+}
+
 // -------------------------------------------------------------- exp / log
 // ln 2 split so that k * LN2_HI is exact for |k| < 2^20.
 #define RL_LN2_HI 0.6931467056274414
@@ -160,21 +171,21 @@ RL_HD double rl_exp(double x) {
         return 0.0;
     }
     const double kd = floor(x * RL_INV_LN2 + 0.5);
-    const double r = (x - kd * RL_LN2_HI) - kd * RL_LN2_LO;
-    // p = sum_{n=2..13} r^(n-2) / n!
-    double p = 1.6059043836821614599e-10;   // 1/13!
-    p = p * r + 2.0876756987868098979e-09;  // 1/12!
-    p = p * r + 2.5052108385441718775e-08;  // 1/11!
-    p = p * r + 2.7557319223985890653e-07;  // 1/10!
-    p = p * r + 2.7557319223985890653e-06;  // 1/9!
-    p = p * r + 2.4801587301587301587e-05;  // 1/8!
-    p = p * r + 1.9841269841269841270e-04;  // 1/7!
-    p = p * r + 1.3888888888888888889e-03;  // 1/6!
-    p = p * r + 8.3333333333333333333e-03;  // 1/5!
-    p = p * r + 4.1666666666666666667e-02;  // 1/4!
-    p = p * r + 1.6666666666666666667e-01;  // 1/3!
-    p = p * r + 0.5;                        // 1/2!
-    const double y = 1.0 + (r + (r * r) * p);
+    const double r = rl_fma(-kd, RL_LN2_LO, x - kd * RL_LN2_HI);  // kd * RL_LN2_HI is exact
+    // p = sum_{n=2..13} r^(n-2) / n!, Horner with fused multiply-adds
+    double p = 1.6059043836821614599e-10;           // 1/13!
+    p = rl_fma(p, r, 2.0876756987868098979e-09);    // 1/12!
+    p = rl_fma(p, r, 2.5052108385441718775e-08);    // 1/11!
+    p = rl_fma(p, r, 2.7557319223985890653e-07);    // 1/10!
+    p = rl_fma(p, r, 2.7557319223985890653e-06);    // 1/9!
+    p = rl_fma(p, r, 2.4801587301587301587e-05);    // 1/8!
+    p = rl_fma(p, r, 1.9841269841269841270e-04);    // 1/7!
+    p = rl_fma(p, r, 1.3888888888888888889e-03);    // 1/6!
+    p = rl_fma(p, r, 8.3333333333333333333e-03);    // 1/5!
+    p = rl_fma(p, r, 4.1666666666666666667e-02);    // 1/4!
+    p = rl_fma(p, r, 1.6666666666666666667e-01);    // 1/3!
+    p = rl_fma(p, r, 0.5);                          // 1/2!
+    const double y = 1.0 + rl_fma(r * r, p, r);
     return scale_pow2(y, (int)kd);
 }
 
@@ -192,21 +203,21 @@ RL_HD double rl_log(double x) {
     const double s = f / (2.0 + f);
     const double z = s * s;
     double R = 1.0 / 23.0;
-    R = R * z + 1.0 / 21.0;
-    R = R * z + 1.0 / 19.0;
-    R = R * z + 1.0 / 17.0;
-    R = R * z + 1.0 / 15.0;
-    R = R * z + 1.0 / 13.0;
-    R = R * z + 1.0 / 11.0;
-    R = R * z + 1.0 / 9.0;
-    R = R * z + 1.0 / 7.0;
-    R = R * z + 1.0 / 5.0;
-    R = R * z + 1.0 / 3.0;
+    R = rl_fma(R, z, 1.0 / 21.0);
+    R = rl_fma(R, z, 1.0 / 19.0);
+    R = rl_fma(R, z, 1.0 / 17.0);
+    R = rl_fma(R, z, 1.0 / 15.0);
+    R = rl_fma(R, z, 1.0 / 13.0);
+    R = rl_fma(R, z, 1.0 / 11.0);
+    R = rl_fma(R, z, 1.0 / 9.0);
+    R = rl_fma(R, z, 1.0 / 7.0);
+    R = rl_fma(R, z, 1.0 / 5.0);
+    R = rl_fma(R, z, 1.0 / 3.0);
     R = R * z;
     const double two_s = 2.0 * s;
-    const double logm = two_s + two_s * R;
+    const double logm = rl_fma(two_s, R, two_s);
     const double ed = (double)e;
-    return ed * RL_LN2_HI + (logm + ed * RL_LN2_LO);
+    return ed * RL_LN2_HI + rl_fma(ed, RL_LN2_LO, logm);
 }
 
 // ----------------------------------------------------------------- hypot3
@@ -293,21 +304,21 @@ RL_HD double normal_quantile(double p) {
     if (fabs(q) <= 0.425) {
         const double r = 0.180625 - q * q;
         double num = 2.5090809287301226727e+3;
-        num = num * r + 3.3430575583588128105e+4;
-        num = num * r + 6.7265770927008700853e+4;
-        num = num * r + 4.5921953931549871457e+4;
-        num = num * r + 1.3731693765509461125e+4;
-        num = num * r + 1.9715909503065514427e+3;
-        num = num * r + 1.3314166789178437745e+2;
-        num = num * r + 3.3871328727963666080e+0;
+        num = rl_fma(num, r, 3.3430575583588128105e+4);
+        num = rl_fma(num, r, 6.7265770927008700853e+4);
+        num = rl_fma(num, r, 4.5921953931549871457e+4);
+        num = rl_fma(num, r, 1.3731693765509461125e+4);
+        num = rl_fma(num, r, 1.9715909503065514427e+3);
+        num = rl_fma(num, r, 1.3314166789178437745e+2);
+        num = rl_fma(num, r, 3.3871328727963666080e+0);
         double den = 5.2264952788528545610e+3;
-        den = den * r + 2.8729085735721942674e+4;
-        den = den * r + 3.9307895800092710610e+4;
-        den = den * r + 2.1213794301586595867e+4;
-        den = den * r + 5.3941960214247511077e+3;
-        den = den * r + 6.8718700749205790830e+2;
-        den = den * r + 4.2313330701600911252e+1;
-        den = den * r + 1.0;
+        den = rl_fma(den, r, 2.8729085735721942674e+4);
+        den = rl_fma(den, r, 3.9307895800092710610e+4);
+        den = rl_fma(den, r, 2.1213794301586595867e+4);
+        den = rl_fma(den, r, 5.3941960214247511077e+3);
+        den = rl_fma(den, r, 6.8718700749205790830e+2);
+        den = rl_fma(den, r, 4.2313330701600911252e+1);
+        den = rl_fma(den, r, 1.0);
         return (num * q) / den;
     }
     double r = q < 0.0 ? p : 1.0 - p;
@@ -317,39 +328,39 @@ RL_HD double normal_quantile(double p) {
     if (r <= 5.0) {
         r = r - 1.6;
         num = 7.7454501427834140764e-4;
-        num = num * r + 2.2723844989269184583e-2;
-        num = num * r + 2.4178072517745061177e-1;
-        num = num * r + 1.2704582524523683826e+0;
-        num = num * r + 3.6478483247632046050e+0;
-        num = num * r + 5.7694972214606914055e+0;
-        num = num * r + 4.6303378461565452959e+0;
-        num = num * r + 1.4234371107496835773e+0;
+        num = rl_fma(num, r, 2.2723844989269184583e-2);
+        num = rl_fma(num, r, 2.4178072517745061177e-1);
+        num = rl_fma(num, r, 1.2704582524523683826e+0);
+        num = rl_fma(num, r, 3.6478483247632046050e+0);
+        num = rl_fma(num, r, 5.7694972214606914055e+0);
+        num = rl_fma(num, r, 4.6303378461565452959e+0);
+        num = rl_fma(num, r, 1.4234371107496835773e+0);
         den = 1.0507500716444168432e-9;
-        den = den * r + 5.4759380849953449460e-4;
-        den = den * r + 1.5198666563616457197e-2;
-        den = den * r + 1.4810397642748007459e-1;
-        den = den * r + 6.8976733498510000455e-1;
-        den = den * r + 1.6763848301838038494e+0;
-        den = den * r + 2.0531916266377588219e+0;
-        den = den * r + 1.0;
+        den = rl_fma(den, r, 5.4759380849953449460e-4);
+        den = rl_fma(den, r, 1.5198666563616457197e-2);
+        den = rl_fma(den, r, 1.4810397642748007459e-1);
+        den = rl_fma(den, r, 6.8976733498510000455e-1);
+        den = rl_fma(den, r, 1.6763848301838038494e+0);
+        den = rl_fma(den, r, 2.0531916266377588219e+0);
+        den = rl_fma(den, r, 1.0);
     } else {
         r = r - 5.0;
         num = 2.0103343992922881327e-7;
-        num = num * r + 2.7115555687434875782e-5;
-        num = num * r + 1.2426609473880784386e-3;
-        num = num * r + 2.6532189526576123093e-2;
-        num = num * r + 2.9656057182850489123e-1;
-        num = num * r + 1.7848265399172913358e+0;
-        num = num * r + 5.4637849111641143699e+0;
-        num = num * r + 6.6579046435011037772e+0;
+        num = rl_fma(num, r, 2.7115555687434875782e-5);
+        num = rl_fma(num, r, 1.2426609473880784386e-3);
+        num = rl_fma(num, r, 2.6532189526576123093e-2);
+        num = rl_fma(num, r, 2.9656057182850489123e-1);
+        num = rl_fma(num, r, 1.7848265399172913358e+0);
+        num = rl_fma(num, r, 5.4637849111641143699e+0);
+        num = rl_fma(num, r, 6.6579046435011037772e+0);
         den = 2.0442631033899397856e-15;
-        den = den * r + 1.4215117583164458887e-7;
-        den = den * r + 1.8463183175100546818e-5;
-        den = den * r + 7.8686913114561325910e-4;
-        den = den * r + 1.4875361290850614853e-2;
-        den = den * r + 1.3692988092273580531e-1;
-        den = den * r + 5.9983220655588793769e-1;
-        den = den * r + 1.0;
+        den = rl_fma(den, r, 1.4215117583164458887e-7);
+        den = rl_fma(den, r, 1.8463183175100546818e-5);
+        den = rl_fma(den, r, 7.8686913114561325910e-4);
+        den = rl_fma(den, r, 1.4875361290850614853e-2);
+        den = rl_fma(den, r, 1.3692988092273580531e-1);
+        den = rl_fma(den, r, 5.9983220655588793769e-1);
+        den = rl_fma(den, r, 1.0);
     }
     const double x = num / den;
     return q < 0.0 ? -x : x;
