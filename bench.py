@@ -55,17 +55,64 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    every 10 ms from a thread (the timed region of a short run lasts well under
+    a second), nvidia-smi every 200 ms where NVML is missing.  The NVML device is
+    the CUDA device's own, matched by UUID (NVML numbers every GPU of the host)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.01):
         self.device = device
+        self.period = period_s
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []  # (sm_mhz, sm_max_mhz, reason bits)
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            for k in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(k)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = u.decode() if isinstance(u, bytes) else u
+                if u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                    return pynvml, h
+        except Exception:
+            pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _loop(self, nv, h):
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), float(smax), int(get_reasons(h))))
+            except Exception:
+                return
+            if self.stop.wait(self.period):
+                return
 
     def __enter__(self):
+        import threading
+
+        self.stop = threading.Event()
+        try:
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -76,6 +123,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -84,6 +134,11 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
+        if self.rows:
+            sm = [r[0] for r in self.rows]
+            reasons = sorted({name for r in self.rows for bit, name in self.REASONS.items() if r[2] & bit})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons, "samples": len(self.rows),
+                    "source": "nvml, 10 ms"}
         rows = []
         try:
             for line in open(self.path):
@@ -99,7 +154,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def max_over_ranks(x: float, world: int, device) -> float:
@@ -580,9 +635,11 @@ def bh_snapshot(net, n, stream, step):
                              "timed_ms": t["search_ms"]}}
 
 
-def cpu_baseline(args, params, pos, sig, activity_steps=None, searches=20000):
+def cpu_baseline(args, params, pos, sig, activity_steps=1000, searches=100000):
     """The oracle (C++ restatement of the reference's CPU path, OpenMP) on all
-    host cores: a bounded sample of the same workload."""
+    host cores: a bounded sample of the same workload (1,000 activity steps with
+    their 10 plasticity updates, about 10 s on 16 cores, and 100,000 searches
+    of the search snapshot)."""
     from oracle import oracle as O
 
     threads = os.cpu_count() or 1
@@ -590,13 +647,13 @@ def cpu_baseline(args, params, pos, sig, activity_steps=None, searches=20000):
     p.pop("device", None)
     p["use_libm"] = 0
     sim = O.OracleSim(p, pos, sig, threads=threads)
-    steps = activity_steps or PERIOD
+    steps = activity_steps
     t0 = time.perf_counter()
-    sim.simulate(1, steps)  # includes the plasticity update at step 100
+    sim.simulate(1, steps)  # includes the plasticity updates at steps 100, 200, ...
     dt = time.perf_counter() - t0
     n = params["num_neurons"]
     out = {"value": n * steps / dt, "unit": "neuron-steps/s", "cores": threads, "kind": "port",
-           "sample": f"{n} neurons, {steps} activity steps incl. 1 plasticity update ({dt:.1f} s)"}
+           "sample": f"{n} neurons, {steps} activity steps incl. {steps // PERIOD} plasticity updates ({dt:.1f} s)"}
     # search snapshot on a subset of sources
     one = np.ones(n, np.uint32)
     sel = np.zeros(n, np.uint32)
