@@ -274,8 +274,8 @@ def apply_shapes(args, net, precision):
     profiler would pick shapes at random)."""
     if args.act_shape or args.search_shape:
         b, p, v = (int(x) for x in (args.act_shape or "256,0,1").split(","))
-        w, st, pk, cp = (int(x) for x in ((args.search_shape or "4,0,32") + ",1").split(",")[:4])
-        net.set_tuning(search_warps=w, search_stack=st, search_packet=pk, search_cap=cp, act_block=b, act_persistent=p, act_vec=v if precision else 1)
+        w, pk, cp, hot = (int(x) for x in ((args.search_shape or "2,32") + ",1,0").split(",")[:4])
+        net.set_tuning(search_warps=w, search_packet=pk, search_cap=cp, search_hot=hot, act_block=b, act_persistent=p, act_vec=v if precision else 1)
     else:
         net.autotune(1)
 
@@ -631,7 +631,7 @@ def bh_snapshot(net, n, stream, step):
     return {"metric": "BH searches/s", "value": searches / (min(search_ms) / 1e3), "unit": "searches/s",
             "with_tree_update_and_copies": searches / (min(update_ms) / 1e3), "searches_per_update": searches,
             "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron",
-            "search_shape": {"warps_per_block": t["search_warps"], "stack": t["search_stack"], "packet": t["search_packet"], "register_cap": t["search_cap"],
+            "search_shape": {"warps_per_block": t["search_warps"], "packet": t["search_packet"], "register_cap": t["search_cap"], "hot_nodes": t["search_hot"],
                              "timed_ms": t["search_ms"]}}
 
 
@@ -769,7 +769,7 @@ def main():
     ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
     ap.add_argument("--skip-serve", action="store_true", help="do not measure the serving form")
     ap.add_argument("--act-shape", default=None, help="activity launch shape 'block,persistent,vec' instead of the tuner's")
-    ap.add_argument("--search-shape", default=None, help="search launch shape 'warps,stack,packet[,cap]' instead of the tuner's")
+    ap.add_argument("--search-shape", default=None, help="search launch shape 'warps,packet[,cap[,hot]]' instead of the tuner's")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="length of the Poisson request stream (the full one is 600 s)")
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-steps", type=int, default=5000)

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RL_ABI_VERSION 2
+#define RL_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define RL_API __attribute__((visibility("default")))
@@ -326,17 +326,19 @@ RL_API rl_status rl_set_profiling(void* ctx, int enable);
  * last call (arrays of RL_NUM_PHASES entries); resets the accumulators. */
 RL_API rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts);
 
-/* Launch shapes of the hot kernels.  The search kernels walk the octree with
- * `search_warps` warps per block, `search_stack` frames per walk (0: walks
- * without a stack, through per-node escape links) and `search_packet` lanes
- * (sources) walking the descent from the root together;
+/* Launch shapes of the hot kernels.  The search kernels walk the octree
+ * without a stack (through per-node escape links) with `search_warps` warps per
+ * block and `search_packet` lanes (sources) walking the descent from the root
+ * together; `search_hot` > 0 selects the persistent form (one block of 32 warps
+ * per SM taking warp tasks from a counter) that first copies up to
+ * `search_hot` nodes of the top octree levels into shared memory;
  * the activity kernel runs `act_block` threads per block with `act_vec`
  * neurons per thread (vector loads and stores; the FP64 form runs 1), and with
  * `act_persistent` one resident wave of blocks strides over the neurons.  No
  * counterpart in the reference (its CPU loops have no launch shape). */
 typedef struct rl_tuning {
     int32_t search_warps;    /* 2, 4 or 8 */
-    int32_t search_stack;    /* 0 (no stack) or 48 (at least the octree depth + 2) */
+    int32_t search_hot;      /* 0, or 1024 / 4096 top octree nodes in shared memory (search_warps 32) */
     int32_t search_packet;   /* 32 or 16 */
     int32_t search_cap;      /* 1: registers capped at 64 (more resident warps), 0: as compiled */
     int32_t act_block;       /* 128, 256 or 512 */
@@ -346,14 +348,15 @@ typedef struct rl_tuning {
 } rl_tuning;
 
 /* Candidates the tuner times, in the order of the times rl_get_tuning returns:
- * search: cap 0 then 1, packet 32 then 16, stack 0 then 48, warps 2, 4, 8 (24 shapes);
+ * search: cap 0 then 1, packet 32 then 16, warps 2, 4, 8 (12 shapes), then the
+ * persistent form with 1024 and 4096 nodes in shared memory, packet 32 then 16
+ * (4 shapes, 32 warps, registers capped at 64);
  * activity: persistent 0 then 1, block 128, 256, 512, vec 1, 2, 4 (18 shapes). */
-#define RL_NUM_SEARCH_SHAPES 24
+#define RL_NUM_SEARCH_SHAPES 16
 #define RL_NUM_ACT_SHAPES 18
 
 /* Autotuning: 0 keeps the current shapes; 1 times the candidates on the
- * context's own data at the next activity block and the next search (a search
- * shape with a stack needs at least the octree depth + 2 frames) and keeps the fastest,
+ * context's own data at the next activity block and the next search and keeps the fastest,
  * reusing a result the process already has for the same precision, form, size
  * class (power of two of the neuron count), neuron model and kernel; 2 times them
  * again even then.

@@ -129,12 +129,14 @@ class RlStats(C.Structure):
 
 
 class RlTuning(C.Structure):
-    _fields_ = [(k, C.c_int32) for k in ("search_warps", "search_stack", "search_packet", "search_cap", "act_block", "act_persistent", "act_vec",
+    _fields_ = [(k, C.c_int32) for k in ("search_warps", "search_hot", "search_packet", "search_cap", "act_block", "act_persistent", "act_vec",
                                          "tuned")]
 
 
-NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 24, 18
-SEARCH_SHAPES = [(w, s, p, c) for c in (0, 1) for p in (32, 16) for s in (0, 48) for w in (2, 4, 8)]  # (warps, stack (0: none), packet, cap), timing order
+NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 16, 18
+# (warps, packet, cap, hot), timing order: plain shapes, then the persistent form
+# with the top octree nodes in shared memory
+SEARCH_SHAPES = [(w, p, c, 0) for c in (0, 1) for p in (32, 16) for w in (2, 4, 8)] + [(32, p, 1, h) for h in (1024, 4096) for p in (32, 16)]
 ACT_SHAPES = [(b, p, v) for p in (0, 1) for b in (128, 256, 512) for v in (1, 2, 4)]  # (block, persistent, neurons per thread)
 
 
@@ -549,12 +551,12 @@ class Network:
         am = (C.c_float * NUM_ACT_SHAPES)()
         self._check(self.lib.rl_get_tuning(self.h, C.byref(t), sm, am))
         d = {f: getattr(t, f) for f, _ in RlTuning._fields_}
-        d["search_ms"] = {f"w{w}_s{st}_p{p}_c{cp}": float(sm[k]) for k, (w, st, p, cp) in enumerate(SEARCH_SHAPES) if sm[k] > 0}
+        d["search_ms"] = {f"w{w}_p{p}_c{cp}" + (f"_hot{h}" if h else ""): float(sm[k]) for k, (w, p, cp, h) in enumerate(SEARCH_SHAPES) if sm[k] > 0}
         d["act_ms"] = {f"b{b}_v{v}_{'persistent' if p else 'grid'}": float(am[k]) for k, (b, p, v) in enumerate(ACT_SHAPES) if am[k] > 0}
         return d
 
-    def set_tuning(self, search_warps=4, search_stack=0, search_packet=32, act_block=256, act_persistent=0, act_vec=1, search_cap=1):
-        t = RlTuning(search_warps, search_stack, search_packet, search_cap, act_block, act_persistent, act_vec, 0)
+    def set_tuning(self, search_warps=2, search_packet=32, search_cap=1, search_hot=0, act_block=256, act_persistent=0, act_vec=1):
+        t = RlTuning(search_warps, search_hot, search_packet, search_cap, act_block, act_persistent, act_vec, 0)
         self._check(self.lib.rl_set_tuning(self.h, C.byref(t)))
 
     def memory(self) -> tuple:

@@ -19,15 +19,16 @@
 // Work split on the GPU:
 //   * The descent from the root (about 3,000 candidates per search at 1M
 //     neurons) runs as a warp packet: the 32 lanes are 32 searches whose
-//     sources are adjacent in Morton order; the warp walks one shared
-//     depth-first stack, a node is expanded when any lane expands it, and each
-//     lane evaluates and sums only the nodes it would visit itself.  Node
-//     records are loaded once per warp (broadcast).  The running sum at the
-//     start of every child subtree of the root is kept as a checkpoint, so the
-//     pick re-walks a single root-child subtree per lane instead of the whole
-//     candidate list.
+//     sources are adjacent in Morton order; the warp walks the tree once, a
+//     node is expanded when any lane expands it, and each lane evaluates and
+//     sums only the nodes it would visit itself.  Node records are loaded once
+//     per warp (broadcast).  The running sum at the start of every child
+//     subtree of the root is kept as a checkpoint, so the pick re-walks a
+//     single root-child subtree per lane instead of the whole candidate list.
 //   * Deeper descents (a handful of candidates) run per lane: a sum pass and a
 //     pick pass over the chosen node's subtree.
+//   * Walks carry no stack: they follow per-node escape links.
+//   * A persistent form keeps the top levels of the octree in shared memory.
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -39,9 +40,9 @@ enum : int { ST_DISCARD = 0, ST_EXPAND = 1, ST_ACCEPT = 2 };
 
 struct SearchArgs {
     const double4* rec;  // records of the searched dendrite type
-    const uint2* topo;
     const double* maxdim;
     const uint4* meta;     // topo, escape link, FP32 cell length (k_meta)
+    uint32_t* tasks;       // persistent form: warp tasks handed out so far
     uint32_t num_nodes;
     const double *px, *py, *pz;
     const uint32_t* list_src;
@@ -126,168 +127,59 @@ __device__ __forceinline__ double pick_threshold(double total, uint64_t seed, ui
     return r;
 }
 
-// Per-lane depth-first walk below `sub` (not evaluating `sub` itself when
-// `include_root` is false).  Mode 0 sums all weights; mode 1 stops at the first
-// candidate whose running sum reaches r and returns it.
-struct WalkResult {
-    double sum;
-    int32_t picked;  // node index in pick mode, -1 otherwise
-    uint32_t touched;
-    bool overflow;
+// The shared-memory copy of the first nodes of the node array (the top
+// levels of the octree, breadth-first) in the persistent form; n = 0 elsewhere.
+struct Hot64 {
+    const double4* rec;
+    const uint4* meta;
+    const double* maxdim;
+    uint32_t n;
 };
 
-template <int SD>
-__device__ WalkResult lane_walk(const SearchArgs& A, const WarpNet& W, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r,
-                                double sx, double sy, double sz, uint32_t source, bool fallback) {
-    WalkResult res{ start_sum, -1, 0, false };
-    uint32_t fnode[SD];
-    uint32_t frem[SD];
-    int depth = 0;
-    if (include_root) {
-        const double4 rr = ldg4(&A.rec[sub]);
-        const uint2 tt = __ldg(&A.topo[sub]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
-        ++res.touched;
-        if (e.status == ST_ACCEPT) {
-            res.sum += e.w;
-            if (pick_mode && res.sum >= r) {
-                res.picked = (int32_t)sub;
-            }
-            return res;
-        }
-        if (e.status == ST_DISCARD) {
-            return res;
-        }
+template <bool HOT>
+__device__ __forceinline__ void load_node(const SearchArgs& A, const Hot64& H, uint32_t i, double4& r, uint4& m, double& md) {
+    if (HOT && i < H.n) {
+        r = H.rec[i];
+        m = H.meta[i];
+        md = H.maxdim[i];
+    } else {
+        r = ldg4(&A.rec[i]);
+        m = __ldg(&A.meta[i]);
+        md = __ldg(&A.maxdim[i]);
     }
-    {
-        const uint2 tt = __ldg(&A.topo[sub]);
-        fnode[0] = sub;
-        frem[0] = topo_mask(tt.y);
-        depth = 1;
-    }
-    while (depth > 0) {
-        const int top = depth - 1;
-        const uint32_t rem = frem[top];
-        if (rem == 0) {
-            --depth;
-            continue;
-        }
-        const int oct = 31 - __clz(rem);
-        frem[top] = rem & ~(1u << oct);
-        const uint2 pt = __ldg(&A.topo[fnode[top]]);
-        const uint32_t child = child_index(pt, oct);
-        const double4 rr = ldg4(&A.rec[child]);
-        const uint2 tt = __ldg(&A.topo[child]);
-        const Eval e = evaluate(rr, tt, __ldg(&A.maxdim[child]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
-        ++res.touched;
-        if (e.status == ST_ACCEPT) {
-            res.sum += e.w;
-            if (pick_mode && res.sum >= r) {
-                res.picked = (int32_t)child;
-                return res;
-            }
-        } else if (e.status == ST_EXPAND) {
-            if (depth >= SD) {
-                res.overflow = true;
-                return res;
-            }
-            fnode[depth] = child;
-            frem[depth] = topo_mask(tt.y);
-            ++depth;
-        }
-    }
-    return res;
 }
 
-// Packet walk over the whole tree: the lanes of packet mask `pm` (a warp or
-// an aligned part of it) walk one shared depth-first stack; `lanes` are the
-// packet's active lanes.  Each lane returns its sequential sum and the running
-// sum before every root child.
-template <int SD>
-__device__ double packet_walk(const SearchArgs& A, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz, uint32_t source,
-                              bool fallback, double* cp_lane, uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, uint32_t& touched, bool& overflow) {
-    const int lane = threadIdx.x & 31;
-    const bool leader = lane == __ffs(pm) - 1;
-    const bool me = (lanes >> lane) & 1u;
-    double sum = 0.0;
-    const uint2 root = __ldg(&A.topo[W.root]);
-    if (leader) {
-        s_node[0] = W.root;
-        s_rem[0] = topo_mask(root.y);
-        s_act[0] = lanes;
-    }
-    __syncwarp(pm);
-    int depth = 1;
-    while (depth > 0) {
-        const int top = depth - 1;
-        const uint32_t rem = s_rem[top];
-        if (rem == 0) {
-            --depth;
-            continue;
-        }
-        const uint32_t node = s_node[top];
-        const uint32_t act = s_act[top];
-        const int oct = 31 - __clz(rem);
-        __syncwarp(pm);
-        if (leader) {
-            s_rem[top] = rem & ~(1u << oct);
-        }
-        if (depth == 1 && me) {
-            cp_lane[oct * 32] = sum;  // running sum before the subtree of root child `oct`
-        }
-        const uint2 pt = __ldg(&A.topo[node]);
-        const uint32_t child = child_index(pt, oct);
-        const double4 rr = ldg4(&A.rec[child]);
-        const uint2 tt = __ldg(&A.topo[child]);
-        const double md = __ldg(&A.maxdim[child]);
-        int status = ST_DISCARD;
-        if ((act >> lane) & 1u) {
-            const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
-            status = e.status;
-            ++touched;
-            if (e.status == ST_ACCEPT) {
-                sum += e.w;
-            }
-        }
-        const uint32_t expand = __ballot_sync(pm, status == ST_EXPAND);
-        __syncwarp(pm);
-        if (expand) {
-            if (depth >= SD) {
-                overflow = true;
-                break;
-            }
-            if (leader) {
-                s_node[depth] = child;
-                s_rem[depth] = topo_mask(tt.y);
-                s_act[depth] = expand;
-            }
-            ++depth;
-        }
-        __syncwarp(pm);
-    }
-    __syncwarp(pm);
-    return sum;
-}
-
-// Walks without a stack: the depth-first order is followed through the
-// escape links (after a node that is not expanded, the walk continues at
-// skip[node]; after an expanded node, at its last child), so a walk keeps one
-// node index instead of a stack of frames.  The order of visits, and with it
-// every sum, is that of the stack walks above.  Every walk visits a node at
-// most once; a walk that leaves the node range or runs longer than the node
-// count reports DERR_WALK instead of looping.
+// Walks follow the reference's depth-first order without a stack: after a
+// node that is not expanded the walk continues at the node's escape link
+// (meta.z, k_meta), after an expanded node at its last child (children are
+// visited 7..0, the LIFO order of BarnesHutBase::get_nodes_to_consider), so a
+// walk keeps one node index.  Every walk visits a node at most once; a walk
+// that leaves the node range or runs longer than the node count reports
+// DERR_WALK instead of looping.
 __device__ __forceinline__ uint32_t last_child(uint2 t) {
     return t.x + (uint32_t)__popc(topo_mask(t.y)) - 1u;
 }
 
-__device__ WalkResult lane_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t sub, bool include_root, double start_sum, bool pick_mode, double r,
-                                   double sx, double sy, double sz, uint32_t source, bool fallback, bool& bad) {
-    WalkResult res{ start_sum, -1, 0, false };
-    const uint4 ms = __ldg(&A.meta[sub]);
+struct WalkResult {
+    double sum;
+    int32_t picked;  // node index in pick mode, -1 otherwise
+    uint32_t touched;
+};
+
+// Per-lane walk of the subtree of `sub` (evaluating `sub` itself when
+// `include_root`).  Sum mode adds all weights; pick mode stops at the first
+// candidate whose running sum reaches r and returns it.
+template <bool HOT>
+__device__ WalkResult lane_walk(const SearchArgs& A, const Hot64& H, const WarpNet& W, uint32_t sub, bool include_root, double start_sum,
+                                bool pick_mode, double r, double sx, double sy, double sz, uint32_t source, bool fallback, bool& bad) {
+    WalkResult res{ start_sum, -1, 0 };
+    double4 rs;
+    uint4 ms;
+    double mds;
+    load_node<HOT>(A, H, sub, rs, ms, mds);
     const uint2 ts = make_uint2(ms.x, ms.y);
     if (include_root) {
-        const double4 rr = ldg4(&A.rec[sub]);
-        const Eval e = evaluate(rr, ts, __ldg(&A.maxdim[sub]), sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
+        const Eval e = evaluate(rs, ts, mds, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
             res.sum += e.w;
@@ -307,11 +199,11 @@ __device__ WalkResult lane_walk_sl(const SearchArgs& A, const WarpNet& W, uint32
             bad = true;
             return res;
         }
-        const double4 rr = ldg4(&A.rec[node]);
-        const uint4 mm = __ldg(&A.meta[node]);
-        const double md = __ldg(&A.maxdim[node]);
+        double4 rr;
+        uint4 mm;
+        double md;
+        load_node<HOT>(A, H, node, rr, mm, md);
         const uint2 tt = make_uint2(mm.x, mm.y);
-        const uint32_t sk = mm.z;
         const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
         ++res.touched;
         if (e.status == ST_ACCEPT) {
@@ -321,22 +213,27 @@ __device__ WalkResult lane_walk_sl(const SearchArgs& A, const WarpNet& W, uint32
                 return res;
             }
         }
-        node = e.status == ST_EXPAND ? last_child(tt) : sk;
+        node = e.status == ST_EXPAND ? last_child(tt) : mm.z;
     }
     return res;
 }
 
-// Packet walk without a stack.  A lane that does not expand a node the packet
-// expands sits out the node's subtree: it records the node's escape link and
-// joins again when the walk arrives there.  The root's children are visited
-// in descending octant order; the running sum before each is the lane's
-// checkpoint for that octant.
-__device__ double packet_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz, uint32_t source,
-                                 bool fallback, double* cp_lane, uint32_t& touched, bool& bad) {
+// Packet walk over the whole tree: the lanes of packet mask `pm` (a warp or
+// an aligned part of it) walk together; `lanes` are the packet's active lanes.
+// A node is expanded when any lane expands it; a lane that does not expand a
+// node the packet expands sits out the node's subtree (it keeps the node's
+// escape link and joins again there), so each lane evaluates exactly the nodes
+// of its own walk and returns its own sequential sum.  The root's children are
+// visited in descending octant order; the running sum before each is the
+// lane's checkpoint for that octant.
+template <bool HOT>
+__device__ double packet_walk(const SearchArgs& A, const Hot64& H, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz,
+                              uint32_t source, bool fallback, double* cp_lane, uint32_t& touched, bool& bad) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     double sum = 0.0;
-    const uint2 root = __ldg(&A.topo[W.root]);
+    const uint4 rm = __ldg(&A.meta[W.root]);
+    const uint2 root = make_uint2(rm.x, rm.y);
     const uint32_t first = root.x;
     const uint32_t nrc = (uint32_t)__popc(topo_mask(root.y));
     uint32_t rc_left = topo_mask(root.y);  // root children not reached yet
@@ -359,11 +256,11 @@ __device__ double packet_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t
                 cp_lane[oct * 32] = sum;  // running sum before the subtree of root child `oct`
             }
         }
-        const double4 rr = ldg4(&A.rec[node]);
-        const uint4 mm = __ldg(&A.meta[node]);
-        const double md = __ldg(&A.maxdim[node]);
+        double4 rr;
+        uint4 mm;
+        double md;
+        load_node<HOT>(A, H, node, rr, mm, md);
         const uint2 tt = make_uint2(mm.x, mm.y);
-        const uint32_t sk = mm.z;
         int status = ST_DISCARD;
         if (act) {
             const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
@@ -377,36 +274,25 @@ __device__ double packet_walk_sl(const SearchArgs& A, const WarpNet& W, uint32_t
         if (expand) {
             if (act && status != ST_EXPAND) {
                 act = false;
-                resume = sk;
+                resume = mm.z;
             }
             node = last_child(tt);
         } else {
-            node = sk;
+            node = mm.z;
         }
     }
     __syncwarp(pm);
     return sum;
 }
 
-// One warp handles 32 consecutive entries of the search list (Morton-adjacent
-// sources) as 32/PW packets of PW lanes.  WPB warps per block; SD stack frames,
-// or walks without a stack for SD = 0.
-// CAP = 1 caps the registers at 64 (a resident block count of 32 / WPB), for
-// more warps in flight at the price of a few spills.
-template <int WPB, int SD, int PW, int CAP>
-__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchArgs A) {
-    constexpr int kPackets = 32 / PW;
-    constexpr int kFrames = SD > 0 ? SD : 1;
-    constexpr uint32_t kDescents = SD > 0 ? (uint32_t)SD : (uint32_t)kMaxLevels + 2u;
-    __shared__ uint32_t s_node[WPB][kPackets][kFrames];
-    __shared__ uint32_t s_rem[WPB][kPackets][kFrames];
-    __shared__ uint32_t s_act[WPB][kPackets][kFrames];
-    __shared__ double s_cp[WPB][8 * 32];
+// The searches of one warp task: 32 consecutive entries of the search list
+// (Morton-adjacent sources) as 32/PW packets of PW lanes.  `cp` is the warp's
+// checkpoint area (8 per lane).
+template <int PW, bool HOT>
+__device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H, uint32_t warp_global, double* cp_warp) {
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
     const int pk = lane / PW;
     const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
-    const uint32_t warp_global = blockIdx.x * WPB + wib;
     if (warp_global >= A.seg_warp[A.num_segs]) {
         return;  // whole warp idle
     }
@@ -436,37 +322,22 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     const double sx = active ? A.px[source] : 0.0;
     const double sy = active ? A.py[source] : 0.0;
     const double sz = active ? A.pz[source] : 0.0;
-    double* cp = &s_cp[wib][lane];
+    double* cp = cp_warp + lane;
     uint32_t touched = 0;
     bool overflow = false;
     bool bad = false;
     const uint32_t lanes = __ballot_sync(pm, active);
-    // the walks of this shape (SD = 0: without a stack)
-    auto packet = [&](uint32_t ls, bool fb, uint32_t& t) -> double {
-        if constexpr (SD == 0) {
-            return packet_walk_sl(A, W, pm, ls, sx, sy, sz, source, fb, cp, t, bad);
-        } else {
-            return packet_walk<SD>(A, W, pm, ls, sx, sy, sz, source, fb, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], t, overflow);
-        }
-    };
-    auto walk = [&](uint32_t sub, bool include_root, double start, bool pick_mode, double r, bool fb) -> WalkResult {
-        if constexpr (SD == 0) {
-            return lane_walk_sl(A, W, sub, include_root, start, pick_mode, r, sx, sy, sz, source, fb, bad);
-        } else {
-            return lane_walk<SD>(A, W, sub, include_root, start, pick_mode, r, sx, sy, sz, source, fb);
-        }
-    };
     int32_t result = -1;
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
         // ---- descent 0: packet walk over the whole tree
-        double total = packet(lanes, false, touched);
+        double total = packet_walk<HOT>(A, H, W, pm, lanes, sx, sy, sz, source, false, cp, touched, bad);
         bool fallback = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total == 0.0);
         if (need_fb) {
             uint32_t t2 = 0;
-            const double fb = packet(need_fb, true, t2);
+            const double fb = packet_walk<HOT>(A, H, W, pm, need_fb, sx, sy, sz, source, true, cp, t2, bad);
             if ((need_fb >> lane) & 1u) {
                 total = fb;
                 fallback = true;
@@ -479,7 +350,8 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
             const double r = pick_threshold(total, W.seed, A.step, source - W.first, j, 0);
             // the crossing lies in the last root-child subtree (DFS order) whose
             // checkpoint is below r
-            const uint2 root = __ldg(&A.topo[W.root]);
+            const uint4 rm = __ldg(&A.meta[W.root]);
+            const uint2 root = make_uint2(rm.x, rm.y);
             const uint32_t mask = topo_mask(root.y);
             int cstar = -1;
             for (int oct = 7; oct >= 0; --oct) {
@@ -496,8 +368,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
                 done = true;
             } else {
                 const uint32_t c0 = child_index(root, cstar);
-                const WalkResult wr = walk(c0, true, cp[cstar * 32], true, r, fallback);
-                overflow |= wr.overflow;
+                const WalkResult wr = lane_walk<HOT>(A, H, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback, bad);
                 if (wr.picked < 0) {
                     atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
                     done = true;
@@ -509,30 +380,29 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     }
     // ---- deeper descents, per lane
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > kDescents) {
+        if (depth > (uint32_t)kMaxLevels + 2u) {
             overflow = true;  // a descent always moves one level down; cannot recur this often
             break;
         }
-        const uint2 st = __ldg(&A.topo[sub]);
-        if (topo_leaf(st.y)) {
-            result = (int32_t)st.x;
+        const uint4 sm = __ldg(&A.meta[sub]);
+        if (topo_leaf(sm.y)) {
+            result = (int32_t)sm.x;
             done = true;
             break;
         }
-        WalkResult s1 = walk(sub, false, 0.0, false, 0.0, false);
+        WalkResult s1 = lane_walk<HOT>(A, H, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, false, bad);
         touched += s1.touched;
         bool fb = false;
         if (s1.sum == 0.0) {
-            s1 = walk(sub, false, 0.0, false, 0.0, true);
+            s1 = lane_walk<HOT>(A, H, W, sub, false, 0.0, false, 0.0, sx, sy, sz, source, true, bad);
             fb = true;
         }
-        overflow |= s1.overflow;
-        if (s1.sum == 0.0) {
+        if (s1.sum == 0.0 || bad) {
             done = true;
             break;
         }
         const double r = pick_threshold(s1.sum, W.seed, A.step, source - W.first, j, depth);
-        const WalkResult s2 = walk(sub, false, 0.0, true, r, fb);
+        const WalkResult s2 = lane_walk<HOT>(A, H, W, sub, false, 0.0, true, r, sx, sy, sz, source, fb, bad);
         if (s2.picked < 0) {
             atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
             done = true;
@@ -561,21 +431,68 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
     }
 }
 
+// One warp task per warp.  WPB warps per block; CAP = 1 caps the registers at
+// 64 (a resident block count of 32 / WPB), for more warps in flight.
+template <int WPB, int PW, int CAP>
+__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchArgs A) {
+    __shared__ double s_cp[WPB][8 * 32];
+    const int wib = threadIdx.x >> 5;
+    search_task<PW, false>(A, Hot64{ nullptr, nullptr, nullptr, 0u }, blockIdx.x * WPB + wib, s_cp[wib]);
+}
+
+// Persistent form: one block of 32 warps per SM.  The block first copies the
+// first `hot` nodes (the top levels of the octree) into shared memory, then
+// its warps take warp tasks until none are left: one each by block and warp
+// index, then the next free one from the task counter.
+template <int PW>
+__global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t hot) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* s_cp = reinterpret_cast<double*>(smem);  // 32 warps x 256
+    double4* hrec = reinterpret_cast<double4*>(smem + 32 * 256 * sizeof(double));
+    uint4* hmeta = reinterpret_cast<uint4*>(hrec + hot);
+    double* hmd = reinterpret_cast<double*>(hmeta + hot);
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
+        hrec[i] = ldg4(&A.rec[i]);
+        hmeta[i] = __ldg(&A.meta[i]);
+        hmd[i] = __ldg(&A.maxdim[i]);
+    }
+    __syncthreads();
+    const Hot64 H{ hrec, hmeta, hmd, hot };
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t total = A.seg_warp[A.num_segs];
+    uint32_t w = blockIdx.x * 32 + wib;
+    while (w < total) {
+        search_task<PW, true>(A, H, w, s_cp + wib * 256);
+        uint32_t next = 0;
+        if (lane == 0) {
+            next = atomicAdd(A.tasks, 1u) + gridDim.x * 32;
+        }
+        w = __shfl_sync(0xFFFFFFFFu, next, 0);
+    }
+}
+
 using SearchKernel = void (*)(SearchArgs);
+using HotKernel = void (*)(SearchArgs, uint32_t);
 
 // The search variants the tuner chooses from, indexed by SearchVariant.
-
 SearchKernel fp64_search_kernel(const SearchVariant& v) {
-#define RL_SV(w, s, p, c)                                                 \
-    if (v.warps == w && v.stack == s && v.packet == p && v.cap == c) {    \
-        return &k_search<w, s, p, c>;                                    \
+#define RL_SV(w, p, c)                                            \
+    if (v.hot == 0 && v.warps == w && v.packet == p && v.cap == c) { \
+        return &k_search<w, p, c>;                                \
     }
-#define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
-    RL_SV2(2, 0, 32) RL_SV2(4, 0, 32) RL_SV2(8, 0, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
-    RL_SV2(2, 0, 16) RL_SV2(4, 0, 16) RL_SV2(8, 0, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+#define RL_SV2(w, p) RL_SV(w, p, 0) RL_SV(w, p, 1)
+    RL_SV2(2, 32) RL_SV2(4, 32) RL_SV2(8, 32) RL_SV2(2, 16) RL_SV2(4, 16) RL_SV2(8, 16)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;
+}
+
+HotKernel fp64_hot_kernel(const SearchVariant& v) {
+    if (v.hot == 0) {
+        return nullptr;
+    }
+    return v.packet == 16 ? &k_search_hot<16> : &k_search_hot<32>;
 }
 
 // ---------------------------------------------------------- search list
@@ -685,9 +602,6 @@ void tune_search(Ctx& c, F&& launch_all) {
     float best = 1e30f;
     SearchVariant pick = c.tune.search;
     for (const SearchVariant& v : search_variants()) {
-        if (!stack_fits(v, c.tree)) {
-            continue;  // the stacks must hold a walk from the root to the deepest leaf
-        }
         launch_all(v);
         RL_CUDA_TRY(cudaEventRecord(e0, st));
         launch_all(v);
@@ -713,16 +627,32 @@ const std::vector<SearchVariant>& search_variants() {
         std::vector<SearchVariant> out;
         for (int cap : { 0, 1 }) {
             for (int p : { 32, 16 }) {
-                for (int s : { 0, 48 }) {
-                    for (int w : { 2, 4, 8 }) {
-                        out.push_back(SearchVariant{ w, s, p, cap });
-                    }
+                for (int w : { 2, 4, 8 }) {
+                    out.push_back(SearchVariant{ w, p, cap, 0 });
                 }
+            }
+        }
+        for (int hot : { 1024, 4096 }) {
+            for (int p : { 32, 16 }) {
+                out.push_back(SearchVariant{ 32, p, 1, hot });
             }
         }
         return out;
     }();
     return v;
+}
+
+// Nodes of the persistent form's shared-memory copy: the shape's cap, no more
+// than the octree has and than fit beside the 64 KiB of checkpoints.
+uint32_t hot_nodes(const Ctx& c, const SearchVariant& v, size_t node_bytes) {
+    if (v.hot <= 0) {
+        return 0;
+    }
+    const size_t optin = (size_t)c.smem_optin;
+    const size_t room = (optin > kHotCheckpointBytes ? optin - kHotCheckpointBytes : 0) / node_bytes;
+    size_t h = std::min<size_t>((size_t)v.hot, room);
+    h = std::min<size_t>(h, c.tree.num_nodes);
+    return (uint32_t)(h & ~(size_t)1);  // even: keeps the last array of the copy 16-byte aligned
 }
 
 void run_search(Ctx& c, uint32_t step) {
@@ -751,6 +681,7 @@ void run_search(Ctx& c, uint32_t step) {
         return;
     }
     S.first_fail.ensure(n);
+    S.tasks.ensure(2);
     S.req_count.ensure(n);
     S.req_off.ensure(n);
     k_fill_u32<<<blocks_for(n, 256), 256, 0, st>>>(S.first_fail.p, n, 0xFFFFFFFFu);
@@ -822,8 +753,8 @@ void run_search(Ctx& c, uint32_t step) {
             }
             SearchArgs& A = args[t];
             A.rec = c.tree.rec[t].p;
-            A.topo = c.tree.topo.p;
             A.maxdim = c.tree.maxdim.p;
+            A.tasks = S.tasks.p + t;
             A.meta = c.tree.meta.p;
             A.num_nodes = c.tree.num_nodes;
             A.px = c.nr.px.p;
@@ -849,8 +780,20 @@ void run_search(Ctx& c, uint32_t step) {
                 if (!launches[t].on) {
                     continue;
                 }
+                if (v.hot > 0) {
+                    RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p + t, 0, sizeof(uint32_t), st));
+                }
                 if (is_fp32(c)) {
-                    launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, launches[t].segs, launches[t].warps, step, v);
+                    launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, launches[t].segs, launches[t].warps, step, v,
+                                      S.tasks.p + t);
+                } else if (v.hot > 0) {
+                    const HotKernel kern = fp64_hot_kernel(v);
+                    const uint32_t hot = hot_nodes(c, v, sizeof(double4) + sizeof(uint4) + sizeof(double));
+                    const size_t smem = kHotCheckpointBytes + (size_t)hot * (sizeof(double4) + sizeof(uint4) + sizeof(double));
+                    RL_CUDA_TRY(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    const unsigned blocks = std::min<unsigned>((unsigned)c.num_sms, (launches[t].warps + 31) / 32);
+                    kern<<<blocks, 1024, smem, st>>>(args[t], hot);
+                    RL_LAUNCH_CHECK();
                 } else {
                     const SearchKernel kern = fp64_search_kernel(v);
                     RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");

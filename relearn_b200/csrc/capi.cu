@@ -252,6 +252,8 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     RL_CUDA_TRY(cudaGetDeviceCount(&count));
     RL_CHECK(k.device >= 0 && k.device < count, RL_ERR_DEVICE, "no such CUDA device");
     RL_CUDA_TRY(cudaSetDevice(k.device));
+    RL_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, k.device));
+    RL_CUDA_TRY(cudaDeviceGetAttribute(&c.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, k.device));
     RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
     c.stream = c.own_stream;
     g_bind = Binding{ c.stream, &c.launches, &c.device_bytes, &c.device_peak };
@@ -425,7 +427,7 @@ void remember_search_tuning(const Ctx& c) {
 bool recall_search_tuning(Ctx& c) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_search_shapes.find(tune_key(c));
-    if (it == g_search_shapes.end() || !stack_fits(it->second, c.tree)) {
+    if (it == g_search_shapes.end()) {
         return false;
     }
     c.tune.search = it->second;
@@ -1031,19 +1033,17 @@ rl_status rl_get_tuning(void* ctx, rl_tuning* out, float* search_ms, float* act_
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(out != nullptr, RL_ERR_INVALID, "null output");
         out->search_warps = c.tune.search.warps;
-        out->search_stack = c.tune.search.stack;
+        out->search_hot = c.tune.search.hot;
         out->search_packet = c.tune.search.packet;
         out->search_cap = c.tune.search.cap;
         out->act_block = c.tune.act.block;
         out->act_persistent = c.tune.act.persistent;
         out->act_vec = c.tune.act.vec;
         out->tuned = (c.tune.search_state == rl::TUNE_DONE ? 1 : 0) | (c.tune.act_state == rl::TUNE_DONE ? 2 : 0);
-        // times are recorded for the shapes that fit, in candidate order
+        // times in candidate order (0 where none was taken)
         if (search_ms) {
-            size_t k = 0;
             for (size_t v = 0; v < rl::search_variants().size(); ++v) {
-                const bool fits = rl::stack_fits(rl::search_variants()[v], c.tree);
-                search_ms[v] = fits && k < c.tune.search_ms.size() ? c.tune.search_ms[k++] : 0.0f;
+                search_ms[v] = v < c.tune.search_ms.size() ? c.tune.search_ms[v] : 0.0f;
             }
         }
         if (act_ms) {
@@ -1059,16 +1059,14 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
         RL_CHECK(t != nullptr, RL_ERR_INVALID, "null tuning");
         bool s_ok = false, a_ok = false;
         for (const auto& v : rl::search_variants()) {
-            s_ok = s_ok || (v.warps == t->search_warps && v.stack == t->search_stack && v.packet == t->search_packet && v.cap == t->search_cap);
+            s_ok = s_ok || (v.warps == t->search_warps && v.hot == t->search_hot && v.packet == t->search_packet && v.cap == t->search_cap);
         }
         for (const auto& v : rl::act_variants()) {
             a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent && v.vec == t->act_vec);
         }
         RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
         RL_CHECK(rl::is_fp32(c) || t->act_vec == 1, RL_ERR_INVALID, "the FP64 activity kernel runs one neuron per thread");
-        RL_CHECK(!c.positions_set || rl::stack_fits(rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet, t->search_cap }, c.tree),
-                 RL_ERR_INVALID, "search stack shallower than the octree");
-        c.tune.search = rl::SearchVariant{ t->search_warps, t->search_stack, t->search_packet, t->search_cap };
+        c.tune.search = rl::SearchVariant{ t->search_warps, t->search_packet, t->search_cap, t->search_hot };
         c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent, t->act_vec };
         c.tune.search_state = rl::TUNE_OFF;
         c.tune.act_state = rl::TUNE_OFF;

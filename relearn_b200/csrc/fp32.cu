@@ -416,6 +416,7 @@ struct Search32 {
     const uint4* rec;
     const uint4* meta;  // topo, escape link, FP32 cell length (k_meta)
     uint32_t num_nodes;
+    uint32_t* tasks;    // persistent form: warp tasks handed out so far
     const double *px, *py, *pz;
     const uint32_t* list_src;
     const uint32_t* list_j;
@@ -528,142 +529,42 @@ __device__ __forceinline__ float threshold32(float total, const Search32& A, con
 struct Walk32 {
     KSum sum;
     int32_t picked;
-    bool overflow;
 };
 
-template <int SD>
-__device__ Walk32 lane_walk32(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, const QPos& sp,
-                              uint32_t source, bool fb) {
-    Walk32 res{ start, -1, false };
-    uint32_t fnode[SD];
-    uint32_t frem[SD];
-    if (include_root) {
-        const uint4 ms = A.meta[sub];
-        const E32 e = eval32(A.rec[sub], mtopo(ms), mmaxdim(ms), sp, source, A, W, fb);
-        if (e.status == S_ACCEPT) {
-            res.sum.add(e.w);
-            if (pick && res.sum.s >= r) {
-                res.picked = (int32_t)sub;
-            }
-            return res;
-        }
-        if (e.status == S_DISCARD) {
-            return res;
-        }
+// Shared-memory copy of the first nodes (the top octree levels) in the
+// persistent form; n = 0 elsewhere.
+struct Hot32 {
+    const uint4* rec;
+    const uint4* meta;
+    uint32_t n;
+};
+
+template <bool HOT>
+__device__ __forceinline__ void load_node32(const Search32& A, const Hot32& H, uint32_t i, uint4& r, uint4& m) {
+    if (HOT && i < H.n) {
+        r = H.rec[i];
+        m = H.meta[i];
+    } else {
+        r = A.rec[i];
+        m = A.meta[i];
     }
-    fnode[0] = sub;
-    frem[0] = A.meta[sub].y & 0xFFu;
-    int depth = 1;
-    while (depth > 0) {
-        const int top = depth - 1;
-        const uint32_t rem = frem[top];
-        if (rem == 0) {
-            --depth;
-            continue;
-        }
-        const int oct = 31 - __clz(rem);
-        frem[top] = rem & ~(1u << oct);
-        const uint32_t child = child_of(mtopo(A.meta[fnode[top]]), oct);
-        const uint4 mc = A.meta[child];
-        const uint2 tt = mtopo(mc);
-        const E32 e = eval32(A.rec[child], tt, mmaxdim(mc), sp, source, A, W, fb);
-        if (e.status == S_ACCEPT) {
-            res.sum.add(e.w);
-            if (pick && res.sum.s >= r) {
-                res.picked = (int32_t)child;
-                return res;
-            }
-        } else if (e.status == S_EXPAND) {
-            if (depth >= SD) {
-                res.overflow = true;
-                return res;
-            }
-            fnode[depth] = child;
-            frem[depth] = topo_mask(tt.y);
-            ++depth;
-        }
-    }
-    return res;
 }
 
-// Packet walk of the lanes in packet mask `pm` (see the FP64 search).
-template <int SD>
-__device__ KSum packet32(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb, float2* cp,
-                         uint32_t* s_node, uint32_t* s_rem, uint32_t* s_act, bool& overflow) {
-    const int lane = threadIdx.x & 31;
-    const bool leader = lane == __ffs(pm) - 1;
-    const bool me = (lanes >> lane) & 1u;
-    KSum sum{ 0.0f, 0.0f };
-    if (leader) {
-        s_node[0] = W.root;
-        s_rem[0] = topo_mask(A.meta[W.root].y);
-        s_act[0] = lanes;
-    }
-    __syncwarp(pm);
-    int depth = 1;
-    while (depth > 0) {
-        const int top = depth - 1;
-        const uint32_t rem = s_rem[top];
-        if (rem == 0) {
-            --depth;
-            continue;
-        }
-        const uint32_t node = s_node[top];
-        const uint32_t act = s_act[top];
-        const int oct = 31 - __clz(rem);
-        __syncwarp(pm);
-        if (leader) {
-            s_rem[top] = rem & ~(1u << oct);
-        }
-        if (depth == 1 && me) {
-            cp[oct * 32] = make_float2(sum.s, sum.c);
-        }
-        const uint32_t child = child_of(mtopo(A.meta[node]), oct);
-        const uint4 rr = A.rec[child];
-        const uint4 mc = A.meta[child];
-        const uint2 tt = mtopo(mc);
-        const float md = mmaxdim(mc);
-        int status = S_DISCARD;
-        if ((act >> lane) & 1u) {
-            const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
-            status = e.status;
-            if (e.status == S_ACCEPT) {
-                sum.add(e.w);
-            }
-        }
-        const uint32_t expand = __ballot_sync(pm, status == S_EXPAND);
-        __syncwarp(pm);
-        if (expand) {
-            if (depth >= SD) {
-                overflow = true;
-                break;
-            }
-            if (leader) {
-                s_node[depth] = child;
-                s_rem[depth] = topo_mask(tt.y);
-                s_act[depth] = expand;
-            }
-            ++depth;
-        }
-        __syncwarp(pm);
-    }
-    __syncwarp(pm);
-    return sum;
-}
-
-// Walks without a stack through the escape links (see the FP64 search): the
-// same visiting order as the stack walks above.
+// Walks without a stack through the escape links, in the reference's
+// depth-first order (see the FP64 search).
 __device__ __forceinline__ uint32_t last_child32(uint2 t) {
     return t.x + (uint32_t)__popc(topo_mask(t.y)) - 1u;
 }
 
-__device__ Walk32 lane_walk32_sl(const Search32& A, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r, const QPos& sp,
-                                 uint32_t source, bool fb, bool& bad) {
-    Walk32 res{ start, -1, false };
-    const uint4 ms = A.meta[sub];
+template <bool HOT>
+__device__ Walk32 lane_walk32(const Search32& A, const Hot32& H, const Net32& W, uint32_t sub, bool include_root, KSum start, bool pick, float r,
+                              const QPos& sp, uint32_t source, bool fb, bool& bad) {
+    Walk32 res{ start, -1 };
+    uint4 rs, ms;
+    load_node32<HOT>(A, H, sub, rs, ms);
     const uint2 ts = mtopo(ms);
     if (include_root) {
-        const E32 e = eval32(A.rec[sub], ts, mmaxdim(ms), sp, source, A, W, fb);
+        const E32 e = eval32(rs, ts, mmaxdim(ms), sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -682,12 +583,10 @@ __device__ Walk32 lane_walk32_sl(const Search32& A, const Net32& W, uint32_t sub
             bad = true;
             return res;
         }
-        const uint4 rr = A.rec[node];
-        const uint4 mm = A.meta[node];
+        uint4 rr, mm;
+        load_node32<HOT>(A, H, node, rr, mm);
         const uint2 tt = mtopo(mm);
-        const float md = mmaxdim(mm);
-        const uint32_t sk = mm.z;
-        const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
+        const E32 e = eval32(rr, tt, mmaxdim(mm), sp, source, A, W, fb);
         if (e.status == S_ACCEPT) {
             res.sum.add(e.w);
             if (pick && res.sum.s >= r) {
@@ -695,13 +594,15 @@ __device__ Walk32 lane_walk32_sl(const Search32& A, const Net32& W, uint32_t sub
                 return res;
             }
         }
-        node = e.status == S_EXPAND ? last_child32(tt) : sk;
+        node = e.status == S_EXPAND ? last_child32(tt) : mm.z;
     }
     return res;
 }
 
-__device__ KSum packet32_sl(const Search32& A, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb, float2* cp,
-                            bool& bad) {
+// Packet walk of the lanes in packet mask `pm` (see the FP64 search).
+template <bool HOT>
+__device__ KSum packet32(const Search32& A, const Hot32& H, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb,
+                         float2* cp, bool& bad) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     KSum sum{ 0.0f, 0.0f };
@@ -728,14 +629,12 @@ __device__ KSum packet32_sl(const Search32& A, const Net32& W, uint32_t pm, uint
                 cp[oct * 32] = make_float2(sum.s, sum.c);
             }
         }
-        const uint4 rr = A.rec[node];
-        const uint4 mm = A.meta[node];
+        uint4 rr, mm;
+        load_node32<HOT>(A, H, node, rr, mm);
         const uint2 tt = mtopo(mm);
-        const float md = mmaxdim(mm);
-        const uint32_t sk = mm.z;
         int status = S_DISCARD;
         if (act) {
-            const E32 e = eval32(rr, tt, md, sp, source, A, W, fb);
+            const E32 e = eval32(rr, tt, mmaxdim(mm), sp, source, A, W, fb);
             status = e.status;
             if (e.status == S_ACCEPT) {
                 sum.add(e.w);
@@ -745,31 +644,23 @@ __device__ KSum packet32_sl(const Search32& A, const Net32& W, uint32_t pm, uint
         if (expand) {
             if (act && status != S_EXPAND) {
                 act = false;
-                resume = sk;
+                resume = mm.z;
             }
             node = last_child32(tt);
         } else {
-            node = sk;
+            node = mm.z;
         }
     }
     __syncwarp(pm);
     return sum;
 }
 
-template <int WPB, int SD, int PW, int CAP>
-__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Search32 A) {
-    constexpr int kPackets = 32 / PW;
-    constexpr int kFrames = SD > 0 ? SD : 1;
-    constexpr uint32_t kDescents = SD > 0 ? (uint32_t)SD : (uint32_t)kMaxLevels + 2u;
-    __shared__ uint32_t s_node[WPB][kPackets][kFrames];
-    __shared__ uint32_t s_rem[WPB][kPackets][kFrames];
-    __shared__ uint32_t s_act[WPB][kPackets][kFrames];
-    __shared__ float2 s_cp[WPB][8 * 32];
+// The searches of one warp task (see the FP64 search).
+template <int PW, bool HOT>
+__device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H, uint32_t warp_global, float2* cp_warp) {
     const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
     const int pk = lane / PW;
     const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
-    const uint32_t warp_global = blockIdx.x * WPB + wib;
     if (warp_global >= A.seg_warp[A.num_segs]) {
         return;
     }
@@ -798,34 +689,19 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
     const QPos sp = active ? QPos{ quantize(A.px[source], F.origin[0], F.inv_quantum), quantize(A.py[source], F.origin[1], F.inv_quantum),
                                    quantize(A.pz[source], F.origin[2], F.inv_quantum) }
                            : QPos{ 0u, 0u, 0u };
-    float2* cp = &s_cp[wib][lane];
+    float2* cp = cp_warp + lane;
     bool overflow = false;
     bool bad = false;
     const uint32_t lanes = __ballot_sync(pm, active);
-    // the walks of this shape (SD = 0: without a stack)
-    auto packet = [&](uint32_t ls, bool f) -> KSum {
-        if constexpr (SD == 0) {
-            return packet32_sl(A, W, pm, ls, sp, source, f, cp, bad);
-        } else {
-            return packet32<SD>(A, W, pm, ls, sp, source, f, cp, s_node[wib][pk], s_rem[wib][pk], s_act[wib][pk], overflow);
-        }
-    };
-    auto walk = [&](uint32_t sub, bool include_root, KSum start, bool pick, float r, bool f) -> Walk32 {
-        if constexpr (SD == 0) {
-            return lane_walk32_sl(A, W, sub, include_root, start, pick, r, sp, source, f, bad);
-        } else {
-            return lane_walk32<SD>(A, W, sub, include_root, start, pick, r, sp, source, f);
-        }
-    };
     int32_t result = -1;
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
-        KSum total = packet(lanes, false);
+        KSum total = packet32<HOT>(A, H, W, pm, lanes, sp, source, false, cp, bad);
         bool fb = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total.s == 0.0f);
         if (need_fb) {
-            const KSum t2 = packet(need_fb, true);
+            const KSum t2 = packet32<HOT>(A, H, W, pm, need_fb, sp, source, true, cp, bad);
             if ((need_fb >> lane) & 1u) {
                 total = t2;
                 fb = true;
@@ -850,8 +726,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
                 done = true;
             } else {
                 const float2 c0 = cp[cstar * 32];
-                const Walk32 wr = walk(child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, fb);
-                overflow |= wr.overflow;
+                const Walk32 wr = lane_walk32<HOT>(A, H, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sp, source, fb, bad);
                 if (wr.picked < 0) {
                     done = true;  // rounding left the crossing past the last candidate: no pick
                 } else {
@@ -861,7 +736,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
         }
     }
     for (uint32_t depth = 1; !done; ++depth) {
-        if (depth > kDescents) {
+        if (depth > (uint32_t)kMaxLevels + 2u) {
             overflow = true;
             break;
         }
@@ -870,18 +745,17 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
             result = (int32_t)st.x;
             break;
         }
-        Walk32 s1 = walk(sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, false);
+        Walk32 s1 = lane_walk32<HOT>(A, H, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, false, bad);
         bool f = false;
         if (s1.sum.s == 0.0f) {
-            s1 = walk(sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, true);
+            s1 = lane_walk32<HOT>(A, H, W, sub, false, KSum{ 0.0f, 0.0f }, false, 0.0f, sp, source, true, bad);
             f = true;
         }
-        overflow |= s1.overflow;
-        if (s1.sum.s == 0.0f) {
+        if (s1.sum.s == 0.0f || bad) {
             break;
         }
         const float r = threshold32(s1.sum.s, A, W, source, j, depth);
-        const Walk32 s2 = walk(sub, false, KSum{ 0.0f, 0.0f }, true, r, f);
+        const Walk32 s2 = lane_walk32<HOT>(A, H, W, sub, false, KSum{ 0.0f, 0.0f }, true, r, sp, source, f, bad);
         if (s2.picked < 0) {
             break;
         }
@@ -900,16 +774,50 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
     }
 }
 
+template <int WPB, int PW, int CAP>
+__global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Search32 A) {
+    __shared__ float2 s_cp[WPB][8 * 32];
+    const int wib = threadIdx.x >> 5;
+    search_task32<PW, false>(A, Hot32{ nullptr, nullptr, 0u }, blockIdx.x * WPB + wib, s_cp[wib]);
+}
+
+// Persistent form with the top octree nodes in shared memory (see the FP64
+// search).
+template <int PW>
+__global__ void __launch_bounds__(1024, 1) k_search_f32_hot(Search32 A, uint32_t hot) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* s_cp = reinterpret_cast<float2*>(smem);  // 32 warps x 256
+    uint4* hrec = reinterpret_cast<uint4*>(smem + kHotCheckpointBytes);
+    uint4* hmeta = hrec + hot;
+    for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
+        hrec[i] = A.rec[i];
+        hmeta[i] = A.meta[i];
+    }
+    __syncthreads();
+    const Hot32 H{ hrec, hmeta, hot };
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t total = A.seg_warp[A.num_segs];
+    uint32_t w = blockIdx.x * 32 + wib;
+    while (w < total) {
+        search_task32<PW, true>(A, H, w, s_cp + wib * 256);
+        uint32_t next = 0;
+        if (lane == 0) {
+            next = atomicAdd(A.tasks, 1u) + gridDim.x * 32;
+        }
+        w = __shfl_sync(0xFFFFFFFFu, next, 0);
+    }
+}
+
 using Search32Kernel = void (*)(Search32);
 
 Search32Kernel fp32_search_kernel(const SearchVariant& v) {
-#define RL_SV(w, s, p, c)                                                 \
-    if (v.warps == w && v.stack == s && v.packet == p && v.cap == c) {    \
-        return &k_search_f32<w, s, p, c>;                                    \
+#define RL_SV(w, p, c)                                            \
+    if (v.hot == 0 && v.warps == w && v.packet == p && v.cap == c) { \
+        return &k_search_f32<w, p, c>;                            \
     }
-#define RL_SV2(w, s, p) RL_SV(w, s, p, 0) RL_SV(w, s, p, 1)
-    RL_SV2(2, 0, 32) RL_SV2(4, 0, 32) RL_SV2(8, 0, 32) RL_SV2(2, 48, 32) RL_SV2(4, 48, 32) RL_SV2(8, 48, 32)
-    RL_SV2(2, 0, 16) RL_SV2(4, 0, 16) RL_SV2(8, 0, 16) RL_SV2(2, 48, 16) RL_SV2(4, 48, 16) RL_SV2(8, 48, 16)
+#define RL_SV2(w, p) RL_SV(w, p, 0) RL_SV(w, p, 1)
+    RL_SV2(2, 32) RL_SV2(4, 32) RL_SV2(8, 32) RL_SV2(2, 16) RL_SV2(4, 16) RL_SV2(8, 16)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;
@@ -1174,11 +1082,12 @@ void pack_tree_f32(Ctx& c) {
 }
 
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
-                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v) {
+                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v, uint32_t* tasks) {
     Search32 A;
     A.rec = c.tree.recq[type].p;
     A.meta = c.tree.meta.p;
     A.num_nodes = c.tree.num_nodes;
+    A.tasks = tasks;
     A.px = c.nr.px.p;
     A.py = c.nr.py.p;
     A.pz = c.nr.pz.p;
@@ -1195,6 +1104,16 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     A.step = step;
     A.err = c.err.p;
     A.kernel = Kernel32{ c.kernel.type, c.kernel.cutoff_inf, (float)c.kernel.k_minus_1, (float)c.kernel.a, (float)c.kernel.b, (float)c.kernel.cutoff };
+    if (v.hot > 0) {
+        const auto kern = v.packet == 16 ? &k_search_f32_hot<16> : &k_search_f32_hot<32>;
+        const uint32_t hot = hot_nodes(c, v, 2 * sizeof(uint4));
+        const size_t smem = kHotCheckpointBytes + (size_t)hot * 2 * sizeof(uint4);
+        RL_CUDA_TRY(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const unsigned blocks = std::min<unsigned>((unsigned)c.num_sms, (warps + 31) / 32);
+        kern<<<blocks, 1024, smem, c.stream>>>(A, hot);
+        RL_LAUNCH_CHECK();
+        return;
+    }
     const Search32Kernel kern = fp32_search_kernel(v);
     RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");
     const unsigned blocks = (warps + v.warps - 1) / v.warps;

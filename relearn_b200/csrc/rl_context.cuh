@@ -103,6 +103,7 @@ struct Search {
     DBuf<uint32_t> req_off;      // per neuron: output offset
     DBuf<uint32_t> req_tgt, req_src, req_j, req_sig;  // requests in (source, j) order
     DBuf<uint32_t> seg_starts;
+    DBuf<uint32_t> tasks;    // persistent search form: task counter per signal type
     DBuf<uint32_t> seg_warp[2], seg_net[2];
     DBuf<uint64_t> seg_begin[2], seg_end[2];
     uint64_t num_searches = 0;
@@ -224,11 +225,15 @@ struct ActDesc {
 
 // Launch shape of the Barnes-Hut search kernels.
 struct SearchVariant {
-    int warps = 4;    // warps per block
-    int stack = 0;    // frames of the per-lane and per-packet stacks; 0 = walks without a stack
+    int warps = 2;    // warps per block
     int packet = 32;  // lanes (sources) that walk the descent from the root together
     int cap = 1;      // 1: registers capped at 64 for more resident warps
+    int hot = 0;      // > 0: persistent form, one block of 32 warps per SM with up
+                      // to `hot` top octree nodes in shared memory
 };
+// Shared memory of the persistent search form besides its node copy: 8
+// checkpoint sums per lane of 32 warps.
+constexpr size_t kHotCheckpointBytes = 32 * 256 * sizeof(double);
 
 // Launch shape of the activity kernel.
 struct ActVariant {
@@ -251,17 +256,15 @@ struct Tuning {
 };
 
 const std::vector<SearchVariant>& search_variants();
-// A shape with a stack needs frames for a walk from the root to the deepest
-// leaf; stack 0 walks without a stack and fits every octree.
-inline bool stack_fits(const SearchVariant& v, const Tree& t) {
-    return v.stack == 0 || (uint32_t)v.stack >= t.max_level + 2;
-}
+uint32_t hot_nodes(const Ctx& c, const SearchVariant& v, size_t node_bytes);
 const std::vector<ActVariant>& act_variants();
 
 struct Ctx {
     rl_config cfg{};
     uint32_t n = 0;
     int device = 0;
+    int num_sms = 148;          // streaming multiprocessors of the device
+    int smem_optin = 232448;    // shared memory a block may opt in to (bytes)
     cudaStream_t stream = nullptr;      // stream all work is issued on
     cudaStream_t own_stream = nullptr;  // the context's own stream
     PhaseTimer timer;
@@ -335,7 +338,7 @@ void launch_activity_fp64(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t
 uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
-                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v);
+                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v, uint32_t* tasks);
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu

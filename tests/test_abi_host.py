@@ -67,7 +67,7 @@ def test_host_only_entry_points(built_lib):
     import relearn_b200 as R
 
     L = R.load_library()
-    assert L.rl_abi_version() == 2
+    assert L.rl_abi_version() == 3
     cfg = R.RlConfig()
     L.rl_config_default(C.byref(cfg), 2000, 1000.0)
     # reference defaults: Parameters.h:123-130, CalciumCalculatorBase.h:206-210, Gaussian.h:38-39

@@ -1,6 +1,6 @@
 """Autotuned launch shapes: every candidate shape of the search and activity
 kernels computes the same results (bit for bit), so tuning never changes what
-a run produces; the tuner times the candidates that fit the octree."""
+a run produces."""
 import numpy as np
 import pytest
 
@@ -27,20 +27,15 @@ def test_every_search_shape_finds_the_same_targets(precision):
     net = make(n, 3100.0, 21, precision)
     one = np.full(n, 2, np.uint32)
     net.prepare_update_connectivity(one, one, one)
-    depth = net.tree_info()[1]
     ref = None
-    tried = 0
-    for w, st, p, cp in SEARCH_SHAPES:
-        if st < depth + 2:
-            continue
-        net.set_tuning(search_warps=w, search_stack=st, search_packet=p, search_cap=cp)
+    for w, p, cp, hot in SEARCH_SHAPES:
+        net.set_tuning(search_warps=w, search_packet=p, search_cap=cp, search_hot=hot)
         req = net.find_targets(100)
         if ref is None:
             ref = req
         else:
-            assert np.array_equal(req, ref), (w, st, p, cp)
-        tried += 1
-    assert tried >= 12 and len(ref) > 0
+            assert np.array_equal(req, ref), (w, p, cp, hot)
+    assert len(ref) > 0
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -87,3 +82,30 @@ def test_tuned_run_equals_untuned(precision):
     for a, b in zip(e0, e1):
         assert np.array_equal(a, b)
     assert len(e0[0]) > 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_search_shape_on_a_forest(precision):
+    """Many networks in one context: the persistent form's shared-memory copy
+    then holds the top levels of every network's octree."""
+    from relearn_b200 import SEARCH_SHAPES, Network, default_params
+    from test_gpu_ensemble import ensemble_spec, net_inputs
+
+    nets = ensemble_spec(11 + precision, 9, 200, 6000)
+    base = default_params(1, 1.0)
+    base["precision"] = precision
+    ens = Network(base, networks=nets)
+    inputs = [net_inputs(d, k) for k, d in enumerate(nets)]
+    ens.set_positions(np.concatenate([p for p, _, _ in inputs]), np.concatenate([s for _, s, _ in inputs]))
+    n = sum(d["num_neurons"] for d in nets)
+    one = np.full(n, 2, np.uint32)
+    ens.prepare_update_connectivity(one, one, one)
+    ref = None
+    for w, p, cp, hot in SEARCH_SHAPES:
+        ens.set_tuning(search_warps=w, search_packet=p, search_cap=cp, search_hot=hot)
+        req = ens.find_targets(100)
+        if ref is None:
+            ref = req
+        else:
+            assert np.array_equal(req, ref), (w, p, cp, hot)
+    assert len(ref) > 0
