@@ -42,6 +42,8 @@ struct SearchArgs {
     const double4* rec;  // records of the searched dendrite type
     const double* maxdim;
     const uint4* meta;     // topo, escape link, FP32 cell length (k_meta)
+    const uint32_t* first_key;  // Morton rank of the first neuron under a node
+    const uint32_t* leaf_of;    // neuron -> leaf node
     uint32_t* tasks;       // persistent form: warp tasks handed out so far
     uint32_t num_nodes;
     const double *px, *py, *pz;
@@ -218,26 +220,41 @@ __device__ WalkResult lane_walk(const SearchArgs& A, const Hot64& H, const WarpN
     return res;
 }
 
+// Checkpoints of a packet walk, per lane: the running sum before each child
+// of the root, and, where the lane expanded them, before each child of its own
+// level-1 and level-2 ancestors (the cells that contain its source; every
+// walk expands them for theta < 1/sqrt(3)).  The pick re-walks only the
+// smallest of these subtrees that holds the crossing.  Kept in local memory
+// (written at the top three levels only).
+constexpr int kCpPerLevel = 8;
+struct Ancestry {
+    uint32_t a1 = kNoNode, a1_first = 0, a1_n = 0;  // level-1 ancestor and its children
+    uint32_t a2 = kNoNode, a2_first = 0, a2_n = 0;  // level-2 ancestor and its children
+    bool valid2 = false, valid3 = false;            // checkpoints below a1 / a2 recorded
+};
+
+__device__ __forceinline__ uint32_t inner_children(const uint4& m) {
+    return topo_leaf(m.y) ? 0u : (uint32_t)__popc(topo_mask(m.y));
+}
+
 // Packet walk over the whole tree: the lanes of packet mask `pm` (a warp or
 // an aligned part of it) walk together; `lanes` are the packet's active lanes.
 // A node is expanded when any lane expands it; a lane that does not expand a
 // node the packet expands sits out the node's subtree (it keeps the node's
 // escape link and joins again there), so each lane evaluates exactly the nodes
-// of its own walk and returns its own sequential sum.  The root's children are
-// visited in descending octant order; the running sum before each is the
-// lane's checkpoint for that octant.
+// of its own walk and returns its own sequential sum.  `my_rank` is the Morton
+// rank of the lane's source; `cp` receives its checkpoints.
 template <bool HOT>
 __device__ double packet_walk(const SearchArgs& A, const Hot64& H, const WarpNet& W, uint32_t pm, uint32_t lanes, double sx, double sy, double sz,
-                              uint32_t source, bool fallback, double* cp_lane, uint32_t& touched, bool& bad) {
+                              uint32_t source, uint32_t my_rank, bool fallback, double* cp, Ancestry& an, uint32_t& touched, bool& bad) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     double sum = 0.0;
+    an = Ancestry{};
     const uint4 rm = __ldg(&A.meta[W.root]);
-    const uint2 root = make_uint2(rm.x, rm.y);
-    const uint32_t first = root.x;
-    const uint32_t nrc = (uint32_t)__popc(topo_mask(root.y));
-    uint32_t rc_left = topo_mask(root.y);  // root children not reached yet
-    uint32_t node = last_child(root);
+    const uint32_t first0 = rm.x;
+    const uint32_t root_level = topo_level(rm.y);
+    uint32_t node = last_child(make_uint2(rm.x, rm.y));
     bool act = me;
     uint32_t resume = kNoNode;
     for (uint32_t guard = 0; node != kNoNode; ++guard) {
@@ -249,18 +266,39 @@ __device__ double packet_walk(const SearchArgs& A, const Hot64& H, const WarpNet
             act = true;
             resume = kNoNode;
         }
-        if (node - first < nrc) {
-            const int oct = 31 - __clz(rc_left);
-            rc_left &= ~(1u << oct);
-            if (me) {
-                cp_lane[oct * 32] = sum;  // running sum before the subtree of root child `oct`
-            }
-        }
         double4 rr;
         uint4 mm;
         double md;
         load_node<HOT>(A, H, node, rr, mm, md);
         const uint2 tt = make_uint2(mm.x, mm.y);
+        const uint32_t lvl = topo_level(mm.y) - root_level;
+        if (lvl <= 3u) {  // the top of the tree: checkpoints (the branch is uniform)
+            if (lvl == 1u) {
+                if (me) {
+                    cp[node - first0] = sum;
+                    if (an.a1 == kNoNode && __ldg(&A.first_key[node]) <= my_rank) {
+                        an.a1 = node;
+                        an.a1_first = mm.x;
+                        an.a1_n = inner_children(mm);
+                    }
+                }
+            } else if (lvl == 2u) {
+                if (act && node - an.a1_first < an.a1_n) {
+                    cp[kCpPerLevel + (node - an.a1_first)] = sum;
+                    an.valid2 = true;
+                    if (an.a2 == kNoNode && __ldg(&A.first_key[node]) <= my_rank) {
+                        an.a2 = node;
+                        an.a2_first = mm.x;
+                        an.a2_n = inner_children(mm);
+                    }
+                }
+            } else if (lvl == 3u) {
+                if (act && node - an.a2_first < an.a2_n) {
+                    cp[2 * kCpPerLevel + (node - an.a2_first)] = sum;
+                    an.valid3 = true;
+                }
+            }
+        }
         int status = ST_DISCARD;
         if (act) {
             const Eval e = evaluate(rr, tt, md, sx, sy, sz, source, W.theta, A.mu, W.scale, fallback, A.kernel);
@@ -285,11 +323,25 @@ __device__ double packet_walk(const SearchArgs& A, const Hot64& H, const WarpNet
     return sum;
 }
 
+// The child (first + k) of a checkpointed level that holds the crossing of r:
+// the last child in walking order (children are walked in descending rank)
+// whose checkpoint lies below r; -1 if none does.
+__device__ __forceinline__ int crossing_child(const double* cp, uint32_t n, double r) {
+    int k = -1;
+    for (int q = (int)n - 1; q >= 0; --q) {
+        if (cp[q] < r) {
+            k = q;
+        } else {
+            break;
+        }
+    }
+    return k;
+}
+
 // The searches of one warp task: 32 consecutive entries of the search list
-// (Morton-adjacent sources) as 32/PW packets of PW lanes.  `cp` is the warp's
-// checkpoint area (8 per lane).
+// (Morton-adjacent sources) as 32/PW packets of PW lanes.
 template <int PW, bool HOT>
-__device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H, uint32_t warp_global, double* cp_warp) {
+__device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H, uint32_t warp_global) {
     const int lane = threadIdx.x & 31;
     const int pk = lane / PW;
     const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
@@ -322,7 +374,9 @@ __device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H,
     const double sx = active ? A.px[source] : 0.0;
     const double sy = active ? A.py[source] : 0.0;
     const double sz = active ? A.pz[source] : 0.0;
-    double* cp = cp_warp + lane;
+    const uint32_t my_rank = active ? __ldg(&A.first_key[__ldg(&A.leaf_of[source])]) : 0u;
+    double cp[3 * kCpPerLevel];
+    Ancestry an;
     uint32_t touched = 0;
     bool overflow = false;
     bool bad = false;
@@ -332,15 +386,17 @@ __device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H,
     uint32_t sub = 0;
     if (lanes) {
         // ---- descent 0: packet walk over the whole tree
-        double total = packet_walk<HOT>(A, H, W, pm, lanes, sx, sy, sz, source, false, cp, touched, bad);
+        double total = packet_walk<HOT>(A, H, W, pm, lanes, sx, sy, sz, source, my_rank, false, cp, an, touched, bad);
         bool fallback = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total == 0.0);
         if (need_fb) {
             uint32_t t2 = 0;
-            const double fb = packet_walk<HOT>(A, H, W, pm, need_fb, sx, sy, sz, source, true, cp, t2, bad);
+            Ancestry an_fb;
+            const double fb = packet_walk<HOT>(A, H, W, pm, need_fb, sx, sy, sz, source, my_rank, true, cp, an_fb, t2, bad);
             if ((need_fb >> lane) & 1u) {
                 total = fb;
                 fallback = true;
+                an = an_fb;
             }
         }
         if (active && total == 0.0) {
@@ -348,27 +404,32 @@ __device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H,
         }
         if (!done) {
             const double r = pick_threshold(total, W.seed, A.step, source - W.first, j, 0);
-            // the crossing lies in the last root-child subtree (DFS order) whose
-            // checkpoint is below r
+            // the crossing lies in the last root child (walking order) whose
+            // checkpoint is below r; inside the lane's own ancestors, in the
+            // last of their checkpointed children below r
             const uint4 rm = __ldg(&A.meta[W.root]);
-            const uint2 root = make_uint2(rm.x, rm.y);
-            const uint32_t mask = topo_mask(root.y);
-            int cstar = -1;
-            for (int oct = 7; oct >= 0; --oct) {
-                if ((mask >> oct) & 1u) {
-                    if (cp[oct * 32] < r) {
-                        cstar = oct;
-                    } else {
-                        break;
-                    }
-                }
-            }
-            if (cstar < 0) {
+            const int k1 = crossing_child(cp, inner_children(rm), r);
+            if (k1 < 0) {
                 atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
                 done = true;
             } else {
-                const uint32_t c0 = child_index(root, cstar);
-                const WalkResult wr = lane_walk<HOT>(A, H, W, c0, true, cp[cstar * 32], true, r, sx, sy, sz, source, fallback, bad);
+                uint32_t c0 = rm.x + (uint32_t)k1;
+                double start = cp[k1];
+                if (an.valid2 && c0 == an.a1) {
+                    const int k2 = crossing_child(cp + kCpPerLevel, an.a1_n, r);
+                    if (k2 >= 0) {
+                        c0 = an.a1_first + (uint32_t)k2;
+                        start = cp[kCpPerLevel + k2];
+                        if (an.valid3 && c0 == an.a2) {
+                            const int k3 = crossing_child(cp + 2 * kCpPerLevel, an.a2_n, r);
+                            if (k3 >= 0) {
+                                c0 = an.a2_first + (uint32_t)k3;
+                                start = cp[2 * kCpPerLevel + k3];
+                            }
+                        }
+                    }
+                }
+                const WalkResult wr = lane_walk<HOT>(A, H, W, c0, true, start, true, r, sx, sy, sz, source, fallback, bad);
                 if (wr.picked < 0) {
                     atomicOr(A.err, (uint32_t)DERR_NO_CROSSING);
                     done = true;
@@ -435,9 +496,8 @@ __device__ __forceinline__ void search_task(const SearchArgs& A, const Hot64& H,
 // 64 (a resident block count of 32 / WPB), for more warps in flight.
 template <int WPB, int PW, int CAP>
 __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchArgs A) {
-    __shared__ double s_cp[WPB][8 * 32];
     const int wib = threadIdx.x >> 5;
-    search_task<PW, false>(A, Hot64{ nullptr, nullptr, nullptr, 0u }, blockIdx.x * WPB + wib, s_cp[wib]);
+    search_task<PW, false>(A, Hot64{ nullptr, nullptr, nullptr, 0u }, blockIdx.x * WPB + wib);
 }
 
 // Persistent form: one block of 32 warps per SM.  The block first copies the
@@ -447,8 +507,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search(SearchA
 template <int PW>
 __global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t hot) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double* s_cp = reinterpret_cast<double*>(smem);  // 32 warps x 256
-    double4* hrec = reinterpret_cast<double4*>(smem + 32 * 256 * sizeof(double));
+    double4* hrec = reinterpret_cast<double4*>(smem);
     uint4* hmeta = reinterpret_cast<uint4*>(hrec + hot);
     double* hmd = reinterpret_cast<double*>(hmeta + hot);
     for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
@@ -463,7 +522,7 @@ __global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t h
     const uint32_t total = A.seg_warp[A.num_segs];
     uint32_t w = blockIdx.x * 32 + wib;
     while (w < total) {
-        search_task<PW, true>(A, H, w, s_cp + wib * 256);
+        search_task<PW, true>(A, H, w);
         uint32_t next = 0;
         if (lane == 0) {
             next = atomicAdd(A.tasks, 1u) + gridDim.x * 32;
@@ -643,13 +702,12 @@ const std::vector<SearchVariant>& search_variants() {
 }
 
 // Nodes of the persistent form's shared-memory copy: the shape's cap, no more
-// than the octree has and than fit beside the 64 KiB of checkpoints.
+// than the octree has and than fit in a block's shared memory.
 uint32_t hot_nodes(const Ctx& c, const SearchVariant& v, size_t node_bytes) {
     if (v.hot <= 0) {
         return 0;
     }
-    const size_t optin = (size_t)c.smem_optin;
-    const size_t room = (optin > kHotCheckpointBytes ? optin - kHotCheckpointBytes : 0) / node_bytes;
+    const size_t room = (size_t)c.smem_optin / node_bytes;
     size_t h = std::min<size_t>((size_t)v.hot, room);
     h = std::min<size_t>(h, c.tree.num_nodes);
     return (uint32_t)(h & ~(size_t)1);  // even: keeps the last array of the copy 16-byte aligned
@@ -755,6 +813,8 @@ void run_search(Ctx& c, uint32_t step) {
             A.rec = c.tree.rec[t].p;
             A.maxdim = c.tree.maxdim.p;
             A.tasks = S.tasks.p + t;
+            A.first_key = c.tree.first_key.p;
+            A.leaf_of = c.tree.leaf_of.p;
             A.meta = c.tree.meta.p;
             A.num_nodes = c.tree.num_nodes;
             A.px = c.nr.px.p;
@@ -789,7 +849,7 @@ void run_search(Ctx& c, uint32_t step) {
                 } else if (v.hot > 0) {
                     const HotKernel kern = fp64_hot_kernel(v);
                     const uint32_t hot = hot_nodes(c, v, sizeof(double4) + sizeof(uint4) + sizeof(double));
-                    const size_t smem = kHotCheckpointBytes + (size_t)hot * (sizeof(double4) + sizeof(uint4) + sizeof(double));
+                    const size_t smem = (size_t)hot * (sizeof(double4) + sizeof(uint4) + sizeof(double));
                     RL_CUDA_TRY(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                     const unsigned blocks = std::min<unsigned>((unsigned)c.num_sms, (launches[t].warps + 31) / 32);
                     kern<<<blocks, 1024, smem, st>>>(args[t], hot);

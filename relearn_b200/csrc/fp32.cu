@@ -416,6 +416,8 @@ struct Search32 {
     const uint4* rec;
     const uint4* meta;  // topo, escape link, FP32 cell length (k_meta)
     uint32_t num_nodes;
+    const uint32_t* first_key;  // Morton rank of the first neuron under a node
+    const uint32_t* leaf_of;    // neuron -> leaf node
     uint32_t* tasks;    // persistent form: warp tasks handed out so far
     const double *px, *py, *pz;
     const uint32_t* list_src;
@@ -599,18 +601,32 @@ __device__ Walk32 lane_walk32(const Search32& A, const Hot32& H, const Net32& W,
     return res;
 }
 
+// Checkpoints of a packet walk (see the FP64 search): the running sum before
+// each root child and, where the lane expanded them, before each child of its
+// level-1 and level-2 ancestors.
+constexpr int kCp32PerLevel = 8;
+struct Ancestry32 {
+    uint32_t a1 = kNoNode, a1_first = 0, a1_n = 0;
+    uint32_t a2 = kNoNode, a2_first = 0, a2_n = 0;
+    bool valid2 = false, valid3 = false;
+};
+
+__device__ __forceinline__ uint32_t inner_children32(const uint4& m) {
+    return topo_leaf(m.y) ? 0u : (uint32_t)__popc(topo_mask(m.y));
+}
+
 // Packet walk of the lanes in packet mask `pm` (see the FP64 search).
 template <bool HOT>
-__device__ KSum packet32(const Search32& A, const Hot32& H, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source, bool fb,
-                         float2* cp, bool& bad) {
+__device__ KSum packet32(const Search32& A, const Hot32& H, const Net32& W, uint32_t pm, uint32_t lanes, const QPos& sp, uint32_t source,
+                         uint32_t my_rank, bool fb, float2* cp, Ancestry32& an, bool& bad) {
     const int lane = threadIdx.x & 31;
     const bool me = (lanes >> lane) & 1u;
     KSum sum{ 0.0f, 0.0f };
-    const uint2 root = mtopo(A.meta[W.root]);
-    const uint32_t first = root.x;
-    const uint32_t nrc = (uint32_t)__popc(topo_mask(root.y));
-    uint32_t rc_left = topo_mask(root.y);
-    uint32_t node = last_child32(root);
+    an = Ancestry32{};
+    const uint4 rm = A.meta[W.root];
+    const uint32_t first0 = rm.x;
+    const uint32_t root_level = topo_level(rm.y);
+    uint32_t node = last_child32(mtopo(rm));
     bool act = me;
     uint32_t resume = kNoNode;
     for (uint32_t guard = 0; node != kNoNode; ++guard) {
@@ -622,16 +638,38 @@ __device__ KSum packet32(const Search32& A, const Hot32& H, const Net32& W, uint
             act = true;
             resume = kNoNode;
         }
-        if (node - first < nrc) {
-            const int oct = 31 - __clz(rc_left);
-            rc_left &= ~(1u << oct);
-            if (me) {
-                cp[oct * 32] = make_float2(sum.s, sum.c);
-            }
-        }
         uint4 rr, mm;
         load_node32<HOT>(A, H, node, rr, mm);
         const uint2 tt = mtopo(mm);
+        const uint32_t lvl = topo_level(mm.y) - root_level;
+        if (lvl <= 3u) {  // the top of the tree: checkpoints (the branch is uniform)
+            const float2 now = make_float2(sum.s, sum.c);
+            if (lvl == 1u) {
+                if (me) {
+                    cp[node - first0] = now;
+                    if (an.a1 == kNoNode && A.first_key[node] <= my_rank) {
+                        an.a1 = node;
+                        an.a1_first = mm.x;
+                        an.a1_n = inner_children32(mm);
+                    }
+                }
+            } else if (lvl == 2u) {
+                if (act && node - an.a1_first < an.a1_n) {
+                    cp[kCp32PerLevel + (node - an.a1_first)] = now;
+                    an.valid2 = true;
+                    if (an.a2 == kNoNode && A.first_key[node] <= my_rank) {
+                        an.a2 = node;
+                        an.a2_first = mm.x;
+                        an.a2_n = inner_children32(mm);
+                    }
+                }
+            } else if (lvl == 3u) {
+                if (act && node - an.a2_first < an.a2_n) {
+                    cp[2 * kCp32PerLevel + (node - an.a2_first)] = now;
+                    an.valid3 = true;
+                }
+            }
+        }
         int status = S_DISCARD;
         if (act) {
             const E32 e = eval32(rr, tt, mmaxdim(mm), sp, source, A, W, fb);
@@ -655,9 +693,21 @@ __device__ KSum packet32(const Search32& A, const Hot32& H, const Net32& W, uint
     return sum;
 }
 
+__device__ __forceinline__ int crossing_child32(const float2* cp, uint32_t n, float r) {
+    int k = -1;
+    for (int q = (int)n - 1; q >= 0; --q) {
+        if (cp[q].x < r) {
+            k = q;
+        } else {
+            break;
+        }
+    }
+    return k;
+}
+
 // The searches of one warp task (see the FP64 search).
 template <int PW, bool HOT>
-__device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H, uint32_t warp_global, float2* cp_warp) {
+__device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H, uint32_t warp_global) {
     const int lane = threadIdx.x & 31;
     const int pk = lane / PW;
     const uint32_t pm = PW == 32 ? 0xFFFFFFFFu : (((1u << PW) - 1u) << (pk * PW));
@@ -689,7 +739,9 @@ __device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H,
     const QPos sp = active ? QPos{ quantize(A.px[source], F.origin[0], F.inv_quantum), quantize(A.py[source], F.origin[1], F.inv_quantum),
                                    quantize(A.pz[source], F.origin[2], F.inv_quantum) }
                            : QPos{ 0u, 0u, 0u };
-    float2* cp = cp_warp + lane;
+    const uint32_t my_rank = active ? A.first_key[A.leaf_of[source]] : 0u;
+    float2 cp[3 * kCp32PerLevel];
+    Ancestry32 an;
     bool overflow = false;
     bool bad = false;
     const uint32_t lanes = __ballot_sync(pm, active);
@@ -697,36 +749,43 @@ __device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H,
     bool done = !active;
     uint32_t sub = 0;
     if (lanes) {
-        KSum total = packet32<HOT>(A, H, W, pm, lanes, sp, source, false, cp, bad);
+        KSum total = packet32<HOT>(A, H, W, pm, lanes, sp, source, my_rank, false, cp, an, bad);
         bool fb = false;
         const uint32_t need_fb = __ballot_sync(pm, active && total.s == 0.0f);
         if (need_fb) {
-            const KSum t2 = packet32<HOT>(A, H, W, pm, need_fb, sp, source, true, cp, bad);
+            Ancestry32 an_fb;
+            const KSum t2 = packet32<HOT>(A, H, W, pm, need_fb, sp, source, my_rank, true, cp, an_fb, bad);
             if ((need_fb >> lane) & 1u) {
                 total = t2;
                 fb = true;
+                an = an_fb;
             }
         }
         done = done || total.s == 0.0f;
         if (!done) {
             const float r = threshold32(total.s, A, W, source, j, 0);
-            const uint2 root = mtopo(A.meta[W.root]);
-            const uint32_t mask = topo_mask(root.y);
-            int cstar = -1;
-            for (int oct = 7; oct >= 0; --oct) {
-                if ((mask >> oct) & 1u) {
-                    if (cp[oct * 32].x < r) {
-                        cstar = oct;
-                    } else {
-                        break;
-                    }
-                }
-            }
-            if (cstar < 0) {
+            const uint4 rm = A.meta[W.root];
+            const int k1 = crossing_child32(cp, inner_children32(rm), r);
+            if (k1 < 0) {
                 done = true;
             } else {
-                const float2 c0 = cp[cstar * 32];
-                const Walk32 wr = lane_walk32<HOT>(A, H, W, child_of(root, cstar), true, KSum{ c0.x, c0.y }, true, r, sp, source, fb, bad);
+                uint32_t c0 = rm.x + (uint32_t)k1;
+                float2 start = cp[k1];
+                if (an.valid2 && c0 == an.a1) {
+                    const int k2 = crossing_child32(cp + kCp32PerLevel, an.a1_n, r);
+                    if (k2 >= 0) {
+                        c0 = an.a1_first + (uint32_t)k2;
+                        start = cp[kCp32PerLevel + k2];
+                        if (an.valid3 && c0 == an.a2) {
+                            const int k3 = crossing_child32(cp + 2 * kCp32PerLevel, an.a2_n, r);
+                            if (k3 >= 0) {
+                                c0 = an.a2_first + (uint32_t)k3;
+                                start = cp[2 * kCp32PerLevel + k3];
+                            }
+                        }
+                    }
+                }
+                const Walk32 wr = lane_walk32<HOT>(A, H, W, c0, true, KSum{ start.x, start.y }, true, r, sp, source, fb, bad);
                 if (wr.picked < 0) {
                     done = true;  // rounding left the crossing past the last candidate: no pick
                 } else {
@@ -776,9 +835,8 @@ __device__ __forceinline__ void search_task32(const Search32& A, const Hot32& H,
 
 template <int WPB, int PW, int CAP>
 __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Search32 A) {
-    __shared__ float2 s_cp[WPB][8 * 32];
     const int wib = threadIdx.x >> 5;
-    search_task32<PW, false>(A, Hot32{ nullptr, nullptr, 0u }, blockIdx.x * WPB + wib, s_cp[wib]);
+    search_task32<PW, false>(A, Hot32{ nullptr, nullptr, 0u }, blockIdx.x * WPB + wib);
 }
 
 // Persistent form with the top octree nodes in shared memory (see the FP64
@@ -786,8 +844,7 @@ __global__ void __launch_bounds__(WPB * 32, CAP ? 32 / WPB : 1) k_search_f32(Sea
 template <int PW>
 __global__ void __launch_bounds__(1024, 1) k_search_f32_hot(Search32 A, uint32_t hot) {
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* s_cp = reinterpret_cast<float2*>(smem);  // 32 warps x 256
-    uint4* hrec = reinterpret_cast<uint4*>(smem + kHotCheckpointBytes);
+    uint4* hrec = reinterpret_cast<uint4*>(smem);
     uint4* hmeta = hrec + hot;
     for (uint32_t i = threadIdx.x; i < hot; i += blockDim.x) {
         hrec[i] = A.rec[i];
@@ -800,7 +857,7 @@ __global__ void __launch_bounds__(1024, 1) k_search_f32_hot(Search32 A, uint32_t
     const uint32_t total = A.seg_warp[A.num_segs];
     uint32_t w = blockIdx.x * 32 + wib;
     while (w < total) {
-        search_task32<PW, true>(A, H, w, s_cp + wib * 256);
+        search_task32<PW, true>(A, H, w);
         uint32_t next = 0;
         if (lane == 0) {
             next = atomicAdd(A.tasks, 1u) + gridDim.x * 32;
@@ -1088,6 +1145,8 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     A.meta = c.tree.meta.p;
     A.num_nodes = c.tree.num_nodes;
     A.tasks = tasks;
+    A.first_key = c.tree.first_key.p;
+    A.leaf_of = c.tree.leaf_of.p;
     A.px = c.nr.px.p;
     A.py = c.nr.py.p;
     A.pz = c.nr.pz.p;
@@ -1107,7 +1166,7 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     if (v.hot > 0) {
         const auto kern = v.packet == 16 ? &k_search_f32_hot<16> : &k_search_f32_hot<32>;
         const uint32_t hot = hot_nodes(c, v, 2 * sizeof(uint4));
-        const size_t smem = kHotCheckpointBytes + (size_t)hot * 2 * sizeof(uint4);
+        const size_t smem = (size_t)hot * 2 * sizeof(uint4);
         RL_CUDA_TRY(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned blocks = std::min<unsigned>((unsigned)c.num_sms, (warps + 31) / 32);
         kern<<<blocks, 1024, smem, c.stream>>>(A, hot);

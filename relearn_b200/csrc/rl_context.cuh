@@ -231,9 +231,7 @@ struct SearchVariant {
     int hot = 0;      // > 0: persistent form, one block of 32 warps per SM with up
                       // to `hot` top octree nodes in shared memory
 };
-// Shared memory of the persistent search form besides its node copy: 8
-// checkpoint sums per lane of 32 warps.
-constexpr size_t kHotCheckpointBytes = 32 * 256 * sizeof(double);
+
 
 // Launch shape of the activity kernel.
 struct ActVariant {
