@@ -893,8 +893,7 @@ void activity_step(Sim& s, uint32_t step) {
         double input = 0.0;
         input += inp * c.conductance;
         // NormalActivityInputCPU::update_input_range (NormalActivityInputCPU.cpp:21-39)
-        const oracle::Words r = oracle::stream_draw(c.seed, step, (uint32_t)i, 0, oracle::S_NOISE, 0);
-        const double z = oracle::as241(oracle::unit_open(r), [&](double v) { return s.lg(v); });
+        const double z = oracle::as241(oracle::noise_unit_open(c.seed, step, (uint32_t)i), [&](double v) { return s.lg(v); });
         input += c.noise_mean + c.noise_stddev * z;
         s.input[i] = input;
         double xv = s.x[i];
@@ -1345,8 +1344,7 @@ double orc_hypot3(double x, double y, double z) {
     return oracle::hypot3(x, y, z);
 }
 double orc_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
-    const oracle::Words r = oracle::stream_draw(seed, step, neuron, 0, oracle::S_NOISE, 0);
-    return mean + stddev * oracle::as241(oracle::unit_open(r), [](double v) { return oracle::own_log(v); });
+    return mean + stddev * oracle::as241(oracle::noise_unit_open(seed, step, neuron), [](double v) { return oracle::own_log(v); });
 }
 double orc_quantile(double p) {
     return oracle::as241(p, [](double v) { return oracle::own_log(v); });

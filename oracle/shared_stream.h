@@ -74,6 +74,14 @@ inline double unit_closed_open(const Words& r) {
 inline double unit_open(const Words& r) {
     return ((double)take53(r) + 0.5) * 0x1.0p-53;
 }
+// Background input: one block per neuron pair (2m, 2m + 1) and step, words
+// 0-1 for the even neuron and 2-3 for the odd one.
+inline double noise_unit_open(uint64_t seed, uint32_t step, uint32_t neuron) {
+    const Words r = stream_draw(seed, step, neuron >> 1, 0, S_NOISE, 0);
+    const int o = (neuron & 1u) ? 2 : 0;
+    const uint64_t b = ((uint64_t)r.w[o] << 21) | (uint64_t)(r.w[o + 1] >> 11);
+    return ((double)b + 0.5) * 0x1.0p-53;
+}
 inline uint64_t take64(const Words& r) {
     return ((uint64_t)r.w[0] << 32) | (uint64_t)r.w[1];
 }

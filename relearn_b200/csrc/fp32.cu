@@ -117,10 +117,10 @@ __device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
 
 // One neuron's activity step on registers: `x`, `u`, `ca` and the three
 // deltas are read and updated in place; `input` and `fired` are outputs.
+// `k24`: the neuron's 24 random bits of this step's background draw.
 template <int H>
-__device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, bool enabled, uint8_t fired_prev,
-                                           uint64_t seed, uint32_t local, const float* nu, float& x, float& u, double& ca, float (&delta)[3],
-                                           float& input, uint8_t& fired) {
+__device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
+                                           const float* nu, float& x, float& u, double& ca, float (&delta)[3], float& input, uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
         fired = fired_prev;
@@ -138,9 +138,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
             }
         }
     }
-    // the same Philox draw as the FP64 form, 24 bits of it
-    const u32x4 w = draw(seed, step, local, 0u, STREAM_NOISE, 0u);
-    input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(w.x >> 8), A.noise_mean));
+    input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(k24), A.noise_mean));
 
     float xv = x;
     float uv = u;
@@ -283,16 +281,29 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     ld_f<V>(A.delta[0] + i, d0);
     ld_f<V>(A.delta[1] + i, d1);
     ld_f<V>(A.delta[2] + i, d2);
+    // Background draws: the same Philox blocks as the FP64 form, 24 bits of
+    // each neuron's words; one block serves an even-odd pair of a network, so
+    // a thread with two neurons of a pair draws once.  Draws are keyed on the
+    // network's seed and the neuron's index in its network.
+    uint32_t k24[V];
+    u32x4 blk{ 0u, 0u, 0u, 0u };
+    bool have = false;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const uint64_t seed = MULTI ? A.nets[net[k]].seed : A.seed1;
+        const uint32_t local = MULTI ? i + k - A.nets[net[k]].first : i + k;
+        const bool reuse = have && (local & 1u) && (!MULTI || net[k] == net[k - 1 < 0 ? 0 : k - 1]);
+        if (!reuse) {
+            blk = noise_block(seed, step, local);
+        }
+        have = (local & 1u) == 0u;
+        k24[k] = ((local & 1u) ? blk.z : blk.x) >> 8;
+    }
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         float d[3] = { d0[k], d1[k], d2[k] };
-        if (MULTI) {
-            // draws are keyed on the network's seed and the neuron's index in its network
-            const NetInfo& N = A.nets[net[k]];
-            neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], N.seed, i + k - N.first, N.nu32, x[k], u[k], ca[k], d, input[k], fired[k]);
-        } else {
-            neuron_f32<H>(A, D, step, i + k, en[k] != 0, fp[k], A.seed1, i + k, A.nu1, x[k], u[k], ca[k], d, input[k], fired[k]);
-        }
+        const float* nu = MULTI ? A.nets[net[k]].nu32 : A.nu1;
+        neuron_f32<H>(A, D, i + k, en[k] != 0, fp[k], k24[k], nu, x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     st_f<V>(A.input + i, input);

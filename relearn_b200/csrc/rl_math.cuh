@@ -94,7 +94,7 @@ RL_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
 enum Stream : uint32_t {
     STREAM_BH_PICK = 1,    // Barnes-Hut weighted pick (per descent)
     STREAM_CONNECTOR = 2,  // connector shuffle key (per request)
-    STREAM_NOISE = 3,      // normal background input (per neuron-step)
+    STREAM_NOISE = 3,      // normal background input (per neuron pair and step)
     STREAM_DELETION = 4,   // synapse deletion picks
     STREAM_POISSON = 5,    // Poisson model spike thresholds (per neuron-step)
 };
@@ -367,9 +367,20 @@ RL_HD double normal_quantile(double p) {
 }
 
 // Normal(mean, stddev) background draw for (seed, step, neuron).
+// One Philox block serves the background draws of the neuron pair (2m, 2m + 1)
+// of a network at a step: words (x, y) for the even neuron, (z, w) for the odd
+// one, so that a thread updating a pair draws once.
+RL_HD u32x4 noise_block(uint64_t seed, uint32_t step, uint32_t neuron) {
+    return draw(seed, step, neuron >> 1, 0u, STREAM_NOISE, 0u);
+}
+RL_HD uint64_t noise_bits53(const u32x4& r, uint32_t neuron) {
+    return (neuron & 1u) ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
+}
+
 RL_HD double background_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
-    const u32x4 r = draw(seed, step, neuron, 0u, STREAM_NOISE, 0u);
-    return mean + stddev * normal_quantile(uniform_open01(r));
+    const u32x4 r = noise_block(seed, step, neuron);
+    const double u = ((double)noise_bits53(r, neuron) + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
+    return mean + stddev * normal_quantile(u);
 }
 
 }  // namespace rl
