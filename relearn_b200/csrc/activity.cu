@@ -196,6 +196,7 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
 // persistent shape) each thread strides over the neurons.
 template <int BLOCK, int H, int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
+    pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
         activity_neuron<H, MODEL>(A, D, k, i);
@@ -304,13 +305,13 @@ template <int H, int MODEL>
 void launch_act64_m(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
     switch (v.block) {
         case 128:
-            k_activity<128, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<128, H, MODEL>), 128, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            launch_pdl(&k_activity<128, H, MODEL>, act_grid(c, v, (const void*)&k_activity<128, H, MODEL>), 128, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
             break;
         case 512:
-            k_activity<512, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<512, H, MODEL>), 512, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            launch_pdl(&k_activity<512, H, MODEL>, act_grid(c, v, (const void*)&k_activity<512, H, MODEL>), 512, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
             break;
         default:
-            k_activity<256, H, MODEL><<<act_grid(c, v, (const void*)&k_activity<256, H, MODEL>), 256, 0, c.stream>>>(A, c.act_desc.p, kstep);
+            launch_pdl(&k_activity<256, H, MODEL>, act_grid(c, v, (const void*)&k_activity<256, H, MODEL>), 256, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
             break;
     }
 }
@@ -391,7 +392,6 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     } else {
         launch_act64<0>(c, v, A, kstep);
     }
-    RL_LAUNCH_CHECK();
 }
 
 namespace {

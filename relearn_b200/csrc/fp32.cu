@@ -321,6 +321,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 // resident wave.  The last n % V neurons go one per thread.
 template <int H, int BLOCK, int V, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
+    pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t step = D->base_step + k;
     const uint32_t groups = A.n / V;
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
@@ -1018,10 +1019,11 @@ void f64_from_f32(Ctx& c) {
 template <int H, int BLOCK, int V>
 void launch_act32(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
     if (c.multi()) {
-        k_activity_f32<H, BLOCK, V, true><<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, true>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+        launch_pdl(&k_activity_f32<H, BLOCK, V, true>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, true>), BLOCK, c.stream, A,
+                   (const ActDesc*)c.act_desc.p, kstep);
     } else {
-        k_activity_f32<H, BLOCK, V, false>
-            <<<act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, false>), BLOCK, 0, c.stream>>>(A, c.act_desc.p, kstep);
+        launch_pdl(&k_activity_f32<H, BLOCK, V, false>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, false>), BLOCK, c.stream, A,
+                   (const ActDesc*)c.act_desc.p, kstep);
     }
 }
 
@@ -1113,7 +1115,6 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     } else {
         launch_act32_h<0>(c, v, A, kstep);
     }
-    RL_LAUNCH_CHECK();
 }
 
 void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n) {

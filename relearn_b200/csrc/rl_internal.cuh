@@ -57,6 +57,37 @@ extern thread_local Binding g_bind;
 
 constexpr int kSmCount = 148;
 
+// Programmatic dependent launch: a kernel launched this way may be scheduled
+// while its stream predecessor is still draining (its blocks become resident
+// as the predecessor's last wave leaves the SMs), which hides the launch gap
+// between the short kernels of an activity block.  Such a kernel begins with
+// pdl_wait(), which returns once the predecessor grid has completed and its
+// memory is visible, and then lets its own successor launch.
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RL_CUDA_TRY(cudaLaunchKernelEx(&cfg, kernel, args...));
+    if (g_bind.launches) {
+        ++*g_bind.launches;
+    }
+}
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ void pdl_wait_then_release() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
+
 inline unsigned blocks_for(uint64_t n, unsigned threads) {
     uint64_t b = (n + threads - 1) / threads;
     if (b == 0) {
