@@ -193,8 +193,8 @@ def build_network(n, side, seed, placement):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one activity launch at 1M
-# neurons (ncu --set full, see profiles/): FP64 59.0 + 4.0 MB, FP32 30.0 + 0.1 MB
-PROFILED_TRAFFIC = {0: 63.0e6, 1: 30.1e6}
+# neurons (ncu --set full, see profiles/): FP64 59.0 + 4.2 MB, FP32 30.0 + 0.02 MB
+PROFILED_TRAFFIC = {0: 63.2e6, 1: 30.0e6}
 
 ACT_BYTES_FP32 = 62  # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes input 4 + x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12
 
