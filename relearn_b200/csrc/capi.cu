@@ -324,6 +324,7 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.commit_cnt.alloc(4);
+    RL_CUDA_TRY(cudaMallocHost(&c.h_commit, 4 * sizeof(unsigned long long)));
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
     setup_nets(c, nets, num_nets);
@@ -349,21 +350,33 @@ void plasticity_update(Ctx& c, uint32_t step) {
         // commits go out at once, each skipping itself on the device when an
         // earlier one left deletions, and a single read says where the
         // sequential path has to take over.
-        PhaseScope ps(c, PH_COMMIT);
-        RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 4 * sizeof(unsigned long long), c.stream));
-        for (int t = 0; t < 3; ++t) {
-            launch_commit_guarded(c, t);
+        {
+            PhaseScope ps(c, PH_COMMIT);
+            RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 4 * sizeof(unsigned long long), c.stream));
+            for (int t = 0; t < 3; ++t) {
+                launch_commit_guarded(c, t);
+            }
+            // the same read says whether the search will have anything to do
+            launch_vacant_axon_count(c, c.commit_cnt.p + 3);
+            RL_CUDA_TRY(cudaMemcpyAsync(c.h_commit, c.commit_cnt.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
         }
-        // the same read says whether the search will have anything to do
-        launch_vacant_axon_count(c, c.commit_cnt.p + 3);
-        unsigned long long h[4] = { 0, 0, 0, 0 };
-        RL_CUDA_TRY(cudaMemcpyAsync(h, c.commit_cnt.p, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        // The octree update goes out before the host reads the counts, so that
+        // the GPU works while the host waits; it is correct unless deletions
+        // follow, which change vacant dendrites: then it runs again below
+        // (incrementally: only the leaves the deletions changed).
+        RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
+        {
+            PhaseScope ps(c, PH_TREE_UPDATE);
+            update_tree(c);
+        }
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        const unsigned long long* h = c.h_commit;
         c.stats.bound_to_delete += h[0] + h[1] + h[2];
         const int first = h[0] ? 0 : (h[1] ? 1 : (h[2] ? 2 : 3));
         // deletions change vacant axons: then the search counts them itself
         c.no_searches = first == 3 && h[3] == 0;
         if (first < 3) {
+            PhaseScope ps(c, PH_COMMIT);
             c.stats.synapses_deleted += run_deletion(c, step, first);
             for (int t = first + 1; t < 3; ++t) {
                 if (run_commit(c, t) > 0) {
@@ -371,14 +384,13 @@ void plasticity_update(Ctx& c, uint32_t step) {
                 }
             }
         }
+        if (first < 3) {
+            PhaseScope ps(c, PH_TREE_UPDATE);
+            update_tree(c);
+        }
     }
     // Neurons::create_synapses: search from the committed vacant axons
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));
-    RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
-    {
-        PhaseScope ps(c, PH_TREE_UPDATE);
-        update_tree(c);
-    }
     {
         PhaseScope ps(c, PH_SEARCH);
         if (c.no_searches) {
@@ -657,6 +669,10 @@ void discard(Ctx* c) {
         if (g) {
             cudaGraphExecDestroy(g);
         }
+    }
+    if (c->h_commit) {
+        cudaFreeHost(c->h_commit);
+        c->h_commit = nullptr;
     }
     // device buffers are freed on their streams; the context's own stream
     // goes last

@@ -445,6 +445,7 @@ struct ReduceArgs {
     uint32_t* arrive;
     // incremental update: nodes to recompute, and the leaf counts of the last update
     uint8_t* dirty;
+    uint32_t* level_dirty;  // per level: some node of the level is marked
     uint2* last;
     // leaf counts: vacant dendrites of the neurons that take part
     const uint8_t* enabled;
@@ -465,6 +466,7 @@ struct ReduceArgs {
 // one thread per neuron; a leaf whose vacant counts differ from the last
 // update gets the new counts and marks its parent for recomputation.
 __global__ void k_leaf_update(ReduceArgs A) {
+    pdl_wait_then_release();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) {
         return;
@@ -486,6 +488,7 @@ __global__ void k_leaf_update(ReduceArgs A) {
     const int32_t p = A.parent[leaf];
     if (p >= 0) {
         A.dirty[p] = 1;
+        A.level_dirty[topo_level(A.topo[p].y)] = 1u;
     }
 }
 
@@ -495,12 +498,24 @@ __global__ void k_leaf_update(ReduceArgs A) {
 // octant order as the reference sums them (OctreeNodeUpdater::update_node),
 // and marks its parent.  Recomputing only the nodes above changed leaves gives
 // the same records as recomputing all.  The children of a node are contiguous,
-// so neighbouring threads read neighbouring records.
-__global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
-    const uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= hi || !A.dirty[node]) {
+// so neighbouring threads read neighbouring records.  A level with no marked
+// node (most levels, most updates) returns at once; the grid strides over the
+// level so that such a launch stays a few blocks.
+__device__ __forceinline__ void reduce_node(const ReduceArgs& A, uint32_t node);
+
+__global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi, uint32_t level) {
+    pdl_wait_then_release();
+    if (!A.level_dirty[level]) {
         return;
     }
+    for (uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x; node < hi; node += gridDim.x * blockDim.x) {
+        if (A.dirty[node]) {
+            reduce_node(A, node);
+        }
+    }
+}
+
+__device__ __forceinline__ void reduce_node(const ReduceArgs& A, uint32_t node) {
     A.dirty[node] = 0;
     const uint2 t = A.topo[node];
     const uint32_t mask = topo_mask(t.y);
@@ -545,6 +560,7 @@ __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi) {
     const int32_t p = A.parent[node];
     if (p >= 0) {
         A.dirty[p] = 1;
+        A.level_dirty[topo_level(t.y) - 1u] = 1u;
     }
 }
 
@@ -681,6 +697,7 @@ void build_octree(Ctx& c, const double* h_xyz) {
     T.meta.alloc(m);
     T.dirty.alloc(m);
     RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m, st));
+    T.level_dirty.alloc(kMaxLevels + 2);
     T.last_counts.alloc(n);
     T.first_key.alloc(m);
     T.leaf_of.alloc(n);
@@ -772,6 +789,7 @@ void update_tree(Ctx& c) {
     A.rec1 = T.rec[1].p;
     A.arrive = nullptr;
     A.dirty = T.dirty.p;
+    A.level_dirty = T.level_dirty.p;
     A.last = T.last_counts.p;
     A.enabled = c.nr.enabled.p;
     A.update = c.nr.update.p;
@@ -796,14 +814,15 @@ void update_tree(Ctx& c) {
     auto enqueue = [&](cudaStream_t st, int force) {
         ReduceArgs a = A;
         a.force = force;
-        k_leaf_update<<<blocks_for(n, 256), 256, 0, st>>>(a);
-        RL_LAUNCH_CHECK();
+        RL_CUDA_TRY(cudaMemsetAsync(T.level_dirty.p, 0, T.level_dirty.n * sizeof(uint32_t), st));
+        launch_pdl(&k_leaf_update, blocks_for(n, 256), 256, st, a);
         uint32_t kernels = 1;
+        const unsigned cap = 4u * (unsigned)c.num_sms;
         for (int l = deepest - 1; l >= 0; --l) {
             const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
             if (hi > lo) {
-                k_reduce_level<<<blocks_for(hi - lo, 128), 128, 0, st>>>(a, lo, hi);
-                RL_LAUNCH_CHECK();
+                const unsigned blocks = blocks_for(hi - lo, 128);
+                launch_pdl(&k_reduce_level, blocks < cap ? blocks : cap, 128, st, a, lo, hi, (uint32_t)l);
                 ++kernels;
             }
         }

@@ -45,6 +45,7 @@ struct Tree {
     DBuf<uint32_t> morton;     // Morton rank -> neuron
     std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
     DBuf<uint8_t> dirty;        // nodes to recompute in the running update
+    DBuf<uint32_t> level_dirty; // per level: a node of the level is marked
     DBuf<uint2> last_counts;    // per neuron: leaf counts (exc, inh) of the last update
     bool force_full = true;     // next update takes every leaf as changed
     bool recq_valid = false;    // fixed-point records match the FP64 records
@@ -286,6 +287,7 @@ struct Ctx {
     DBuf<uint32_t> err;       // device error word
     DBuf<uint64_t> counters;  // device counters
     DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update, then vacant axons
+    unsigned long long* h_commit = nullptr;  // pinned host copy of commit_cnt (read without blocking the enqueue)
     bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
