@@ -45,6 +45,15 @@ struct ActArgs {
     double eta[3];
     const NetInfo* nets;
     const uint16_t* net_of;
+    // a context with one network: its seed and growth rates (the kernel then
+    // reads no network table)
+    uint64_t seed1;
+    double nu1[3];
+    // one target calcium for every neuron: the growth curves' constants,
+    // computed on the host with the same operations as growth_curve
+    int uniform_target;
+    int flat_u[3];
+    double xi_u[3], zeta_u[3];
     // other neuron models (neurons/models/*)
     double p_x0, p_tau_inv;  // Poisson
     uint32_t p_refractory;
@@ -65,9 +74,21 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
+// gaussian_growth_curve with xi and zeta of a uniform target (growth_curve's
+// own operations, done once on the host).
+__device__ __forceinline__ double growth_curve_pre(double current, double eta, int flat, double xi, double zeta) {
+    if (flat) {
+        return current == eta ? 0.0 : -1.0;
+    }
+    const double diff = current - xi;
+    const double quot = diff / zeta;
+    const double prod = quot * quot;
+    return (2.0 * rl_exp(-prod)) - 1.0;
+}
+
 // H > 0: h_model and h_calcium are both H, fixed at compile time.  MODEL is
-// the neuron model (RL_MODEL_*).
-template <int H, int MODEL>
+// the neuron model (RL_MODEL_*); MULTI: several networks in the context.
+template <int H, int MODEL, bool MULTI>
 __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
     const uint32_t step = D->base_step + k;
     if (!A.enabled[i]) {
@@ -91,10 +112,18 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
         }
     }
     // draws are keyed on the network's seed and the neuron's index in its network
-    const NetInfo& N = A.nets[A.net_of[i]];
+    uint64_t seed = A.seed1;
+    uint32_t local = i;
+    const double* nu = A.nu1;
+    if (MULTI) {
+        const NetInfo& N = A.nets[A.net_of[i]];
+        seed = N.seed;
+        local = i - N.first;
+        nu = N.nu;
+    }
     double input = 0.0;
     input += (double)isum * A.conductance;
-    input += background_normal(N.seed, step, i - N.first, A.noise_mean, A.noise_stddev);
+    input += background_normal(seed, step, local, A.noise_mean, A.noise_stddev);
     A.input[i] = input;
 
     double xv = A.x[i];
@@ -123,7 +152,7 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
             xv += ((A.p_x0 - xv) * A.p_tau_inv + input) * A.scale_m;
         }
         if (uv == 0.0) {
-            const double threshold = uniform01(draw(N.seed, step, i - N.first, 0u, STREAM_POISSON, 0u));
+            const double threshold = uniform01(draw(seed, step, local, 0u, STREAM_POISSON, 0u));
             if (xv >= threshold) {
                 spiked = 1;
                 uv = (double)A.p_refractory;
@@ -181,25 +210,33 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
     }
     A.calcium[i] = ca;
 
-    const double tgt = A.target[i];
     double* deltas[3] = { A.delta0, A.delta1, A.delta2 };
+    if (A.uniform_target) {
 #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const double eta = A.eta[t];
-        const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
-        const double inc = growth_curve(ca, eta, eps) * N.nu[t];
-        deltas[t][i] = deltas[t][i] + inc;
+        for (int t = 0; t < 3; ++t) {
+            const double inc = growth_curve_pre(ca, A.eta[t], A.flat_u[t], A.xi_u[t], A.zeta_u[t]) * nu[t];
+            deltas[t][i] = deltas[t][i] + inc;
+        }
+    } else {
+        const double tgt = A.target[i];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const double eta = A.eta[t];
+            const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
+            const double inc = growth_curve(ca, eta, eps) * nu[t];
+            deltas[t][i] = deltas[t][i] + inc;
+        }
     }
 }
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
 // persistent shape) each thread strides over the neurons.
-template <int BLOCK, int H, int MODEL>
+template <int BLOCK, int H, int MODEL, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
     pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        activity_neuron<H, MODEL>(A, D, k, i);
+        activity_neuron<H, MODEL, MULTI>(A, D, k, i);
     }
 }
 
@@ -301,17 +338,28 @@ void launch_vacant_axon_count(Ctx& c, unsigned long long* out) {
     RL_LAUNCH_CHECK();
 }
 
+template <int BLOCK, int H, int MODEL>
+void launch_act64_b(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+    if (c.multi()) {
+        launch_pdl(&k_activity<BLOCK, H, MODEL, true>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, true>), BLOCK, c.stream, A,
+                   (const ActDesc*)c.act_desc.p, kstep);
+    } else {
+        launch_pdl(&k_activity<BLOCK, H, MODEL, false>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, false>), BLOCK, c.stream, A,
+                   (const ActDesc*)c.act_desc.p, kstep);
+    }
+}
+
 template <int H, int MODEL>
 void launch_act64_m(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
     switch (v.block) {
         case 128:
-            launch_pdl(&k_activity<128, H, MODEL>, act_grid(c, v, (const void*)&k_activity<128, H, MODEL>), 128, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
+            launch_act64_b<128, H, MODEL>(c, v, A, kstep);
             break;
         case 512:
-            launch_pdl(&k_activity<512, H, MODEL>, act_grid(c, v, (const void*)&k_activity<512, H, MODEL>), 512, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
+            launch_act64_b<512, H, MODEL>(c, v, A, kstep);
             break;
         default:
-            launch_pdl(&k_activity<256, H, MODEL>, act_grid(c, v, (const void*)&k_activity<256, H, MODEL>), 256, c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
+            launch_act64_b<256, H, MODEL>(c, v, A, kstep);
             break;
     }
 }
@@ -371,6 +419,19 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
+    A.seed1 = c.nets[0].seed;
+    A.uniform_target = c.target_uniform ? 1 : 0;
+    const double factor_inv = 1.0 / 1.6651092223153955127063292897904020952611777045288814583336582344;
+    for (int t = 0; t < 3; ++t) {
+        A.nu1[t] = c.nets[0].nu[t];
+        // gaussian_growth_curve's constants for the one target, in its operation order
+        const double eta = k.min_calcium[t];
+        const double tgt = k.target_calcium;
+        const double eps = tgt < eta ? eta : tgt;
+        A.flat_u[t] = eta == eps ? 1 : 0;
+        A.xi_u[t] = (eta + eps) * 0.5;
+        A.zeta_u[t] = (eta - eps) * factor_inv;
+    }
     A.p_x0 = k.poisson_x0;
     A.p_tau_inv = 1.0 / k.poisson_tau_x;
     A.p_refractory = k.poisson_refractory;

@@ -852,11 +852,14 @@ rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const doub
 rl_status rl_set_target_calcium(void* ctx, const double* target) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(target != nullptr, RL_ERR_INVALID, "null target");
-        if (rl::is_fp32(c)) {
-            // the FP32 kernel folds one target into its growth-curve constants
-            for (uint32_t i = 1; i < c.n; ++i) {
-                RL_CHECK(target[i] == target[0], RL_ERR_UNSUPPORTED, "the FP32 form runs one target calcium for all neurons");
-            }
+        bool same = true;
+        for (uint32_t i = 1; i < c.n && same; ++i) {
+            same = target[i] == target[0];
+        }
+        // the FP32 kernel folds one target into its growth-curve constants
+        RL_CHECK(same || !rl::is_fp32(c), RL_ERR_UNSUPPORTED, "the FP32 form runs one target calcium for all neurons");
+        c.target_uniform = same;
+        if (same && c.n > 0) {
             c.cfg.target_calcium = target[0];
         }
         rl::drop_activity_graphs(c);  // captured intervals hold the growth-curve constants

@@ -288,6 +288,7 @@ struct Ctx {
     DBuf<uint64_t> counters;  // device counters
     DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update, then vacant axons
     unsigned long long* h_commit = nullptr;  // pinned host copy of commit_cnt (read without blocking the enqueue)
+    bool target_uniform = true;  // every neuron has cfg.target_calcium as its target
     bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
