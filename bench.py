@@ -343,6 +343,20 @@ def run_b200(args, world, rank, local):
                 other["bh_search"]["vs_fp64_drop_in"] = bh32["value"] / bh["value"]
         o["net"].close()
 
+    # the second placement of the same workload: a 64-component Gaussian
+    # mixture (component std 200 um) that unbalances the octree
+    mixture = None
+    if not args.skip_mixture and args.placement == "uniform":
+        mparams, mpos, msig = build_network(n, side, args.seed + rank, "mixture")
+        mparams["device"] = local
+        mm = measure_form(args, 0, dev, stream, world, mpos, msig, mparams)
+        mixture = {"placement": "64-component Gaussian mixture, component std 200 um, centres uniform in the cube", "precision": "fp64",
+                   "value": mm["value"], "unit": "neuron-steps/s", "ms_per_step": mm["total_ms"] / args.steps, "roofline": mm["roofline"],
+                   "phases_ms": mm["phases"], "octree": {"nodes": mm["net"].tree_info()[0], "max_level": mm["net"].tree_info()[1]}}
+        if not args.skip_bh:
+            mixture["bh_search"] = bh_snapshot(mm["net"], n, stream, mm["step"])
+        mm["net"].close()
+
     ens = None
     if not args.skip_ensemble:
         ens = ensemble_figure(args, dev, stream, world, rank)
@@ -387,6 +401,8 @@ def run_b200(args, world, rank, local):
         line["bh_search"] = bh
     if other:
         line["fp32_form"] = other
+    if mixture:
+        line["mixture"] = mixture
     if ens:
         line["ensemble"] = ens
     if prec:
@@ -765,6 +781,7 @@ def main():
     ap.add_argument("--skip-fp32", action="store_true", help="do not measure the FP32 form beside the FP64 drop-in")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64", help="form of the headline figure")
     ap.add_argument("--skip-ensemble", action="store_true", help="do not measure the batched form (128 networks)")
+    ap.add_argument("--skip-mixture", action="store_true", help="do not measure the Gaussian-mixture placement beside the uniform one")
     ap.add_argument("--ensemble-networks", type=int, default=128)
     ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
     ap.add_argument("--skip-serve", action="store_true", help="do not measure the serving form")
