@@ -79,7 +79,7 @@ void check_device_error(Ctx& c, const char* phase) {
         st = RL_ERR_INVALID;
     }
     if (h & DERR_STACK) {
-        msg += " [traversal stack overflow]";
+        msg += " [octree walk deeper than its bound]";
         st = RL_ERR_OVERFLOW;
     }
     if (h & DERR_WALK) {

@@ -101,7 +101,7 @@ enum DeviceError : uint32_t {
     DERR_NONE = 0,
     DERR_OUT_OF_BOX = 1u << 0,      // a position outside the root cell
     DERR_DUPLICATE = 1u << 1,       // two positions share all key levels
-    DERR_STACK = 1u << 2,           // traversal stack overflow
+    DERR_STACK = 1u << 2,           // a walk or descent ran past its depth bound
     DERR_NO_CROSSING = 1u << 3,     // pick scan found no crossing
     DERR_CAPACITY = 1u << 4,        // a device buffer was too small
     DERR_CONNECT = 1u << 5,         // connector bookkeeping underflow
