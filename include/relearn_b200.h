@@ -250,6 +250,19 @@ RL_API rl_status rl_get_elements(void* ctx, int type, double* grown, double* del
 RL_API rl_status rl_set_neurons(void* ctx, const double* x, const double* u, const double* calcium, const uint8_t* fired);
 RL_API rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8_t* fired, double* input);
 
+/* Asynchronous read of calcium and fired flags (either may be NULL), for
+ * monitoring a running simulation without stalling it: the state is copied to
+ * a device staging buffer in order with the context's work, and from there to
+ * the caller's buffers on a copy stream of the context, so the copy overlaps
+ * whatever the context runs next.  The buffers receive the values as of the
+ * call (after the work issued before it) and must stay valid until
+ * rl_snapshot_wait returns; pinned host memory makes the copy asynchronous.
+ * Two snapshots may be in flight.  Serves what the reference's NeuronMonitor
+ * records between steps (sim/Simulation.cpp:428-430) without a host stall. */
+RL_API rl_status rl_snapshot_neurons(void* ctx, double* calcium, uint8_t* fired);
+/* Waits until every snapshot issued so far has landed in host memory. */
+RL_API rl_status rl_snapshot_wait(void* ctx);
+
 /* Target calcium per neuron (the target function CalciumIO builds from a
  * --file-calcium, io/CalciumIO.cpp:27-130; otherwise every neuron has
  * rl_config.target_calcium).  The FP32 form runs one target for all neurons of

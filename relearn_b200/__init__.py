@@ -168,7 +168,7 @@ ABI_FUNCTIONS = [
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
     "rl_candidate_weights", "rl_set_graphs", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
     "rl_serve_fetch", "rl_serve_load", "rl_serve_destroy", "rl_autotune", "rl_get_tuning", "rl_set_tuning",
-    "rl_set_target_calcium", "rl_get_target_calcium",
+    "rl_set_target_calcium", "rl_get_target_calcium", "rl_snapshot_neurons", "rl_snapshot_wait",
 ]
 PHASES = ["activity_kernel", "commit", "tree_update", "search_kernel", "search", "connector", "graph"]
 
@@ -222,6 +222,10 @@ def load_library(path: str = LIB_PATH):
     L.rl_get_neurons.argtypes = [vp] * 6
     L.rl_set_enabled.restype = st
     L.rl_set_enabled.argtypes = [vp, vp]
+    L.rl_snapshot_neurons.restype = st
+    L.rl_snapshot_neurons.argtypes = [vp, vp, vp]
+    L.rl_snapshot_wait.restype = st
+    L.rl_snapshot_wait.argtypes = [vp]
     L.rl_add_edges.restype = st
     L.rl_add_edges.argtypes = [vp, u64, vp, vp, vp]
     L.rl_get_edges.restype = st
@@ -455,6 +459,18 @@ class Network:
     def set_enabled(self, enabled):
         e = np.ascontiguousarray(enabled, np.uint8)
         self._check(self.lib.rl_set_enabled(self.h, _p(e)))
+
+    def snapshot_neurons(self, calcium=None, fired=None):
+        """Start an asynchronous copy of calcium (float64) and fired flags
+        (uint8) into the given arrays (pinned memory keeps it asynchronous);
+        they hold the values once snapshot_wait returns."""
+        for a, dt in ((calcium, np.float64), (fired, np.uint8)):
+            if a is not None and (a.dtype != dt or not a.flags["C_CONTIGUOUS"] or a.size < self.n):
+                raise ValueError(f"snapshot buffers must be contiguous {np.dtype(dt).name} arrays of at least {self.n} entries")
+        self._check(self.lib.rl_snapshot_neurons(self.h, _p(calcium) if calcium is not None else None, _p(fired) if fired is not None else None))
+
+    def snapshot_wait(self):
+        self._check(self.lib.rl_snapshot_wait(self.h))
 
     def add_edges(self, target, source, weight):
         t = np.ascontiguousarray(target, np.uint32); s = np.ascontiguousarray(source, np.uint32)

@@ -653,6 +653,9 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     }
     c.nr.cur ^= (int)(nsteps & 1u);
     c.stats.activity_steps += nsteps;
+    if (c.copy_stream) {
+        issue_snapshots(c);  // the block is queued: snapshot copies now overlap it
+    }
 }
 
 void launch_commit_guarded(Ctx& c, int type) {

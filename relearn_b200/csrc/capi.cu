@@ -650,9 +650,62 @@ rl_status rl_ctx_destroy(void* ctx) {
 
 namespace rl {
 
+void ensure_copy_stream(Ctx& c) {
+    if (c.copy_stream) {
+        return;
+    }
+    RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.upload_stream, cudaStreamNonBlocking));
+    RL_CUDA_TRY(cudaEventCreateWithFlags(&c.upload_done, cudaEventDisableTiming));
+    RL_CUDA_TRY(cudaEventCreateWithFlags(&c.stage_free, cudaEventDisableTiming));
+    for (auto& s : c.snap) {
+        RL_CUDA_TRY(cudaEventCreateWithFlags(&s.staged, cudaEventDisableTiming));
+        RL_CUDA_TRY(cudaEventCreateWithFlags(&s.landed, cudaEventDisableTiming));
+    }
+}
+
+void issue_snapshots(Ctx& c) {
+    for (int k = 0; k < 2; ++k) {
+        // the older slot first, so the host copies land in call order
+        Ctx::SnapSlot& s = c.snap[(c.snap_next + k) & 1];
+        if (!s.pending || s.issued) {
+            continue;
+        }
+        RL_CUDA_TRY(cudaStreamWaitEvent(c.copy_stream, s.staged, 0));
+        if (s.host_calcium) {
+            RL_CUDA_TRY(cudaMemcpyAsync(s.host_calcium, s.calcium.p, c.n * sizeof(double), cudaMemcpyDeviceToHost, c.copy_stream));
+        }
+        if (s.host_fired) {
+            RL_CUDA_TRY(cudaMemcpyAsync(s.host_fired, s.fired.p, c.n, cudaMemcpyDeviceToHost, c.copy_stream));
+        }
+        RL_CUDA_TRY(cudaEventRecord(s.landed, c.copy_stream));
+        s.issued = true;
+    }
+}
+
 void discard(Ctx* c) {
     cudaSetDevice(c->device);
+    if (c->copy_stream) {
+        try {
+            issue_snapshots(*c);  // buffers handed over must still be written
+        } catch (...) {
+        }
+    }
     g_bind = Binding{ c->stream, &c->launches, &c->device_bytes, &c->device_peak };
+    if (c->copy_stream) {
+        // snapshots in flight read the staging buffers: let them land first
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamSynchronize(c->upload_stream);
+        cudaStreamDestroy(c->copy_stream);
+        cudaStreamDestroy(c->upload_stream);
+        c->copy_stream = nullptr;
+        c->upload_stream = nullptr;
+        for (cudaEvent_t e : { c->upload_done, c->stage_free, c->snap[0].staged, c->snap[0].landed, c->snap[1].staged, c->snap[1].landed }) {
+            if (e) {
+                cudaEventDestroy(e);
+            }
+        }
+    }
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
     }
@@ -893,8 +946,65 @@ rl_status rl_get_neurons(void* ctx, double* x, double* u, double* calcium, uint8
 rl_status rl_set_enabled(void* ctx, const uint8_t* enabled) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(enabled != nullptr, RL_ERR_INVALID, "enabled flags are required");
-        rl::upload(c.nr.enabled, enabled, c.n, c.stream);
-        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        // host -> staging on the upload stream (the caller's buffer is free when
+        // that copy has landed), staging -> state in order on the context's
+        // stream: the upload overlaps the work already queued there
+        rl::ensure_copy_stream(c);
+        if (c.enabled_stage.n < c.n) {
+            c.enabled_stage.ensure(c.n);
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));  // the allocation is stream-ordered
+        }
+        if (c.stage_used) {
+            RL_CUDA_TRY(cudaStreamWaitEvent(c.upload_stream, c.stage_free, 0));
+        }
+        RL_CUDA_TRY(cudaMemcpyAsync(c.enabled_stage.p, enabled, c.n, cudaMemcpyHostToDevice, c.upload_stream));
+        RL_CUDA_TRY(cudaEventRecord(c.upload_done, c.upload_stream));
+        RL_CUDA_TRY(cudaEventSynchronize(c.upload_done));
+        RL_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.upload_done, 0));
+        RL_CUDA_TRY(cudaMemcpyAsync(c.nr.enabled.p, c.enabled_stage.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
+        RL_CUDA_TRY(cudaEventRecord(c.stage_free, c.stream));
+        c.stage_used = true;
+    });
+}
+
+rl_status rl_snapshot_neurons(void* ctx, double* calcium, uint8_t* fired) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(calcium != nullptr || fired != nullptr, RL_ERR_INVALID, "no output buffer");
+        rl::ensure_copy_stream(c);
+        Ctx::SnapSlot& s = c.snap[c.snap_next];
+        c.snap_next ^= 1;
+        if (s.calcium.n < c.n) {
+            s.calcium.ensure(c.n);
+            s.fired.ensure(c.n);
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));  // the allocation is stream-ordered
+        }
+        if (s.pending) {
+            rl::issue_snapshots(c);
+            RL_CUDA_TRY(cudaStreamWaitEvent(c.stream, s.landed, 0));  // the slot's last copy has left it
+        }
+        if (calcium) {
+            RL_CUDA_TRY(cudaMemcpyAsync(s.calcium.p, c.nr.calcium.p, c.n * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+        }
+        if (fired) {
+            RL_CUDA_TRY(cudaMemcpyAsync(s.fired.p, c.nr.fired[c.nr.cur].p, c.n, cudaMemcpyDeviceToDevice, c.stream));
+        }
+        RL_CUDA_TRY(cudaEventRecord(s.staged, c.stream));
+        s.host_calcium = calcium;
+        s.host_fired = fired;
+        s.pending = true;
+        s.issued = false;  // the host copy goes out with the next work
+    });
+}
+
+rl_status rl_snapshot_wait(void* ctx) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        rl::issue_snapshots(c);
+        for (auto& s : c.snap) {
+            if (s.pending) {
+                RL_CUDA_TRY(cudaEventSynchronize(s.landed));
+                s.pending = false;
+            }
+        }
     });
 }
 

@@ -289,6 +289,28 @@ struct Ctx {
     DBuf<unsigned long long> commit_cnt;  // bound elements to delete per element type of an update, then vacant axons
     unsigned long long* h_commit = nullptr;  // pinned host copy of commit_cnt (read without blocking the enqueue)
     bool target_uniform = true;  // every neuron has cfg.target_calcium as its target
+    // Host transfers that overlap the work on the context's stream: uploads
+    // of enabled flags and snapshots of calcium and fired flags go through
+    // device staging buffers and copy streams of their own (one per
+    // direction, so that an upload never queues behind a snapshot).
+    cudaStream_t copy_stream = nullptr;    // snapshots (device -> host)
+    cudaStream_t upload_stream = nullptr;  // enabled flags (host -> device)
+    DBuf<uint8_t> enabled_stage;
+    cudaEvent_t upload_done = nullptr;   // the last upload reached the staging buffer
+    cudaEvent_t stage_free = nullptr;    // the context's stream has consumed it
+    bool stage_used = false;
+    struct SnapSlot {
+        DBuf<double> calcium;
+        DBuf<uint8_t> fired;
+        cudaEvent_t staged = nullptr;  // state copied into the slot (context's stream)
+        cudaEvent_t landed = nullptr;  // slot copied to the host (copy stream)
+        double* host_calcium = nullptr;
+        uint8_t* host_fired = nullptr;
+        bool pending = false;  // not waited for yet
+        bool issued = false;   // the copy to the host is on the copy stream
+    };
+    SnapSlot snap[2];
+    int snap_next = 0;
     bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
@@ -348,6 +370,11 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
 void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps);
 // Frees a context and everything it holds (after its stream has drained).
 void discard(Ctx* c);
+void ensure_copy_stream(Ctx& c);
+// Puts the host copies of staged snapshots on the copy stream.  Called after
+// the next work has been queued on the context's stream, so that the copies
+// overlap it (and do not hold up an upload issued in between).
+void issue_snapshots(Ctx& c);
 uint64_t run_commit(Ctx& c, int type);
 // Commit of `type` that does nothing when an earlier type of the same update
 // (its count in commit_cnt) left bound elements to delete; counts into
