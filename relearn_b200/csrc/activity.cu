@@ -86,19 +86,35 @@ __device__ __forceinline__ double growth_curve_pre(double current, double eta, i
     return (2.0 * rl_exp(-prod)) - 1.0;
 }
 
-// H > 0: h_model and h_calcium are both H, fixed at compile time.  MODEL is
-// the neuron model (RL_MODEL_*); MULTI: several networks in the context.
-template <int H, int MODEL, bool MULTI>
-__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t i) {
-    const uint32_t step = D->base_step + k;
-    if (!A.enabled[i]) {
-        A.input[i] = 0.0;
-        A.fired_cur[i] = A.fired_prev[i];
-        A.delta0[i] = A.delta0[i] + 0.0;
-        A.delta1[i] = A.delta1[i] + 0.0;
-        A.delta2[i] = A.delta2[i] + 0.0;
-        return;
+// The network of neuron i: draws are keyed on the network's seed and the
+// neuron's index in its network.
+template <bool MULTI>
+__device__ __forceinline__ void neuron_net(const ActArgs& A, uint32_t i, uint64_t& seed, uint32_t& local, const double*& nu) {
+    seed = A.seed1;
+    local = i;
+    nu = A.nu1;
+    if (MULTI) {
+        const NetInfo& N = A.nets[A.net_of[i]];
+        seed = N.seed;
+        local = i - N.first;
+        nu = N.nu;
     }
+}
+
+__device__ __forceinline__ void disabled_neuron(const ActArgs& A, uint32_t i) {
+    A.input[i] = 0.0;
+    A.fired_cur[i] = A.fired_prev[i];
+    A.delta0[i] = A.delta0[i] + 0.0;
+    A.delta1[i] = A.delta1[i] + 0.0;
+    A.delta2[i] = A.delta2[i] + 0.0;
+}
+
+// One enabled neuron's step.  H > 0: h_model and h_calcium are both H, fixed
+// at compile time.  MODEL is the neuron model (RL_MODEL_*).  `z` is the
+// neuron's standard normal draw of this step.
+template <int H, int MODEL>
+__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, uint64_t seed,
+                                                uint32_t local, const double* nu, double z) {
     long long isum = 0;
     if (D->has_edges) {
         const uint32_t* __restrict__ off = D->off;
@@ -111,19 +127,9 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
             }
         }
     }
-    // draws are keyed on the network's seed and the neuron's index in its network
-    uint64_t seed = A.seed1;
-    uint32_t local = i;
-    const double* nu = A.nu1;
-    if (MULTI) {
-        const NetInfo& N = A.nets[A.net_of[i]];
-        seed = N.seed;
-        local = i - N.first;
-        nu = N.nu;
-    }
     double input = 0.0;
     input += (double)isum * A.conductance;
-    input += background_normal(seed, step, local, A.noise_mean, A.noise_stddev);
+    input += A.noise_mean + A.noise_stddev * z;  // NormalActivityInputCPU's draw
     A.input[i] = input;
 
     double xv = A.x[i];
@@ -231,12 +237,69 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
 // persistent shape) each thread strides over the neurons.
+// The background draw's tail piece (about 15 % of the draws, but some lane
+// of nearly every warp) is run for the whole block together: lanes whose
+// uniform falls in the tails queue it in shared memory, the first warps of the
+// block evaluate the queue at full width, and each lane takes its value back.
+// The same function as the per-lane evaluation, so the same bits.  The loop
+// over a block's neurons has the same trip count in every thread (the block
+// synchronises inside it).
 template <int BLOCK, int H, int MODEL, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
+    __shared__ double s_p[BLOCK];
+    __shared__ double s_z[BLOCK];
+    __shared__ uint16_t s_who[BLOCK];
+    __shared__ uint32_t s_cnt[2];
     pdl_wait_then_release();  // every input is the previous step's output
+    const uint32_t step = D->base_step + k;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (threadIdx.x < 2) {
+        s_cnt[threadIdx.x] = 0u;
+    }
+    __syncthreads();
     const uint32_t stride = gridDim.x * BLOCK;
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        activity_neuron<H, MODEL, MULTI>(A, D, k, i);
+    uint32_t parity = 0;
+    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride, parity ^= 1u) {
+        const uint32_t i = base + threadIdx.x;
+        const bool on = i < A.n && A.enabled[i];
+        uint64_t seed = 0;
+        uint32_t local = 0;
+        const double* nu = nullptr;
+        double p = 0.5;
+        if (on) {
+            neuron_net<MULTI>(A, i, seed, local, nu);
+            p = noise_uniform(seed, step, local);
+        }
+        const bool tail = on && normal_in_tail(p);
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
+        uint32_t first = 0;
+        if (lane == 0 && mask) {
+            first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
+        }
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        if (tail) {
+            const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+            s_p[slot] = p;
+            s_who[slot] = (uint16_t)threadIdx.x;
+        }
+        double z = on && !tail ? normal_quantile_central(p) : 0.0;
+        __syncthreads();
+        const uint32_t cnt = s_cnt[parity];
+        for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
+            s_z[s_who[q]] = normal_quantile_tail(s_p[q]);
+        }
+        if (threadIdx.x == 0) {
+            s_cnt[parity ^ 1u] = 0u;  // the next round's counter; nobody reads it before the barrier below
+        }
+        __syncthreads();
+        if (tail) {
+            z = s_z[threadIdx.x];
+        }
+        if (on) {
+            activity_neuron<H, MODEL>(A, D, step, i, seed, local, nu, z);
+        } else if (i < A.n) {
+            disabled_neuron(A, i);
+        }
     }
 }
 

@@ -298,10 +298,17 @@ RL_HD double next_up_eps(double total) {
 }
 
 // ------------------------------------------------------ normal quantile
-// AS241 / PPND16: standard normal quantile for p in (0, 1).
-RL_HD double normal_quantile(double p) {
+// AS241 / PPND16: standard normal quantile for p in (0, 1), in two pieces:
+// the central rational function for |p - 0.5| <= 0.425 and the tails.  A
+// kernel that draws for many neurons runs the tail piece for the few that need
+// it together (it holds a log, a square root and two divisions).
+RL_HD bool normal_in_tail(double p) {
+    return !(fabs(p - 0.5) <= 0.425);
+}
+
+RL_HD double normal_quantile_central(double p) {
     const double q = p - 0.5;
-    if (fabs(q) <= 0.425) {
+    {
         const double r = 0.180625 - q * q;
         double num = 2.5090809287301226727e+3;
         num = rl_fma(num, r, 3.3430575583588128105e+4);
@@ -321,6 +328,10 @@ RL_HD double normal_quantile(double p) {
         den = rl_fma(den, r, 1.0);
         return (num * q) / den;
     }
+}
+
+RL_HD double normal_quantile_tail(double p) {
+    const double q = p - 0.5;
     double r = q < 0.0 ? p : 1.0 - p;
     r = sqrt(-rl_log(r));
     double num;
@@ -366,6 +377,10 @@ RL_HD double normal_quantile(double p) {
     return q < 0.0 ? -x : x;
 }
 
+RL_HD double normal_quantile(double p) {
+    return normal_in_tail(p) ? normal_quantile_tail(p) : normal_quantile_central(p);
+}
+
 // Normal(mean, stddev) background draw for (seed, step, neuron).
 // One Philox block serves the background draws of the neuron pair (2m, 2m + 1)
 // of a network at a step: words (x, y) for the even neuron, (z, w) for the odd
@@ -377,10 +392,14 @@ RL_HD uint64_t noise_bits53(const u32x4& r, uint32_t neuron) {
     return (neuron & 1u) ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
 }
 
-RL_HD double background_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
+// The open-interval uniform of a neuron's background draw.
+RL_HD double noise_uniform(uint64_t seed, uint32_t step, uint32_t neuron) {
     const u32x4 r = noise_block(seed, step, neuron);
-    const double u = ((double)noise_bits53(r, neuron) + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
-    return mean + stddev * normal_quantile(u);
+    return ((double)noise_bits53(r, neuron) + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
+}
+
+RL_HD double background_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
+    return mean + stddev * normal_quantile(noise_uniform(seed, step, neuron));
 }
 
 }  // namespace rl
