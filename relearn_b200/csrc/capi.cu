@@ -1214,6 +1214,14 @@ rl_status rl_get_stats(void* ctx, rl_stats* out) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(out != nullptr, RL_ERR_INVALID, "null output");
         *out = c.stats;
+        if (c.tree.level_runs.p) {
+            // level reductions the captured octree updates ran (conditional graph node)
+            unsigned long long runs = 0;
+            RL_CUDA_TRY(cudaMemcpyAsync(&runs, c.tree.level_runs.p, sizeof(runs), cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            c.launches += runs - c.tree.level_runs_seen;
+            c.tree.level_runs_seen = runs;
+        }
         out->gpu_launches = c.launches;
         out->num_nodes = c.tree.num_nodes;
         out->max_level = c.tree.max_level;

@@ -460,6 +460,11 @@ struct ReduceArgs {
     const uint32_t* morton;
     const uint16_t* net_of;
     const NetInfo* nets;
+    // captured update: the leaf pass switches the level reductions on
+    // (conditional graph node) and each level launch counts itself
+    int has_cond;
+    cudaGraphConditionalHandle cond;
+    unsigned long long* level_runs;
 };
 
 // Leaf pass of the incremental update (OctreeAlgorithm::update_leaf_nodes):
@@ -489,6 +494,9 @@ __global__ void k_leaf_update(ReduceArgs A) {
     if (p >= 0) {
         A.dirty[p] = 1;
         A.level_dirty[topo_level(A.topo[p].y)] = 1u;
+        if (A.has_cond) {
+            cudaGraphSetConditional(A.cond, 1u);  // some level has work: run the reductions
+        }
     }
 }
 
@@ -505,6 +513,9 @@ __device__ __forceinline__ void reduce_node(const ReduceArgs& A, uint32_t node);
 
 __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi, uint32_t level) {
     pdl_wait_then_release();
+    if (A.level_runs && blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(A.level_runs, 1ull);
+    }
     if (!A.level_dirty[level]) {
         return;
     }
@@ -698,6 +709,9 @@ void build_octree(Ctx& c, const double* h_xyz) {
     T.dirty.alloc(m);
     RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m, st));
     T.level_dirty.alloc(kMaxLevels + 2);
+    T.level_runs.alloc(1);
+    RL_CUDA_TRY(cudaMemsetAsync(T.level_runs.p, 0, sizeof(unsigned long long), st));
+    T.level_runs_seen = 0;
     T.last_counts.alloc(n);
     T.first_key.alloc(m);
     T.leaf_of.alloc(n);
@@ -811,12 +825,15 @@ void update_tree(Ctx& c) {
     while (deepest > 0 && T.level_off[deepest + 1] == T.level_off[deepest]) {
         --deepest;
     }
-    auto enqueue = [&](cudaStream_t st, int force) {
-        ReduceArgs a = A;
-        a.force = force;
+    A.has_cond = 0;
+    A.cond = 0;
+    A.level_runs = nullptr;
+    auto enqueue_leaves = [&](cudaStream_t st, const ReduceArgs& a) {
         RL_CUDA_TRY(cudaMemsetAsync(T.level_dirty.p, 0, T.level_dirty.n * sizeof(uint32_t), st));
         launch_pdl(&k_leaf_update, blocks_for(n, 256), 256, st, a);
-        uint32_t kernels = 1;
+    };
+    auto enqueue_levels = [&](cudaStream_t st, const ReduceArgs& a) {
+        uint32_t kernels = 0;
         const unsigned cap = 4u * (unsigned)c.num_sms;
         for (int l = deepest - 1; l >= 0; --l) {
             const uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
@@ -833,31 +850,68 @@ void update_tree(Ctx& c) {
     const int force = T.force_full ? 1 : 0;
     T.force_full = false;
     if (force || !c.use_graphs || c.stream == nullptr || c.capturing) {
-        enqueue(c.stream, force);
+        ReduceArgs a = A;
+        a.force = force;
+        enqueue_leaves(c.stream, a);
+        enqueue_levels(c.stream, a);
         return;
     }
     if (T.update_graph != nullptr && keep_q != T.graph_keeps_q) {
         T.drop_graph();
     }
-    // the launches depend only on the octree's shape: captured once per build
+    // The launches depend only on the octree's shape: captured once per build,
+    // as the leaf pass followed by a conditional node whose body holds the
+    // level reductions.  The leaf pass sets the condition when it changes a
+    // leaf, so an update that changes none (most of them in a long run) ends
+    // after one kernel.  The level launches count themselves on the device.
     if (T.update_graph == nullptr) {
         T.graph_keeps_q = keep_q;
         const uint64_t launches = c.launches;
         cudaGraph_t gr = nullptr;
-        RL_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-        c.capturing = true;
+        RL_CUDA_TRY(cudaGraphCreate(&gr, 0));
+        cudaGraphConditionalHandle cond = 0;
+        ReduceArgs a = A;
+        a.force = 0;
+        bool capturing = false;
         try {
-            T.update_graph_kernels = enqueue(c.stream, 0);
+            RL_CUDA_TRY(cudaGraphConditionalHandleCreate(&cond, gr, 0u, cudaGraphCondAssignDefault));
+            a.has_cond = 1;
+            a.cond = cond;
+            a.level_runs = T.level_runs.p;
+            RL_CUDA_TRY(cudaStreamBeginCaptureToGraph(c.stream, gr, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            capturing = c.capturing = true;
+            enqueue_leaves(c.stream, a);
+            cudaStreamCaptureStatus status;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t ndeps = 0;
+            RL_CUDA_TRY(cudaStreamGetCaptureInfo(c.stream, &status, nullptr, nullptr, &deps, &ndeps));
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t cnode = nullptr;
+            RL_CUDA_TRY(cudaGraphAddNode(&cnode, gr, deps, ndeps, &cp));
+            RL_CUDA_TRY(cudaStreamUpdateCaptureDependencies(c.stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+            RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &gr));
+            capturing = c.capturing = false;
+            // the body: the level reductions
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            RL_CUDA_TRY(cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            capturing = c.capturing = true;
+            enqueue_levels(c.stream, a);
+            RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &body));
+            capturing = c.capturing = false;
         } catch (...) {
-            c.capturing = false;
-            cudaStreamEndCapture(c.stream, &gr);
-            if (gr) {
-                cudaGraphDestroy(gr);
+            if (capturing) {
+                cudaGraph_t g2 = nullptr;
+                cudaStreamEndCapture(c.stream, &g2);
             }
+            c.capturing = false;
+            cudaGraphDestroy(gr);
+            c.launches = launches;
             throw;
         }
-        c.capturing = false;
-        RL_CUDA_TRY(cudaStreamEndCapture(c.stream, &gr));
         c.launches = launches;
         cudaGraphExec_t ex = nullptr;
         const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
@@ -866,7 +920,7 @@ void update_tree(Ctx& c) {
         T.update_graph = ex;
     }
     RL_CUDA_TRY(cudaGraphLaunch(T.update_graph, c.stream));
-    c.launches += T.update_graph_kernels;
+    c.launches += 1;  // the leaf pass; the level launches are counted on the device
 }
 
 void launch_tree_update_scratch(Ctx& c, const uint32_t* d_vac_exc, const uint32_t* d_vac_inh, const uint8_t* d_update, uint32_t* arrive,

@@ -46,12 +46,13 @@ struct Tree {
     std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
     DBuf<uint8_t> dirty;        // nodes to recompute in the running update
     DBuf<uint32_t> level_dirty; // per level: a node of the level is marked
+    DBuf<unsigned long long> level_runs;  // level launches the captured update ran (counted on the device)
+    unsigned long long level_runs_seen = 0;  // of those, already added to the launch count
     DBuf<uint2> last_counts;    // per neuron: leaf counts (exc, inh) of the last update
     bool force_full = true;     // next update takes every leaf as changed
     bool recq_valid = false;    // fixed-point records match the FP64 records
     bool graph_keeps_q = false; // the captured update also maintains them
     cudaGraphExec_t update_graph = nullptr;  // the bottom-up update of this octree, captured once
-    uint32_t update_graph_kernels = 0;
     void drop_graph() {
         if (update_graph) {
             cudaGraphExecDestroy(update_graph);
