@@ -392,20 +392,22 @@ void plasticity_update(Ctx& c, uint32_t step) {
     // Neurons::create_synapses: search from the committed vacant axons
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));
     {
-        PhaseScope ps(c, PH_SEARCH);
+        // phases without work record no timing events (they would only add
+        // host calls while the device waits)
         if (c.no_searches) {
             c.search.num_searches = 0;  // no enabled neuron has a vacant axon
             c.search.num_requests = 0;
         } else {
+            PhaseScope ps(c, PH_SEARCH);
             run_search(c, step);
         }
         c.no_searches = false;
     }
-    {
+    if (c.search.num_requests > 0) {
         PhaseScope ps(c, PH_CONNECTOR);
         run_connector(c, step);
     }
-    {
+    if (c.graph.num_new > 0) {
         PhaseScope ps(c, PH_GRAPH);
         rebuild_graph(c);
     }
