@@ -37,10 +37,12 @@ sys.path.insert(0, ROOT)
 N_DEFAULT = 1_000_000
 SIDE_DEFAULT = 10_000.0
 PERIOD = 100
-# algorithmic bytes of the fused activity kernel per neuron-step (FP64 SoA):
-# reads enabled 1 + x 8 + u 8 + calcium 8 + target 8 + 3 deltas 24 = 57,
-# writes input 8 + x 8 + u 8 + fired 1 + calcium 8 + 3 deltas 24 = 57
-ACT_BYTES_PER_NEURON = 114
+# algorithmic bytes of the fused activity kernel per neuron-step (FP64 SoA,
+# one target calcium for all neurons, so no per-neuron target is read):
+# reads enabled 1 + x 8 + u 8 + calcium 8 + 3 deltas 24 = 49,
+# writes x 8 + u 8 + fired 1 + calcium 8 + 3 deltas 24 = 49,
+# and the input (8) on the last step of each 100-step block only
+ACT_BYTES_PER_NEURON = 98 + 8 / 100
 ACT_BYTES_PER_EDGE = 9  # pull over in-edges: source id 4 + weight 4 + fired flag 1
 ACT_BYTES_CSR_ROW = 8   # two row offsets when the graph is not empty
 
@@ -193,10 +195,12 @@ def build_network(n, side, seed, placement):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one activity launch at 1M
-# neurons (ncu --set full, see profiles/): FP64 59.0 + 4.2 MB, FP32 30.0 + 0.02 MB
-PROFILED_TRAFFIC = {0: 63.2e6, 1: 30.0e6}
+# neurons (ncu --set full, see profiles/): FP64 49.0 + 0.65 MB, FP32 30.0 + 0.02 MB
+PROFILED_TRAFFIC = {0: 49.7e6, 1: 30.0e6}
 
-ACT_BYTES_FP32 = 62  # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes input 4 + x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12
+# reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12;
+# the input (4) on the last step of each 100-step block only
+ACT_BYTES_FP32 = 58 + 4 / 100
 
 
 def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None):
@@ -246,7 +250,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     act_ms, act_cnt = phases["activity_kernel"]
     edges = int(net.stats().get("synapses_created", 0))
     per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
-    bytes_per_launch = per_neuron * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)
+    bytes_per_launch = int(round(per_neuron * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)))
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
     # DRAM bytes per launch from one ncu capture of the same kernel on this
@@ -482,7 +486,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     act_ms, act_cnt = ph["activity_kernel"]
     tuning = ens.tuning()
     hbm, peak_kind = peaks()
-    bytes_per_launch = ACT_BYTES_FP32 * total
+    bytes_per_launch = int(round(ACT_BYTES_FP32 * total))
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
     ens.close()
     return {"metric": "neuron-steps/s", "value": world * total * PERIOD * periods / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),

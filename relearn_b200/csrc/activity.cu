@@ -102,7 +102,9 @@ __device__ __forceinline__ void neuron_net(const ActArgs& A, uint32_t i, uint64_
 }
 
 __device__ __forceinline__ void disabled_neuron(const ActArgs& A, uint32_t i) {
-    A.input[i] = 0.0;
+    if (A.input) {
+        A.input[i] = 0.0;
+    }
     A.fired_cur[i] = A.fired_prev[i];
     A.delta0[i] = A.delta0[i] + 0.0;
     A.delta1[i] = A.delta1[i] + 0.0;
@@ -130,7 +132,9 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
     double input = 0.0;
     input += (double)isum * A.conductance;
     input += A.noise_mean + A.noise_stddev * z;  // NormalActivityInputCPU's draw
-    A.input[i] = input;
+    if (A.input) {
+        A.input[i] = input;
+    }
 
     double xv = A.x[i];
     double uv = A.u[i];
@@ -456,7 +460,9 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     A.u = c.nr.u.p;
     A.calcium = c.nr.calcium.p;
     A.target = c.nr.target.p;
-    A.input = c.nr.input.p;
+    // the input is state a caller can read only between blocks: the block's
+    // last step stores it, the others skip the store
+    A.input = kstep + 1 >= c.act_block_len ? c.nr.input.p : nullptr;
     A.delta0 = c.nr.delta[0].p;
     A.delta1 = c.nr.delta[1].p;
     A.delta2 = c.nr.delta[2].p;
@@ -653,6 +659,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     if (nsteps == 0) {
         return;
     }
+    c.act_block_len = nsteps;
     const ActDesc v{ first_step, c.graph.num_edges > 0 ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p };
     k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
     RL_LAUNCH_CHECK();

@@ -306,7 +306,9 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
         neuron_f32<H>(A, D, i + k, en[k] != 0, fp[k], k24[k], nu, x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
-    st_f<V>(A.input + i, input);
+    if (A.input) {
+        st_f<V>(A.input + i, input);
+    }
     st_b<V>(A.fired_cur + i, fired);
     st_f<V>(A.x + i, x);
     st_f<V>(A.u + i, u);
@@ -1066,7 +1068,7 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     A.fired_cur = fired_cur;
     A.x = c.nr.x32.p;
     A.u = c.nr.u32.p;
-    A.input = c.nr.input32.p;
+    A.input = kstep + 1 >= c.act_block_len ? c.nr.input32.p : nullptr;  // the block's last step stores the input
     A.calcium = c.nr.calcium.p;
     for (int t = 0; t < 3; ++t) {
         A.delta[t] = c.nr.delta32[t].p;

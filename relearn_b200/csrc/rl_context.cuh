@@ -271,6 +271,7 @@ struct Ctx {
     DBuf<ActDesc> act_desc;
     cudaGraphExec_t act_graph[2] = { nullptr, nullptr };  // per fired-buffer parity
     uint32_t act_graph_len = 0;
+    uint32_t act_block_len = 0;  // steps of the activity block being issued: only its last step stores the input
     bool use_graphs = true;
     bool capturing = false;
     std::vector<NetInfo> nets;  // host copy
