@@ -79,6 +79,7 @@ struct Act32 {
     // kernel reads no network table
     uint64_t seed1;
     float nu1[3];
+    uint32_t rk0[10], rk1[10];  // that network's Philox round keys
 };
 
 // Standard normal quantile of u = (k + 0.5) 2^-24 in FP32 as sqrt(2) erfinv(2u - 1),
@@ -117,6 +118,13 @@ __device__ __forceinline__ float normal_from_bits24(uint32_t k24) {
 
 // One neuron's activity step on registers: `x`, `u`, `ca` and the three
 // deltas are read and updated in place; `input` and `fired` are outputs.
+// 2^x with the special-function unit (ex2.approx, relative error ~2^-22).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // `k24`: the neuron's 24 random bits of this step's background draw.
 template <int H>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
@@ -170,7 +178,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
             dz = caf == A.eta[t] ? 0.0f : -1.0f;
         } else {
             const float q = (caf - A.xi[t]) * A.inv_zeta[t];
-            dz = fmaf(2.0f, __expf(-q * q), -1.0f);
+            dz = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
         }
         delta[t] = fmaf(dz, nu[t], delta[t]);
     }
@@ -294,7 +302,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
         const uint32_t local = MULTI ? i + k - A.nets[net[k]].first : i + k;
         const bool reuse = have && (local & 1u) && (!MULTI || net[k] == net[k - 1 < 0 ? 0 : k - 1]);
         if (!reuse) {
-            blk = noise_block(seed, step, local);
+            blk = MULTI ? noise_block(seed, step, local) : noise_block_rk(A.rk0, A.rk1, step, local);
         }
         have = (local & 1u) == 0u;
         k24[k] = ((local & 1u) ? blk.z : blk.x) >> 8;
@@ -1104,11 +1112,16 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
         A.flat[t] = eta == eps;
         A.eta[t] = (float)eta;
         A.xi[t] = (float)((eta + eps) * 0.5);
-        A.inv_zeta[t] = A.flat[t] ? 0.0f : (float)(1.0 / ((eta - eps) * factor_inv));
+        // scaled by sqrt(log2 e), so that exp(-q^2) is one exp2 of -(q')^2
+        A.inv_zeta[t] = A.flat[t] ? 0.0f : (float)(1.2011224087864498 / ((eta - eps) * factor_inv));
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
     A.seed1 = c.nets[0].seed;
+    for (int r = 0; r < 10; ++r) {
+        A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
+        A.rk1[r] = (uint32_t)(A.seed1 >> 32) + (uint32_t)r * 0xBB67AE85u;
+    }
     for (int t = 0; t < 3; ++t) {
         A.nu1[t] = c.nets[0].nu32[t];
     }

@@ -90,6 +90,19 @@ RL_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
     return c;
 }
 
+// The same generator with the round keys given (k0 + r W0, k1 + r W1 for
+// r = 0..9), for kernels whose key is the same in every thread.
+RL_HD u32x4 philox4x32_10_rk(u32x4 c, const uint32_t* rk0, const uint32_t* rk1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c.x, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c.z, hi1, lo1);
+        c = u32x4{ hi1 ^ c.y ^ rk0[round], lo1, hi0 ^ c.w ^ rk1[round], lo0 };
+    }
+    return c;
+}
+
 // Stream identifiers (upper byte of the fourth counter word).
 enum Stream : uint32_t {
     STREAM_BH_PICK = 1,    // Barnes-Hut weighted pick (per descent)
@@ -387,6 +400,9 @@ RL_HD double normal_quantile(double p) {
 // one, so that a thread updating a pair draws once.
 RL_HD u32x4 noise_block(uint64_t seed, uint32_t step, uint32_t neuron) {
     return draw(seed, step, neuron >> 1, 0u, STREAM_NOISE, 0u);
+}
+RL_HD u32x4 noise_block_rk(const uint32_t* rk0, const uint32_t* rk1, uint32_t step, uint32_t neuron) {
+    return philox4x32_10_rk(u32x4{ step, neuron >> 1, 0u, (uint32_t)STREAM_NOISE << 24 }, rk0, rk1);
 }
 RL_HD uint64_t noise_bits53(const u32x4& r, uint32_t neuron) {
     return (neuron & 1u) ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
