@@ -49,6 +49,7 @@ struct ActArgs {
     // reads no network table)
     uint64_t seed1;
     double nu1[3];
+    uint32_t rk0[10], rk1[10];  // that network's Philox round keys
     // one target calcium for every neuron: the growth curves' constants,
     // computed on the host with the same operations as growth_curve
     int uniform_target;
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
         double p = 0.5;
         if (on) {
             neuron_net<MULTI>(A, i, seed, local, nu);
-            p = noise_uniform(seed, step, local);
+            p = MULTI ? noise_uniform(seed, step, local) : noise_uniform_rk(A.rk0, A.rk1, step, local);
         }
         const bool tail = on && normal_in_tail(p);
         const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
@@ -489,6 +490,10 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
     A.seed1 = c.nets[0].seed;
+    for (int r = 0; r < 10; ++r) {
+        A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
+        A.rk1[r] = (uint32_t)(A.seed1 >> 32) + (uint32_t)r * 0xBB67AE85u;
+    }
     A.uniform_target = c.target_uniform ? 1 : 0;
     const double factor_inv = 1.0 / 1.6651092223153955127063292897904020952611777045288814583336582344;
     for (int t = 0; t < 3; ++t) {

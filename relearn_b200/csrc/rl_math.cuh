@@ -414,6 +414,11 @@ RL_HD double noise_uniform(uint64_t seed, uint32_t step, uint32_t neuron) {
     return ((double)noise_bits53(r, neuron) + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
 }
 
+RL_HD double noise_uniform_rk(const uint32_t* rk0, const uint32_t* rk1, uint32_t step, uint32_t neuron) {
+    const u32x4 r = noise_block_rk(rk0, rk1, step, neuron);
+    return ((double)noise_bits53(r, neuron) + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
+}
+
 RL_HD double background_normal(uint64_t seed, uint32_t step, uint32_t neuron, double mean, double stddev) {
     return mean + stddev * normal_quantile(noise_uniform(seed, step, neuron));
 }
