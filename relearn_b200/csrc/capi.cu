@@ -242,6 +242,34 @@ void setup_nets(Ctx& c, const rl_network* nets, uint32_t num) {
     RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
 }
 
+// Small pinned host slots (four counters each) for the contexts' count reads.
+// Pinned memory is taken from the driver a page at a time and never given
+// back: cudaMallocHost and cudaFreeHost are slow and cudaFreeHost waits for the
+// whole device, which a serving loop that creates and destroys contexts while
+// others run must not do.
+std::mutex g_pinned_mu;
+std::vector<unsigned long long*> g_pinned_free;
+
+unsigned long long* pinned_slot_take() {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    if (g_pinned_free.empty()) {
+        constexpr size_t kSlot = 4, kSlots = 512;  // 16 KiB per page
+        unsigned long long* page = nullptr;
+        RL_CUDA_TRY(cudaMallocHost(&page, kSlot * kSlots * sizeof(unsigned long long)));
+        for (size_t k = 0; k < kSlots; ++k) {
+            g_pinned_free.push_back(page + k * kSlot);
+        }
+    }
+    unsigned long long* s = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    return s;
+}
+
+void pinned_slot_give(unsigned long long* s) {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.push_back(s);
+}
+
 void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32_t num_nets = 0) {
     validate(k);
     c.cfg = k;
@@ -324,7 +352,7 @@ void create(Ctx& c, const rl_config& k, const rl_network* nets = nullptr, uint32
     c.err.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(c.err.p, 0, sizeof(uint32_t), c.stream));
     c.commit_cnt.alloc(4);
-    RL_CUDA_TRY(cudaMallocHost(&c.h_commit, 4 * sizeof(unsigned long long)));
+    c.h_commit = pinned_slot_take();
     c.counters.alloc(4);
     RL_CUDA_TRY(cudaMemsetAsync(c.counters.p, 0, 4 * sizeof(uint64_t), c.stream));
     setup_nets(c, nets, num_nets);
@@ -726,7 +754,7 @@ void discard(Ctx* c) {
         }
     }
     if (c->h_commit) {
-        cudaFreeHost(c->h_commit);
+        pinned_slot_give(c->h_commit);
         c->h_commit = nullptr;
     }
     // device buffers are freed on their streams; the context's own stream
