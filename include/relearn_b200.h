@@ -105,8 +105,7 @@ typedef struct rl_config {
 /* Neuron models (--neuron-model; the classes under neurons/models), defaults of their
  * Parameters.h.  The second state variable (rl_get_neurons' u) is the
  * Izhikevich recovery u, the FitzHugh-Nagumo and AEIF adaptation w, or the
- * Poisson model's refractory steps left.  The FP32 form runs the Izhikevich
- * model only. */
+ * Poisson model's refractory steps left.  Both precision forms run all four. */
 enum { RL_MODEL_IZHIKEVICH = 0, RL_MODEL_POISSON = 1, RL_MODEL_FITZHUGH_NAGUMO = 2, RL_MODEL_AEIF = 3 };
 
 /* Probability kernels of the search (algorithm/Kernel/KernelType.h): the

@@ -137,8 +137,6 @@ void validate(const rl_config& k) {
     RL_CHECK(k.precision == RL_PRECISION_FP64 || k.precision == RL_PRECISION_FP32, RL_ERR_INVALID, "precision must be FP64 or FP32");
     RL_CHECK(k.kernel_type >= RL_KERNEL_GAUSSIAN && k.kernel_type <= RL_KERNEL_WEIBULL, RL_ERR_INVALID, "unknown kernel type");
     RL_CHECK(k.neuron_model >= RL_MODEL_IZHIKEVICH && k.neuron_model <= RL_MODEL_AEIF, RL_ERR_INVALID, "unknown neuron model");
-    RL_CHECK(k.precision == RL_PRECISION_FP64 || k.neuron_model == RL_MODEL_IZHIKEVICH, RL_ERR_UNSUPPORTED,
-             "the FP32 form runs the Izhikevich model only");
     RL_CHECK(k.neuron_model != RL_MODEL_POISSON || k.poisson_tau_x > 0.0, RL_ERR_INVALID, "Poisson tau_x must be positive");
     RL_CHECK(k.neuron_model != RL_MODEL_AEIF || (k.aeif_C > 0.0 && k.aeif_d_T > 0.0 && k.aeif_tau_w > 0.0), RL_ERR_INVALID,
              "AEIF C, d_T and tau_w must be positive");

@@ -80,6 +80,10 @@ struct Act32 {
     uint64_t seed1;
     float nu1[3];
     uint32_t rk0[10], rk1[10];  // that network's Philox round keys
+    // the other neuron models (neurons/models/*), their constants in FP32
+    float p_x0, p_tau_inv, p_refractory;                                   // Poisson
+    float f_a, f_b, f_phi;                                                 // FitzHugh-Nagumo
+    float e_g_L, e_E_L, e_V_T, e_g_L_d_T, e_d_T_inv, e_tau_w_inv, e_C_inv, e_a, e_b, e_V_spike;  // AEIF
 };
 
 // Standard normal quantile of u = (k + 0.5) 2^-24 in FP32 as sqrt(2) erfinv(2u - 1),
@@ -125,10 +129,12 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-// `k24`: the neuron's 24 random bits of this step's background draw.
-template <int H>
+// `k24`: the neuron's 24 random bits of this step's background draw;
+// `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
+template <int H, int MODEL>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
-                                           const float* nu, float& x, float& u, double& ca, float (&delta)[3], float& input, uint8_t& fired) {
+                                           uint32_t k24p, const float* nu, float& x, float& u, double& ca, float (&delta)[3], float& input,
+                                           uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
         fired = fired_prev;
@@ -152,18 +158,61 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     float uv = u;
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
-    const float sc = fmaf(A.s, input, A.sk3);
-    const float ms = -A.s;
+    if (MODEL == RL_MODEL_IZHIKEVICH) {
+        const float sc = fmaf(A.s, input, A.sk3);
+        const float ms = -A.s;
 #pragma unroll
-    for (uint32_t it = 0; it < h; ++it) {
-        const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
-        uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
-        xv = xv + inc;
-        if (xv >= A.v_spike) {
-            xv = A.c;
-            uv += A.d;
-            spiked = 1;
-            break;
+        for (uint32_t it = 0; it < h; ++it) {
+            const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
+            uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
+            xv = xv + inc;
+            if (xv >= A.v_spike) {
+                xv = A.c;
+                uv += A.d;
+                spiked = 1;
+                break;
+            }
+        }
+    } else if (MODEL == RL_MODEL_POISSON) {
+        // PoissonModelCPU::update_activity; u counts the refractory steps left
+        for (uint32_t it = 0; it < h; ++it) {
+            xv = fmaf(fmaf(A.p_x0 - xv, A.p_tau_inv, input), A.s, xv);
+        }
+        if (uv == 0.0f) {
+            const float threshold = (float)k24p * 5.9604644775390625e-8f;  // the FP64 form's uniform, 24 bits of it
+            if (xv >= threshold) {
+                spiked = 1;
+                uv = A.p_refractory;
+            }
+        } else {
+            uv -= 1.0f;
+        }
+    } else if (MODEL == RL_MODEL_FITZHUGH_NAGUMO) {
+        // FitzHughNagumoModelCPU::update_activity: no reset, spike test after the substeps
+        const float third = 1.0f / 3.0f;
+        for (uint32_t it = 0; it < h; ++it) {
+            const float x3 = xv * xv * xv;
+            const float x_inc = fmaf(-x3, third, xv) - uv + input;
+            const float w_inc = A.f_phi * fmaf(-A.f_b, uv, xv + A.f_a);
+            xv = fmaf(x_inc, A.s, xv);
+            uv = fmaf(w_inc, A.s, uv);
+        }
+        spiked = (uv > fmaf(-xv * xv * xv, third, xv) && xv > 1.0f) ? 1 : 0;
+    } else {
+        // AEIFModelCPU::update_activity
+        for (uint32_t it = 0; it < h; ++it) {
+            const float lin = -A.e_g_L * (xv - A.e_E_L);
+            const float ex = A.e_g_L_d_T * __expf((xv - A.e_V_T) * A.e_d_T_inv);
+            const float x_inc = (lin + ex - uv + input) * A.e_C_inv;
+            const float w_inc = fmaf(A.e_a, xv - A.e_E_L, -uv) * A.e_tau_w_inv;
+            xv = fmaf(x_inc, A.s, xv);
+            uv = fmaf(w_inc, A.s, uv);
+            if (xv >= A.e_V_spike) {
+                xv = A.e_E_L;
+                uv += A.e_b;
+                spiked = 1;
+                break;
+            }
         }
     }
     x = xv;
@@ -272,7 +321,7 @@ __device__ __forceinline__ void ld_h(const uint16_t* p, uint16_t (&v)[V]) {
 // V consecutive neurons from index i (a multiple of V): all loads first, so
 // that each thread keeps its whole footprint in flight, then the updates,
 // then the stores.
-template <int H, int V, bool MULTI>
+template <int H, int V, bool MULTI, int MODEL>
 __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i) {
     uint8_t en[V], fp[V], fired[V];
     uint16_t net[V];
@@ -294,6 +343,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     // a thread with two neurons of a pair draws once.  Draws are keyed on the
     // network's seed and the neuron's index in its network.
     uint32_t k24[V];
+    uint32_t k24p[V] = {};
     u32x4 blk{ 0u, 0u, 0u, 0u };
     bool have = false;
 #pragma unroll
@@ -306,12 +356,18 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
         }
         have = (local & 1u) == 0u;
         k24[k] = ((local & 1u) ? blk.z : blk.x) >> 8;
+        if (MODEL == RL_MODEL_POISSON) {
+            // the threshold draw of PoissonModelCPU, keyed as in the FP64 form
+            const u32x4 w = MULTI ? draw(seed, step, local, 0u, STREAM_POISSON, 0u)
+                                  : philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, A.rk0, A.rk1);
+            k24p[k] = w.x >> 8;
+        }
     }
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         float d[3] = { d0[k], d1[k], d2[k] };
         const float* nu = MULTI ? A.nets[net[k]].nu32 : A.nu1;
-        neuron_f32<H>(A, D, i + k, en[k] != 0, fp[k], k24[k], nu, x[k], u[k], ca[k], d, input[k], fired[k]);
+        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     if (A.input) {
@@ -329,7 +385,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 // H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
 // block, V neurons per thread, striding over the neurons when the grid is one
 // resident wave.  The last n % V neurons go one per thread.
-template <int H, int BLOCK, int V, bool MULTI>
+template <int H, int BLOCK, int V, bool MULTI, int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
     pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t step = D->base_step + k;
@@ -337,10 +393,10 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* 
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t g = tid; g < groups; g += stride) {
-        neurons_f32<H, V, MULTI>(A, D, step, g * V);
+        neurons_f32<H, V, MULTI, MODEL>(A, D, step, g * V);
     }
     if (V > 1 && tid < A.n - groups * V) {
-        neurons_f32<H, 1, MULTI>(A, D, step, groups * V + tid);
+        neurons_f32<H, 1, MULTI, MODEL>(A, D, step, groups * V + tid);
     }
 }
 
@@ -1026,43 +1082,43 @@ void f64_from_f32(Ctx& c) {
     }
 }
 
-template <int H, int BLOCK, int V>
+template <int H, int BLOCK, int V, int MODEL>
 void launch_act32(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
     if (c.multi()) {
-        launch_pdl(&k_activity_f32<H, BLOCK, V, true>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, true>), BLOCK, c.stream, A,
-                   (const ActDesc*)c.act_desc.p, kstep);
+        launch_pdl(&k_activity_f32<H, BLOCK, V, true, MODEL>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, true, MODEL>), BLOCK, c.stream,
+                   A, (const ActDesc*)c.act_desc.p, kstep);
     } else {
-        launch_pdl(&k_activity_f32<H, BLOCK, V, false>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, false>), BLOCK, c.stream, A,
-                   (const ActDesc*)c.act_desc.p, kstep);
+        launch_pdl(&k_activity_f32<H, BLOCK, V, false, MODEL>, act_grid(c, v, (const void*)&k_activity_f32<H, BLOCK, V, false, MODEL>), BLOCK,
+                   c.stream, A, (const ActDesc*)c.act_desc.p, kstep);
     }
 }
 
-template <int H, int BLOCK>
+template <int H, int BLOCK, int MODEL>
 void launch_act32_b(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
     switch (v.vec) {
         case 4:
-            launch_act32<H, BLOCK, 4>(c, v, A, kstep);
+            launch_act32<H, BLOCK, 4, MODEL>(c, v, A, kstep);
             break;
         case 2:
-            launch_act32<H, BLOCK, 2>(c, v, A, kstep);
+            launch_act32<H, BLOCK, 2, MODEL>(c, v, A, kstep);
             break;
         default:
-            launch_act32<H, BLOCK, 1>(c, v, A, kstep);
+            launch_act32<H, BLOCK, 1, MODEL>(c, v, A, kstep);
             break;
     }
 }
 
-template <int H>
+template <int H, int MODEL = RL_MODEL_IZHIKEVICH>
 void launch_act32_h(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep) {
     switch (v.block) {
         case 128:
-            launch_act32_b<H, 128>(c, v, A, kstep);
+            launch_act32_b<H, 128, MODEL>(c, v, A, kstep);
             break;
         case 512:
-            launch_act32_b<H, 512>(c, v, A, kstep);
+            launch_act32_b<H, 512, MODEL>(c, v, A, kstep);
             break;
         default:
-            launch_act32_b<H, 256>(c, v, A, kstep);
+            launch_act32_b<H, 256, MODEL>(c, v, A, kstep);
             break;
     }
 }
@@ -1125,7 +1181,29 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     for (int t = 0; t < 3; ++t) {
         A.nu1[t] = c.nets[0].nu32[t];
     }
-    if (k.h_model == 10) {
+    A.p_x0 = (float)k.poisson_x0;
+    A.p_tau_inv = (float)(1.0 / k.poisson_tau_x);
+    A.p_refractory = (float)k.poisson_refractory;
+    A.f_a = (float)k.fhn_a;
+    A.f_b = (float)k.fhn_b;
+    A.f_phi = (float)k.fhn_phi;
+    A.e_g_L = (float)k.aeif_g_L;
+    A.e_E_L = (float)k.aeif_E_L;
+    A.e_V_T = (float)k.aeif_V_T;
+    A.e_g_L_d_T = (float)(k.aeif_g_L * k.aeif_d_T);
+    A.e_d_T_inv = (float)(1.0 / k.aeif_d_T);
+    A.e_tau_w_inv = (float)(1.0 / k.aeif_tau_w);
+    A.e_C_inv = (float)(1.0 / k.aeif_C);
+    A.e_a = (float)k.aeif_a;
+    A.e_b = (float)k.aeif_b;
+    A.e_V_spike = (float)k.aeif_V_spike;
+    if (k.neuron_model == RL_MODEL_POISSON) {
+        launch_act32_h<0, RL_MODEL_POISSON>(c, v, A, kstep);
+    } else if (k.neuron_model == RL_MODEL_FITZHUGH_NAGUMO) {
+        launch_act32_h<0, RL_MODEL_FITZHUGH_NAGUMO>(c, v, A, kstep);
+    } else if (k.neuron_model == RL_MODEL_AEIF) {
+        launch_act32_h<0, RL_MODEL_AEIF>(c, v, A, kstep);
+    } else if (k.h_model == 10) {
         launch_act32_h<10>(c, v, A, kstep);
     } else {
         launch_act32_h<0>(c, v, A, kstep);

@@ -299,12 +299,3 @@ def test_other_neuron_models(model):
     assert net.neurons()["fired"].sum() > 0 or model == 2
     assert len(net.edges()[0]) > 0
 
-
-def test_fp32_form_runs_izhikevich_only():
-    from relearn_b200 import Network, RelearnError
-
-    params, _, _ = small_network(100, 200.0, 1)
-    params["precision"] = 1
-    params["neuron_model"] = 2
-    with pytest.raises(RelearnError):
-        Network(params)
