@@ -1,5 +1,6 @@
-"""Bit-exact parity at the benchmark's size: 1M neurons uniform in a 10,000 um
-cube with the bench workload's parameters, synaptic elements seeded U[0, 4] per
+"""Bit-exact parity at the benchmark's size: 1M neurons in a 10,000 um cube
+(uniform, and the 64-component Gaussian mixture) with the bench workload's
+parameters, synaptic elements seeded U[0, 4] per
 type so that every plasticity update searches for about a million axons, 301
 steps (three plasticity updates) through the C ABI against the oracle on all
 host cores: potentials, calcium, elements, octree and the synapse list must be
@@ -15,14 +16,15 @@ from test_gpu_parity import assert_tree_equal, compare_state
 pytestmark = pytest.mark.gpu
 
 
-def test_one_million_neurons_301_steps():
+@pytest.mark.parametrize("placement", ["uniform", "mixture"])
+def test_one_million_neurons_301_steps(placement):
     from oracle import oracle as O
     from relearn_b200 import Network, default_params, workloads
 
     n, side, seed = 1_000_000, 10_000.0, 1
     params = default_params(n, side)
     params["seed"] = seed
-    pos = workloads.uniform_cube(n, side, seed)
+    pos = workloads.uniform_cube(n, side, seed) if placement == "uniform" else workloads.gaussian_mixture(n, side, seed)
     sig = workloads.signal_types(n, seed)
     net = Network(params)
     net.set_positions(pos, sig)
