@@ -111,10 +111,6 @@ __device__ __forceinline__ Eval evaluate(const double4& r, uint2 t, double md, d
     return e;
 }
 
-__device__ __forceinline__ uint32_t child_index(uint2 t, int octant) {
-    return t.x + (uint32_t)__popc(topo_mask(t.y) & ((1u << octant) - 1u));
-}
-
 // Random number of ProbabilityPicker::pick_target(values, key) for a total.
 __device__ __forceinline__ double pick_threshold(double total, uint64_t seed, uint32_t step, uint32_t source, uint32_t j, uint32_t depth) {
     const double next = next_up_eps(total);

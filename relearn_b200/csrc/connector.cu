@@ -112,13 +112,6 @@ __global__ void k_emit_edges(uint64_t m, const uint32_t* __restrict__ accepted, 
 }
 
 // ---- graph
-__global__ void k_iota(uint64_t m, uint32_t* __restrict__ p) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) {
-        p[i] = (uint32_t)i;
-    }
-}
-
 __global__ void k_pair_keys(uint64_t m, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint64_t* __restrict__ key,
                             uint32_t* __restrict__ idx) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
