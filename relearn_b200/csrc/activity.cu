@@ -19,6 +19,8 @@
 // writes each of its words once per step.
 #include <memory>
 
+#include <cooperative_groups.h>
+
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -741,6 +743,160 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     if (c.copy_stream) {
         issue_snapshots(c);  // the block is queued: snapshot copies now overlap it
     }
+}
+
+namespace {
+
+// The three commits of a plasticity update in one cooperative launch
+// (SynapseDeletionFinderCPU::delete_synapses order: axons, excitatory,
+// inhibitory dendrites).  A type whose commit leaves bound elements to delete
+// ends the launch after a grid-wide barrier, so the later types wait for the
+// deletions exactly as with one launch per type; the axon pass also sums the
+// vacant axons of enabled neurons (counts in cnt[0..2], cnt[3]).  D is the
+// delta type of the precision form.
+template <typename D>
+struct CommitAll {
+    uint32_t n;
+    const uint8_t* enabled;
+    double* grown[3];
+    D* delta[3];
+    uint32_t* connected[3];
+    uint32_t* vacant[3];
+    double retract[3];
+    uint32_t* to_delete;
+    unsigned long long* cnt;
+};
+
+// ElementBaseBase::update for one neuron and type (the arithmetic of k_commit
+// and k_commit_f32); returns the bound elements to delete.
+template <typename D>
+__device__ __forceinline__ uint32_t commit_one(const CommitAll<D>& A, int t, uint32_t i) {
+    if (!A.enabled[i]) {
+        A.to_delete[i] = 0u;
+        return 0u;
+    }
+    const double current_count = A.grown[t][i];
+    const double current_delta = (double)A.delta[t][i];
+    const uint32_t conn_int = A.connected[t][i];
+    const double conn = (double)conn_int;
+    const double current_vacant = current_count - conn;
+    const double new_vacant = current_vacant + current_delta;
+    const double keep = 1.0 - A.retract[t];
+    uint32_t del = 0;
+    if (new_vacant >= 0.0) {
+        const double after = keep * new_vacant;
+        A.grown[t][i] = after + conn;
+        A.vacant[t][i] = (uint32_t)after;
+    } else if (current_count + current_delta <= 0.0) {
+        A.grown[t][i] = 0.0;
+        A.vacant[t][i] = 0u;
+        A.connected[t][i] = 0u;
+        del = conn_int;
+    } else {
+        const double new_count = current_count + current_delta;
+        const double new_conn = floor(new_count);
+        const double num_vacant = new_count - new_conn;
+        A.grown[t][i] = (keep * num_vacant) + new_conn;
+        A.vacant[t][i] = 0u;
+        A.connected[t][i] = (uint32_t)new_conn;
+        del = (uint32_t)(conn - new_conn);
+    }
+    A.delta[t][i] = (D)0;
+    A.to_delete[i] = del;
+    return del;
+}
+
+__device__ __forceinline__ void block_add(unsigned long long v, unsigned long long* out, unsigned long long* part) {
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        part[threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned long long w = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            w += __shfl_down_sync(0xFFFFFFFFu, w, o);
+        }
+        if (threadIdx.x == 0 && w) {
+            atomicAdd(out, w);
+        }
+    }
+    __syncthreads();
+}
+
+template <typename D>
+__global__ void __launch_bounds__(256) k_commit_all(CommitAll<D> A) {
+    __shared__ unsigned long long part[8];
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (int t = 0; t < 3; ++t) {
+        if (t > 0) {
+            grid.sync();
+            if (A.cnt[t - 1] != 0ull) {
+                return;  // the same decision in every thread: deletions first
+            }
+        }
+        unsigned long long del = 0, vac = 0;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+            del += commit_one<D>(A, t, i);
+            if (t == 0 && A.enabled[i]) {
+                vac += A.vacant[0][i];
+            }
+        }
+        block_add(del, &A.cnt[t], part);
+        if (t == 0) {
+            block_add(vac, &A.cnt[3], part);
+        }
+    }
+}
+
+template <typename D>
+bool launch_commit_all_t(Ctx& c, D* const* delta) {
+    CommitAll<D> A;
+    A.n = c.n;
+    A.enabled = c.nr.enabled.p;
+    for (int t = 0; t < 3; ++t) {
+        A.grown[t] = c.nr.grown[t].p;
+        A.delta[t] = delta[t];
+        A.connected[t] = c.nr.connected[t].p;
+        A.vacant[t] = c.nr.vacant[t].p;
+        A.retract[t] = c.cfg.retract_ratio[t];
+    }
+    A.to_delete = c.to_delete.p;
+    A.cnt = c.commit_cnt.p;
+    int per_sm = 0;
+    RL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)&k_commit_all<D>, 256, 0));
+    if (per_sm <= 0) {
+        return false;
+    }
+    unsigned blocks = (unsigned)per_sm * (unsigned)c.num_sms;
+    const unsigned need = blocks_for(c.n, 256);
+    if (need < blocks) {
+        blocks = need;
+    }
+    void* args[] = { &A };
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)&k_commit_all<D>, dim3(blocks), dim3(256), args, 0, c.stream);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();  // cooperative launch unavailable: the caller takes the per-type launches
+        return false;
+    }
+    if (g_bind.launches) {
+        ++*g_bind.launches;
+    }
+    return true;
+}
+
+}  // namespace
+
+bool launch_commit_all(Ctx& c) {
+    if (is_fp32(c)) {
+        float* d[3] = { c.nr.delta32[0].p, c.nr.delta32[1].p, c.nr.delta32[2].p };
+        return launch_commit_all_t<float>(c, d);
+    }
+    double* d[3] = { c.nr.delta[0].p, c.nr.delta[1].p, c.nr.delta[2].p };
+    return launch_commit_all_t<double>(c, d);
 }
 
 void launch_commit_guarded(Ctx& c, int type) {

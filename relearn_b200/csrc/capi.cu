@@ -379,11 +379,13 @@ void plasticity_update(Ctx& c, uint32_t step) {
         {
             PhaseScope ps(c, PH_COMMIT);
             RL_CUDA_TRY(cudaMemsetAsync(c.commit_cnt.p, 0, 4 * sizeof(unsigned long long), c.stream));
-            for (int t = 0; t < 3; ++t) {
-                launch_commit_guarded(c, t);
+            if (!launch_commit_all(c)) {
+                for (int t = 0; t < 3; ++t) {
+                    launch_commit_guarded(c, t);
+                }
+                // the same read says whether the search will have anything to do
+                launch_vacant_axon_count(c, c.commit_cnt.p + 3);
             }
-            // the same read says whether the search will have anything to do
-            launch_vacant_axon_count(c, c.commit_cnt.p + 3);
             RL_CUDA_TRY(cudaMemcpyAsync(c.h_commit, c.commit_cnt.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c.stream));
         }
         // The octree update goes out before the host reads the counts, so that

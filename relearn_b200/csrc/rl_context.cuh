@@ -382,6 +382,9 @@ uint64_t run_commit(Ctx& c, int type);
 // (its count in commit_cnt) left bound elements to delete; counts into
 // commit_cnt[type].  The three are launched back to back and read once.
 void launch_commit_guarded(Ctx& c, int type);
+// All three commits and the vacant-axon count in one cooperative launch, with
+// the same skip rule; false when a cooperative launch is not available.
+bool launch_commit_all(Ctx& c);
 // Adds the vacant axons of the enabled neurons to *out.
 void launch_vacant_axon_count(Ctx& c, unsigned long long* out);
 void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n);  // commit one element type; to_delete[] per neuron, returns the sum
