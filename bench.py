@@ -198,6 +198,26 @@ def build_network(n, side, seed, placement):
 # neurons (ncu --set full, see profiles/): FP64 49.0 + 0.65 MB, FP32 30.0 + 0.02 MB
 PROFILED_TRAFFIC = {0: 49.7e6, 1: 30.0e6}
 
+# FP64 warp instructions (DADD 3.97M + DMUL 3.44M + DFMA 2.39M + DSETP 0.74M) of one
+# k_activity launch at 1M neurons, from ncu's instruction mix of the FP64
+# drop-in (profiles/k_activity_fp64_1M.md): 10.54 per neuron-step.  The FP64
+# pipe of an SM takes 2 warp instructions per cycle (64 lanes), so the launch
+# cannot take less than 10.54 n / (2 * SMs * clock).
+FP64_WARP_INSTR_PER_NEURON = 10.54
+B200_SMS = 148
+
+
+def fp64_pipe_roofline(roof: dict, n: int, sm_mhz) -> dict:
+    """The FP64 drop-in's activity kernel is bound by its FP64 pipe, not by
+    HBM: its floor time against its measured launch time."""
+    mhz = sm_mhz or 1965.0
+    floor_us = FP64_WARP_INSTR_PER_NEURON * n / (2 * B200_SMS * mhz * 1e6) * 1e6
+    avg = roof.get("avg_launch_us")
+    return {"bound": "fp64 pipe", "warp_instr_per_neuron_step": FP64_WARP_INSTR_PER_NEURON, "sm_mhz": mhz, "floor_us": floor_us,
+            "avg_launch_us": avg, "frac": floor_us / avg if avg else None,
+            "how": "FP64 warp instructions per launch (ncu instruction mix) / (2 per SM per cycle x 148 SMs x median SM clock)"}
+
+
 # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12;
 # the input (4) on the last step of each 100-step block only
 ACT_BYTES_FP32 = 58 + 4 / 100
@@ -383,6 +403,8 @@ def run_b200(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, params, pos, sig)
     clocks = clk.summary()
+    if main_prec == 0 and args.placement == "uniform":
+        m["roofline"]["fp64_pipe"] = fp64_pipe_roofline(m["roofline"], n, clocks.get("sm_mhz"))
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -38,25 +38,42 @@ def test_every_search_shape_finds_the_same_targets(precision):
     assert len(ref) > 0
 
 
+def _activity_state(net):
+    a = net.neurons()
+    got = [a["x"].view(np.uint64), a["u"].view(np.uint64), a["calcium"].view(np.uint64), a["fired"], a["input"].view(np.uint64)]
+    for t in range(3):
+        got.append(net.get_elements(t)["delta"].view(np.uint64))
+    return got
+
+
 @pytest.mark.parametrize("precision", [0, 1])
-def test_every_activity_shape_gives_the_same_state(precision):
+@pytest.mark.parametrize("mode", ["all", "disabled", "targets"])
+def test_every_activity_shape_gives_the_same_state(precision, mode):
+    """Every block size, grid form and neurons-per-thread count gives the same
+    bits (state, input and deltas): with all neurons enabled, with neurons
+    disabled and with per-neuron target calcium."""
     from relearn_b200 import ACT_SHAPES
 
+    if mode == "targets" and precision == 1:
+        pytest.skip("the FP32 form runs one target calcium for all neurons")
     n = 50000
     ref = None
     for b, p, v in ACT_SHAPES:
         if precision == 0 and v != 1:
             continue
         net = make(n + 3, 3700.0, 8, precision)  # n % 4 == 3: the vector shapes have a tail
+        if mode == "disabled":
+            net.set_enabled((np.random.default_rng(5).random(n + 3) > 0.3).astype(np.uint8))
+        elif mode == "targets":
+            net.set_target_calcium(np.random.default_rng(6).uniform(0.3, 0.9, n + 3))
         net.set_tuning(act_block=b, act_persistent=p, act_vec=v)
         net.activity_block(1, 37)
-        a = net.neurons()
-        got = [a["x"].view(np.uint64), a["u"].view(np.uint64), a["calcium"].view(np.uint64), a["fired"]]
+        got = _activity_state(net)
         if ref is None:
             ref = got
         else:
-            for g, r in zip(got, ref):
-                assert np.array_equal(g, r), (b, p)
+            for j, (g, r) in enumerate(zip(got, ref)):
+                assert np.array_equal(g, r), (b, p, v, j)
         net.close()
 
 
