@@ -199,16 +199,30 @@ def build_network(n, side, seed, placement):
 PROFILED_TRAFFIC = {0: 49.7e6, 1: 30.0e6}
 
 # FP64 warp instructions (DADD 3.97M + DMUL 3.44M + DFMA 2.39M + DSETP 0.74M) of one
-# k_activity launch at 1M neurons, from ncu's instruction mix of the FP64
-# drop-in (profiles/k_activity_fp64_1M.md): 10.54 per neuron-step.  The FP64
-# pipe of an SM takes 2 warp instructions per cycle (64 lanes), so the launch
+# per-step k_activity launch at 1M neurons, from ncu's instruction mix of the
+# FP64 drop-in (profiles/k_activity_fp64_1M.md): 10.54 per neuron-step.  The
+# FP64 pipe of an SM takes 2 warp instructions per cycle (64 lanes), so a step
 # cannot take less than 10.54 n / (2 * SMs * clock).
 FP64_WARP_INSTR_PER_NEURON = 10.54
 B200_SMS = 148
 
+# The fused block kernels (a network without synapses: a block of steps per
+# launch, state in registers), from ncu's instruction mix of a 4-step launch
+# at 1M neurons (profiles/k_activity_steps_1M.md), per neuron-step:
+# k_activity_steps 10.77 FP64 warp instructions (43.10M / 4 steps / 1M);
+# k_activity_f32_steps 8.36 warp instructions of every kind (33.44M / 4 / 1M),
+# issued at one per SM sub-partition (4 per SM) per cycle.
+FUSED64_FP64_WARP_INSTR = 10.77
+FUSED32_WARP_INSTR = 8.36
+# memory per neuron and launch: reads enabled, spike flag, x, u, calcium, three
+# deltas; writes x, u, calcium, deltas, both spike-flag buffers, the input
+FUSED_BYTES = {0: 50 + 58, 1: 30 + 34}
+# ncu dram read + write of that 4-step launch (the same for any block length)
+FUSED_TRAFFIC = {0: 50.03e6 + 4.35e6, 1: 30.02e6 + 0.11e6}
+
 
 def fp64_pipe_roofline(roof: dict, n: int, sm_mhz) -> dict:
-    """The FP64 drop-in's activity kernel is bound by its FP64 pipe, not by
+    """The per-step FP64 activity kernel is bound by its FP64 pipe, not by
     HBM: its floor time against its measured launch time."""
     mhz = sm_mhz or 1965.0
     floor_us = FP64_WARP_INSTR_PER_NEURON * n / (2 * B200_SMS * mhz * 1e6) * 1e6
@@ -216,6 +230,33 @@ def fp64_pipe_roofline(roof: dict, n: int, sm_mhz) -> dict:
     return {"bound": "fp64 pipe", "warp_instr_per_neuron_step": FP64_WARP_INSTR_PER_NEURON, "sm_mhz": mhz, "floor_us": floor_us,
             "avg_launch_us": avg, "frac": floor_us / avg if avg else None,
             "how": "FP64 warp instructions per launch (ncu instruction mix) / (2 per SM per cycle x 148 SMs x median SM clock)"}
+
+
+def fused_roofline(precision: int, n: int, step_us: float, act_cnt: int, sm_mhz, hbm: float, peak_kind: str, profiled: bool) -> dict:
+    """Roofline of the fused block kernel: compute-bound (the FP64 pipe for
+    the FP64 drop-in, instruction issue for the FP32 form), with the memory
+    side (state once per launch) beside it."""
+    mhz = sm_mhz or 1965.0
+    launch_us = step_us * PERIOD
+    if precision == 0:
+        lane_ops = FUSED64_FP64_WARP_INSTR * 32  # FP64 lane operations per neuron-step
+        achieved = lane_ops * n / (step_us * 1e-6) / 1e12
+        peak = 64 * B200_SMS * mhz * 1e6 / 1e12
+        roof = {"bound": "fp64", "kernel": "k_activity_steps", "achieved": achieved, "peak": peak, "unit": "T FP64 lane-op/s",
+                "frac": achieved / peak, "ops_per_neuron_step": lane_ops,
+                "peak_kind": "nominal issue rate at the median SM clock: 64 FP64 lanes per SM x 148 SMs (no measured FP64 peak)"}
+    else:
+        achieved = FUSED32_WARP_INSTR * n / (step_us * 1e-6) / 1e12
+        peak = 4 * B200_SMS * mhz * 1e6 / 1e12
+        roof = {"bound": "issue", "kernel": "k_activity_f32_steps", "achieved": achieved, "peak": peak, "unit": "T warp-inst/s",
+                "frac": achieved / peak, "warp_instr_per_neuron_step": FUSED32_WARP_INSTR,
+                "peak_kind": "nominal issue rate at the median SM clock: 1 warp instruction per SM sub-partition per cycle x 592"}
+    bytes_per_launch = FUSED_BYTES[precision] * n
+    roof.update({"sm_mhz": mhz, "steps_per_launch": PERIOD, "avg_step_us": step_us, "avg_launch_us": launch_us, "launches": act_cnt // PERIOD,
+                 "traffic": FUSED_TRAFFIC[precision] if profiled else None, "traffic_unit": "bytes per launch (ncu dram read + write)",
+                 "hbm": {"bytes_per_launch": bytes_per_launch, "achieved": bytes_per_launch / (launch_us * 1e-6) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_per_launch / (launch_us * 1e-6) / 1e9 / hbm if hbm else None, "peak_kind": peak_kind}})
+    return roof
 
 
 # reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12;
@@ -236,6 +277,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     net = R.Network(p)
     net.set_stream(stream.cuda_stream)
     net.set_positions(pos, sig)
+    net.set_step_fusion(bool(args.step_fusion))
     apply_shapes(args, net, precision)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     step = 1
@@ -277,6 +319,13 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     # workload (profiles/k_activity_f32_1M.md, k_activity_fp64_1M.md): reads
     # equal the algorithmic read bytes, writes stay in L2 during the launch
     traffic = PROFILED_TRAFFIC.get(precision) if (n == 1_000_000 and args.placement == "uniform" and not edges) else None
+    if args.step_fusion and not edges and act_cnt:
+        # no synapses: each 100-step block ran as one launch of the fused kernel
+        sm_mhz = clk.summary().get("sm_mhz") if clk is not None else None
+        roof = fused_roofline(precision, n, 1e3 * act_ms / act_cnt, act_cnt, sm_mhz, hbm, peak_kind,
+                              n == 1_000_000 and args.placement == "uniform")
+        return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof,
+                    tuning=net.tuning())
     roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm if hbm else None, "traffic": traffic, "traffic_unit": "bytes per launch (ncu dram read + write)",
             "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
@@ -403,7 +452,7 @@ def run_b200(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, params, pos, sig)
     clocks = clk.summary()
-    if main_prec == 0 and args.placement == "uniform":
+    if main_prec == 0 and args.placement == "uniform" and m["roofline"]["kernel"] == "k_activity":
         m["roofline"]["fp64_pipe"] = fp64_pipe_roofline(m["roofline"], n, clocks.get("sm_mhz"))
     if world > 1:
         torch.distributed.barrier()
@@ -482,6 +531,7 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     ens = R.Network(base, networks=nets)
     ens.set_stream(stream.cuda_stream)
     ens.set_positions(pos, sig)
+    ens.set_step_fusion(bool(args.step_fusion))
     ens.autotune(1)  # launch shapes timed during the warm-up
     step = 1
     for _ in range(args.warmup):
@@ -510,11 +560,18 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     hbm, peak_kind = peaks()
     bytes_per_launch = int(round(ACT_BYTES_FP32 * total))
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+    fused = bool(args.step_fusion) and int(ens.stats().get("synapses_created", 0)) == 0
     ens.close()
+    if fused:
+        # no synapses in any network: each 100-step block ran as one launch for all networks
+        roof = fused_roofline(1, total, 1e3 * act_ms / act_cnt, act_cnt, None, hbm, peak_kind, False)
+        how = "100-step activity blocks, one launch each"
+    else:
+        roof = {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
+        how = "100-step activity blocks as CUDA graphs, one launch per step"
     return {"metric": "neuron-steps/s", "value": world * total * PERIOD * periods / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),
-            "neurons": total, "periods": periods, "precision": "fp32", "launches_per_step": 1, "graphs": "100-step activity blocks",
-            "roofline": {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None},
+            "neurons": total, "periods": periods, "precision": "fp32", "activity": how, "roofline": roof,
             "phases_ms": {k: v[0] for k, v in ph.items()}, "tuning": tuning}
 
 
@@ -780,6 +837,7 @@ def run_case(args):
     net = R.Network(params)
     if args.act_shape or args.search_shape:
         apply_shapes(args, net, params["precision"])
+    net.set_step_fusion(bool(args.step_fusion))
     if args.case == "activity":
         net.activity_block(1, 4)
     elif args.case == "plasticity":
@@ -827,6 +885,8 @@ def main():
     ap.add_argument("--serve-steps", type=int, default=5000)
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-precision", choices=["fp64", "fp32"], default="fp32")
+    ap.add_argument("--step-fusion", type=int, choices=[0, 1], default=1,
+                    help="1: blocks of activity steps of a network without synapses in one launch (default); 0: one launch per step")
     ap.add_argument("--case", choices=["activity", "search", "plasticity"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()

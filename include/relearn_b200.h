@@ -331,6 +331,14 @@ RL_API rl_status rl_candidate_weights(void* ctx, uint32_t source, int precision,
  * a stream other than the legacy default stream. */
 RL_API rl_status rl_set_graphs(void* ctx, int enable);
 
+/* While the network has no synapses (no in-edges anywhere: the start of a
+ * simulation, before the first connections), a neuron's step reads nothing of
+ * the other neurons, so a block of activity steps runs as one launch with each
+ * neuron's state kept in registers for the whole block (1, the default); 0
+ * runs one launch per step.  The results are the same bits either way.  No
+ * counterpart in the reference (its CPU loops run step by step). */
+RL_API rl_status rl_set_step_fusion(void* ctx, int enable);
+
 /* Turn per-phase CUDA-event timing on (1) or off (0). */
 RL_API rl_status rl_set_profiling(void* ctx, int enable);
 

@@ -166,7 +166,7 @@ ABI_FUNCTIONS = [
     "rl_update_connectivity", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
-    "rl_candidate_weights", "rl_set_graphs", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
+    "rl_candidate_weights", "rl_set_graphs", "rl_set_step_fusion", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
     "rl_serve_fetch", "rl_serve_load", "rl_serve_destroy", "rl_autotune", "rl_get_tuning", "rl_set_tuning",
     "rl_set_target_calcium", "rl_get_target_calcium", "rl_snapshot_neurons", "rl_snapshot_wait",
 ]
@@ -248,6 +248,8 @@ def load_library(path: str = LIB_PATH):
     L.rl_get_phase_times.argtypes = [vp, vp, vp]
     L.rl_set_graphs.restype = st
     L.rl_set_graphs.argtypes = [vp, C.c_int]
+    L.rl_set_step_fusion.restype = st
+    L.rl_set_step_fusion.argtypes = [vp, C.c_int]
     L.rl_candidate_weights.restype = st
     L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
@@ -546,6 +548,11 @@ class Network:
 
     def set_graphs(self, on: bool = True):
         self._check(self.lib.rl_set_graphs(self.h, int(on)))
+
+    def set_step_fusion(self, on: bool = True):
+        """Blocks of activity steps of a network without synapses in one
+        launch (the default), or one launch per step; the same bits."""
+        self._check(self.lib.rl_set_step_fusion(self.h, int(on)))
 
     def set_profiling(self, on: bool = True):
         self._check(self.lib.rl_set_profiling(self.h, int(on)))

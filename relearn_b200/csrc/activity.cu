@@ -123,33 +123,22 @@ __device__ __forceinline__ void disabled_neuron(const ActArgs& A, uint32_t i) {
     A.delta2[i] = A.delta2[i] + 0.0;
 }
 
-// One enabled neuron's step.  H > 0: h_model and h_calcium are both H, fixed
-// at compile time.  MODEL is the neuron model (RL_MODEL_*).  `z` is the
-// neuron's standard normal draw of this step.
-template <int H, int MODEL>
-__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, uint64_t seed,
-                                                uint32_t local, const double* nu, double z) {
-    long long isum = 0;
-    if (D->has_edges) {
-        const uint32_t* __restrict__ off = D->off;
-        const uint32_t* __restrict__ src = D->src;
-        const int32_t* __restrict__ wt = D->w;
-        const uint32_t e0 = off[i], e1 = off[i + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-            if (A.fired_prev[src[e]]) {
-                isum += wt[e];
-            }
-        }
-    }
+// This step's input: the synaptic sum (an integer, exact in any order) times
+// the conductance, then NormalActivityInputCPU's draw z.
+__device__ __forceinline__ double step_input(const ActArgs& A, long long isum, double z) {
     double input = 0.0;
     input += (double)isum * A.conductance;
-    input += A.noise_mean + A.noise_stddev * z;  // NormalActivityInputCPU's draw
-    if (A.input) {
-        A.input[i] = input;
-    }
+    input += A.noise_mean + A.noise_stddev * z;
+    return input;
+}
 
-    double xv = A.x[i];
-    double uv = A.u[i];
+// The neuron model's h substeps on (x, u); returns the spike flag.  H > 0:
+// h_model is H, fixed at compile time.  MODEL is the neuron model (RL_MODEL_*).
+template <int H, int MODEL>
+__device__ __forceinline__ uint8_t model_step(const ActArgs& A, uint32_t step, uint64_t seed, uint32_t local, double input, double& x,
+                                              double& u) {
+    double xv = x;
+    double uv = u;
     uint8_t spiked = 0;
     const uint32_t hm = H > 0 ? (uint32_t)H : A.h_model;
     if (MODEL == RL_MODEL_IZHIKEVICH) {
@@ -210,11 +199,15 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
             }
         }
     }
-    A.x[i] = xv;
-    A.u[i] = uv;
-    A.fired_cur[i] = spiked;
+    x = xv;
+    u = uv;
+    return spiked;
+}
 
-    double ca = A.calcium[i];
+// CalciumCalculatorCPU::update_current_calcium: h substeps of
+// ca += (ca * (-1/tau) + beta * fired) / h.
+template <int H>
+__device__ __forceinline__ double calcium_step(const ActArgs& A, uint8_t spiked, double ca) {
     const uint32_t hc = H > 0 ? (uint32_t)H : A.h_calcium;
     if (spiked) {
         const double local_beta = A.beta * 1.0;
@@ -230,24 +223,59 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
             ca += A.scale_c * (ca * A.tau_inv);
         }
     }
+    return ca;
+}
+
+// The growth of element type t this step (update_number_elements_openmp with
+// gaussian_growth_curve); tgt is the neuron's target calcium when the targets
+// are not uniform.
+__device__ __forceinline__ double growth_step(const ActArgs& A, int t, double ca, double tgt, const double* nu) {
+    if (A.uniform_target) {
+        return growth_curve_pre(ca, A.eta[t], A.flat_u[t], A.xi_u[t], A.zeta_u[t], A.zeta_inv_u[t]) * nu[t];
+    }
+    const double eta = A.eta[t];
+    const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
+    return growth_curve(ca, eta, eps) * nu[t];
+}
+
+// One enabled neuron's step.  `z` is the neuron's standard normal draw of
+// this step.
+template <int H, int MODEL>
+__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, uint64_t seed,
+                                                uint32_t local, const double* nu, double z) {
+    long long isum = 0;
+    if (D->has_edges) {
+        const uint32_t* __restrict__ off = D->off;
+        const uint32_t* __restrict__ src = D->src;
+        const int32_t* __restrict__ wt = D->w;
+        const uint32_t e0 = off[i], e1 = off[i + 1];
+        for (uint32_t e = e0; e < e1; ++e) {
+            if (A.fired_prev[src[e]]) {
+                isum += wt[e];
+            }
+        }
+    }
+    const double input = step_input(A, isum, z);
+    if (A.input) {
+        A.input[i] = input;
+    }
+
+    double xv = A.x[i];
+    double uv = A.u[i];
+    const uint8_t spiked = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
+    A.x[i] = xv;
+    A.u[i] = uv;
+    A.fired_cur[i] = spiked;
+
+    const double ca = calcium_step<H>(A, spiked, A.calcium[i]);
     A.calcium[i] = ca;
 
     double* deltas[3] = { A.delta0, A.delta1, A.delta2 };
-    if (A.uniform_target) {
+    const double tgt = A.uniform_target ? 0.0 : A.target[i];
 #pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const double inc = growth_curve_pre(ca, A.eta[t], A.flat_u[t], A.xi_u[t], A.zeta_u[t], A.zeta_inv_u[t]) * nu[t];
-            deltas[t][i] = deltas[t][i] + inc;
-        }
-    } else {
-        const double tgt = A.target[i];
-#pragma unroll
-        for (int t = 0; t < 3; ++t) {
-            const double eta = A.eta[t];
-            const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
-            const double inc = growth_curve(ca, eta, eps) * nu[t];
-            deltas[t][i] = deltas[t][i] + inc;
-        }
+    for (int t = 0; t < 3; ++t) {
+        const double inc = growth_step(A, t, ca, tgt, nu);
+        deltas[t][i] = deltas[t][i] + inc;
     }
 }
 
@@ -315,6 +343,117 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             activity_neuron<H, MODEL>(A, D, step, i, seed, local, nu, z);
         } else if (i < A.n) {
             disabled_neuron(A, i);
+        }
+    }
+}
+
+// A block of `nsteps` steps in one launch, for a network without synapses:
+// then a neuron's step reads nothing of the other neurons (its input is its
+// own background draw), so each thread carries its neuron's state through the
+// block in registers and touches memory once at each end.  The operations and
+// their order are those of k_activity step by step, so the state is the same
+// bits; so are both spike-flag buffers (the last step's flags in
+// A.fired_cur, the step before's in fired_before_last) and the input (last
+// step).  A disabled neuron keeps x, u, calcium and its spike flag; its
+// deltas become d + 0 as in every step of k_activity.
+template <int BLOCK, int H, int MODEL, bool MULTI>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
+                                                          uint8_t* __restrict__ fired_before_last) {
+    __shared__ double s_p[BLOCK];
+    __shared__ double s_z[BLOCK];
+    __shared__ uint16_t s_who[BLOCK];
+    __shared__ uint32_t s_cnt[2];
+    pdl_wait_then_release();  // every input is the previous launch's output
+    const uint32_t step0 = D->base_step;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (threadIdx.x < 2) {
+        s_cnt[threadIdx.x] = 0u;
+    }
+    __syncthreads();
+    const uint32_t stride = gridDim.x * BLOCK;
+    uint32_t parity = 0;
+    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        const bool in = i < A.n;
+        const bool on = in && A.enabled[i];
+        uint64_t seed = 0;
+        uint32_t local = 0;
+        const double* nu = nullptr;
+        double xv = 0.0, uv = 0.0, ca = 0.0, tgt = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, input = 0.0;
+        uint8_t f = 0;
+        if (in) {
+            f = A.fired_prev[i];
+            d0 = A.delta0[i];
+            d1 = A.delta1[i];
+            d2 = A.delta2[i];
+        }
+        if (on) {
+            neuron_net<MULTI>(A, i, seed, local, nu);
+            xv = A.x[i];
+            uv = A.u[i];
+            ca = A.calcium[i];
+            tgt = A.uniform_target ? 0.0 : A.target[i];
+        }
+        uint8_t f_before = f;
+        for (uint32_t k = 0; k < nsteps; ++k, parity ^= 1u) {
+            const uint32_t step = step0 + k;
+            double p = 0.5;
+            if (on) {
+                p = MULTI ? noise_uniform(seed, step, local) : noise_uniform_rk(A.rk0, A.rk1, step, local);
+            }
+            const bool tail = on && normal_in_tail(p);
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
+            uint32_t first = 0;
+            if (lane == 0 && mask) {
+                first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
+            }
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            if (tail) {
+                const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+                s_p[slot] = p;
+                s_who[slot] = (uint16_t)threadIdx.x;
+            }
+            double z = on && !tail ? normal_quantile_central(p) : 0.0;
+            __syncthreads();
+            const uint32_t cnt = s_cnt[parity];
+            for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
+                s_z[s_who[q]] = normal_quantile_tail(s_p[q]);
+            }
+            if (threadIdx.x == 0) {
+                s_cnt[parity ^ 1u] = 0u;  // the next round's counter; nobody reads it before the barrier below
+            }
+            __syncthreads();
+            if (tail) {
+                z = s_z[threadIdx.x];
+            }
+            if (on) {
+                input = step_input(A, 0, z);
+                f_before = f;
+                f = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
+                ca = calcium_step<H>(A, f, ca);
+                d0 = d0 + growth_step(A, 0, ca, tgt, nu);
+                d1 = d1 + growth_step(A, 1, ca, tgt, nu);
+                d2 = d2 + growth_step(A, 2, ca, tgt, nu);
+            }
+        }
+        if (on) {
+            A.x[i] = xv;
+            A.u[i] = uv;
+            A.calcium[i] = ca;
+            A.delta0[i] = d0;
+            A.delta1[i] = d1;
+            A.delta2[i] = d2;
+        } else if (in) {
+            A.delta0[i] = d0 + 0.0;
+            A.delta1[i] = d1 + 0.0;
+            A.delta2[i] = d2 + 0.0;
+        }
+        if (in) {
+            if (A.input) {
+                A.input[i] = on ? input : 0.0;
+            }
+            A.fired_cur[i] = f;
+            fired_before_last[i] = f_before;
         }
     }
 }
@@ -461,7 +600,9 @@ void launch_act64(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep)
     }
 }
 
-void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
+namespace {
+
+ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
     const rl_config& k = c.cfg;
     ActArgs A;
     A.n = c.n;
@@ -534,10 +675,57 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     A.e_a = k.aeif_a;
     A.e_b = k.aeif_b;
     A.e_V_spike = k.aeif_V_spike;
-    if (k.h_model == 10 && k.h_calcium == 10) {
+    return A;
+}
+
+template <int BLOCK, int H, int MODEL>
+void launch_steps64_m(Ctx& c, const ActArgs& A, uint32_t nsteps, uint8_t* fired_before_last) {
+    const unsigned grid = blocks_for(c.n, BLOCK);
+    if (c.multi()) {
+        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, true>, grid, BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+    } else {
+        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, false>, grid, BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+    }
+}
+
+template <int H>
+void launch_steps64(Ctx& c, const ActArgs& A, uint32_t nsteps, uint8_t* fired_before_last) {
+    switch (c.cfg.neuron_model) {
+        case RL_MODEL_POISSON:
+            launch_steps64_m<128, H, RL_MODEL_POISSON>(c, A, nsteps, fired_before_last);
+            break;
+        case RL_MODEL_FITZHUGH_NAGUMO:
+            launch_steps64_m<128, H, RL_MODEL_FITZHUGH_NAGUMO>(c, A, nsteps, fired_before_last);
+            break;
+        case RL_MODEL_AEIF:
+            launch_steps64_m<128, H, RL_MODEL_AEIF>(c, A, nsteps, fired_before_last);
+            break;
+        default:
+            launch_steps64_m<128, H, RL_MODEL_IZHIKEVICH>(c, A, nsteps, fired_before_last);
+            break;
+    }
+}
+
+}  // namespace
+
+void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
+    const ActArgs A = act64_args(c, kstep, fired_prev, fired_cur);
+    if (c.cfg.h_model == 10 && c.cfg.h_calcium == 10) {
         launch_act64<10>(c, v, A, kstep);
     } else {
         launch_act64<0>(c, v, A, kstep);
+    }
+}
+
+// The whole block of nsteps steps in one launch (a network without synapses).
+void launch_activity_fp64_steps(Ctx& c, uint32_t nsteps) {
+    const int p0 = c.nr.cur & 1;
+    ActArgs A = act64_args(c, nsteps - 1, c.nr.fired[p0].p, c.nr.fired[(p0 + (int)nsteps) & 1].p);
+    uint8_t* before_last = c.nr.fired[(p0 + (int)nsteps - 1) & 1].p;
+    if (c.cfg.h_model == 10 && c.cfg.h_calcium == 10) {
+        launch_steps64<10>(c, A, nsteps, before_last);
+    } else {
+        launch_steps64<0>(c, A, nsteps, before_last);
     }
 }
 
@@ -688,8 +876,17 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         c.tune.act_state = TUNE_DONE;
         drop_activity_graphs(c);
     }
-    const bool graph = c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
-    if (graph) {
+    const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;
+    const bool graph = !fused && c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
+    if (fused) {
+        // no synapses: every neuron's steps are independent of the others'
+        PhaseScope ps(c, PH_ACTIVITY_KERNEL, nsteps);
+        if (is_fp32(c)) {
+            launch_activity_f32_steps(c, nsteps);
+        } else {
+            launch_activity_fp64_steps(c, nsteps);
+        }
+    } else if (graph) {
         const int p = c.nr.cur & 1;
         if (c.act_graph[p] == nullptr || c.act_graph_len != nsteps) {
             for (auto& g : c.act_graph) {

@@ -1158,6 +1158,10 @@ rl_status rl_set_graphs(void* ctx, int enable) {
     return rl::guarded(ctx, [&](Ctx& c) { c.use_graphs = enable != 0; });
 }
 
+rl_status rl_set_step_fusion(void* ctx, int enable) {
+    return rl::guarded(ctx, [&](Ctx& c) { c.step_fusion = enable != 0; });
+}
+
 rl_status rl_set_profiling(void* ctx, int enable) {
     return rl::guarded(ctx, [&](Ctx& c) { c.timer.on = enable != 0; });
 }

@@ -400,6 +400,67 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* 
     }
 }
 
+// A block of `nsteps` steps in one launch, for a network without synapses: a
+// neuron's step then reads nothing of the other neurons, so each thread
+// carries its neuron's state through the block in registers.  The same
+// per-step function and draws as k_activity_f32, so the same bits; the spike
+// flags of the last step go to A.fired_cur and those of the step before to
+// fired_before_last, the input of the last step to A.input.
+template <int H, int BLOCK, bool MULTI, int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const ActDesc* __restrict__ D, uint32_t nsteps,
+                                                              uint8_t* __restrict__ fired_before_last) {
+    pdl_wait_then_release();  // every input is the previous launch's output
+    const uint32_t step0 = D->base_step;
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
+        const bool en = A.enabled[i] != 0;
+        uint8_t f = A.fired_prev[i];
+        float x = A.x[i];
+        float u = A.u[i];
+        double ca = A.calcium[i];
+        float d[3] = { A.delta[0][i], A.delta[1][i], A.delta[2][i] };
+        uint64_t seed = A.seed1;
+        uint32_t local = i;
+        const float* nu = A.nu1;
+        if (MULTI) {
+            const NetInfo& N = A.nets[A.net_of[i]];
+            seed = N.seed;
+            local = i - N.first;
+            nu = N.nu32;
+        }
+        uint8_t f_before = f;
+        float input = 0.0f;
+        for (uint32_t k = 0; k < nsteps; ++k) {
+            const uint32_t step = step0 + k;
+            uint32_t k24 = 0, k24p = 0;
+            if (en) {
+                const u32x4 blk = MULTI ? noise_block(seed, step, local) : noise_block_rk(A.rk0, A.rk1, step, local);
+                k24 = ((local & 1u) ? blk.z : blk.x) >> 8;
+                if (MODEL == RL_MODEL_POISSON) {
+                    const u32x4 w = MULTI ? draw(seed, step, local, 0u, STREAM_POISSON, 0u)
+                                          : philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, A.rk0, A.rk1);
+                    k24p = w.x >> 8;
+                }
+            }
+            uint8_t fired;
+            neuron_f32<H, MODEL>(A, D, i, en, f, k24, k24p, nu, x, u, ca, d, input, fired);
+            f_before = f;
+            f = fired;
+        }
+        A.x[i] = x;
+        A.u[i] = u;
+        A.calcium[i] = ca;
+        A.delta[0][i] = d[0];
+        A.delta[1][i] = d[1];
+        A.delta[2][i] = d[2];
+        if (A.input) {
+            A.input[i] = input;
+        }
+        A.fired_cur[i] = f;
+        fired_before_last[i] = f_before;
+    }
+}
+
 // ElementBaseBase::update with an FP32 delta.
 __global__ void k_commit_f32(uint32_t n, const uint8_t* __restrict__ enabled, double* grown, float* delta, uint32_t* connected, uint32_t* vacant,
                              double retract, uint32_t* to_delete, unsigned long long* total, const unsigned long long* guard, int guard_n) {
@@ -1123,7 +1184,17 @@ void launch_act32_h(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep)
     }
 }
 
-void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
+template <int H, int MODEL = RL_MODEL_IZHIKEVICH>
+void launch_steps32(Ctx& c, const Act32& A, uint32_t nsteps, uint8_t* fired_before_last) {
+    const unsigned grid = blocks_for(c.n, 128);
+    if (c.multi()) {
+        launch_pdl(&k_activity_f32_steps<H, 128, true, MODEL>, grid, 128, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+    } else {
+        launch_pdl(&k_activity_f32_steps<H, 128, false, MODEL>, grid, 128, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+    }
+}
+
+Act32 act32_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur) {
     const rl_config& k = c.cfg;
     Act32 A;
     A.n = c.n;
@@ -1197,6 +1268,12 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
     A.e_a = (float)k.aeif_a;
     A.e_b = (float)k.aeif_b;
     A.e_V_spike = (float)k.aeif_V_spike;
+    return A;
+}
+
+void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v) {
+    const rl_config& k = c.cfg;
+    const Act32 A = act32_args(c, kstep, fired_prev, fired_cur);
     if (k.neuron_model == RL_MODEL_POISSON) {
         launch_act32_h<0, RL_MODEL_POISSON>(c, v, A, kstep);
     } else if (k.neuron_model == RL_MODEL_FITZHUGH_NAGUMO) {
@@ -1207,6 +1284,25 @@ void launch_activity_f32(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint
         launch_act32_h<10>(c, v, A, kstep);
     } else {
         launch_act32_h<0>(c, v, A, kstep);
+    }
+}
+
+// The whole block of nsteps steps in one launch (a network without synapses).
+void launch_activity_f32_steps(Ctx& c, uint32_t nsteps) {
+    const rl_config& k = c.cfg;
+    const int p0 = c.nr.cur & 1;
+    const Act32 A = act32_args(c, nsteps - 1, c.nr.fired[p0].p, c.nr.fired[(p0 + (int)nsteps) & 1].p);
+    uint8_t* before_last = c.nr.fired[(p0 + (int)nsteps - 1) & 1].p;
+    if (k.neuron_model == RL_MODEL_POISSON) {
+        launch_steps32<0, RL_MODEL_POISSON>(c, A, nsteps, before_last);
+    } else if (k.neuron_model == RL_MODEL_FITZHUGH_NAGUMO) {
+        launch_steps32<0, RL_MODEL_FITZHUGH_NAGUMO>(c, A, nsteps, before_last);
+    } else if (k.neuron_model == RL_MODEL_AEIF) {
+        launch_steps32<0, RL_MODEL_AEIF>(c, A, nsteps, before_last);
+    } else if (k.h_model == 10) {
+        launch_steps32<10>(c, A, nsteps, before_last);
+    } else {
+        launch_steps32<0>(c, A, nsteps, before_last);
     }
 }
 

@@ -273,6 +273,7 @@ struct Ctx {
     uint32_t act_graph_len = 0;
     uint32_t act_block_len = 0;  // steps of the activity block being issued: only its last step stores the input
     bool use_graphs = true;
+    bool step_fusion = true;  // blocks of steps of a network without synapses in one launch
     bool capturing = false;
     std::vector<NetInfo> nets;  // host copy
     DBuf<NetInfo> d_nets;
@@ -360,6 +361,9 @@ void f32_from_f64(Ctx& c);  // state arrays FP64 -> FP32 (after a host upload)
 void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download)
 void launch_activity_f32(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);
 void launch_activity_fp64(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);
+// A block of nsteps steps in one launch; only for a network without synapses.
+void launch_activity_f32_steps(Ctx& c, uint32_t nsteps);
+void launch_activity_fp64_steps(Ctx& c, uint32_t nsteps);
 uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,

@@ -234,6 +234,12 @@ struct Server {
         if ((st = rl_set_graphs(ctx, sc.use_graphs)) != RL_OK) {
             return fail(st, "rl_set_graphs");
         }
+        // One launch per activity step: a fused block of steps keeps its SMs
+        // for the whole block (about a millisecond for a large network), which
+        // holds back the kernels of the requests running beside it.
+        if ((st = rl_set_step_fusion(ctx, 0)) != RL_OK) {
+            return fail(st, "rl_set_step_fusion");
+        }
         if ((st = rl_autotune(ctx, sc.autotune)) != RL_OK) {
             return fail(st, "rl_autotune");
         }
