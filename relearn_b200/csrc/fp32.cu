@@ -131,7 +131,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 
 // `k24`: the neuron's 24 random bits of this step's background draw;
 // `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
-template <int H, int MODEL>
+template <int H, int MODEL, bool EDGES = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
                                            uint32_t k24p, const float* nu, float& x, float& u, double& ca, float (&delta)[3], float& input,
                                            uint8_t& fired) {
@@ -141,7 +141,7 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
         return;
     }
     int isum = 0;
-    if (D->has_edges) {
+    if (EDGES && D->has_edges) {  // EDGES false: a network without synapses (the block kernel)
         const uint32_t* __restrict__ off = D->off;
         const uint32_t* __restrict__ src = D->src;
         const int32_t* __restrict__ wt = D->w;
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
                 }
             }
             uint8_t fired;
-            neuron_f32<H, MODEL>(A, D, i, en, f, k24, k24p, nu, x, u, ca, d, input, fired);
+            neuron_f32<H, MODEL, false>(A, D, i, en, f, k24, k24p, nu, x, u, ca, d, input, fired);
             f_before = f;
             f = fired;
         }
