@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
 // step).  A disabled neuron keeps x, u, calcium and its spike flag; its
 // deltas become d + 0 as in every step of k_activity.
 template <int BLOCK, int H, int MODEL, bool MULTI>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
+__global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
                                                           uint8_t* __restrict__ fired_before_last) {
     __shared__ double s_p[BLOCK];
     __shared__ double s_z[BLOCK];
