@@ -210,15 +210,15 @@ B200_SMS = 148
 # launch, state in registers), from ncu's instruction mix of a 4-step launch
 # at 1M neurons (profiles/k_activity_steps_1M.md), per neuron-step:
 # k_activity_steps 10.77 FP64 warp instructions (43.10M / 4 steps / 1M);
-# k_activity_f32_steps 7.85 warp instructions of every kind (31.41M / 4 / 1M),
+# k_activity_f32_steps 6.97 warp instructions of every kind (27.89M / 4 / 1M),
 # issued at one per SM sub-partition (4 per SM) per cycle.
 FUSED64_FP64_WARP_INSTR = 10.77
-FUSED32_WARP_INSTR = 7.85
+FUSED32_WARP_INSTR = 6.97
 # memory per neuron and launch: reads enabled, spike flag, x, u, calcium, three
 # deltas; writes x, u, calcium, deltas, both spike-flag buffers, the input
 FUSED_BYTES = {0: 50 + 58, 1: 30 + 34}
 # ncu dram read + write of that 4-step launch (the same for any block length)
-FUSED_TRAFFIC = {0: 50.03e6 + 4.35e6, 1: 30.01e6 + 0.20e6}
+FUSED_TRAFFIC = {0: 50.03e6 + 4.35e6, 1: 30.03e6 + 0.13e6}
 
 
 def fp64_pipe_roofline(roof: dict, n: int, sm_mhz) -> dict:

@@ -412,17 +412,30 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
     pdl_wait_then_release();  // every input is the previous launch's output
     const uint32_t step0 = D->base_step;
     const uint32_t stride = gridDim.x * BLOCK;
-    for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < A.n; i += stride) {
-        const bool en = A.enabled[i] != 0;
-        uint8_t f = A.fired_prev[i];
-        float x = A.x[i];
-        float u = A.u[i];
-        double ca = A.calcium[i];
-        float d[3] = { A.delta[0][i], A.delta[1][i], A.delta[2][i] };
+    const uint32_t lane = threadIdx.x & 31u;
+    // the trip count is the same for the whole block (the pair draws below
+    // exchange words between lanes)
+    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        const bool in = i < A.n;
+        const bool en = in && A.enabled[i] != 0;
+        uint8_t f = 0;
+        float x = 0.0f, u = 0.0f;
+        double ca = 0.0;
+        float d[3] = { 0.0f, 0.0f, 0.0f };
+        if (in) {
+            f = A.fired_prev[i];
+            x = A.x[i];
+            u = A.u[i];
+            ca = A.calcium[i];
+            d[0] = A.delta[0][i];
+            d[1] = A.delta[1][i];
+            d[2] = A.delta[2][i];
+        }
         uint64_t seed = A.seed1;
         uint32_t local = i;
         const float* nu = A.nu1;
-        if (MULTI) {
+        if (MULTI && in) {
             const NetInfo& N = A.nets[A.net_of[i]];
             seed = N.seed;
             local = i - N.first;
@@ -430,34 +443,52 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
         }
         uint8_t f_before = f;
         float input = 0.0f;
-        for (uint32_t k = 0; k < nsteps; ++k) {
-            const uint32_t step = step0 + k;
-            uint32_t k24 = 0, k24p = 0;
-            if (en) {
-                const u32x4 blk = MULTI ? noise_block(seed, step, local) : noise_block_rk(A.rk0, A.rk1, step, local);
-                k24 = ((local & 1u) ? blk.z : blk.x) >> 8;
-                if (MODEL == RL_MODEL_POISSON) {
-                    const u32x4 w = MULTI ? draw(seed, step, local, 0u, STREAM_POISSON, 0u)
-                                          : philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, A.rk0, A.rk1);
-                    k24p = w.x >> 8;
-                }
+        auto one_step = [&](uint32_t step, uint32_t word) {
+            uint32_t k24p = 0;
+            if (MODEL == RL_MODEL_POISSON && en) {
+                const u32x4 w = MULTI ? draw(seed, step, local, 0u, STREAM_POISSON, 0u)
+                                      : philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, A.rk0, A.rk1);
+                k24p = w.x >> 8;
             }
             uint8_t fired;
-            neuron_f32<H, MODEL, false>(A, D, i, en, f, k24, k24p, nu, x, u, ca, d, input, fired);
+            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, x, u, ca, d, input, fired);
             f_before = f;
             f = fired;
+        };
+        uint32_t k = 0;
+        if (!MULTI) {
+            // Lanes 2m and 2m + 1 hold the neuron pair m (i = local, BLOCK a
+            // multiple of 32), whose background draws of a step are one Philox
+            // block (words x and z).  The even lane computes the block of step
+            // k, the odd lane that of step k + 1, and each hands the other the
+            // word it needs: one block per lane for two steps.
+            const bool odd = (lane & 1u) != 0;
+            for (; k + 1 < nsteps; k += 2) {
+                const u32x4 blk = noise_block_rk(A.rk0, A.rk1, step0 + k + (odd ? 1u : 0u), i);
+                const uint32_t got = __shfl_xor_sync(0xFFFFFFFFu, odd ? blk.x : blk.z, 1);
+                const uint32_t own = odd ? blk.z : blk.x;
+                one_step(step0 + k, odd ? got : own);
+                one_step(step0 + k + 1, odd ? own : got);
+            }
         }
-        A.x[i] = x;
-        A.u[i] = u;
-        A.calcium[i] = ca;
-        A.delta[0][i] = d[0];
-        A.delta[1][i] = d[1];
-        A.delta[2][i] = d[2];
-        if (A.input) {
-            A.input[i] = input;
+        for (; k < nsteps; ++k) {
+            const uint32_t step = step0 + k;
+            const u32x4 blk = MULTI ? noise_block(seed, step, local) : noise_block_rk(A.rk0, A.rk1, step, local);
+            one_step(step, (local & 1u) ? blk.z : blk.x);
         }
-        A.fired_cur[i] = f;
-        fired_before_last[i] = f_before;
+        if (in) {
+            A.x[i] = x;
+            A.u[i] = u;
+            A.calcium[i] = ca;
+            A.delta[0][i] = d[0];
+            A.delta[1][i] = d[1];
+            A.delta[2][i] = d[2];
+            if (A.input) {
+                A.input[i] = input;
+            }
+            A.fired_cur[i] = f;
+            fired_before_last[i] = f_before;
+        }
     }
 }
 
