@@ -565,8 +565,9 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     if fused:
         # no synapses in any network: each 100-step block ran as one launch for all networks
         roof = fused_roofline(1, total, 1e3 * act_ms / act_cnt, act_cnt, None, hbm, peak_kind, False)
-        roof["note"] = ("instruction count of the one-network kernel; the batched kernel draws per neuron (no pair sharing, "
-                        "round keys per network), so it issues more and frac is a lower bound")
+        roof["note"] = ("instruction count of the one-network kernel; the batched kernel shares the draws of a neuron pair only in "
+                        "warps whose lane pairs hold even-odd pairs of one network and derives round keys per network, so it "
+                        "issues more and frac is a lower bound")
         how = "100-step activity blocks, one launch each"
     else:
         roof = {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

@@ -456,15 +456,24 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
             f = fired;
         };
         uint32_t k = 0;
-        if (!MULTI) {
-            // Lanes 2m and 2m + 1 hold the neuron pair m (i = local, BLOCK a
-            // multiple of 32), whose background draws of a step are one Philox
-            // block (words x and z).  The even lane computes the block of step
-            // k, the odd lane that of step k + 1, and each hands the other the
-            // word it needs: one block per lane for two steps.
+        bool share = true;
+        if (MULTI) {
+            // in a batched context only where every lane pair of the warp holds
+            // an even-odd pair of one network
+            const uint64_t pseed = __shfl_xor_sync(0xFFFFFFFFu, seed, 1);
+            const uint32_t plocal = __shfl_xor_sync(0xFFFFFFFFu, local, 1);
+            share = __all_sync(0xFFFFFFFFu, in && (local & 1u) == (lane & 1u) && pseed == seed && (plocal ^ 1u) == local) != 0;
+        }
+        if (share) {
+            // Lanes 2m and 2m + 1 hold a neuron pair (BLOCK a multiple of 32),
+            // whose background draws of a step are one Philox block (words x
+            // and z).  The even lane computes the block of step k, the odd lane
+            // that of step k + 1, and each hands the other the word it needs:
+            // one block per lane for two steps.
             const bool odd = (lane & 1u) != 0;
             for (; k + 1 < nsteps; k += 2) {
-                const u32x4 blk = noise_block_rk(A.rk0, A.rk1, step0 + k + (odd ? 1u : 0u), i);
+                const uint32_t st = step0 + k + (odd ? 1u : 0u);
+                const u32x4 blk = MULTI ? noise_block(seed, st, local) : noise_block_rk(A.rk0, A.rk1, st, i);
                 const uint32_t got = __shfl_xor_sync(0xFFFFFFFFu, odd ? blk.x : blk.z, 1);
                 const uint32_t own = odd ? blk.z : blk.x;
                 one_step(step0 + k, odd ? got : own);
