@@ -241,6 +241,19 @@ RL_API rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* ou
 /* Synaptic-element state per type (RL_AXON, RL_DENDRITE_EXC, RL_DENDRITE_INH):
  * grown (double), delta since the last commit (double), connected and vacant
  * counts (uint32).  NULL pointers are skipped. */
+/* ForwardConnector::process_requests + process_responses
+ * (algorithm/Connector.cpp:33-197) over a caller-given list of `count`
+ * requests, the form the reference's connector tests drive: requests are
+ * processed in the keyed random order of rl_update_connectivity; a request
+ * whose target is its source fails, and so does one whose target has no
+ * vacant dendrite of the request's type left; an accepted request binds one
+ * vacant dendrite of the target and one vacant axon of the source and adds a
+ * synapse of weight +1 (excitatory) or -1 (inhibitory).  A source needs a
+ * vacant axon per accepted request (else RL_ERR_DEVICE).  `accepted` (may be
+ * NULL) receives one flag per request in the caller's order; *created the
+ * number of synapses formed. */
+RL_API rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created);
+
 RL_API rl_status rl_set_elements(void* ctx, int type, const double* grown, const double* delta, const uint32_t* connected, const uint32_t* vacant);
 RL_API rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uint32_t* connected, uint32_t* vacant);
 
@@ -307,14 +320,25 @@ RL_API rl_status rl_set_stream(void* ctx, void* cuda_stream);
  * octree (a runtime that hands out all device memory from its own pool or
  * budget, or a host that must not touch the allocator once set-up is done).
  * Inputs are DEVICE arrays of n entries (vacant excitatory and inhibitory
- * dendrites, optional plasticity flags); the result goes to the context's
- * octree.  The call allocates nothing: its scratch (one counter per octree
- * node) is a file-scope device array of 2,097,152 counters (8 MiB) that every
- * GPU loading the library holds until exit; larger trees are rejected with
+ * dendrites, optional plasticity flags, NULL = the enabled flags); the result
+ * goes to the context's octree, and the dendrite counts and flags are copied
+ * into the context's own arrays, which the connector of the next
+ * rl_update_connectivity accepts against.  The vacant AXON counts (the search
+ * sources) are not an input here: they stay as the last commit or
+ * rl_prepare_update_connectivity left them.
+ * The call allocates nothing: its scratch (one counter per octree node) is a
+ * file-scope device array of 2,097,152 counters (8 MiB) that every GPU
+ * loading the library holds until exit; larger trees are rejected with
  * RL_ERR_OVERFLOW.  All calls share that array, so calls that overlap on the
- * GPU race.  The first call on a device looks up the array's device address
- * and should come before any stream capture.  Work is enqueued on cuda_stream
- * (NULL: the context's stream); the caller synchronizes before reading. */
+ * GPU race.  The first call on a device looks up the array's device address,
+ * and the first call on a context creates two events that order a caller
+ * stream against the context's stream; both should come before any stream
+ * capture.  Work is enqueued on cuda_stream (NULL: the context's stream)
+ * after the context's earlier work, and the context's later work waits for
+ * it; the caller synchronizes that stream before reading results on the
+ * host.  Device errors of this call are reported by the next call that
+ * checks for them (rl_synchronize does).  The caller's current device is
+ * left as it was. */
 RL_API rl_status rl_prepare_update_connectivity_noalloc(void* ctx, const uint32_t* d_vacant_exc, const uint32_t* d_vacant_inh,
                                                         const uint8_t* d_update, void* cuda_stream);
 

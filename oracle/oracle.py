@@ -147,6 +147,17 @@ def lib():
         L.orc_normal.restype = dbl
         L.orc_normal.argtypes = [u64, u32, u32, dbl, dbl]
         L.orc_philox.argtypes = [u32] * 6 + [vp]
+        L.orc_connect_requests.restype = u64
+        L.orc_connect_requests.argtypes = [vp, u32, vp, u64, vp]
+        L.orc_octant_of.restype = C.c_int
+        L.orc_octant_of.argtypes = [vp, vp, vp]
+        L.orc_box_for_octant.argtypes = [vp, vp, C.c_int, vp, vp]
+        L.orc_acceptance.restype = C.c_int
+        L.orc_acceptance.argtypes = [C.c_int, vp, vp, u32, vp, vp, dbl]
+        L.orc_nodes_to_consider.restype = u64
+        L.orc_nodes_to_consider.argtypes = [vp, vp, C.c_int, vp, u64]
+        L.orc_find_target.restype = C.c_int64
+        L.orc_find_target.argtypes = [vp, u32, vp, C.c_int, u32, u32]
     return _lib
 
 
@@ -227,6 +238,27 @@ class OracleSim:
         acc = np.zeros(max(m, 1), np.uint8)
         created = int(lib().orc_connect(self.h, step, _p(acc)))
         return created, acc[:m].copy()
+
+    def connect_requests(self, step: int, requests: np.ndarray):
+        """Connector over a given request list (REQ_DTYPE): returns the
+        number created and one accepted flag per request."""
+        req = np.ascontiguousarray(requests, REQ_DTYPE)
+        acc = np.zeros(max(len(req), 1), np.uint8)
+        created = int(lib().orc_connect_requests(self.h, step, _p(req), len(req), _p(acc)))
+        return created, acc[: len(req)].copy()
+
+    def nodes_to_consider(self, position, dendrite_type: int) -> np.ndarray:
+        """Candidates of a walk from the root for a source at `position`, as
+        breadth-first node indices (those of tree()), in visiting order."""
+        p = np.ascontiguousarray(position, np.float64)
+        cap = int(lib().orc_num_nodes(self.h))
+        out = np.zeros(max(cap, 1), np.int32)
+        k = int(lib().orc_nodes_to_consider(self.h, _p(p), dendrite_type, _p(out), cap))
+        return out[:k].copy()
+
+    def find_target(self, source: int, position, dendrite_type: int, step: int, j: int = 0) -> int:
+        p = np.ascontiguousarray(position, np.float64)
+        return int(lib().orc_find_target(self.h, source, _p(p), dendrite_type, step, j))
 
     def simulate(self, first_step: int, count: int):
         lib().orc_simulate(self.h, first_step, count)
@@ -312,3 +344,28 @@ def philox(c0, c1, c2, c3, k0, k1):
     out = np.zeros(4, np.uint32)
     lib().orc_philox(c0, c1, c2, c3, k0, k1, _p(out))
     return [int(v) for v in out]
+
+
+def octant_of(bmin, bmax, position) -> int:
+    """Cell::get_octant_for_position of one box; -1 outside the box."""
+    a, b, p = (np.ascontiguousarray(v, np.float64) for v in (bmin, bmax, position))
+    return int(lib().orc_octant_of(_p(a), _p(b), _p(p)))
+
+
+def box_for_octant(bmin, bmax, octant: int):
+    """Cell::get_size_for_octant of one box: (lo, hi)."""
+    a, b = (np.ascontiguousarray(v, np.float64) for v in (bmin, bmax))
+    lo = np.zeros(3)
+    hi = np.zeros(3)
+    lib().orc_box_for_octant(_p(a), _p(b), int(octant), _p(lo), _p(hi))
+    return lo, hi
+
+
+DISCARD, EXPAND, ACCEPT = 0, 1, 2
+
+
+def acceptance(parent: bool, bmin, bmax, count: int, dendrite_position, source_position, theta: float) -> int:
+    """BarnesHutBase::test_acceptance_criterion of one node: DISCARD, EXPAND,
+    ACCEPT, or -1 for a theta outside (0, 0.5]."""
+    a, b, d, s = (np.ascontiguousarray(v, np.float64) for v in (bmin, bmax, dendrite_position, source_position))
+    return int(lib().orc_acceptance(int(parent), _p(a), _p(b), int(count), _p(d), _p(s), float(theta)))

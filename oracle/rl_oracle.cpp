@@ -1146,6 +1146,100 @@ uint64_t orc_connect(void* h, uint32_t step, uint8_t* accepted_out) {
     return created;
 }
 
+// Connector over a caller-given request list (ForwardConnector::process_requests
+// + process_responses, Connector.cpp:33-197), as the reference's connector
+// tests drive it.  accepted_out gets one flag per request.
+uint64_t orc_connect_requests(void* h, uint32_t step, const orc_request* req, uint64_t m, uint8_t* accepted_out) {
+    Sim* s = static_cast<Sim*>(h);
+    std::vector<orc_request> list(req, req + m);
+    std::vector<uint8_t> accepted;
+    const uint64_t created = connect(*s, step, list, accepted);
+    s->total_created += created;
+    if (accepted_out) {
+        std::copy(accepted.begin(), accepted.end(), accepted_out);
+    }
+    return created;
+}
+
+// Cell::get_octant_for_position (Cell.h:104-137) of one cell box; -1 when
+// the position lies outside the box (the reference throws).
+int orc_octant_of(const double* bmin, const double* bmax, const double* pos) {
+    Node n{};
+    n.bmin = V3{ bmin[0], bmin[1], bmin[2] };
+    n.bmax = V3{ bmax[0], bmax[1], bmax[2] };
+    const V3 p{ pos[0], pos[1], pos[2] };
+    if (!in_box(p, n.bmin, n.bmax)) {
+        return -1;
+    }
+    return octant_of(n, p);
+}
+
+// Cell::get_size_for_octant (Cell.h:145-178) of one cell box.
+void orc_box_for_octant(const double* bmin, const double* bmax, int oct, double* lo, double* hi) {
+    Node n{};
+    n.bmin = V3{ bmin[0], bmin[1], bmin[2] };
+    n.bmax = V3{ bmax[0], bmax[1], bmax[2] };
+    V3 a, b;
+    box_for_octant(n, oct, a, b);
+    lo[0] = a.x;
+    lo[1] = a.y;
+    lo[2] = a.z;
+    hi[0] = b.x;
+    hi[1] = b.y;
+    hi[2] = b.z;
+}
+
+// BarnesHutBase::test_acceptance_criterion (BarnesHutBase.h:72-114) of one
+// node: a leaf (parent = 0) or an inner node with the given cell box, vacant
+// dendrite count and dendrite position.  Returns 0 discard, 1 expand,
+// 2 accept, -1 for theta outside (0, 0.5] (the reference throws).
+int orc_acceptance(int parent, const double* bmin, const double* bmax, uint32_t count, const double* dpos, const double* src, double theta) {
+    if (!(theta > 0.0) || theta > 0.5) {
+        return -1;
+    }
+    Node n{};
+    n.parent = parent != 0;
+    n.bmin = V3{ bmin[0], bmin[1], bmin[2] };
+    n.bmax = V3{ bmax[0], bmax[1], bmax[2] };
+    n.cnt[0] = count;
+    n.has_dpos[0] = true;
+    n.dpos[0] = V3{ dpos[0], dpos[1], dpos[2] };
+    double d = 0.0;
+    const Status st = acceptance(n, V3{ src[0], src[1], src[2] }, 0, theta, d);
+    return st == Status::Discard ? 0 : (st == Status::Expand ? 1 : 2);
+}
+
+// BarnesHutBase::get_nodes_to_consider (BarnesHutBase.h:129-206) from the
+// root for a source position and dendrite type (0 exc, 1 inh) on the current
+// tree, with the simulation's theta.  Nodes are reported by their index in
+// orc_dump_tree's breadth-first order, in the walk's visiting order.
+uint64_t orc_nodes_to_consider(void* h, const double* src, int type, int32_t* out, uint64_t capacity) {
+    const Sim* s = static_cast<Sim*>(h);
+    const auto order = s->tree.bfs_order();
+    std::vector<int32_t> bfs_index(s->tree.pool.size(), -1);
+    for (size_t i = 0; i < order.size(); ++i) {
+        bfs_index[order[i]] = (int32_t)i;
+    }
+    std::vector<int> cand;
+    SearchStats st;
+    nodes_to_consider(s->tree, V3{ src[0], src[1], src[2] }, 0, type, s->cfg.theta, cand, st);
+    for (size_t i = 0; i < cand.size() && i < capacity; ++i) {
+        out[i] = bfs_index[cand[i]];
+    }
+    return cand.size();
+}
+
+// BarnesHutBase::find_target_neuron (BarnesHutBase.h:223-255) for one source
+// id at a given position, dendrite type and vacant-axon index j: the target
+// neuron, or -1 when the search fails.
+int64_t orc_find_target(void* h, uint32_t source, const double* src, int type, uint32_t step, uint32_t j) {
+    const Sim* s = static_cast<Sim*>(h);
+    std::vector<int> cand;
+    std::vector<double> w;
+    SearchStats st;
+    return find_target(*s, source, V3{ src[0], src[1], src[2] }, type, step, j, cand, w, st);
+}
+
 // Run steps first..first+count-1 of Simulation::simulate: every step one
 // activity update, every plasticity_interval-th step a plasticity update.
 void orc_simulate(void* h, uint32_t first_step, uint32_t count) {

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librelearn_b200.so")
 SOURCES = ["prims.cu", "octree.cu", "bh_search.cu", "connector.cu", "activity.cu", "capi.cu", "noalloc.cu", "fp32.cu", "serve.cpp"]
-HEADERS = ["rl_internal.cuh", "rl_context.cuh", "rl_math.cuh"]
+HEADERS = ["rl_internal.cuh", "rl_context.cuh", "rl_math.cuh", "bh_eval.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include", "relearn_b200.h")
 
 # -fmad=false: no multiply-add contraction, so FP64 results match the CPU

@@ -29,6 +29,7 @@
 //     pick pass over the chosen node's subtree.
 //   * Walks carry no stack: they follow per-node escape links.
 //   * A persistent form keeps the top levels of the octree in shared memory.
+#include "bh_eval.cuh"
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -36,7 +37,6 @@ namespace rl {
 namespace {
 
 
-enum : int { ST_DISCARD = 0, ST_EXPAND = 1, ST_ACCEPT = 2 };
 
 struct SearchArgs {
     const double4* rec;  // records of the searched dendrite type
@@ -73,43 +73,6 @@ struct WarpNet {
     uint32_t root;
     uint32_t first;
 };
-
-__device__ __forceinline__ uint32_t rcount(const double4& r) {
-    return (uint32_t)__double_as_longlong(r.w);
-}
-
-struct Eval {
-    int status;
-    double w;
-};
-
-// test_acceptance_criterion + calculate_attractiveness_to_connect for one node.
-__device__ __forceinline__ Eval evaluate(const double4& r, uint2 t, double md, double sx, double sy, double sz, uint32_t source, double theta, double mu,
-                                         double scale, bool fallback, const KernelParams& K) {
-    Eval e{ ST_DISCARD, 0.0 };
-    const uint32_t cnt = rcount(r);
-    if (cnt == 0) {
-        return e;
-    }
-    const double d = rl_hypot3(r.x - sx, r.y - sy, r.z - sz);
-    if (d == 0.0) {
-        return e;
-    }
-    const bool leaf = topo_leaf(t.y);
-    if (!leaf && !(md < theta * d)) {
-        e.status = ST_EXPAND;
-        return e;
-    }
-    e.status = ST_ACCEPT;
-    if (leaf && t.x == source) {
-        e.w = 0.0;  // a neuron never connects to itself
-    } else if (!fallback) {
-        e.w = (rl_kernel_prob(K.type, d, mu, scale, K.k_minus_1, K.a, K.b, K.cutoff, K.cutoff_inf) * 1.0) * (double)cnt;
-    } else {
-        e.w = (double)cnt / d;
-    }
-    return e;
-}
 
 // Random number of ProbabilityPicker::pick_target(values, key) for a total.
 __device__ __forceinline__ double pick_threshold(double total, uint64_t seed, uint32_t step, uint32_t source, uint32_t j, uint32_t depth) {

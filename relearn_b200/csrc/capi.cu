@@ -739,6 +739,12 @@ void discard(Ctx* c) {
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
     }
+    for (cudaEvent_t e : { c->noalloc_before, c->noalloc_after }) {
+        if (e) {
+            cudaEventSynchronize(e);
+            cudaEventDestroy(e);
+        }
+    }
     for (int p = 0; p < rl::PH_COUNT; ++p) {
         for (auto& pr : c->timer.pending[p]) {
             cudaEventDestroy(pr.start);
@@ -881,6 +887,49 @@ rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* out, uint
                 out[i] = rl_synapse{ t[i], s[i], w[i], 0u };
             }
         }
+        rl::rebuild_graph(c);
+    });
+}
+
+rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(count == 0 || requests != nullptr, RL_ERR_INVALID, "requests are required");
+        RL_CHECK(count < ((uint64_t)1 << 32), RL_ERR_INVALID, "at most 2^32 - 1 requests per call");
+        std::vector<uint32_t> t(count), s(count), j(count), g(count);
+        for (uint64_t i = 0; i < count; ++i) {
+            const rl_request& r = requests[i];
+            RL_CHECK(r.target < c.n && r.source < c.n, RL_ERR_INVALID, "request " + std::to_string(i) + ": neuron id out of range");
+            RL_CHECK(r.signal <= 1, RL_ERR_INVALID, "request " + std::to_string(i) + ": signal must be 0 or 1");
+            t[i] = r.target;
+            s[i] = r.source;
+            j[i] = r.j;
+            g[i] = r.signal;
+        }
+        rl::Search& S = c.search;
+        if (count) {
+            S.req_tgt.ensure(count);
+            S.req_src.ensure(count);
+            S.req_j.ensure(count);
+            S.req_sig.ensure(count);
+            rl::upload(S.req_tgt, t.data(), count, c.stream);
+            rl::upload(S.req_src, s.data(), count, c.stream);
+            rl::upload(S.req_j, j.data(), count, c.stream);
+            rl::upload(S.req_sig, g.data(), count, c.stream);
+        }
+        S.num_requests = count;
+        const uint64_t m = rl::run_connector(c, step);
+        if (created) *created = m;
+        if (accepted && count) {
+            // the connector keeps its flags in processing order; cidx maps back to the request
+            std::vector<uint32_t> flag(count), perm(count);
+            RL_CUDA_TRY(cudaMemcpyAsync(flag.data(), S.accepted.p, count * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaMemcpyAsync(perm.data(), S.cidx.p, count * 4, cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            for (uint64_t p = 0; p < count; ++p) {
+                accepted[perm[p]] = flag[p] ? 1 : 0;
+            }
+        }
+        S.num_requests = 0;
         rl::rebuild_graph(c);
     });
 }

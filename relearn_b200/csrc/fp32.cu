@@ -22,6 +22,7 @@
 // Errors against the FP64 form are measured, not assumed (bench.py
 // --precision-report): selection probabilities, calcium drift, distances of
 // formed synapses.
+#include "bh_eval.cuh"
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -1060,10 +1061,13 @@ Search32Kernel fp32_search_kernel(const SearchVariant& v) {
 }
 
 // ----------------------------------------------------------- diagnostic
+// The weights come from the functions the production searches evaluate every
+// node with: evaluate (FP64, k_search) and eval32 (FP32, k_search_f32), on
+// the searches' own parameters (A32: mu and kernel; W32: the network's theta,
+// 1/sigma^2 and frame).
 __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint2* topo, const double* md64, const uint4* meta, double sx, double sy,
                              double sz, uint32_t source, uint32_t root, int precision, double theta, double mu, double sigma, uint32_t* nodes, double* w,
-                             uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f, KernelParams K) {
-    const Kernel32 K32{ K.type, K.cutoff_inf, (float)K.k_minus_1, (float)K.a, (float)K.b, (float)K.cutoff };
+                             uint64_t capacity, unsigned long long* count, uint32_t* err, QFrame f, KernelParams K, Search32 A32, Net32 W32) {
     const QPos sp{ quantize(sx, f.origin[0], f.inv_quantum), quantize(sy, f.origin[1], f.inv_quantum), quantize(sz, f.origin[2], f.inv_quantum) };
     uint32_t fnode[kStack];
     uint32_t frem[kStack];
@@ -1072,7 +1076,6 @@ __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint
     frem[0] = topo_mask(topo[root].y);
     uint64_t k = 0;
     const double scale = -1.0 / (sigma * sigma);
-    const float inv_s2 = (float)(1.0 / (sigma * sigma));
     while (depth > 0) {
         const int top = depth - 1;
         const uint32_t rem = frem[top];
@@ -1084,42 +1087,17 @@ __global__ void k_candidates(const double4* rec64, const uint4* recq, const uint
         frem[top] = rem & ~(1u << oct);
         const uint32_t child = child_of(topo[fnode[top]], oct);
         const uint2 tt = topo[child];
-        const bool leaf = topo_leaf(tt.y);
         int status = S_DISCARD;
         double weight = 0.0;
         if (precision == RL_PRECISION_FP64) {
-            const double4 r = rec64[child];
-            const uint32_t cnt = (uint32_t)__double_as_longlong(r.w);
-            if (cnt) {
-                const double d = rl_hypot3(r.x - sx, r.y - sy, r.z - sz);
-                if (d != 0.0) {
-                    if (!leaf && !(md64[child] < theta * d)) {
-                        status = S_EXPAND;
-                    } else {
-                        status = S_ACCEPT;
-                        weight = (leaf && tt.x == source) ? 0.0
-                                                          : (rl_kernel_prob(K.type, d, mu, scale, K.k_minus_1, K.a, K.b, K.cutoff, K.cutoff_inf) * 1.0) *
-                                                                (double)cnt;
-                    }
-                }
-            }
+            const Eval e = evaluate(rec64[child], tt, md64[child], sx, sy, sz, source, theta, mu, scale, false, K);
+            status = e.status == ST_ACCEPT ? S_ACCEPT : (e.status == ST_EXPAND ? S_EXPAND : S_DISCARD);
+            weight = e.w;
         } else {
-            const uint4 r = recq[child];
-            const uint32_t cnt = r.w;
-            if (cnt) {
-                const float dx = qdiff(r.x, sp.x, f.quantum), dy = qdiff(r.y, sp.y, f.quantum), dz = qdiff(r.z, sp.z, f.quantum);
-                const float d = dist32(dx, dy, dz);
-                if (d != 0.0f) {
-                    if (!leaf && !(mmaxdim(meta[child]) < (float)theta * d)) {
-                        status = S_EXPAND;
-                    } else {
-                        status = S_ACCEPT;
-                        const float dm = d - (float)mu;
-                        const float kp = K.type == RL_KERNEL_GAUSSIAN ? __expf(-(dm * dm) * inv_s2) : kernel_prob32(K32, d);
-                        weight = (leaf && tt.x == source) ? 0.0 : (double)(kp * (float)cnt);
-                    }
-                }
-            }
+            const uint4 m = meta[child];
+            const E32 e = eval32(recq[child], mtopo(m), mmaxdim(m), sp, source, A32, W32, false);
+            status = e.status;
+            weight = (double)e.w;
         }
         if (status == S_ACCEPT) {
             if (k < capacity) {
@@ -1444,9 +1422,13 @@ void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint3
     dn.alloc(cap);
     dw.alloc(cap);
     dc.alloc(1);
+    Search32 A32{};
+    A32.mu = (float)c.cfg.mu;
+    A32.kernel = Kernel32{ c.kernel.type, c.kernel.cutoff_inf, (float)c.kernel.k_minus_1, (float)c.kernel.a, (float)c.kernel.b, (float)c.kernel.cutoff };
+    const Net32 W32{ N.theta32, N.inv_sigma2_32, N.seed, net, N.first, N.frame.quantum };
     k_candidates<<<1, 1, 0, c.stream>>>(c.tree.rec[sig].p, precision == RL_PRECISION_FP32 ? c.tree.recq[sig].p : nullptr, c.tree.topo.p, c.tree.maxdim.p,
                                         c.tree.meta.p, pos[0], pos[1], pos[2], source, net, precision,
-                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame, c.kernel);
+                                        N.theta, c.cfg.mu, N.sigma, dn.p, dw.p, cap, dc.p, c.err.p, N.frame, c.kernel, A32, W32);
     RL_LAUNCH_CHECK();
     unsigned long long k = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&k, dc.p, sizeof(k), cudaMemcpyDeviceToHost, c.stream));

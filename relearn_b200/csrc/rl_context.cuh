@@ -314,6 +314,10 @@ struct Ctx {
     };
     SnapSlot snap[2];
     int snap_next = 0;
+    // order between the context's stream and a caller stream handed to
+    // rl_prepare_update_connectivity_noalloc (created by its first call on this context)
+    cudaEvent_t noalloc_before = nullptr;
+    cudaEvent_t noalloc_after = nullptr;
     bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context

@@ -4,7 +4,9 @@ Tolerances (stated here, measured at scale by bench.py --precision-report):
 * one activity step from the same state: x and u within 1e-4 relative for
   neurons that spike in neither form; calcium within 1e-12 relative;
 * selection probabilities of the first descent: within 1e-5 relative for every
-  candidate with probability >= 1e-6 in the FP64 form;
+  candidate with probability >= 1e-6 in the FP64 form (weights from eval32, the
+  production search's own evaluation), and the production search's picks
+  distributed as the FP64 probabilities (chi-square, 100,000 searches);
 * a seeded FP32 run keeps the element and synapse bookkeeping consistent;
 * the other neuron models (Poisson, FitzHugh-Nagumo, AEIF) in FP32: one step
   from the same state within 2e-3 relative for neurons that spike in neither
@@ -69,6 +71,70 @@ def test_selection_probabilities(mixture):
             if p >= 1e-6:
                 worst = max(worst, abs(p32.get(node, 0.0) - p) / p)
     assert worst <= 1e-5, worst
+
+
+def first_descent_candidate_of(tree: dict, candidates: np.ndarray) -> np.ndarray:
+    """For every octree node, the first-descent candidate whose subtree holds
+    it (-1 for nodes above or outside the candidates).  The candidates of the
+    walk from the root partition the neurons, and nodes are stored breadth
+    first, so a parent comes before its children."""
+    m = len(tree["level"])
+    parent = np.full(m, -1, np.int64)
+    for i in np.flatnonzero(tree["first_child"] >= 0):
+        k = bin(int(tree["child_mask"][i])).count("1")
+        parent[tree["first_child"][i]: tree["first_child"][i] + k] = i
+    owner = np.full(m, -1, np.int64)
+    is_cand = np.zeros(m, bool)
+    is_cand[candidates] = True
+    for i in range(m):
+        owner[i] = i if is_cand[i] else (owner[parent[i]] if parent[i] >= 0 else -1)
+    return owner
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pick_frequencies_match_fp64_probabilities(precision):
+    """The production search (k_search / k_search_f32: weights by eval32,
+    Kahan-compensated running sums, the 24-bit threshold; Kernel.h:90-173 and
+    ProbabilityPicker.h:97-112 in the reference) picks each first-descent
+    candidate with its FP64 probability: 100,000 searches of one source,
+    repeated over steps and vacant-axon indices, whose final targets are mapped
+    to the first-descent candidate that contains them, against the FP64
+    weights by a chi-square test."""
+    from scipy.stats import chi2
+
+    n, per_step, steps = 3000, 2000, 50
+    net, *_ = make(n, 1000.0, 13, precision)
+    source = 1234
+    va = np.zeros(n, np.uint32)
+    va[source] = per_step
+    one = np.ones(n, np.uint32)
+    net.prepare_update_connectivity(va, one, one)
+    nodes, w64 = net.candidate_weights(source, 0)
+    p = w64 / w64.sum()
+    owner = first_descent_candidate_of(net.tree(), nodes)
+    leaf_of = np.full(n, -1, np.int64)
+    tree = net.tree()
+    leaves = np.flatnonzero(tree["neuron"] >= 0)
+    leaf_of[tree["neuron"][leaves]] = leaves
+    index = {int(v): k for k, v in enumerate(nodes)}
+    counts = np.zeros(len(nodes))
+    for step in range(100, 100 + steps):
+        req = net.find_targets(step)
+        assert len(req) == per_step and np.all(req["source"] == source)
+        cand = owner[leaf_of[req["target"]]]
+        assert np.all(cand >= 0)
+        np.add.at(counts, [index[int(c)] for c in cand], 1)
+    total = counts.sum()
+    expect = p * total
+    big = expect >= 5
+    obs = np.append(counts[big], counts[~big].sum())
+    exp = np.append(expect[big], expect[~big].sum())
+    keep = exp > 0
+    stat = float(np.sum((obs[keep] - exp[keep]) ** 2 / exp[keep]))
+    dof = int(keep.sum()) - 1
+    pval = float(chi2.sf(stat, dof))
+    assert counts[p == 0].sum() == 0
+    assert pval > 1e-4, (stat, dof, pval)
 
 
 def test_seeded_fp32_run_bookkeeping():
