@@ -384,6 +384,12 @@ struct LoadedNeurons {
     std::vector<double> positions;  // x, y, z per neuron
     std::vector<SignalType> signal_types;
     double maximum[3] = { 0.0, 0.0, 0.0 };
+    // simulation box from the "# Minimum x:" .. "# Maximum z:" comment lines
+    // (NeuronIO::parse_additional_position_information, io/NeuronIO.cpp:107-148;
+    // MultipleSubdomainsFromFile sets the box from them), when all six are present
+    bool has_box = false;
+    double box_min[3] = { 0.0, 0.0, 0.0 };
+    double box_max[3] = { 0.0, 0.0, 0.0 };
 };
 
 inline LoadedNeurons read_neuron_positions_and_signals(const std::string& path) {
@@ -392,8 +398,21 @@ inline LoadedNeurons read_neuron_positions_and_signals(const std::string& path) 
     LoadedNeurons out;
     uint64_t expected = 0;
     std::string line;
+    static const char* const box_keys[6] = { "# Minimum x:", "# Minimum y:", "# Minimum z:", "# Maximum x:", "# Maximum y:", "# Maximum z:" };
+    bool box_seen[6] = { false, false, false, false, false, false };
+    double box[6] = { 0.0, 0.0, 0.0, 0.0, 0.0, 0.0 };
     while (std::getline(file, line)) {
-        if (line.empty() || line[0] == '#') {
+        if (line.empty()) {
+            continue;
+        }
+        if (line[0] == '#') {
+            for (int k = 0; k < 6; ++k) {
+                const std::string key = box_keys[k];
+                if (!box_seen[k] && line.compare(0, key.size(), key) == 0) {
+                    box[k] = std::stod(line.substr(key.size()));  // the first matching comment counts
+                    box_seen[k] = true;
+                }
+            }
             continue;
         }
         std::istringstream ss(line);
@@ -413,6 +432,13 @@ inline LoadedNeurons read_neuron_positions_and_signals(const std::string& path) 
         out.maximum[0] = x > out.maximum[0] ? x : out.maximum[0];
         out.maximum[1] = y > out.maximum[1] ? y : out.maximum[1];
         out.maximum[2] = z > out.maximum[2] ? z : out.maximum[2];
+    }
+    out.has_box = box_seen[0] && box_seen[1] && box_seen[2] && box_seen[3] && box_seen[4] && box_seen[5];
+    if (out.has_box) {
+        for (int a = 0; a < 3; ++a) {
+            out.box_min[a] = box[a];
+            out.box_max[a] = box[3 + a];
+        }
     }
     return out;
 }

@@ -60,7 +60,8 @@ void usage() {
         "    --min-calcium-excitatory-dendrites, --min-calcium-inhibitory-dendrites, --retract-ratio,\n"
         "    --synaptic-elements-lower-bound, --synaptic-elements-upper-bound\n"
         "    -g/--graph DIR (rank_0_in_network.txt with plastic synapses), --file-calcium FILE\n"
-        "  added here: --izhikevich-a/-b/-c/-d, --side UM (cube edge; default: the largest coordinate),\n"
+        "  added here: --izhikevich-a/-b/-c/-d, --side UM (cube edge; default: the box of the positions file's\n"
+        "    '# Minimum/Maximum' header lines, else the largest coordinate),\n"
         "    --precision fp64|fp32, --output-prefix P (final calcium and synapses as text),\n"
         "    --output-network DIR (final rank_0_in_network.txt and rank_0_out_network.txt)\n");
 }
@@ -203,17 +204,26 @@ int main(int argc, char** argv) {
             neurons.maximum[0] = neurons.maximum[1] = neurons.maximum[2] = side;
         }
         RelearnException::check(o.num_neurons > 0, "no neurons");
-        double side = o.side;
-        if (side <= 0) {
-            side = std::max(neurons.maximum[0], std::max(neurons.maximum[1], neurons.maximum[2]));
-            side = std::nextafter(side, 2 * side + 1);  // the box must contain the largest coordinate
-        }
         Parameters p;
         p.cfg = o.cfg;
         p.cfg.num_neurons = o.num_neurons;
-        for (int a = 0; a < 3; ++a) {
-            p.cfg.box_min[a] = 0.0;
-            p.cfg.box_max[a] = side;
+        if (o.side <= 0 && neurons.has_box) {
+            // the box of the file's header, as MultipleSubdomainsFromFile::read_neurons_from_file
+            // (sim/file/MultipleSubdomainsFromFile.cpp:60-90) sets it
+            for (int a = 0; a < 3; ++a) {
+                p.cfg.box_min[a] = neurons.box_min[a];
+                p.cfg.box_max[a] = neurons.box_max[a];
+            }
+        } else {
+            double side = o.side;
+            if (side <= 0) {
+                side = std::max(neurons.maximum[0], std::max(neurons.maximum[1], neurons.maximum[2]));
+                side = std::nextafter(side, 2 * side + 1);  // the box must contain the largest coordinate
+            }
+            for (int a = 0; a < 3; ++a) {
+                p.cfg.box_min[a] = 0.0;
+                p.cfg.box_max[a] = side;
+            }
         }
         RelearnException::check(o.precision == "fp64" || o.precision == "fp32", "--precision must be fp64 or fp32");
         p.cfg.precision = o.precision == "fp32" ? RL_PRECISION_FP32 : RL_PRECISION_FP64;

@@ -131,6 +131,27 @@ def read_positions_file(path: str) -> tuple:
     return np.array(pos, np.float64).reshape(-1, 3), np.array(sig, np.uint8)
 
 
+BOX_KEYS = ("# Minimum x:", "# Minimum y:", "# Minimum z:", "# Maximum x:", "# Maximum y:", "# Maximum z:")
+
+
+def read_positions_box(path: str):
+    """The simulation box of a positions file from its "# Minimum x:" ..
+    "# Maximum z:" comment lines (NeuronIO::parse_additional_position_information,
+    io/NeuronIO.cpp:107-148; MultipleSubdomainsFromFile sets the box from them):
+    (box_min, box_max), or None unless all six are present."""
+    found = {}
+    with open(path) as f:
+        for line in f:
+            if not line.startswith("#"):
+                continue
+            for k, key in enumerate(BOX_KEYS):
+                if k not in found and line.startswith(key):
+                    found[k] = float(line[len(key):])
+    if len(found) < 6:
+        return None
+    return np.array([found[0], found[1], found[2]]), np.array([found[3], found[4], found[5]])
+
+
 NETWORK_HEADER = "# <target rank> <target neuron id>\t<source rank> <source neuron id>\t<weight>\t<plastic>\n"
 
 

@@ -61,3 +61,21 @@ def seed_elements(sim_or_net, n: int, seed: int, lower: float, upper: float):
 
     for t, (g, v) in enumerate(workloads.initial_elements(n, seed, lower, upper)):
         sim_or_net.set_elements(t, g, np.zeros(n), np.zeros(n, np.uint32), v)
+
+
+M64 = (1 << 64) - 1
+
+
+def splitmix64_uniform(seed, count):
+    """The C++ driver's SplitMix64 draws (relearn_b200_run.cpp) as doubles in
+    [0, 1)."""
+    x = seed & M64
+    out = np.empty(count)
+    for k in range(count):
+        x = (x + 0x9E3779B97F4A7C15) & M64
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+        z ^= z >> 31
+        out[k] = float(z >> 11) * 2.0**-53
+    return out

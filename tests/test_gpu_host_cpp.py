@@ -9,27 +9,10 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import oracle_params, small_network
+from conftest import oracle_params, small_network, splitmix64_uniform
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-
-
-M64 = (1 << 64) - 1
-
-
-def splitmix64_uniform(seed, count):
-    """The driver's SplitMix64 draws as doubles in [0, 1)."""
-    x = seed & M64
-    out = np.empty(count)
-    for k in range(count):
-        x = (x + 0x9E3779B97F4A7C15) & M64
-        z = x
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
-        z ^= z >> 31
-        out[k] = float(z >> 11) * 2.0**-53
-    return out
 
 
 def test_driver_matches_oracle(tmp_path):
