@@ -194,41 +194,78 @@ def build_network(n, side, seed, placement):
     return params, pos, sig
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one activity launch at 1M
-# neurons (ncu --set full, see profiles/): FP64 49.0 + 0.65 MB, FP32 30.0 + 0.02 MB
-PROFILED_TRAFFIC = {0: 49.7e6, 1: 30.0e6}
-
-# FP64 warp instructions (DADD 3.97M + DMUL 3.44M + DFMA 2.39M + DSETP 0.74M) of one
-# per-step k_activity launch at 1M neurons, from ncu's instruction mix of the
-# FP64 drop-in (profiles/k_activity_fp64_1M.md): 10.54 per neuron-step.  The
-# FP64 pipe of an SM takes 2 warp instructions per cycle (64 lanes), so a step
-# cannot take less than 10.54 n / (2 * SMs * clock).
-FP64_WARP_INSTR_PER_NEURON = 10.54
+# Figures taken from ncu captures of the kernels (instruction mix, DRAM bytes,
+# warp-lane activity, hit rates).  Each group names the kernel sources it was
+# captured at by a digest of them (kernel_digest below); a figure whose
+# sources have changed since is reported with "stale": true until it is
+# captured again.
+CAPTURED = {
+    # dram__bytes_read.sum + dram__bytes_write.sum of one per-step activity
+    # launch at 1M neurons (ncu --set full): FP64 49.0 + 0.65 MB, FP32 30.0 + 0.02 MB;
+    # FP64 warp instructions of one per-step k_activity launch (DADD 3.97M +
+    # DMUL 3.44M + DFMA 2.39M + DSETP 0.74M = 10.54 per neuron-step).  The FP64
+    # pipe of an SM takes 2 warp instructions per cycle (64 lanes).
+    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": None,
+                   "traffic": 49.7e6, "fp64_warp_instr_per_neuron": 10.54},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "traffic": 30.0e6},
+    # the fused block kernels (a network without synapses: a block of steps per
+    # launch, state in registers), from the instruction mix of a 4-step launch
+    # at 1M neurons, per neuron-step: k_activity_steps 10.77 FP64 warp
+    # instructions (43.10M / 4 steps / 1M); k_activity_f32_steps 6.97 warp
+    # instructions of every kind (27.89M / 4 / 1M), issued at one per SM
+    # sub-partition (4 per SM) per cycle; DRAM read + write of that launch
+    # (the same for any block length)
+    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": None, "fp64_warp_instr_per_neuron": 10.77,
+                "traffic": 50.03e6 + 4.35e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "warp_instr_per_neuron": 6.97, "traffic": 30.03e6 + 0.13e6},
+    # the search snapshot at 1M (one search per neuron, both signal types):
+    # lanes active per warp instruction, L1 / L2 hit rates of the walk
+    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "rl_math.cuh"), "digest": None, "lanes_active": 19.7, "l1_hit": 0.81,
+                 "l2_hit": 0.94, "dram_bytes_per_search": 700.0},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "lanes_active": 21.9, "l1_hit": 0.85, "l2_hit": 0.75},
+}
 B200_SMS = 148
-
-# The fused block kernels (a network without synapses: a block of steps per
-# launch, state in registers), from ncu's instruction mix of a 4-step launch
-# at 1M neurons (profiles/k_activity_steps_1M.md), per neuron-step:
-# k_activity_steps 10.77 FP64 warp instructions (43.10M / 4 steps / 1M);
-# k_activity_f32_steps 6.97 warp instructions of every kind (27.89M / 4 / 1M),
-# issued at one per SM sub-partition (4 per SM) per cycle.
-FUSED64_FP64_WARP_INSTR = 10.77
-FUSED32_WARP_INSTR = 6.97
-# memory per neuron and launch: reads enabled, spike flag, x, u, calcium, three
-# deltas; writes x, u, calcium, deltas, both spike-flag buffers, the input
+# algorithmic memory of a fused block launch per neuron: reads enabled, spike
+# flag, x, u, calcium, three deltas; writes x, u, calcium, deltas, both
+# spike-flag buffers, the input
 FUSED_BYTES = {0: 50 + 58, 1: 30 + 34}
-# ncu dram read + write of that 4-step launch (the same for any block length)
-FUSED_TRAFFIC = {0: 50.03e6 + 4.35e6, 1: 30.03e6 + 0.13e6}
+# Bytes the reference's octree node carries for one acceptance test
+# (SURVEY-style count: both types' centroid and count 2 x (3 x 8 + 4) = 56 B,
+# plus 8 B of child links); the search reads one type's record, so this
+# over-counts what one walk step needs (48 B FP64: 32 B record + 8 B
+# topology + 8 B cell length; 28 B FP32).
+SEARCH_BYTES_PER_NODE = 64
+
+
+def kernel_digest(files) -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(ROOT, "relearn_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def captured(name: str) -> dict:
+    """A captured figure group with its staleness against the current sources."""
+    g = dict(CAPTURED[name])
+    cur = kernel_digest(g["sources"])
+    g["stale"] = g["digest"] != cur
+    g["digest_now"] = cur
+    return g
 
 
 def fp64_pipe_roofline(roof: dict, n: int, sm_mhz) -> dict:
     """The per-step FP64 activity kernel is bound by its FP64 pipe, not by
     HBM: its floor time against its measured launch time."""
     mhz = sm_mhz or 1965.0
-    floor_us = FP64_WARP_INSTR_PER_NEURON * n / (2 * B200_SMS * mhz * 1e6) * 1e6
+    cap = captured("activity64")
+    instr = cap["fp64_warp_instr_per_neuron"]
+    floor_us = instr * n / (2 * B200_SMS * mhz * 1e6) * 1e6
     avg = roof.get("avg_launch_us")
-    return {"bound": "fp64 pipe", "warp_instr_per_neuron_step": FP64_WARP_INSTR_PER_NEURON, "sm_mhz": mhz, "floor_us": floor_us,
-            "avg_launch_us": avg, "frac": floor_us / avg if avg else None,
+    return {"bound": "fp64 pipe", "warp_instr_per_neuron_step": instr, "sm_mhz": mhz, "floor_us": floor_us,
+            "avg_launch_us": avg, "frac": floor_us / avg if avg else None, "stale": cap["stale"],
             "how": "FP64 warp instructions per launch (ncu instruction mix) / (2 per SM per cycle x 148 SMs x median SM clock)"}
 
 
@@ -238,22 +275,24 @@ def fused_roofline(precision: int, n: int, step_us: float, act_cnt: int, sm_mhz,
     side (state once per launch) beside it."""
     mhz = sm_mhz or 1965.0
     launch_us = step_us * PERIOD
+    cap = captured("fused64" if precision == 0 else "fused32")
     if precision == 0:
-        lane_ops = FUSED64_FP64_WARP_INSTR * 32  # FP64 lane operations per neuron-step
+        lane_ops = cap["fp64_warp_instr_per_neuron"] * 32  # FP64 lane operations per neuron-step
         achieved = lane_ops * n / (step_us * 1e-6) / 1e12
         peak = 64 * B200_SMS * mhz * 1e6 / 1e12
         roof = {"bound": "fp64", "kernel": "k_activity_steps", "achieved": achieved, "peak": peak, "unit": "T FP64 lane-op/s",
                 "frac": achieved / peak, "ops_per_neuron_step": lane_ops,
                 "peak_kind": "nominal issue rate at the median SM clock: 64 FP64 lanes per SM x 148 SMs (no measured FP64 peak)"}
     else:
-        achieved = FUSED32_WARP_INSTR * n / (step_us * 1e-6) / 1e12
+        achieved = cap["warp_instr_per_neuron"] * n / (step_us * 1e-6) / 1e12
         peak = 4 * B200_SMS * mhz * 1e6 / 1e12
         roof = {"bound": "issue", "kernel": "k_activity_f32_steps", "achieved": achieved, "peak": peak, "unit": "T warp-inst/s",
-                "frac": achieved / peak, "warp_instr_per_neuron_step": FUSED32_WARP_INSTR,
+                "frac": achieved / peak, "warp_instr_per_neuron_step": cap["warp_instr_per_neuron"],
                 "peak_kind": "nominal issue rate at the median SM clock: 1 warp instruction per SM sub-partition per cycle x 592"}
     bytes_per_launch = FUSED_BYTES[precision] * n
     roof.update({"sm_mhz": mhz, "steps_per_launch": PERIOD, "avg_step_us": step_us, "avg_launch_us": launch_us, "launches": act_cnt // PERIOD,
-                 "traffic": FUSED_TRAFFIC[precision] if profiled else None, "traffic_unit": "bytes per launch (ncu dram read + write)",
+                 "traffic": cap["traffic"] if profiled else None, "traffic_unit": "bytes per launch (ncu dram read + write)",
+                 "stale": cap["stale"],
                  "hbm": {"bytes_per_launch": bytes_per_launch, "achieved": bytes_per_launch / (launch_us * 1e-6) / 1e9, "peak": hbm, "unit": "GB/s",
                          "frac": bytes_per_launch / (launch_us * 1e-6) / 1e9 / hbm if hbm else None, "peak_kind": peak_kind}})
     return roof
@@ -316,9 +355,10 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
     # DRAM bytes per launch from one ncu capture of the same kernel on this
-    # workload (profiles/k_activity_f32_1M.md, k_activity_fp64_1M.md): reads
-    # equal the algorithmic read bytes, writes stay in L2 during the launch
-    traffic = PROFILED_TRAFFIC.get(precision) if (n == 1_000_000 and args.placement == "uniform" and not edges) else None
+    # workload: reads equal the algorithmic read bytes, writes stay in L2
+    # during the launch
+    cap = captured("activity64" if precision == 0 else "activity32")
+    traffic = cap["traffic"] if (n == 1_000_000 and args.placement == "uniform" and not edges) else None
     if args.step_fusion and not edges and act_cnt:
         # no synapses: each 100-step block ran as one launch of the fused kernel
         sm_mhz = clk.summary().get("sm_mhz") if clk is not None else None
@@ -328,7 +368,8 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
                     tuning=net.tuning())
     roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm if hbm else None, "traffic": traffic, "traffic_unit": "bytes per launch (ncu dram read + write)",
-            "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "launches": act_cnt, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
+            "stale": cap["stale"], "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "launches": act_cnt,
+            "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
     return dict(net=net, step=step, value=value, total_ms=total_ms, phases={k: v[0] for k, v in phases.items()}, launches=launches, roofline=roof,
                 tuning=net.tuning())
 
@@ -416,7 +457,7 @@ def run_b200(args, world, rank, local):
     other = None
     if not args.skip_fp32 and main_prec == 0:
         o = measure_form(args, 1, dev, stream, world, pos, sig, params)
-        bh32 = bh_snapshot(o["net"], n, stream, o["step"]) if not args.skip_bh else None
+        bh32 = bh_snapshot(o["net"], n, stream, o["step"], 1, bh["roofline"]["touched_per_search"] if bh else None) if not args.skip_bh else None
         other = {"precision": "fp32", "value": o["value"], "unit": "neuron-steps/s", "ms_per_step": o["total_ms"] / args.steps,
                  "vs_fp64_drop_in": o["value"] / m["value"], "roofline": o["roofline"], "phases_ms": o["phases"], "tuning": o["tuning"]}
         if bh32:
@@ -439,11 +480,17 @@ def run_b200(args, world, rank, local):
             mixture["bh_search"] = bh_snapshot(mm["net"], n, stream, mm["step"])
         mm["net"].close()
 
+    syn = None
+    if not args.skip_synapses:
+        syn = {"fp64": synapse_regime(args, dev, stream, world, 0)}
+        if not args.skip_fp32:
+            syn["fp32"] = synapse_regime(args, dev, stream, world, 1)
+            syn["fp32"]["vs_fp64"] = syn["fp32"]["value"] / syn["fp64"]["value"]
     ens = None
     if not args.skip_ensemble:
         ens = ensemble_figure(args, dev, stream, world, rank)
     prec = None
-    if rank == 0 and world == 1 and args.precision_report:
+    if rank == 0 and world == 1 and not args.skip_precision_report:
         prec = precision_report(args, dev, stream)
     serve = None
     if rank == 0 and world == 1 and not args.skip_serve:
@@ -487,6 +534,8 @@ def run_b200(args, world, rank, local):
         line["fp32_form"] = other
     if mixture:
         line["mixture"] = mixture
+    if syn:
+        line["synapse_regime"] = syn
     if ens:
         line["ensemble"] = ens
     if prec:
@@ -496,6 +545,95 @@ def run_b200(args, world, rank, local):
     if cpu:
         line["cpu_baseline"] = cpu
     return line
+
+
+def synapse_regime(args, dev, stream, world, precision):
+    """The regime with synapses: the bench network (1M neurons uniform in the
+    10,000 um cube) with synaptic elements seeded U[0, 4] per type
+    (--synaptic-elements-lower-bound / -upper-bound, relearn.cpp:620-624), so
+    that every plasticity update searches for the vacant axons and the
+    connector forms synapses, and activity runs one launch per step (the
+    in-edges couple the neurons).  One bench step = 100 activity steps + 1
+    plasticity update, as for the headline."""
+    import torch
+
+    import relearn_b200 as R
+    from relearn_b200 import workloads
+
+    n = args.neurons
+    params, pos, sig = build_network(n, args.side, args.seed + 1000, "uniform")
+    p = dict(params)
+    p["precision"] = precision
+    p["device"] = dev.index
+    net = R.Network(p)
+    net.set_stream(stream.cuda_stream)
+    net.set_positions(pos, sig)
+    net.set_step_fusion(bool(args.step_fusion))
+    for t, (g, v) in enumerate(workloads.initial_elements(n, 77, 0.0, 4.0)):
+        net.set_elements(t, g, np.zeros(n), np.zeros(n, np.uint32), v)
+    apply_shapes(args, net, precision)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    step = 1
+    # the first updates search for most initial axons, later ones for the few
+    # still vacant: search shapes are tuned per density class of the search
+    # list, so the warm-up runs until the sparse classes have been met
+    for _ in range(max(args.warmup, 6)):
+        net.simulate(step, PERIOD)
+        step += PERIOD
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    edges_before = len(net.edges()[0])
+    s0 = net.stats()
+    net.phase_times()
+    net.set_profiling(True)
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        net.simulate(step, PERIOD)
+        e1.record(stream)
+        step += PERIOD
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize(dev)
+    phases = net.phase_times()
+    net.set_profiling(False)
+    s1 = net.stats()
+    edges_after = len(net.edges()[0])
+    total_ms = max_over_ranks(float(sum(times)), world, dev)
+    hbm, peak_kind = peaks()
+    act_ms, act_cnt = phases["activity_kernel"]
+    edges = 0.5 * (edges_before + edges_after)
+    per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
+    bytes_per_launch = per_neuron * n + ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges
+    act_achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
+    act_roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": act_achieved, "peak": hbm,
+                "unit": "GB/s", "frac": act_achieved / hbm, "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch,
+                "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None, "launches": act_cnt,
+                "bytes": f"{per_neuron:.2f} B per neuron-step + {ACT_BYTES_CSR_ROW} B row offsets per neuron + {ACT_BYTES_PER_EDGE} B per in-edge"}
+    searches = s1["searches"] - s0["searches"]
+    touched = s1["nodes_touched"] - s0["nodes_touched"]
+    search_ms = phases["search_kernel"][0]
+    out = {"metric": "neuron-steps/s", "value": world * n * PERIOD * args.steps / (total_ms / 1e3), "unit": "neuron-steps/s",
+           "precision": "fp64" if precision == 0 else "fp32", "ms_per_step": total_ms / args.steps, "neurons": n,
+           "elements": "grown U[0, 4] per type at step 1 (vacant = floor)", "first_timed_step": step - PERIOD * args.steps,
+           "timed_periods": args.steps, "edges": [edges_before, edges_after], "searches_per_update": searches / args.steps,
+           "synapses_created_per_update": (s1["synapses_created"] - s0["synapses_created"]) / args.steps,
+           "synapses_deleted_per_update": (s1["synapses_deleted"] - s0["synapses_deleted"]) / args.steps,
+           "phases_ms": {k: v[0] for k, v in phases.items()}, "activity_roofline": act_roof}
+    if searches and search_ms > 0:
+        tps = touched / searches if precision == 0 else None
+        out["bh_searches_per_s"] = searches / (search_ms / 1e3)
+        if tps:
+            out["search_roofline"] = search_roofline(searches, tps, search_ms, precision)
+    dom = max(("activity_kernel", "search_kernel", "connector", "graph", "commit", "tree_update"), key=lambda k: phases[k][0])
+    out["dominant_phase"] = dom
+    out["roofline"] = out.get("search_roofline") if dom == "search_kernel" and "search_roofline" in out else act_roof
+    net.close()
+    return out
 
 
 def ensemble_spec(count, seed):
@@ -512,10 +650,14 @@ def ensemble_spec(count, seed):
     return nets
 
 
-def ensemble_figure(args, dev, stream, world, rank, periods=None):
-    """128 networks in one FP32 context: one launch per activity step over all
-    networks, 100-step blocks replayed as CUDA graphs, plasticity updates over
-    all networks at once."""
+def ensemble_figure(args, dev, stream, world, rank):
+    """128 networks in one FP32 context, each run for steps 1..5,000 (its
+    stated length) with 50 plasticity updates: one launch per activity step
+    (or per 100-step block while no network has synapses) over all networks,
+    100-step blocks replayed as CUDA graphs, plasticity updates over all
+    networks at once.  A first context of the same networks times the launch
+    shapes (the tuner caches them per size class); a second one is timed from
+    step 1 to the last step."""
     import torch
 
     import relearn_b200 as R
@@ -528,27 +670,32 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     total = sum(d["num_neurons"] for d in nets)
     pos = np.concatenate([workloads.uniform_cube(d["num_neurons"], d["side"], 900 + k) for k, d in enumerate(nets)])
     sig = np.concatenate([workloads.signal_types(d["num_neurons"], 900 + k) for k, d in enumerate(nets)])
-    ens = R.Network(base, networks=nets)
-    ens.set_stream(stream.cuda_stream)
-    ens.set_positions(pos, sig)
-    ens.set_step_fusion(bool(args.step_fusion))
-    ens.autotune(1)  # launch shapes timed during the warm-up
+
+    def make():
+        e = R.Network(base, networks=nets)
+        e.set_stream(stream.cuda_stream)
+        e.set_positions(pos, sig)
+        e.set_step_fusion(bool(args.step_fusion))
+        e.autotune(1)
+        return e
+
+    warm = make()
     step = 1
-    for _ in range(args.warmup):
-        ens.simulate(step, PERIOD)
+    for _ in range(max(args.warmup, 3)):
+        warm.simulate(step, PERIOD)
         step += PERIOD
+    warm.close()
+    ens = make()
+    steps = args.ensemble_steps
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    periods = periods or max(args.steps, 3)
     ens.phase_times()
     ens.set_profiling(True)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(periods):
-        ens.simulate(step, PERIOD)
-        step += PERIOD
+    ens.simulate(1, steps)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
@@ -557,24 +704,18 @@ def ensemble_figure(args, dev, stream, world, rank, periods=None):
     ms = max_over_ranks(ms, world, dev)
     act_ms, act_cnt = ph["activity_kernel"]
     tuning = ens.tuning()
+    st = ens.stats()
     hbm, peak_kind = peaks()
-    bytes_per_launch = int(round(ACT_BYTES_FP32 * total))
-    achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
-    fused = bool(args.step_fusion) and int(ens.stats().get("synapses_created", 0)) == 0
     ens.close()
-    if fused:
-        # no synapses in any network: each 100-step block ran as one launch for all networks
-        roof = fused_roofline(1, total, 1e3 * act_ms / act_cnt, act_cnt, None, hbm, peak_kind, False)
-        roof["note"] = ("instruction count of the one-network kernel; the batched kernel shares the draws of a neuron pair only in "
-                        "warps whose lane pairs hold even-odd pairs of one network and derives round keys per network, so it "
-                        "issues more and frac is a lower bound")
-        how = "100-step activity blocks, one launch each"
-    else:
-        roof = {"bound": "hbm", "kernel": "k_activity_f32", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch, "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None}
-        how = "100-step activity blocks as CUDA graphs, one launch per step"
-    return {"metric": "neuron-steps/s", "value": world * total * PERIOD * periods / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),
-            "neurons": total, "periods": periods, "precision": "fp32", "activity": how, "roofline": roof,
+    step_us = 1e3 * act_ms / steps
+    bytes_per_step = ACT_BYTES_FP32 * total
+    roof = {"bound": "hbm", "kernel": "k_activity_f32 / k_activity_f32_steps", "achieved": bytes_per_step / (step_us * 1e-6) / 1e9, "peak": hbm,
+            "unit": "GB/s", "frac": bytes_per_step / (step_us * 1e-6) / 1e9 / hbm, "peak_kind": peak_kind, "bytes_per_step": bytes_per_step,
+            "avg_step_us": step_us, "activity_launches": act_cnt,
+            "note": "per activity step over the whole run: fused 100-step blocks while no network has synapses, one launch per step after"}
+    return {"metric": "neuron-steps/s", "value": world * total * steps / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),
+            "neurons": total, "steps": steps, "steps_of_config": 5000, "precision": "fp32", "timed": "steps 1..%d of a fresh context" % steps,
+            "synapses_created": st["synapses_created"], "searches": st["searches"], "roofline": roof,
             "phases_ms": {k: v[0] for k, v in ph.items()}, "tuning": tuning}
 
 
@@ -699,7 +840,8 @@ def serve_figure(args, dev):
     return {"metric": "p50/p99 completion latency; aggregate neuron-steps/s", "p50_s": summ["p50_s"], "p99_s": summ["p99_s"],
             "max_s": summ["max_s"], "value": summ["neuron_steps_per_s"], "unit": "neuron-steps/s", "requests": len(done), "failed": len(bad),
             "precision": "fp32" if prec else "fp64", "arrivals": f"Poisson {args.serve_rate:g}/s over {args.serve_seconds:g} s (seeded)",
-            "sample": f"the first {args.serve_seconds:g} s of the 600 s stream", "steps_per_request": args.serve_steps,
+            "sample": f"the first {args.serve_seconds:g} s of the 600 s stream", "fraction_of_stream": args.serve_seconds / 600.0,
+            "steps_per_request": args.serve_steps,
             "offered_neuron_steps_per_s": offered, "span_s": summ["span_s"], "mean_queue_s": summ["mean_queue_s"], "p99_queue_s": summ["p99_queue_s"],
             "slots": args.serve_slots, "hbm_budget_bytes": budget, "max_running": max_running, "max_pending": max_pending,
             "max_reserved_bytes": max_reserved, "mean_pack_size": float(np.mean(packs)), "max_pack_size": int(max(packs)),
@@ -712,7 +854,25 @@ def serve_figure(args, dev):
                          "bytes_per_neuron_step": per_ns}}
 
 
-def bh_snapshot(net, n, stream, step):
+def search_roofline(searches: float, touched_per_search: float, kernel_ms: float, precision: int) -> dict:
+    """The search against HBM by algorithmic bytes (acceptance tests the
+    reference's walk runs x the node bytes of one test), with the bound that
+    actually holds beside it: the walk is served from L1 / L2 (ncu DRAM bytes
+    per search are far below the algorithmic ones), so instruction issue with
+    idle lanes bounds it."""
+    hbm, peak_kind = peaks()
+    cap = captured("search64" if precision == 0 else "search32")
+    bytes_per_search = touched_per_search * SEARCH_BYTES_PER_NODE
+    achieved = searches * bytes_per_search / (kernel_ms * 1e-3) / 1e9
+    return {"bound": "issue (walk served from L1/L2)", "kernel": "k_search" if precision == 0 else "k_search_f32", "achieved": achieved,
+            "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind, "touched_per_search": touched_per_search,
+            "bytes_per_touched_node": SEARCH_BYTES_PER_NODE, "lanes_active_of_32": cap["lanes_active"], "l1_hit_rate": cap["l1_hit"],
+            "l2_hit_rate": cap["l2_hit"], "stale": cap["stale"],
+            "how": "touched nodes from the library's counter (the acceptance tests the reference's walk runs) x bytes per node / search-kernel "
+                   "time; lanes active and hit rates from ncu on the 1M snapshot"}
+
+
+def bh_snapshot(net, n, stream, step, precision=0, touched_per_search=None):
     import torch
 
     one = np.ones(n, np.uint32)
@@ -720,6 +880,7 @@ def bh_snapshot(net, n, stream, step):
     reps = 3
     search_ms = []
     update_ms = []
+    t0 = net.stats()["nodes_touched"]
     for r in range(reps + 1):
         for t in range(3):
             net.set_elements(t, grown, np.zeros(n), np.zeros(n, np.uint32), one)
@@ -738,12 +899,19 @@ def bh_snapshot(net, n, stream, step):
             search_ms.append(ph["search_kernel"][0])
             update_ms.append(e0.elapsed_time(e1))
     searches = n
+    if precision == 0:
+        touched_per_search = (net.stats()["nodes_touched"] - t0) / ((reps + 1) * searches)
     t = net.tuning()
-    return {"metric": "BH searches/s", "value": searches / (min(search_ms) / 1e3), "unit": "searches/s",
-            "with_tree_update_and_copies": searches / (min(update_ms) / 1e3), "searches_per_update": searches,
-            "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron",
-            "search_shape": {"warps_per_block": t["search_warps"], "packet": t["search_packet"], "register_cap": t["search_cap"], "hot_nodes": t["search_hot"],
-                             "timed_ms": t["search_ms"]}}
+    out = {"metric": "BH searches/s", "value": searches / (min(search_ms) / 1e3), "unit": "searches/s",
+           "with_tree_update_and_copies": searches / (min(update_ms) / 1e3), "searches_per_update": searches,
+           "search_kernel_ms": min(search_ms), "update_ms": min(update_ms), "snapshot": "1 vacant axon + 1 vacant exc + 1 vacant inh dendrite per neuron",
+           "search_shape": {"warps_per_block": t["search_warps"], "packet": t["search_packet"], "register_cap": t["search_cap"], "hot_nodes": t["search_hot"],
+                            "timed_ms": t["search_ms"]}}
+    if touched_per_search:
+        out["roofline"] = search_roofline(searches, touched_per_search, min(search_ms), precision)
+        if precision == 1:
+            out["roofline"]["touched_from"] = "the FP64 form's counter on the same snapshot (the same walk)"
+    return out
 
 
 def cpu_baseline(args, params, pos, sig, activity_steps=1000, searches=100000):
@@ -879,7 +1047,9 @@ def main():
     ap.add_argument("--skip-ensemble", action="store_true", help="do not measure the batched form (128 networks)")
     ap.add_argument("--skip-mixture", action="store_true", help="do not measure the Gaussian-mixture placement beside the uniform one")
     ap.add_argument("--ensemble-networks", type=int, default=128)
-    ap.add_argument("--precision-report", action="store_true", help="add the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
+    ap.add_argument("--skip-precision-report", action="store_true", help="do not run the FP32-vs-FP64 error report (4M neurons, 1,000 steps)")
+    ap.add_argument("--skip-synapses", action="store_true", help="do not measure the regime with synapses (elements seeded U[0, 4])")
+    ap.add_argument("--ensemble-steps", type=int, default=5000, help="steps of every network of the batched form (config: 5,000)")
     ap.add_argument("--skip-serve", action="store_true", help="do not measure the serving form")
     ap.add_argument("--act-shape", default=None, help="activity launch shape 'block,persistent,vec' instead of the tuner's")
     ap.add_argument("--search-shape", default=None, help="search launch shape 'warps,packet[,cap[,hot]]' instead of the tuner's")

@@ -7,8 +7,8 @@
 //     (seed, step, neuron, sub-index, stream, depth); replaces RandomHolder
 //     (relearn/source/util/Random.h:70-284) at ProbabilityPicker.h:108-109,
 //     Connector.cpp:71 and NormalActivityInputCPU.cpp:35.
-//   * exp / log written from the mathematics (Cody-Waite reduction, Taylor and
-//     atanh series) standing in for glibc's std::exp (Gaussian.h:66,
+//   * exp / log written from the mathematics (Tang's table-driven exp, atanh
+//     series for log) standing in for glibc's std::exp (Gaussian.h:66,
 //     GrowthCurves.h:51); set use_libm to evaluate std::exp / std::log instead.
 //   * hypot of three arguments as libstdc++ evaluates it
 //     (Vec3.hpp:549-551 -> std::hypot(x, y, z)).
@@ -86,7 +86,7 @@ inline uint64_t take64(const Words& r) {
     return ((uint64_t)r.w[0] << 32) | (uint64_t)r.w[1];
 }
 
-// ---- exp: exp(x) = 2^k exp(r), |r| <= ln2/2
+// ---- exp
 inline double times_pow2(double y, int k) {
     if (k > 1023) {
         y *= from_bits((uint64_t)(2046) << 52);
@@ -103,6 +103,78 @@ inline double times_pow2(double y, int k) {
     return y * from_bits((uint64_t)(k + 1023) << 52);
 }
 
+// 2^(j/64) for j = 0..63 as (nearest double, nearest double of the rest);
+// the same 128 numbers as the product's table (relearn_b200/csrc/exp_table.py).
+inline constexpr double kPow2Sixtyfourths[64][2] = {
+    { 0x1.0000000000000p+0, 0x0.0p+0 },
+    { 0x1.02c9a3e778061p+0, -0x1.19083535b085dp-56 },
+    { 0x1.059b0d3158574p+0, 0x1.d73e2a475b465p-55 },
+    { 0x1.0874518759bc8p+0, 0x1.186be4bb284ffp-57 },
+    { 0x1.0b5586cf9890fp+0, 0x1.8a62e4adc610bp-54 },
+    { 0x1.0e3ec32d3d1a2p+0, 0x1.03a1727c57b53p-59 },
+    { 0x1.11301d0125b51p+0, -0x1.6c51039449b3ap-54 },
+    { 0x1.1429aaea92de0p+0, -0x1.32fbf9af1369ep-54 },
+    { 0x1.172b83c7d517bp+0, -0x1.19041b9d78a76p-55 },
+    { 0x1.1a35beb6fcb75p+0, 0x1.e5b4c7b4968e4p-55 },
+    { 0x1.1d4873168b9aap+0, 0x1.e016e00a2643cp-54 },
+    { 0x1.2063b88628cd6p+0, 0x1.dc775814a8495p-55 },
+    { 0x1.2387a6e756238p+0, 0x1.9b07eb6c70573p-54 },
+    { 0x1.26b4565e27cddp+0, 0x1.2bd339940e9d9p-55 },
+    { 0x1.29e9df51fdee1p+0, 0x1.612e8afad1255p-55 },
+    { 0x1.2d285a6e4030bp+0, 0x1.0024754db41d5p-54 },
+    { 0x1.306fe0a31b715p+0, 0x1.6f46ad23182e4p-55 },
+    { 0x1.33c08b26416ffp+0, 0x1.32721843659a6p-54 },
+    { 0x1.371a7373aa9cbp+0, -0x1.63aeabf42eae2p-54 },
+    { 0x1.3a7db34e59ff7p+0, -0x1.5e436d661f5e3p-56 },
+    { 0x1.3dea64c123422p+0, 0x1.ada0911f09ebcp-55 },
+    { 0x1.4160a21f72e2ap+0, -0x1.ef3691c309278p-58 },
+    { 0x1.44e086061892dp+0, 0x1.89b7a04ef80d0p-59 },
+    { 0x1.486a2b5c13cd0p+0, 0x1.3c1a3b69062f0p-56 },
+    { 0x1.4bfdad5362a27p+0, 0x1.d4397afec42e2p-56 },
+    { 0x1.4f9b2769d2ca7p+0, -0x1.4b309d25957e3p-54 },
+    { 0x1.5342b569d4f82p+0, -0x1.07abe1db13cadp-55 },
+    { 0x1.56f4736b527dap+0, 0x1.9bb2c011d93adp-54 },
+    { 0x1.5ab07dd485429p+0, 0x1.6324c054647adp-54 },
+    { 0x1.5e76f15ad2148p+0, 0x1.ba6f93080e65ep-54 },
+    { 0x1.6247eb03a5585p+0, -0x1.383c17e40b497p-54 },
+    { 0x1.6623882552225p+0, -0x1.bb60987591c34p-54 },
+    { 0x1.6a09e667f3bcdp+0, -0x1.bdd3413b26456p-54 },
+    { 0x1.6dfb23c651a2fp+0, -0x1.bbe3a683c88abp-57 },
+    { 0x1.71f75e8ec5f74p+0, -0x1.16e4786887a99p-55 },
+    { 0x1.75feb564267c9p+0, -0x1.0245957316dd3p-54 },
+    { 0x1.7a11473eb0187p+0, -0x1.41577ee04992fp-55 },
+    { 0x1.7e2f336cf4e62p+0, 0x1.05d02ba15797ep-56 },
+    { 0x1.82589994cce13p+0, -0x1.d4c1dd41532d8p-54 },
+    { 0x1.868d99b4492edp+0, -0x1.fc6f89bd4f6bap-54 },
+    { 0x1.8ace5422aa0dbp+0, 0x1.6e9f156864b27p-54 },
+    { 0x1.8f1ae99157736p+0, 0x1.5cc13a2e3976cp-55 },
+    { 0x1.93737b0cdc5e5p+0, -0x1.75fc781b57ebcp-57 },
+    { 0x1.97d829fde4e50p+0, -0x1.d185b7c1b85d1p-54 },
+    { 0x1.9c49182a3f090p+0, 0x1.c7c46b071f2bep-56 },
+    { 0x1.a0c667b5de565p+0, -0x1.359495d1cd533p-54 },
+    { 0x1.a5503b23e255dp+0, -0x1.d2f6edb8d41e1p-54 },
+    { 0x1.a9e6b5579fdbfp+0, 0x1.0fac90ef7fd31p-54 },
+    { 0x1.ae89f995ad3adp+0, 0x1.7a1cd345dcc81p-54 },
+    { 0x1.b33a2b84f15fbp+0, -0x1.2805e3084d708p-57 },
+    { 0x1.b7f76f2fb5e47p+0, -0x1.5584f7e54ac3bp-56 },
+    { 0x1.bcc1e904bc1d2p+0, 0x1.23dd07a2d9e84p-55 },
+    { 0x1.c199bdd85529cp+0, 0x1.11065895048ddp-55 },
+    { 0x1.c67f12e57d14bp+0, 0x1.2884dff483cadp-54 },
+    { 0x1.cb720dcef9069p+0, 0x1.503cbd1e949dbp-56 },
+    { 0x1.d072d4a07897cp+0, -0x1.cbc3743797a9cp-54 },
+    { 0x1.d5818dcfba487p+0, 0x1.2ed02d75b3707p-55 },
+    { 0x1.da9e603db3285p+0, 0x1.c2300696db532p-54 },
+    { 0x1.dfc97337b9b5fp+0, -0x1.1a5cd4f184b5cp-54 },
+    { 0x1.e502ee78b3ff6p+0, 0x1.39e8980a9cc8fp-55 },
+    { 0x1.ea4afa2a490dap+0, -0x1.e9c23179c2893p-54 },
+    { 0x1.efa1bee615a27p+0, 0x1.dc7f486a4b6b0p-54 },
+    { 0x1.f50765b6e4540p+0, 0x1.9d3e12dd8a18bp-54 },
+    { 0x1.fa7c1819e90d8p+0, 0x1.74853f3a5931ep-55 },
+};
+
+// exp by Tang's table method (ACM TOMS 15(2), 1989): k = nearest integer to
+// x * 64/ln2, r = x - k ln2/64 in two parts, exp(r) - 1 by the Taylor
+// polynomial of degree 6, 2^(k mod 64 / 64) from the table, times 2^floor(k/64).
 inline double own_exp(double x) {
     if (std::isnan(x)) {
         return x;
@@ -115,19 +187,18 @@ inline double own_exp(double x) {
     }
     const double ln2_hi = 0.6931467056274414;      // ln 2, low 32 mantissa bits cleared
     const double ln2_lo = 4.7493250390316726e-07;  // ln 2 - ln2_hi
-    const double k = std::floor(x * 1.4426950408889634 + 0.5);
-    const double r = std::fma(-k, ln2_lo, x - k * ln2_hi);
-    // 1/n! for n = 13 .. 2
-    static const double inv_fact[12] = { 1.6059043836821614599e-10, 2.0876756987868098979e-09, 2.5052108385441718775e-08,
-                                         2.7557319223985890653e-07, 2.7557319223985890653e-06, 2.4801587301587301587e-05,
-                                         1.9841269841269841270e-04, 1.3888888888888888889e-03, 8.3333333333333333333e-03,
-                                         4.1666666666666666667e-02, 1.6666666666666666667e-01, 0.5 };
-    double p = inv_fact[0];
-    for (int i = 1; i < 12; ++i) {
-        p = std::fma(p, r, inv_fact[i]);
+    const double k = std::floor(x * 92.332482616893656768 + 0.5);
+    const double r = std::fma(-k, ln2_lo / 64.0, x - k * (ln2_hi / 64.0));
+    const int ki = static_cast<int>(k);
+    const double* t = kPow2Sixtyfourths[ki & 63];
+    // Horner from 1/720 down to 1/2, then r + r^2 * (...)
+    static const double coef[5] = { 1.3888888888888889e-03, 8.3333333333333332e-03, 4.1666666666666664e-02, 1.6666666666666666e-01, 0.5 };
+    double p = coef[0];
+    for (int i = 1; i < 5; ++i) {
+        p = std::fma(p, r, coef[i]);
     }
-    const double y = 1.0 + std::fma(r * r, p, r);
-    return times_pow2(y, (int)k);
+    p = std::fma(r * r, p, r);
+    return times_pow2(t[0] + std::fma(t[0], p, t[1]), ki >> 6);
 }
 
 inline double own_log(double x) {

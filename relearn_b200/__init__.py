@@ -125,7 +125,8 @@ class RlNetwork(C.Structure):
 class RlStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("searches", "requests", "synapses_created", "bound_to_delete", "synapses_deleted", "activity_steps",
                                            "plasticity_updates", "gpu_launches", "num_nodes")] + [("max_level", C.c_uint32),
-                                                                                                  ("reserved", C.c_uint32)]
+                                                                                                  ("reserved", C.c_uint32),
+                                                                                                  ("nodes_touched", C.c_uint64)]
 
 
 class RlTuning(C.Structure):
@@ -133,10 +134,10 @@ class RlTuning(C.Structure):
                                          "tuned")]
 
 
-NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 16, 18
+NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 28, 18
 # (warps, packet, cap, hot), timing order: plain shapes, then the persistent form
 # with the top octree nodes in shared memory
-SEARCH_SHAPES = [(w, p, c, 0) for c in (0, 1) for p in (32, 16) for w in (2, 4, 8)] + [(32, p, 1, h) for h in (1024, 4096) for p in (32, 16)]
+SEARCH_SHAPES = [(w, p, c, 0) for c in (0, 1) for p in (32, 16, 4, 1) for w in (2, 4, 8)] + [(32, p, 1, h) for h in (1024, 4096) for p in (32, 16)]
 ACT_SHAPES = [(b, p, v) for p in (0, 1) for b in (128, 256, 512) for v in (1, 2, 4)]  # (block, persistent, neurons per thread)
 
 

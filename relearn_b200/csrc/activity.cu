@@ -347,6 +347,9 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
     }
 }
 
+// Background draws a block-of-steps launch prepares per barrier round.
+constexpr int kDrawChunk = 10;
+
 // A block of `nsteps` steps in one launch, for a network without synapses:
 // then a neuron's step reads nothing of the other neurons (its input is its
 // own background draw), so each thread carries its neuron's state through the
@@ -356,12 +359,23 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
 // A.fired_cur, the step before's in fired_before_last) and the input (last
 // step).  A disabled neuron keeps x, u, calcium and its spike flag; its
 // deltas become d + 0 as in every step of k_activity.
+//
+// The draws do not depend on the state, so they are made kDrawChunk steps at a
+// time: every thread evaluates its central-piece draws of those steps
+// (independent of one another), queues its tail-piece ones in shared memory,
+// the whole block evaluates the queue after one barrier, and after a second
+// barrier each thread runs its steps on the draws.  Two barriers per chunk
+// instead of two per step, and the tail queue of a chunk spreads over every
+// warp of the block.  In a context with one network, lanes 2j and 2j + 1 hold
+// a neuron pair, whose draws of a step come from one Philox block: the even
+// lane computes step k's block, the odd lane step k + 1's, and each hands the
+// other the two words it needs (the same words as a block per lane).
 template <int BLOCK, int H, int MODEL, bool MULTI>
 __global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
                                                           uint8_t* __restrict__ fired_before_last) {
-    __shared__ double s_p[BLOCK];
-    __shared__ double s_z[BLOCK];
-    __shared__ uint16_t s_who[BLOCK];
+    constexpr int S = kDrawChunk;
+    __shared__ double s_z[S * BLOCK];      // draw of step k0 + k of thread t at k * BLOCK + t
+    __shared__ uint16_t s_who[S * BLOCK];  // tail queue: slots of s_z holding a uniform to map
     __shared__ uint32_t s_cnt[2];
     pdl_wait_then_release();  // every input is the previous launch's output
     const uint32_t step0 = D->base_step;
@@ -395,45 +409,63 @@ __global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_activity_steps(ActArgs 
             tgt = A.uniform_target ? 0.0 : A.target[i];
         }
         uint8_t f_before = f;
-        for (uint32_t k = 0; k < nsteps; ++k, parity ^= 1u) {
-            const uint32_t step = step0 + k;
-            double p = 0.5;
-            if (on) {
-                p = MULTI ? noise_uniform(seed, step, local) : noise_uniform_rk(A.rk0, A.rk1, step, local);
+        for (uint32_t k0 = 0; k0 < nsteps; k0 += S, parity ^= 1u) {
+            const uint32_t m = nsteps - k0 < (uint32_t)S ? nsteps - k0 : (uint32_t)S;
+            const uint32_t stepc = step0 + k0;
+#pragma unroll
+            for (int k = 0; k < S; k += 2) {
+                uint64_t b[2];
+                if (!MULTI) {
+                    const uint32_t odd = lane & 1u;
+                    const u32x4 r = noise_block_rk(A.rk0, A.rk1, stepc + (uint32_t)k + odd, i);
+                    const uint32_t g0 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.x : r.z, 1);
+                    const uint32_t g1 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.y : r.w, 1);
+                    const uint64_t got = ((uint64_t)g0 << 21) | (uint64_t)(g1 >> 11);
+                    b[0] = odd ? got : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
+                    b[1] = odd ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : got;
+                } else {
+                    b[0] = on ? noise_bits53(noise_block(seed, stepc + (uint32_t)k, local), local) : 0u;
+                    b[1] = on ? noise_bits53(noise_block(seed, stepc + (uint32_t)k + 1u, local), local) : 0u;
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const bool use = on && (uint32_t)(k + h) < m;
+                    const double p = ((double)b[h] + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
+                    const bool tail = use && normal_in_tail(p);
+                    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
+                    uint32_t first = 0;
+                    if (lane == 0 && mask) {
+                        first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
+                    }
+                    first = __shfl_sync(0xFFFFFFFFu, first, 0);
+                    const uint32_t slot = (uint32_t)(k + h) * BLOCK + threadIdx.x;
+                    if (tail) {
+                        s_who[first + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = (uint16_t)slot;
+                    }
+                    s_z[slot] = tail ? p : (use ? normal_quantile_central(p) : 0.0);
+                }
             }
-            const bool tail = on && normal_in_tail(p);
-            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
-            uint32_t first = 0;
-            if (lane == 0 && mask) {
-                first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
-            }
-            first = __shfl_sync(0xFFFFFFFFu, first, 0);
-            if (tail) {
-                const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-                s_p[slot] = p;
-                s_who[slot] = (uint16_t)threadIdx.x;
-            }
-            double z = on && !tail ? normal_quantile_central(p) : 0.0;
             __syncthreads();
             const uint32_t cnt = s_cnt[parity];
             for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
-                s_z[s_who[q]] = normal_quantile_tail(s_p[q]);
+                const uint32_t slot = s_who[q];
+                s_z[slot] = normal_quantile_tail(s_z[slot]);
             }
             if (threadIdx.x == 0) {
-                s_cnt[parity ^ 1u] = 0u;  // the next round's counter; nobody reads it before the barrier below
+                s_cnt[parity ^ 1u] = 0u;  // the next chunk's counter; nobody reads it before the barrier below
             }
             __syncthreads();
-            if (tail) {
-                z = s_z[threadIdx.x];
-            }
             if (on) {
-                input = step_input(A, 0, z);
-                f_before = f;
-                f = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
-                ca = calcium_step<H>(A, f, ca);
-                d0 = d0 + growth_step(A, 0, ca, tgt, nu);
-                d1 = d1 + growth_step(A, 1, ca, tgt, nu);
-                d2 = d2 + growth_step(A, 2, ca, tgt, nu);
+                for (uint32_t k = 0; k < m; ++k) {
+                    const uint32_t step = stepc + k;
+                    input = step_input(A, 0, s_z[k * BLOCK + threadIdx.x]);
+                    f_before = f;
+                    f = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
+                    ca = calcium_step<H>(A, f, ca);
+                    d0 = d0 + growth_step(A, 0, ca, tgt, nu);
+                    d1 = d1 + growth_step(A, 1, ca, tgt, nu);
+                    d2 = d2 + growth_step(A, 2, ca, tgt, nu);
+                }
             }
         }
         if (on) {

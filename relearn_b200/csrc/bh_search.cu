@@ -501,6 +501,7 @@ SearchKernel fp64_search_kernel(const SearchVariant& v) {
     }
 #define RL_SV2(w, p) RL_SV(w, p, 0) RL_SV(w, p, 1)
     RL_SV2(2, 32) RL_SV2(4, 32) RL_SV2(8, 32) RL_SV2(2, 16) RL_SV2(4, 16) RL_SV2(8, 16)
+    RL_SV2(2, 4) RL_SV2(4, 4) RL_SV2(8, 4) RL_SV2(2, 1) RL_SV2(4, 1) RL_SV2(8, 1)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;
@@ -643,8 +644,12 @@ void tune_search(Ctx& c, F&& launch_all) {
 const std::vector<SearchVariant>& search_variants() {
     static const std::vector<SearchVariant> v = [] {
         std::vector<SearchVariant> out;
+        // packets of 32 or 16 Morton-adjacent searches suit dense search lists;
+        // on sparse ones the sources of a packet lie far apart and the packet
+        // walks the union of their walks, so packets of 4 and single-lane walks
+        // are candidates too
         for (int cap : { 0, 1 }) {
-            for (int p : { 32, 16 }) {
+            for (int p : { 32, 16, 4, 1 }) {
                 for (int w : { 2, 4, 8 }) {
                     out.push_back(SearchVariant{ w, p, cap, 0 });
                 }
@@ -822,10 +827,18 @@ void run_search(Ctx& c, uint32_t step) {
                 }
             }
         };
-        if (c.tune.search_state == TUNE_REQUESTED) {
-            if (c.tune.force || !recall_search_tuning(c)) {
-                tune_search(c, launch_all);
-                remember_search_tuning(c);
+        if (c.tune.search_state != TUNE_OFF) {
+            // automatic shapes: one per density class of the search list
+            const int dc = search_density_class(c.n, m);
+            auto known = c.tune.search_by_class.find(dc);
+            if (known != c.tune.search_by_class.end()) {
+                c.tune.search = known->second;
+            } else {
+                if (c.tune.force || !recall_search_tuning(c, dc)) {
+                    tune_search(c, launch_all);
+                    remember_search_tuning(c, dc);
+                }
+                c.tune.search_by_class[dc] = c.tune.search;
             }
             c.tune.search_state = TUNE_DONE;
         }

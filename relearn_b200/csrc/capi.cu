@@ -448,7 +448,7 @@ void plasticity_update(Ctx& c, uint32_t step) {
 namespace {
 std::mutex g_tune_mu;
 using TuneKey = std::tuple<int, int, int, int, int>;
-std::map<TuneKey, SearchVariant> g_search_shapes;
+std::map<std::pair<TuneKey, int>, SearchVariant> g_search_shapes;  // with the search list's density class
 std::map<TuneKey, ActVariant> g_act_shapes;
 
 // precision, batched or not, power of two of the neuron count, neuron model, kernel
@@ -461,14 +461,14 @@ TuneKey tune_key(const Ctx& c) {
 }
 }  // namespace
 
-void remember_search_tuning(const Ctx& c) {
+void remember_search_tuning(const Ctx& c, int density_class) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_search_shapes[tune_key(c)] = c.tune.search;
+    g_search_shapes[std::make_pair(tune_key(c), density_class)] = c.tune.search;
 }
 
-bool recall_search_tuning(Ctx& c) {
+bool recall_search_tuning(Ctx& c, int density_class) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_search_shapes.find(tune_key(c));
+    auto it = g_search_shapes.find(std::make_pair(tune_key(c), density_class));
     if (it == g_search_shapes.end()) {
         return false;
     }
@@ -1237,6 +1237,7 @@ rl_status rl_autotune(void* ctx, int mode) {
         if (mode != 0) {
             c.tune.search_ms.clear();
             c.tune.act_ms.clear();
+            c.tune.search_by_class.clear();
         }
     });
 }
@@ -1306,6 +1307,12 @@ rl_status rl_get_stats(void* ctx, rl_stats* out) {
             c.tree.level_runs_seen = runs;
         }
         out->gpu_launches = c.launches;
+        {
+            unsigned long long touched = 0;
+            RL_CUDA_TRY(cudaMemcpyAsync(&touched, c.counters.p, sizeof(touched), cudaMemcpyDeviceToHost, c.stream));
+            RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            out->nodes_touched = touched;
+        }
         out->num_nodes = c.tree.num_nodes;
         out->max_level = c.tree.max_level;
     });

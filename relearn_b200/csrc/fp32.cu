@@ -1055,6 +1055,7 @@ Search32Kernel fp32_search_kernel(const SearchVariant& v) {
     }
 #define RL_SV2(w, p) RL_SV(w, p, 0) RL_SV(w, p, 1)
     RL_SV2(2, 32) RL_SV2(4, 32) RL_SV2(8, 32) RL_SV2(2, 16) RL_SV2(4, 16) RL_SV2(8, 16)
+    RL_SV2(2, 4) RL_SV2(4, 4) RL_SV2(8, 4) RL_SV2(2, 1) RL_SV2(4, 1) RL_SV2(8, 1)
 #undef RL_SV2
 #undef RL_SV
     return nullptr;

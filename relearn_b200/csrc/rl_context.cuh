@@ -1,6 +1,8 @@
 // Device-resident state of one network (one rl_ctx).
 #pragma once
 
+#include <map>
+
 #include "rl_internal.cuh"
 
 namespace rl {
@@ -251,6 +253,8 @@ struct Tuning {
     int search_state = TUNE_OFF;
     int act_state = TUNE_OFF;
     bool force = false;            // time again even when the process has a result for this shape
+    // automatic search shapes per density class of the search list (search_density_class)
+    std::map<int, SearchVariant> search_by_class;
     std::vector<float> search_ms;  // per variant tried, in search_variants() order
     std::vector<float> act_ms;     // per variant tried, in act_variants() order
 };
@@ -330,8 +334,16 @@ struct Ctx {
 
 // Tuning results shared by the contexts of a process, keyed by precision,
 // batched or not, and the neuron count's power of two.
-void remember_search_tuning(const Ctx& c);
-bool recall_search_tuning(Ctx& c);
+void remember_search_tuning(const Ctx& c, int density_class);
+bool recall_search_tuning(Ctx& c, int density_class);
+// Density class of a search list of m searches over n neurons: 0 when more
+// than a quarter of the neurons search, 1 above 1/32, 2 above 1/256, else 3.
+inline int search_density_class(uint64_t n, uint64_t m) {
+    if (4 * m > n) return 0;
+    if (32 * m > n) return 1;
+    if (256 * m > n) return 2;
+    return 3;
+}
 void remember_act_tuning(const Ctx& c);
 bool recall_act_tuning(Ctx& c);
 // Releases the captured activity intervals (they are captured again on use).

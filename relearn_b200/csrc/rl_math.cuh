@@ -16,8 +16,8 @@
 //     replaces the reference's thread_local std::mt19937 draws
 //     (relearn/source/util/Random.h:245-283) by a stream keyed on
 //     (seed, step, neuron, sub-index, stream/depth).
-//   * rl_exp, rl_log   : exponential and natural log written from the
-//     mathematics (Cody-Waite argument reduction + Taylor / atanh series).
+//   * rl_exp, rl_log   : exponential (Tang's table-driven method) and natural
+//     log (atanh series) written from the mathematics.
 //     They stand in for std::exp in GaussianDistributionKernel::get_probability
 //     (relearn/source/algorithm/Kernel/Gaussian.h:62-68) and
 //     gaussian_growth_curve (relearn/source/neurons/synaptic_elements/GrowthCurves.h:30-53).
@@ -171,8 +171,86 @@ RL_HD double scale_pow2(double y, int k) {
     return y * as_f64((uint64_t)(k + 1023) << 52);
 }
 
-// exp(x): x = k ln2 + r with |r| <= ln2/2, exp(r) from its Taylor series to
-// degree 13 (truncation error < 5e-18), result scaled by 2^k.
+// 2^(j/64), j = 0..63, as hi + lo (hi rounded to nearest, lo the rounded
+// remainder), from 60-digit decimal arithmetic (exp_table.py beside this file).
+#define RL_EXP_TABLE_INIT \
+    { 0x1.0000000000000p+0, 0x0.0p+0 }, \
+    { 0x1.02c9a3e778061p+0, -0x1.19083535b085dp-56 }, \
+    { 0x1.059b0d3158574p+0, 0x1.d73e2a475b465p-55 }, \
+    { 0x1.0874518759bc8p+0, 0x1.186be4bb284ffp-57 }, \
+    { 0x1.0b5586cf9890fp+0, 0x1.8a62e4adc610bp-54 }, \
+    { 0x1.0e3ec32d3d1a2p+0, 0x1.03a1727c57b53p-59 }, \
+    { 0x1.11301d0125b51p+0, -0x1.6c51039449b3ap-54 }, \
+    { 0x1.1429aaea92de0p+0, -0x1.32fbf9af1369ep-54 }, \
+    { 0x1.172b83c7d517bp+0, -0x1.19041b9d78a76p-55 }, \
+    { 0x1.1a35beb6fcb75p+0, 0x1.e5b4c7b4968e4p-55 }, \
+    { 0x1.1d4873168b9aap+0, 0x1.e016e00a2643cp-54 }, \
+    { 0x1.2063b88628cd6p+0, 0x1.dc775814a8495p-55 }, \
+    { 0x1.2387a6e756238p+0, 0x1.9b07eb6c70573p-54 }, \
+    { 0x1.26b4565e27cddp+0, 0x1.2bd339940e9d9p-55 }, \
+    { 0x1.29e9df51fdee1p+0, 0x1.612e8afad1255p-55 }, \
+    { 0x1.2d285a6e4030bp+0, 0x1.0024754db41d5p-54 }, \
+    { 0x1.306fe0a31b715p+0, 0x1.6f46ad23182e4p-55 }, \
+    { 0x1.33c08b26416ffp+0, 0x1.32721843659a6p-54 }, \
+    { 0x1.371a7373aa9cbp+0, -0x1.63aeabf42eae2p-54 }, \
+    { 0x1.3a7db34e59ff7p+0, -0x1.5e436d661f5e3p-56 }, \
+    { 0x1.3dea64c123422p+0, 0x1.ada0911f09ebcp-55 }, \
+    { 0x1.4160a21f72e2ap+0, -0x1.ef3691c309278p-58 }, \
+    { 0x1.44e086061892dp+0, 0x1.89b7a04ef80d0p-59 }, \
+    { 0x1.486a2b5c13cd0p+0, 0x1.3c1a3b69062f0p-56 }, \
+    { 0x1.4bfdad5362a27p+0, 0x1.d4397afec42e2p-56 }, \
+    { 0x1.4f9b2769d2ca7p+0, -0x1.4b309d25957e3p-54 }, \
+    { 0x1.5342b569d4f82p+0, -0x1.07abe1db13cadp-55 }, \
+    { 0x1.56f4736b527dap+0, 0x1.9bb2c011d93adp-54 }, \
+    { 0x1.5ab07dd485429p+0, 0x1.6324c054647adp-54 }, \
+    { 0x1.5e76f15ad2148p+0, 0x1.ba6f93080e65ep-54 }, \
+    { 0x1.6247eb03a5585p+0, -0x1.383c17e40b497p-54 }, \
+    { 0x1.6623882552225p+0, -0x1.bb60987591c34p-54 }, \
+    { 0x1.6a09e667f3bcdp+0, -0x1.bdd3413b26456p-54 }, \
+    { 0x1.6dfb23c651a2fp+0, -0x1.bbe3a683c88abp-57 }, \
+    { 0x1.71f75e8ec5f74p+0, -0x1.16e4786887a99p-55 }, \
+    { 0x1.75feb564267c9p+0, -0x1.0245957316dd3p-54 }, \
+    { 0x1.7a11473eb0187p+0, -0x1.41577ee04992fp-55 }, \
+    { 0x1.7e2f336cf4e62p+0, 0x1.05d02ba15797ep-56 }, \
+    { 0x1.82589994cce13p+0, -0x1.d4c1dd41532d8p-54 }, \
+    { 0x1.868d99b4492edp+0, -0x1.fc6f89bd4f6bap-54 }, \
+    { 0x1.8ace5422aa0dbp+0, 0x1.6e9f156864b27p-54 }, \
+    { 0x1.8f1ae99157736p+0, 0x1.5cc13a2e3976cp-55 }, \
+    { 0x1.93737b0cdc5e5p+0, -0x1.75fc781b57ebcp-57 }, \
+    { 0x1.97d829fde4e50p+0, -0x1.d185b7c1b85d1p-54 }, \
+    { 0x1.9c49182a3f090p+0, 0x1.c7c46b071f2bep-56 }, \
+    { 0x1.a0c667b5de565p+0, -0x1.359495d1cd533p-54 }, \
+    { 0x1.a5503b23e255dp+0, -0x1.d2f6edb8d41e1p-54 }, \
+    { 0x1.a9e6b5579fdbfp+0, 0x1.0fac90ef7fd31p-54 }, \
+    { 0x1.ae89f995ad3adp+0, 0x1.7a1cd345dcc81p-54 }, \
+    { 0x1.b33a2b84f15fbp+0, -0x1.2805e3084d708p-57 }, \
+    { 0x1.b7f76f2fb5e47p+0, -0x1.5584f7e54ac3bp-56 }, \
+    { 0x1.bcc1e904bc1d2p+0, 0x1.23dd07a2d9e84p-55 }, \
+    { 0x1.c199bdd85529cp+0, 0x1.11065895048ddp-55 }, \
+    { 0x1.c67f12e57d14bp+0, 0x1.2884dff483cadp-54 }, \
+    { 0x1.cb720dcef9069p+0, 0x1.503cbd1e949dbp-56 }, \
+    { 0x1.d072d4a07897cp+0, -0x1.cbc3743797a9cp-54 }, \
+    { 0x1.d5818dcfba487p+0, 0x1.2ed02d75b3707p-55 }, \
+    { 0x1.da9e603db3285p+0, 0x1.c2300696db532p-54 }, \
+    { 0x1.dfc97337b9b5fp+0, -0x1.1a5cd4f184b5cp-54 }, \
+    { 0x1.e502ee78b3ff6p+0, 0x1.39e8980a9cc8fp-55 }, \
+    { 0x1.ea4afa2a490dap+0, -0x1.e9c23179c2893p-54 }, \
+    { 0x1.efa1bee615a27p+0, 0x1.dc7f486a4b6b0p-54 }, \
+    { 0x1.f50765b6e4540p+0, 0x1.9d3e12dd8a18bp-54 }, \
+    { 0x1.fa7c1819e90d8p+0, 0x1.74853f3a5931ep-55 },
+
+#if defined(__CUDACC__)
+static __device__ const double2 rl_exp_table_dev[64] = { RL_EXP_TABLE_INIT };
+#endif
+static const double rl_exp_table_host[64][2] = { RL_EXP_TABLE_INIT };
+
+// exp(x) by Tang's table-driven method (P. T. P. Tang, "Table-driven
+// implementation of the exponential function in IEEE floating-point
+// arithmetic", ACM TOMS 15(2), 1989, 144-157): x = (64 m + j) ln2/64 + r with
+// |r| <= ln2/128 (up to the rounding of k), exp(x) = 2^m 2^(j/64) exp(r),
+// exp(r) - 1 by its Taylor polynomial of degree 6 (truncation error below
+// 1e-19), 2^(j/64) from the table as hi + lo.  12 FP64 operations and one
+// table load; differs from glibc's exp in 0.2 % of arguments, by one ulp.
 RL_HD double rl_exp(double x) {
     if (x != x) {
         return x;
@@ -183,23 +261,26 @@ RL_HD double rl_exp(double x) {
     if (x < -745.1332191019412) {
         return 0.0;
     }
-    const double kd = floor(x * RL_INV_LN2 + 0.5);
-    const double r = rl_fma(-kd, RL_LN2_LO, x - kd * RL_LN2_HI);  // kd * RL_LN2_HI is exact
-    // p = sum_{n=2..13} r^(n-2) / n!, Horner with fused multiply-adds
-    double p = 1.6059043836821614599e-10;           // 1/13!
-    p = rl_fma(p, r, 2.0876756987868098979e-09);    // 1/12!
-    p = rl_fma(p, r, 2.5052108385441718775e-08);    // 1/11!
-    p = rl_fma(p, r, 2.7557319223985890653e-07);    // 1/10!
-    p = rl_fma(p, r, 2.7557319223985890653e-06);    // 1/9!
-    p = rl_fma(p, r, 2.4801587301587301587e-05);    // 1/8!
-    p = rl_fma(p, r, 1.9841269841269841270e-04);    // 1/7!
-    p = rl_fma(p, r, 1.3888888888888888889e-03);    // 1/6!
-    p = rl_fma(p, r, 8.3333333333333333333e-03);    // 1/5!
-    p = rl_fma(p, r, 4.1666666666666666667e-02);    // 1/4!
-    p = rl_fma(p, r, 1.6666666666666666667e-01);    // 1/3!
-    p = rl_fma(p, r, 0.5);                          // 1/2!
-    const double y = 1.0 + rl_fma(r * r, p, r);
-    return scale_pow2(y, (int)kd);
+    const double kd = floor(x * 92.332482616893656768 + 0.5);  // 64 / ln 2
+    // kd * (RL_LN2_HI / 64) is exact; so is the subtraction (Sterbenz, or kd = 0)
+    const double r = rl_fma(-kd, RL_LN2_LO / 64.0, x - kd * (RL_LN2_HI / 64.0));
+    const int ki = (int)kd;
+    const int j = ki & 63;
+    const int m = ki >> 6;  // floor(ki / 64)
+    // exp(r) - 1 = r + r^2 (1/2 + r/6 + r^2/24 + r^3/120 + r^4/720)
+    double p = rl_fma(1.3888888888888889e-03, r, 8.3333333333333332e-03);  // 1/720, 1/120
+    p = rl_fma(p, r, 4.1666666666666664e-02);                              // 1/24
+    p = rl_fma(p, r, 1.6666666666666666e-01);                              // 1/6
+    p = rl_fma(p, r, 0.5);
+    p = rl_fma(r * r, p, r);
+#if defined(__CUDA_ARCH__)
+    const double2 t = __ldg(&rl_exp_table_dev[j]);
+    const double t_hi = t.x, t_lo = t.y;
+#else
+    const double t_hi = rl_exp_table_host[j][0], t_lo = rl_exp_table_host[j][1];
+#endif
+    // 2^(j/64) (1 + p) = hi + (hi p + lo), dropping lo p (below 1e-18 of the result)
+    return scale_pow2(t_hi + rl_fma(t_hi, p, t_lo), m);
 }
 
 // log(x) for finite x > 0 (normal range): x = m 2^e with m in

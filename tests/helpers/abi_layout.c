@@ -23,6 +23,7 @@ int main(void) {
     F(rl_config, kernel_scale);
     F(rl_config, linear_cutoff);
     F(rl_stats, max_level);
+    F(rl_stats, nodes_touched);
     printf("rl_network %zu\n", sizeof(rl_network));
     printf("rl_tuning %zu\n", sizeof(rl_tuning));
     printf("RL_NUM_SEARCH_SHAPES %d\n", RL_NUM_SEARCH_SHAPES);

@@ -49,6 +49,7 @@ def test_struct_layout(tmp_path):
               "linear_cutoff"):
         assert int(lines[f"rl_config.{f}"]) == getattr(R.RlConfig, f).offset
     assert int(lines["rl_stats.max_level"]) == R.RlStats.max_level.offset
+    assert int(lines["rl_stats.nodes_touched"]) == R.RlStats.nodes_touched.offset
     assert int(lines["RL_NUM_SEARCH_SHAPES"]) == R.NUM_SEARCH_SHAPES == len(R.SEARCH_SHAPES)
     assert int(lines["RL_NUM_ACT_SHAPES"]) == R.NUM_ACT_SHAPES == len(R.ACT_SHAPES)
     for name, cls in (("rl_tuning", R.RlTuning), ("rl_network", R.RlNetwork), ("rl_serve_config", R.RlServeConfig), ("rl_serve_request", R.RlServeRequest),
@@ -67,7 +68,7 @@ def test_host_only_entry_points(built_lib):
     import relearn_b200 as R
 
     L = R.load_library()
-    assert L.rl_abi_version() == 3
+    assert L.rl_abi_version() == 4
     cfg = R.RlConfig()
     L.rl_config_default(C.byref(cfg), 2000, 1000.0)
     # reference defaults: Parameters.h:123-130, CalciumCalculatorBase.h:206-210, Gaussian.h:38-39
