@@ -230,7 +230,7 @@ B200_SMS = 148
 # spike-flag buffers, the input
 FUSED_BYTES = {0: 50 + 58, 1: 30 + 34}
 # Bytes the reference's octree node carries for one acceptance test
-# (SURVEY-style count: both types' centroid and count 2 x (3 x 8 + 4) = 56 B,
+# (both types' centroid and count 2 x (3 x 8 + 4) = 56 B,
 # plus 8 B of child links); the search reads one type's record, so this
 # over-counts what one walk step needs (48 B FP64: 32 B record + 8 B
 # topology + 8 B cell length; 28 B FP32).

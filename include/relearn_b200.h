@@ -255,6 +255,32 @@ RL_API rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* ou
  * number of synapses formed. */
 RL_API rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created);
 
+/* The two halves of the connector for a network split over ranks, each rank
+ * a context over every neuron's position (the octree is replicated) that owns
+ * a share of the neurons; neuron ids are global, so every draw is the one a
+ * single context makes.
+ *
+ * ForwardConnector::process_requests (algorithm/Connector.cpp:33-117) on the
+ * rank that owns the requests' targets: the requests of all ranks, processed
+ * in the keyed random order of rl_connect; a request whose target is its
+ * source fails, and so does one whose target has no vacant dendrite of the
+ * request's type left; an accepted request binds one vacant dendrite of the
+ * target and adds the synapse to the context's synapse list.  The sources'
+ * axons are not touched.  `accepted` (may be NULL) receives one flag per
+ * request in the caller's order (the responses); *created the number of
+ * synapses formed. */
+RL_API rl_status rl_process_requests(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created);
+
+/* ForwardConnector::process_responses (algorithm/Connector.cpp:119-197) on the
+ * rank that owns the requests' sources: one vacant axon of the source is bound
+ * per accepted request (a source without one gives RL_ERR_DEVICE, the
+ * reference's exception); requests with `append` set (may be NULL: none) add
+ * their synapse to the context's synapse list — those whose target lives on
+ * another rank, whose synapse rl_process_requests did not add here.
+ * *bound (may be NULL) receives the number of axons bound. */
+RL_API rl_status rl_process_responses(void* ctx, const rl_request* requests, const uint8_t* accepted, const uint8_t* append, uint64_t count,
+                                      uint64_t* bound);
+
 RL_API rl_status rl_set_elements(void* ctx, int type, const double* grown, const double* delta, const uint32_t* connected, const uint32_t* vacant);
 RL_API rl_status rl_get_elements(void* ctx, int type, double* grown, double* delta, uint32_t* connected, uint32_t* vacant);
 
@@ -278,8 +304,8 @@ RL_API rl_status rl_snapshot_wait(void* ctx);
 
 /* Target calcium per neuron (the target function CalciumIO builds from a
  * --file-calcium, io/CalciumIO.cpp:27-130; otherwise every neuron has
- * rl_config.target_calcium).  The FP32 form runs one target for all neurons of
- * a context: there, targets that are not all equal give RL_ERR_UNSUPPORTED. */
+ * rl_config.target_calcium), in either precision form (the FP32 form keeps an
+ * FP32 copy and evaluates each neuron's growth curves in FP32). */
 RL_API rl_status rl_set_target_calcium(void* ctx, const double* target);
 RL_API rl_status rl_get_target_calcium(void* ctx, double* target);
 

@@ -149,6 +149,10 @@ def lib():
         L.orc_philox.argtypes = [u32] * 6 + [vp]
         L.orc_connect_requests.restype = u64
         L.orc_connect_requests.argtypes = [vp, u32, vp, u64, vp]
+        L.orc_process_requests.restype = u64
+        L.orc_process_requests.argtypes = [vp, u32, vp, u64, vp]
+        L.orc_process_responses.restype = C.c_int
+        L.orc_process_responses.argtypes = [vp, vp, vp, vp, u64]
         L.orc_octant_of.restype = C.c_int
         L.orc_octant_of.argtypes = [vp, vp, vp]
         L.orc_box_for_octant.argtypes = [vp, vp, C.c_int, vp, vp]
@@ -246,6 +250,24 @@ class OracleSim:
         acc = np.zeros(max(len(req), 1), np.uint8)
         created = int(lib().orc_connect_requests(self.h, step, _p(req), len(req), _p(acc)))
         return created, acc[: len(req)].copy()
+
+    def process_requests(self, step: int, requests: np.ndarray):
+        """The target half of the connector (ForwardConnector::process_requests):
+        returns the number created and one accepted flag per request."""
+        req = np.ascontiguousarray(requests, REQ_DTYPE)
+        acc = np.zeros(max(len(req), 1), np.uint8)
+        created = int(lib().orc_process_requests(self.h, step, _p(req), len(req), _p(acc)))
+        return created, acc[: len(req)].copy()
+
+    def process_responses(self, requests: np.ndarray, accepted: np.ndarray, append=None) -> int:
+        """The axon half (ForwardConnector::process_responses); synapses flagged
+        in `append` join the synapse list.  Returns the number of axons bound."""
+        req = np.ascontiguousarray(requests, REQ_DTYPE)
+        acc = np.ascontiguousarray(accepted, np.uint8)
+        app = None if append is None else np.ascontiguousarray(append, np.uint8)
+        if lib().orc_process_responses(self.h, _p(req), _p(acc), None if app is None else _p(app), len(req)) != 0:
+            raise RuntimeError("process_responses: a source has no vacant axon")
+        return int(acc.astype(np.int64).sum())
 
     def nodes_to_consider(self, position, dendrite_type: int) -> np.ndarray:
         """Candidates of a walk from the root for a source at `position`, as

@@ -602,9 +602,10 @@ std::vector<orc_request> find_target_neurons(Sim& s, uint32_t step) {
     return out;
 }
 
-// ForwardConnector::process_requests / process_responses (Connector.cpp:33-197)
-// with the keyed shuffle stated at the top of this file.
-uint64_t connect(Sim& s, uint32_t step, const std::vector<orc_request>& req, std::vector<uint8_t>& accepted) {
+// ForwardConnector::process_requests (Connector.cpp:33-117) with the keyed
+// shuffle stated at the top of this file: the target side (dendrites and the
+// synapse list) of every accepted request.
+uint64_t process_requests(Sim& s, uint32_t step, const std::vector<orc_request>& req, std::vector<uint8_t>& accepted) {
     const size_t m = req.size();
     std::vector<std::pair<uint64_t, size_t>> order(m);
     for (size_t i = 0; i < m; ++i) {
@@ -649,13 +650,29 @@ uint64_t connect(Sim& s, uint32_t step, const std::vector<orc_request>& req, std
             }
         }
     }
-    // process_responses: the axon side of every accepted request.
-    for (size_t i = 0; i < m; ++i) {
+    return created;
+}
+
+// ForwardConnector::process_responses (Connector.cpp:119-197): the axon side of
+// every accepted request.  Returns false when a source has no vacant axon left
+// (the reference throws).
+bool process_responses(Sim& s, const std::vector<orc_request>& req, const std::vector<uint8_t>& accepted) {
+    for (size_t i = 0; i < req.size(); ++i) {
         if (accepted[i]) {
+            if (s.el[0].vacant[req[i].source] == 0) {
+                return false;
+            }
             s.el[0].connected[req[i].source] += 1;
             s.el[0].vacant[req[i].source] -= 1;
         }
     }
+    return true;
+}
+
+// Both halves on one rank.
+uint64_t connect(Sim& s, uint32_t step, const std::vector<orc_request>& req, std::vector<uint8_t>& accepted) {
+    const uint64_t created = process_requests(s, step, req, accepted);
+    process_responses(s, req, accepted);
     return created;
 }
 
@@ -1159,6 +1176,48 @@ uint64_t orc_connect_requests(void* h, uint32_t step, const orc_request* req, ui
         std::copy(accepted.begin(), accepted.end(), accepted_out);
     }
     return created;
+}
+
+// The target half of the connector over a caller-given request list (the
+// requests that reach the rank owning their targets).
+uint64_t orc_process_requests(void* h, uint32_t step, const orc_request* req, uint64_t m, uint8_t* accepted_out) {
+    Sim* s = static_cast<Sim*>(h);
+    std::vector<orc_request> list(req, req + m);
+    std::vector<uint8_t> accepted;
+    const uint64_t created = process_requests(*s, step, list, accepted);
+    s->total_created += created;
+    if (accepted_out) {
+        std::copy(accepted.begin(), accepted.end(), accepted_out);
+    }
+    return created;
+}
+
+// The axon half over the responses to this rank's requests; requests flagged
+// in `append` (may be null) add their synapse to the synapse list (their
+// target lives on another rank).  Returns -1 when a source has no vacant axon.
+int orc_process_responses(void* h, const orc_request* req, const uint8_t* accepted, const uint8_t* append, uint64_t m) {
+    Sim* s = static_cast<Sim*>(h);
+    std::vector<orc_request> list(req, req + m);
+    std::vector<uint8_t> acc(accepted, accepted + m);
+    if (!process_responses(*s, list, acc)) {
+        return -1;
+    }
+    for (uint64_t i = 0; i < m; ++i) {
+        if (acc[i] && append && append[i]) {
+            const int32_t weight = list[i].signal == 1 ? -1 : 1;
+            auto& edges = s->in_edges[list[i].target];
+            auto it = edges.find(list[i].source);
+            if (it == edges.end()) {
+                edges.emplace(list[i].source, weight);
+            } else {
+                it->second += weight;
+                if (it->second == 0) {
+                    edges.erase(it);
+                }
+            }
+        }
+    }
+    return 0;
 }
 
 // Cell::get_octant_for_position (Cell.h:104-137) of one cell box; -1 when

@@ -164,7 +164,7 @@ SYNAPSE_DTYPE = np.dtype([("target", "<u4"), ("source", "<u4"), ("weight", "<i4"
 ABI_FUNCTIONS = [
     "rl_config_default", "rl_ctx_create", "rl_ensemble_create", "rl_ctx_destroy", "rl_last_error", "rl_status_string", "rl_abi_version",
     "rl_set_positions", "rl_tree_info", "rl_dump_tree", "rl_prepare_update_connectivity", "rl_find_targets",
-    "rl_update_connectivity", "rl_connect", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
+    "rl_update_connectivity", "rl_connect", "rl_process_requests", "rl_process_responses", "rl_set_elements", "rl_get_elements", "rl_set_neurons", "rl_get_neurons", "rl_set_enabled",
     "rl_add_edges", "rl_get_edges", "rl_activity_block", "rl_plasticity_update", "rl_simulate", "rl_synchronize",
     "rl_get_stats", "rl_set_stream", "rl_set_profiling", "rl_get_phase_times", "rl_prepare_update_connectivity_noalloc",
     "rl_candidate_weights", "rl_set_graphs", "rl_set_step_fusion", "rl_ctx_memory", "rl_serve_footprint", "rl_serve_create", "rl_serve_submit", "rl_serve_poll",
@@ -253,6 +253,10 @@ def load_library(path: str = LIB_PATH):
     L.rl_set_step_fusion.argtypes = [vp, C.c_int]
     L.rl_connect.restype = st
     L.rl_connect.argtypes = [vp, u32, vp, u64, vp, P(u64)]
+    L.rl_process_requests.restype = st
+    L.rl_process_requests.argtypes = [vp, u32, vp, u64, vp, P(u64)]
+    L.rl_process_responses.restype = st
+    L.rl_process_responses.argtypes = [vp, vp, vp, vp, u64, P(u64)]
     L.rl_candidate_weights.restype = st
     L.rl_candidate_weights.argtypes = [vp, u32, C.c_int, vp, vp, u64, P(u64)]
     L.rl_prepare_update_connectivity_noalloc.restype = st
@@ -445,6 +449,30 @@ class Network:
         cnt = C.c_uint64()
         self._check(self.lib.rl_connect(self.h, step, _p(req), len(req), _p(acc), C.byref(cnt)))
         return int(cnt.value), acc[: len(req)].copy()
+
+    def process_requests(self, step: int, requests: np.ndarray):
+        """ForwardConnector::process_requests on the rank owning the
+        requests' targets: binds dendrites and adds synapses, leaves the
+        sources' axons alone; returns (synapses created, accepted flag per
+        request in the given order)."""
+        req = np.ascontiguousarray(requests, REQUEST_DTYPE)
+        acc = np.zeros(max(len(req), 1), np.uint8)
+        cnt = C.c_uint64()
+        self._check(self.lib.rl_process_requests(self.h, step, _p(req), len(req), _p(acc), C.byref(cnt)))
+        return int(cnt.value), acc[: len(req)].copy()
+
+    def process_responses(self, requests: np.ndarray, accepted: np.ndarray, append: Optional[np.ndarray] = None) -> int:
+        """ForwardConnector::process_responses on the rank owning the
+        requests' sources: binds one vacant axon per accepted request and adds
+        the synapses flagged in `append`; returns the number of axons bound."""
+        req = np.ascontiguousarray(requests, REQUEST_DTYPE)
+        acc = np.ascontiguousarray(accepted, np.uint8)
+        app = None if append is None else np.ascontiguousarray(append, np.uint8)
+        if len(acc) != len(req) or (app is not None and len(app) != len(req)):
+            raise ValueError("one accepted (and append) flag per request")
+        cnt = C.c_uint64()
+        self._check(self.lib.rl_process_responses(self.h, _p(req), _p(acc), _p(app), len(req), C.byref(cnt)))
+        return int(cnt.value)
 
     # ---- state
     def set_elements(self, etype: int, grown=None, delta=None, connected=None, vacant=None):

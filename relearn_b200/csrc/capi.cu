@@ -891,7 +891,12 @@ rl_status rl_update_connectivity(void* ctx, uint32_t step, rl_synapse* out, uint
     });
 }
 
-rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created) {
+namespace {
+
+// The connector over caller-given requests; bind_axons false leaves the
+// sources' axons alone (process_requests on the rank owning the targets).
+rl_status connect_given(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created,
+                        bool bind_axons) {
     return rl::guarded(ctx, [&](Ctx& c) {
         RL_CHECK(count == 0 || requests != nullptr, RL_ERR_INVALID, "requests are required");
         RL_CHECK(count < ((uint64_t)1 << 32), RL_ERR_INVALID, "at most 2^32 - 1 requests per call");
@@ -917,7 +922,7 @@ rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint6
             rl::upload(S.req_sig, g.data(), count, c.stream);
         }
         S.num_requests = count;
-        const uint64_t m = rl::run_connector(c, step);
+        const uint64_t m = rl::run_connector(c, step, bind_axons);
         if (created) *created = m;
         if (accepted && count) {
             // the connector keeps its flags in processing order; cidx maps back to the request
@@ -931,6 +936,43 @@ rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint6
         }
         S.num_requests = 0;
         rl::rebuild_graph(c);
+    });
+}
+
+}  // namespace
+
+rl_status rl_connect(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created) {
+    return connect_given(ctx, step, requests, count, accepted, created, true);
+}
+
+rl_status rl_process_requests(void* ctx, uint32_t step, const rl_request* requests, uint64_t count, uint8_t* accepted, uint64_t* created) {
+    return connect_given(ctx, step, requests, count, accepted, created, false);
+}
+
+rl_status rl_process_responses(void* ctx, const rl_request* requests, const uint8_t* accepted, const uint8_t* append, uint64_t count,
+                               uint64_t* bound) {
+    return rl::guarded(ctx, [&](Ctx& c) {
+        RL_CHECK(count == 0 || (requests != nullptr && accepted != nullptr), RL_ERR_INVALID, "requests and accepted flags are required");
+        std::vector<uint32_t> src;
+        std::vector<uint32_t> et, es;
+        std::vector<int32_t> ew;
+        for (uint64_t i = 0; i < count; ++i) {
+            const rl_request& r = requests[i];
+            RL_CHECK(r.target < c.n && r.source < c.n, RL_ERR_INVALID, "request " + std::to_string(i) + ": neuron id out of range");
+            RL_CHECK(r.signal <= 1, RL_ERR_INVALID, "request " + std::to_string(i) + ": signal must be 0 or 1");
+            if (!accepted[i]) {
+                continue;
+            }
+            src.push_back(r.source);
+            if (append && append[i]) {
+                et.push_back(r.target);
+                es.push_back(r.source);
+                ew.push_back(r.signal ? -1 : 1);
+            }
+        }
+        if (bound) *bound = src.size();
+        rl::bind_axons_host(c, src.size(), src.data());
+        rl::add_edges_host(c, et.size(), et.data(), es.data(), ew.data());
     });
 }
 
@@ -988,14 +1030,15 @@ rl_status rl_set_target_calcium(void* ctx, const double* target) {
         for (uint32_t i = 1; i < c.n && same; ++i) {
             same = target[i] == target[0];
         }
-        // the FP32 kernel folds one target into its growth-curve constants
-        RL_CHECK(same || !rl::is_fp32(c), RL_ERR_UNSUPPORTED, "the FP32 form runs one target calcium for all neurons");
         c.target_uniform = same;
         if (same && c.n > 0) {
             c.cfg.target_calcium = target[0];
         }
         rl::drop_activity_graphs(c);  // captured intervals hold the growth-curve constants
         rl::upload(c.nr.target, target, c.n, c.stream);
+        if (rl::is_fp32(c) && !same) {
+            rl::target_f32_from_f64(c);  // the FP32 kernels read an FP32 copy
+        }
         RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
     });
 }

@@ -86,15 +86,36 @@ __global__ void k_accept(AcceptArgs A) {
             acc = 1;
             atomicAdd(inh ? &A.con_inh[t] : &A.con_exc[t], 1u);
             atomicSub(inh ? &A.vac_inh[t] : &A.vac_exc[t], 1u);
-            const uint32_t s = A.src[i];
-            const uint32_t old = atomicSub(&A.vac_axon[s], 1u);
-            if (old == 0) {
-                atomicOr(A.err, (uint32_t)DERR_CONNECT);
+            if (A.vac_axon) {  // null: the sources live on other ranks (process_requests only)
+                const uint32_t s = A.src[i];
+                const uint32_t old = atomicSub(&A.vac_axon[s], 1u);
+                if (old == 0) {
+                    atomicOr(A.err, (uint32_t)DERR_CONNECT);
+                }
+                atomicAdd(&A.con_axon[s], 1u);
             }
-            atomicAdd(&A.con_axon[s], 1u);
         }
     }
     A.accepted[p] = acc;
+}
+
+// ForwardConnector::process_responses (Connector.cpp:119-197): one vacant
+// axon of the source bound per accepted request; a source without one is an
+// error (the reference throws).
+__global__ void k_bind_axons(uint64_t m, const uint32_t* __restrict__ src, uint32_t* __restrict__ vac_axon, uint32_t* __restrict__ con_axon,
+                             uint32_t* __restrict__ err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) {
+        return;
+    }
+    const uint32_t s = src[i];
+    const uint32_t old = atomicSub(&vac_axon[s], 1u);
+    if (old == 0) {
+        atomicAdd(&vac_axon[s], 1u);  // leave the count as it was
+        atomicOr(err, (uint32_t)DERR_CONNECT);
+        return;
+    }
+    atomicAdd(&con_axon[s], 1u);
 }
 
 __global__ void k_emit_edges(uint64_t m, const uint32_t* __restrict__ accepted, const uint32_t* __restrict__ pos, const uint32_t* __restrict__ perm,
@@ -278,7 +299,7 @@ __global__ void k_delete(DeleteArgs A) {
 
 }  // namespace
 
-uint64_t run_connector(Ctx& c, uint32_t step) {
+uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons) {
     const uint64_t m = c.search.num_requests;
     Search& S = c.search;
     Graph& G = c.graph;
@@ -326,8 +347,8 @@ uint64_t run_connector(Ctx& c, uint32_t step) {
     A.vac_inh = c.nr.vacant[2].p;
     A.con_exc = c.nr.connected[1].p;
     A.con_inh = c.nr.connected[2].p;
-    A.vac_axon = c.nr.vacant[0].p;
-    A.con_axon = c.nr.connected[0].p;
+    A.vac_axon = bind_axons ? c.nr.vacant[0].p : nullptr;
+    A.con_axon = bind_axons ? c.nr.connected[0].p : nullptr;
     A.vac_exc_before = before.p;
     A.vac_inh_before = before.p + n;
     A.accepted = S.accepted.p;
@@ -504,6 +525,21 @@ uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
     }
     RL_CUDA_TRY(cudaStreamSynchronize(st));
     return deleted;
+}
+
+void bind_axons_host(Ctx& c, uint64_t m, const uint32_t* src) {
+    if (m == 0) {
+        return;
+    }
+    for (uint64_t k = 0; k < m; ++k) {
+        RL_CHECK(src[k] < c.n, RL_ERR_INVALID, "source out of range");
+    }
+    DBuf<uint32_t> d;
+    d.alloc(m);
+    RL_CUDA_TRY(cudaMemcpyAsync(d.p, src, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c.stream));
+    k_bind_axons<<<blocks_for(m, 256), 256, 0, c.stream>>>(m, d.p, c.nr.vacant[0].p, c.nr.connected[0].p, c.err.p);
+    RL_LAUNCH_CHECK();
+    check_device_error(c, "process_responses");
 }
 
 void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w) {

@@ -74,6 +74,10 @@ struct Act32 {
     float xi[3], inv_zeta[3];
     int flat[3];            // eta == epsilon corner case of gaussian_growth_curve
     float eta[3];
+    // per-neuron target calcium (null: one target, folded into xi / inv_zeta);
+    // kz / (eta - epsilon) is a neuron's inv_zeta
+    const float* target;
+    float kz;
     const NetInfo* nets;
     const uint16_t* net_of;
     // a context with one network: its seed and growth rates, so that the
@@ -134,8 +138,8 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
 template <int H, int MODEL, bool EDGES = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
-                                           uint32_t k24p, const float* nu, float& x, float& u, double& ca, float (&delta)[3], float& input,
-                                           uint8_t& fired) {
+                                           uint32_t k24p, const float* nu, float tgt, float& x, float& u, double& ca, float (&delta)[3],
+                                           float& input, uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
         fired = fired_prev;
@@ -224,10 +228,20 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
         float dz;
-        if (A.flat[t]) {
+        bool flat = A.flat[t];
+        float xi = A.xi[t], inv_zeta = A.inv_zeta[t];
+        if (A.target) {
+            // gaussian_growth_curve with the neuron's own epsilon = max(target, eta)
+            const float eta = A.eta[t];
+            const float eps = fmaxf(tgt, eta);
+            flat = eta == eps;
+            xi = 0.5f * (eta + eps);
+            inv_zeta = flat ? 0.0f : __fdividef(A.kz, eta - eps);
+        }
+        if (flat) {
             dz = caf == A.eta[t] ? 0.0f : -1.0f;
         } else {
-            const float q = (caf - A.xi[t]) * A.inv_zeta[t];
+            const float q = (caf - xi) * inv_zeta;
             dz = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
         }
         delta[t] = fmaf(dz, nu[t], delta[t]);
@@ -339,6 +353,10 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     ld_f<V>(A.delta[0] + i, d0);
     ld_f<V>(A.delta[1] + i, d1);
     ld_f<V>(A.delta[2] + i, d2);
+    float tg[V] = {};
+    if (A.target) {
+        ld_f<V>(A.target + i, tg);
+    }
     // Background draws: the same Philox blocks as the FP64 form, 24 bits of
     // each neuron's words; one block serves an even-odd pair of a network, so
     // a thread with two neurons of a pair draws once.  Draws are keyed on the
@@ -368,7 +386,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     for (int k = 0; k < V; ++k) {
         float d[3] = { d0[k], d1[k], d2[k] };
         const float* nu = MULTI ? A.nets[net[k]].nu32 : A.nu1;
-        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, x[k], u[k], ca[k], d, input[k], fired[k]);
+        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, tg[k], x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     if (A.input) {
@@ -424,7 +442,11 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
         float x = 0.0f, u = 0.0f;
         double ca = 0.0;
         float d[3] = { 0.0f, 0.0f, 0.0f };
+        float tg = 0.0f;
         if (in) {
+            if (A.target) {
+                tg = A.target[i];
+            }
             f = A.fired_prev[i];
             x = A.x[i];
             u = A.u[i];
@@ -452,7 +474,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
                 k24p = w.x >> 8;
             }
             uint8_t fired;
-            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, x, u, ca, d, input, fired);
+            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, tg, x, u, ca, d, input, fired);
             f_before = f;
             f = fired;
         };
@@ -1147,6 +1169,12 @@ void f32_from_f64(Ctx& c) {
     }
 }
 
+void target_f32_from_f64(Ctx& c) {
+    c.nr.target32.ensure(c.n);
+    k_d2f<<<blocks_for(c.n, 256), 256, 0, c.stream>>>(c.n, c.nr.target.p, c.nr.target32.p);
+    RL_LAUNCH_CHECK();
+}
+
 void f64_from_f32(Ctx& c) {
     const uint32_t n = c.n;
     const unsigned b = blocks_for(n, 256);
@@ -1261,6 +1289,8 @@ Act32 act32_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fir
         // scaled by sqrt(log2 e), so that exp(-q^2) is one exp2 of -(q')^2
         A.inv_zeta[t] = A.flat[t] ? 0.0f : (float)(1.2011224087864498 / ((eta - eps) * factor_inv));
     }
+    A.target = c.target_uniform ? nullptr : c.nr.target32.p;
+    A.kz = (float)(1.2011224087864498 / factor_inv);
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
     A.seed1 = c.nets[0].seed;

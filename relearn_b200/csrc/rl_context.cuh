@@ -79,6 +79,7 @@ struct Neurons {
     DBuf<uint32_t> search_vacant;  // vacant axons handed to the next search
     // FP32 form: authoritative membrane / growth state in FP32
     DBuf<float> x32, u32, input32, delta32[3];
+    DBuf<float> target32;  // per-neuron target calcium (allocated when the targets differ)
 };
 
 // Synapse list: one entry per (target, source) synapse group with an integer
@@ -365,7 +366,10 @@ void dump_tree(Ctx& c, int32_t* level, int32_t* neuron, uint8_t* child_mask, int
 void run_search(Ctx& c, uint32_t step);  // fills search.req_* (requests in (source, j) order)
 
 // connector.cu
-uint64_t run_connector(Ctx& c, uint32_t step);  // accepts requests, updates elements, appends new edges
+// accepts requests, updates elements, appends new edges; bind_axons false:
+// the target side only (the sources' axons are bound by bind_axons_host)
+uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons = true);
+void bind_axons_host(Ctx& c, uint64_t m, const uint32_t* src);  // one vacant axon per listed source
 void rebuild_graph(Ctx& c);                     // merge new edges into the CSR
 uint64_t run_deletion(Ctx& c, uint32_t step, int type);  // delete to_delete[] synapses per neuron for one element type
 void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, const int32_t* w);
@@ -374,6 +378,7 @@ void add_edges_host(Ctx& c, uint64_t m, const uint32_t* t, const uint32_t* s, co
 bool is_fp32(const Ctx& c);
 void alloc_fp32(Ctx& c);
 void f32_from_f64(Ctx& c);  // state arrays FP64 -> FP32 (after a host upload)
+void target_f32_from_f64(Ctx& c);  // per-neuron target calcium FP64 -> FP32
 void f64_from_f32(Ctx& c);  // state arrays FP32 -> FP64 (before a host download)
 void launch_activity_f32(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);
 void launch_activity_fp64(Ctx& c, uint32_t k, const uint8_t* fired_prev, uint8_t* fired_cur, const ActVariant& v);

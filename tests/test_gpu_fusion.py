@@ -46,8 +46,6 @@ def assert_same(a, b, what):
 @pytest.mark.parametrize("model", [0, 1, 2, 3])
 @pytest.mark.parametrize("mode", ["all", "disabled", "targets"])
 def test_fused_block_equals_steps(precision, model, mode):
-    if mode == "targets" and precision == 1:
-        pytest.skip("the FP32 form runs one target calcium for all neurons")
     n = 20011  # odd: the last block of threads is partial
     runs = []
     for fused in (True, False):

@@ -219,11 +219,11 @@ def test_search_properties_at_1m():
 
 def test_per_neuron_target_calcium():
     """Targets from a calcium file (per neuron) steer growth as in the oracle;
-    the FP32 form refuses targets that differ between neurons."""
-    from relearn_b200 import Network, RelearnError
+    the FP32 form follows the FP64 form's growth with them."""
+    from relearn_b200 import Network
 
     n = 2000
-    net, sim, params, *_ = net_and_oracle(n, 1000.0, 77)
+    net, sim, params, pos, sig = net_and_oracle(n, 1000.0, 77)
     rng = np.random.default_rng(2)
     target = rng.choice([0.05, 0.3, 0.7], n)
     initial = rng.uniform(0.0, 0.2, n)
@@ -237,12 +237,28 @@ def test_per_neuron_target_calcium():
     sim.simulate(1, 1001)
     assert np.array_equal(net.target_calcium(), target)
     compare_state(net, sim, n)
-    p32 = dict(params)
-    p32["precision"] = 1
-    f = Network(p32)
-    f.set_target_calcium(np.full(n, 0.5))
-    with pytest.raises(RelearnError):
+    # FP32 form: the same per-neuron targets; calcium spread over both sides
+    # of every eta and target, so that each growth-curve branch is taken
+    forms = []
+    for precision in (0, 1):
+        p = dict(params)
+        p["precision"] = precision
+        f = Network(p)
+        f.set_positions(pos, sig)
         f.set_target_calcium(target)
+        f.set_neurons(calcium=np.random.default_rng(9).uniform(0.0, 0.9, n))
+        f.simulate(1, 1)
+        one = [f.get_elements(t)["delta"] for t in range(3)]
+        f.simulate(2, 100)
+        forms.append((one, [f.get_elements(t)["delta"] for t in range(3)], f.target_calcium()))
+        f.close()
+    (one64, run64, tg64), (one32, run32, tg32) = forms
+    assert np.array_equal(tg32, target)
+    for t in range(3):
+        # one step: nu (2 exp(-q^2) - 1) with nu = 1e-4, FP32 within 1e-9 absolute
+        assert np.max(np.abs(one32[t] - one64[t])) < 1e-9, t
+        # 100 steps: the summed deltas within 1e-3 relative
+        assert abs(run32[t].sum() - run64[t].sum()) <= 1e-3 * abs(run64[t]).sum(), t
 
 
 KERNELS = [("gamma", dict(kernel_type=1, kernel_k=2.0, kernel_scale=400.0)), ("gamma_k1", dict(kernel_type=1, kernel_k=1.0, kernel_scale=300.0)),

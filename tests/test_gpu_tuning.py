@@ -54,8 +54,6 @@ def test_every_activity_shape_gives_the_same_state(precision, mode):
     disabled and with per-neuron target calcium."""
     from relearn_b200 import ACT_SHAPES
 
-    if mode == "targets" and precision == 1:
-        pytest.skip("the FP32 form runs one target calcium for all neurons")
     n = 50000
     ref = None
     for b, p, v in ACT_SHAPES:
