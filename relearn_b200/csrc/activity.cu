@@ -41,6 +41,7 @@ struct ActArgs {
     double* delta1;
     double* delta2;
     double conductance, noise_mean, noise_stddev;
+    double syn0;  // the synaptic input without in-edges: 0.0 + 0.0 * conductance
     uint32_t h_model, h_calcium;
     double a, ab, c, d, v_spike, k1, k2, k3, scale_m;
     double beta, tau_inv, scale_c;
@@ -74,7 +75,7 @@ __device__ __forceinline__ double growth_curve(double current, double eta, doubl
     const double diff = current - xi;
     const double quot = diff / zeta;
     const double prod = quot * quot;
-    return (2.0 * rl_exp(-prod)) - 1.0;
+    return rl_fma(2.0, rl_exp(-prod), -1.0);  // (2 e) - 1: 2 e is exact, so one rounding either way
 }
 
 // gaussian_growth_curve with xi and zeta of a uniform target (growth_curve's
@@ -95,7 +96,19 @@ __device__ __forceinline__ double growth_curve_pre(double current, double eta, i
     const double r = rl_fma(-zeta, q0, diff);
     const double quot = rl_fma(r, zeta_inv, q0);  // == diff / zeta
     const double prod = quot * quot;
-    return (2.0 * rl_exp(-prod)) - 1.0;
+    return rl_fma(2.0, rl_exp(-prod), -1.0);  // (2 e) - 1, as in growth_curve
+}
+
+// growth_curve_pre without branches (rl_exp_flat; the eta == epsilon case
+// selected), for the software-pipelined block kernel.
+__device__ __forceinline__ double growth_curve_flat(double current, double eta, int flat, double xi, double zeta, double zeta_inv) {
+    const double diff = current - xi;
+    const double q0 = diff * zeta_inv;
+    const double r = rl_fma(-zeta, q0, diff);
+    const double quot = rl_fma(r, zeta_inv, q0);
+    const double prod = quot * quot;
+    const double g = rl_fma(2.0, rl_exp_flat(-prod), -1.0);
+    return flat ? (current == eta ? 0.0 : -1.0) : g;
 }
 
 // The network of neuron i: draws are keyed on the network's seed and the
@@ -238,6 +251,86 @@ __device__ __forceinline__ double growth_step(const ActArgs& A, int t, double ca
     return growth_curve(ca, eta, eps) * nu[t];
 }
 
+// The Izhikevich model's H substeps with the reference's break replaced by
+// freezing the state once the neuron spiked: every lane that has not spiked
+// runs the same operations on the same values, so the bits are those of
+// model_step, and the function has no branch (a branch ends the stretch of
+// code the compiler schedules together).  u + d of the spiking substep is
+// applied after the loop, to the frozen u.
+template <int H>
+__device__ __forceinline__ uint8_t izhikevich_frozen(const ActArgs& A, double input, double& x, double& u) {
+    double xv = x;
+    double uv = u;
+    bool done = false;
+#pragma unroll
+    for (int it = 0; it < H; ++it) {
+        const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
+        const double u_inc = (A.ab * xv) - (A.a * uv);
+        const double xn = xv + x_inc * A.scale_m;
+        const double un = uv + u_inc * A.scale_m;
+        const bool cross = xn >= A.v_spike;
+        xv = done ? xv : (cross ? A.c : xn);
+        uv = done ? uv : un;
+        done = done || cross;
+    }
+    x = xv;
+    u = done ? uv + A.d : uv;
+    return done ? 1 : 0;
+}
+
+// calcium_step without the branch on the spike: beta * fired is added in
+// every substep, as the reference writes it (beta * 0 = +0 leaves every value
+// as it was, the sign of a zero included).
+template <int H>
+__device__ __forceinline__ double calcium_flat(const ActArgs& A, uint8_t spiked, double ca) {
+    const double local_beta = A.beta * (spiked ? 1.0 : 0.0);
+#pragma unroll
+    for (int it = 0; it < H; ++it) {
+        ca += A.scale_c * (ca * A.tau_inv + local_beta);
+    }
+    return ca;
+}
+
+// Calcium and growth of one step (one target calcium for all neurons).
+template <int H>
+__device__ __forceinline__ void calcium_growth_flat(const ActArgs& A, uint8_t spiked, const double* nu, double& ca, double& d0, double& d1,
+                                                    double& d2) {
+    ca = calcium_flat<H>(A, spiked, ca);
+    d0 = d0 + growth_curve_flat(ca, A.eta[0], A.flat_u[0], A.xi_u[0], A.zeta_u[0], A.zeta_inv_u[0]) * nu[0];
+    d1 = d1 + growth_curve_flat(ca, A.eta[1], A.flat_u[1], A.xi_u[1], A.zeta_u[1], A.zeta_inv_u[1]) * nu[1];
+    d2 = d2 + growth_curve_flat(ca, A.eta[2], A.flat_u[2], A.xi_u[2], A.zeta_u[2], A.zeta_inv_u[2]) * nu[2];
+}
+
+// m consecutive steps of an Izhikevich neuron without synaptic input (one
+// target calcium for all neurons), software-pipelined: the model of step
+// k + 1 reads only x and u, not the calcium and growth of step k, so each
+// loop iteration computes both, and with every function in it free of
+// branches the compiler interleaves the two chains of dependent FP64
+// operations.  The operations and values are those of the step-by-step
+// order, so the bits are too.  zs[k * stride] is step k's standard normal
+// draw; `input` receives the last step's input, f and f_before the last two
+// spike flags.
+template <int H>
+__device__ __forceinline__ void izhikevich_chunk(const ActArgs& A, const double* zs, uint32_t stride, uint32_t m, const double* nu, double& xv,
+                                                 double& uv, double& ca, double& d0, double& d1, double& d2, double& input, uint8_t& f,
+                                                 uint8_t& f_before) {
+    double in_k = A.syn0 + (A.noise_mean + A.noise_stddev * zs[0]);
+    uint8_t sp = izhikevich_frozen<H>(A, in_k, xv, uv);
+    for (uint32_t k = 0; k + 1 < m; ++k) {
+        const double in_n = A.syn0 + (A.noise_mean + A.noise_stddev * zs[(k + 1) * stride]);
+        const uint8_t sp_n = izhikevich_frozen<H>(A, in_n, xv, uv);
+        calcium_growth_flat<H>(A, sp, nu, ca, d0, d1, d2);
+        f_before = f;
+        f = sp;
+        sp = sp_n;
+        in_k = in_n;
+    }
+    calcium_growth_flat<H>(A, sp, nu, ca, d0, d1, d2);
+    f_before = f;
+    f = sp;
+    input = in_k;
+}
+
 // One enabled neuron's step.  `z` is the neuron's standard normal draw of
 // this step.
 template <int H, int MODEL>
@@ -371,7 +464,7 @@ constexpr int kDrawChunk = 10;
 // lane computes step k's block, the odd lane step k + 1's, and each hands the
 // other the two words it needs (the same words as a block per lane).
 template <int BLOCK, int H, int MODEL, bool MULTI>
-__global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
                                                           uint8_t* __restrict__ fired_before_last) {
     constexpr int S = kDrawChunk;
     __shared__ double s_z[S * BLOCK];      // draw of step k0 + k of thread t at k * BLOCK + t
@@ -455,7 +548,14 @@ __global__ void __launch_bounds__(BLOCK, 1152 / BLOCK) k_activity_steps(ActArgs 
                 s_cnt[parity ^ 1u] = 0u;  // the next chunk's counter; nobody reads it before the barrier below
             }
             __syncthreads();
-            if (on) {
+            bool piped = false;
+            if constexpr (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
+                if (on && A.uniform_target) {
+                    izhikevich_chunk<H>(A, s_z + threadIdx.x, BLOCK, m, nu, xv, uv, ca, d0, d1, d2, input, f, f_before);
+                    piped = true;
+                }
+            }
+            if (on && !piped) {
                 for (uint32_t k = 0; k < m; ++k) {
                     const uint32_t step = stepc + k;
                     input = step_input(A, 0, s_z[k * BLOCK + threadIdx.x]);
@@ -654,6 +754,10 @@ ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* f
     A.conductance = k.conductance;
     A.noise_mean = k.noise_mean;
     A.noise_stddev = k.noise_stddev;
+    {
+        volatile double zero = 0.0;  // evaluated at run time, as the kernels' step_input does
+        A.syn0 = zero + zero * k.conductance;
+    }
     A.h_model = k.h_model;
     A.h_calcium = k.h_calcium;
     A.a = k.iz_a;

@@ -29,6 +29,9 @@
 //     pick pass over the chosen node's subtree.
 //   * Walks carry no stack: they follow per-node escape links.
 //   * A persistent form keeps the top levels of the octree in shared memory.
+//   * For sparse search lists, one search per warp (k_search_wide): the lanes
+//     evaluate a tree level of candidates side by side and the sum runs in
+//     the reference's order over the collected candidates.
 #include "bh_eval.cuh"
 #include "rl_context.cuh"
 #include "rl_math.cuh"
@@ -490,6 +493,347 @@ __global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t h
     }
 }
 
+// ------------------------------------------------- one search per warp
+// For search lists whose sources lie far apart (a network whose elements grow
+// slowly searches for a few thousand of its million neurons per update), a
+// packet of 32 sources walks the union of 32 unrelated walks, and one lane per
+// search leaves the device nearly idle.  Here a whole warp runs ONE search:
+//   * Candidates are collected in rounds, one tree level at a time: the lanes
+//     evaluate a round's nodes side by side (acceptance test and weight do not
+//     depend on the walk), and the children of expanded nodes, appended in
+//     visiting order (descending octant) behind each other by a warp scan,
+//     form the next round.  Every round lies in the reference's visiting order.
+//   * The position of every accepted candidate in the reference's depth-first
+//     visiting order follows from the rounds: bottom-up, each expanded node
+//     counts the candidates below it; top-down, a node's position is its
+//     parent's plus the counts of its earlier siblings.  The weights are
+//     scattered into that order.
+//   * The running sum is one sequential FP64 chain in that order (all lanes
+//     add, each keeps the sum at its own element), so every partial sum has
+//     the bits of the reference's sequential sum; the pick is the first
+//     partial sum that reaches r.
+// Deeper descents run the same way from the picked node.  The scratch of a
+// warp holds `cap` walk entries; a search that does not fit is redone by the
+// packet kernel (target kRedo, counted in `overflow`).
+constexpr int32_t kRedo = -2;
+
+struct WideArgs {
+    SearchArgs S;
+    // per warp slot, `cap` entries each
+    uint32_t* node;      // node of a walk entry
+    uint32_t* info;      // status | children << 2
+    uint32_t* child;     // first entry of an expanded node's children
+    uint32_t* cnt;       // candidates in the entry's subtree
+    uint32_t* pos;       // position of the entry's first candidate in visiting order
+    double* w;           // weight of an accepted entry
+    double* ord_w;       // weights in visiting order, then the running sums
+    uint32_t* ord_node;  // candidates in visiting order
+    uint32_t cap;
+    uint32_t slots;
+    uint32_t* tasks;     // task counter of this signal type
+    uint32_t* overflow;  // searches left to the packet kernel
+};
+
+struct WideSlot {
+    uint32_t *node, *info, *child, *cnt, *pos, *ord_node;
+    double *w, *ord_w;
+};
+
+constexpr int kWideRounds = kMaxLevels + 2;
+
+// Warp inclusive prefix sum of v.
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) {
+            v += t;
+        }
+    }
+    return v;
+}
+
+// The candidates of the subtree of `sub` (its children and down) in visiting
+// order: returns their number F (ord_node / ord_w), or -1 when a walk entry
+// did not fit, -2 when the walk left the node range.  `fallback` selects the
+// count / distance weights.
+__device__ int64_t wide_collect(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t sub, double sx, double sy, double sz,
+                                uint32_t source, uint32_t* s_round, uint32_t& touched) {
+    const int lane = threadIdx.x & 31;
+    const SearchArgs& S = A.S;
+    const uint4 sm = __ldg(&S.meta[sub]);
+    const uint32_t k0 = inner_children(sm);
+    if ((uint32_t)lane < k0) {
+        P.node[lane] = sm.x + k0 - 1u - (uint32_t)lane;  // children in visiting order: last octant first
+    }
+    s_round[0] = 0;
+    s_round[1] = k0;
+    int rounds = 0;
+    bool bad = false;
+    __syncwarp();
+    // forward: evaluate round after round
+    for (;;) {
+        const uint32_t rb = s_round[rounds], re = s_round[rounds + 1];
+        if (rb == re) {
+            break;
+        }
+        if (rounds + 2 >= kWideRounds) {
+            return -2;
+        }
+        uint32_t next = re;
+        for (uint32_t base = rb; base < re; base += 32) {
+            const uint32_t e = base + (uint32_t)lane;
+            int st = ST_DISCARD;
+            double w = 0.0;
+            uint32_t nch = 0, first = 0;
+            if (e < re) {
+                const uint32_t nd = P.node[e];
+                if (nd >= S.num_nodes) {
+                    bad = true;
+                } else {
+                    const double4 rr = ldg4(&S.rec[nd]);
+                    const uint4 mm = __ldg(&S.meta[nd]);
+                    const double md = __ldg(&S.maxdim[nd]);
+                    const Eval ev = evaluate(rr, make_uint2(mm.x, mm.y), md, sx, sy, sz, source, W.theta, S.mu, W.scale, false, S.kernel);
+                    st = ev.status;
+                    w = ev.w;
+                    ++touched;
+                    if (st == ST_EXPAND) {
+                        nch = (uint32_t)__popc(topo_mask(mm.y));
+                        first = mm.x;
+                    }
+                }
+            }
+            const uint32_t inc = warp_inclusive(nch);
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+            if (next + total > A.cap) {
+                return -1;
+            }
+            const uint32_t cs = next + inc - nch;
+            if (e < re) {
+                P.info[e] = (uint32_t)st | (nch << 2);
+                P.child[e] = cs;
+                P.w[e] = w;
+            }
+            for (uint32_t c = 0; c < nch; ++c) {
+                P.node[cs + c] = first + nch - 1u - c;
+            }
+            next += total;
+        }
+        if (__any_sync(0xFFFFFFFFu, bad)) {
+            return -2;
+        }
+        ++rounds;
+        if (lane == 0) {
+            s_round[rounds + 1] = next;
+        }
+        __syncwarp();
+    }
+    // bottom-up: candidates below every entry
+    for (int r = rounds - 1; r >= 0; --r) {
+        const uint32_t rb = s_round[r], re = s_round[r + 1];
+        for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
+            const uint32_t inf = P.info[e];
+            const int st = (int)(inf & 3u);
+            uint32_t n = st == ST_ACCEPT ? 1u : 0u;
+            if (st == ST_EXPAND) {
+                const uint32_t c0 = P.child[e];
+                for (uint32_t c = 0; c < (inf >> 2); ++c) {
+                    n += P.cnt[c0 + c];
+                }
+            }
+            P.cnt[e] = n;
+        }
+        __syncwarp();
+    }
+    // top-down: positions in visiting order; the candidates go to their place
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < k0; base += 32) {
+        const uint32_t e = base + (uint32_t)lane;
+        const uint32_t n = e < k0 ? P.cnt[e] : 0u;
+        const uint32_t inc = warp_inclusive(n);
+        if (e < k0) {
+            P.pos[e] = carry + inc - n;
+        }
+        carry += __shfl_sync(0xFFFFFFFFu, inc, 31);
+    }
+    __syncwarp();
+    for (int r = 0; r < rounds; ++r) {
+        const uint32_t rb = s_round[r], re = s_round[r + 1];
+        for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
+            const uint32_t inf = P.info[e];
+            const int st = (int)(inf & 3u);
+            const uint32_t p = P.pos[e];
+            if (st == ST_ACCEPT) {
+                P.ord_node[p] = P.node[e];
+                P.ord_w[p] = P.w[e];
+            } else if (st == ST_EXPAND) {
+                const uint32_t c0 = P.child[e];
+                uint32_t acc = p;
+                for (uint32_t c = 0; c < (inf >> 2); ++c) {
+                    P.pos[c0 + c] = acc;
+                    acc += P.cnt[c0 + c];
+                }
+            }
+        }
+        __syncwarp();
+    }
+    return (int64_t)carry;
+}
+
+// The running sum of ord_w[0, F) in order, one FP64 addition after the other
+// (the reference's sum); ord_w[i] becomes the sum up to and including i.
+// Returns the total.
+__device__ double wide_running_sum(double* ord_w, uint32_t F) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (uint32_t base = 0; base < F; base += 32) {
+        const uint32_t i = base + (uint32_t)lane;
+        const double v = i < F ? ord_w[i] : 0.0;
+        double mine = 0.0;
+        if (F - base >= 32) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                s = s + __shfl_sync(0xFFFFFFFFu, v, q);
+                mine = q == lane ? s : mine;
+            }
+        } else {
+            const uint32_t lim = F - base;
+            for (uint32_t q = 0; q < lim; ++q) {
+                s = s + __shfl_sync(0xFFFFFFFFu, v, (int)q);
+                mine = q == (uint32_t)lane ? s : mine;
+            }
+        }
+        if (i < F) {
+            ord_w[i] = mine;
+        }
+    }
+    __syncwarp();
+    return s;
+}
+
+// One search (one vacant axon element j of `source`) by the whole warp:
+// the target neuron, -1 when the search fails, kRedo when it did not fit.
+__device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t source, uint32_t j, uint32_t* s_round,
+                               uint32_t& touched) {
+    const SearchArgs& S = A.S;
+    const double sx = S.px[source], sy = S.py[source], sz = S.pz[source];
+    uint32_t sub = W.root;
+    for (uint32_t depth = 0; depth <= (uint32_t)kMaxLevels + 2u; ++depth) {
+        const uint4 sm = __ldg(&S.meta[sub]);
+        if (topo_leaf(sm.y)) {
+            return depth == 0 ? -1 : (int32_t)sm.x;
+        }
+        const int64_t got = wide_collect(A, P, W, sub, sx, sy, sz, source, s_round, touched);
+        if (got == -1) {
+            return kRedo;
+        }
+        if (got < 0) {
+            atomicOr(S.err, (uint32_t)DERR_WALK);
+            return -1;
+        }
+        const uint32_t F = (uint32_t)got;
+        double total = wide_running_sum(P.ord_w, F);
+        if (total == 0.0) {
+            // every weight underflowed: count / distance weights over the same candidates
+            for (uint32_t i = threadIdx.x & 31; i < F; i += 32) {
+                const uint32_t nd = P.ord_node[i];
+                const uint4 mm = __ldg(&S.meta[nd]);
+                const Eval ev = evaluate(ldg4(&S.rec[nd]), make_uint2(mm.x, mm.y), __ldg(&S.maxdim[nd]), sx, sy, sz, source, W.theta, S.mu, W.scale,
+                                         true, S.kernel);
+                P.ord_w[i] = ev.w;
+            }
+            __syncwarp();
+            total = wide_running_sum(P.ord_w, F);
+        }
+        if (total == 0.0) {
+            return -1;  // no candidate: the search fails
+        }
+        const double r = pick_threshold(total, W.seed, S.step, source - W.first, j, depth);
+        int64_t pick = -1;
+        for (uint32_t base = 0; base < F; base += 32) {
+            const uint32_t i = base + (threadIdx.x & 31);
+            const uint32_t hit = __ballot_sync(0xFFFFFFFFu, i < F && P.ord_w[i] >= r);
+            if (hit) {
+                pick = P.ord_node[base + (uint32_t)(__ffs((int)hit) - 1)];
+                break;
+            }
+        }
+        if (pick < 0) {
+            atomicOr(S.err, (uint32_t)DERR_NO_CROSSING);
+            return -1;
+        }
+        sub = (uint32_t)pick;
+        __syncwarp();  // the next descent overwrites the scratch this one read
+    }
+    atomicOr(S.err, (uint32_t)DERR_STACK);
+    return -1;
+}
+
+// Persistent warps, one search per task: the task counter hands out list
+// entries (32 per warp task of the packet kernels' segment layout).
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32, 2) k_search_wide(WideArgs A) {
+    __shared__ uint32_t s_round_all[WPB][kWideRounds + 1];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * WPB + (uint32_t)wib;
+    if (slot >= A.slots) {
+        return;  // whole warp
+    }
+    uint32_t* s_round = s_round_all[wib];
+    const SearchArgs& S = A.S;
+    const uint64_t off = (uint64_t)slot * A.cap;
+    const WideSlot P{ A.node + off, A.info + off, A.child + off, A.cnt + off, A.pos + off, A.ord_node + off, A.w + off, A.ord_w + off };
+    const uint32_t total_tasks = S.seg_warp[S.num_segs] * 32u;
+    uint32_t touched = 0;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) {
+            task = atomicAdd(A.tasks, 1u);
+        }
+        task = __shfl_sync(0xFFFFFFFFu, task, 0);
+        if (task >= total_tasks) {
+            break;
+        }
+        const uint32_t wg = task >> 5;
+        uint32_t lo = 0, hi = S.num_segs;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (S.seg_warp[mid] <= wg) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
+        }
+        const uint64_t idx = S.seg_begin[lo] + (uint64_t)(wg - S.seg_warp[lo]) * 32 + (task & 31u);
+        if (idx >= S.seg_end[lo]) {
+            continue;
+        }
+        const NetInfo& N = S.nets[S.seg_net[lo]];
+        const WarpNet W{ N.theta, N.scale, N.seed, S.seg_net[lo], N.first };
+        int32_t result = -1;
+        if (!N.root_leaf) {
+            result = wide_search(A, P, W, S.list_src[idx], S.list_j[idx], s_round, touched);
+        }
+        if (lane == 0) {
+            S.target[idx] = result;
+            if (result == kRedo) {
+                atomicAdd(A.overflow, 1u);
+            }
+        }
+        __syncwarp();
+    }
+    unsigned long long t = touched;
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+    }
+    if (lane == 0) {
+        atomicAdd(S.touched, t);
+    }
+}
+
 using SearchKernel = void (*)(SearchArgs);
 using HotKernel = void (*)(SearchArgs, uint32_t);
 
@@ -605,6 +949,65 @@ __global__ void k_req_scatter(uint64_t m, const uint32_t* __restrict__ list_src,
 
 }  // namespace
 
+// Whether a candidate shape runs on this context: the one-search-per-warp
+// form is written for the FP64 search and pays off on large networks.
+bool search_variant_applies(const Ctx& c, const SearchVariant& v) {
+    return v.packet != 0 || (!is_fp32(c) && c.n >= kWideMinNeurons);
+}
+
+namespace {
+
+// The one-search-per-warp kernel on signal type t's list; searches that did
+// not fit their warp's scratch are redone by the packet kernel (which writes
+// every target of the list again).
+void launch_wide(Ctx& c, const SearchArgs& a, uint32_t warps, int t, const SearchVariant& v) {
+    constexpr int WPB = 4;
+    Search& S = c.search;
+    cudaStream_t st = c.stream;
+    const uint32_t tasks = warps * 32u;
+    const uint32_t cap = (uint32_t)std::min<uint64_t>(kWideCap, (c.tree.num_nodes + 31) / 32 * 32);
+    const uint32_t slots = std::min<uint32_t>(tasks, (uint32_t)c.num_sms * kWideWarpsPerSM);
+    const size_t cells = (size_t)slots * cap;
+    S.w_node.ensure(cells);
+    S.w_info.ensure(cells);
+    S.w_child.ensure(cells);
+    S.w_cnt.ensure(cells);
+    S.w_pos.ensure(cells);
+    S.w_ord_node.ensure(cells);
+    S.w_w.ensure(cells);
+    S.w_ord_w.ensure(cells);
+    S.w_overflow.ensure(2);
+    RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p + t, 0, sizeof(uint32_t), st));
+    RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p + t, 0, sizeof(uint32_t), st));
+    WideArgs A;
+    A.S = a;
+    A.node = S.w_node.p;
+    A.info = S.w_info.p;
+    A.child = S.w_child.p;
+    A.cnt = S.w_cnt.p;
+    A.pos = S.w_pos.p;
+    A.w = S.w_w.p;
+    A.ord_w = S.w_ord_w.p;
+    A.ord_node = S.w_ord_node.p;
+    A.cap = cap;
+    A.slots = slots;
+    A.tasks = S.tasks.p + t;
+    A.overflow = S.w_overflow.p + t;
+    k_search_wide<WPB><<<(slots + WPB - 1) / WPB, WPB * 32, 0, st>>>(A);
+    RL_LAUNCH_CHECK();
+    uint32_t over = 0;
+    RL_CUDA_TRY(cudaMemcpyAsync(&over, S.w_overflow.p + t, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    RL_CUDA_TRY(cudaStreamSynchronize(st));
+    if (over) {
+        const SearchVariant fb{ 2, 32, 1, 0 };
+        k_search<2, 32, 1><<<(warps + fb.warps - 1) / fb.warps, fb.warps * 32, 0, st>>>(a);
+        RL_LAUNCH_CHECK();
+    }
+    (void)v;
+}
+
+}  // namespace
+
 // Times every search variant that fits the octree on the current search list
 // and keeps the fastest.  Each variant runs twice (the second run is timed);
 // the searches are deterministic, so the variants leave the same targets, and
@@ -621,6 +1024,10 @@ void tune_search(Ctx& c, F&& launch_all) {
     float best = 1e30f;
     SearchVariant pick = c.tune.search;
     for (const SearchVariant& v : search_variants()) {
+        if (!search_variant_applies(c, v)) {
+            c.tune.search_ms.push_back(0.0f);  // keeps the times in candidate order
+            continue;
+        }
         launch_all(v);
         RL_CUDA_TRY(cudaEventRecord(e0, st));
         launch_all(v);
@@ -660,6 +1067,9 @@ const std::vector<SearchVariant>& search_variants() {
                 out.push_back(SearchVariant{ 32, p, 1, hot });
             }
         }
+        // one search per warp (packet 0; FP64 form, large networks): for
+        // search lists whose sources lie far apart
+        out.push_back(SearchVariant{ 4, 0, 0, 0 });
         return out;
     }();
     return v;
@@ -810,6 +1220,8 @@ void run_search(Ctx& c, uint32_t step) {
                 if (is_fp32(c)) {
                     launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, launches[t].segs, launches[t].warps, step, v,
                                       S.tasks.p + t);
+                } else if (v.packet == 0) {
+                    launch_wide(c, args[t], launches[t].warps, t, v);
                 } else if (v.hot > 0) {
                     const HotKernel kern = fp64_hot_kernel(v);
                     const uint32_t hot = hot_nodes(c, v, sizeof(double4) + sizeof(uint4) + sizeof(double));

@@ -111,6 +111,9 @@ struct Search {
     DBuf<uint32_t> tasks;    // persistent search form: task counter per signal type
     DBuf<uint32_t> seg_warp[2], seg_net[2];
     DBuf<uint64_t> seg_begin[2], seg_end[2];
+    // one-search-per-warp form: walk entries of every warp slot
+    DBuf<uint32_t> w_node, w_info, w_child, w_cnt, w_pos, w_ord_node, w_overflow;
+    DBuf<double> w_w, w_ord_w;
     uint64_t num_searches = 0;
     uint64_t num_exc = 0;
     uint64_t num_requests = 0;
@@ -261,6 +264,11 @@ struct Tuning {
 };
 
 const std::vector<SearchVariant>& search_variants();
+bool search_variant_applies(const Ctx& c, const SearchVariant& v);
+// one-search-per-warp form: walk entries per warp, warps per SM, smallest network
+constexpr uint32_t kWideCap = 6144;
+constexpr uint32_t kWideWarpsPerSM = 8;
+constexpr uint32_t kWideMinNeurons = 65536;
 uint32_t hot_nodes(const Ctx& c, const SearchVariant& v, size_t node_bytes);
 const std::vector<ActVariant>& act_variants();
 

@@ -283,6 +283,50 @@ RL_HD double rl_exp(double x) {
     return scale_pow2(t_hi + rl_fma(t_hi, p, t_lo), m);
 }
 
+// rl_exp without branches, for kernels that interleave independent chains of
+// arithmetic (a branch ends the stretch of code the compiler schedules as
+// one): the main path always runs, the scaling by 2^m is always two
+// multiplications by powers of two — 2^m and 1 in the normal range,
+// 2^1023 and 2^(m-1023) above it, 2^(m+54) and 2^-54 into the subnormals, as
+// scale_pow2 does — and NaN, overflow and underflow are selected at the end.
+// The same bits as rl_exp for every argument: in range every operation is
+// the same, and every product by a power of two is exact except the one
+// rounding both forms make.  Out of range the main path's value is discarded
+// (the host clamps the argument first, so that its int conversion is
+// defined; on the device the conversion saturates).
+RL_HD double rl_exp_flat(double x) {
+#if defined(__CUDA_ARCH__)
+    const double xc = x;
+#else
+    const double xc = x != x ? 0.0 : fmin(fmax(x, -746.0), 710.0);
+#endif
+    const double kd = floor(xc * 92.332482616893656768 + 0.5);  // 64 / ln 2
+    const double r = rl_fma(-kd, RL_LN2_LO / 64.0, xc - kd * (RL_LN2_HI / 64.0));
+    const int ki = (int)kd;
+    const int j = ki & 63;
+    const int m = ki >> 6;
+    double p = rl_fma(1.3888888888888889e-03, r, 8.3333333333333332e-03);
+    p = rl_fma(p, r, 4.1666666666666664e-02);
+    p = rl_fma(p, r, 1.6666666666666666e-01);
+    p = rl_fma(p, r, 0.5);
+    p = rl_fma(r * r, p, r);
+#if defined(__CUDA_ARCH__)
+    const double2 t = __ldg(&rl_exp_table_dev[j]);
+    const double t_hi = t.x, t_lo = t.y;
+#else
+    const double t_hi = rl_exp_table_host[j][0], t_lo = rl_exp_table_host[j][1];
+#endif
+    const double y = t_hi + rl_fma(t_hi, p, t_lo);
+    const bool low = m < -1021;
+    const bool high = m > 1023;
+    int a = low ? m + 54 : (high ? 1023 : m);
+    int b = low ? -54 : (high ? m - 1023 : 0);
+    a = a < -1022 ? -1022 : (a > 1023 ? 1023 : a);  // only out-of-range arguments reach the clamps
+    b = b < -1022 ? -1022 : (b > 1023 ? 1023 : b);
+    const double v = (y * as_f64((uint64_t)(a + 1023) << 52)) * as_f64((uint64_t)(b + 1023) << 52);
+    return x != x ? x : (x > 709.782712893384 ? as_f64(0x7FF0000000000000ull) : (x < -745.1332191019412 ? 0.0 : v));
+}
+
 // log(x) for finite x > 0 (normal range): x = m 2^e with m in
 // [sqrt(2)/2, sqrt(2)), log(m) = 2 atanh(s), s = (m-1)/(m+1), odd series in s.
 RL_HD double rl_log(double x) {

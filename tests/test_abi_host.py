@@ -106,7 +106,7 @@ def probe(tmp_path_factory):
     subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(so),
                     os.path.join(ROOT, "tests", "helpers", "math_probe.cpp")], check=True)
     L = C.CDLL(str(so))
-    for name in ("probe_exp", "probe_log", "probe_quantile", "probe_next_up"):
+    for name in ("probe_exp", "probe_exp_flat", "probe_log", "probe_quantile", "probe_next_up"):
         getattr(L, name).restype = C.c_double
         getattr(L, name).argtypes = [C.c_double]
     for name in ("probe_hypot3", "probe_std_hypot3"):
@@ -144,6 +144,21 @@ def test_shared_math_bitwise_agreement(probe, oracle_mod):
         assert list(out) == oracle_mod.philox(*map(int, c))
     for t in rng.uniform(1e-3, 1e6, 1000):
         assert probe.probe_next_up(float(t)) == np.nextafter(float(t), float(t) + 1e-5)
+
+
+def test_branch_free_exp_equals_exp(probe):
+    """rl_exp_flat (the form the block activity kernel interleaves) gives
+    rl_exp's bits for every argument: across the range, at the overflow and
+    underflow edges, in the subnormal results, and for infinities and NaN."""
+    rng = np.random.default_rng(12)
+    xs = np.concatenate([rng.uniform(-750, 712, 30000), rng.uniform(-40, 0, 20000), rng.uniform(-745.2, -707.0, 10000),
+                         rng.uniform(709.0, 709.8, 5000), [709.782712893384, 709.7827128933841, 709.78271289338397, -745.1332191019412,
+                         -745.1332191019411, -708.3964185322641, -708.39641853226, 0.0, -0.0, 1e-300, -1e-300, 710.0, -746.0, 1e308,
+                         -1e308, float("inf"), float("-inf")]])
+    for x in xs:
+        a, b = probe.probe_exp(float(x)), probe.probe_exp_flat(float(x))
+        assert np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64), (x, a, b)
+    assert np.isnan(probe.probe_exp_flat(float("nan")))
 
 
 @pytest.mark.parametrize("kernel", [(1, 2.0, 400.0, 0.0), (1, 1.0, 300.0, 0.0), (2, 1.0, 1.0, 1500.0), (2, 1.0, 1.0, float("inf")),

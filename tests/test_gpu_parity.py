@@ -77,6 +77,31 @@ def test_search_requests(n, mixture, lower, upper):
             assert np.array_equal(g[k], o[k]), k
 
 
+@pytest.mark.parametrize("n,mixture,sources", [(80000, False, 700), (80000, True, 700), (20000, True, 20000)])
+def test_search_one_per_warp(n, mixture, sources):
+    """The one-search-per-warp kernel (search_packet 0) against the oracle:
+    a few hundred sources spread over the network (the sparse lists it is
+    for), and every neuron a source, with 1-3 vacant axons each."""
+    net, sim, params, pos, sig = net_and_oracle(n, 1000.0 * (n / 2000) ** (1 / 3), 7 + n, mixture)
+    rng = np.random.default_rng(n + sources)
+    va = np.zeros(n, np.uint32)
+    va[rng.choice(n, sources, replace=False)] = rng.integers(1, 4, sources).astype(np.uint32)
+    ve = rng.integers(0, 4, n).astype(np.uint32)
+    vi = rng.integers(0, 3, n).astype(np.uint32)
+    for t, v in enumerate((va, ve, vi)):
+        sim.set_elements(t, v.astype(np.float64) + 0.5, np.zeros(n), np.zeros(n, np.uint32), v)
+    sim.update_tree(ve, vi)
+    net.prepare_update_connectivity(va, ve, vi)
+    net.set_tuning(search_warps=4, search_packet=0, search_cap=0, search_hot=0)
+    for step in (100, 200):
+        g = net.find_targets(step)
+        o = sim.find_targets(step)
+        assert len(g) == len(o) > 0
+        for k in ("target", "source", "j", "signal"):
+            assert np.array_equal(g[k], o[k]), k
+    assert net.stats()["nodes_touched"] > 0
+
+
 def test_connector_and_edges():
     n = 3000
     net, sim, *_ = net_and_oracle(n, 1100.0, 51)
