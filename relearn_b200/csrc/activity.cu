@@ -126,16 +126,6 @@ __device__ __forceinline__ void neuron_net(const ActArgs& A, uint32_t i, uint64_
     }
 }
 
-__device__ __forceinline__ void disabled_neuron(const ActArgs& A, uint32_t i) {
-    if (A.input) {
-        A.input[i] = 0.0;
-    }
-    A.fired_cur[i] = A.fired_prev[i];
-    A.delta0[i] = A.delta0[i] + 0.0;
-    A.delta1[i] = A.delta1[i] + 0.0;
-    A.delta2[i] = A.delta2[i] + 0.0;
-}
-
 // This step's input: the synaptic sum (an integer, exact in any order) times
 // the conductance, then NormalActivityInputCPU's draw z.
 __device__ __forceinline__ double step_input(const ActArgs& A, long long isum, double z) {
@@ -331,11 +321,9 @@ __device__ __forceinline__ void izhikevich_chunk(const ActArgs& A, const double*
     input = in_k;
 }
 
-// One enabled neuron's step.  `z` is the neuron's standard normal draw of
-// this step.
-template <int H, int MODEL>
-__device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i, uint64_t seed,
-                                                uint32_t local, const double* nu, double z) {
+// The synaptic input's integer sum: the weights of in-edges whose source
+// fired in the previous step (exact in any order).
+__device__ __forceinline__ long long synaptic_sum(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t i) {
     long long isum = 0;
     if (D->has_edges) {
         const uint32_t* __restrict__ off = D->off;
@@ -348,32 +336,35 @@ __device__ __forceinline__ void activity_neuron(const ActArgs& A, const ActDesc*
             }
         }
     }
+    return isum;
+}
+
+// One enabled neuron's step on state already in registers (loaded before
+// the kernel's draw phase).  `z` is the neuron's standard normal draw of this
+// step.
+template <int H, int MODEL>
+__device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const double* nu,
+                                                     double z, long long isum, double xv, double uv, double ca, double tgt, double d0, double d1,
+                                                     double d2) {
     const double input = step_input(A, isum, z);
     if (A.input) {
         A.input[i] = input;
     }
-
-    double xv = A.x[i];
-    double uv = A.u[i];
     const uint8_t spiked = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
     A.x[i] = xv;
     A.u[i] = uv;
     A.fired_cur[i] = spiked;
-
-    const double ca = calcium_step<H>(A, spiked, A.calcium[i]);
+    ca = calcium_step<H>(A, spiked, ca);
     A.calcium[i] = ca;
-
-    double* deltas[3] = { A.delta0, A.delta1, A.delta2 };
-    const double tgt = A.uniform_target ? 0.0 : A.target[i];
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const double inc = growth_step(A, t, ca, tgt, nu);
-        deltas[t][i] = deltas[t][i] + inc;
-    }
+    A.delta0[i] = d0 + growth_step(A, 0, ca, tgt, nu);
+    A.delta1[i] = d1 + growth_step(A, 1, ca, tgt, nu);
+    A.delta2[i] = d2 + growth_step(A, 2, ca, tgt, nu);
 }
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
-// persistent shape) each thread strides over the neurons.
+// persistent shape) each thread strides over the neurons.  A neuron's state
+// and synaptic sum are loaded first, so that their memory latency overlaps
+// the draw and its tail queue.
 // The background draw's tail piece (about 15 % of the draws, but some lane
 // of nearly every warp) is run for the whole block together: lanes whose
 // uniform falls in the tails queue it in shared memory, the first warps of the
@@ -403,7 +394,19 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
         uint32_t local = 0;
         const double* nu = nullptr;
         double p = 0.5;
+        double xv = 0.0, uv = 0.0, cav = 0.0, tg = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0;
+        long long isum = 0;
+        if (i < A.n) {
+            d0 = A.delta0[i];
+            d1 = A.delta1[i];
+            d2 = A.delta2[i];
+        }
         if (on) {
+            xv = A.x[i];
+            uv = A.u[i];
+            cav = A.calcium[i];
+            tg = A.uniform_target ? 0.0 : A.target[i];
+            isum = synaptic_sum(A, D, i);
             neuron_net<MULTI>(A, i, seed, local, nu);
             p = MULTI ? noise_uniform(seed, step, local) : noise_uniform_rk(A.rk0, A.rk1, step, local);
         }
@@ -433,9 +436,15 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             z = s_z[threadIdx.x];
         }
         if (on) {
-            activity_neuron<H, MODEL>(A, D, step, i, seed, local, nu, z);
+            activity_neuron_regs<H, MODEL>(A, step, i, seed, local, nu, z, isum, xv, uv, cav, tg, d0, d1, d2);
         } else if (i < A.n) {
-            disabled_neuron(A, i);
+            if (A.input) {
+                A.input[i] = 0.0;
+            }
+            A.fired_cur[i] = A.fired_prev[i];
+            A.delta0[i] = d0 + 0.0;
+            A.delta1[i] = d1 + 0.0;
+            A.delta2[i] = d2 + 0.0;
         }
     }
 }
