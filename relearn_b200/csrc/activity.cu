@@ -107,7 +107,7 @@ __device__ __forceinline__ double growth_curve_flat(double current, double eta, 
     const double r = rl_fma(-zeta, q0, diff);
     const double quot = rl_fma(r, zeta_inv, q0);
     const double prod = quot * quot;
-    const double g = rl_fma(2.0, rl_exp_flat(-prod), -1.0);
+    const double g = rl_fma(2.0, rl_exp_flat_nonpos(-prod), -1.0);
     return flat ? (current == eta ? 0.0 : -1.0) : g;
 }
 
@@ -241,30 +241,32 @@ __device__ __forceinline__ double growth_step(const ActArgs& A, int t, double ca
     return growth_curve(ca, eta, eps) * nu[t];
 }
 
-// The Izhikevich model's H substeps with the reference's break replaced by
-// freezing the state once the neuron spiked: every lane that has not spiked
-// runs the same operations on the same values, so the bits are those of
-// model_step, and the function has no branch (a branch ends the stretch of
-// code the compiler schedules together).  u + d of the spiking substep is
-// applied after the loop, to the frozen u.
+// The Izhikevich model's H substeps without the reference's break: the
+// substeps run on, and the state at the first crossing is what the function
+// returns — x = c and u = u(crossing) + d, as model_step leaves them — so the
+// bits are model_step's.  The substeps after a crossing compute values that
+// are discarded (they may grow to infinity; nothing traps).  The function has
+// no branch (a branch ends the stretch of code the compiler schedules
+// together), and a substep costs one select (the u of a first crossing) on
+// top of the model's arithmetic.
 template <int H>
 __device__ __forceinline__ uint8_t izhikevich_frozen(const ActArgs& A, double input, double& x, double& u) {
     double xv = x;
     double uv = u;
+    double u_cross = 0.0;
     bool done = false;
 #pragma unroll
     for (int it = 0; it < H; ++it) {
         const double x_inc = (A.k1 * xv * xv) + (A.k2 * xv) + A.k3 - uv + input;
         const double u_inc = (A.ab * xv) - (A.a * uv);
-        const double xn = xv + x_inc * A.scale_m;
-        const double un = uv + u_inc * A.scale_m;
-        const bool cross = xn >= A.v_spike;
-        xv = done ? xv : (cross ? A.c : xn);
-        uv = done ? uv : un;
-        done = done || cross;
+        xv = xv + x_inc * A.scale_m;
+        uv = uv + u_inc * A.scale_m;
+        const bool first = !done && xv >= A.v_spike;
+        u_cross = first ? uv : u_cross;
+        done = done || first;
     }
-    x = xv;
-    u = done ? uv + A.d : uv;
+    x = done ? A.c : xv;
+    u = done ? u_cross + A.d : uv;
     return done ? 1 : 0;
 }
 

@@ -33,6 +33,7 @@
 //     evaluate a tree level of candidates side by side and the sum runs in
 //     the reference's order over the collected candidates.
 #include "bh_eval.cuh"
+#include "bh_wide.cuh"
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -494,223 +495,42 @@ __global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t h
 }
 
 // ------------------------------------------------- one search per warp
-// For search lists whose sources lie far apart (a network whose elements grow
-// slowly searches for a few thousand of its million neurons per update), a
-// packet of 32 sources walks the union of 32 unrelated walks, and one lane per
-// search leaves the device nearly idle.  Here a whole warp runs ONE search:
-//   * Candidates are collected in rounds, one tree level at a time: the lanes
-//     evaluate a round's nodes side by side (acceptance test and weight do not
-//     depend on the walk), and the children of expanded nodes, appended in
-//     visiting order (descending octant) behind each other by a warp scan,
-//     form the next round.  Every round lies in the reference's visiting order.
-//   * The position of every accepted candidate in the reference's depth-first
-//     visiting order follows from the rounds: bottom-up, each expanded node
-//     counts the candidates below it; top-down, a node's position is its
-//     parent's plus the counts of its earlier siblings.  The weights are
-//     scattered into that order.
-//   * The running sum is one sequential FP64 chain in that order (all lanes
-//     add, each keeps the sum at its own element), so every partial sum has
-//     the bits of the reference's sequential sum; the pick is the first
-//     partial sum that reaches r.
-// Deeper descents run the same way from the picked node.  The scratch of a
-// warp holds `cap` walk entries; a search that does not fit is redone by the
-// packet kernel (target kRedo, counted in `overflow`).
-constexpr int32_t kRedo = -2;
-
+// (bh_wide.cuh): the FP64 evaluation, search and kernel.
 struct WideArgs {
     SearchArgs S;
-    // per warp slot, `cap` entries each
-    uint32_t* node;      // node of a walk entry
-    uint32_t* info;      // status | children << 2
-    uint32_t* child;     // first entry of an expanded node's children
-    uint32_t* cnt;       // candidates in the entry's subtree
-    uint32_t* pos;       // position of the entry's first candidate in visiting order
-    double* w;           // weight of an accepted entry
-    double* ord_w;       // weights in visiting order, then the running sums
-    uint32_t* ord_node;  // candidates in visiting order
+    WideSlot all;        // scratch of every warp slot, `cap` entries each
     uint32_t cap;
     uint32_t slots;
     uint32_t* tasks;     // task counter of this signal type
     uint32_t* overflow;  // searches left to the packet kernel
 };
 
-struct WideSlot {
-    uint32_t *node, *info, *child, *cnt, *pos, *ord_node;
-    double *w, *ord_w;
-};
-
-constexpr int kWideRounds = kMaxLevels + 2;
-
-// Warp inclusive prefix sum of v.
-__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
-        if (lane >= o) {
-            v += t;
-        }
-    }
-    return v;
+__device__ __forceinline__ WideSlot wide_slot(const WideSlot& all, uint64_t off) {
+    return WideSlot{ all.node + off, all.info + off, all.child + off, all.cnt + off, all.pos + off, all.ord_node + off, all.w + off, all.ord_w + off };
 }
 
-// The candidates of the subtree of `sub` (its children and down) in visiting
-// order: returns their number F (ord_node / ord_w), or -1 when a walk entry
-// did not fit, -2 when the walk left the node range.  `fallback` selects the
-// count / distance weights.
-__device__ int64_t wide_collect(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t sub, double sx, double sy, double sz,
-                                uint32_t source, uint32_t* s_round, uint32_t& touched) {
-    const int lane = threadIdx.x & 31;
+// The FP64 candidates of the subtree of `sub` in visiting order.
+__device__ __forceinline__ int64_t wide_collect64(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t sub, double sx, double sy,
+                                                  double sz, uint32_t source, uint32_t* s_round, uint32_t& touched) {
     const SearchArgs& S = A.S;
     const uint4 sm = __ldg(&S.meta[sub]);
-    const uint32_t k0 = inner_children(sm);
-    if ((uint32_t)lane < k0) {
-        P.node[lane] = sm.x + k0 - 1u - (uint32_t)lane;  // children in visiting order: last octant first
-    }
-    s_round[0] = 0;
-    s_round[1] = k0;
-    int rounds = 0;
-    bool bad = false;
-    __syncwarp();
-    // forward: evaluate round after round
-    for (;;) {
-        const uint32_t rb = s_round[rounds], re = s_round[rounds + 1];
-        if (rb == re) {
-            break;
+    return wide_collect(P, A.cap, sm.x, inner_children(sm), s_round, touched, [&](uint32_t nd) {
+        WideEval r{ ST_DISCARD, 0.0, 0u, 0u, false };
+        if (nd >= S.num_nodes) {
+            r.bad = true;
+            return r;
         }
-        if (rounds + 2 >= kWideRounds) {
-            return -2;
+        const uint4 mm = __ldg(&S.meta[nd]);
+        const Eval ev = evaluate(ldg4(&S.rec[nd]), make_uint2(mm.x, mm.y), __ldg(&S.maxdim[nd]), sx, sy, sz, source, W.theta, S.mu, W.scale, false,
+                                 S.kernel);
+        r.status = ev.status;
+        r.w = ev.w;
+        if (ev.status == ST_EXPAND) {
+            r.nch = (uint32_t)__popc(topo_mask(mm.y));
+            r.first = mm.x;
         }
-        uint32_t next = re;
-        for (uint32_t base = rb; base < re; base += 32) {
-            const uint32_t e = base + (uint32_t)lane;
-            int st = ST_DISCARD;
-            double w = 0.0;
-            uint32_t nch = 0, first = 0;
-            if (e < re) {
-                const uint32_t nd = P.node[e];
-                if (nd >= S.num_nodes) {
-                    bad = true;
-                } else {
-                    const double4 rr = ldg4(&S.rec[nd]);
-                    const uint4 mm = __ldg(&S.meta[nd]);
-                    const double md = __ldg(&S.maxdim[nd]);
-                    const Eval ev = evaluate(rr, make_uint2(mm.x, mm.y), md, sx, sy, sz, source, W.theta, S.mu, W.scale, false, S.kernel);
-                    st = ev.status;
-                    w = ev.w;
-                    ++touched;
-                    if (st == ST_EXPAND) {
-                        nch = (uint32_t)__popc(topo_mask(mm.y));
-                        first = mm.x;
-                    }
-                }
-            }
-            const uint32_t inc = warp_inclusive(nch);
-            const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-            if (next + total > A.cap) {
-                return -1;
-            }
-            const uint32_t cs = next + inc - nch;
-            if (e < re) {
-                P.info[e] = (uint32_t)st | (nch << 2);
-                P.child[e] = cs;
-                P.w[e] = w;
-            }
-            for (uint32_t c = 0; c < nch; ++c) {
-                P.node[cs + c] = first + nch - 1u - c;
-            }
-            next += total;
-        }
-        if (__any_sync(0xFFFFFFFFu, bad)) {
-            return -2;
-        }
-        ++rounds;
-        if (lane == 0) {
-            s_round[rounds + 1] = next;
-        }
-        __syncwarp();
-    }
-    // bottom-up: candidates below every entry
-    for (int r = rounds - 1; r >= 0; --r) {
-        const uint32_t rb = s_round[r], re = s_round[r + 1];
-        for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
-            const uint32_t inf = P.info[e];
-            const int st = (int)(inf & 3u);
-            uint32_t n = st == ST_ACCEPT ? 1u : 0u;
-            if (st == ST_EXPAND) {
-                const uint32_t c0 = P.child[e];
-                for (uint32_t c = 0; c < (inf >> 2); ++c) {
-                    n += P.cnt[c0 + c];
-                }
-            }
-            P.cnt[e] = n;
-        }
-        __syncwarp();
-    }
-    // top-down: positions in visiting order; the candidates go to their place
-    uint32_t carry = 0;
-    for (uint32_t base = 0; base < k0; base += 32) {
-        const uint32_t e = base + (uint32_t)lane;
-        const uint32_t n = e < k0 ? P.cnt[e] : 0u;
-        const uint32_t inc = warp_inclusive(n);
-        if (e < k0) {
-            P.pos[e] = carry + inc - n;
-        }
-        carry += __shfl_sync(0xFFFFFFFFu, inc, 31);
-    }
-    __syncwarp();
-    for (int r = 0; r < rounds; ++r) {
-        const uint32_t rb = s_round[r], re = s_round[r + 1];
-        for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
-            const uint32_t inf = P.info[e];
-            const int st = (int)(inf & 3u);
-            const uint32_t p = P.pos[e];
-            if (st == ST_ACCEPT) {
-                P.ord_node[p] = P.node[e];
-                P.ord_w[p] = P.w[e];
-            } else if (st == ST_EXPAND) {
-                const uint32_t c0 = P.child[e];
-                uint32_t acc = p;
-                for (uint32_t c = 0; c < (inf >> 2); ++c) {
-                    P.pos[c0 + c] = acc;
-                    acc += P.cnt[c0 + c];
-                }
-            }
-        }
-        __syncwarp();
-    }
-    return (int64_t)carry;
-}
-
-// The running sum of ord_w[0, F) in order, one FP64 addition after the other
-// (the reference's sum); ord_w[i] becomes the sum up to and including i.
-// Returns the total.
-__device__ double wide_running_sum(double* ord_w, uint32_t F) {
-    const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (uint32_t base = 0; base < F; base += 32) {
-        const uint32_t i = base + (uint32_t)lane;
-        const double v = i < F ? ord_w[i] : 0.0;
-        double mine = 0.0;
-        if (F - base >= 32) {
-#pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                s = s + __shfl_sync(0xFFFFFFFFu, v, q);
-                mine = q == lane ? s : mine;
-            }
-        } else {
-            const uint32_t lim = F - base;
-            for (uint32_t q = 0; q < lim; ++q) {
-                s = s + __shfl_sync(0xFFFFFFFFu, v, (int)q);
-                mine = q == (uint32_t)lane ? s : mine;
-            }
-        }
-        if (i < F) {
-            ord_w[i] = mine;
-        }
-    }
-    __syncwarp();
-    return s;
+        return r;
+    });
 }
 
 // One search (one vacant axon element j of `source`) by the whole warp:
@@ -725,7 +545,7 @@ __device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpN
         if (topo_leaf(sm.y)) {
             return depth == 0 ? -1 : (int32_t)sm.x;
         }
-        const int64_t got = wide_collect(A, P, W, sub, sx, sy, sz, source, s_round, touched);
+        const int64_t got = wide_collect64(A, P, W, sub, sx, sy, sz, source, s_round, touched);
         if (got == -1) {
             return kRedo;
         }
@@ -734,7 +554,7 @@ __device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpN
             return -1;
         }
         const uint32_t F = (uint32_t)got;
-        double total = wide_running_sum(P.ord_w, F);
+        double total = wide_running_sum64(P.ord_w, F);
         if (total == 0.0) {
             // every weight underflowed: count / distance weights over the same candidates
             for (uint32_t i = threadIdx.x & 31; i < F; i += 32) {
@@ -745,21 +565,13 @@ __device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpN
                 P.ord_w[i] = ev.w;
             }
             __syncwarp();
-            total = wide_running_sum(P.ord_w, F);
+            total = wide_running_sum64(P.ord_w, F);
         }
         if (total == 0.0) {
             return -1;  // no candidate: the search fails
         }
         const double r = pick_threshold(total, W.seed, S.step, source - W.first, j, depth);
-        int64_t pick = -1;
-        for (uint32_t base = 0; base < F; base += 32) {
-            const uint32_t i = base + (threadIdx.x & 31);
-            const uint32_t hit = __ballot_sync(0xFFFFFFFFu, i < F && P.ord_w[i] >= r);
-            if (hit) {
-                pick = P.ord_node[base + (uint32_t)(__ffs((int)hit) - 1)];
-                break;
-            }
-        }
+        const int64_t pick = wide_pick(P.ord_w, P.ord_node, F, r);
         if (pick < 0) {
             atomicOr(S.err, (uint32_t)DERR_NO_CROSSING);
             return -1;
@@ -784,8 +596,7 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide(WideArgs A) {
     }
     uint32_t* s_round = s_round_all[wib];
     const SearchArgs& S = A.S;
-    const uint64_t off = (uint64_t)slot * A.cap;
-    const WideSlot P{ A.node + off, A.info + off, A.child + off, A.cnt + off, A.pos + off, A.ord_node + off, A.w + off, A.ord_w + off };
+    const WideSlot P = wide_slot(A.all, (uint64_t)slot * A.cap);
     const uint32_t total_tasks = S.seg_warp[S.num_segs] * 32u;
     uint32_t touched = 0;
     for (;;) {
@@ -797,18 +608,9 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide(WideArgs A) {
         if (task >= total_tasks) {
             break;
         }
-        const uint32_t wg = task >> 5;
-        uint32_t lo = 0, hi = S.num_segs;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (S.seg_warp[mid] <= wg) {
-                lo = mid;
-            } else {
-                hi = mid;
-            }
-        }
-        const uint64_t idx = S.seg_begin[lo] + (uint64_t)(wg - S.seg_warp[lo]) * 32 + (task & 31u);
-        if (idx >= S.seg_end[lo]) {
+        uint32_t lo = 0;
+        uint64_t idx = 0;
+        if (!wide_task_entry(task, S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, lo, idx)) {
             continue;
         }
         const NetInfo& N = S.nets[S.seg_net[lo]];
@@ -949,6 +751,27 @@ __global__ void k_req_scatter(uint64_t m, const uint32_t* __restrict__ list_src,
 
 }  // namespace
 
+// Walk entries per warp of the one-search-per-warp form: a descent evaluates
+// every node at most once, so a small tree never overflows.
+uint32_t wide_cap(const Ctx& c) {
+    return (uint32_t)std::min<uint64_t>(kWideCap, (c.tree.num_nodes + 31) / 32 * 32);
+}
+
+// The scratch of `slots` warps of `cap` entries each (grown as needed).
+WideSlot wide_scratch(Ctx& c, uint32_t slots, uint32_t cap) {
+    Search& S = c.search;
+    const size_t cells = (size_t)slots * cap;
+    S.w_node.ensure(cells);
+    S.w_info.ensure(cells);
+    S.w_child.ensure(cells);
+    S.w_cnt.ensure(cells);
+    S.w_pos.ensure(cells);
+    S.w_ord_node.ensure(cells);
+    S.w_w.ensure(cells);
+    S.w_ord_w.ensure(cells);
+    return WideSlot{ S.w_node.p, S.w_info.p, S.w_child.p, S.w_cnt.p, S.w_pos.p, S.w_ord_node.p, S.w_w.p, S.w_ord_w.p };
+}
+
 // Whether a candidate shape runs on this context: the one-search-per-warp
 // form is written for the FP64 search and pays off on large networks.
 bool search_variant_applies(const Ctx& c, const SearchVariant& v) {
@@ -965,30 +788,14 @@ void launch_wide(Ctx& c, const SearchArgs& a, uint32_t warps, int t, const Searc
     Search& S = c.search;
     cudaStream_t st = c.stream;
     const uint32_t tasks = warps * 32u;
-    const uint32_t cap = (uint32_t)std::min<uint64_t>(kWideCap, (c.tree.num_nodes + 31) / 32 * 32);
+    const uint32_t cap = wide_cap(c);
     const uint32_t slots = std::min<uint32_t>(tasks, (uint32_t)c.num_sms * kWideWarpsPerSM);
-    const size_t cells = (size_t)slots * cap;
-    S.w_node.ensure(cells);
-    S.w_info.ensure(cells);
-    S.w_child.ensure(cells);
-    S.w_cnt.ensure(cells);
-    S.w_pos.ensure(cells);
-    S.w_ord_node.ensure(cells);
-    S.w_w.ensure(cells);
-    S.w_ord_w.ensure(cells);
     S.w_overflow.ensure(2);
     RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p + t, 0, sizeof(uint32_t), st));
     RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p + t, 0, sizeof(uint32_t), st));
     WideArgs A;
     A.S = a;
-    A.node = S.w_node.p;
-    A.info = S.w_info.p;
-    A.child = S.w_child.p;
-    A.cnt = S.w_cnt.p;
-    A.pos = S.w_pos.p;
-    A.w = S.w_w.p;
-    A.ord_w = S.w_ord_w.p;
-    A.ord_node = S.w_ord_node.p;
+    A.all = wide_scratch(c, slots, cap);
     A.cap = cap;
     A.slots = slots;
     A.tasks = S.tasks.p + t;

@@ -265,6 +265,9 @@ struct Tuning {
 
 const std::vector<SearchVariant>& search_variants();
 bool search_variant_applies(const Ctx& c, const SearchVariant& v);
+struct WideSlot;
+uint32_t wide_cap(const Ctx& c);
+WideSlot wide_scratch(Ctx& c, uint32_t slots, uint32_t cap);
 // one-search-per-warp form: walk entries per warp, warps per SM, smallest network
 constexpr uint32_t kWideCap = 6144;
 constexpr uint32_t kWideWarpsPerSM = 8;

@@ -34,6 +34,7 @@
 #include <stdint.h>
 #include <math.h>
 
+
 #if defined(__CUDACC__)
 #define RL_HD __host__ __device__ __forceinline__
 #else
@@ -244,6 +245,22 @@ static __device__ const double2 rl_exp_table_dev[64] = { RL_EXP_TABLE_INIT };
 #endif
 static const double rl_exp_table_host[64][2] = { RL_EXP_TABLE_INIT };
 
+// exp's constants: the Taylor coefficients 1/720, 1/120, 1/24, 1/6, 1/2,
+// 64 / ln 2 and ln 2 / 64 as hi + lo (device: constant memory, as the normal
+// quantile's coefficients).
+#define RL_EXP_CONST_INIT \
+    { 1.3888888888888889e-03, 8.3333333333333332e-03, 4.1666666666666664e-02, 1.6666666666666666e-01, 0.5, 92.332482616893656768, \
+      RL_LN2_HI / 64.0, RL_LN2_LO / 64.0 }
+#if defined(__CUDACC__)
+static __constant__ double rl_exp_const_dev[8] = RL_EXP_CONST_INIT;
+#endif
+static const double rl_exp_const_host[8] = RL_EXP_CONST_INIT;
+#if defined(__CUDA_ARCH__)
+#define RL_EXPC(k) rl_exp_const_dev[k]
+#else
+#define RL_EXPC(k) rl_exp_const_host[k]
+#endif
+
 // exp(x) by Tang's table-driven method (P. T. P. Tang, "Table-driven
 // implementation of the exponential function in IEEE floating-point
 // arithmetic", ACM TOMS 15(2), 1989, 144-157): x = (64 m + j) ln2/64 + r with
@@ -261,17 +278,17 @@ RL_HD double rl_exp(double x) {
     if (x < -745.1332191019412) {
         return 0.0;
     }
-    const double kd = floor(x * 92.332482616893656768 + 0.5);  // 64 / ln 2
+    const double kd = floor(x * RL_EXPC(5) + 0.5);  // 64 / ln 2
     // kd * (RL_LN2_HI / 64) is exact; so is the subtraction (Sterbenz, or kd = 0)
-    const double r = rl_fma(-kd, RL_LN2_LO / 64.0, x - kd * (RL_LN2_HI / 64.0));
+    const double r = rl_fma(-kd, RL_EXPC(7), x - kd * RL_EXPC(6));
     const int ki = (int)kd;
     const int j = ki & 63;
     const int m = ki >> 6;  // floor(ki / 64)
     // exp(r) - 1 = r + r^2 (1/2 + r/6 + r^2/24 + r^3/120 + r^4/720)
-    double p = rl_fma(1.3888888888888889e-03, r, 8.3333333333333332e-03);  // 1/720, 1/120
-    p = rl_fma(p, r, 4.1666666666666664e-02);                              // 1/24
-    p = rl_fma(p, r, 1.6666666666666666e-01);                              // 1/6
-    p = rl_fma(p, r, 0.5);
+    double p = rl_fma(RL_EXPC(0), r, RL_EXPC(1));  // 1/720, 1/120
+    p = rl_fma(p, r, RL_EXPC(2));  // 1/24
+    p = rl_fma(p, r, RL_EXPC(3));  // 1/6
+    p = rl_fma(p, r, RL_EXPC(4));
     p = rl_fma(r * r, p, r);
 #if defined(__CUDA_ARCH__)
     const double2 t = __ldg(&rl_exp_table_dev[j]);
@@ -300,15 +317,15 @@ RL_HD double rl_exp_flat(double x) {
 #else
     const double xc = x != x ? 0.0 : fmin(fmax(x, -746.0), 710.0);
 #endif
-    const double kd = floor(xc * 92.332482616893656768 + 0.5);  // 64 / ln 2
-    const double r = rl_fma(-kd, RL_LN2_LO / 64.0, xc - kd * (RL_LN2_HI / 64.0));
+    const double kd = floor(xc * RL_EXPC(5) + 0.5);  // 64 / ln 2
+    const double r = rl_fma(-kd, RL_EXPC(7), xc - kd * RL_EXPC(6));
     const int ki = (int)kd;
     const int j = ki & 63;
     const int m = ki >> 6;
-    double p = rl_fma(1.3888888888888889e-03, r, 8.3333333333333332e-03);
-    p = rl_fma(p, r, 4.1666666666666664e-02);
-    p = rl_fma(p, r, 1.6666666666666666e-01);
-    p = rl_fma(p, r, 0.5);
+    double p = rl_fma(RL_EXPC(0), r, RL_EXPC(1));
+    p = rl_fma(p, r, RL_EXPC(2));
+    p = rl_fma(p, r, RL_EXPC(3));
+    p = rl_fma(p, r, RL_EXPC(4));
     p = rl_fma(r * r, p, r);
 #if defined(__CUDA_ARCH__)
     const double2 t = __ldg(&rl_exp_table_dev[j]);
@@ -325,6 +342,38 @@ RL_HD double rl_exp_flat(double x) {
     b = b < -1022 ? -1022 : (b > 1023 ? 1023 : b);
     const double v = (y * as_f64((uint64_t)(a + 1023) << 52)) * as_f64((uint64_t)(b + 1023) << 52);
     return x != x ? x : (x > 709.782712893384 ? as_f64(0x7FF0000000000000ull) : (x < -745.1332191019412 ? 0.0 : v));
+}
+
+// rl_exp_flat for x <= 0 and NaN (the growth curves' exp(-q^2)): the same
+// bits as rl_exp there, without the overflow case (m <= 0 for x <= 0).
+RL_HD double rl_exp_flat_nonpos(double x) {
+#if defined(__CUDA_ARCH__)
+    const double xc = x;
+#else
+    const double xc = x != x ? 0.0 : fmin(fmax(x, -746.0), 0.0);
+#endif
+    const double kd = floor(xc * RL_EXPC(5) + 0.5);  // 64 / ln 2
+    const double r = rl_fma(-kd, RL_EXPC(7), xc - kd * RL_EXPC(6));
+    const int ki = (int)kd;
+    const int j = ki & 63;
+    const int m = ki >> 6;
+    double p = rl_fma(RL_EXPC(0), r, RL_EXPC(1));
+    p = rl_fma(p, r, RL_EXPC(2));
+    p = rl_fma(p, r, RL_EXPC(3));
+    p = rl_fma(p, r, RL_EXPC(4));
+    p = rl_fma(r * r, p, r);
+#if defined(__CUDA_ARCH__)
+    const double2 t = __ldg(&rl_exp_table_dev[j]);
+    const double t_hi = t.x, t_lo = t.y;
+#else
+    const double t_hi = rl_exp_table_host[j][0], t_lo = rl_exp_table_host[j][1];
+#endif
+    const double y = t_hi + rl_fma(t_hi, p, t_lo);
+    const bool low = m < -1021;
+    int a = low ? m + 54 : m;
+    a = a < -1022 ? -1022 : a;  // only arguments below the underflow reach the clamp
+    const double v = (y * as_f64((uint64_t)(a + 1023) << 52)) * as_f64((uint64_t)((low ? -54 : 0) + 1023) << 52);
+    return x != x ? x : (x < -745.1332191019412 ? 0.0 : v);
 }
 
 // log(x) for finite x > 0 (normal range): x = m 2^e with m in
@@ -444,28 +493,39 @@ RL_HD bool normal_in_tail(double p) {
     return !(fabs(p - 0.5) <= 0.425);
 }
 
+// The central piece's coefficients, highest power first (numerator, then
+// denominator).  On the device they sit in constant memory, where a fused
+// multiply-add reads them as an operand (no instructions to materialise the
+// 64-bit literals in registers); the host reads the same values.
+#define RL_AS241_CENTRAL_INIT                                                                                                 \
+    { 2.5090809287301226727e+3, 3.3430575583588128105e+4, 6.7265770927008700853e+4, 4.5921953931549871457e+4,              \
+      1.3731693765509461125e+4, 1.9715909503065514427e+3, 1.3314166789178437745e+2, 3.3871328727963666080e+0,              \
+      5.2264952788528545610e+3, 2.8729085735721942674e+4, 3.9307895800092710610e+4, 2.1213794301586595867e+4,              \
+      5.3941960214247511077e+3, 6.8718700749205790830e+2, 4.2313330701600911252e+1, 1.0 }
+#if defined(__CUDACC__)
+static __constant__ double rl_as241_central_dev[16] = RL_AS241_CENTRAL_INIT;
+#endif
+static const double rl_as241_central_host[16] = RL_AS241_CENTRAL_INIT;
+#if defined(__CUDA_ARCH__)
+#define RL_AS241_C(k) rl_as241_central_dev[k]
+#else
+#define RL_AS241_C(k) rl_as241_central_host[k]
+#endif
+
 RL_HD double normal_quantile_central(double p) {
     const double q = p - 0.5;
-    {
-        const double r = 0.180625 - q * q;
-        double num = 2.5090809287301226727e+3;
-        num = rl_fma(num, r, 3.3430575583588128105e+4);
-        num = rl_fma(num, r, 6.7265770927008700853e+4);
-        num = rl_fma(num, r, 4.5921953931549871457e+4);
-        num = rl_fma(num, r, 1.3731693765509461125e+4);
-        num = rl_fma(num, r, 1.9715909503065514427e+3);
-        num = rl_fma(num, r, 1.3314166789178437745e+2);
-        num = rl_fma(num, r, 3.3871328727963666080e+0);
-        double den = 5.2264952788528545610e+3;
-        den = rl_fma(den, r, 2.8729085735721942674e+4);
-        den = rl_fma(den, r, 3.9307895800092710610e+4);
-        den = rl_fma(den, r, 2.1213794301586595867e+4);
-        den = rl_fma(den, r, 5.3941960214247511077e+3);
-        den = rl_fma(den, r, 6.8718700749205790830e+2);
-        den = rl_fma(den, r, 4.2313330701600911252e+1);
-        den = rl_fma(den, r, 1.0);
-        return (num * q) / den;
+    const double r = 0.180625 - q * q;
+    double num = RL_AS241_C(0);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) {
+        num = rl_fma(num, r, RL_AS241_C(k));
     }
+    double den = RL_AS241_C(8);
+#pragma unroll
+    for (int k = 9; k < 16; ++k) {
+        den = rl_fma(den, r, RL_AS241_C(k));
+    }
+    return (num * q) / den;
 }
 
 RL_HD double normal_quantile_tail(double p) {

@@ -6,6 +6,7 @@
 extern "C" {
 double probe_exp(double x) { return rl::rl_exp(x); }
 double probe_exp_flat(double x) { return rl::rl_exp_flat(x); }
+double probe_exp_flat_nonpos(double x) { return rl::rl_exp_flat_nonpos(x); }
 double probe_log(double x) { return rl::rl_log(x); }
 double probe_hypot3(double x, double y, double z) { return rl::rl_hypot3(x, y, z); }
 // libstdc++'s own three-argument std::hypot, which the reference calls

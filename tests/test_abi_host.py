@@ -106,7 +106,7 @@ def probe(tmp_path_factory):
     subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(so),
                     os.path.join(ROOT, "tests", "helpers", "math_probe.cpp")], check=True)
     L = C.CDLL(str(so))
-    for name in ("probe_exp", "probe_exp_flat", "probe_log", "probe_quantile", "probe_next_up"):
+    for name in ("probe_exp", "probe_exp_flat", "probe_exp_flat_nonpos", "probe_log", "probe_quantile", "probe_next_up"):
         getattr(L, name).restype = C.c_double
         getattr(L, name).argtypes = [C.c_double]
     for name in ("probe_hypot3", "probe_std_hypot3"):
@@ -159,6 +159,11 @@ def test_branch_free_exp_equals_exp(probe):
         a, b = probe.probe_exp(float(x)), probe.probe_exp_flat(float(x))
         assert np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64), (x, a, b)
     assert np.isnan(probe.probe_exp_flat(float("nan")))
+    # the form for arguments <= 0 (the growth curves' exp(-q^2))
+    for x in xs[xs <= 0]:
+        a, b = probe.probe_exp(float(x)), probe.probe_exp_flat_nonpos(float(x))
+        assert np.float64(a).view(np.uint64) == np.float64(b).view(np.uint64), (x, a, b)
+    assert np.isnan(probe.probe_exp_flat_nonpos(float("nan")))
 
 
 @pytest.mark.parametrize("kernel", [(1, 2.0, 400.0, 0.0), (1, 1.0, 300.0, 0.0), (2, 1.0, 1.0, 1500.0), (2, 1.0, 1.0, float("inf")),
