@@ -411,7 +411,7 @@ typedef struct rl_tuning {
     int32_t search_warps;    /* 2, 4 or 8 */
     int32_t search_hot;      /* 0, or 1024 / 4096 top octree nodes in shared memory (search_warps 32) */
     int32_t search_packet;   /* 32, 16, 4 or 1 searches of Morton-adjacent sources walking the first descent together;
-                                0: one search per warp (FP64 form, networks of 65,536 neurons or more; search_warps 4) */
+                                0: one search per warp (search_warps 4; the tuner times it on networks of 65,536 neurons or more) */
     int32_t search_cap;      /* 1: registers capped at 64 (more resident warps), 0: as compiled */
     int32_t act_block;       /* 128, 256 or 512 */
     int32_t act_persistent;  /* 0 or 1 */
@@ -423,7 +423,7 @@ typedef struct rl_tuning {
  * search: cap 0 then 1, packet 32, 16, 4, 1, warps 2, 4, 8 (24 shapes), then the
  * persistent form with 1024 and 4096 nodes in shared memory, packet 32 then 16
  * (4 shapes, 32 warps, registers capped at 64), then one search per warp
- * (packet 0, 4 warps per block; FP64 contexts of 65,536 neurons or more, 0 ms
+ * (packet 0, 4 warps per block; timed on networks of 65,536 neurons or more, 0 ms
  * elsewhere); the search shape is tuned per
  * density class of the search list (searches per neuron above 1/4, 1/32,
  * 1/256, or below), since sparse lists favour narrow packets;

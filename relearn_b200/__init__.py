@@ -138,7 +138,7 @@ NUM_SEARCH_SHAPES, NUM_ACT_SHAPES = 29, 18
 # (warps, packet, cap, hot), timing order: plain shapes, then the persistent form
 # with the top octree nodes in shared memory
 SEARCH_SHAPES = ([(w, p, c, 0) for c in (0, 1) for p in (32, 16, 4, 1) for w in (2, 4, 8)] + [(32, p, 1, h) for h in (1024, 4096) for p in (32, 16)]
-                 + [(4, 0, 0, 0)])  # packet 0: one search per warp (FP64)
+                 + [(4, 0, 0, 0)])  # packet 0: one search per warp
 ACT_SHAPES = [(b, p, v) for p in (0, 1) for b in (128, 256, 512) for v in (1, 2, 4)]  # (block, persistent, neurons per thread)
 
 

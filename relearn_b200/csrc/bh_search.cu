@@ -772,10 +772,10 @@ WideSlot wide_scratch(Ctx& c, uint32_t slots, uint32_t cap) {
     return WideSlot{ S.w_node.p, S.w_info.p, S.w_child.p, S.w_cnt.p, S.w_pos.p, S.w_ord_node.p, S.w_w.p, S.w_ord_w.p };
 }
 
-// Whether a candidate shape runs on this context: the one-search-per-warp
-// form is written for the FP64 search and pays off on large networks.
+// Whether the tuner times a candidate shape on this context: the
+// one-search-per-warp form pays off on large networks only.
 bool search_variant_applies(const Ctx& c, const SearchVariant& v) {
-    return v.packet != 0 || (!is_fp32(c) && c.n >= kWideMinNeurons);
+    return v.packet != 0 || c.n >= kWideMinNeurons;
 }
 
 namespace {

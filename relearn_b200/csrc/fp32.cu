@@ -23,6 +23,7 @@
 // --precision-report): selection probabilities, calcium drift, distances of
 // formed synapses.
 #include "bh_eval.cuh"
+#include "bh_wide.cuh"
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
@@ -1068,6 +1069,126 @@ __global__ void __launch_bounds__(1024, 1) k_search_f32_hot(Search32 A, uint32_t
     }
 }
 
+// One search per warp (bh_wide.cuh) in the FP32 form: the same visiting
+// order and the same Kahan sums as the packet kernels, so the same targets.
+struct WideArgs32 {
+    Search32 S;
+    WideSlot all;
+    uint32_t cap;
+    uint32_t slots;
+    uint32_t* tasks;
+    uint32_t* overflow;
+};
+
+__device__ int32_t wide_search32(const WideArgs32& A, const WideSlot& P, const Net32& W, const QPos& sp, uint32_t source, uint32_t j,
+                                 uint32_t* s_round) {
+    const Search32& S = A.S;
+    uint32_t touched = 0;
+    uint32_t sub = W.root;
+    for (uint32_t depth = 0; depth <= (uint32_t)kMaxLevels + 2u; ++depth) {
+        const uint4 sm = S.meta[sub];
+        if (topo_leaf(sm.y)) {
+            return depth == 0 ? -1 : (int32_t)sm.x;
+        }
+        auto collect = [&](bool fb) {
+            return wide_collect(P, A.cap, sm.x, inner_children32(sm), s_round, touched, [&](uint32_t nd) {
+                WideEval r{ S_DISCARD, 0.0, 0u, 0u, false };
+                if (nd >= S.num_nodes) {
+                    r.bad = true;
+                    return r;
+                }
+                const uint4 mm = S.meta[nd];
+                const E32 e = eval32(S.rec[nd], mtopo(mm), mmaxdim(mm), sp, source, S, W, fb);
+                r.status = e.status;
+                r.w = (double)e.w;
+                if (e.status == S_EXPAND) {
+                    r.nch = (uint32_t)__popc(topo_mask(mm.y));
+                    r.first = mm.x;
+                }
+                return r;
+            });
+        };
+        int64_t got = collect(false);
+        if (got == -1) {
+            return kRedo;
+        }
+        if (got < 0) {
+            atomicOr(S.err, (uint32_t)DERR_WALK);
+            return -1;
+        }
+        float total = wide_running_sum32(P.ord_w, (uint32_t)got);
+        if (total == 0.0f) {
+            // every weight underflowed: count / distance weights (the same walk)
+            __syncwarp();
+            got = collect(true);
+            if (got < 0) {
+                return got == -1 ? kRedo : -1;
+            }
+            total = wide_running_sum32(P.ord_w, (uint32_t)got);
+        }
+        if (total == 0.0f) {
+            return -1;
+        }
+        const float r = threshold32(total, S, W, source, j, depth);
+        const int64_t pick = wide_pick(P.ord_w, P.ord_node, (uint32_t)got, (double)r);
+        if (pick < 0) {
+            return -1;  // rounding left the crossing past the last candidate: no pick
+        }
+        sub = (uint32_t)pick;
+        __syncwarp();
+    }
+    atomicOr(S.err, (uint32_t)DERR_STACK);
+    return -1;
+}
+
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32, 2) k_search_wide32(WideArgs32 A) {
+    __shared__ uint32_t s_round_all[WPB][kWideRounds + 1];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * WPB + (uint32_t)wib;
+    if (slot >= A.slots) {
+        return;  // whole warp
+    }
+    const Search32& S = A.S;
+    const uint64_t off = (uint64_t)slot * A.cap;
+    const WideSlot P{ A.all.node + off, A.all.info + off, A.all.child + off, A.all.cnt + off, A.all.pos + off, A.all.ord_node + off, A.all.w + off,
+                      A.all.ord_w + off };
+    const uint32_t total_tasks = S.seg_warp[S.num_segs] * 32u;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) {
+            task = atomicAdd(A.tasks, 1u);
+        }
+        task = __shfl_sync(0xFFFFFFFFu, task, 0);
+        if (task >= total_tasks) {
+            break;
+        }
+        uint32_t seg = 0;
+        uint64_t idx = 0;
+        if (!wide_task_entry(task, S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, seg, idx)) {
+            continue;
+        }
+        const NetInfo& N = S.nets[S.seg_net[seg]];
+        const Net32 W{ N.theta32, N.inv_sigma2_32, N.seed, S.seg_net[seg], N.first, N.frame.quantum };
+        int32_t result = -1;
+        if (!N.root_leaf) {
+            const uint32_t source = S.list_src[idx];
+            const QFrame& F = N.frame;
+            const QPos sp{ quantize(S.px[source], F.origin[0], F.inv_quantum), quantize(S.py[source], F.origin[1], F.inv_quantum),
+                           quantize(S.pz[source], F.origin[2], F.inv_quantum) };
+            result = wide_search32(A, P, W, sp, source, S.list_j[idx], s_round_all[wib]);
+        }
+        if (lane == 0) {
+            S.target[idx] = result;
+            if (result == kRedo) {
+                atomicAdd(A.overflow, 1u);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 using Search32Kernel = void (*)(Search32);
 
 Search32Kernel fp32_search_kernel(const SearchVariant& v) {
@@ -1420,6 +1541,28 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
         RL_CUDA_TRY(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned blocks = std::min<unsigned>((unsigned)c.num_sms, (warps + 31) / 32);
         kern<<<blocks, 1024, smem, c.stream>>>(A, hot);
+        RL_LAUNCH_CHECK();
+        return;
+    }
+    if (v.packet == 0) {
+        // one search per warp; searches that did not fit are redone by the packet kernel
+        constexpr int WPB = 4;
+        Search& S = c.search;
+        const uint32_t cap = wide_cap(c);
+        const uint32_t slots = std::min<uint32_t>(warps * 32u, (uint32_t)c.num_sms * kWideWarpsPerSM);
+        S.w_overflow.ensure(2);
+        RL_CUDA_TRY(cudaMemsetAsync(tasks, 0, sizeof(uint32_t), c.stream));
+        RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p + type, 0, sizeof(uint32_t), c.stream));
+        WideArgs32 W{ A, wide_scratch(c, slots, cap), cap, slots, tasks, S.w_overflow.p + type };
+        k_search_wide32<WPB><<<(slots + WPB - 1) / WPB, WPB * 32, 0, c.stream>>>(W);
+        RL_LAUNCH_CHECK();
+        uint32_t over = 0;
+        RL_CUDA_TRY(cudaMemcpyAsync(&over, S.w_overflow.p + type, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        if (!over) {
+            return;
+        }
+        k_search_f32<2, 32, 1><<<(warps + 1) / 2, 64, 0, c.stream>>>(A);
         RL_LAUNCH_CHECK();
         return;
     }

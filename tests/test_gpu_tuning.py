@@ -29,8 +29,6 @@ def test_every_search_shape_finds_the_same_targets(precision):
     net.prepare_update_connectivity(one, one, one)
     ref = None
     for w, p, cp, hot in SEARCH_SHAPES:
-        if p == 0 and precision == 1:
-            continue  # one search per warp is a shape of the FP64 search
         net.set_tuning(search_warps=w, search_packet=p, search_cap=cp, search_hot=hot)
         req = net.find_targets(100)
         if ref is None:
@@ -119,8 +117,6 @@ def test_every_search_shape_on_a_forest(precision):
     ens.prepare_update_connectivity(one, one, one)
     ref = None
     for w, p, cp, hot in SEARCH_SHAPES:
-        if p == 0 and precision == 1:
-            continue
         ens.set_tuning(search_warps=w, search_packet=p, search_cap=cp, search_hot=hot)
         req = ens.find_targets(100)
         if ref is None:
@@ -128,3 +124,24 @@ def test_every_search_shape_on_a_forest(precision):
         else:
             assert np.array_equal(req, ref), (w, p, cp, hot)
     assert len(ref) > 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_one_search_per_warp_on_a_sparse_list(precision):
+    """The one-search-per-warp kernel gives the packet kernel's targets on the
+    lists it is for: a few hundred sources spread over a large network, with
+    1-3 vacant axons each."""
+    n = 100000
+    net = make(n, 4600.0, 33, precision)
+    rng = np.random.default_rng(5)
+    va = np.zeros(n, np.uint32)
+    va[rng.choice(n, 900, replace=False)] = rng.integers(1, 4, 900).astype(np.uint32)
+    ve = rng.integers(0, 3, n).astype(np.uint32)
+    vi = rng.integers(0, 3, n).astype(np.uint32)
+    net.prepare_update_connectivity(va, ve, vi)
+    got = []
+    for shape in ((2, 32, 1, 0), (4, 0, 0, 0)):
+        net.set_tuning(search_warps=shape[0], search_packet=shape[1], search_cap=shape[2], search_hot=shape[3])
+        got.append(net.find_targets(300))
+    assert len(got[0]) > 1000
+    assert np.array_equal(got[0], got[1])
