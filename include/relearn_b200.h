@@ -404,7 +404,8 @@ RL_API rl_status rl_get_phase_times(void* ctx, double* ms, uint64_t* counts);
  * per SM taking warp tasks from a counter) that first copies up to
  * `search_hot` nodes of the top octree levels into shared memory;
  * the activity kernel runs `act_block` threads per block with `act_vec`
- * neurons per thread (vector loads and stores; the FP64 form runs 1), and with
+ * neurons per thread (FP32: vector loads and stores; FP64: 1, or 2 whose
+ * steps the compiler interleaves), and with
  * `act_persistent` one resident wave of blocks strides over the neurons.  No
  * counterpart in the reference (its CPU loops have no launch shape). */
 typedef struct rl_tuning {
@@ -415,7 +416,7 @@ typedef struct rl_tuning {
     int32_t search_cap;      /* 1: registers capped at 64 (more resident warps), 0: as compiled */
     int32_t act_block;       /* 128, 256 or 512 */
     int32_t act_persistent;  /* 0 or 1 */
-    int32_t act_vec;         /* 1, 2 or 4 */
+    int32_t act_vec;         /* 1, 2 or 4 (FP64: 1 or 2) */
     int32_t tuned;           /* bit 0: search shape timed or recalled, bit 1: activity shape */
 } rl_tuning;
 

@@ -374,11 +374,11 @@ __device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t 
 // The same function as the per-lane evaluation, so the same bits.  The loop
 // over a block's neurons has the same trip count in every thread (the block
 // synchronises inside it).
-template <int BLOCK, int H, int MODEL, bool MULTI>
+template <int BLOCK, int H, int MODEL, bool MULTI, int V>
 __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __restrict__ D, uint32_t k) {
-    __shared__ double s_p[BLOCK];
-    __shared__ double s_z[BLOCK];
-    __shared__ uint16_t s_who[BLOCK];
+    __shared__ double s_p[V * BLOCK];
+    __shared__ double s_z[V * BLOCK];
+    __shared__ uint16_t s_who[V * BLOCK];
     __shared__ uint32_t s_cnt[2];
     pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t step = D->base_step + k;
@@ -387,44 +387,57 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
         s_cnt[threadIdx.x] = 0u;
     }
     __syncthreads();
-    const uint32_t stride = gridDim.x * BLOCK;
+    const uint32_t stride = gridDim.x * V * BLOCK;
     uint32_t parity = 0;
-    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride, parity ^= 1u) {
-        const uint32_t i = base + threadIdx.x;
-        const bool on = i < A.n && A.enabled[i];
-        uint64_t seed = 0;
-        uint32_t local = 0;
-        const double* nu = nullptr;
-        double p = 0.5;
-        double xv = 0.0, uv = 0.0, cav = 0.0, tg = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0;
-        long long isum = 0;
-        if (i < A.n) {
-            d0 = A.delta0[i];
-            d1 = A.delta1[i];
-            d2 = A.delta2[i];
+    for (uint32_t base = blockIdx.x * V * BLOCK; base < A.n; base += stride, parity ^= 1u) {
+        uint32_t i[V];
+        bool on[V], tail[V];
+        uint64_t seed[V];
+        uint32_t local[V];
+        const double* nu[V];
+        double p[V], z[V], xv[V], uv[V], cav[V], tg[V], d0[V], d1[V], d2[V];
+        long long isum[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            i[v] = base + (uint32_t)v * BLOCK + threadIdx.x;
+            on[v] = i[v] < A.n && A.enabled[i[v]];
+            seed[v] = 0;
+            local[v] = 0;
+            nu[v] = nullptr;
+            p[v] = 0.5;
+            xv[v] = uv[v] = cav[v] = tg[v] = d0[v] = d1[v] = d2[v] = 0.0;
+            isum[v] = 0;
+            if (i[v] < A.n) {
+                d0[v] = A.delta0[i[v]];
+                d1[v] = A.delta1[i[v]];
+                d2[v] = A.delta2[i[v]];
+            }
+            if (on[v]) {
+                xv[v] = A.x[i[v]];
+                uv[v] = A.u[i[v]];
+                cav[v] = A.calcium[i[v]];
+                tg[v] = A.uniform_target ? 0.0 : A.target[i[v]];
+                isum[v] = synaptic_sum(A, D, i[v]);
+                neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
+                p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
+            }
         }
-        if (on) {
-            xv = A.x[i];
-            uv = A.u[i];
-            cav = A.calcium[i];
-            tg = A.uniform_target ? 0.0 : A.target[i];
-            isum = synaptic_sum(A, D, i);
-            neuron_net<MULTI>(A, i, seed, local, nu);
-            p = MULTI ? noise_uniform(seed, step, local) : noise_uniform_rk(A.rk0, A.rk1, step, local);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            tail[v] = on[v] && normal_in_tail(p[v]);
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail[v]);
+            uint32_t first = 0;
+            if (lane == 0 && mask) {
+                first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
+            }
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            if (tail[v]) {
+                const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+                s_p[slot] = p[v];
+                s_who[slot] = (uint16_t)(v * BLOCK + threadIdx.x);
+            }
+            z[v] = on[v] && !tail[v] ? normal_quantile_central(p[v]) : 0.0;
         }
-        const bool tail = on && normal_in_tail(p);
-        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
-        uint32_t first = 0;
-        if (lane == 0 && mask) {
-            first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
-        }
-        first = __shfl_sync(0xFFFFFFFFu, first, 0);
-        if (tail) {
-            const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-            s_p[slot] = p;
-            s_who[slot] = (uint16_t)threadIdx.x;
-        }
-        double z = on && !tail ? normal_quantile_central(p) : 0.0;
         __syncthreads();
         const uint32_t cnt = s_cnt[parity];
         for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
@@ -434,19 +447,60 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             s_cnt[parity ^ 1u] = 0u;  // the next round's counter; nobody reads it before the barrier below
         }
         __syncthreads();
-        if (tail) {
-            z = s_z[threadIdx.x];
-        }
-        if (on) {
-            activity_neuron_regs<H, MODEL>(A, step, i, seed, local, nu, z, isum, xv, uv, cav, tg, d0, d1, d2);
-        } else if (i < A.n) {
-            if (A.input) {
-                A.input[i] = 0.0;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (tail[v]) {
+                z[v] = s_z[v * BLOCK + threadIdx.x];
             }
-            A.fired_cur[i] = A.fired_prev[i];
-            A.delta0[i] = d0 + 0.0;
-            A.delta1[i] = d1 + 0.0;
-            A.delta2[i] = d2 + 0.0;
+        }
+        bool done = false;
+        if constexpr (V == 2 && MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
+            if (A.uniform_target) {
+                // both neurons' steps in one stretch without branches, so that
+                // the compiler interleaves their chains of FP64 operations
+                double in[V];
+                uint8_t sp[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    in[v] = step_input(A, isum[v], z[v]);
+                    sp[v] = izhikevich_frozen<H>(A, in[v], xv[v], uv[v]);
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    calcium_growth_flat<H>(A, sp[v], on[v] ? nu[v] : A.nu1, cav[v], d0[v], d1[v], d2[v]);
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    if (on[v]) {
+                        if (A.input) {
+                            A.input[i[v]] = in[v];
+                        }
+                        A.x[i[v]] = xv[v];
+                        A.u[i[v]] = uv[v];
+                        A.fired_cur[i[v]] = sp[v];
+                        A.calcium[i[v]] = cav[v];
+                        A.delta0[i[v]] = d0[v];
+                        A.delta1[i[v]] = d1[v];
+                        A.delta2[i[v]] = d2[v];
+                    }
+                }
+                done = true;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (on[v] && !done) {
+                activity_neuron_regs<H, MODEL>(A, step, i[v], seed[v], local[v], nu[v], z[v], isum[v], xv[v], uv[v], cav[v], tg[v], d0[v], d1[v],
+                                               d2[v]);
+            } else if (!on[v] && i[v] < A.n) {
+                if (A.input) {
+                    A.input[i[v]] = 0.0;
+                }
+                A.fired_cur[i[v]] = A.fired_prev[i[v]];
+                A.delta0[i[v]] = d0[v] + 0.0;
+                A.delta1[i[v]] = d1[v] + 0.0;
+                A.delta2[i[v]] = d2[v] + 0.0;
+            }
         }
     }
 }
@@ -699,14 +753,24 @@ void launch_vacant_axon_count(Ctx& c, unsigned long long* out) {
     RL_LAUNCH_CHECK();
 }
 
-template <int BLOCK, int H, int MODEL>
-void launch_act64_b(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+template <int BLOCK, int H, int MODEL, int V>
+void launch_act64_v(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
     if (c.multi()) {
-        launch_pdl(&k_activity<BLOCK, H, MODEL, true>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, true>), BLOCK, c.stream, A,
+        launch_pdl(&k_activity<BLOCK, H, MODEL, true, V>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, true, V>), BLOCK, c.stream, A,
                    (const ActDesc*)c.act_desc.p, kstep);
     } else {
-        launch_pdl(&k_activity<BLOCK, H, MODEL, false>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, false>), BLOCK, c.stream, A,
+        launch_pdl(&k_activity<BLOCK, H, MODEL, false, V>, act_grid(c, v, (const void*)&k_activity<BLOCK, H, MODEL, false, V>), BLOCK, c.stream, A,
                    (const ActDesc*)c.act_desc.p, kstep);
+    }
+}
+
+// One or two neurons per thread (rows i and i + BLOCK of a block's range).
+template <int BLOCK, int H, int MODEL>
+void launch_act64_b(Ctx& c, const ActVariant& v, const ActArgs& A, uint32_t kstep) {
+    if (v.vec == 2) {
+        launch_act64_v<BLOCK, H, MODEL, 2>(c, v, A, kstep);
+    } else {
+        launch_act64_v<BLOCK, H, MODEL, 1>(c, v, A, kstep);
     }
 }
 
@@ -940,8 +1004,8 @@ void tune_activity(Ctx& c) {
     float best = 1e30f;
     ActVariant pick = c.tune.act;
     for (const ActVariant& v : act_variants()) {
-        if (!is_fp32(c) && v.vec != 1) {
-            c.tune.act_ms.push_back(0.0f);  // the FP64 kernel runs one neuron per thread
+        if (!is_fp32(c) && v.vec > 2) {
+            c.tune.act_ms.push_back(0.0f);  // the FP64 kernel runs one or two neurons per thread
             continue;
         }
         launch_step(c, 0, v);

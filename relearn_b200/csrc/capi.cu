@@ -435,7 +435,7 @@ void plasticity_update(Ctx& c, uint32_t step) {
         PhaseScope ps(c, PH_CONNECTOR);
         run_connector(c, step);
     }
-    if (c.graph.num_new > 0) {
+    if (c.graph.num_new > 0 || c.graph.zeros) {
         PhaseScope ps(c, PH_GRAPH);
         rebuild_graph(c);
     }
@@ -1321,7 +1321,7 @@ rl_status rl_set_tuning(void* ctx, const rl_tuning* t) {
             a_ok = a_ok || (v.block == t->act_block && v.persistent == t->act_persistent && v.vec == t->act_vec);
         }
         RL_CHECK(s_ok && a_ok, RL_ERR_INVALID, "not a candidate shape");
-        RL_CHECK(rl::is_fp32(c) || t->act_vec == 1, RL_ERR_INVALID, "the FP64 activity kernel runs one neuron per thread");
+        RL_CHECK(rl::is_fp32(c) || t->act_vec <= 2, RL_ERR_INVALID, "the FP64 activity kernel runs one or two neurons per thread");
         c.tune.search = rl::SearchVariant{ t->search_warps, t->search_packet, t->search_cap, t->search_hot };
         c.tune.act = rl::ActVariant{ t->act_block, t->act_persistent, t->act_vec };
         c.tune.search_state = rl::TUNE_OFF;

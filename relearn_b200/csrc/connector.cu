@@ -428,9 +428,37 @@ void finish_graph(Ctx& c, uint64_t m) {
 
 }  // namespace
 
+// Drops the entries of weight 0 that deletions left (order kept); returns
+// the new entry count.
+uint64_t drop_zero_weights(Ctx& c, uint64_t m) {
+    Graph& G = c.graph;
+    cudaStream_t st = c.stream;
+    DBuf<uint32_t> keep, pos, t2, s2;
+    DBuf<int32_t> w2;
+    keep.alloc(m);
+    pos.alloc(m);
+    k_keep_flags<<<blocks_for(m, 256), 256, 0, st>>>(m, G.weight.p, keep.p);
+    RL_LAUNCH_CHECK();
+    const uint64_t kept = exclusive_scan_u32(keep.p, pos.p, m, c.prim, st);
+    t2.alloc(kept ? kept : 1);
+    s2.alloc(kept ? kept : 1);
+    w2.alloc(kept ? kept : 1);
+    k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, pos.p, G.tgt.p, G.src.p, G.weight.p, t2.p, s2.p, w2.p);
+    RL_LAUNCH_CHECK();
+    G.tgt.swap(t2);
+    G.src.swap(s2);
+    G.weight.swap(w2);
+    return kept;
+}
+
 void rebuild_graph(Ctx& c) {
     Graph& G = c.graph;
     if (G.num_new == 0) {
+        if (G.zeros) {
+            // only deletions since the last rebuild: the order stands, the zero entries go
+            G.zeros = false;
+            finish_graph(c, G.num_edges ? drop_zero_weights(c, G.num_edges) : 0);
+        }
         return;
     }
     cudaStream_t st = c.stream;
@@ -464,7 +492,12 @@ void rebuild_graph(Ctx& c) {
     k_gather_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, perm.p, tgt.p, srcs.p, ws.p, G.tgt.p, G.src.p, G.weight.p);
     RL_LAUNCH_CHECK();
     G.num_new = 0;
-    finish_graph(c, m);
+    uint64_t kept = m;
+    if (G.zeros) {
+        G.zeros = false;
+        kept = drop_zero_weights(c, m);
+    }
+    finish_graph(c, kept);
 }
 
 uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
@@ -503,27 +536,14 @@ uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
     check_device_error(c, "synapse deletion");
     unsigned long long deleted = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&deleted, d_cnt, sizeof(deleted), cudaMemcpyDeviceToHost, st));
-    // drop entries whose weight reached zero
-    const uint64_t m = G.num_edges;
-    if (m) {
-        DBuf<uint32_t> keep, pos, t2, s2;
-        DBuf<int32_t> w2;
-        keep.alloc(m);
-        pos.alloc(m);
-        k_keep_flags<<<blocks_for(m, 256), 256, 0, st>>>(m, G.weight.p, keep.p);
-        RL_LAUNCH_CHECK();
-        const uint64_t kept = exclusive_scan_u32(keep.p, pos.p, m, c.prim, st);
-        t2.alloc(kept ? kept : 1);
-        s2.alloc(kept ? kept : 1);
-        w2.alloc(kept ? kept : 1);
-        k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, pos.p, G.tgt.p, G.src.p, G.weight.p, t2.p, s2.p, w2.p);
-        RL_LAUNCH_CHECK();
-        G.tgt.swap(t2);
-        G.src.swap(s2);
-        G.weight.swap(w2);
-        finish_graph(c, kept);
-    }
     RL_CUDA_TRY(cudaStreamSynchronize(st));
+    // Entries whose weight reached zero stay until the next rebuild: a zero
+    // entry adds nothing to a neuron's input and is no synapse to a later
+    // deletion (a partner appears |weight| times), and the edge order and
+    // both CSRs stay valid meanwhile.
+    if (deleted) {
+        G.zeros = true;
+    }
     return deleted;
 }
 

@@ -97,6 +97,7 @@ struct Graph {
     DBuf<uint32_t> new_tgt, new_src;
     DBuf<int32_t> new_w;
     uint64_t num_new = 0;
+    bool zeros = false;  // deletions left entries of weight 0 (dropped at the next rebuild)
 };
 
 struct Search {

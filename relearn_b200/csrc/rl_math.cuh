@@ -408,6 +408,34 @@ RL_HD double rl_log(double x) {
 }
 
 // ----------------------------------------------------------------- hypot3
+// The correctly rounded reciprocal 1/a (both sides round to nearest).
+RL_HD double rl_recip(double a) {
+#if defined(__CUDA_ARCH__)
+    return __drcp_rn(a);
+#else
+    return 1.0 / a;
+#endif
+}
+
+// p / a rounded once, from the correctly rounded reciprocal ra = 1/a:
+// q0 = p ra, r = p - a q0 (exact with an FMA), q0 + r ra rounded once is the
+// correctly rounded quotient (Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34 (1990)), as
+// long as nothing under- or overflows.
+RL_HD double quotient_from_recip(double p, double a, double ra) {
+    const double q0 = p * ra;
+    const double r = rl_fma(-a, q0, p);
+    return rl_fma(r, ra, q0);
+}
+
+// Whether quotient_from_recip is exact for p / a: a in [2^-900, 2^901) and p
+// zero, or normal, at least 2^-963 and at most 2^900 below a.
+RL_HD bool recip_quotient_safe(double p, double a) {
+    const int ea = (int)((as_u64(a) >> 52) & 0x7FF);
+    const int ep = (int)((as_u64(p) >> 52) & 0x7FF);
+    return ea >= 123 && ea <= 1923 && (p == 0.0 || (ep >= 60 && ep >= ea - 900));
+}
+
 RL_HD double rl_hypot3(double x, double y, double z) {
     x = fabs(x);
     y = fabs(y);
@@ -423,8 +451,17 @@ RL_HD double rl_hypot3(double x, double y, double z) {
     const bool ymax = !zmax && a == y;
     const double p = zmax || ymax ? x : y;  // first component that is not the maximum
     const double q = zmax ? y : z;          // second one
-    const double ps = p / a;
-    const double qs = q / a;
+    // p / a and q / a from one reciprocal (the same bits as the two
+    // divisions wherever that is exact, which covers every realistic distance)
+    double ps, qs;
+    if (recip_quotient_safe(p, a) && recip_quotient_safe(q, a)) {
+        const double ra = rl_recip(a);
+        ps = quotient_from_recip(p, a, ra);
+        qs = quotient_from_recip(q, a, ra);
+    } else {
+        ps = p / a;
+        qs = q / a;
+    }
     const double p2 = ps * ps, q2 = qs * qs;
     const double t0 = zmax || ymax ? p2 : 1.0;
     const double t1 = zmax ? q2 : (ymax ? 1.0 : p2);
