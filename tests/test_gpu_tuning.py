@@ -90,7 +90,7 @@ def test_tuned_run_equals_untuned(precision):
         if tune:
             t = net.tuning()
             assert t["tuned"] == 3
-            assert len(t["act_ms"]) == (18 if precision else 6) and len(t["search_ms"]) >= 6
+            assert len(t["act_ms"]) == (18 if precision else 12) and len(t["search_ms"]) >= 6
         net.close()
     (x0, c0, e0), (x1, c1, e1) = runs
     assert np.array_equal(x0, x1) and np.array_equal(c0, c1)
