@@ -996,8 +996,10 @@ def run_reference(args, world, rank):
 
 
 def run_case(args):
-    """Small cases for kernel profiles: `activity` runs 4 activity steps of a
-    network of --neurons neurons (no octree needed); `search` runs the search
+    """Small cases for kernel profiles: `activity` runs --case-steps (4)
+    activity steps of a network of --neurons neurons (no octree needed; a
+    network without synapses runs them as one launch of the block kernel
+    unless --step-fusion 0); `search` runs the search
     snapshot (one vacant axon and dendrite of each type per neuron) once;
     `plasticity` seeds 0-3 elements per type and runs two plasticity periods
     (100 activity steps + 1 plasticity update each)."""
@@ -1010,7 +1012,7 @@ def run_case(args):
         apply_shapes(args, net, params["precision"])
     net.set_step_fusion(bool(args.step_fusion))
     if args.case == "activity":
-        net.activity_block(1, 4)
+        net.activity_block(1, args.case_steps)
     elif args.case == "plasticity":
         from relearn_b200 import workloads
 
@@ -1060,6 +1062,7 @@ def main():
     ap.add_argument("--serve-precision", choices=["fp64", "fp32"], default="fp32")
     ap.add_argument("--step-fusion", type=int, choices=[0, 1], default=1,
                     help="1: blocks of activity steps of a network without synapses in one launch (default); 0: one launch per step")
+    ap.add_argument("--case-steps", type=int, default=4, help="activity steps of --case activity")
     ap.add_argument("--case", choices=["activity", "search", "plasticity"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()

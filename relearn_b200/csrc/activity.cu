@@ -113,16 +113,22 @@ __device__ __forceinline__ double growth_curve_flat(double current, double eta, 
 
 // The network of neuron i: draws are keyed on the network's seed and the
 // neuron's index in its network.
+// A neuron's growth rates per element type, held in registers (read once per
+// neuron, not per use).
+struct Nu {
+    double v[3];
+};
+
 template <bool MULTI>
-__device__ __forceinline__ void neuron_net(const ActArgs& A, uint32_t i, uint64_t& seed, uint32_t& local, const double*& nu) {
+__device__ __forceinline__ void neuron_net(const ActArgs& A, uint32_t i, uint64_t& seed, uint32_t& local, Nu& nu) {
     seed = A.seed1;
     local = i;
-    nu = A.nu1;
+    nu = Nu{ { A.nu1[0], A.nu1[1], A.nu1[2] } };
     if (MULTI) {
         const NetInfo& N = A.nets[A.net_of[i]];
         seed = N.seed;
         local = i - N.first;
-        nu = N.nu;
+        nu = Nu{ { N.nu[0], N.nu[1], N.nu[2] } };
     }
 }
 
@@ -232,13 +238,13 @@ __device__ __forceinline__ double calcium_step(const ActArgs& A, uint8_t spiked,
 // The growth of element type t this step (update_number_elements_openmp with
 // gaussian_growth_curve); tgt is the neuron's target calcium when the targets
 // are not uniform.
-__device__ __forceinline__ double growth_step(const ActArgs& A, int t, double ca, double tgt, const double* nu) {
+__device__ __forceinline__ double growth_step(const ActArgs& A, int t, double ca, double tgt, const Nu& nu) {
     if (A.uniform_target) {
-        return growth_curve_pre(ca, A.eta[t], A.flat_u[t], A.xi_u[t], A.zeta_u[t], A.zeta_inv_u[t]) * nu[t];
+        return growth_curve_pre(ca, A.eta[t], A.flat_u[t], A.xi_u[t], A.zeta_u[t], A.zeta_inv_u[t]) * nu.v[t];
     }
     const double eta = A.eta[t];
     const double eps = tgt < eta ? eta : tgt;  // std::max(target, eta)
-    return growth_curve(ca, eta, eps) * nu[t];
+    return growth_curve(ca, eta, eps) * nu.v[t];
 }
 
 // The Izhikevich model's H substeps without the reference's break: the
@@ -284,13 +290,15 @@ __device__ __forceinline__ double calcium_flat(const ActArgs& A, uint8_t spiked,
 }
 
 // Calcium and growth of one step (one target calcium for all neurons).
-template <int H>
-__device__ __forceinline__ void calcium_growth_flat(const ActArgs& A, uint8_t spiked, const double* nu, double& ca, double& d0, double& d1,
+// MULTI false: the context's one network, whose growth rates the kernel
+// reads from its parameters (nu is not used).
+template <int H, bool MULTI>
+__device__ __forceinline__ void calcium_growth_flat(const ActArgs& A, uint8_t spiked, const Nu& nu, double& ca, double& d0, double& d1,
                                                     double& d2) {
     ca = calcium_flat<H>(A, spiked, ca);
-    d0 = d0 + growth_curve_flat(ca, A.eta[0], A.flat_u[0], A.xi_u[0], A.zeta_u[0], A.zeta_inv_u[0]) * nu[0];
-    d1 = d1 + growth_curve_flat(ca, A.eta[1], A.flat_u[1], A.xi_u[1], A.zeta_u[1], A.zeta_inv_u[1]) * nu[1];
-    d2 = d2 + growth_curve_flat(ca, A.eta[2], A.flat_u[2], A.xi_u[2], A.zeta_u[2], A.zeta_inv_u[2]) * nu[2];
+    d0 = d0 + growth_curve_flat(ca, A.eta[0], A.flat_u[0], A.xi_u[0], A.zeta_u[0], A.zeta_inv_u[0]) * (MULTI ? nu.v[0] : A.nu1[0]);
+    d1 = d1 + growth_curve_flat(ca, A.eta[1], A.flat_u[1], A.xi_u[1], A.zeta_u[1], A.zeta_inv_u[1]) * (MULTI ? nu.v[1] : A.nu1[1]);
+    d2 = d2 + growth_curve_flat(ca, A.eta[2], A.flat_u[2], A.xi_u[2], A.zeta_u[2], A.zeta_inv_u[2]) * (MULTI ? nu.v[2] : A.nu1[2]);
 }
 
 // m consecutive steps of an Izhikevich neuron without synaptic input (one
@@ -302,8 +310,8 @@ __device__ __forceinline__ void calcium_growth_flat(const ActArgs& A, uint8_t sp
 // order, so the bits are too.  zs[k * stride] is step k's standard normal
 // draw; `input` receives the last step's input, f and f_before the last two
 // spike flags.
-template <int H>
-__device__ __forceinline__ void izhikevich_chunk(const ActArgs& A, const double* zs, uint32_t stride, uint32_t m, const double* nu, double& xv,
+template <int H, bool MULTI>
+__device__ __forceinline__ void izhikevich_chunk(const ActArgs& A, const double* zs, uint32_t stride, uint32_t m, const Nu& nu, double& xv,
                                                  double& uv, double& ca, double& d0, double& d1, double& d2, double& input, uint8_t& f,
                                                  uint8_t& f_before) {
     double in_k = A.syn0 + (A.noise_mean + A.noise_stddev * zs[0]);
@@ -311,13 +319,13 @@ __device__ __forceinline__ void izhikevich_chunk(const ActArgs& A, const double*
     for (uint32_t k = 0; k + 1 < m; ++k) {
         const double in_n = A.syn0 + (A.noise_mean + A.noise_stddev * zs[(k + 1) * stride]);
         const uint8_t sp_n = izhikevich_frozen<H>(A, in_n, xv, uv);
-        calcium_growth_flat<H>(A, sp, nu, ca, d0, d1, d2);
+        calcium_growth_flat<H, MULTI>(A, sp, nu, ca, d0, d1, d2);
         f_before = f;
         f = sp;
         sp = sp_n;
         in_k = in_n;
     }
-    calcium_growth_flat<H>(A, sp, nu, ca, d0, d1, d2);
+    calcium_growth_flat<H, MULTI>(A, sp, nu, ca, d0, d1, d2);
     f_before = f;
     f = sp;
     input = in_k;
@@ -345,7 +353,7 @@ __device__ __forceinline__ long long synaptic_sum(const ActArgs& A, const ActDes
 // the kernel's draw phase).  `z` is the neuron's standard normal draw of this
 // step.
 template <int H, int MODEL>
-__device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const double* nu,
+__device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const Nu& nu,
                                                      double z, long long isum, double xv, double uv, double ca, double tgt, double d0, double d1,
                                                      double d2) {
     const double input = step_input(A, isum, z);
@@ -389,34 +397,64 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
     __syncthreads();
     const uint32_t stride = gridDim.x * V * BLOCK;
     uint32_t parity = 0;
+    // a neuron's state, loaded one round ahead: with fewer blocks than the
+    // neurons need (the persistent shape) the loads of the next round are in
+    // flight while this round computes
+    struct State {
+        bool on;
+        double x, u, ca, tg, d0, d1, d2;
+    };
+    auto fetch = [&](uint32_t b, State (&S)[V]) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const uint32_t j = b + (uint32_t)v * BLOCK + threadIdx.x;
+            State& t = S[v];
+            t.on = j < A.n && A.enabled[j];
+            t.x = t.u = t.ca = t.tg = t.d0 = t.d1 = t.d2 = 0.0;
+            if (j < A.n) {
+                t.d0 = A.delta0[j];
+                t.d1 = A.delta1[j];
+                t.d2 = A.delta2[j];
+            }
+            if (t.on) {
+                t.x = A.x[j];
+                t.u = A.u[j];
+                t.ca = A.calcium[j];
+                t.tg = A.uniform_target ? 0.0 : A.target[j];
+            }
+        }
+    };
+    State cur[V];
+    fetch(blockIdx.x * V * BLOCK, cur);
     for (uint32_t base = blockIdx.x * V * BLOCK; base < A.n; base += stride, parity ^= 1u) {
+        State nxt[V];
+        if (base + stride < A.n) {
+            fetch(base + stride, nxt);
+        }
         uint32_t i[V];
         bool on[V], tail[V];
         uint64_t seed[V];
         uint32_t local[V];
-        const double* nu[V];
+        Nu nu[V];
         double p[V], z[V], xv[V], uv[V], cav[V], tg[V], d0[V], d1[V], d2[V];
         long long isum[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             i[v] = base + (uint32_t)v * BLOCK + threadIdx.x;
-            on[v] = i[v] < A.n && A.enabled[i[v]];
+            on[v] = cur[v].on;
             seed[v] = 0;
             local[v] = 0;
-            nu[v] = nullptr;
+            nu[v] = Nu{ { 0.0, 0.0, 0.0 } };
             p[v] = 0.5;
-            xv[v] = uv[v] = cav[v] = tg[v] = d0[v] = d1[v] = d2[v] = 0.0;
+            xv[v] = cur[v].x;
+            uv[v] = cur[v].u;
+            cav[v] = cur[v].ca;
+            tg[v] = cur[v].tg;
+            d0[v] = cur[v].d0;
+            d1[v] = cur[v].d1;
+            d2[v] = cur[v].d2;
             isum[v] = 0;
-            if (i[v] < A.n) {
-                d0[v] = A.delta0[i[v]];
-                d1[v] = A.delta1[i[v]];
-                d2[v] = A.delta2[i[v]];
-            }
             if (on[v]) {
-                xv[v] = A.x[i[v]];
-                uv[v] = A.u[i[v]];
-                cav[v] = A.calcium[i[v]];
-                tg[v] = A.uniform_target ? 0.0 : A.target[i[v]];
                 isum[v] = synaptic_sum(A, D, i[v]);
                 neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
                 p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
@@ -467,7 +505,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 }
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
-                    calcium_growth_flat<H>(A, sp[v], on[v] ? nu[v] : A.nu1, cav[v], d0[v], d1[v], d2[v]);
+                    calcium_growth_flat<H, MULTI>(A, sp[v], nu[v], cav[v], d0[v], d1[v], d2[v]);
                 }
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
@@ -501,6 +539,10 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 A.delta1[i[v]] = d1[v] + 0.0;
                 A.delta2[i[v]] = d2[v] + 0.0;
             }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            cur[v] = nxt[v];
         }
     }
 }
@@ -550,7 +592,7 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK) k_activity_steps(ActArgs A
         const bool on = in && A.enabled[i];
         uint64_t seed = 0;
         uint32_t local = 0;
-        const double* nu = nullptr;
+        Nu nu{ { 0.0, 0.0, 0.0 } };
         double xv = 0.0, uv = 0.0, ca = 0.0, tgt = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, input = 0.0;
         uint8_t f = 0;
         if (in) {
@@ -616,7 +658,7 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK) k_activity_steps(ActArgs A
             bool piped = false;
             if constexpr (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
                 if (on && A.uniform_target) {
-                    izhikevich_chunk<H>(A, s_z + threadIdx.x, BLOCK, m, nu, xv, uv, ca, d0, d1, d2, input, f, f_before);
+                    izhikevich_chunk<H, MULTI>(A, s_z + threadIdx.x, BLOCK, m, nu, xv, uv, ca, d0, d1, d2, input, f, f_before);
                     piped = true;
                 }
             }

@@ -139,7 +139,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
 template <int H, int MODEL, bool EDGES = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
-                                           uint32_t k24p, const float* nu, float tgt, float& x, float& u, double& ca, float (&delta)[3],
+                                           uint32_t k24p, const float (&nu)[3], float tgt, float& x, float& u, double& ca, float (&delta)[3],
                                            float& input, uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
@@ -386,7 +386,13 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         float d[3] = { d0[k], d1[k], d2[k] };
-        const float* nu = MULTI ? A.nets[net[k]].nu32 : A.nu1;
+        float nu[3] = { A.nu1[0], A.nu1[1], A.nu1[2] };  // growth rates in registers (the network's own when batched)
+        if (MULTI) {
+            const NetInfo& N = A.nets[net[k]];
+            nu[0] = N.nu32[0];
+            nu[1] = N.nu32[1];
+            nu[2] = N.nu32[2];
+        }
         neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, tg[k], x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
@@ -458,12 +464,14 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
         }
         uint64_t seed = A.seed1;
         uint32_t local = i;
-        const float* nu = A.nu1;
+        float nu[3] = { A.nu1[0], A.nu1[1], A.nu1[2] };
         if (MULTI && in) {
             const NetInfo& N = A.nets[A.net_of[i]];
             seed = N.seed;
             local = i - N.first;
-            nu = N.nu32;
+            nu[0] = N.nu32[0];
+            nu[1] = N.nu32[1];
+            nu[2] = N.nu32[2];
         }
         uint8_t f_before = f;
         float input = 0.0f;
