@@ -397,40 +397,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
     __syncthreads();
     const uint32_t stride = gridDim.x * V * BLOCK;
     uint32_t parity = 0;
-    // a neuron's state, loaded one round ahead: with fewer blocks than the
-    // neurons need (the persistent shape) the loads of the next round are in
-    // flight while this round computes
-    struct State {
-        bool on;
-        double x, u, ca, tg, d0, d1, d2;
-    };
-    auto fetch = [&](uint32_t b, State (&S)[V]) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const uint32_t j = b + (uint32_t)v * BLOCK + threadIdx.x;
-            State& t = S[v];
-            t.on = j < A.n && A.enabled[j];
-            t.x = t.u = t.ca = t.tg = t.d0 = t.d1 = t.d2 = 0.0;
-            if (j < A.n) {
-                t.d0 = A.delta0[j];
-                t.d1 = A.delta1[j];
-                t.d2 = A.delta2[j];
-            }
-            if (t.on) {
-                t.x = A.x[j];
-                t.u = A.u[j];
-                t.ca = A.calcium[j];
-                t.tg = A.uniform_target ? 0.0 : A.target[j];
-            }
-        }
-    };
-    State cur[V];
-    fetch(blockIdx.x * V * BLOCK, cur);
     for (uint32_t base = blockIdx.x * V * BLOCK; base < A.n; base += stride, parity ^= 1u) {
-        State nxt[V];
-        if (base + stride < A.n) {
-            fetch(base + stride, nxt);
-        }
         uint32_t i[V];
         bool on[V], tail[V];
         uint64_t seed[V];
@@ -441,20 +408,23 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             i[v] = base + (uint32_t)v * BLOCK + threadIdx.x;
-            on[v] = cur[v].on;
+            on[v] = i[v] < A.n && A.enabled[i[v]];
             seed[v] = 0;
             local[v] = 0;
             nu[v] = Nu{ { 0.0, 0.0, 0.0 } };
             p[v] = 0.5;
-            xv[v] = cur[v].x;
-            uv[v] = cur[v].u;
-            cav[v] = cur[v].ca;
-            tg[v] = cur[v].tg;
-            d0[v] = cur[v].d0;
-            d1[v] = cur[v].d1;
-            d2[v] = cur[v].d2;
+            xv[v] = uv[v] = cav[v] = tg[v] = d0[v] = d1[v] = d2[v] = 0.0;
             isum[v] = 0;
+            if (i[v] < A.n) {
+                d0[v] = A.delta0[i[v]];
+                d1[v] = A.delta1[i[v]];
+                d2[v] = A.delta2[i[v]];
+            }
             if (on[v]) {
+                xv[v] = A.x[i[v]];
+                uv[v] = A.u[i[v]];
+                cav[v] = A.calcium[i[v]];
+                tg[v] = A.uniform_target ? 0.0 : A.target[i[v]];
                 isum[v] = synaptic_sum(A, D, i[v]);
                 neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
                 p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
@@ -539,10 +509,6 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 A.delta1[i[v]] = d1[v] + 0.0;
                 A.delta2[i[v]] = d2[v] + 0.0;
             }
-        }
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            cur[v] = nxt[v];
         }
     }
 }

@@ -135,11 +135,42 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
+// A neuron's growth-curve constants per element type (gaussian_growth_curve
+// with epsilon = max(target, eta)): xi, the scaled 1 / zeta, and the eta ==
+// epsilon case as a bit; from the context's constants when every neuron has
+// the same target, else from the neuron's own target.  Made once per neuron
+// and launch, not per step.
+struct Grow32 {
+    float xi[3], iz[3];
+    uint32_t flat;
+};
+
+__device__ __forceinline__ Grow32 grow32_of(const Act32& A, float tgt) {
+    Grow32 G;
+    G.flat = 0;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        if (A.target) {
+            const float eta = A.eta[t];
+            const float eps = fmaxf(tgt, eta);
+            const bool flat = eta == eps;
+            G.xi[t] = 0.5f * (eta + eps);
+            G.iz[t] = flat ? 0.0f : __fdividef(A.kz, eta - eps);
+            G.flat |= (flat ? 1u : 0u) << t;
+        } else {
+            G.xi[t] = A.xi[t];
+            G.iz[t] = A.inv_zeta[t];
+            G.flat |= (A.flat[t] ? 1u : 0u) << t;
+        }
+    }
+    return G;
+}
+
 // `k24`: the neuron's 24 random bits of this step's background draw;
 // `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
 template <int H, int MODEL, bool EDGES = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
-                                           uint32_t k24p, const float (&nu)[3], float tgt, float& x, float& u, double& ca, float (&delta)[3],
+                                           uint32_t k24p, const float (&nu)[3], const Grow32& G, float& x, float& u, double& ca, float (&delta)[3],
                                            float& input, uint8_t& fired) {
     if (!enabled) {
         input = 0.0f;
@@ -164,10 +195,29 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     float uv = u;
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
-    if (MODEL == RL_MODEL_IZHIKEVICH) {
+    if (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
+        // the substeps run on past a spike without a branch; the state at the
+        // first crossing is what the step returns (x = c, u + d), as with the
+        // reference's break
         const float sc = fmaf(A.s, input, A.sk3);
         const float ms = -A.s;
+        float u_cross = 0.0f;
+        bool done = false;
 #pragma unroll
+        for (int it = 0; it < H; ++it) {
+            const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
+            uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
+            xv = xv + inc;
+            const bool first = !done && xv >= A.v_spike;
+            u_cross = first ? uv : u_cross;
+            done = done || first;
+        }
+        xv = done ? A.c : xv;
+        uv = done ? u_cross + A.d : uv;
+        spiked = done ? 1 : 0;
+    } else if (MODEL == RL_MODEL_IZHIKEVICH) {
+        const float sc = fmaf(A.s, input, A.sk3);
+        const float ms = -A.s;
         for (uint32_t it = 0; it < h; ++it) {
             const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
             uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
@@ -228,23 +278,9 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     const float caf = (float)ca;
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
-        float dz;
-        bool flat = A.flat[t];
-        float xi = A.xi[t], inv_zeta = A.inv_zeta[t];
-        if (A.target) {
-            // gaussian_growth_curve with the neuron's own epsilon = max(target, eta)
-            const float eta = A.eta[t];
-            const float eps = fmaxf(tgt, eta);
-            flat = eta == eps;
-            xi = 0.5f * (eta + eps);
-            inv_zeta = flat ? 0.0f : __fdividef(A.kz, eta - eps);
-        }
-        if (flat) {
-            dz = caf == A.eta[t] ? 0.0f : -1.0f;
-        } else {
-            const float q = (caf - xi) * inv_zeta;
-            dz = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
-        }
+        const float q = (caf - G.xi[t]) * G.iz[t];
+        const float curve = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
+        const float dz = ((G.flat >> t) & 1u) ? (caf == A.eta[t] ? 0.0f : -1.0f) : curve;
         delta[t] = fmaf(dz, nu[t], delta[t]);
     }
 }
@@ -393,7 +429,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
             nu[1] = N.nu32[1];
             nu[2] = N.nu32[2];
         }
-        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, tg[k], x[k], u[k], ca[k], d, input[k], fired[k]);
+        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, grow32_of(A, tg[k]), x[k], u[k], ca[k], d, input[k], fired[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     if (A.input) {
@@ -475,6 +511,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
         }
         uint8_t f_before = f;
         float input = 0.0f;
+        const Grow32 G = grow32_of(A, tg);
         auto one_step = [&](uint32_t step, uint32_t word) {
             uint32_t k24p = 0;
             if (MODEL == RL_MODEL_POISSON && en) {
@@ -483,7 +520,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
                 k24p = w.x >> 8;
             }
             uint8_t fired;
-            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, tg, x, u, ca, d, input, fired);
+            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, G, x, u, ca, d, input, fired);
             f_before = f;
             f = fired;
         };
