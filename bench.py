@@ -1000,7 +1000,8 @@ def run_case(args):
     activity steps of a network of --neurons neurons (no octree needed; a
     network without synapses runs them as one launch of the block kernel
     unless --step-fusion 0); `search` runs the search
-    snapshot (one vacant axon and dendrite of each type per neuron) once;
+    snapshot (one vacant axon and dendrite of each type per neuron, or a vacant
+    axon on --search-sources random neurons only) once;
     `plasticity` seeds 0-3 elements per type and runs two plasticity periods
     (100 activity steps + 1 plasticity update each)."""
     import relearn_b200 as R
@@ -1023,11 +1024,16 @@ def run_case(args):
     else:
         net.set_positions(pos, sig)
         one = np.ones(args.neurons, np.uint32)
+        axons = one
+        if args.search_sources:
+            # a sparse search list: a vacant axon on that many neurons drawn at random
+            axons = np.zeros(args.neurons, np.uint32)
+            axons[np.random.default_rng(3).choice(args.neurons, args.search_sources, replace=False)] = 1
         for t in range(3):
-            net.set_elements(t, np.full(args.neurons, 1.5), np.zeros(args.neurons), np.zeros(args.neurons, np.uint32), one)
-        net.prepare_update_connectivity(one, one, one)
+            net.set_elements(t, np.full(args.neurons, 1.5), np.zeros(args.neurons), np.zeros(args.neurons, np.uint32), axons if t == 0 else one)
+        net.prepare_update_connectivity(axons, one, one)
         req = net.find_targets(100)
-        print(json.dumps({"case": "search", "searches": args.neurons, "requests": int(len(req))}))
+        print(json.dumps({"case": "search", "searches": int(axons.sum()), "requests": int(len(req))}))
     net.synchronize()
     print(json.dumps({"case": args.case, "neurons": args.neurons, "stats": net.stats()}))
 
@@ -1063,6 +1069,7 @@ def main():
     ap.add_argument("--step-fusion", type=int, choices=[0, 1], default=1,
                     help="1: blocks of activity steps of a network without synapses in one launch (default); 0: one launch per step")
     ap.add_argument("--case-steps", type=int, default=4, help="activity steps of --case activity")
+    ap.add_argument("--search-sources", type=int, default=0, help="--case search: vacant axons on this many random neurons (0: on every neuron)")
     ap.add_argument("--case", choices=["activity", "search", "plasticity"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()

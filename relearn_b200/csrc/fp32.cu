@@ -195,29 +195,10 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     float uv = u;
     uint8_t spiked = 0;
     const uint32_t h = H > 0 ? (uint32_t)H : A.h_model;
-    if (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
-        // the substeps run on past a spike without a branch; the state at the
-        // first crossing is what the step returns (x = c, u + d), as with the
-        // reference's break
+    if (MODEL == RL_MODEL_IZHIKEVICH) {
         const float sc = fmaf(A.s, input, A.sk3);
         const float ms = -A.s;
-        float u_cross = 0.0f;
-        bool done = false;
 #pragma unroll
-        for (int it = 0; it < H; ++it) {
-            const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
-            uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
-            xv = xv + inc;
-            const bool first = !done && xv >= A.v_spike;
-            u_cross = first ? uv : u_cross;
-            done = done || first;
-        }
-        xv = done ? A.c : xv;
-        uv = done ? u_cross + A.d : uv;
-        spiked = done ? 1 : 0;
-    } else if (MODEL == RL_MODEL_IZHIKEVICH) {
-        const float sc = fmaf(A.s, input, A.sk3);
-        const float ms = -A.s;
         for (uint32_t it = 0; it < h; ++it) {
             const float inc = fmaf(xv, fmaf(A.sk1, xv, A.sk2), fmaf(ms, uv, sc));
             uv = fmaf(A.sa, fmaf(A.b, xv, -uv), uv);
