@@ -632,6 +632,8 @@ def synapse_regime(args, dev, stream, world, precision):
     dom = max(("activity_kernel", "search_kernel", "connector", "graph", "commit", "tree_update"), key=lambda k: phases[k][0])
     out["dominant_phase"] = dom
     out["roofline"] = out.get("search_roofline") if dom == "search_kernel" and "search_roofline" in out else act_roof
+    t = net.tuning()
+    out["tuning"] = {k: t[k] for k in ("act_block", "act_persistent", "act_vec", "search_warps", "search_packet", "search_cap", "search_hot")}
     net.close()
     return out
 

@@ -1087,7 +1087,11 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     const ActDesc v{ first_step, c.graph.num_edges > 0 ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p };
     k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
     RL_LAUNCH_CHECK();
-    if (c.tune.act_state == TUNE_REQUESTED) {
+    const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;
+    // the launch shape is a shape of the per-step kernel: it is timed at the
+    // first block that runs one launch per step (with the synapses it will
+    // read), not while blocks run as one fused launch
+    if (c.tune.act_state == TUNE_REQUESTED && !fused) {
         if (c.tune.force || !recall_act_tuning(c)) {
             tune_activity(c);
             remember_act_tuning(c);
@@ -1095,7 +1099,6 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         c.tune.act_state = TUNE_DONE;
         drop_activity_graphs(c);
     }
-    const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;
     const bool graph = !fused && c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
     if (fused) {
         // no synapses: every neuron's steps are independent of the others'

@@ -457,7 +457,8 @@ TuneKey tune_key(const Ctx& c) {
     while (lg < 40 && (1ull << (lg + 1)) <= (uint64_t)c.n) {
         ++lg;
     }
-    return std::make_tuple(c.cfg.precision, c.multi() ? 1 : 0, lg, c.cfg.neuron_model, c.cfg.kernel_type);
+    // networks with synapses read in-edges every step: a class of their own
+    return std::make_tuple(c.cfg.precision, (c.multi() ? 1 : 0) | (c.graph.num_edges > 0 ? 2 : 0), lg, c.cfg.neuron_model, c.cfg.kernel_type);
 }
 }  // namespace
 

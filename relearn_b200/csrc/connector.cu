@@ -133,33 +133,6 @@ __global__ void k_emit_edges(uint64_t m, const uint32_t* __restrict__ accepted, 
 }
 
 // ---- graph
-__global__ void k_pair_keys(uint64_t m, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, uint64_t* __restrict__ key,
-                            uint32_t* __restrict__ idx) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) {
-        key[i] = ((uint64_t)hi[i] << 32) | lo[i];
-        idx[i] = (uint32_t)i;
-    }
-}
-
-__global__ void k_count_u32(uint64_t m, const uint32_t* __restrict__ v, uint32_t* __restrict__ cnt) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) {
-        atomicAdd(&cnt[v[i]], 1u);
-    }
-}
-
-__global__ void k_gather_edges(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ t_in, const uint32_t* __restrict__ s_in,
-                               const int32_t* __restrict__ w_in, uint32_t* __restrict__ t_out, uint32_t* __restrict__ s_out, int32_t* __restrict__ w_out) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) {
-        const uint32_t k = perm[i];
-        t_out[i] = t_in[k];
-        s_out[i] = s_in[k];
-        w_out[i] = w_in[k];
-    }
-}
-
 __global__ void k_keep_flags(uint64_t m, const int32_t* __restrict__ w, uint32_t* __restrict__ keep) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m) {
@@ -176,6 +149,184 @@ __global__ void k_compact_edges(uint64_t m, const uint32_t* __restrict__ keep, c
         t_out[o] = t_in[i];
         s_out[o] = s_in[i];
         w_out[o] = w_in[i];
+    }
+}
+
+// ---- incremental graph update
+// The edge list stays sorted by (target, source) and the out-CSR permutation
+// by (source, target), equal pairs in insertion order.  A plasticity update
+// adds a few thousand synapses to a list of millions, so the new ones are
+// sorted alone and merged in: an old entry moves up by the number of new keys
+// below its own, a new entry lands after every old entry with a key at or
+// below its own (old entries first among equals, as a stable sort of the
+// concatenation orders them).
+
+__device__ __forceinline__ uint64_t pair_key(uint32_t hi, uint32_t lo, int bn) {
+    return ((uint64_t)hi << bn) | lo;
+}
+
+// Number of keys in the sorted array k[0, n) below x (or at or below it).
+__device__ __forceinline__ uint64_t count_below(const uint64_t* __restrict__ k, uint64_t n, uint64_t x, bool or_equal) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        const bool below = or_equal ? k[mid] <= x : k[mid] < x;
+        if (below) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Keys of the new entries and their indices, for the small sort.
+__global__ void k_new_keys(uint64_t m, const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ map, int bn,
+                           uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        key[i] = pair_key(hi[i], lo[i], bn);
+        val[i] = map ? map[i] : (uint32_t)i;
+    }
+}
+
+// Sorts up to kSmallSort (key, value) pairs in one block: a bitonic network on
+// (key, value) — the values are distinct, so the order is total and equal keys
+// keep the order of their values (insertion order).
+constexpr uint32_t kSmallSort = 4096;
+__global__ void __launch_bounds__(1024) k_small_sort(uint64_t* key, uint32_t* val, uint32_t m) {
+    __shared__ uint64_t sk[kSmallSort];
+    __shared__ uint32_t sv[kSmallSort];
+    uint32_t p2 = 1;
+    while (p2 < m) {
+        p2 <<= 1;
+    }
+    for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
+        sk[i] = i < m ? key[i] : ~0ull;
+        sv[i] = i < m ? val[i] : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    for (uint32_t size = 2; size <= p2; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
+                const uint32_t j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const bool greater = sk[i] > sk[j] || (sk[i] == sk[j] && sv[i] > sv[j]);
+                    if (greater == up) {
+                        const uint64_t tk = sk[i];
+                        sk[i] = sk[j];
+                        sk[j] = tk;
+                        const uint32_t tv = sv[i];
+                        sv[i] = sv[j];
+                        sv[j] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        key[i] = sk[i];
+        val[i] = sv[i];
+    }
+}
+
+// Old entries (sorted by (target, source)) into the merged list.
+__global__ void k_merge_old(uint64_t m, const uint32_t* __restrict__ t, const uint32_t* __restrict__ src, const int32_t* __restrict__ w,
+                            const uint64_t* __restrict__ nkey, uint64_t mn, int bn, uint32_t* __restrict__ pos, uint32_t* __restrict__ t_out,
+                            uint32_t* __restrict__ s_out, int32_t* __restrict__ w_out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        const uint64_t o = i + count_below(nkey, mn, pair_key(t[i], src[i], bn), false);
+        pos[i] = (uint32_t)o;
+        t_out[o] = t[i];
+        s_out[o] = src[i];
+        w_out[o] = w[i];
+    }
+}
+
+// Number of old entries with a key at or below x (keys made from the sorted
+// old arrays on the fly).
+__device__ __forceinline__ uint64_t count_old_at_or_below(const uint32_t* __restrict__ hi, const uint32_t* __restrict__ lo,
+                                                          const uint32_t* __restrict__ perm, uint64_t n, uint64_t x, int bn) {
+    uint64_t a = 0, b = n;
+    while (a < b) {
+        const uint64_t mid = (a + b) >> 1;
+        const uint32_t e = perm ? perm[mid] : (uint32_t)mid;
+        if (pair_key(hi[e], lo[e], bn) <= x) {
+            a = mid + 1;
+        } else {
+            b = mid;
+        }
+    }
+    return a;
+}
+
+// New entries (sorted; val = index among the new ones) into the merged list;
+// newpos[val] receives each one's place.
+__global__ void k_merge_new(uint64_t mn, const uint64_t* __restrict__ nkey, const uint32_t* __restrict__ nval, const uint32_t* __restrict__ nt,
+                            const uint32_t* __restrict__ ns, const int32_t* __restrict__ nw, const uint32_t* __restrict__ t, const uint32_t* __restrict__ src,
+                            uint64_t m, int bn, uint32_t* __restrict__ newpos, uint32_t* __restrict__ t_out, uint32_t* __restrict__ s_out,
+                            int32_t* __restrict__ w_out) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < mn) {
+        const uint64_t o = j + count_old_at_or_below(t, src, nullptr, m, nkey[j], bn);
+        const uint32_t v = nval[j];
+        newpos[v] = (uint32_t)o;
+        t_out[o] = nt[v];
+        s_out[o] = ns[v];
+        w_out[o] = nw[v];
+    }
+}
+
+// The out-CSR permutation: old entries (in (source, target) order, as edge
+// indices of the old list) moved to their merged indices and places.
+__global__ void k_merge_out_old(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ t, const uint32_t* __restrict__ src,
+                                const uint32_t* __restrict__ pos, const uint64_t* __restrict__ nkey, uint64_t mn, int bn, uint32_t* __restrict__ out) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) {
+        const uint32_t e = perm[k];
+        out[k + count_below(nkey, mn, pair_key(src[e], t[e], bn), false)] = pos[e];
+    }
+}
+
+__global__ void k_merge_out_new(uint64_t mn, const uint64_t* __restrict__ nkey, const uint32_t* __restrict__ nval, const uint32_t* __restrict__ perm,
+                                const uint32_t* __restrict__ t, const uint32_t* __restrict__ src, uint64_t m, int bn, uint32_t* __restrict__ out) {
+    const uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < mn) {
+        out[j + count_old_at_or_below(src, t, perm, m, nkey[j], bn)] = nval[j];
+    }
+}
+
+// Row offsets of a list sorted by row: off[r] = the first entry whose row is
+// r or more, for r = 0..n (entries e in [0, m]; `perm` maps list order to
+// edge indices, or null).
+__global__ void k_row_offsets(uint64_t m, const uint32_t* __restrict__ row, const uint32_t* __restrict__ perm, uint32_t n, uint32_t* __restrict__ off) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e > m) {
+        return;
+    }
+    const uint32_t lo = e == 0 ? 0u : row[perm ? perm[e - 1] : (uint32_t)(e - 1)] + 1u;
+    const uint32_t hi = e == m ? n : row[perm ? perm[e] : (uint32_t)e];
+    for (uint32_t r = lo; r <= hi; ++r) {
+        off[r] = (uint32_t)e;
+    }
+}
+
+// Out-CSR entries that survive the zero compaction, renumbered.
+__global__ void k_keep_out(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ keep, uint32_t* __restrict__ keep_out) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) {
+        keep_out[k] = keep[perm[k]];
+    }
+}
+
+__global__ void k_compact_out(uint64_t m, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ keep_out, const uint32_t* __restrict__ opos,
+                              const uint32_t* __restrict__ epos, uint32_t* __restrict__ out) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m && keep_out[k]) {
+        out[opos[k]] = epos[perm[k]];
     }
 }
 
@@ -395,109 +546,117 @@ int bits_for(uint64_t v) {
     return b;
 }
 
-// In-CSR offsets and the out-CSR of the sorted edge list.
-void finish_graph(Ctx& c, uint64_t m) {
-    Graph& G = c.graph;
-    cudaStream_t st = c.stream;
-    const uint32_t n = c.n;
-    G.num_edges = m;
-    G.offsets.ensure((size_t)n + 1);
-    G.out_off.ensure((size_t)n + 1);
-    DBuf<uint32_t> cnt;
-    cnt.alloc((size_t)n + 1);
-    RL_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, ((size_t)n + 1) * sizeof(uint32_t), st));
-    if (m) {
-        k_count_u32<<<blocks_for(m, 256), 256, 0, st>>>(m, G.tgt.p, cnt.p);
-        RL_LAUNCH_CHECK();
+// The new entries' keys sorted with their values (insertion order among
+// equal keys): one block for a plasticity update's few thousand, the radix
+// sort beyond that.
+void sort_new(Ctx& c, uint64_t* key, uint32_t* val, uint64_t m, int bits) {
+    if (m <= 1) {
+        return;
     }
-    exclusive_scan_u32(cnt.p, G.offsets.p, (uint64_t)n + 1, c.prim, st);
-    RL_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, ((size_t)n + 1) * sizeof(uint32_t), st));
-    G.out_perm.ensure(m ? m : 1);
-    if (m) {
-        k_count_u32<<<blocks_for(m, 256), 256, 0, st>>>(m, G.src.p, cnt.p);
+    if (m <= kSmallSort) {
+        k_small_sort<<<1, 1024, 0, c.stream>>>(key, val, (uint32_t)m);
         RL_LAUNCH_CHECK();
-        DBuf<uint64_t> key;
-        key.alloc(m);
-        k_pair_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, G.src.p, G.tgt.p, key.p, G.out_perm.p);
-        RL_LAUNCH_CHECK();
-        radix_sort_u64(key.p, G.out_perm.p, m, 32 + bits_for(n), c.prim, st);
+    } else {
+        radix_sort_u64(key, val, m, bits, c.prim, c.stream);
     }
-    exclusive_scan_u32(cnt.p, G.out_off.p, (uint64_t)n + 1, c.prim, st);
-    RL_CUDA_TRY(cudaStreamSynchronize(st));
 }
 
 }  // namespace
 
-// Drops the entries of weight 0 that deletions left (order kept); returns
-// the new entry count.
-uint64_t drop_zero_weights(Ctx& c, uint64_t m) {
-    Graph& G = c.graph;
-    cudaStream_t st = c.stream;
-    DBuf<uint32_t> keep, pos, t2, s2;
-    DBuf<int32_t> w2;
-    keep.alloc(m);
-    pos.alloc(m);
-    k_keep_flags<<<blocks_for(m, 256), 256, 0, st>>>(m, G.weight.p, keep.p);
-    RL_LAUNCH_CHECK();
-    const uint64_t kept = exclusive_scan_u32(keep.p, pos.p, m, c.prim, st);
-    t2.alloc(kept ? kept : 1);
-    s2.alloc(kept ? kept : 1);
-    w2.alloc(kept ? kept : 1);
-    k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, pos.p, G.tgt.p, G.src.p, G.weight.p, t2.p, s2.p, w2.p);
-    RL_LAUNCH_CHECK();
-    G.tgt.swap(t2);
-    G.src.swap(s2);
-    G.weight.swap(w2);
-    return kept;
-}
-
+// Merges the new synapses into the sorted list and the out-CSR, drops the
+// entries deletions left at weight 0, and rebuilds both row-offset arrays.
 void rebuild_graph(Ctx& c) {
     Graph& G = c.graph;
-    if (G.num_new == 0) {
-        if (G.zeros) {
-            // only deletions since the last rebuild: the order stands, the zero entries go
-            G.zeros = false;
-            finish_graph(c, G.num_edges ? drop_zero_weights(c, G.num_edges) : 0);
-        }
+    if (G.num_new == 0 && !G.zeros) {
         return;
     }
     cudaStream_t st = c.stream;
     const uint32_t n = c.n;
-    const uint64_t old = G.num_edges;
-    const uint64_t m = old + G.num_new;
+    const uint64_t mo = G.num_edges;
+    const uint64_t mn = G.num_new;
+    uint64_t m = mo + mn;
     RL_CHECK(m < 0xFFFFFFFFull, RL_ERR_OVERFLOW, "synapse count exceeds 2^32");
-    DBuf<uint32_t> tgt, srcs, perm;
-    DBuf<int32_t> ws;
-    DBuf<uint64_t> key;
-    tgt.alloc(m);
-    srcs.alloc(m);
-    ws.alloc(m);
-    perm.alloc(m);
-    key.alloc(m);
-    if (old) {
-        RL_CUDA_TRY(cudaMemcpyAsync(tgt.p, G.tgt.p, old * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-        RL_CUDA_TRY(cudaMemcpyAsync(srcs.p, G.src.p, old * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-        RL_CUDA_TRY(cudaMemcpyAsync(ws.p, G.weight.p, old * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    const int bn = bits_for(n);
+    DBuf<uint32_t> T, S, out, pos, newpos;
+    DBuf<int32_t> W;
+    DBuf<uint64_t> nk;
+    DBuf<uint32_t> nv;
+    T.alloc(m ? m : 1);
+    S.alloc(m ? m : 1);
+    W.alloc(m ? m : 1);
+    out.alloc(m ? m : 1);
+    pos.alloc(mo ? mo : 1);
+    newpos.alloc(mn ? mn : 1);
+    nk.alloc(mn ? mn : 1);
+    nv.alloc(mn ? mn : 1);
+    // list order: new entries by (target, source), merged behind equal old ones
+    if (mn) {
+        k_new_keys<<<blocks_for(mn, 256), 256, 0, st>>>(mn, G.new_tgt.p, G.new_src.p, nullptr, bn, nk.p, nv.p);
+        RL_LAUNCH_CHECK();
+        sort_new(c, nk.p, nv.p, mn, 2 * bn);
     }
-    RL_CUDA_TRY(cudaMemcpyAsync(tgt.p + old, G.new_tgt.p, G.num_new * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    RL_CUDA_TRY(cudaMemcpyAsync(srcs.p + old, G.new_src.p, G.num_new * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-    RL_CUDA_TRY(cudaMemcpyAsync(ws.p + old, G.new_w.p, G.num_new * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-    // canonical order: (target, source), equal pairs in insertion order
-    k_pair_keys<<<blocks_for(m, 256), 256, 0, st>>>(m, tgt.p, srcs.p, key.p, perm.p);
-    RL_LAUNCH_CHECK();
-    radix_sort_u64(key.p, perm.p, m, 32 + bits_for(n), c.prim, st);
-    G.tgt.ensure(m);
-    G.src.ensure(m);
-    G.weight.ensure(m);
-    k_gather_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, perm.p, tgt.p, srcs.p, ws.p, G.tgt.p, G.src.p, G.weight.p);
-    RL_LAUNCH_CHECK();
+    if (mo) {
+        k_merge_old<<<blocks_for(mo, 256), 256, 0, st>>>(mo, G.tgt.p, G.src.p, G.weight.p, nk.p, mn, bn, pos.p, T.p, S.p, W.p);
+        RL_LAUNCH_CHECK();
+    }
+    if (mn) {
+        k_merge_new<<<blocks_for(mn, 256), 256, 0, st>>>(mn, nk.p, nv.p, G.new_tgt.p, G.new_src.p, G.new_w.p, G.tgt.p, G.src.p, mo, bn, newpos.p, T.p,
+                                                        S.p, W.p);
+        RL_LAUNCH_CHECK();
+        // out order: new entries by (source, target), valued by their merged index
+        k_new_keys<<<blocks_for(mn, 256), 256, 0, st>>>(mn, G.new_src.p, G.new_tgt.p, newpos.p, bn, nk.p, nv.p);
+        RL_LAUNCH_CHECK();
+        sort_new(c, nk.p, nv.p, mn, 2 * bn);
+    }
+    if (mo) {
+        k_merge_out_old<<<blocks_for(mo, 256), 256, 0, st>>>(mo, G.out_perm.p, G.tgt.p, G.src.p, pos.p, nk.p, mn, bn, out.p);
+        RL_LAUNCH_CHECK();
+    }
+    if (mn) {
+        k_merge_out_new<<<blocks_for(mn, 256), 256, 0, st>>>(mn, nk.p, nv.p, G.out_perm.p, G.tgt.p, G.src.p, mo, bn, out.p);
+        RL_LAUNCH_CHECK();
+    }
+    if (G.zeros && m) {
+        // the entries deletions left at weight 0 go; the order stays
+        DBuf<uint32_t> keep, epos, keep_out, opos, T2, S2, out2;
+        DBuf<int32_t> W2;
+        keep.alloc(m);
+        epos.alloc(m);
+        keep_out.alloc(m);
+        opos.alloc(m);
+        k_keep_flags<<<blocks_for(m, 256), 256, 0, st>>>(m, W.p, keep.p);
+        RL_LAUNCH_CHECK();
+        const uint64_t kept = exclusive_scan_u32(keep.p, epos.p, m, c.prim, st);
+        k_keep_out<<<blocks_for(m, 256), 256, 0, st>>>(m, out.p, keep.p, keep_out.p);
+        RL_LAUNCH_CHECK();
+        exclusive_scan_u32_async(keep_out.p, opos.p, m, c.prim, st);
+        T2.alloc(kept ? kept : 1);
+        S2.alloc(kept ? kept : 1);
+        W2.alloc(kept ? kept : 1);
+        out2.alloc(kept ? kept : 1);
+        k_compact_edges<<<blocks_for(m, 256), 256, 0, st>>>(m, keep.p, epos.p, T.p, S.p, W.p, T2.p, S2.p, W2.p);
+        RL_LAUNCH_CHECK();
+        k_compact_out<<<blocks_for(m, 256), 256, 0, st>>>(m, out.p, keep_out.p, opos.p, epos.p, out2.p);
+        RL_LAUNCH_CHECK();
+        T.swap(T2);
+        S.swap(S2);
+        W.swap(W2);
+        out.swap(out2);
+        m = kept;
+    }
+    G.tgt.swap(T);
+    G.src.swap(S);
+    G.weight.swap(W);
+    G.out_perm.swap(out);
+    G.num_edges = m;
     G.num_new = 0;
-    uint64_t kept = m;
-    if (G.zeros) {
-        G.zeros = false;
-        kept = drop_zero_weights(c, m);
-    }
-    finish_graph(c, kept);
+    G.zeros = false;
+    G.offsets.ensure((size_t)n + 1);
+    G.out_off.ensure((size_t)n + 1);
+    k_row_offsets<<<blocks_for(m + 1, 256), 256, 0, st>>>(m, G.tgt.p, nullptr, n, G.offsets.p);
+    RL_LAUNCH_CHECK();
+    k_row_offsets<<<blocks_for(m + 1, 256), 256, 0, st>>>(m, G.src.p, G.out_perm.p, n, G.out_off.p);
+    RL_LAUNCH_CHECK();
 }
 
 uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
