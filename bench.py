@@ -389,7 +389,7 @@ def apply_shapes(args, net, precision):
     if args.act_shape or args.search_shape:
         b, p, v = (int(x) for x in (args.act_shape or "256,0,1").split(","))
         w, pk, cp, hot = (int(x) for x in ((args.search_shape or "2,32") + ",1,0").split(",")[:4])
-        net.set_tuning(search_warps=w, search_packet=pk, search_cap=cp, search_hot=hot, act_block=b, act_persistent=p, act_vec=v if precision else 1)
+        net.set_tuning(search_warps=w, search_packet=pk, search_cap=cp, search_hot=hot, act_block=b, act_persistent=p, act_vec=v if precision else min(v, 2))
     else:
         net.autotune(1)
 
