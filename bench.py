@@ -201,28 +201,30 @@ def build_network(n, side, seed, placement):
 # captured again.
 CAPTURED = {
     # dram__bytes_read.sum + dram__bytes_write.sum of one per-step activity
-    # launch at 1M neurons (ncu --set full): FP64 49.0 + 0.65 MB, FP32 30.0 + 0.02 MB;
-    # FP64 warp instructions of one per-step k_activity launch (DADD 3.97M +
-    # DMUL 3.44M + DFMA 2.39M + DSETP 0.74M = 10.54 per neuron-step).  The FP64
-    # pipe of an SM takes 2 warp instructions per cycle (64 lanes).
-    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": None,
-                   "traffic": 49.7e6, "fp64_warp_instr_per_neuron": 10.54},
-    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "traffic": 30.0e6},
+    # launch at 1M neurons (bench.py --case activity --step-fusion 0): FP64
+    # 49.03 + 0.60 MB, FP32 30.03 + 0.03 MB; FP64 warp instructions of one
+    # per-step k_activity launch (DMUL, DADD, DFMA, DSETP: 9.98 per
+    # neuron-step).  The FP64 pipe of an SM takes 2 warp instructions per
+    # cycle (64 lanes).
+    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "bdfa4a271091a59c",
+                   "traffic": 49.03e6 + 0.60e6, "fp64_warp_instr_per_neuron": 9.98},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "traffic": 30.03e6 + 0.03e6},
     # the fused block kernels (a network without synapses: a block of steps per
-    # launch, state in registers), from the instruction mix of a 4-step launch
-    # at 1M neurons, per neuron-step: k_activity_steps 10.77 FP64 warp
-    # instructions (43.10M / 4 steps / 1M); k_activity_f32_steps 6.97 warp
-    # instructions of every kind (27.89M / 4 / 1M), issued at one per SM
-    # sub-partition (4 per SM) per cycle; DRAM read + write of that launch
-    # (the same for any block length)
-    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": None, "fp64_warp_instr_per_neuron": 10.77,
-                "traffic": 50.03e6 + 4.35e6},
-    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "warp_instr_per_neuron": 6.97, "traffic": 30.03e6 + 0.13e6},
-    # the search snapshot at 1M (one search per neuron, both signal types):
-    # lanes active per warp instruction, L1 / L2 hit rates of the walk
-    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "rl_math.cuh"), "digest": None, "lanes_active": 19.7, "l1_hit": 0.81,
-                 "l2_hit": 0.94, "dram_bytes_per_search": 700.0},
-    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": None, "lanes_active": 21.9, "l1_hit": 0.85, "l2_hit": 0.75},
+    # launch, state in registers), from the instruction mix of one 100-step
+    # launch at 1M neurons (bench.py --case activity --case-steps 100), per
+    # neuron-step: k_activity_steps 10.08 FP64 warp instructions (DMUL 3.80,
+    # DADD 3.55, DFMA 1.82, DSETP 0.92); k_activity_f32_steps 5.85 warp
+    # instructions of every kind, issued at one per SM sub-partition (4 per
+    # SM) per cycle; DRAM read + write of that launch
+    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "bdfa4a271091a59c", "fp64_warp_instr_per_neuron": 10.08,
+                "traffic": 50.06e6 + 4.50e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.17e6},
+    # the search snapshot at 1M (bench.py --case search; the excitatory pass,
+    # 0.8M searches): lanes active per warp instruction, L1 / L2 hit rates of
+    # the walk, DRAM bytes per search
+    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "ec16784ac6a68489", "lanes_active": 19.85,
+                 "l1_hit": 0.924, "l2_hit": 0.774, "dram_bytes_per_search": 681.0},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.938},
 }
 B200_SMS = 148
 # algorithmic memory of a fused block launch per neuron: reads enabled, spike
