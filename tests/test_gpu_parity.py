@@ -174,6 +174,34 @@ def test_config0_organic_20001_steps():
     compare_state(net, sim, n)
 
 
+def test_organic_connectome_5001_steps():
+    """The config[0] network with elements that grow from the first step and a
+    target calcium below the network's own (eta 0 for every element type,
+    growth rate 5e-3, target 0.035): synapses form organically at the plasticity
+    updates, and once calcium passes the target the elements retract and bound
+    synapses are deleted (the oracle forms about 20,700 and deletes about 7,300
+    in 50 updates); every field and the synapse list equal the oracle's bit for
+    bit.  (With the reference's eta and target the config[0] run forms no
+    synapse in 20,001 steps: calcium never reaches the axons' 0.4.)"""
+    from oracle import oracle as O
+    from relearn_b200 import Network
+
+    n = 2000
+    params, pos, sig = small_network(n, 1000.0, 1)
+    params["min_calcium"] = (0.0, 0.0, 0.0)
+    params["growth_rate"] = (5e-3, 5e-3, 5e-3)
+    params["target_calcium"] = 0.035
+    net = Network(params)
+    net.set_positions(pos, sig)
+    sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    net.simulate(1, 5001)
+    sim.simulate(1, 5001)
+    compare_state(net, sim, n)
+    st = net.stats()
+    assert len(net.edges()[0]) > 5000
+    assert st["synapses_created"] > 10000 and st["synapses_deleted"] > 3000
+
+
 @pytest.mark.parametrize("name", ["golden_uniform_300.npz", "golden_mixture_400.npz"])
 def test_golden_fixtures(name):
     from relearn_b200 import Network, default_params
