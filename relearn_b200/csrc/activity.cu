@@ -48,6 +48,8 @@ struct ActArgs {
     double eta[3];
     const NetInfo* nets;
     const uint16_t* net_of;
+    const NetBlock* blocks;  // a batched context's neurons in blocks of one network
+    uint32_t num_blocks;
     // a context with one network: its seed and growth rates (the kernel then
     // reads no network table)
     uint64_t seed1;
@@ -516,6 +518,124 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
 // Background draws a block-of-steps launch prepares per barrier round.
 constexpr int kDrawChunk = 10;
 
+// One neuron's block of `nsteps` steps on registers (k_activity_steps): neuron
+// i of the context, `local` its index in its network, whose seed is `seed`
+// (its round keys rk0 / rk1 in a context with one network) and whose growth
+// rates are nu.  A lane with `in` false holds no
+// neuron but still draws for its lane pair.  Lanes 2j and 2j + 1 hold a neuron
+// pair (or its even member and an idle lane), whose draws of a step come from
+// one Philox block: the even lane computes step k's block, the odd lane step
+// k + 1's, and each hands the other the two words it needs (the same words as
+// a block per lane).  `parity` selects the shared tail-queue counter of the
+// next chunk.
+template <int BLOCK, int H, int MODEL, bool MULTI>
+__device__ __forceinline__ void neuron_steps64(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t nsteps,
+                                               uint8_t* __restrict__ fired_before_last, uint32_t i, bool in, uint64_t seed, uint32_t local,
+                                               const Nu& nu, const uint32_t (&rk0)[10], const uint32_t (&rk1)[10], uint32_t& parity, double* s_z,
+                                               uint16_t* s_who, uint32_t* s_cnt) {
+    constexpr int S = kDrawChunk;
+    const uint32_t step0 = D->base_step;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool on = in && A.enabled[i];
+    double xv = 0.0, uv = 0.0, ca = 0.0, tgt = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, input = 0.0;
+    uint8_t f = 0;
+    if (in) {
+        f = A.fired_prev[i];
+        d0 = A.delta0[i];
+        d1 = A.delta1[i];
+        d2 = A.delta2[i];
+    }
+    if (on) {
+        xv = A.x[i];
+        uv = A.u[i];
+        ca = A.calcium[i];
+        tgt = A.uniform_target ? 0.0 : A.target[i];
+    }
+    uint8_t f_before = f;
+    for (uint32_t k0 = 0; k0 < nsteps; k0 += S, parity ^= 1u) {
+        const uint32_t m = nsteps - k0 < (uint32_t)S ? nsteps - k0 : (uint32_t)S;
+        const uint32_t stepc = step0 + k0;
+#pragma unroll
+        for (int k = 0; k < S; k += 2) {
+            uint64_t b[2];
+            const uint32_t odd = lane & 1u;
+            // a batched context derives the round keys from the seed as it goes
+            // (twenty more registers would spill)
+            const u32x4 r = MULTI ? noise_block(seed, stepc + (uint32_t)k + odd, local) : noise_block_rk(rk0, rk1, stepc + (uint32_t)k + odd, local);
+            const uint32_t g0 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.x : r.z, 1);
+            const uint32_t g1 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.y : r.w, 1);
+            const uint64_t got = ((uint64_t)g0 << 21) | (uint64_t)(g1 >> 11);
+            b[0] = odd ? got : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
+            b[1] = odd ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : got;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool use = on && (uint32_t)(k + h) < m;
+                const double p = ((double)b[h] + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
+                const bool tail = use && normal_in_tail(p);
+                const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
+                uint32_t first = 0;
+                if (lane == 0 && mask) {
+                    first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
+                }
+                first = __shfl_sync(0xFFFFFFFFu, first, 0);
+                const uint32_t slot = (uint32_t)(k + h) * BLOCK + threadIdx.x;
+                if (tail) {
+                    s_who[first + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = (uint16_t)slot;
+                }
+                s_z[slot] = tail ? p : (use ? normal_quantile_central(p) : 0.0);
+            }
+        }
+        __syncthreads();
+        const uint32_t cnt = s_cnt[parity];
+        for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
+            const uint32_t slot = s_who[q];
+            s_z[slot] = normal_quantile_tail(s_z[slot]);
+        }
+        if (threadIdx.x == 0) {
+            s_cnt[parity ^ 1u] = 0u;  // the next chunk's counter; nobody reads it before the barrier below
+        }
+        __syncthreads();
+        bool piped = false;
+        if constexpr (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
+            if (on && A.uniform_target) {
+                izhikevich_chunk<H, MULTI>(A, s_z + threadIdx.x, BLOCK, m, nu, xv, uv, ca, d0, d1, d2, input, f, f_before);
+                piped = true;
+            }
+        }
+        if (on && !piped) {
+            for (uint32_t k = 0; k < m; ++k) {
+                const uint32_t step = stepc + k;
+                input = step_input(A, 0, s_z[k * BLOCK + threadIdx.x]);
+                f_before = f;
+                f = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
+                ca = calcium_step<H>(A, f, ca);
+                d0 = d0 + growth_step(A, 0, ca, tgt, nu);
+                d1 = d1 + growth_step(A, 1, ca, tgt, nu);
+                d2 = d2 + growth_step(A, 2, ca, tgt, nu);
+            }
+        }
+    }
+    if (on) {
+        A.x[i] = xv;
+        A.u[i] = uv;
+        A.calcium[i] = ca;
+        A.delta0[i] = d0;
+        A.delta1[i] = d1;
+        A.delta2[i] = d2;
+    } else if (in) {
+        A.delta0[i] = d0 + 0.0;
+        A.delta1[i] = d1 + 0.0;
+        A.delta2[i] = d2 + 0.0;
+    }
+    if (in) {
+        if (A.input) {
+            A.input[i] = on ? input : 0.0;
+        }
+        A.fired_cur[i] = f;
+        fired_before_last[i] = f_before;
+    }
+}
+
 // A block of `nsteps` steps in one launch, for a network without synapses:
 // then a neuron's step reads nothing of the other neurons (its input is its
 // own background draw), so each thread carries its neuron's state through the
@@ -532,133 +652,38 @@ constexpr int kDrawChunk = 10;
 // the whole block evaluates the queue after one barrier, and after a second
 // barrier each thread runs its steps on the draws.  Two barriers per chunk
 // instead of two per step, and the tail queue of a chunk spreads over every
-// warp of the block.  In a context with one network, lanes 2j and 2j + 1 hold
-// a neuron pair, whose draws of a step come from one Philox block: the even
-// lane computes step k's block, the odd lane step k + 1's, and each hands the
-// other the two words it needs (the same words as a block per lane).
+// warp of the block.  A batched context (MULTI) runs its neurons in the blocks
+// of A.blocks, each of one network and starting at an even index of it (a
+// multiple of kNetBlock), so that the seed and growth rates are the block's
+// and every lane pair holds a neuron pair.
 template <int BLOCK, int H, int MODEL, bool MULTI>
-__global__ void __launch_bounds__(BLOCK, 768 / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
-                                                          uint8_t* __restrict__ fired_before_last) {
-    constexpr int S = kDrawChunk;
-    __shared__ double s_z[S * BLOCK];      // draw of step k0 + k of thread t at k * BLOCK + t
-    __shared__ uint16_t s_who[S * BLOCK];  // tail queue: slots of s_z holding a uniform to map
+__global__ void __launch_bounds__(BLOCK, (MULTI ? 640 : 768) / BLOCK) k_activity_steps(ActArgs A, const ActDesc* __restrict__ D, uint32_t nsteps,
+                                                                          uint8_t* __restrict__ fired_before_last) {
+    __shared__ double s_z[kDrawChunk * BLOCK];      // draw of step k0 + k of thread t at k * BLOCK + t
+    __shared__ uint16_t s_who[kDrawChunk * BLOCK];  // tail queue: slots of s_z holding a uniform to map
     __shared__ uint32_t s_cnt[2];
     pdl_wait_then_release();  // every input is the previous launch's output
-    const uint32_t step0 = D->base_step;
-    const uint32_t lane = threadIdx.x & 31u;
     if (threadIdx.x < 2) {
         s_cnt[threadIdx.x] = 0u;
     }
     __syncthreads();
-    const uint32_t stride = gridDim.x * BLOCK;
     uint32_t parity = 0;
-    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
-        const uint32_t i = base + threadIdx.x;
-        const bool in = i < A.n;
-        const bool on = in && A.enabled[i];
-        uint64_t seed = 0;
-        uint32_t local = 0;
-        Nu nu{ { 0.0, 0.0, 0.0 } };
-        double xv = 0.0, uv = 0.0, ca = 0.0, tgt = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, input = 0.0;
-        uint8_t f = 0;
-        if (in) {
-            f = A.fired_prev[i];
-            d0 = A.delta0[i];
-            d1 = A.delta1[i];
-            d2 = A.delta2[i];
+    if constexpr (MULTI) {
+        static_assert(BLOCK == (int)kNetBlock, "a thread block is a block of A.blocks");
+        for (uint32_t b = blockIdx.x; b < A.num_blocks; b += gridDim.x) {
+            const NetBlock B = A.blocks[b];
+            const NetInfo& N = A.nets[B.net];
+            const Nu nu{ { N.nu[0], N.nu[1], N.nu[2] } };
+            neuron_steps64<BLOCK, H, MODEL, true>(A, D, nsteps, fired_before_last, B.first + threadIdx.x, threadIdx.x < B.count, N.seed,
+                                                  B.first - N.first + threadIdx.x, nu, A.rk0, A.rk1, parity, s_z, s_who, s_cnt);
         }
-        if (on) {
-            neuron_net<MULTI>(A, i, seed, local, nu);
-            xv = A.x[i];
-            uv = A.u[i];
-            ca = A.calcium[i];
-            tgt = A.uniform_target ? 0.0 : A.target[i];
-        }
-        uint8_t f_before = f;
-        for (uint32_t k0 = 0; k0 < nsteps; k0 += S, parity ^= 1u) {
-            const uint32_t m = nsteps - k0 < (uint32_t)S ? nsteps - k0 : (uint32_t)S;
-            const uint32_t stepc = step0 + k0;
-#pragma unroll
-            for (int k = 0; k < S; k += 2) {
-                uint64_t b[2];
-                if (!MULTI) {
-                    const uint32_t odd = lane & 1u;
-                    const u32x4 r = noise_block_rk(A.rk0, A.rk1, stepc + (uint32_t)k + odd, i);
-                    const uint32_t g0 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.x : r.z, 1);
-                    const uint32_t g1 = __shfl_xor_sync(0xFFFFFFFFu, odd ? r.y : r.w, 1);
-                    const uint64_t got = ((uint64_t)g0 << 21) | (uint64_t)(g1 >> 11);
-                    b[0] = odd ? got : (((uint64_t)r.x << 21) | (uint64_t)(r.y >> 11));
-                    b[1] = odd ? (((uint64_t)r.z << 21) | (uint64_t)(r.w >> 11)) : got;
-                } else {
-                    b[0] = on ? noise_bits53(noise_block(seed, stepc + (uint32_t)k, local), local) : 0u;
-                    b[1] = on ? noise_bits53(noise_block(seed, stepc + (uint32_t)k + 1u, local), local) : 0u;
-                }
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const bool use = on && (uint32_t)(k + h) < m;
-                    const double p = ((double)b[h] + 0.5) * 1.1102230246251565404e-16;  // open (0, 1)
-                    const bool tail = use && normal_in_tail(p);
-                    const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tail);
-                    uint32_t first = 0;
-                    if (lane == 0 && mask) {
-                        first = atomicAdd(&s_cnt[parity], (uint32_t)__popc(mask));
-                    }
-                    first = __shfl_sync(0xFFFFFFFFu, first, 0);
-                    const uint32_t slot = (uint32_t)(k + h) * BLOCK + threadIdx.x;
-                    if (tail) {
-                        s_who[first + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = (uint16_t)slot;
-                    }
-                    s_z[slot] = tail ? p : (use ? normal_quantile_central(p) : 0.0);
-                }
-            }
-            __syncthreads();
-            const uint32_t cnt = s_cnt[parity];
-            for (uint32_t q = threadIdx.x; q < cnt; q += BLOCK) {
-                const uint32_t slot = s_who[q];
-                s_z[slot] = normal_quantile_tail(s_z[slot]);
-            }
-            if (threadIdx.x == 0) {
-                s_cnt[parity ^ 1u] = 0u;  // the next chunk's counter; nobody reads it before the barrier below
-            }
-            __syncthreads();
-            bool piped = false;
-            if constexpr (MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
-                if (on && A.uniform_target) {
-                    izhikevich_chunk<H, MULTI>(A, s_z + threadIdx.x, BLOCK, m, nu, xv, uv, ca, d0, d1, d2, input, f, f_before);
-                    piped = true;
-                }
-            }
-            if (on && !piped) {
-                for (uint32_t k = 0; k < m; ++k) {
-                    const uint32_t step = stepc + k;
-                    input = step_input(A, 0, s_z[k * BLOCK + threadIdx.x]);
-                    f_before = f;
-                    f = model_step<H, MODEL>(A, step, seed, local, input, xv, uv);
-                    ca = calcium_step<H>(A, f, ca);
-                    d0 = d0 + growth_step(A, 0, ca, tgt, nu);
-                    d1 = d1 + growth_step(A, 1, ca, tgt, nu);
-                    d2 = d2 + growth_step(A, 2, ca, tgt, nu);
-                }
-            }
-        }
-        if (on) {
-            A.x[i] = xv;
-            A.u[i] = uv;
-            A.calcium[i] = ca;
-            A.delta0[i] = d0;
-            A.delta1[i] = d1;
-            A.delta2[i] = d2;
-        } else if (in) {
-            A.delta0[i] = d0 + 0.0;
-            A.delta1[i] = d1 + 0.0;
-            A.delta2[i] = d2 + 0.0;
-        }
-        if (in) {
-            if (A.input) {
-                A.input[i] = on ? input : 0.0;
-            }
-            A.fired_cur[i] = f;
-            fired_before_last[i] = f_before;
+    } else {
+        const uint32_t stride = gridDim.x * BLOCK;
+        const Nu nu{ { A.nu1[0], A.nu1[1], A.nu1[2] } };
+        for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
+            const uint32_t i = base + threadIdx.x;
+            neuron_steps64<BLOCK, H, MODEL, false>(A, D, nsteps, fired_before_last, i, i < A.n, A.seed1, i, nu, A.rk0, A.rk1, parity, s_z,
+                                                   s_who, s_cnt);
         }
     }
 }
@@ -860,6 +885,8 @@ ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* f
     }
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
+    A.blocks = c.net_blocks.p;
+    A.num_blocks = c.num_net_blocks;
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
@@ -899,11 +926,12 @@ ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* f
 
 template <int BLOCK, int H, int MODEL>
 void launch_steps64_m(Ctx& c, const ActArgs& A, uint32_t nsteps, uint8_t* fired_before_last) {
-    const unsigned grid = blocks_for(c.n, BLOCK);
     if (c.multi()) {
-        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, true>, grid, BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, true>, c.num_net_blocks, BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps,
+                   fired_before_last);
     } else {
-        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, false>, grid, BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+        launch_pdl(&k_activity_steps<BLOCK, H, MODEL, false>, blocks_for(c.n, BLOCK), BLOCK, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps,
+                   fired_before_last);
     }
 }
 

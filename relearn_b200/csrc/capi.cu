@@ -237,6 +237,16 @@ void setup_nets(Ctx& c, const rl_network* nets, uint32_t num) {
     }
     c.net_of.alloc(c.n);
     RL_CUDA_TRY(cudaMemcpyAsync(c.net_of.p, net_of.data(), c.n * sizeof(uint16_t), cudaMemcpyHostToDevice, c.stream));
+    std::vector<NetBlock> blocks;
+    for (size_t k = 0; k < c.nets.size(); ++k) {
+        for (uint32_t b = 0; b < c.nets[k].count; b += kNetBlock) {
+            const uint32_t left = c.nets[k].count - b;
+            blocks.push_back(NetBlock{ c.nets[k].first + b, (uint16_t)k, (uint16_t)(left < kNetBlock ? left : kNetBlock) });
+        }
+    }
+    c.num_net_blocks = (uint32_t)blocks.size();
+    c.net_blocks.alloc(blocks.size());
+    RL_CUDA_TRY(cudaMemcpyAsync(c.net_blocks.p, blocks.data(), blocks.size() * sizeof(NetBlock), cudaMemcpyHostToDevice, c.stream));
     RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
 }
 

@@ -81,6 +81,8 @@ struct Act32 {
     float kz;
     const NetInfo* nets;
     const uint16_t* net_of;
+    const NetBlock* blocks;  // a batched context's neurons in blocks of one network
+    uint32_t num_blocks;
     // a context with one network: its seed and growth rates, so that the
     // kernel reads no network table
     uint64_t seed1;
@@ -443,110 +445,120 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* 
     }
 }
 
+// One neuron's block of `nsteps` steps on registers (k_activity_f32_steps):
+// neuron i of the context, `local` its index in its network, whose growth
+// rates are nu and whose Philox round keys are rk0 / rk1.  A lane with `in`
+// false holds no neuron but still draws for its lane pair.  With `share`, lanes
+// 2m and 2m + 1 hold the even and odd member of one neuron pair (or the even
+// member and an idle lane), whose background draws of a step are one Philox
+// block (words x and z): the even lane computes the block of step k, the odd
+// lane that of step k + 1, and each hands the other the word it needs, one
+// block per lane for two steps.  The trip count is the same for the whole
+// warp (the pair draws exchange words between lanes).
+template <int H, bool MULTI, int MODEL>
+__device__ __forceinline__ void neuron_steps_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t nsteps, uint8_t* __restrict__ fired_before_last,
+                                                 uint32_t i, bool in, uint32_t local, bool share, const float (&nu)[3], const uint32_t (&rk0)[10],
+                                                 const uint32_t (&rk1)[10]) {
+    const uint32_t step0 = D->base_step;
+    const bool en = in && A.enabled[i] != 0;
+    uint8_t f = 0;
+    float x = 0.0f, u = 0.0f;
+    double ca = 0.0;
+    float d[3] = { 0.0f, 0.0f, 0.0f };
+    float tg = 0.0f;
+    if (in) {
+        if (A.target) {
+            tg = A.target[i];
+        }
+        f = A.fired_prev[i];
+        x = A.x[i];
+        u = A.u[i];
+        ca = A.calcium[i];
+        d[0] = A.delta[0][i];
+        d[1] = A.delta[1][i];
+        d[2] = A.delta[2][i];
+    }
+    uint8_t f_before = f;
+    float input = 0.0f;
+    const Grow32 G = grow32_of(A, tg);
+    auto one_step = [&](uint32_t step, uint32_t word) {
+        uint32_t k24p = 0;
+        if (MODEL == RL_MODEL_POISSON && en) {
+            // the threshold draw of PoissonModelCPU, keyed as in the FP64 form
+            k24p = philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, rk0, rk1).x >> 8;
+        }
+        uint8_t fired;
+        neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, G, x, u, ca, d, input, fired);
+        f_before = f;
+        f = fired;
+    };
+    uint32_t k = 0;
+    if (share) {
+        const bool odd = (threadIdx.x & 1u) != 0;
+        for (; k + 1 < nsteps; k += 2) {
+            const uint32_t st = step0 + k + (odd ? 1u : 0u);
+            const u32x4 blk = noise_block_rk(rk0, rk1, st, local);
+            const uint32_t got = __shfl_xor_sync(0xFFFFFFFFu, odd ? blk.x : blk.z, 1);
+            const uint32_t own = odd ? blk.z : blk.x;
+            one_step(step0 + k, odd ? got : own);
+            one_step(step0 + k + 1, odd ? own : got);
+        }
+    }
+    for (; k < nsteps; ++k) {
+        const uint32_t step = step0 + k;
+        const u32x4 blk = noise_block_rk(rk0, rk1, step, local);
+        one_step(step, (local & 1u) ? blk.z : blk.x);
+    }
+    if (in) {
+        A.x[i] = x;
+        A.u[i] = u;
+        A.calcium[i] = ca;
+        A.delta[0][i] = d[0];
+        A.delta[1][i] = d[1];
+        A.delta[2][i] = d[2];
+        if (A.input) {
+            A.input[i] = input;
+        }
+        A.fired_cur[i] = f;
+        fired_before_last[i] = f_before;
+    }
+}
+
 // A block of `nsteps` steps in one launch, for a network without synapses: a
 // neuron's step then reads nothing of the other neurons, so each thread
 // carries its neuron's state through the block in registers.  The same
 // per-step function and draws as k_activity_f32, so the same bits; the spike
 // flags of the last step go to A.fired_cur and those of the step before to
-// fired_before_last, the input of the last step to A.input.
+// fired_before_last, the input of the last step to A.input.  A batched context
+// (MULTI) runs its neurons in the blocks of A.blocks, each of one network and
+// starting at an even index of it (a multiple of kNetBlock), so that its seed,
+// round keys and growth rates are the block's and every lane pair holds a
+// neuron pair.
 template <int H, int BLOCK, bool MULTI, int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const ActDesc* __restrict__ D, uint32_t nsteps,
                                                               uint8_t* __restrict__ fired_before_last) {
     pdl_wait_then_release();  // every input is the previous launch's output
-    const uint32_t step0 = D->base_step;
-    const uint32_t stride = gridDim.x * BLOCK;
-    const uint32_t lane = threadIdx.x & 31u;
-    // the trip count is the same for the whole block (the pair draws below
-    // exchange words between lanes)
-    for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
-        const uint32_t i = base + threadIdx.x;
-        const bool in = i < A.n;
-        const bool en = in && A.enabled[i] != 0;
-        uint8_t f = 0;
-        float x = 0.0f, u = 0.0f;
-        double ca = 0.0;
-        float d[3] = { 0.0f, 0.0f, 0.0f };
-        float tg = 0.0f;
-        if (in) {
-            if (A.target) {
-                tg = A.target[i];
+    if constexpr (MULTI) {
+        static_assert(BLOCK == (int)kNetBlock, "a thread block is a block of A.blocks");
+        for (uint32_t b = blockIdx.x; b < A.num_blocks; b += gridDim.x) {
+            const NetBlock B = A.blocks[b];
+            const NetInfo& N = A.nets[B.net];
+            const uint64_t seed = N.seed;
+            uint32_t rk0[10], rk1[10];
+#pragma unroll
+            for (int r = 0; r < 10; ++r) {
+                rk0[r] = (uint32_t)seed + (uint32_t)r * 0x9E3779B9u;
+                rk1[r] = (uint32_t)(seed >> 32) + (uint32_t)r * 0xBB67AE85u;
             }
-            f = A.fired_prev[i];
-            x = A.x[i];
-            u = A.u[i];
-            ca = A.calcium[i];
-            d[0] = A.delta[0][i];
-            d[1] = A.delta[1][i];
-            d[2] = A.delta[2][i];
+            const float nu[3] = { N.nu32[0], N.nu32[1], N.nu32[2] };
+            neuron_steps_f32<H, true, MODEL>(A, D, nsteps, fired_before_last, B.first + threadIdx.x, threadIdx.x < B.count,
+                                             B.first - N.first + threadIdx.x, true, nu, rk0, rk1);
         }
-        uint64_t seed = A.seed1;
-        uint32_t local = i;
-        float nu[3] = { A.nu1[0], A.nu1[1], A.nu1[2] };
-        if (MULTI && in) {
-            const NetInfo& N = A.nets[A.net_of[i]];
-            seed = N.seed;
-            local = i - N.first;
-            nu[0] = N.nu32[0];
-            nu[1] = N.nu32[1];
-            nu[2] = N.nu32[2];
-        }
-        uint8_t f_before = f;
-        float input = 0.0f;
-        const Grow32 G = grow32_of(A, tg);
-        auto one_step = [&](uint32_t step, uint32_t word) {
-            uint32_t k24p = 0;
-            if (MODEL == RL_MODEL_POISSON && en) {
-                const u32x4 w = MULTI ? draw(seed, step, local, 0u, STREAM_POISSON, 0u)
-                                      : philox4x32_10_rk(u32x4{ step, local, 0u, (uint32_t)STREAM_POISSON << 24 }, A.rk0, A.rk1);
-                k24p = w.x >> 8;
-            }
-            uint8_t fired;
-            neuron_f32<H, MODEL, false>(A, D, i, en, f, word >> 8, k24p, nu, G, x, u, ca, d, input, fired);
-            f_before = f;
-            f = fired;
-        };
-        uint32_t k = 0;
-        bool share = true;
-        if (MULTI) {
-            // in a batched context only where every lane pair of the warp holds
-            // an even-odd pair of one network
-            const uint64_t pseed = __shfl_xor_sync(0xFFFFFFFFu, seed, 1);
-            const uint32_t plocal = __shfl_xor_sync(0xFFFFFFFFu, local, 1);
-            share = __all_sync(0xFFFFFFFFu, in && (local & 1u) == (lane & 1u) && pseed == seed && (plocal ^ 1u) == local) != 0;
-        }
-        if (share) {
-            // Lanes 2m and 2m + 1 hold a neuron pair (BLOCK a multiple of 32),
-            // whose background draws of a step are one Philox block (words x
-            // and z).  The even lane computes the block of step k, the odd lane
-            // that of step k + 1, and each hands the other the word it needs:
-            // one block per lane for two steps.
-            const bool odd = (lane & 1u) != 0;
-            for (; k + 1 < nsteps; k += 2) {
-                const uint32_t st = step0 + k + (odd ? 1u : 0u);
-                const u32x4 blk = MULTI ? noise_block(seed, st, local) : noise_block_rk(A.rk0, A.rk1, st, i);
-                const uint32_t got = __shfl_xor_sync(0xFFFFFFFFu, odd ? blk.x : blk.z, 1);
-                const uint32_t own = odd ? blk.z : blk.x;
-                one_step(step0 + k, odd ? got : own);
-                one_step(step0 + k + 1, odd ? own : got);
-            }
-        }
-        for (; k < nsteps; ++k) {
-            const uint32_t step = step0 + k;
-            const u32x4 blk = MULTI ? noise_block(seed, step, local) : noise_block_rk(A.rk0, A.rk1, step, local);
-            one_step(step, (local & 1u) ? blk.z : blk.x);
-        }
-        if (in) {
-            A.x[i] = x;
-            A.u[i] = u;
-            A.calcium[i] = ca;
-            A.delta[0][i] = d[0];
-            A.delta[1][i] = d[1];
-            A.delta[2][i] = d[2];
-            if (A.input) {
-                A.input[i] = input;
-            }
-            A.fired_cur[i] = f;
-            fired_before_last[i] = f_before;
+    } else {
+        const uint32_t stride = gridDim.x * BLOCK;
+        for (uint32_t base = blockIdx.x * BLOCK; base < A.n; base += stride) {
+            const uint32_t i = base + threadIdx.x;
+            neuron_steps_f32<H, false, MODEL>(A, D, nsteps, fired_before_last, i, i < A.n, i, true, A.nu1, A.rk0, A.rk1);
         }
     }
 }
@@ -1380,11 +1392,12 @@ void launch_act32_h(Ctx& c, const ActVariant& v, const Act32& A, uint32_t kstep)
 
 template <int H, int MODEL = RL_MODEL_IZHIKEVICH>
 void launch_steps32(Ctx& c, const Act32& A, uint32_t nsteps, uint8_t* fired_before_last) {
-    const unsigned grid = blocks_for(c.n, 128);
     if (c.multi()) {
-        launch_pdl(&k_activity_f32_steps<H, 128, true, MODEL>, grid, 128, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+        launch_pdl(&k_activity_f32_steps<H, kNetBlock, true, MODEL>, c.num_net_blocks, kNetBlock, c.stream, A, (const ActDesc*)c.act_desc.p,
+                   nsteps, fired_before_last);
     } else {
-        launch_pdl(&k_activity_f32_steps<H, 128, false, MODEL>, grid, 128, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps, fired_before_last);
+        launch_pdl(&k_activity_f32_steps<H, 128, false, MODEL>, blocks_for(c.n, 128), 128, c.stream, A, (const ActDesc*)c.act_desc.p, nsteps,
+                   fired_before_last);
     }
 }
 
@@ -1440,6 +1453,8 @@ Act32 act32_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fir
     A.kz = (float)(1.2011224087864498 / factor_inv);
     A.nets = c.d_nets.p;
     A.net_of = c.net_of.p;
+    A.blocks = c.net_blocks.p;
+    A.num_blocks = c.num_net_blocks;
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;

@@ -200,6 +200,14 @@ struct NetInfo {
     QFrame frame;
 };
 
+// A block of at most kNetBlock neurons of one network: [first, first + count).
+constexpr uint32_t kNetBlock = 128;
+struct NetBlock {
+    uint32_t first;
+    uint16_t net;
+    uint16_t count;
+};
+
 // Probability kernel of the search: `type` is an RL_KERNEL_* value; a and b
 // are the kernel's constants (gamma: 1/(Gamma(k) theta^k) and -1/theta;
 // Weibull: b k and b); k_minus_1 the exponent of d; the linear cut-off.
@@ -295,6 +303,12 @@ struct Ctx {
     std::vector<NetInfo> nets;  // host copy
     DBuf<NetInfo> d_nets;
     DBuf<uint16_t> net_of;      // network of each neuron
+    // The neurons of a batched context in blocks of kNetBlock that never span
+    // two networks (a network's last block may be short), for the kernels that
+    // run a block of steps per launch: a thread block holds one network, so its
+    // seed is the same in every thread and lane pairs hold neuron pairs.
+    DBuf<NetBlock> net_blocks;
+    uint32_t num_net_blocks = 0;
     bool multi() const { return nets.size() > 1; }
     std::string last_error;
     bool positions_set = false;
