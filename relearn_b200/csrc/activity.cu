@@ -50,6 +50,7 @@ struct ActArgs {
     const uint16_t* net_of;
     const NetBlock* blocks;  // a batched context's neurons in blocks of one network
     uint32_t num_blocks;
+    long long* syn_in[2];  // pushed synaptic sums by step parity (ActDesc)
     // a context with one network: its seed and growth rates (the kernel then
     // reads no network table)
     uint64_t seed1;
@@ -351,13 +352,46 @@ __device__ __forceinline__ long long synaptic_sum(const ActArgs& A, const ActDes
     return isum;
 }
 
+// Neuron i's synaptic sum at step k of the block: pulled over its in-edges at
+// the block's first step, else the sum its sources pushed at the step before
+// (read and cleared; every neuron clears its own entry, enabled or not).
+__device__ __forceinline__ long long synaptic_sum_k(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t step, uint32_t i,
+                                                    bool on) {
+    if (!D->has_edges) {
+        return 0;
+    }
+    if (k == 0) {
+        return on ? synaptic_sum(A, D, i) : 0;
+    }
+    long long* in = A.syn_in[step & 1u];
+    const long long s = in[i];
+    if (s != 0) {
+        in[i] = 0;
+    }
+    return on ? s : 0;
+}
+
+// A set spike flag of neuron i at step k of the block: its out-edges' weights
+// go to their targets' sums of the next step (none after the block's last).
+__device__ __forceinline__ void push_spike(const ActArgs& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t step, uint32_t i) {
+    if (!D->has_edges || k + 1 >= D->block_len) {
+        return;
+    }
+    unsigned long long* next = reinterpret_cast<unsigned long long*>(A.syn_in[(step + 1u) & 1u]);
+    const uint32_t e0 = D->out_off[i], e1 = D->out_off[i + 1];
+    for (uint32_t j = e0; j < e1; ++j) {
+        const uint32_t e = D->out_perm[j];
+        atomicAdd(next + D->tgt[e], (unsigned long long)(long long)D->w[e]);  // two's complement: the signed sum
+    }
+}
+
 // One enabled neuron's step on state already in registers (loaded before
 // the kernel's draw phase).  `z` is the neuron's standard normal draw of this
 // step.
 template <int H, int MODEL>
-__device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const Nu& nu,
-                                                     double z, long long isum, double xv, double uv, double ca, double tgt, double d0, double d1,
-                                                     double d2) {
+__device__ __forceinline__ uint8_t activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const Nu& nu,
+                                                        double z, long long isum, double xv, double uv, double ca, double tgt, double d0, double d1,
+                                                        double d2) {
     const double input = step_input(A, isum, z);
     if (A.input) {
         A.input[i] = input;
@@ -371,6 +405,7 @@ __device__ __forceinline__ void activity_neuron_regs(const ActArgs& A, uint32_t 
     A.delta0[i] = d0 + growth_step(A, 0, ca, tgt, nu);
     A.delta1[i] = d1 + growth_step(A, 1, ca, tgt, nu);
     A.delta2[i] = d2 + growth_step(A, 2, ca, tgt, nu);
+    return spiked;
 }
 
 // One thread per neuron; with fewer blocks than neurons / BLOCK (the
@@ -421,13 +456,13 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 d0[v] = A.delta0[i[v]];
                 d1[v] = A.delta1[i[v]];
                 d2[v] = A.delta2[i[v]];
+                isum[v] = synaptic_sum_k(A, D, k, step, i[v], on[v]);
             }
             if (on[v]) {
                 xv[v] = A.x[i[v]];
                 uv[v] = A.u[i[v]];
                 cav[v] = A.calcium[i[v]];
                 tg[v] = A.uniform_target ? 0.0 : A.target[i[v]];
-                isum[v] = synaptic_sum(A, D, i[v]);
                 neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
                 p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
             }
@@ -464,6 +499,11 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             }
         }
         bool done = false;
+        uint8_t spike[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            spike[v] = 0;
+        }
         if constexpr (V == 2 && MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
             if (A.uniform_target) {
                 // both neurons' steps in one stretch without branches, so that
@@ -492,6 +532,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                         A.delta0[i[v]] = d0[v];
                         A.delta1[i[v]] = d1[v];
                         A.delta2[i[v]] = d2[v];
+                        spike[v] = sp[v];
                     }
                 }
                 done = true;
@@ -500,16 +541,24 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             if (on[v] && !done) {
-                activity_neuron_regs<H, MODEL>(A, step, i[v], seed[v], local[v], nu[v], z[v], isum[v], xv[v], uv[v], cav[v], tg[v], d0[v], d1[v],
-                                               d2[v]);
+                spike[v] = activity_neuron_regs<H, MODEL>(A, step, i[v], seed[v], local[v], nu[v], z[v], isum[v], xv[v], uv[v], cav[v], tg[v],
+                                                          d0[v], d1[v], d2[v]);
             } else if (!on[v] && i[v] < A.n) {
                 if (A.input) {
                     A.input[i[v]] = 0.0;
                 }
-                A.fired_cur[i[v]] = A.fired_prev[i[v]];
+                spike[v] = A.fired_prev[i[v]];  // a disabled neuron keeps its flag (and its targets still read it)
+                A.fired_cur[i[v]] = spike[v];
                 A.delta0[i[v]] = d0[v] + 0.0;
                 A.delta1[i[v]] = d1[v] + 0.0;
                 A.delta2[i[v]] = d2[v] + 0.0;
+            }
+        }
+        // the spikes' pushes last, with the neurons' state already stored
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (spike[v]) {
+                push_spike(A, D, k, step, i[v]);
             }
         }
     }
@@ -887,6 +936,8 @@ ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* f
     A.net_of = c.net_of.p;
     A.blocks = c.net_blocks.p;
     A.num_blocks = c.num_net_blocks;
+    A.syn_in[0] = c.syn_in64[0].p;
+    A.syn_in[1] = c.syn_in64[1].p;
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
@@ -1026,6 +1077,7 @@ struct ActSnapshot {
         for (size_t b = 0; b < bufs.size(); ++b) {
             RL_CUDA_TRY(cudaMemcpyAsync(bufs[b].first, copies[b]->p, bufs[b].second, cudaMemcpyDeviceToDevice, c.stream));
         }
+        clear_syn_in(c);  // the timed steps left sums pushed for a step that will not run
     }
 };
 
@@ -1098,6 +1150,32 @@ unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel) {
     return full < wave ? full : wave;
 }
 
+void ensure_syn_in(Ctx& c) {
+    if (is_fp32(c) ? c.syn_in32[0].p != nullptr : c.syn_in64[0].p != nullptr) {
+        return;
+    }
+    for (int p = 0; p < 2; ++p) {
+        if (is_fp32(c)) {
+            c.syn_in32[p].alloc(c.n);
+        } else {
+            c.syn_in64[p].alloc(c.n);
+        }
+    }
+    drop_activity_graphs(c);  // captured launches hold the kernel arguments
+    clear_syn_in(c);
+}
+
+void clear_syn_in(Ctx& c) {
+    for (int p = 0; p < 2; ++p) {
+        if (c.syn_in64[p].p) {
+            RL_CUDA_TRY(cudaMemsetAsync(c.syn_in64[p].p, 0, c.syn_in64[p].n * sizeof(long long), c.stream));
+        }
+        if (c.syn_in32[p].p) {
+            RL_CUDA_TRY(cudaMemsetAsync(c.syn_in32[p].p, 0, c.syn_in32[p].n * sizeof(int32_t), c.stream));
+        }
+    }
+}
+
 void drop_activity_graphs(Ctx& c) {
     for (auto& g : c.act_graph) {
         if (g) {
@@ -1112,7 +1190,12 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         return;
     }
     c.act_block_len = nsteps;
-    const ActDesc v{ first_step, c.graph.num_edges > 0 ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p };
+    const bool edges = c.graph.num_edges > 0;
+    if (edges) {
+        ensure_syn_in(c);
+    }
+    const ActDesc v{ first_step, edges ? 1u : 0u, c.graph.offsets.p, c.graph.src.p, c.graph.weight.p, nsteps, c.graph.out_off.p, c.graph.out_perm.p,
+                     c.graph.tgt.p };
     k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
     RL_LAUNCH_CHECK();
     const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;

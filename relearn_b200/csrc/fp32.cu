@@ -83,6 +83,7 @@ struct Act32 {
     const uint16_t* net_of;
     const NetBlock* blocks;  // a batched context's neurons in blocks of one network
     uint32_t num_blocks;
+    int32_t* syn_in[2];  // pushed synaptic sums by step parity (ActDesc)
     // a context with one network: its seed and growth rates, so that the
     // kernel reads no network table
     uint64_t seed1;
@@ -169,11 +170,13 @@ __device__ __forceinline__ Grow32 grow32_of(const Act32& A, float tgt) {
 }
 
 // `k24`: the neuron's 24 random bits of this step's background draw;
-// `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).
+// `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).  The
+// synaptic sum is pulled over the in-edges (`pull`, a block's first step) or
+// is `pushed`, what the sources that fired at the step before pushed.
 template <int H, int MODEL, bool EDGES = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
                                            uint32_t k24p, const float (&nu)[3], const Grow32& G, float& x, float& u, double& ca, float (&delta)[3],
-                                           float& input, uint8_t& fired) {
+                                           float& input, uint8_t& fired, bool pull = true, int pushed = 0) {
     if (!enabled) {
         input = 0.0f;
         fired = fired_prev;
@@ -181,14 +184,18 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     }
     int isum = 0;
     if (EDGES && D->has_edges) {  // EDGES false: a network without synapses (the block kernel)
-        const uint32_t* __restrict__ off = D->off;
-        const uint32_t* __restrict__ src = D->src;
-        const int32_t* __restrict__ wt = D->w;
-        const uint32_t e0 = off[i], e1 = off[i + 1];
-        for (uint32_t e = e0; e < e1; ++e) {
-            if (A.fired_prev[src[e]]) {
-                isum += wt[e];
+        if (pull) {
+            const uint32_t* __restrict__ off = D->off;
+            const uint32_t* __restrict__ src = D->src;
+            const int32_t* __restrict__ wt = D->w;
+            const uint32_t e0 = off[i], e1 = off[i + 1];
+            for (uint32_t e = e0; e < e1; ++e) {
+                if (A.fired_prev[src[e]]) {
+                    isum += wt[e];
+                }
             }
+        } else {
+            isum = pushed;
         }
     }
     input = fmaf((float)isum, A.conductance, fmaf(A.noise_stddev, normal_from_bits24(k24), A.noise_mean));
@@ -353,11 +360,25 @@ __device__ __forceinline__ void ld_h(const uint16_t* p, uint16_t (&v)[V]) {
     }
 }
 
-// V consecutive neurons from index i (a multiple of V): all loads first, so
-// that each thread keeps its whole footprint in flight, then the updates,
-// then the stores.
+// A set spike flag of neuron i at step k of the block: its out-edges' weights
+// go to their targets' sums of the next step (none after the block's last).
+__device__ __forceinline__ void push_spike32(const Act32& A, const ActDesc* __restrict__ D, uint32_t k, uint32_t step, uint32_t i) {
+    if (!D->has_edges || k + 1 >= D->block_len) {
+        return;
+    }
+    int32_t* next = A.syn_in[(step + 1u) & 1u];
+    const uint32_t e0 = D->out_off[i], e1 = D->out_off[i + 1];
+    for (uint32_t j = e0; j < e1; ++j) {
+        const uint32_t e = D->out_perm[j];
+        atomicAdd(next + D->tgt[e], D->w[e]);
+    }
+}
+
+// V consecutive neurons from index i (a multiple of V) at step kstep of the block:
+// all loads first, so that each thread keeps its whole footprint in flight,
+// then the updates, then the stores; the spikes' pushes last.
 template <int H, int V, bool MULTI, int MODEL>
-__device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t step, uint32_t i) {
+__device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t kstep, uint32_t step, uint32_t i) {
     uint8_t en[V], fp[V], fired[V];
     uint16_t net[V];
     float x[V], u[V], d0[V], d1[V], d2[V], input[V];
@@ -376,6 +397,20 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     float tg[V] = {};
     if (A.target) {
         ld_f<V>(A.target + i, tg);
+    }
+    // the sums pushed at the step before (read and cleared; a block's first
+    // step pulls instead)
+    const bool pull = kstep == 0;
+    int pushed[V] = {};
+    if (D->has_edges && !pull) {
+        int32_t* in = A.syn_in[step & 1u];
+        ld_f<V>(reinterpret_cast<const float*>(in + i), reinterpret_cast<float(&)[V]>(pushed));
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (pushed[v] != 0) {
+                in[i + v] = 0;
+            }
+        }
     }
     // Background draws: the same Philox blocks as the FP64 form, 24 bits of
     // each neuron's words; one block serves an even-odd pair of a network, so
@@ -412,7 +447,8 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
             nu[1] = N.nu32[1];
             nu[2] = N.nu32[2];
         }
-        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, grow32_of(A, tg[k]), x[k], u[k], ca[k], d, input[k], fired[k]);
+        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, grow32_of(A, tg[k]), x[k], u[k], ca[k], d, input[k], fired[k], pull,
+                             pushed[k]);
         d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
     }
     if (A.input) {
@@ -425,6 +461,12 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     st_f<V>(A.delta[0] + i, d0);
     st_f<V>(A.delta[1] + i, d1);
     st_f<V>(A.delta[2] + i, d2);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        if (fired[v]) {
+            push_spike32(A, D, kstep, step, i + v);
+        }
+    }
 }
 
 // H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
@@ -438,10 +480,10 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* 
     const uint32_t tid = blockIdx.x * BLOCK + threadIdx.x;
     const uint32_t stride = gridDim.x * BLOCK;
     for (uint32_t g = tid; g < groups; g += stride) {
-        neurons_f32<H, V, MULTI, MODEL>(A, D, step, g * V);
+        neurons_f32<H, V, MULTI, MODEL>(A, D, k, step, g * V);
     }
     if (V > 1 && tid < A.n - groups * V) {
-        neurons_f32<H, 1, MULTI, MODEL>(A, D, step, groups * V + tid);
+        neurons_f32<H, 1, MULTI, MODEL>(A, D, k, step, groups * V + tid);
     }
 }
 
@@ -1455,6 +1497,8 @@ Act32 act32_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fir
     A.net_of = c.net_of.p;
     A.blocks = c.net_blocks.p;
     A.num_blocks = c.num_net_blocks;
+    A.syn_in[0] = c.syn_in32[0].p;
+    A.syn_in[1] = c.syn_in32[1].p;
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;

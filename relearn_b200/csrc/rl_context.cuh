@@ -235,9 +235,18 @@ struct PhaseScope {
 struct ActDesc {
     uint32_t base_step;
     uint32_t has_edges;
-    const uint32_t* off;
+    const uint32_t* off;  // in-CSR
     const uint32_t* src;
     const int32_t* w;
+    // Steps of the block.  Its first step pulls each neuron's synaptic sum
+    // over the in-CSR; a neuron whose spike flag is set at a step before the
+    // block's last adds its out-edges' weights (out-CSR: out_off, out_perm into
+    // tgt and w) to its targets' sums of the next step, which that step reads
+    // and clears.  Integer sums: the same values in any order.
+    uint32_t block_len;
+    const uint32_t* out_off;
+    const uint32_t* out_perm;
+    const uint32_t* tgt;
 };
 
 // Launch shape of the Barnes-Hut search kernels.
@@ -294,6 +303,10 @@ struct Ctx {
     cudaStream_t own_stream = nullptr;  // the context's own stream
     PhaseTimer timer;
     DBuf<ActDesc> act_desc;
+    // synaptic sums pushed by the spikes of a step, by step parity (FP64 form:
+    // syn_in64, FP32 form: syn_in32); zero at every block boundary
+    DBuf<long long> syn_in64[2];
+    DBuf<int32_t> syn_in32[2];
     cudaGraphExec_t act_graph[2] = { nullptr, nullptr };  // per fired-buffer parity
     uint32_t act_graph_len = 0;
     uint32_t act_block_len = 0;  // steps of the activity block being issued: only its last step stores the input
@@ -375,6 +388,10 @@ void remember_act_tuning(const Ctx& c);
 bool recall_act_tuning(Ctx& c);
 // Releases the captured activity intervals (they are captured again on use).
 void drop_activity_graphs(Ctx& c);
+// The pushed synaptic sums (ActDesc): allocated (zero) before the first block
+// with synapses; cleared after steps that are undone.
+void ensure_syn_in(Ctx& c);
+void clear_syn_in(Ctx& c);
 // Blocks of an activity launch of variant v of `kernel`.
 unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel);
 
