@@ -496,13 +496,19 @@ __global__ void __launch_bounds__(1024, 1) k_search_hot(SearchArgs A, uint32_t h
 
 // ------------------------------------------------- one search per warp
 // (bh_wide.cuh): the FP64 evaluation, search and kernel.
+// Both signal types' search lists in one launch: the tasks of S[0] (the
+// excitatory list) first, then those of S[1]; a type without searches has no
+// tasks.  Every search waits on memory round after round, so the lists of the
+// two types share the device instead of running one launch after the other.
 struct WideArgs {
-    SearchArgs S;
+    SearchArgs S[2];
+    uint32_t num_tasks[2];
     WideSlot all;        // scratch of every warp slot, `cap` entries each
     uint32_t cap;
     uint32_t slots;
-    uint32_t* tasks;     // task counter of this signal type
-    uint32_t* overflow;  // searches left to the packet kernel
+    uint32_t* tasks;     // task counter over both lists
+    uint32_t* overflow;  // per type: searches left to the packet kernel
+    unsigned long long* touched;
 };
 
 __device__ __forceinline__ WideSlot wide_slot(const WideSlot& all, uint64_t off) {
@@ -510,11 +516,10 @@ __device__ __forceinline__ WideSlot wide_slot(const WideSlot& all, uint64_t off)
 }
 
 // The FP64 candidates of the subtree of `sub` in visiting order.
-__device__ __forceinline__ int64_t wide_collect64(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t sub, double sx, double sy,
-                                                  double sz, uint32_t source, uint32_t* s_round, uint32_t& touched) {
-    const SearchArgs& S = A.S;
+__device__ __forceinline__ int64_t wide_collect64(const SearchArgs& S, uint32_t cap, const WideSlot& P, const WarpNet& W, uint32_t sub, double sx,
+                                                  double sy, double sz, uint32_t source, uint32_t* s_round, uint32_t& touched) {
     const uint4 sm = __ldg(&S.meta[sub]);
-    return wide_collect(P, A.cap, sm.x, inner_children(sm), s_round, touched, [&](uint32_t nd) {
+    return wide_collect(P, cap, sm.x, inner_children(sm), s_round, touched, [&](uint32_t nd) {
         WideEval r{ ST_DISCARD, 0.0, 0u, 0u, false };
         if (nd >= S.num_nodes) {
             r.bad = true;
@@ -535,9 +540,8 @@ __device__ __forceinline__ int64_t wide_collect64(const WideArgs& A, const WideS
 
 // One search (one vacant axon element j of `source`) by the whole warp:
 // the target neuron, -1 when the search fails, kRedo when it did not fit.
-__device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpNet& W, uint32_t source, uint32_t j, uint32_t* s_round,
+__device__ int32_t wide_search(const SearchArgs& S, uint32_t cap, const WideSlot& P, const WarpNet& W, uint32_t source, uint32_t j, uint32_t* s_round,
                                uint32_t& touched) {
-    const SearchArgs& S = A.S;
     const double sx = S.px[source], sy = S.py[source], sz = S.pz[source];
     uint32_t sub = W.root;
     for (uint32_t depth = 0; depth <= (uint32_t)kMaxLevels + 2u; ++depth) {
@@ -545,7 +549,7 @@ __device__ int32_t wide_search(const WideArgs& A, const WideSlot& P, const WarpN
         if (topo_leaf(sm.y)) {
             return depth == 0 ? -1 : (int32_t)sm.x;
         }
-        const int64_t got = wide_collect64(A, P, W, sub, sx, sy, sz, source, s_round, touched);
+        const int64_t got = wide_collect64(S, cap, P, W, sub, sx, sy, sz, source, s_round, touched);
         if (got == -1) {
             return kRedo;
         }
@@ -595,9 +599,9 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide(WideArgs A) {
         return;  // whole warp
     }
     uint32_t* s_round = s_round_all[wib];
-    const SearchArgs& S = A.S;
     const WideSlot P = wide_slot(A.all, (uint64_t)slot * A.cap);
-    const uint32_t total_tasks = S.seg_warp[S.num_segs] * 32u;
+    const uint32_t total0 = A.num_tasks[0];
+    const uint32_t total_tasks = total0 + A.num_tasks[1];
     uint32_t touched = 0;
     for (;;) {
         uint32_t task = 0;
@@ -608,31 +612,33 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide(WideArgs A) {
         if (task >= total_tasks) {
             break;
         }
+        const int t = task < total0 ? 0 : 1;
+        const SearchArgs& S = A.S[t];
         uint32_t lo = 0;
         uint64_t idx = 0;
-        if (!wide_task_entry(task, S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, lo, idx)) {
+        if (!wide_task_entry(task - (t ? total0 : 0u), S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, lo, idx)) {
             continue;
         }
         const NetInfo& N = S.nets[S.seg_net[lo]];
         const WarpNet W{ N.theta, N.scale, N.seed, S.seg_net[lo], N.first };
         int32_t result = -1;
         if (!N.root_leaf) {
-            result = wide_search(A, P, W, S.list_src[idx], S.list_j[idx], s_round, touched);
+            result = wide_search(S, A.cap, P, W, S.list_src[idx], S.list_j[idx], s_round, touched);
         }
         if (lane == 0) {
             S.target[idx] = result;
             if (result == kRedo) {
-                atomicAdd(A.overflow, 1u);
+                atomicAdd(A.overflow + t, 1u);
             }
         }
         __syncwarp();
     }
-    unsigned long long t = touched;
+    unsigned long long sum = touched;
     for (int o = 16; o > 0; o >>= 1) {
-        t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+        sum += __shfl_down_sync(0xFFFFFFFFu, sum, o);
     }
     if (lane == 0) {
-        atomicAdd(S.touched, t);
+        atomicAdd(A.touched, sum);
     }
 }
 
@@ -772,45 +778,52 @@ WideSlot wide_scratch(Ctx& c, uint32_t slots, uint32_t cap) {
     return WideSlot{ S.w_node.p, S.w_info.p, S.w_child.p, S.w_cnt.p, S.w_pos.p, S.w_ord_node.p, S.w_w.p, S.w_ord_w.p };
 }
 
-// Whether the tuner times a candidate shape on this context: the
-// one-search-per-warp form pays off on large networks only.
+// Whether the tuner times a candidate shape on this context's search list:
+// the one-search-per-warp form pays off on large networks with sparse lists
+// only (on a dense list its scratch would hold a warp slot per resident warp
+// for nothing: packets of Morton neighbours are several times faster there).
 bool search_variant_applies(const Ctx& c, const SearchVariant& v) {
-    return v.packet != 0 || c.n >= kWideMinNeurons;
+    return v.packet != 0 || (c.n >= kWideMinNeurons && search_density_class(c.n, c.search.num_searches) != 0);
 }
 
 namespace {
 
-// The one-search-per-warp kernel on signal type t's list; searches that did
-// not fit their warp's scratch are redone by the packet kernel (which writes
-// every target of the list again).
-void launch_wide(Ctx& c, const SearchArgs& a, uint32_t warps, int t, const SearchVariant& v) {
+// The one-search-per-warp kernel on both signal types' lists (warps[t]
+// packet-layout warps of type t, 0 for a type without searches); a type with
+// searches that did not fit their warp's scratch is redone by the packet
+// kernel (which writes every target of its list again).
+void launch_wide(Ctx& c, const SearchArgs (&a)[2], const uint32_t (&warps)[2]) {
     constexpr int WPB = 4;
     Search& S = c.search;
     cudaStream_t st = c.stream;
-    const uint32_t tasks = warps * 32u;
+    const uint32_t tasks = (warps[0] + warps[1]) * 32u;
     const uint32_t cap = wide_cap(c);
     const uint32_t slots = std::min<uint32_t>(tasks, (uint32_t)c.num_sms * kWideWarpsPerSM);
     S.w_overflow.ensure(2);
-    RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p + t, 0, sizeof(uint32_t), st));
-    RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p + t, 0, sizeof(uint32_t), st));
+    RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p, 0, sizeof(uint32_t), st));
+    RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p, 0, 2 * sizeof(uint32_t), st));
     WideArgs A;
-    A.S = a;
+    for (int t = 0; t < 2; ++t) {
+        A.S[t] = a[t];
+        A.num_tasks[t] = warps[t] * 32u;
+    }
     A.all = wide_scratch(c, slots, cap);
     A.cap = cap;
     A.slots = slots;
-    A.tasks = S.tasks.p + t;
-    A.overflow = S.w_overflow.p + t;
+    A.tasks = S.tasks.p;
+    A.overflow = S.w_overflow.p;
+    A.touched = reinterpret_cast<unsigned long long*>(c.counters.p);
     k_search_wide<WPB><<<(slots + WPB - 1) / WPB, WPB * 32, 0, st>>>(A);
     RL_LAUNCH_CHECK();
-    uint32_t over = 0;
-    RL_CUDA_TRY(cudaMemcpyAsync(&over, S.w_overflow.p + t, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    uint32_t over[2] = { 0, 0 };
+    RL_CUDA_TRY(cudaMemcpyAsync(over, S.w_overflow.p, sizeof(over), cudaMemcpyDeviceToHost, st));
     RL_CUDA_TRY(cudaStreamSynchronize(st));
-    if (over) {
-        const SearchVariant fb{ 2, 32, 1, 0 };
-        k_search<2, 32, 1><<<(warps + fb.warps - 1) / fb.warps, fb.warps * 32, 0, st>>>(a);
-        RL_LAUNCH_CHECK();
+    for (int t = 0; t < 2; ++t) {
+        if (over[t]) {
+            k_search<2, 32, 1><<<(warps[t] + 1) / 2, 64, 0, st>>>(a[t]);
+            RL_LAUNCH_CHECK();
+        }
     }
-    (void)v;
 }
 
 }  // namespace
@@ -954,7 +967,7 @@ void run_search(Ctx& c, uint32_t step) {
             uint32_t segs = 0;
         };
         SearchLaunch launches[2];
-        SearchArgs args[2];
+        SearchArgs args[2] = {};
         for (int t = 0; t < 2; ++t) {
             const uint64_t base = t == 0 ? 0 : num_exc;
             const uint64_t total = t == 0 ? num_exc : num_inh;
@@ -1017,6 +1030,16 @@ void run_search(Ctx& c, uint32_t step) {
             A.kernel = c.kernel;
         }
         auto launch_all = [&](const SearchVariant& v) {
+            if (v.packet == 0) {
+                // one search per warp: both types in one launch
+                const uint32_t w[2] = { launches[0].on ? launches[0].warps : 0u, launches[1].on ? launches[1].warps : 0u };
+                if (is_fp32(c)) {
+                    launch_search_wide_f32(c, w, launches[0].segs, launches[1].segs, step);
+                } else {
+                    launch_wide(c, args, w);
+                }
+                return;
+            }
             for (int t = 0; t < 2; ++t) {
                 if (!launches[t].on) {
                     continue;
@@ -1027,8 +1050,6 @@ void run_search(Ctx& c, uint32_t step) {
                 if (is_fp32(c)) {
                     launch_search_f32(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, launches[t].segs, launches[t].warps, step, v,
                                       S.tasks.p + t);
-                } else if (v.packet == 0) {
-                    launch_wide(c, args[t], launches[t].warps, t, v);
                 } else if (v.hot > 0) {
                     const HotKernel kern = fp64_hot_kernel(v);
                     const uint32_t hot = hot_nodes(c, v, sizeof(double4) + sizeof(uint4) + sizeof(double));

@@ -1151,18 +1151,19 @@ __global__ void __launch_bounds__(1024, 1) k_search_f32_hot(Search32 A, uint32_t
 
 // One search per warp (bh_wide.cuh) in the FP32 form: the same visiting
 // order and the same Kahan sums as the packet kernels, so the same targets.
+// Both signal types' lists in one launch (the FP64 form's WideArgs).
 struct WideArgs32 {
-    Search32 S;
+    Search32 S[2];
+    uint32_t num_tasks[2];
     WideSlot all;
     uint32_t cap;
     uint32_t slots;
     uint32_t* tasks;
-    uint32_t* overflow;
+    uint32_t* overflow;  // per type
 };
 
-__device__ int32_t wide_search32(const WideArgs32& A, const WideSlot& P, const Net32& W, const QPos& sp, uint32_t source, uint32_t j,
+__device__ int32_t wide_search32(const Search32& S, uint32_t cap, const WideSlot& P, const Net32& W, const QPos& sp, uint32_t source, uint32_t j,
                                  uint32_t* s_round) {
-    const Search32& S = A.S;
     uint32_t touched = 0;
     uint32_t sub = W.root;
     for (uint32_t depth = 0; depth <= (uint32_t)kMaxLevels + 2u; ++depth) {
@@ -1171,7 +1172,7 @@ __device__ int32_t wide_search32(const WideArgs32& A, const WideSlot& P, const N
             return depth == 0 ? -1 : (int32_t)sm.x;
         }
         auto collect = [&](bool fb) {
-            return wide_collect(P, A.cap, sm.x, inner_children32(sm), s_round, touched, [&](uint32_t nd) {
+            return wide_collect(P, cap, sm.x, inner_children32(sm), s_round, touched, [&](uint32_t nd) {
                 WideEval r{ S_DISCARD, 0.0, 0u, 0u, false };
                 if (nd >= S.num_nodes) {
                     r.bad = true;
@@ -1230,11 +1231,11 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide32(WideArgs32 A) {
     if (slot >= A.slots) {
         return;  // whole warp
     }
-    const Search32& S = A.S;
     const uint64_t off = (uint64_t)slot * A.cap;
     const WideSlot P{ A.all.node + off, A.all.info + off, A.all.child + off, A.all.cnt + off, A.all.pos + off, A.all.ord_node + off, A.all.w + off,
                       A.all.ord_w + off };
-    const uint32_t total_tasks = S.seg_warp[S.num_segs] * 32u;
+    const uint32_t total0 = A.num_tasks[0];
+    const uint32_t total_tasks = total0 + A.num_tasks[1];
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) {
@@ -1244,9 +1245,11 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide32(WideArgs32 A) {
         if (task >= total_tasks) {
             break;
         }
+        const int t = task < total0 ? 0 : 1;
+        const Search32& S = A.S[t];
         uint32_t seg = 0;
         uint64_t idx = 0;
-        if (!wide_task_entry(task, S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, seg, idx)) {
+        if (!wide_task_entry(task - (t ? total0 : 0u), S.seg_warp, S.seg_begin, S.seg_end, S.num_segs, seg, idx)) {
             continue;
         }
         const NetInfo& N = S.nets[S.seg_net[seg]];
@@ -1257,12 +1260,12 @@ __global__ void __launch_bounds__(WPB * 32, 2) k_search_wide32(WideArgs32 A) {
             const QFrame& F = N.frame;
             const QPos sp{ quantize(S.px[source], F.origin[0], F.inv_quantum), quantize(S.py[source], F.origin[1], F.inv_quantum),
                            quantize(S.pz[source], F.origin[2], F.inv_quantum) };
-            result = wide_search32(A, P, W, sp, source, S.list_j[idx], s_round_all[wib]);
+            result = wide_search32(S, A.cap, P, W, sp, source, S.list_j[idx], s_round_all[wib]);
         }
         if (lane == 0) {
             S.target[idx] = result;
             if (result == kRedo) {
-                atomicAdd(A.overflow, 1u);
+                atomicAdd(A.overflow + t, 1u);
             }
         }
         __syncwarp();
@@ -1594,8 +1597,11 @@ void pack_tree_f32(Ctx& c) {
     T.recq_valid = true;
 }
 
-void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
-                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v, uint32_t* tasks) {
+namespace {
+
+// The FP32 search arguments of signal type `type`'s list.
+Search32 search32_args(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
+                       uint32_t num_segs, uint32_t step, uint32_t* tasks) {
     Search32 A;
     A.rec = c.tree.recq[type].p;
     A.meta = c.tree.meta.p;
@@ -1619,6 +1625,14 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
     A.step = step;
     A.err = c.err.p;
     A.kernel = Kernel32{ c.kernel.type, c.kernel.cutoff_inf, (float)c.kernel.k_minus_1, (float)c.kernel.a, (float)c.kernel.b, (float)c.kernel.cutoff };
+    return A;
+}
+
+}  // namespace
+
+void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
+                       uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v, uint32_t* tasks) {
+    const Search32 A = search32_args(c, type, seg_warp, seg_begin, seg_end, seg_net, num_segs, step, tasks);
     if (v.hot > 0) {
         const auto kern = v.packet == 16 ? &k_search_f32_hot<16> : &k_search_f32_hot<32>;
         const uint32_t hot = hot_nodes(c, v, 2 * sizeof(uint4));
@@ -1629,33 +1643,49 @@ void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_
         RL_LAUNCH_CHECK();
         return;
     }
-    if (v.packet == 0) {
-        // one search per warp; searches that did not fit are redone by the packet kernel
-        constexpr int WPB = 4;
-        Search& S = c.search;
-        const uint32_t cap = wide_cap(c);
-        const uint32_t slots = std::min<uint32_t>(warps * 32u, (uint32_t)c.num_sms * kWideWarpsPerSM);
-        S.w_overflow.ensure(2);
-        RL_CUDA_TRY(cudaMemsetAsync(tasks, 0, sizeof(uint32_t), c.stream));
-        RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p + type, 0, sizeof(uint32_t), c.stream));
-        WideArgs32 W{ A, wide_scratch(c, slots, cap), cap, slots, tasks, S.w_overflow.p + type };
-        k_search_wide32<WPB><<<(slots + WPB - 1) / WPB, WPB * 32, 0, c.stream>>>(W);
-        RL_LAUNCH_CHECK();
-        uint32_t over = 0;
-        RL_CUDA_TRY(cudaMemcpyAsync(&over, S.w_overflow.p + type, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
-        RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
-        if (!over) {
-            return;
-        }
-        k_search_f32<2, 32, 1><<<(warps + 1) / 2, 64, 0, c.stream>>>(A);
-        RL_LAUNCH_CHECK();
-        return;
-    }
+    RL_CHECK(v.packet != 0, RL_ERR_INVALID, "one search per warp runs both types at once (launch_search_wide_f32)");
     const Search32Kernel kern = fp32_search_kernel(v);
     RL_CHECK(kern != nullptr, RL_ERR_INVALID, "no such search variant");
     const unsigned blocks = (warps + v.warps - 1) / v.warps;
     kern<<<blocks, v.warps * 32, 0, c.stream>>>(A);
     RL_LAUNCH_CHECK();
+}
+
+// One search per warp over both signal types' lists (warps[t] packet-layout
+// warps of type t, 0 for a type without searches, num_segs[t] segments in
+// c.search.seg_*[t]); a type with searches that did not fit their warp's
+// scratch is redone by the packet kernel.
+void launch_search_wide_f32(Ctx& c, const uint32_t (&warps)[2], uint32_t segs0, uint32_t segs1, uint32_t step) {
+    constexpr int WPB = 4;
+    Search& S = c.search;
+    const uint32_t segs[2] = { segs0, segs1 };
+    WideArgs32 W;
+    for (int t = 0; t < 2; ++t) {
+        W.S[t] = warps[t] ? search32_args(c, t, S.seg_warp[t].p, S.seg_begin[t].p, S.seg_end[t].p, S.seg_net[t].p, segs[t], step, S.tasks.p + t)
+                          : Search32{};
+        W.num_tasks[t] = warps[t] * 32u;
+    }
+    const uint32_t cap = wide_cap(c);
+    const uint32_t slots = std::min<uint32_t>((warps[0] + warps[1]) * 32u, (uint32_t)c.num_sms * kWideWarpsPerSM);
+    S.w_overflow.ensure(2);
+    RL_CUDA_TRY(cudaMemsetAsync(S.tasks.p, 0, sizeof(uint32_t), c.stream));
+    RL_CUDA_TRY(cudaMemsetAsync(S.w_overflow.p, 0, 2 * sizeof(uint32_t), c.stream));
+    W.all = wide_scratch(c, slots, cap);
+    W.cap = cap;
+    W.slots = slots;
+    W.tasks = S.tasks.p;
+    W.overflow = S.w_overflow.p;
+    k_search_wide32<WPB><<<(slots + WPB - 1) / WPB, WPB * 32, 0, c.stream>>>(W);
+    RL_LAUNCH_CHECK();
+    uint32_t over[2] = { 0, 0 };
+    RL_CUDA_TRY(cudaMemcpyAsync(over, S.w_overflow.p, sizeof(over), cudaMemcpyDeviceToHost, c.stream));
+    RL_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    for (int t = 0; t < 2; ++t) {
+        if (over[t]) {
+            k_search_f32<2, 32, 1><<<(warps[t] + 1) / 2, 64, 0, c.stream>>>(W.S[t]);
+            RL_LAUNCH_CHECK();
+        }
+    }
 }
 
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w) {

@@ -288,7 +288,7 @@ uint32_t wide_cap(const Ctx& c);
 WideSlot wide_scratch(Ctx& c, uint32_t slots, uint32_t cap);
 // one-search-per-warp form: walk entries per warp, warps per SM, smallest network
 constexpr uint32_t kWideCap = 6144;
-constexpr uint32_t kWideWarpsPerSM = 8;
+constexpr uint32_t kWideWarpsPerSM = 16;
 constexpr uint32_t kWideMinNeurons = 65536;
 uint32_t hot_nodes(const Ctx& c, const SearchVariant& v, size_t node_bytes);
 const std::vector<ActVariant>& act_variants();
@@ -432,6 +432,8 @@ uint64_t run_commit_f32(Ctx& c, int type);
 void pack_tree_f32(Ctx& c);
 void launch_search_f32(Ctx& c, int type, const uint32_t* seg_warp, const uint64_t* seg_begin, const uint64_t* seg_end, const uint32_t* seg_net,
                        uint32_t num_segs, uint32_t warps, uint32_t step, const SearchVariant& v, uint32_t* tasks);
+// One search per warp over both signal types' lists at once.
+void launch_search_wide_f32(Ctx& c, const uint32_t (&warps)[2], uint32_t segs0, uint32_t segs1, uint32_t step);
 void candidate_weights(Ctx& c, uint32_t source, int precision, std::vector<uint32_t>& nodes, std::vector<double>& w);
 
 // activity.cu
