@@ -37,14 +37,29 @@ sys.path.insert(0, ROOT)
 N_DEFAULT = 1_000_000
 SIDE_DEFAULT = 10_000.0
 PERIOD = 100
-# algorithmic bytes of the fused activity kernel per neuron-step (FP64 SoA,
-# one target calcium for all neurons, so no per-neuron target is read):
-# reads enabled 1 + x 8 + u 8 + calcium 8 + 3 deltas 24 = 49,
-# writes x 8 + u 8 + fired 1 + calcium 8 + 3 deltas 24 = 49,
-# and the input (8) on the last step of each 100-step block only
-ACT_BYTES_PER_NEURON = 98 + 8 / 100
-ACT_BYTES_PER_EDGE = 9  # pull over in-edges: source id 4 + weight 4 + fired flag 1
-ACT_BYTES_CSR_ROW = 8   # two row offsets when the graph is not empty
+# Algorithmic bytes per neuron-step of one launch per step (a network with
+# synapses, or step fusion off), FP64 SoA, one target calcium for all neurons:
+# the step kernel reads enabled 1 + x 8 + u 8 and writes x 8 + u 8 + spike
+# flag 1 + spike-history byte 1 = 35; calcium and growth of a 100-step chunk
+# (one launch) read each history byte (1) and read and write calcium 8 and
+# three deltas 24 once per chunk (64 / 100); the input (8) on the last step of
+# each block only.
+ACT_BYTES_PER_NEURON = 35 + 1 + (64 + 8) / 100
+# With synapses: a block's first step pulls over the in-CSR (two row offsets 8
+# per neuron, source id 4 + weight 4 + spike flag 1 per in-edge); the other
+# steps read the pushed sum (8 B FP64, 4 B FP32) of every neuron (the pushes
+# of the about 1 % of neurons that fire, along their out-edges, not counted).
+ACT_BYTES_PER_EDGE = 9
+ACT_BYTES_CSR_ROW = 8
+ACT_BYTES_PUSHED = {0: 8, 1: 4}
+
+
+def step_bytes(precision: int, n: int, edges: float) -> float:
+    """Algorithmic bytes of one activity step of n neurons, one launch per step."""
+    b = (ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32) * n
+    if edges:
+        b += ACT_BYTES_PUSHED[precision] * n * (PERIOD - 1) / PERIOD + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges) / PERIOD
+    return b
 
 
 def peaks():
@@ -300,9 +315,11 @@ def fused_roofline(precision: int, n: int, step_us: float, act_cnt: int, sm_mhz,
     return roof
 
 
-# reads enabled 1 + x 4 + u 4 + calcium 8 + 3 deltas 12; writes x 4 + u 4 + fired 1 + calcium 8 + 3 deltas 12;
-# the input (4) on the last step of each 100-step block only
-ACT_BYTES_FP32 = 58 + 4 / 100
+# FP32: the step kernel reads enabled 1 + spike flag 1 + x 4 + u 4 and writes
+# x 4 + u 4 + spike flag 1 + history byte 1 = 20; the chunk's calcium and
+# growth read each history byte (1) and calcium 8 + three deltas 12, read and
+# written once per chunk (40 / 100); the input (4) on a block's last step
+ACT_BYTES_FP32 = 20 + 1 + (40 + 4) / 100
 
 
 def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None):
@@ -352,8 +369,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     value = replica_value(world, n * PERIOD * args.steps, total_ms)
     act_ms, act_cnt = phases["activity_kernel"]
     edges = int(net.stats().get("synapses_created", 0))
-    per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
-    bytes_per_launch = int(round(per_neuron * n + (ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges if edges else 0)))
+    bytes_per_launch = int(round(step_bytes(precision, n, edges)))
     hbm, peak_kind = peaks()
     achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
     # DRAM bytes per launch from one ncu capture of the same kernel on this
@@ -610,12 +626,15 @@ def synapse_regime(args, dev, stream, world, precision):
     act_ms, act_cnt = phases["activity_kernel"]
     edges = 0.5 * (edges_before + edges_after)
     per_neuron = ACT_BYTES_PER_NEURON if precision == 0 else ACT_BYTES_FP32
-    bytes_per_launch = per_neuron * n + ACT_BYTES_CSR_ROW * n + ACT_BYTES_PER_EDGE * edges
+    bytes_per_launch = step_bytes(precision, n, edges)
     act_achieved = bytes_per_launch / (act_ms / act_cnt / 1e3) / 1e9 if act_cnt else 0.0
     act_roof = {"bound": "hbm", "kernel": "k_activity" if precision == 0 else "k_activity_f32", "achieved": act_achieved, "peak": hbm,
                 "unit": "GB/s", "frac": act_achieved / hbm, "peak_kind": peak_kind, "bytes_per_launch": bytes_per_launch,
                 "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None, "launches": act_cnt,
-                "bytes": f"{per_neuron:.2f} B per neuron-step + {ACT_BYTES_CSR_ROW} B row offsets per neuron + {ACT_BYTES_PER_EDGE} B per in-edge"}
+                "bytes": f"{per_neuron:.2f} B per neuron-step + {ACT_BYTES_PUSHED[precision]} B pushed sum per neuron-step + per 100-step block "
+                         f"{ACT_BYTES_CSR_ROW} B row offsets per neuron and {ACT_BYTES_PER_EDGE} B per in-edge",
+                "kernels": "the step kernel (k_activity / k_activity_f32, one launch per step) and the chunk's calcium and growth (k_calcium_growth / "
+                           "k_calcium_growth_f32, one launch per 100 steps)"}
     searches = s1["searches"] - s0["searches"]
     touched = s1["nodes_touched"] - s0["nodes_touched"]
     search_ms = phases["search_kernel"][0]

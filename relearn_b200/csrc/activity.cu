@@ -51,6 +51,8 @@ struct ActArgs {
     const NetBlock* blocks;  // a batched context's neurons in blocks of one network
     uint32_t num_blocks;
     long long* syn_in[2];  // pushed synaptic sums by step parity (ActDesc)
+    uint8_t* hist;         // spike history (kHistSteps rows of hist_stride bytes)
+    size_t hist_stride;
     // a context with one network: its seed and growth rates (the kernel then
     // reads no network table)
     uint64_t seed1;
@@ -385,13 +387,13 @@ __device__ __forceinline__ void push_spike(const ActArgs& A, const ActDesc* __re
     }
 }
 
-// One enabled neuron's step on state already in registers (loaded before
-// the kernel's draw phase).  `z` is the neuron's standard normal draw of this
-// step.
+// One enabled neuron's input and model step on state already in registers
+// (loaded before the kernel's draw phase); `z` is the neuron's standard normal
+// draw of this step.  Calcium and growth follow from the spike history at the
+// end of the chunk (k_calcium_growth).
 template <int H, int MODEL>
-__device__ __forceinline__ uint8_t activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, const Nu& nu,
-                                                        double z, long long isum, double xv, double uv, double ca, double tgt, double d0, double d1,
-                                                        double d2) {
+__device__ __forceinline__ uint8_t activity_neuron_regs(const ActArgs& A, uint32_t step, uint32_t i, uint64_t seed, uint32_t local, double z,
+                                                        long long isum, double xv, double uv) {
     const double input = step_input(A, isum, z);
     if (A.input) {
         A.input[i] = input;
@@ -400,11 +402,6 @@ __device__ __forceinline__ uint8_t activity_neuron_regs(const ActArgs& A, uint32
     A.x[i] = xv;
     A.u[i] = uv;
     A.fired_cur[i] = spiked;
-    ca = calcium_step<H>(A, spiked, ca);
-    A.calcium[i] = ca;
-    A.delta0[i] = d0 + growth_step(A, 0, ca, tgt, nu);
-    A.delta1[i] = d1 + growth_step(A, 1, ca, tgt, nu);
-    A.delta2[i] = d2 + growth_step(A, 2, ca, tgt, nu);
     return spiked;
 }
 
@@ -440,7 +437,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
         uint64_t seed[V];
         uint32_t local[V];
         Nu nu[V];
-        double p[V], z[V], xv[V], uv[V], cav[V], tg[V], d0[V], d1[V], d2[V];
+        double p[V], z[V], xv[V], uv[V];
         long long isum[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
@@ -450,19 +447,14 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             local[v] = 0;
             nu[v] = Nu{ { 0.0, 0.0, 0.0 } };
             p[v] = 0.5;
-            xv[v] = uv[v] = cav[v] = tg[v] = d0[v] = d1[v] = d2[v] = 0.0;
+            xv[v] = uv[v] = 0.0;
             isum[v] = 0;
             if (i[v] < A.n) {
-                d0[v] = A.delta0[i[v]];
-                d1[v] = A.delta1[i[v]];
-                d2[v] = A.delta2[i[v]];
                 isum[v] = synaptic_sum_k(A, D, k, step, i[v], on[v]);
             }
             if (on[v]) {
                 xv[v] = A.x[i[v]];
                 uv[v] = A.u[i[v]];
-                cav[v] = A.calcium[i[v]];
-                tg[v] = A.uniform_target ? 0.0 : A.target[i[v]];
                 neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
                 p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
             }
@@ -505,53 +497,42 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
             spike[v] = 0;
         }
         if constexpr (V == 2 && MODEL == RL_MODEL_IZHIKEVICH && H > 0) {
-            if (A.uniform_target) {
-                // both neurons' steps in one stretch without branches, so that
-                // the compiler interleaves their chains of FP64 operations
-                double in[V];
-                uint8_t sp[V];
+            // both neurons' steps in one stretch without branches, so that
+            // the compiler interleaves their chains of FP64 operations
+            double in[V];
+            uint8_t sp[V];
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    in[v] = step_input(A, isum[v], z[v]);
-                    sp[v] = izhikevich_frozen<H>(A, in[v], xv[v], uv[v]);
-                }
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    calcium_growth_flat<H, MULTI>(A, sp[v], nu[v], cav[v], d0[v], d1[v], d2[v]);
-                }
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    if (on[v]) {
-                        if (A.input) {
-                            A.input[i[v]] = in[v];
-                        }
-                        A.x[i[v]] = xv[v];
-                        A.u[i[v]] = uv[v];
-                        A.fired_cur[i[v]] = sp[v];
-                        A.calcium[i[v]] = cav[v];
-                        A.delta0[i[v]] = d0[v];
-                        A.delta1[i[v]] = d1[v];
-                        A.delta2[i[v]] = d2[v];
-                        spike[v] = sp[v];
-                    }
-                }
-                done = true;
+            for (int v = 0; v < V; ++v) {
+                in[v] = step_input(A, isum[v], z[v]);
+                sp[v] = izhikevich_frozen<H>(A, in[v], xv[v], uv[v]);
             }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (on[v]) {
+                    if (A.input) {
+                        A.input[i[v]] = in[v];
+                    }
+                    A.x[i[v]] = xv[v];
+                    A.u[i[v]] = uv[v];
+                    A.fired_cur[i[v]] = sp[v];
+                    spike[v] = sp[v];
+                }
+            }
+            done = true;
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             if (on[v] && !done) {
-                spike[v] = activity_neuron_regs<H, MODEL>(A, step, i[v], seed[v], local[v], nu[v], z[v], isum[v], xv[v], uv[v], cav[v], tg[v],
-                                                          d0[v], d1[v], d2[v]);
+                spike[v] = activity_neuron_regs<H, MODEL>(A, step, i[v], seed[v], local[v], z[v], isum[v], xv[v], uv[v]);
             } else if (!on[v] && i[v] < A.n) {
                 if (A.input) {
                     A.input[i[v]] = 0.0;
                 }
                 spike[v] = A.fired_prev[i[v]];  // a disabled neuron keeps its flag (and its targets still read it)
                 A.fired_cur[i[v]] = spike[v];
-                A.delta0[i[v]] = d0[v] + 0.0;
-                A.delta1[i[v]] = d1[v] + 0.0;
-                A.delta2[i[v]] = d2[v] + 0.0;
+            }
+            if (on[v]) {
+                A.hist[(k % kHistSteps) * A.hist_stride + i[v]] = spike[v];
             }
         }
         // the spikes' pushes last, with the neurons' state already stored
@@ -561,6 +542,57 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 push_spike(A, D, k, step, i[v]);
             }
         }
+    }
+}
+
+// Calcium and the growth deltas of the last m steps (a chunk of one launch per
+// step) from the spike history: row j holds the spike flags of the chunk's
+// step j.  A neuron's calcium and growth read nothing but its own spike flags,
+// so they run here once per chunk with the state in registers instead of in
+// every step's launch; the operations and their order are those of one step
+// after the other, so the bits are the same.  A disabled neuron keeps its
+// calcium, and its deltas become d + 0 (as at each of its steps).
+template <int H, bool MULTI>
+__global__ void __launch_bounds__(256) k_calcium_growth(ActArgs A, uint32_t m) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) {
+        return;
+    }
+    double d0 = A.delta0[i], d1 = A.delta1[i], d2 = A.delta2[i];
+    if (A.enabled[i]) {
+        uint64_t seed;
+        uint32_t local;
+        Nu nu;
+        neuron_net<MULTI>(A, i, seed, local, nu);
+        double ca = A.calcium[i];
+        const uint8_t* __restrict__ h = A.hist + i;
+        bool flat = false;
+        if constexpr (H > 0) {
+            if (A.uniform_target) {
+#pragma unroll 4
+                for (uint32_t j = 0; j < m; ++j) {
+                    calcium_growth_flat<H, MULTI>(A, h[j * A.hist_stride], nu, ca, d0, d1, d2);
+                }
+                flat = true;
+            }
+        }
+        if (!flat) {
+            const double tgt = A.uniform_target ? 0.0 : A.target[i];
+            for (uint32_t j = 0; j < m; ++j) {
+                ca = calcium_step<H>(A, h[j * A.hist_stride], ca);
+                d0 = d0 + growth_step(A, 0, ca, tgt, nu);
+                d1 = d1 + growth_step(A, 1, ca, tgt, nu);
+                d2 = d2 + growth_step(A, 2, ca, tgt, nu);
+            }
+        }
+        A.calcium[i] = ca;
+        A.delta0[i] = d0;
+        A.delta1[i] = d1;
+        A.delta2[i] = d2;
+    } else {
+        A.delta0[i] = d0 + 0.0;
+        A.delta1[i] = d1 + 0.0;
+        A.delta2[i] = d2 + 0.0;
     }
 }
 
@@ -938,6 +970,8 @@ ActArgs act64_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* f
     A.num_blocks = c.num_net_blocks;
     A.syn_in[0] = c.syn_in64[0].p;
     A.syn_in[1] = c.syn_in64[1].p;
+    A.hist = c.spike_hist.p;
+    A.hist_stride = hist_stride(c.n);
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
@@ -1013,6 +1047,19 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     } else {
         launch_act64<0>(c, v, A, kstep);
     }
+}
+
+// Calcium and growth of the last m steps of one launch per step.
+void launch_calcium_growth64(Ctx& c, uint32_t m) {
+    const ActArgs A = act64_args(c, 0, nullptr, nullptr);
+    const unsigned grid = blocks_for(c.n, 256);
+    const bool h10 = c.cfg.h_model == 10 && c.cfg.h_calcium == 10;
+    if (c.multi()) {
+        (h10 ? k_calcium_growth<10, true> : k_calcium_growth<0, true>)<<<grid, 256, 0, c.stream>>>(A, m);
+    } else {
+        (h10 ? k_calcium_growth<10, false> : k_calcium_growth<0, false>)<<<grid, 256, 0, c.stream>>>(A, m);
+    }
+    RL_LAUNCH_CHECK();
 }
 
 // The whole block of nsteps steps in one launch (a network without synapses).
@@ -1165,6 +1212,22 @@ void ensure_syn_in(Ctx& c) {
     clear_syn_in(c);
 }
 
+void ensure_spike_hist(Ctx& c) {
+    const size_t need = hist_stride(c.n) * kHistSteps;
+    if (c.spike_hist.p == nullptr || c.spike_hist.n < need) {
+        c.spike_hist.alloc(need);
+        drop_activity_graphs(c);  // captured launches hold the kernel arguments
+    }
+}
+
+void launch_calcium_growth(Ctx& c, uint32_t m) {
+    if (is_fp32(c)) {
+        launch_calcium_growth32(c, m);
+    } else {
+        launch_calcium_growth64(c, m);
+    }
+}
+
 void clear_syn_in(Ctx& c) {
     for (int p = 0; p < 2; ++p) {
         if (c.syn_in64[p].p) {
@@ -1199,6 +1262,9 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     k_set_desc<<<1, 1, 0, c.stream>>>(c.act_desc.p, v);
     RL_LAUNCH_CHECK();
     const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;
+    if (!fused) {
+        ensure_spike_hist(c);
+    }
     // the launch shape is a shape of the per-step kernel: it is timed at the
     // first block that runs one launch per step (with the synapses it will
     // read), not while blocks run as one fused launch
@@ -1211,6 +1277,14 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         drop_activity_graphs(c);
     }
     const bool graph = !fused && c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
+    // one launch per step, and calcium and growth of each chunk of kHistSteps
+    // steps from the spike history at the chunk's end
+    auto step_and_growth = [&](uint32_t k) {
+        launch_step(c, k);
+        if ((k + 1) % kHistSteps == 0 || k + 1 == nsteps) {
+            launch_calcium_growth(c, k % kHistSteps + 1);
+        }
+    };
     if (fused) {
         // no synapses: every neuron's steps are independent of the others'
         PhaseScope ps(c, PH_ACTIVITY_KERNEL, nsteps);
@@ -1237,7 +1311,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
             c.capturing = true;
             try {
                 for (uint32_t k = 0; k < nsteps; ++k) {
-                    launch_step(c, k);
+                    step_and_growth(k);
                 }
             } catch (...) {
                 c.capturing = false;
@@ -1265,7 +1339,7 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     } else {
         for (uint32_t k = 0; k < nsteps; ++k) {
             PhaseScope ps(c, PH_ACTIVITY_KERNEL);
-            launch_step(c, k);
+            step_and_growth(k);
         }
     }
     c.nr.cur ^= (int)(nsteps & 1u);

@@ -84,6 +84,8 @@ struct Act32 {
     const NetBlock* blocks;  // a batched context's neurons in blocks of one network
     uint32_t num_blocks;
     int32_t* syn_in[2];  // pushed synaptic sums by step parity (ActDesc)
+    uint8_t* hist;       // spike history (kHistSteps rows of hist_stride bytes)
+    size_t hist_stride;
     // a context with one network: its seed and growth rates, so that the
     // kernel reads no network table
     uint64_t seed1;
@@ -169,11 +171,28 @@ __device__ __forceinline__ Grow32 grow32_of(const Act32& A, float tgt) {
     return G;
 }
 
+// One step of calcium (FP64: the h substeps' closed form) and of the three
+// growth deltas after the spike flag `spiked`.
+__device__ __forceinline__ void calcium_growth_f32(const Act32& A, uint8_t spiked, const float (&nu)[3], const Grow32& G, double& ca,
+                                                   float (&delta)[3]) {
+    ca = fma(ca, A.ca_mul, spiked ? A.ca_add : 0.0);
+    const float caf = (float)ca;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const float q = (caf - G.xi[t]) * G.iz[t];
+        const float curve = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
+        const float dz = ((G.flat >> t) & 1u) ? (caf == A.eta[t] ? 0.0f : -1.0f) : curve;
+        delta[t] = fmaf(dz, nu[t], delta[t]);
+    }
+}
+
 // `k24`: the neuron's 24 random bits of this step's background draw;
 // `k24p`: 24 bits of its Poisson-threshold draw (Poisson model only).  The
 // synaptic sum is pulled over the in-edges (`pull`, a block's first step) or
-// is `pushed`, what the sources that fired at the step before pushed.
-template <int H, int MODEL, bool EDGES = true>
+// is `pushed`, what the sources that fired at the step before pushed.  GROW
+// false: calcium and growth are left to k_calcium_growth_f32 at the end of the
+// chunk (ca, delta, nu and G are not used).
+template <int H, int MODEL, bool EDGES = true, bool GROW = true>
 __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t i, bool enabled, uint8_t fired_prev, uint32_t k24,
                                            uint32_t k24p, const float (&nu)[3], const Grow32& G, float& x, float& u, double& ca, float (&delta)[3],
                                            float& input, uint8_t& fired, bool pull = true, int pushed = 0) {
@@ -264,14 +283,8 @@ __device__ __forceinline__ void neuron_f32(const Act32& A, const ActDesc* __rest
     x = xv;
     u = uv;
     fired = spiked;
-    ca = fma(ca, A.ca_mul, spiked ? A.ca_add : 0.0);
-    const float caf = (float)ca;
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-        const float q = (caf - G.xi[t]) * G.iz[t];
-        const float curve = fmaf(2.0f, ex2_approx(-q * q), -1.0f);
-        const float dz = ((G.flat >> t) & 1u) ? (caf == A.eta[t] ? 0.0f : -1.0f) : curve;
-        delta[t] = fmaf(dz, nu[t], delta[t]);
+    if (GROW) {
+        calcium_growth_f32(A, spiked, nu, G, ca, delta);
     }
 }
 
@@ -381,8 +394,7 @@ template <int H, int V, bool MULTI, int MODEL>
 __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __restrict__ D, uint32_t kstep, uint32_t step, uint32_t i) {
     uint8_t en[V], fp[V], fired[V];
     uint16_t net[V];
-    float x[V], u[V], d0[V], d1[V], d2[V], input[V];
-    double ca[V];
+    float x[V], u[V], input[V];
     ld_b<V>(A.enabled + i, en);
     ld_b<V>(A.fired_prev + i, fp);
     if (MULTI) {
@@ -390,14 +402,6 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     }
     ld_f<V>(A.x + i, x);
     ld_f<V>(A.u + i, u);
-    ld_d<V>(A.calcium + i, ca);
-    ld_f<V>(A.delta[0] + i, d0);
-    ld_f<V>(A.delta[1] + i, d1);
-    ld_f<V>(A.delta[2] + i, d2);
-    float tg[V] = {};
-    if (A.target) {
-        ld_f<V>(A.target + i, tg);
-    }
     // the sums pushed at the step before (read and cleared; a block's first
     // step pulls instead)
     const bool pull = kstep == 0;
@@ -439,17 +443,12 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     }
 #pragma unroll
     for (int k = 0; k < V; ++k) {
-        float d[3] = { d0[k], d1[k], d2[k] };
-        float nu[3] = { A.nu1[0], A.nu1[1], A.nu1[2] };  // growth rates in registers (the network's own when batched)
-        if (MULTI) {
-            const NetInfo& N = A.nets[net[k]];
-            nu[0] = N.nu32[0];
-            nu[1] = N.nu32[1];
-            nu[2] = N.nu32[2];
-        }
-        neuron_f32<H, MODEL>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, grow32_of(A, tg[k]), x[k], u[k], ca[k], d, input[k], fired[k], pull,
-                             pushed[k]);
-        d0[k] = d[0], d1[k] = d[1], d2[k] = d[2];
+        const float nu[3] = { 0.0f, 0.0f, 0.0f };  // calcium and growth: k_calcium_growth_f32
+        double ca = 0.0;
+        float d[3] = { 0.0f, 0.0f, 0.0f };
+        const Grow32 G{};
+        neuron_f32<H, MODEL, true, false>(A, D, i + k, en[k] != 0, fp[k], k24[k], k24p[k], nu, G, x[k], u[k], ca, d, input[k], fired[k], pull,
+                                          pushed[k]);
     }
     if (A.input) {
         st_f<V>(A.input + i, input);
@@ -457,10 +456,7 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
     st_b<V>(A.fired_cur + i, fired);
     st_f<V>(A.x + i, x);
     st_f<V>(A.u + i, u);
-    st_d<V>(A.calcium + i, ca);
-    st_f<V>(A.delta[0] + i, d0);
-    st_f<V>(A.delta[1] + i, d1);
-    st_f<V>(A.delta[2] + i, d2);
+    st_b<V>(A.hist + (kstep % kHistSteps) * A.hist_stride + i, fired);  // a disabled neuron's entry is not read
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         if (fired[v]) {
@@ -603,6 +599,37 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
             neuron_steps_f32<H, false, MODEL>(A, D, nsteps, fired_before_last, i, i < A.n, i, true, A.nu1, A.rk0, A.rk1);
         }
     }
+}
+
+// Calcium and the growth deltas of the last m steps of one launch per step
+// from the spike history (row j: the chunk's step j), with the state in
+// registers: the same function and order as step by step, so the same bits.
+// A disabled neuron keeps its calcium and deltas.
+template <bool MULTI>
+__global__ void __launch_bounds__(256) k_calcium_growth_f32(Act32 A, uint32_t m) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n || !A.enabled[i]) {
+        return;
+    }
+    float nu[3] = { A.nu1[0], A.nu1[1], A.nu1[2] };
+    if (MULTI) {
+        const NetInfo& N = A.nets[A.net_of[i]];
+        nu[0] = N.nu32[0];
+        nu[1] = N.nu32[1];
+        nu[2] = N.nu32[2];
+    }
+    const Grow32 G = grow32_of(A, A.target ? A.target[i] : 0.0f);
+    double ca = A.calcium[i];
+    float d[3] = { A.delta[0][i], A.delta[1][i], A.delta[2][i] };
+    const uint8_t* __restrict__ h = A.hist + i;
+#pragma unroll 4
+    for (uint32_t j = 0; j < m; ++j) {
+        calcium_growth_f32(A, h[j * A.hist_stride], nu, G, ca, d);
+    }
+    A.calcium[i] = ca;
+    A.delta[0][i] = d[0];
+    A.delta[1][i] = d[1];
+    A.delta[2][i] = d[2];
 }
 
 // ElementBaseBase::update with an FP32 delta.
@@ -1502,6 +1529,8 @@ Act32 act32_args(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uint8_t* fir
     A.num_blocks = c.num_net_blocks;
     A.syn_in[0] = c.syn_in32[0].p;
     A.syn_in[1] = c.syn_in32[1].p;
+    A.hist = c.spike_hist.p;
+    A.hist_stride = hist_stride(c.n);
     A.seed1 = c.nets[0].seed;
     for (int r = 0; r < 10; ++r) {
         A.rk0[r] = (uint32_t)A.seed1 + (uint32_t)r * 0x9E3779B9u;
@@ -1562,6 +1591,17 @@ void launch_activity_f32_steps(Ctx& c, uint32_t nsteps) {
     } else {
         launch_steps32<0>(c, A, nsteps, before_last);
     }
+}
+
+void launch_calcium_growth32(Ctx& c, uint32_t m) {
+    const Act32 A = act32_args(c, 0, nullptr, nullptr);
+    const unsigned grid = blocks_for(c.n, 256);
+    if (c.multi()) {
+        k_calcium_growth_f32<true><<<grid, 256, 0, c.stream>>>(A, m);
+    } else {
+        k_calcium_growth_f32<false><<<grid, 256, 0, c.stream>>>(A, m);
+    }
+    RL_LAUNCH_CHECK();
 }
 
 void launch_commit_f32(Ctx& c, int type, unsigned long long* total, const unsigned long long* guard, int guard_n) {

@@ -200,6 +200,16 @@ struct NetInfo {
     QFrame frame;
 };
 
+// Steps whose calcium and growth one launch computes from the spike history
+// when the activity runs one launch per step.  A row of the history holds one
+// byte per neuron and is padded to a multiple of 16 bytes, so that a thread's
+// vector store of its V flags (V = 1, 2, 4 from a multiple of V) is aligned
+// in every row.
+constexpr uint32_t kHistSteps = 128;
+inline size_t hist_stride(uint32_t n) {
+    return ((size_t)n + 15) / 16 * 16;
+}
+
 // A block of at most kNetBlock neurons of one network: [first, first + count).
 constexpr uint32_t kNetBlock = 128;
 struct NetBlock {
@@ -307,6 +317,10 @@ struct Ctx {
     // syn_in64, FP32 form: syn_in32); zero at every block boundary
     DBuf<long long> syn_in64[2];
     DBuf<int32_t> syn_in32[2];
+    // one launch per step: the spike flags of up to kHistSteps steps (row k:
+    // step k of the chunk, one byte per neuron), from which calcium and the
+    // growth deltas of the chunk are computed at its end
+    DBuf<uint8_t> spike_hist;
     cudaGraphExec_t act_graph[2] = { nullptr, nullptr };  // per fired-buffer parity
     uint32_t act_graph_len = 0;
     uint32_t act_block_len = 0;  // steps of the activity block being issued: only its last step stores the input
@@ -392,6 +406,12 @@ void drop_activity_graphs(Ctx& c);
 // with synapses; cleared after steps that are undone.
 void ensure_syn_in(Ctx& c);
 void clear_syn_in(Ctx& c);
+// The spike history of one launch per step (allocated before the first such
+// block), and calcium and growth of the last m steps from it.
+void ensure_spike_hist(Ctx& c);
+void launch_calcium_growth(Ctx& c, uint32_t m);
+void launch_calcium_growth64(Ctx& c, uint32_t m);
+void launch_calcium_growth32(Ctx& c, uint32_t m);
 // Blocks of an activity launch of variant v of `kernel`.
 unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel);
 
