@@ -215,15 +215,19 @@ def build_network(n, side, seed, placement):
 # sources have changed since is reported with "stale": true until it is
 # captured again.
 CAPTURED = {
-    # dram__bytes_read.sum + dram__bytes_write.sum of one per-step activity
-    # launch at 1M neurons (bench.py --case activity --step-fusion 0): FP64
-    # 49.03 + 0.60 MB, FP32 30.03 + 0.03 MB; FP64 warp instructions of one
-    # per-step k_activity launch (DMUL, DADD, DFMA, DSETP: 9.98 per
-    # neuron-step).  The FP64 pipe of an SM takes 2 warp instructions per
-    # cycle (64 lanes).
-    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "bdfa4a271091a59c",
-                   "traffic": 49.03e6 + 0.60e6, "fp64_warp_instr_per_neuron": 9.98},
-    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "traffic": 30.03e6 + 0.03e6},
+    # one launch per step at 1M neurons with synapses (bench.py --case
+    # plasticity --step-fusion 0, a launch of the second block): the step
+    # kernel's DRAM read + write per launch plus that of the chunk's calcium
+    # and growth launch per step (FP64 34.94 + 0.10 MB + (133.04 + 14.67) / 100
+    # MB; FP32 23.74 + 0.00 MB + (121.02 + 9.42) / 100 MB); FP64 warp
+    # instructions per neuron-step of both (DMUL, DADD, DFMA, DSETP: 6.26 +
+    # 3.72), and for the FP32 form warp instructions of every kind (7.99 +
+    # 1.25).  The FP64 pipe of an SM takes 2 warp instructions per cycle (64
+    # lanes).
+    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "6ae1210c4a75dc83",
+                   "traffic": 34.94e6 + 0.10e6 + (133.04e6 + 14.67e6) / 100, "fp64_warp_instr_per_neuron": 9.97},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818",
+                   "traffic": 23.74e6 + (121.02e6 + 9.42e6) / 100, "warp_instr_per_neuron": 9.23},
     # the fused block kernels (a network without synapses: a block of steps per
     # launch, state in registers), from the instruction mix of one 100-step
     # launch at 1M neurons (bench.py --case activity --case-steps 100), per
@@ -231,15 +235,20 @@ CAPTURED = {
     # DADD 3.55, DFMA 1.82, DSETP 0.92); k_activity_f32_steps 5.85 warp
     # instructions of every kind, issued at one per SM sub-partition (4 per
     # SM) per cycle; DRAM read + write of that launch
-    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "bdfa4a271091a59c", "fp64_warp_instr_per_neuron": 10.08,
-                "traffic": 50.06e6 + 4.50e6},
-    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.17e6},
+    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "6ae1210c4a75dc83", "fp64_warp_instr_per_neuron": 10.08,
+                "traffic": 50.06e6 + 4.35e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.01e6},
+    # the batched block kernel over the 128-network configuration (7.15M
+    # neurons, bench.py --case ensemble --case-steps 100 --precision fp32):
+    # warp instructions per neuron-step, DRAM read + write of the launch
+    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "warp_instr_per_neuron": 5.95,
+                   "traffic": 215.94e6 + 189.96e6},
     # the search snapshot at 1M (bench.py --case search; the excitatory pass,
     # 0.8M searches): lanes active per warp instruction, L1 / L2 hit rates of
     # the walk, DRAM bytes per search
-    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "ec16784ac6a68489", "lanes_active": 19.85,
+    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "3ba2b94c4a357fb7", "lanes_active": 19.85,
                  "l1_hit": 0.924, "l2_hit": 0.774, "dram_bytes_per_search": 681.0},
-    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "5449da2e1537de31", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.938},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
 }
 B200_SMS = 148
 # algorithmic memory of a fused block launch per neuron: reads enabled, spike
@@ -315,6 +324,26 @@ def fused_roofline(precision: int, n: int, step_us: float, act_cnt: int, sm_mhz,
     return roof
 
 
+def step_compute(precision: int, n: int, step_us: float, sm_mhz=None) -> dict:
+    """The compute side of one launch per step (step kernel + the chunk's
+    calcium and growth) from the captured instruction counts: FP64 lane
+    operations against the FP64 pipe (FP64 form), warp instructions against
+    the issue rate (FP32 form)."""
+    mhz = sm_mhz or 1965.0
+    cap = captured("activity64" if precision == 0 else "activity32")
+    if precision == 0:
+        lane_ops = cap["fp64_warp_instr_per_neuron"] * 32
+        achieved = lane_ops * n / (step_us * 1e-6) / 1e12
+        peak = 64 * B200_SMS * mhz * 1e6 / 1e12
+        return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "T FP64 lane-op/s", "frac": achieved / peak,
+                "ops_per_neuron_step": lane_ops, "stale": cap["stale"], "peak_kind": "nominal: 64 FP64 lanes per SM x 148 SMs at %g MHz" % mhz}
+    achieved = cap["warp_instr_per_neuron"] * n / (step_us * 1e-6) / 1e12
+    peak = 4 * B200_SMS * mhz * 1e6 / 1e12
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "T warp-inst/s", "frac": achieved / peak,
+            "warp_instr_per_neuron_step": cap["warp_instr_per_neuron"], "stale": cap["stale"],
+            "peak_kind": "nominal: 1 warp instruction per SM sub-partition per cycle x 592 at %g MHz" % mhz}
+
+
 # FP32: the step kernel reads enabled 1 + spike flag 1 + x 4 + u 4 and writes
 # x 4 + u 4 + spike flag 1 + history byte 1 = 20; the chunk's calcium and
 # growth read each history byte (1) and calcium 8 + three deltas 12, read and
@@ -376,7 +405,7 @@ def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None
     # workload: reads equal the algorithmic read bytes, writes stay in L2
     # during the launch
     cap = captured("activity64" if precision == 0 else "activity32")
-    traffic = cap["traffic"] if (n == 1_000_000 and args.placement == "uniform" and not edges) else None
+    traffic = cap["traffic"] if (n == 1_000_000 and args.placement == "uniform") else None  # captured at 1M with synapses
     if args.step_fusion and not edges and act_cnt:
         # no synapses: each 100-step block ran as one launch of the fused kernel
         sm_mhz = clk.summary().get("sm_mhz") if clk is not None else None
@@ -635,6 +664,13 @@ def synapse_regime(args, dev, stream, world, precision):
                          f"{ACT_BYTES_CSR_ROW} B row offsets per neuron and {ACT_BYTES_PER_EDGE} B per in-edge",
                 "kernels": "the step kernel (k_activity / k_activity_f32, one launch per step) and the chunk's calcium and growth (k_calcium_growth / "
                            "k_calcium_growth_f32, one launch per 100 steps)"}
+    if act_cnt:
+        comp = step_compute(precision, n, 1e3 * act_ms / act_cnt)
+        act_roof["compute"] = comp
+        if comp["frac"] > act_roof["frac"]:
+            # the arithmetic side is the nearer bound: report it first
+            act_roof = dict(comp, kernel=act_roof["kernel"], kernels=act_roof["kernels"], avg_launch_us=act_roof["avg_launch_us"],
+                            launches=act_cnt, hbm={k: act_roof[k] for k in ("achieved", "peak", "unit", "frac", "peak_kind", "bytes_per_launch", "bytes")})
     searches = s1["searches"] - s0["searches"]
     touched = s1["nodes_touched"] - s0["nodes_touched"]
     search_ms = phases["search_kernel"][0]
@@ -731,11 +767,25 @@ def ensemble_figure(args, dev, stream, world, rank):
     hbm, peak_kind = peaks()
     ens.close()
     step_us = 1e3 * act_ms / steps
-    bytes_per_step = ACT_BYTES_FP32 * total
-    roof = {"bound": "hbm", "kernel": "k_activity_f32 / k_activity_f32_steps", "achieved": bytes_per_step / (step_us * 1e-6) / 1e9, "peak": hbm,
-            "unit": "GB/s", "frac": bytes_per_step / (step_us * 1e-6) / 1e9 / hbm, "peak_kind": peak_kind, "bytes_per_step": bytes_per_step,
-            "avg_step_us": step_us, "activity_launches": act_cnt,
-            "note": "per activity step over the whole run: fused 100-step blocks while no network has synapses, one launch per step after"}
+    if st["synapses_created"] == 0 and args.step_fusion:
+        # no network formed a synapse: every block ran as one launch of the
+        # batched block kernel, bound by instruction issue
+        cap = captured("ensemble32")
+        mhz = 1965.0
+        achieved = cap["warp_instr_per_neuron"] * total / (step_us * 1e-6) / 1e12
+        peak = 4 * B200_SMS * mhz * 1e6 / 1e12
+        roof = {"bound": "issue", "kernel": "k_activity_f32_steps (batched: thread blocks of one network)", "achieved": achieved, "peak": peak,
+                "unit": "T warp-inst/s", "frac": achieved / peak, "warp_instr_per_neuron_step": cap["warp_instr_per_neuron"], "stale": cap["stale"],
+                "peak_kind": "nominal: 1 warp instruction per SM sub-partition per cycle x 592 at 1965 MHz", "avg_step_us": step_us,
+                "traffic": cap["traffic"], "traffic_unit": "bytes per 100-step launch (ncu dram read + write)",
+                "hbm": {"bytes_per_launch": FUSED_BYTES[1] * total, "achieved": FUSED_BYTES[1] * total / (step_us * PERIOD * 1e-6) / 1e9, "peak": hbm,
+                        "unit": "GB/s", "frac": FUSED_BYTES[1] * total / (step_us * PERIOD * 1e-6) / 1e9 / hbm, "peak_kind": peak_kind}}
+    else:
+        bytes_per_step = step_bytes(1, total, 0)
+        roof = {"bound": "hbm", "kernel": "k_activity_f32 / k_activity_f32_steps", "achieved": bytes_per_step / (step_us * 1e-6) / 1e9, "peak": hbm,
+                "unit": "GB/s", "frac": bytes_per_step / (step_us * 1e-6) / 1e9 / hbm, "peak_kind": peak_kind, "bytes_per_step": bytes_per_step,
+                "avg_step_us": step_us, "activity_launches": act_cnt,
+                "note": "per activity step over the whole run: fused 100-step blocks while no network has synapses, one launch per step after"}
     return {"metric": "neuron-steps/s", "value": world * total * steps / (ms / 1e3), "unit": "neuron-steps/s", "networks": len(nets),
             "neurons": total, "steps": steps, "steps_of_config": 5000, "precision": "fp32", "timed": "steps 1..%d of a fresh context" % steps,
             "synapses_created": st["synapses_created"], "searches": st["searches"], "roofline": roof,
@@ -1026,9 +1076,25 @@ def run_case(args):
     snapshot (one vacant axon and dendrite of each type per neuron, or a vacant
     axon on --search-sources random neurons only) once;
     `plasticity` seeds 0-3 elements per type and runs two plasticity periods
-    (100 activity steps + 1 plasticity update each)."""
+    (100 activity steps + 1 plasticity update each); `ensemble` runs
+    --case-steps activity steps of the batched configuration (--ensemble-networks
+    networks; the bench measures it in the FP32 form, --precision fp32)."""
     import relearn_b200 as R
 
+    if args.case == "ensemble":
+        from relearn_b200 import workloads
+
+        nets = ensemble_spec(args.ensemble_networks, 7)
+        base = R.default_params(1, 1.0)
+        base["precision"] = 1 if args.precision == "fp32" else 0
+        ens = R.Network(base, networks=nets)
+        ens.set_positions(np.concatenate([workloads.uniform_cube(d["num_neurons"], d["side"], 900 + k) for k, d in enumerate(nets)]),
+                          np.concatenate([workloads.signal_types(d["num_neurons"], 900 + k) for k, d in enumerate(nets)]))
+        ens.set_step_fusion(bool(args.step_fusion))
+        ens.activity_block(1, args.case_steps)
+        ens.synchronize()
+        print(json.dumps({"case": args.case, "networks": len(nets), "neurons": int(sum(d["num_neurons"] for d in nets)), "stats": ens.stats()}))
+        return
     params, pos, sig = build_network(args.neurons, args.side, args.seed, args.placement)
     params["precision"] = 1 if args.precision == "fp32" else 0
     net = R.Network(params)
@@ -1093,7 +1159,7 @@ def main():
                     help="1: blocks of activity steps of a network without synapses in one launch (default); 0: one launch per step")
     ap.add_argument("--case-steps", type=int, default=4, help="activity steps of --case activity")
     ap.add_argument("--search-sources", type=int, default=0, help="--case search: vacant axons on this many random neurons (0: on every neuron)")
-    ap.add_argument("--case", choices=["activity", "search", "plasticity"], default=None,
+    ap.add_argument("--case", choices=["activity", "search", "plasticity", "ensemble"], default=None,
                     help="run a small profiling case of one kernel instead of the benchmark")
     args = ap.parse_args()
     world, rank, local = dist_setup()
