@@ -190,48 +190,6 @@ __global__ void k_new_keys(uint64_t m, const uint32_t* __restrict__ hi, const ui
     }
 }
 
-// Sorts up to kSmallSort (key, value) pairs in one block: a bitonic network on
-// (key, value) — the values are distinct, so the order is total and equal keys
-// keep the order of their values (insertion order).
-constexpr uint32_t kSmallSort = 4096;
-__global__ void __launch_bounds__(1024) k_small_sort(uint64_t* key, uint32_t* val, uint32_t m) {
-    __shared__ uint64_t sk[kSmallSort];
-    __shared__ uint32_t sv[kSmallSort];
-    uint32_t p2 = 1;
-    while (p2 < m) {
-        p2 <<= 1;
-    }
-    for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
-        sk[i] = i < m ? key[i] : ~0ull;
-        sv[i] = i < m ? val[i] : 0xFFFFFFFFu;
-    }
-    __syncthreads();
-    for (uint32_t size = 2; size <= p2; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
-                const uint32_t j = i ^ stride;
-                if (j > i) {
-                    const bool up = (i & size) == 0;
-                    const bool greater = sk[i] > sk[j] || (sk[i] == sk[j] && sv[i] > sv[j]);
-                    if (greater == up) {
-                        const uint64_t tk = sk[i];
-                        sk[i] = sk[j];
-                        sk[j] = tk;
-                        const uint32_t tv = sv[i];
-                        sv[i] = sv[j];
-                        sv[j] = tv;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-        key[i] = sk[i];
-        val[i] = sv[i];
-    }
-}
-
 // Old entries (sorted by (target, source)) into the merged list.
 __global__ void k_merge_old(uint64_t m, const uint32_t* __restrict__ t, const uint32_t* __restrict__ src, const int32_t* __restrict__ w,
                             const uint64_t* __restrict__ nkey, uint64_t mn, int bn, uint32_t* __restrict__ pos, uint32_t* __restrict__ t_out,
@@ -549,16 +507,11 @@ int bits_for(uint64_t v) {
 // The new entries' keys sorted with their values (insertion order among
 // equal keys): one block for a plasticity update's few thousand, the radix
 // sort beyond that.
+// Stable sort of the new entries' keys (values: insertion index, or merged
+// positions increasing with it among equal keys, so equal keys keep their
+// insertion order); up to 4,096 entries in one launch.
 void sort_new(Ctx& c, uint64_t* key, uint32_t* val, uint64_t m, int bits) {
-    if (m <= 1) {
-        return;
-    }
-    if (m <= kSmallSort) {
-        k_small_sort<<<1, 1024, 0, c.stream>>>(key, val, (uint32_t)m);
-        RL_LAUNCH_CHECK();
-    } else {
-        radix_sort_u64(key, val, m, bits, c.prim, c.stream);
-    }
+    radix_sort_u64(key, val, m, bits, c.prim, c.stream);
 }
 
 }  // namespace

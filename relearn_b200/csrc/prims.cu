@@ -94,6 +94,31 @@ __global__ void scan_sums_single(uint32_t* sums, uint32_t m) {
     }
 }
 
+// An array of at most one tile in one launch: the exclusive scan and its
+// total (in and out may be the same array).
+__global__ void scan_one_tile(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* __restrict__ total_out) {
+    const uint64_t base = (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) {
+            out[base + k] = run;
+        }
+        run += v[k];
+    }
+    if (threadIdx.x == 0) {
+        *total_out = total;
+    }
+}
+
 __global__ void scan_apply(const uint32_t* in, uint32_t* out, uint64_t n, const uint32_t* __restrict__ sums) {
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
@@ -193,9 +218,128 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter(const K* __restric
     }
 }
 
+// Up to kSmallRadix pairs are sorted by one block with the pairs in shared
+// memory: the same 8-bit passes and the same stable order as the multi-block
+// sort (a pass counts the digits, scans the 256 counts, and scatters rounds of
+// kSmallThreads consecutive keys, ranking equal digits by their position), so
+// the same permutation, in one launch instead of five per pass.
+constexpr uint32_t kSmallRadix = 4096;
+constexpr int kSmallThreads = 1024;
+
+template <typename K>
+__global__ void __launch_bounds__(kSmallThreads) radix_small(K* keys, uint32_t* vals, uint32_t n, int passes) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    K* ka = reinterpret_cast<K*>(smem);
+    K* kb = ka + kSmallRadix;
+    uint32_t* va = reinterpret_cast<uint32_t*>(kb + kSmallRadix);
+    uint32_t* vb = va + kSmallRadix;
+    __shared__ uint32_t run[256];
+    __shared__ uint32_t wsum[8];
+    __shared__ uint32_t wc[kSmallThreads / 32][256];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    for (uint32_t i = tid; i < n; i += kSmallThreads) {
+        ka[i] = keys[i];
+        va[i] = vals[i];
+    }
+    for (int e = tid; e < (kSmallThreads / 32) * 256; e += kSmallThreads) {
+        wc[e >> 8][e & 255] = 0u;
+    }
+    __syncthreads();
+    K* kin = ka;
+    K* kout = kb;
+    uint32_t* vin = va;
+    uint32_t* vout = vb;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        if (tid < 256) {
+            run[tid] = 0u;
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += kSmallThreads) {
+            atomicAdd(&run[(uint32_t)(kin[i] >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        // exclusive scan of the 256 digit counts by the first eight warps
+        uint32_t cnt = 0, inc = 0;
+        if (tid < 256) {
+            cnt = run[tid];
+            inc = warp_inclusive_scan(cnt);
+            if (lane == 31) {
+                wsum[warp] = inc;
+            }
+        }
+        __syncthreads();
+        if (tid < 256) {
+            uint32_t before = 0;
+            for (int w = 0; w < warp; ++w) {
+                before += wsum[w];
+            }
+            run[tid] = before + inc - cnt;
+        }
+        __syncthreads();
+        for (uint32_t base = 0; base < n; base += kSmallThreads) {
+            const uint32_t i = base + (uint32_t)tid;
+            const bool valid = i < n;
+            K k = 0;
+            uint32_t v = 0;
+            uint32_t d = 256u;
+            if (valid) {
+                k = kin[i];
+                v = vin[i];
+                d = (uint32_t)(k >> shift) & 255u;
+            }
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+            const uint32_t lrank = __popc(peers & lt_mask);
+            if (valid && lrank == 0) {
+                wc[warp][d] = __popc(peers);
+            }
+            __syncthreads();
+            if (valid) {
+                uint32_t off = run[d];
+                for (int w = 0; w < warp; ++w) {
+                    off += wc[w][d];
+                }
+                kout[off + lrank] = k;
+                vout[off + lrank] = v;
+            }
+            __syncthreads();
+            if (tid < 256) {
+                uint32_t tsum = 0;
+#pragma unroll 8
+                for (int w = 0; w < kSmallThreads / 32; ++w) {
+                    tsum += wc[w][tid];
+                    wc[w][tid] = 0u;
+                }
+                run[tid] += tsum;
+            }
+            __syncthreads();
+        }
+        K* tk = kin;
+        kin = kout;
+        kout = tk;
+        uint32_t* tv = vin;
+        vin = vout;
+        vout = tv;
+    }
+    for (uint32_t i = tid; i < n; i += kSmallThreads) {
+        keys[i] = kin[i];
+        vals[i] = vin[i];
+    }
+}
+
 template <typename K>
 void radix_sort_impl(K* keys, uint32_t* vals, uint64_t n, int bits, DBuf<K>& ktmp, PrimScratch& s, cudaStream_t st) {
     if (n <= 1 || bits <= 0) {
+        return;
+    }
+    if (n <= kSmallRadix) {
+        const size_t smem = (size_t)kSmallRadix * 2 * (sizeof(K) + sizeof(uint32_t));
+        RL_CUDA_TRY(cudaFuncSetAttribute((const void*)&radix_small<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        radix_small<K><<<1, kSmallThreads, smem, st>>>(keys, vals, (uint32_t)n, (bits + 7) / 8);
+        RL_LAUNCH_CHECK();
         return;
     }
     const uint32_t num_tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
@@ -233,6 +377,11 @@ uint32_t* exclusive_scan_u32_async(const uint32_t* in, uint32_t* out, uint64_t n
     const uint32_t tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
     const uint32_t t = tiles ? tiles : 1;
     s.c.ensure((size_t)t + 1);
+    if (tiles == 1) {
+        scan_one_tile<<<1, kScanThreads, 0, st>>>(in, out, n, s.c.p + 1);
+        RL_LAUNCH_CHECK();
+        return s.c.p + 1;
+    }
     if (n > 0) {
         scan_tile_sums<<<t, kScanThreads, 0, st>>>(in, n, s.c.p);
         RL_LAUNCH_CHECK();
