@@ -218,16 +218,16 @@ CAPTURED = {
     # one launch per step at 1M neurons with synapses (bench.py --case
     # plasticity --step-fusion 0, a launch of the second block): the step
     # kernel's DRAM read + write per launch plus that of the chunk's calcium
-    # and growth launch per step (FP64 34.94 + 0.10 MB + (133.04 + 14.67) / 100
-    # MB; FP32 23.74 + 0.00 MB + (121.02 + 9.42) / 100 MB); FP64 warp
+    # and growth launch per step (FP64 34.95 + 0.10 MB + (133.06 + 15.09) / 100
+    # MB; FP32 23.75 + 0.00 MB + (121.05 + 9.03) / 100 MB); FP64 warp
     # instructions per neuron-step of both (DMUL, DADD, DFMA, DSETP: 6.26 +
-    # 3.72), and for the FP32 form warp instructions of every kind (7.99 +
-    # 1.25).  The FP64 pipe of an SM takes 2 warp instructions per cycle (64
+    # 3.72), and for the FP32 form warp instructions of every kind (7.98 +
+    # 1.24).  The FP64 pipe of an SM takes 2 warp instructions per cycle (64
     # lanes).
-    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "6ae1210c4a75dc83",
-                   "traffic": 34.94e6 + 0.10e6 + (133.04e6 + 14.67e6) / 100, "fp64_warp_instr_per_neuron": 9.97},
-    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818",
-                   "traffic": 23.74e6 + (121.02e6 + 9.42e6) / 100, "warp_instr_per_neuron": 9.23},
+    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c",
+                   "traffic": 34.95e6 + 0.10e6 + (133.06e6 + 15.09e6) / 100, "fp64_warp_instr_per_neuron": 9.97},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7",
+                   "traffic": 23.75e6 + (121.05e6 + 9.03e6) / 100, "warp_instr_per_neuron": 9.22},
     # the fused block kernels (a network without synapses: a block of steps per
     # launch, state in registers), from the instruction mix of one 100-step
     # launch at 1M neurons (bench.py --case activity --case-steps 100), per
@@ -235,20 +235,20 @@ CAPTURED = {
     # DADD 3.55, DFMA 1.82, DSETP 0.92); k_activity_f32_steps 5.85 warp
     # instructions of every kind, issued at one per SM sub-partition (4 per
     # SM) per cycle; DRAM read + write of that launch
-    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "6ae1210c4a75dc83", "fp64_warp_instr_per_neuron": 10.08,
-                "traffic": 50.06e6 + 4.35e6},
-    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.01e6},
+    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c", "fp64_warp_instr_per_neuron": 10.08,
+                "traffic": 50.07e6 + 3.92e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.12e6},
     # the batched block kernel over the 128-network configuration (7.15M
     # neurons, bench.py --case ensemble --case-steps 100 --precision fp32):
     # warp instructions per neuron-step, DRAM read + write of the launch
-    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "warp_instr_per_neuron": 5.95,
-                   "traffic": 215.94e6 + 189.96e6},
+    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "warp_instr_per_neuron": 5.95,
+                   "traffic": 215.31e6 + 187.62e6},
     # the search snapshot at 1M (bench.py --case search; the excitatory pass,
     # 0.8M searches): lanes active per warp instruction, L1 / L2 hit rates of
     # the walk, DRAM bytes per search
     "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "3ba2b94c4a357fb7", "lanes_active": 19.85,
                  "l1_hit": 0.924, "l2_hit": 0.774, "dram_bytes_per_search": 681.0},
-    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "2d46ac03b96b4818", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
 }
 B200_SMS = 148
 # algorithmic memory of a fused block launch per neuron: reads enabled, spike

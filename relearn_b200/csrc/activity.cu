@@ -430,6 +430,10 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
     }
     __syncthreads();
     const uint32_t stride = gridDim.x * V * BLOCK;
+    // V = 2 in a context with one network: a thread's two neurons are the
+    // even-odd pair 2t, 2t + 1 of its block's 2 BLOCK neurons, whose
+    // background draws of a step are one Philox block (words x, y and z, w)
+    constexpr bool PAIR = V == 2 && !MULTI;
     uint32_t parity = 0;
     for (uint32_t base = blockIdx.x * V * BLOCK; base < A.n; base += stride, parity ^= 1u) {
         uint32_t i[V];
@@ -441,7 +445,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
         long long isum[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            i[v] = base + (uint32_t)v * BLOCK + threadIdx.x;
+            i[v] = base + (PAIR ? 2u * threadIdx.x + (uint32_t)v : (uint32_t)v * BLOCK + threadIdx.x);
             on[v] = i[v] < A.n && A.enabled[i[v]];
             seed[v] = 0;
             local[v] = 0;
@@ -456,7 +460,20 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
                 xv[v] = A.x[i[v]];
                 uv[v] = A.u[i[v]];
                 neuron_net<MULTI>(A, i[v], seed[v], local[v], nu[v]);
-                p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
+                if (!PAIR) {
+                    p[v] = MULTI ? noise_uniform(seed[v], step, local[v]) : noise_uniform_rk(A.rk0, A.rk1, step, local[v]);
+                }
+            }
+        }
+        if constexpr (PAIR) {
+            if (on[0] || on[1]) {
+                const u32x4 r = noise_block_rk(A.rk0, A.rk1, step, i[0]);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    if (on[v]) {
+                        p[v] = ((double)noise_bits53(r, i[v]) + 0.5) * 1.1102230246251565404e-16;  // noise_uniform_rk's open (0, 1)
+                    }
+                }
             }
         }
 #pragma unroll

@@ -467,9 +467,12 @@ __device__ __forceinline__ void neurons_f32(const Act32& A, const ActDesc* __res
 
 // H > 0: h_model fixed at compile time (the loop unrolls); BLOCK threads per
 // block, V neurons per thread, striding over the neurons when the grid is one
-// resident wave.  The last n % V neurons go one per thread.
+// resident wave.  The last n % V neurons go one per thread.  Registers are
+// capped for 1,536 resident threads per SM: the step waits on its loads, and
+// more resident warps hide them (1M neurons with synapses: 15.1 -> 14.4 us per
+// step with the calcium-and-growth replay).
 template <int H, int BLOCK, int V, bool MULTI, int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
+__global__ void __launch_bounds__(BLOCK, 1536 / BLOCK) k_activity_f32(Act32 A, const ActDesc* __restrict__ D, uint32_t k) {
     pdl_wait_then_release();  // every input is the previous step's output
     const uint32_t step = D->base_step + k;
     const uint32_t groups = A.n / V;
