@@ -44,10 +44,12 @@ using Clock = std::chrono::steady_clock;
 // out-edge permutation) and its search and connector entries.  Measured peaks
 // (rl_ctx_memory) over uniform and clustered networks of 2,000 to 4,000,000
 // neurons: 454-555 B per neuron (FP64) and 478-655 B (FP32) at 1.48 octree
-// nodes per neuron, 55-100 B per axon of the bound; the constants below leave
-// headroom for trees of up to 2 nodes per neuron.
+// nodes per neuron, 55-100 B per axon of the bound; one launch per step adds
+// the spike history (128 steps of one byte, rows padded to 16 bytes) and the
+// two pushed-sum arrays (16 B FP64, 8 B FP32) per neuron.  The constants below
+// leave headroom for trees of up to 2 nodes per neuron.
 constexpr double kBaseBytes = 32.0 * 1024 * 1024;
-constexpr double kNeuronBytes[2] = { 600.0, 680.0 };
+constexpr double kNeuronBytes[2] = { 760.0, 830.0 };
 constexpr double kAxonBytes[2] = { 120.0, 160.0 };
 
 uint64_t footprint(const rl_config& base, const rl_network& net, double initial_axons, uint32_t steps) {
