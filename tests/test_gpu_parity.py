@@ -164,6 +164,34 @@ def test_seeded_vacancy_simulation():
     assert st["synapses_deleted"] == so["deleted"]
 
 
+def test_seeded_vacancy_other_substep_counts():
+    """h_model 7 and h_calcium 13 (the kernels with the substep counts as
+    runtime values): the first block runs fused, the later ones one launch per
+    step with calcium and growth replayed from the spike history; every field
+    and the synapse list equal the oracle's bit for bit."""
+    from oracle import oracle as O
+    from relearn_b200 import Network
+
+    n = 2000
+    params, pos, sig = small_network(n, 1000.0, 73)
+    params["h_model"] = 7
+    params["h_calcium"] = 13
+    net = Network(params)
+    net.set_positions(pos, sig)
+    sim = O.OracleSim(oracle_params(params), pos, sig, threads=8)
+    seed_elements(sim, n, 7, 0.0, 3.0)
+    seed_elements(net, n, 7, 0.0, 3.0)
+    net.simulate(1, 601)
+    sim.simulate(1, 601)
+    compare_state(net, sim, n)
+    st = net.stats()
+    so = sim.stats()
+    assert st["synapses_created"] == so["created"] > 0
+    assert st["synapses_deleted"] == so["deleted"]
+    for a, b in zip(net.edges(), sim.edges()):
+        assert np.array_equal(a, b)
+
+
 def test_config0_organic_20001_steps():
     """2,000 neurons in a 1000 um cube, reference parameters, 20,001 steps
     (Simulation::simulate runs number_steps + 1)."""
