@@ -535,6 +535,12 @@ __device__ __forceinline__ int64_t wide_collect64(const SearchArgs& S, uint32_t 
             r.first = mm.x;
         }
         return r;
+    }, [&](uint32_t nd) {
+        if (nd < S.num_nodes) {
+            prefetch_l1(&S.meta[nd]);
+            prefetch_l1(&S.rec[nd]);
+            prefetch_l1(&S.maxdim[nd]);
+        }
     });
 }
 

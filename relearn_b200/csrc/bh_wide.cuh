@@ -69,12 +69,22 @@ __device__ __forceinline__ uint32_t warp_inclusive(uint32_t v) {
     return v;
 }
 
+// L1 prefetch of a global address (no data is returned, nothing waits for it).
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // The candidates of the subtree whose root has k0 children from `first0` on,
 // in visiting order (P.ord_node, weights in P.ord_w): returns their number
 // F, or -1 when a walk entry did not fit, -2 when the walk left the node range
-// or went deeper than any octree.  eval(node) evaluates one node.
-template <class Eval>
-__device__ int64_t wide_collect(const WideSlot& P, uint32_t cap, uint32_t first0, uint32_t k0, uint32_t* s_round, uint32_t& touched, Eval&& eval) {
+// or went deeper than any octree.  eval(node) evaluates one node; pre(node)
+// prefetches what eval will read of it.  Each pass over a round's entries, 32
+// at a time, loads the entries of its next 32 while it works on the current
+// ones (a round's entries are all written before the round starts), so that a
+// step of the walk waits on one memory round trip instead of two.
+template <class Eval, class Pre>
+__device__ int64_t wide_collect(const WideSlot& P, uint32_t cap, uint32_t first0, uint32_t k0, uint32_t* s_round, uint32_t& touched, Eval&& eval,
+                                Pre&& pre) {
     const int lane = threadIdx.x & 31;
     if ((uint32_t)lane < k0) {
         P.node[lane] = first0 + k0 - 1u - (uint32_t)lane;  // children in visiting order: last octant first
@@ -94,14 +104,21 @@ __device__ int64_t wide_collect(const WideSlot& P, uint32_t cap, uint32_t first0
             return -2;
         }
         uint32_t next = re;
+        uint32_t nd_cur = rb + (uint32_t)lane < re ? P.node[rb + (uint32_t)lane] : 0u;
         for (uint32_t base = rb; base < re; base += 32) {
             const uint32_t e = base + (uint32_t)lane;
+            // the next 32 entries lie below re: this round writes only behind re
+            const uint32_t nd_next = e + 32u < re ? P.node[e + 32u] : 0u;
             WideEval ev{ 0, 0.0, 0u, 0u, false };
             if (e < re) {
-                ev = eval(P.node[e]);
+                ev = eval(nd_cur);
                 bad = bad || ev.bad;
                 ++touched;
             }
+            if (e + 32u < re) {
+                pre(nd_next);
+            }
+            nd_cur = nd_next;
             const uint32_t nch = ev.status == 1 ? ev.nch : 0u;
             const uint32_t inc = warp_inclusive(nch);
             const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
@@ -131,12 +148,21 @@ __device__ int64_t wide_collect(const WideSlot& P, uint32_t cap, uint32_t first0
     // bottom-up: candidates below every entry
     for (int r = rounds - 1; r >= 0; --r) {
         const uint32_t rb = s_round[r], re = s_round[r + 1];
+        uint32_t inf_n = 0u, c0_n = 0u;
+        if (rb + (uint32_t)lane < re) {
+            inf_n = P.info[rb + (uint32_t)lane];
+            c0_n = P.child[rb + (uint32_t)lane];
+        }
         for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
-            const uint32_t inf = P.info[e];
+            const uint32_t inf = inf_n;
+            const uint32_t c0 = c0_n;
+            if (e + 32u < re) {
+                inf_n = P.info[e + 32u];
+                c0_n = P.child[e + 32u];
+            }
             const int st = (int)(inf & 3u);
             uint32_t n = st == 2 ? 1u : 0u;
             if (st == 1) {
-                const uint32_t c0 = P.child[e];
                 for (uint32_t c = 0; c < (inf >> 2); ++c) {
                     n += P.cnt[c0 + c];
                 }
@@ -159,8 +185,12 @@ __device__ int64_t wide_collect(const WideSlot& P, uint32_t cap, uint32_t first0
     __syncwarp();
     for (int r = 0; r < rounds; ++r) {
         const uint32_t rb = s_round[r], re = s_round[r + 1];
+        uint32_t inf_n = rb + (uint32_t)lane < re ? P.info[rb + (uint32_t)lane] : 0u;
         for (uint32_t e = rb + (uint32_t)lane; e < re; e += 32) {
-            const uint32_t inf = P.info[e];
+            const uint32_t inf = inf_n;
+            if (e + 32u < re) {
+                inf_n = P.info[e + 32u];
+            }
             const int st = (int)(inf & 3u);
             const uint32_t p = P.pos[e];
             if (st == 2) {

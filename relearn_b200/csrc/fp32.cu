@@ -1217,6 +1217,11 @@ __device__ int32_t wide_search32(const Search32& S, uint32_t cap, const WideSlot
                     r.first = mm.x;
                 }
                 return r;
+            }, [&](uint32_t nd) {
+                if (nd < S.num_nodes) {
+                    prefetch_l1(&S.meta[nd]);
+                    prefetch_l1(&S.rec[nd]);
+                }
             });
         };
         int64_t got = collect(false);
