@@ -226,8 +226,8 @@ CAPTURED = {
     # lanes).
     "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c",
                    "traffic": 34.95e6 + 0.10e6 + (133.06e6 + 15.09e6) / 100, "fp64_warp_instr_per_neuron": 9.97},
-    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7",
-                   "traffic": 23.75e6 + (121.05e6 + 9.03e6) / 100, "warp_instr_per_neuron": 9.22},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b",
+                   "traffic": 23.74e6 + (121.02e6 + 9.66e6) / 100, "warp_instr_per_neuron": 9.22},
     # the fused block kernels (a network without synapses: a block of steps per
     # launch, state in registers), from the instruction mix of one 100-step
     # launch at 1M neurons (bench.py --case activity --case-steps 100), per
@@ -237,18 +237,18 @@ CAPTURED = {
     # SM) per cycle; DRAM read + write of that launch
     "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c", "fp64_warp_instr_per_neuron": 10.08,
                 "traffic": 50.07e6 + 3.92e6},
-    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.12e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.11e6},
     # the batched block kernel over the 128-network configuration (7.15M
     # neurons, bench.py --case ensemble --case-steps 100 --precision fp32):
     # warp instructions per neuron-step, DRAM read + write of the launch
-    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "warp_instr_per_neuron": 5.95,
-                   "traffic": 215.31e6 + 187.62e6},
+    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "warp_instr_per_neuron": 5.95,
+                   "traffic": 215.84e6 + 187.73e6},
     # the search snapshot at 1M (bench.py --case search; the excitatory pass,
     # 0.8M searches): lanes active per warp instruction, L1 / L2 hit rates of
     # the walk, DRAM bytes per search
-    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "3ba2b94c4a357fb7", "lanes_active": 19.85,
+    "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "290d6ed0479e64d4", "lanes_active": 19.85,
                  "l1_hit": 0.924, "l2_hit": 0.774, "dram_bytes_per_search": 681.0},
-    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6c53cbc16cda84e7", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
 }
 B200_SMS = 148
 # algorithmic memory of a fused block launch per neuron: reads enabled, spike
