@@ -562,15 +562,15 @@ __global__ void __launch_bounds__(BLOCK) k_activity(ActArgs A, const ActDesc* __
     }
 }
 
-// Calcium and the growth deltas of the last m steps (a chunk of one launch per
-// step) from the spike history: row j holds the spike flags of the chunk's
+// Calcium and the growth deltas of m steps (a chunk of one launch per step)
+// from the spike history: row row0 + j holds the spike flags of the chunk's
 // step j.  A neuron's calcium and growth read nothing but its own spike flags,
 // so they run here once per chunk with the state in registers instead of in
 // every step's launch; the operations and their order are those of one step
 // after the other, so the bits are the same.  A disabled neuron keeps its
 // calcium, and its deltas become d + 0 (as at each of its steps).
 template <int H, bool MULTI>
-__global__ void __launch_bounds__(256) k_calcium_growth(ActArgs A, uint32_t m) {
+__global__ void __launch_bounds__(256) k_calcium_growth(ActArgs A, uint32_t row0, uint32_t m) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) {
         return;
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(256) k_calcium_growth(ActArgs A, uint32_t m) {
         Nu nu;
         neuron_net<MULTI>(A, i, seed, local, nu);
         double ca = A.calcium[i];
-        const uint8_t* __restrict__ h = A.hist + i;
+        const uint8_t* __restrict__ h = A.hist + row0 * A.hist_stride + i;
         bool flat = false;
         if constexpr (H > 0) {
             if (A.uniform_target) {
@@ -1066,15 +1066,15 @@ void launch_activity_fp64(Ctx& c, uint32_t kstep, const uint8_t* fired_prev, uin
     }
 }
 
-// Calcium and growth of the last m steps of one launch per step.
-void launch_calcium_growth64(Ctx& c, uint32_t m) {
+// Calcium and growth of m steps of one launch per step (history rows row0 on).
+void launch_calcium_growth64(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st) {
     const ActArgs A = act64_args(c, 0, nullptr, nullptr);
     const unsigned grid = blocks_for(c.n, 256);
     const bool h10 = c.cfg.h_model == 10 && c.cfg.h_calcium == 10;
     if (c.multi()) {
-        (h10 ? k_calcium_growth<10, true> : k_calcium_growth<0, true>)<<<grid, 256, 0, c.stream>>>(A, m);
+        (h10 ? k_calcium_growth<10, true> : k_calcium_growth<0, true>)<<<grid, 256, 0, st>>>(A, row0, m);
     } else {
-        (h10 ? k_calcium_growth<10, false> : k_calcium_growth<0, false>)<<<grid, 256, 0, c.stream>>>(A, m);
+        (h10 ? k_calcium_growth<10, false> : k_calcium_growth<0, false>)<<<grid, 256, 0, st>>>(A, row0, m);
     }
     RL_LAUNCH_CHECK();
 }
@@ -1237,11 +1237,11 @@ void ensure_spike_hist(Ctx& c) {
     }
 }
 
-void launch_calcium_growth(Ctx& c, uint32_t m) {
+void launch_calcium_growth(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st) {
     if (is_fp32(c)) {
-        launch_calcium_growth32(c, m);
+        launch_calcium_growth32(c, row0, m, st);
     } else {
-        launch_calcium_growth64(c, m);
+        launch_calcium_growth64(c, row0, m, st);
     }
 }
 
@@ -1281,6 +1281,11 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
     const bool fused = c.step_fusion && c.graph.num_edges == 0 && nsteps > 1;
     if (!fused) {
         ensure_spike_hist(c);
+        if (nsteps > kGrowthChunk && c.growth_stream == nullptr) {
+            RL_CUDA_TRY(cudaStreamCreateWithFlags(&c.growth_stream, cudaStreamNonBlocking));
+            RL_CUDA_TRY(cudaEventCreateWithFlags(&c.growth_fork, cudaEventDisableTiming));
+            RL_CUDA_TRY(cudaEventCreateWithFlags(&c.growth_join, cudaEventDisableTiming));
+        }
     }
     // the launch shape is a shape of the per-step kernel: it is timed at the
     // first block that runs one launch per step (with the synapses it will
@@ -1294,12 +1299,33 @@ void run_activity_block(Ctx& c, uint32_t first_step, uint32_t nsteps) {
         drop_activity_graphs(c);
     }
     const bool graph = !fused && c.use_graphs && c.stream != nullptr && nsteps > 1 && nsteps == c.cfg.plasticity_interval;
-    // one launch per step, and calcium and growth of each chunk of kHistSteps
-    // steps from the spike history at the chunk's end
+    // One launch per step; calcium and growth of each chunk of kGrowthChunk
+    // steps from the spike history.  A chunk's calcium and growth go to the
+    // growth stream, after the chunk's steps, and run beside the next chunk's
+    // steps; the context's stream waits for them at the next chunk's end
+    // (the chunk after next reuses their history rows, and each chunk's
+    // calcium and growth continue the one before).  The last chunk's run on
+    // the context's stream after the growth stream's.
+    bool forked = false;
     auto step_and_growth = [&](uint32_t k) {
         launch_step(c, k);
-        if ((k + 1) % kHistSteps == 0 || k + 1 == nsteps) {
-            launch_calcium_growth(c, k % kHistSteps + 1);
+        if ((k + 1) % kGrowthChunk != 0 && k + 1 != nsteps) {
+            return;
+        }
+        const uint32_t row0 = (k - k % kGrowthChunk) % kHistSteps;
+        const uint32_t m = k % kGrowthChunk + 1;
+        if (forked) {
+            RL_CUDA_TRY(cudaEventRecord(c.growth_join, c.growth_stream));
+            RL_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.growth_join, 0));
+        }
+        if (k + 1 == nsteps) {
+            launch_calcium_growth(c, row0, m, c.stream);
+            forked = false;
+        } else {
+            RL_CUDA_TRY(cudaEventRecord(c.growth_fork, c.stream));
+            RL_CUDA_TRY(cudaStreamWaitEvent(c.growth_stream, c.growth_fork, 0));
+            launch_calcium_growth(c, row0, m, c.growth_stream);
+            forked = true;
         }
     };
     if (fused) {

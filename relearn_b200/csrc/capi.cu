@@ -750,6 +750,13 @@ void discard(Ctx* c) {
     if (c->stream) {
         cudaStreamSynchronize(c->stream);
     }
+    if (c->growth_stream) {
+        cudaStreamSynchronize(c->growth_stream);
+        cudaStreamDestroy(c->growth_stream);
+        cudaEventDestroy(c->growth_fork);
+        cudaEventDestroy(c->growth_join);
+        c->growth_stream = nullptr;
+    }
     for (cudaEvent_t e : { c->noalloc_before, c->noalloc_after }) {
         if (e) {
             cudaEventSynchronize(e);

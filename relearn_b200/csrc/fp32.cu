@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(BLOCK) k_activity_f32_steps(Act32 A, const Act
 // registers: the same function and order as step by step, so the same bits.
 // A disabled neuron keeps its calcium and deltas.
 template <bool MULTI>
-__global__ void __launch_bounds__(256) k_calcium_growth_f32(Act32 A, uint32_t m) {
+__global__ void __launch_bounds__(256) k_calcium_growth_f32(Act32 A, uint32_t row0, uint32_t m) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n || !A.enabled[i]) {
         return;
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(256) k_calcium_growth_f32(Act32 A, uint32_t m)
     const Grow32 G = grow32_of(A, A.target ? A.target[i] : 0.0f);
     double ca = A.calcium[i];
     float d[3] = { A.delta[0][i], A.delta[1][i], A.delta[2][i] };
-    const uint8_t* __restrict__ h = A.hist + i;
+    const uint8_t* __restrict__ h = A.hist + row0 * A.hist_stride + i;
 #pragma unroll 4
     for (uint32_t j = 0; j < m; ++j) {
         calcium_growth_f32(A, h[j * A.hist_stride], nu, G, ca, d);
@@ -1601,13 +1601,13 @@ void launch_activity_f32_steps(Ctx& c, uint32_t nsteps) {
     }
 }
 
-void launch_calcium_growth32(Ctx& c, uint32_t m) {
+void launch_calcium_growth32(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st) {
     const Act32 A = act32_args(c, 0, nullptr, nullptr);
     const unsigned grid = blocks_for(c.n, 256);
     if (c.multi()) {
-        k_calcium_growth_f32<true><<<grid, 256, 0, c.stream>>>(A, m);
+        k_calcium_growth_f32<true><<<grid, 256, 0, st>>>(A, row0, m);
     } else {
-        k_calcium_growth_f32<false><<<grid, 256, 0, c.stream>>>(A, m);
+        k_calcium_growth_f32<false><<<grid, 256, 0, st>>>(A, row0, m);
     }
     RL_LAUNCH_CHECK();
 }

@@ -200,12 +200,14 @@ struct NetInfo {
     QFrame frame;
 };
 
-// Steps whose calcium and growth one launch computes from the spike history
-// when the activity runs one launch per step.  A row of the history holds one
-// byte per neuron and is padded to a multiple of 16 bytes, so that a thread's
-// vector store of its V flags (V = 1, 2, 4 from a multiple of V) is aligned
-// in every row.
+// Rows of the spike history of one launch per step (row k % kHistSteps holds
+// the flags of the block's step k); calcium and growth are computed per chunk
+// of kGrowthChunk steps, the chunk before the last one beside the next
+// chunk's steps (their rows differ).  A row holds one byte per neuron and is
+// padded to a multiple of 16 bytes, so that a thread's vector store of its V
+// flags (V = 1, 2, 4 from a multiple of V) is aligned in every row.
 constexpr uint32_t kHistSteps = 128;
+constexpr uint32_t kGrowthChunk = 64;
 inline size_t hist_stride(uint32_t n) {
     return ((size_t)n + 15) / 16 * 16;
 }
@@ -356,6 +358,11 @@ struct Ctx {
     // direction, so that an upload never queues behind a snapshot).
     cudaStream_t copy_stream = nullptr;    // snapshots (device -> host)
     cudaStream_t upload_stream = nullptr;  // enabled flags (host -> device)
+    // calcium and growth of a chunk of one launch per step run here while the
+    // context's stream runs the next chunk's steps (fork and join events)
+    cudaStream_t growth_stream = nullptr;
+    cudaEvent_t growth_fork = nullptr;
+    cudaEvent_t growth_join = nullptr;
     DBuf<uint8_t> enabled_stage;
     cudaEvent_t upload_done = nullptr;   // the last upload reached the staging buffer
     cudaEvent_t stage_free = nullptr;    // the context's stream has consumed it
@@ -409,9 +416,9 @@ void clear_syn_in(Ctx& c);
 // The spike history of one launch per step (allocated before the first such
 // block), and calcium and growth of the last m steps from it.
 void ensure_spike_hist(Ctx& c);
-void launch_calcium_growth(Ctx& c, uint32_t m);
-void launch_calcium_growth64(Ctx& c, uint32_t m);
-void launch_calcium_growth32(Ctx& c, uint32_t m);
+void launch_calcium_growth(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st);
+void launch_calcium_growth64(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st);
+void launch_calcium_growth32(Ctx& c, uint32_t row0, uint32_t m, cudaStream_t st);
 // Blocks of an activity launch of variant v of `kernel`.
 unsigned act_grid(Ctx& c, const ActVariant& v, const void* kernel);
 
