@@ -40,11 +40,11 @@ PERIOD = 100
 # Algorithmic bytes per neuron-step of one launch per step (a network with
 # synapses, or step fusion off), FP64 SoA, one target calcium for all neurons:
 # the step kernel reads enabled 1 + x 8 + u 8 and writes x 8 + u 8 + spike
-# flag 1 + spike-history byte 1 = 35; calcium and growth of a 100-step chunk
-# (one launch) read each history byte (1) and read and write calcium 8 and
-# three deltas 24 once per chunk (64 / 100); the input (8) on the last step of
-# each block only.
-ACT_BYTES_PER_NEURON = 35 + 1 + (64 + 8) / 100
+# flag 1 + spike-history byte 1 = 35; calcium and growth (one launch per chunk
+# of up to 64 steps: two per 100-step block) read each history byte (1) and
+# read and write calcium 8 and three deltas 24 once per chunk (2 x 64 / 100);
+# the input (8) on the last step of each block only.
+ACT_BYTES_PER_NEURON = 35 + 1 + (2 * 64 + 8) / 100
 # With synapses: a block's first step pulls over the in-CSR (two row offsets 8
 # per neuron, source id 4 + weight 4 + spike flag 1 per in-edge); the other
 # steps read the pushed sum (8 B FP64, 4 B FP32) of every neuron (the pushes
@@ -216,18 +216,18 @@ def build_network(n, side, seed, placement):
 # captured again.
 CAPTURED = {
     # one launch per step at 1M neurons with synapses (bench.py --case
-    # plasticity --step-fusion 0, a launch of the second block): the step
-    # kernel's DRAM read + write per launch plus that of the chunk's calcium
-    # and growth launch per step (FP64 34.95 + 0.10 MB + (133.06 + 15.09) / 100
-    # MB; FP32 23.75 + 0.00 MB + (121.05 + 9.03) / 100 MB); FP64 warp
+    # plasticity --step-fusion 0, launches of the second block): the step
+    # kernel's DRAM read + write per launch plus that of a 64-step chunk's
+    # calcium and growth launch per step (FP64 34.95 + 0.11 MB + (97.04 +
+    # 7.33) / 64 MB; FP32 23.75 + 0.00 MB + (85.01 + 3.90) / 64 MB); FP64 warp
     # instructions per neuron-step of both (DMUL, DADD, DFMA, DSETP: 6.26 +
     # 3.72), and for the FP32 form warp instructions of every kind (7.98 +
-    # 1.24).  The FP64 pipe of an SM takes 2 warp instructions per cycle (64
+    # 1.36).  The FP64 pipe of an SM takes 2 warp instructions per cycle (64
     # lanes).
-    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c",
-                   "traffic": 34.95e6 + 0.10e6 + (133.06e6 + 15.09e6) / 100, "fp64_warp_instr_per_neuron": 9.97},
-    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b",
-                   "traffic": 23.74e6 + (121.02e6 + 9.66e6) / 100, "warp_instr_per_neuron": 9.22},
+    "activity64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "e6ef1fe863ecbbd9",
+                   "traffic": 34.95e6 + 0.11e6 + (97.04e6 + 7.33e6) / 64, "fp64_warp_instr_per_neuron": 9.97},
+    "activity32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "ae16ba4013f08c25",
+                   "traffic": 23.75e6 + (85.01e6 + 3.90e6) / 64, "warp_instr_per_neuron": 9.34},
     # the fused block kernels (a network without synapses: a block of steps per
     # launch, state in registers), from the instruction mix of one 100-step
     # launch at 1M neurons (bench.py --case activity --case-steps 100), per
@@ -235,20 +235,20 @@ CAPTURED = {
     # DADD 3.55, DFMA 1.82, DSETP 0.92); k_activity_f32_steps 5.85 warp
     # instructions of every kind, issued at one per SM sub-partition (4 per
     # SM) per cycle; DRAM read + write of that launch
-    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "1556593db39c3a9c", "fp64_warp_instr_per_neuron": 10.08,
-                "traffic": 50.07e6 + 3.92e6},
-    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.11e6},
+    "fused64": {"sources": ("activity.cu", "rl_math.cuh"), "digest": "e6ef1fe863ecbbd9", "fp64_warp_instr_per_neuron": 10.08,
+                "traffic": 50.06e6 + 4.06e6},
+    "fused32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "ae16ba4013f08c25", "warp_instr_per_neuron": 5.85, "traffic": 30.02e6 + 0.14e6},
     # the batched block kernel over the 128-network configuration (7.15M
     # neurons, bench.py --case ensemble --case-steps 100 --precision fp32):
     # warp instructions per neuron-step, DRAM read + write of the launch
-    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "warp_instr_per_neuron": 5.95,
-                   "traffic": 215.84e6 + 187.73e6},
+    "ensemble32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "ae16ba4013f08c25", "warp_instr_per_neuron": 5.95,
+                   "traffic": 215.10e6 + 187.94e6},
     # the search snapshot at 1M (bench.py --case search; the excitatory pass,
     # 0.8M searches): lanes active per warp instruction, L1 / L2 hit rates of
     # the walk, DRAM bytes per search
     "search64": {"sources": ("bh_search.cu", "bh_eval.cuh", "bh_wide.cuh", "rl_math.cuh"), "digest": "290d6ed0479e64d4", "lanes_active": 19.85,
                  "l1_hit": 0.924, "l2_hit": 0.774, "dram_bytes_per_search": 681.0},
-    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "6e5ad73249332e2b", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
+    "search32": {"sources": ("fp32.cu", "rl_math.cuh"), "digest": "ae16ba4013f08c25", "lanes_active": 21.88, "l1_hit": 0.812, "l2_hit": 0.936},
 }
 B200_SMS = 148
 # algorithmic memory of a fused block launch per neuron: reads enabled, spike
@@ -345,10 +345,10 @@ def step_compute(precision: int, n: int, step_us: float, sm_mhz=None) -> dict:
 
 
 # FP32: the step kernel reads enabled 1 + spike flag 1 + x 4 + u 4 and writes
-# x 4 + u 4 + spike flag 1 + history byte 1 = 20; the chunk's calcium and
+# x 4 + u 4 + spike flag 1 + history byte 1 = 20; the chunks' calcium and
 # growth read each history byte (1) and calcium 8 + three deltas 12, read and
-# written once per chunk (40 / 100); the input (4) on a block's last step
-ACT_BYTES_FP32 = 20 + 1 + (40 + 4) / 100
+# written once per chunk (2 x 40 / 100); the input (4) on a block's last step
+ACT_BYTES_FP32 = 20 + 1 + (2 * 40 + 4) / 100
 
 
 def measure_form(args, precision, dev, stream, world, pos, sig, params, clk=None):
@@ -662,8 +662,8 @@ def synapse_regime(args, dev, stream, world, precision):
                 "avg_launch_us": 1e3 * act_ms / act_cnt if act_cnt else None, "launches": act_cnt,
                 "bytes": f"{per_neuron:.2f} B per neuron-step + {ACT_BYTES_PUSHED[precision]} B pushed sum per neuron-step + per 100-step block "
                          f"{ACT_BYTES_CSR_ROW} B row offsets per neuron and {ACT_BYTES_PER_EDGE} B per in-edge",
-                "kernels": "the step kernel (k_activity / k_activity_f32, one launch per step) and the chunk's calcium and growth (k_calcium_growth / "
-                           "k_calcium_growth_f32, one launch per 100 steps)"}
+                "kernels": "the step kernel (k_activity / k_activity_f32, one launch per step) and the chunks' calcium and growth (k_calcium_growth / "
+                           "k_calcium_growth_f32, one launch per chunk of up to 64 steps)"}
     if act_cnt:
         comp = step_compute(precision, n, 1e3 * act_ms / act_cnt)
         act_roof["compute"] = comp
