@@ -517,10 +517,12 @@ void sort_new(Ctx& c, uint64_t* key, uint32_t* val, uint64_t m, int bits) {
 }  // namespace
 
 // Merges the new synapses into the sorted list and the out-CSR, drops the
-// entries deletions left at weight 0, and rebuilds both row-offset arrays.
+// entries deletions left at weight 0 once they may be an eighth of the list,
+// and rebuilds both row-offset arrays.
 void rebuild_graph(Ctx& c) {
     Graph& G = c.graph;
-    if (G.num_new == 0 && !G.zeros) {
+    const bool compact = G.zeros && G.zero_bound * 8 >= G.num_edges + G.num_new;
+    if (G.num_new == 0 && !compact) {
         return;
     }
     cudaStream_t st = c.stream;
@@ -569,7 +571,7 @@ void rebuild_graph(Ctx& c) {
         k_merge_out_new<<<blocks_for(mn, 256), 256, 0, st>>>(mn, nk.p, nv.p, G.out_perm.p, G.tgt.p, G.src.p, mo, bn, out.p);
         RL_LAUNCH_CHECK();
     }
-    if (G.zeros && m) {
+    if (compact && m) {
         // the entries deletions left at weight 0 go; the order stays
         DBuf<uint32_t> keep, epos, keep_out, opos, T2, S2, out2;
         DBuf<int32_t> W2;
@@ -603,7 +605,10 @@ void rebuild_graph(Ctx& c) {
     G.out_perm.swap(out);
     G.num_edges = m;
     G.num_new = 0;
-    G.zeros = false;
+    if (compact) {
+        G.zeros = false;
+        G.zero_bound = 0;
+    }
     G.offsets.ensure((size_t)n + 1);
     G.out_off.ensure((size_t)n + 1);
     k_row_offsets<<<blocks_for(m + 1, 256), 256, 0, st>>>(m, G.tgt.p, nullptr, n, G.offsets.p);
@@ -649,12 +654,14 @@ uint64_t run_deletion(Ctx& c, uint32_t step, int type) {
     unsigned long long deleted = 0;
     RL_CUDA_TRY(cudaMemcpyAsync(&deleted, d_cnt, sizeof(deleted), cudaMemcpyDeviceToHost, st));
     RL_CUDA_TRY(cudaStreamSynchronize(st));
-    // Entries whose weight reached zero stay until the next rebuild: a zero
-    // entry adds nothing to a neuron's input and is no synapse to a later
-    // deletion (a partner appears |weight| times), and the edge order and
-    // both CSRs stay valid meanwhile.
+    // Entries whose weight reached zero stay until a rebuild drops them (once
+    // they may be an eighth of the list): a zero entry adds nothing to a
+    // neuron's input and is no synapse to a later deletion (a partner appears
+    // |weight| times), and the edge order and both CSRs stay valid meanwhile;
+    // rl_get_edges aggregates pairs and leaves zero weights out.
     if (deleted) {
         G.zeros = true;
+        G.zero_bound += deleted;
     }
     return deleted;
 }

@@ -97,7 +97,12 @@ struct Graph {
     DBuf<uint32_t> new_tgt, new_src;
     DBuf<int32_t> new_w;
     uint64_t num_new = 0;
-    bool zeros = false;  // deletions left entries of weight 0 (dropped at the next rebuild)
+    bool zeros = false;  // deletions left entries of weight 0
+    // Deletions since the zero entries were last dropped (at least the number
+    // of zero entries).  A zero entry adds nothing to a pulled or pushed sum
+    // and is no partner to a deletion, so the rebuild drops them only once
+    // they may be an eighth of the list.
+    uint64_t zero_bound = 0;
 };
 
 struct Search {
