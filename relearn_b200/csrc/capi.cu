@@ -401,9 +401,14 @@ void plasticity_update(Ctx& c, uint32_t step) {
         // The octree update goes out before the host reads the counts, so that
         // the GPU works while the host waits; it is correct unless deletions
         // follow, which change vacant dendrites: then it runs again below
-        // (incrementally: only the leaves the deletions changed).
+        // (incrementally: only the leaves the deletions changed).  A network
+        // whose last update deleted synapses will most likely delete again
+        // (once synapses exist, every update deletes some), so there the
+        // update waits for the deletions and runs once.  Either way every
+        // changed leaf is reduced before the search, so the octree is the same.
         RL_CUDA_TRY(cudaMemcpyAsync(c.nr.update.p, c.nr.enabled.p, c.n, cudaMemcpyDeviceToDevice, c.stream));
-        {
+        const bool speculate = !c.deleted_last;
+        if (speculate) {
             PhaseScope ps(c, PH_TREE_UPDATE);
             update_tree(c);
         }
@@ -422,10 +427,11 @@ void plasticity_update(Ctx& c, uint32_t step) {
                 }
             }
         }
-        if (first < 3) {
+        if (first < 3 || !speculate) {
             PhaseScope ps(c, PH_TREE_UPDATE);
             update_tree(c);
         }
+        c.deleted_last = first < 3;
     }
     // Neurons::create_synapses: search from the committed vacant axons
     RL_CUDA_TRY(cudaMemcpyAsync(c.nr.search_vacant.p, c.nr.vacant[0].p, c.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c.stream));

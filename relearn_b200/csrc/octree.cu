@@ -443,9 +443,13 @@ struct ReduceArgs {
     double4* rec0;
     double4* rec1;
     uint32_t* arrive;
-    // incremental update: nodes to recompute, and the leaf counts of the last update
-    uint8_t* dirty;
-    uint32_t* level_dirty;  // per level: some node of the level is marked
+    // incremental update: nodes to recompute (a per-level list of the marked
+    // nodes: level l's at work[level_lo[l] ...], level_dirty[l] of them), and
+    // the leaf counts of the last update
+    uint32_t* dirty;
+    uint32_t* level_dirty;
+    uint32_t* work;
+    const uint32_t* level_lo;
     uint2* last;
     // leaf counts: vacant dendrites of the neurons that take part
     const uint8_t* enabled;
@@ -466,6 +470,16 @@ struct ReduceArgs {
     cudaGraphConditionalHandle cond;
     unsigned long long* level_runs;
 };
+
+// Marks node p for recomputation: the first mark of the update appends it to
+// its level's list (a node is on it at most once).
+__device__ __forceinline__ void mark_node(const ReduceArgs& A, int32_t p) {
+    if (atomicExch(&A.dirty[p], 1u) == 0u) {
+        const uint32_t l = topo_level(A.topo[p].y);
+        const uint32_t slot = atomicAdd(&A.level_dirty[l], 1u);
+        A.work[A.level_lo[l] + slot] = (uint32_t)p;
+    }
+}
 
 // Leaf pass of the incremental update (OctreeAlgorithm::update_leaf_nodes):
 // one thread per neuron; a leaf whose vacant counts differ from the last
@@ -492,23 +506,23 @@ __global__ void k_leaf_update(ReduceArgs A) {
     }
     const int32_t p = A.parent[leaf];
     if (p >= 0) {
-        A.dirty[p] = 1;
-        A.level_dirty[topo_level(A.topo[p].y)] = 1u;
+        mark_node(A, p);
         if (A.has_cond) {
             cudaGraphSetConditional(A.cond, 1u);  // some level has work: run the reductions
         }
     }
 }
 
-// One level of the bottom-up reduction: one thread per node of the level; a
-// node marked dirty is recomputed from its children (leaves refreshed by the
-// leaf pass, inner children by the previous launch, one level deeper), read in
-// octant order as the reference sums them (OctreeNodeUpdater::update_node),
-// and marks its parent.  Recomputing only the nodes above changed leaves gives
-// the same records as recomputing all.  The children of a node are contiguous,
-// so neighbouring threads read neighbouring records.  A level with no marked
-// node (most levels, most updates) returns at once; the grid strides over the
-// level so that such a launch stays a few blocks.
+// One level of the bottom-up reduction: one thread per marked node of the
+// level (the level's list, filled by the launch one level deeper or by the
+// leaf pass); a marked node is recomputed from its children (leaves refreshed
+// by the leaf pass, inner children by the previous launch, one level deeper),
+// read in octant order as the reference sums them
+// (OctreeNodeUpdater::update_node), and marks its parent.  Recomputing only
+// the nodes above changed leaves gives the same records as recomputing all,
+// and a node's record does not depend on the order of the list.  A level with
+// no marked node (most levels, most updates) returns at once; the grid strides
+// over the list, capped at a few blocks per SM.
 __device__ __forceinline__ void reduce_node(const ReduceArgs& A, uint32_t node);
 
 __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi, uint32_t level) {
@@ -516,13 +530,9 @@ __global__ void k_reduce_level(ReduceArgs A, uint32_t lo, uint32_t hi, uint32_t 
     if (A.level_runs && blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(A.level_runs, 1ull);
     }
-    if (!A.level_dirty[level]) {
-        return;
-    }
-    for (uint32_t node = lo + blockIdx.x * blockDim.x + threadIdx.x; node < hi; node += gridDim.x * blockDim.x) {
-        if (A.dirty[node]) {
-            reduce_node(A, node);
-        }
+    const uint32_t marked = A.level_dirty[level];  // at most hi - lo: each node is listed once
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < marked; t += gridDim.x * blockDim.x) {
+        reduce_node(A, A.work[lo + t]);
     }
 }
 
@@ -570,8 +580,7 @@ __device__ __forceinline__ void reduce_node(const ReduceArgs& A, uint32_t node) 
     }
     const int32_t p = A.parent[node];
     if (p >= 0) {
-        A.dirty[p] = 1;
-        A.level_dirty[topo_level(t.y) - 1u] = 1u;
+        mark_node(A, p);
     }
 }
 
@@ -707,7 +716,8 @@ void build_octree(Ctx& c, const double* h_xyz) {
     T.parent.alloc(m);
     T.meta.alloc(m);
     T.dirty.alloc(m);
-    RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m, st));
+    RL_CUDA_TRY(cudaMemsetAsync(T.dirty.p, 0, m * sizeof(uint32_t), st));
+    T.work.alloc(m);
     T.level_dirty.alloc(kMaxLevels + 2);
     T.level_runs.alloc(1);
     RL_CUDA_TRY(cudaMemsetAsync(T.level_runs.p, 0, sizeof(unsigned long long), st));
@@ -760,6 +770,8 @@ void build_octree(Ctx& c, const double* h_xyz) {
         hoff[l + 1] = hoff[l] + hcount[l];
     }
     T.level_off = hoff;
+    T.level_lo.alloc(hoff.size());
+    RL_CUDA_TRY(cudaMemcpyAsync(T.level_lo.p, T.level_off.data(), hoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     DBuf<uint32_t> level_off;
     level_off.alloc(hoff.size());
     RL_CUDA_TRY(cudaMemcpyAsync(level_off.p, hoff.data(), hoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -804,6 +816,8 @@ void update_tree(Ctx& c) {
     A.arrive = nullptr;
     A.dirty = T.dirty.p;
     A.level_dirty = T.level_dirty.p;
+    A.work = T.work.p;
+    A.level_lo = T.level_lo.p;
     A.last = T.last_counts.p;
     A.enabled = c.nr.enabled.p;
     A.update = c.nr.update.p;

@@ -46,8 +46,10 @@ struct Tree {
     DBuf<uint32_t> leaf_of;    // neuron -> node
     DBuf<uint32_t> morton;     // Morton rank -> neuron
     std::vector<uint32_t> level_off;  // host copy: nodes of level l are [level_off[l], level_off[l+1])
-    DBuf<uint8_t> dirty;        // nodes to recompute in the running update
-    DBuf<uint32_t> level_dirty; // per level: a node of the level is marked
+    DBuf<uint32_t> dirty;       // nodes to recompute in the running update
+    DBuf<uint32_t> level_dirty; // per level: nodes of the level marked so far (entries of `work`)
+    DBuf<uint32_t> work;        // marked nodes of level l at [level_off[l], level_off[l] + level_dirty[l])
+    DBuf<uint32_t> level_lo;    // device copy of level_off
     DBuf<unsigned long long> level_runs;  // level launches the captured update ran (counted on the device)
     unsigned long long level_runs_seen = 0;  // of those, already added to the launch count
     DBuf<uint2> last_counts;    // per neuron: leaf counts (exc, inh) of the last update
@@ -389,6 +391,7 @@ struct Ctx {
     cudaEvent_t noalloc_before = nullptr;
     cudaEvent_t noalloc_after = nullptr;
     bool no_searches = false;             // the update's commit left no vacant axon: the search has nothing to do
+    bool deleted_last = false;            // the last plasticity update deleted synapses
     rl_stats stats{};
     uint64_t launches = 0;     // kernels launched for this context
     int64_t device_bytes = 0;  // device memory held now
