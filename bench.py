@@ -680,7 +680,8 @@ def synapse_regime(args, dev, stream, world, precision):
            "timed_periods": args.steps, "edges": [edges_before, edges_after], "searches_per_update": searches / args.steps,
            "synapses_created_per_update": (s1["synapses_created"] - s0["synapses_created"]) / args.steps,
            "synapses_deleted_per_update": (s1["synapses_deleted"] - s0["synapses_deleted"]) / args.steps,
-           "phases_ms": {k: v[0] for k, v in phases.items()}, "activity_roofline": act_roof}
+           "phases_ms": {k: v[0] for k, v in phases.items()}, "activity_roofline": act_roof,
+           "period_ms": {"min": min(times), "median": float(np.median(times)), "max": max(times)}}
     if searches and search_ms > 0:
         tps = touched / searches if precision == 0 else None
         out["bh_searches_per_s"] = searches / (search_ms / 1e3)

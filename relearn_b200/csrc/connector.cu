@@ -532,18 +532,25 @@ void rebuild_graph(Ctx& c) {
     uint64_t m = mo + mn;
     RL_CHECK(m < 0xFFFFFFFFull, RL_ERR_OVERFLOW, "synapse count exceeds 2^32");
     const int bn = bits_for(n);
-    DBuf<uint32_t> T, S, out, pos, newpos;
-    DBuf<int32_t> W;
-    DBuf<uint64_t> nk;
-    DBuf<uint32_t> nv;
-    T.alloc(m ? m : 1);
-    S.alloc(m ? m : 1);
-    W.alloc(m ? m : 1);
-    out.alloc(m ? m : 1);
-    pos.alloc(mo ? mo : 1);
-    newpos.alloc(mn ? mn : 1);
-    nk.alloc(mn ? mn : 1);
-    nv.alloc(mn ? mn : 1);
+    // the working arrays persist in the graph, so that a rebuild allocates
+    // only when the list outgrows them; T, S, W and out become the graph's
+    // lists below, and the lists they replace are the next rebuild's arrays
+    DBuf<uint32_t>& T = G.m_tgt;
+    DBuf<uint32_t>& S = G.m_src;
+    DBuf<int32_t>& W = G.m_w;
+    DBuf<uint32_t>& out = G.m_out;
+    DBuf<uint32_t>& pos = G.m_pos;
+    DBuf<uint32_t>& newpos = G.m_newpos;
+    DBuf<uint64_t>& nk = G.m_nk;
+    DBuf<uint32_t>& nv = G.m_nv;
+    T.ensure(m ? m : 1);
+    S.ensure(m ? m : 1);
+    W.ensure(m ? m : 1);
+    out.ensure(m ? m : 1);
+    pos.ensure(mo ? mo : 1);
+    newpos.ensure(mn ? mn : 1);
+    nk.ensure(mn ? mn : 1);
+    nv.ensure(mn ? mn : 1);
     // list order: new entries by (target, source), merged behind equal old ones
     if (mn) {
         k_new_keys<<<blocks_for(mn, 256), 256, 0, st>>>(mn, G.new_tgt.p, G.new_src.p, nullptr, bn, nk.p, nv.p);

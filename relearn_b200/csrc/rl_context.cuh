@@ -105,6 +105,12 @@ struct Graph {
     // and is no partner to a deletion, so the rebuild drops them only once
     // they may be an eighth of the list.
     uint64_t zero_bound = 0;
+    // working arrays of the rebuild, kept between rebuilds (grown, never
+    // shrunk): the merged lists before they swap with the ones above, merge
+    // positions, and the keys and values of the new entries
+    DBuf<uint32_t> m_tgt, m_src, m_out, m_pos, m_newpos, m_nv;
+    DBuf<int32_t> m_w;
+    DBuf<uint64_t> m_nk;
 };
 
 struct Search {
