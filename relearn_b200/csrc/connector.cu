@@ -439,8 +439,8 @@ uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons) {
     k_group_heads<<<blocks_for(m, 256), 256, 0, st>>>(m, S.rank.p, S.flags.p);
     RL_LAUNCH_CHECK();
     // vacant dendrite counts before the connector
-    DBuf<uint32_t> before;
-    before.alloc(2 * (size_t)n);
+    DBuf<uint32_t>& before = S.vac_before;
+    before.ensure(2 * (size_t)n);
     RL_CUDA_TRY(cudaMemcpyAsync(before.p, c.nr.vacant[1].p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     RL_CUDA_TRY(cudaMemcpyAsync(before.p + n, c.nr.vacant[2].p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     AcceptArgs A;
@@ -465,8 +465,8 @@ uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons) {
     k_accept<<<blocks_for(m, 256), 256, 0, st>>>(A);
     RL_LAUNCH_CHECK();
     // compact accepted into the new-edge buffer (sorted-position order)
-    DBuf<uint32_t> pos;
-    pos.alloc(m);
+    DBuf<uint32_t>& pos = S.accept_pos;
+    pos.ensure(m);
     const uint64_t created = exclusive_scan_u32(S.accepted.p, pos.p, m, c.prim, st);
     const uint64_t need = G.num_new + created;
     if (need > G.new_tgt.n) {

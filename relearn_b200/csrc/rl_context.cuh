@@ -121,6 +121,8 @@ struct Search {
     DBuf<uint32_t> req_count;    // per neuron: valid requests
     DBuf<uint32_t> req_off;      // per neuron: output offset
     DBuf<uint32_t> req_tgt, req_src, req_j, req_sig;  // requests in (source, j) order
+    DBuf<uint32_t> vac_before;   // connector: vacant dendrite counts before it (exc, then inh)
+    DBuf<uint32_t> accept_pos;   // connector: output position of each accepted request
     DBuf<uint32_t> seg_starts;
     DBuf<uint32_t> tasks;    // persistent search form: task counter per signal type
     DBuf<uint32_t> seg_warp[2], seg_net[2];
