@@ -440,7 +440,7 @@ uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons) {
     RL_LAUNCH_CHECK();
     // vacant dendrite counts before the connector
     DBuf<uint32_t>& before = S.vac_before;
-    before.ensure(2 * (size_t)n);
+    before.fit(2 * (size_t)n);
     RL_CUDA_TRY(cudaMemcpyAsync(before.p, c.nr.vacant[1].p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     RL_CUDA_TRY(cudaMemcpyAsync(before.p + n, c.nr.vacant[2].p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     AcceptArgs A;
@@ -466,7 +466,7 @@ uint64_t run_connector(Ctx& c, uint32_t step, bool bind_axons) {
     RL_LAUNCH_CHECK();
     // compact accepted into the new-edge buffer (sorted-position order)
     DBuf<uint32_t>& pos = S.accept_pos;
-    pos.ensure(m);
+    pos.fit(m);
     const uint64_t created = exclusive_scan_u32(S.accepted.p, pos.p, m, c.prim, st);
     const uint64_t need = G.num_new + created;
     if (need > G.new_tgt.n) {
@@ -543,14 +543,14 @@ void rebuild_graph(Ctx& c) {
     DBuf<uint32_t>& newpos = G.m_newpos;
     DBuf<uint64_t>& nk = G.m_nk;
     DBuf<uint32_t>& nv = G.m_nv;
-    T.ensure(m ? m : 1);
-    S.ensure(m ? m : 1);
-    W.ensure(m ? m : 1);
-    out.ensure(m ? m : 1);
-    pos.ensure(mo ? mo : 1);
-    newpos.ensure(mn ? mn : 1);
-    nk.ensure(mn ? mn : 1);
-    nv.ensure(mn ? mn : 1);
+    T.fit(m ? m : 1);
+    S.fit(m ? m : 1);
+    W.fit(m ? m : 1);
+    out.fit(m ? m : 1);
+    pos.fit(mo ? mo : 1);
+    newpos.fit(mn ? mn : 1);
+    nk.fit(mn ? mn : 1);
+    nv.fit(mn ? mn : 1);
     // list order: new entries by (target, source), merged behind equal old ones
     if (mn) {
         k_new_keys<<<blocks_for(mn, 256), 256, 0, st>>>(mn, G.new_tgt.p, G.new_src.p, nullptr, bn, nk.p, nv.p);

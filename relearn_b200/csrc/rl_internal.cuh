@@ -145,6 +145,13 @@ struct DBuf {
             alloc(c);
         }
     }
+    // Capacity for `count` with an eighth of headroom, for arrays kept
+    // between calls whose size drifts a little from call to call.
+    void fit(size_t count) {
+        if (count > n || p == nullptr) {
+            alloc(count + count / 8);
+        }
+    }
     void release() {
         if (p) {
             if (g_bind.stream) {
