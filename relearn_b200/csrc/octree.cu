@@ -22,7 +22,11 @@
 #include "rl_context.cuh"
 #include "rl_math.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
+
+namespace cg = cooperative_groups;
 
 namespace rl {
 namespace {
@@ -472,12 +476,21 @@ struct ReduceArgs {
 };
 
 // Marks node p for recomputation: the first mark of the update appends it to
-// its level's list (a node is on it at most once).
+// its level's list (a node is on it at most once).  The lanes of a warp that
+// append to the same level take their slots with one atomic between them: in
+// an update that changes most leaves, every node of a level is appended, and
+// one counter per level would otherwise take an atomic per node.
 __device__ __forceinline__ void mark_node(const ReduceArgs& A, int32_t p) {
     if (atomicExch(&A.dirty[p], 1u) == 0u) {
         const uint32_t l = topo_level(A.topo[p].y);
-        const uint32_t slot = atomicAdd(&A.level_dirty[l], 1u);
-        A.work[A.level_lo[l] + slot] = (uint32_t)p;
+        const cg::coalesced_group appending = cg::coalesced_threads();
+        const cg::coalesced_group same_level = cg::labeled_partition(appending, l);
+        uint32_t base = 0;
+        if (same_level.thread_rank() == 0) {
+            base = atomicAdd(&A.level_dirty[l], same_level.size());
+        }
+        base = same_level.shfl(base, 0);
+        A.work[A.level_lo[l] + base + same_level.thread_rank()] = (uint32_t)p;
     }
 }
 
