@@ -548,6 +548,9 @@ def run_b200(args, world, rank, local):
     clocks = clk.summary()
     if main_prec == 0 and args.placement == "uniform" and m["roofline"]["kernel"] == "k_activity":
         m["roofline"]["fp64_pipe"] = fp64_pipe_roofline(m["roofline"], n, clocks.get("sm_mhz"))
+    if main_prec == 1 and args.placement == "uniform" and m["roofline"]["kernel"] == "k_activity_f32" and m["roofline"].get("avg_launch_us"):
+        # the FP32 step kernel (with its chunks' calcium and growth) against instruction issue
+        m["roofline"]["issue"] = step_compute(1, n, m["roofline"]["avg_launch_us"], clocks.get("sm_mhz"))
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
